@@ -1,0 +1,309 @@
+"""ctypes bindings for the C restatement (``_ref/liboracle.so``) and readers for
+the reference executable's ``oracle_dump`` / ``oracle_dump_neigh`` output.
+
+TEST INFRASTRUCTURE, NOT PRODUCT CODE.  Only the tests, the smoke check and
+the benchmark's CPU-baseline leg import this module, and only as the checker.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from typing import Optional
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF_DIR = os.path.join(HERE, "_ref")
+LIB_PATH = os.path.join(REF_DIR, "liboracle.so")
+REF_EXE = os.path.join(REF_DIR, "cac")
+REF_EXE_EAMFIX = os.path.join(REF_DIR, "cac_eamfix")
+
+_dp = C.POINTER(C.c_double)
+_i64p = C.POINTER(C.c_int64)
+_i32p = C.POINTER(C.c_int32)
+_i8p = C.POINTER(C.c_int8)
+
+
+class _State(C.Structure):
+    _fields_ = [("boxlo", C.c_double * 3), ("boxhi", C.c_double * 3),
+                ("natoms", C.c_int), ("nelements", C.c_int),
+                ("x", _dp), ("v", _dp), ("f", _dp),
+                ("nodex", _dp), ("nodev", _dp), ("nodef", _dp), ("gaussf", _dp),
+                ("mass", C.c_double)]
+
+
+class _List(C.Structure):
+    _fields_ = [("nsites", C.c_int), ("nentries", C.c_int64), ("offset", _i64p),
+                ("jidx", _i32p), ("jsite", _i32p), ("jkind", _i8p), ("img", _i8p)]
+
+
+class _Ev(C.Structure):
+    _fields_ = [("energy", C.c_double), ("virial", C.c_double * 6),
+                ("eatom", _dp), ("vatom", _dp), ("enode", _dp), ("vnode", _dp)]
+
+
+class _Eam(C.Structure):
+    _fields_ = [("nrho", C.c_int), ("nr", C.c_int), ("drho", C.c_double), ("dr", C.c_double),
+                ("cut", C.c_double), ("rhomax", C.c_double),
+                ("frho_spline", _dp), ("rhor_spline", _dp), ("z2r_spline", _dp)]
+
+
+_lib = None
+
+
+def build() -> None:
+    """Compile the restatement (and, where the reference tree exists, the reference)."""
+    subprocess.run(["make", "-s", "-C", HERE, "all"], check=True)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            subprocess.run(["make", "-s", "-C", HERE, "restatement"], check=True)
+        L = C.CDLL(LIB_PATH)
+        L.oracle_build_list.argtypes = [C.POINTER(_State), C.c_double, C.c_int, C.POINTER(_List)]
+        L.oracle_free_list.argtypes = [C.POINTER(_List)]
+        L.oracle_lj_compute.argtypes = [C.POINTER(_State), C.POINTER(_List), C.c_double,
+                                        C.c_double, C.c_double, C.POINTER(_Ev)]
+        L.oracle_eam_load_setfl.argtypes = [C.c_char_p, C.POINTER(_Eam)]
+        L.oracle_eam_free.argtypes = [C.POINTER(_Eam)]
+        L.oracle_eam_compute.argtypes = [C.POINTER(_State), C.POINTER(_List), C.POINTER(_Eam),
+                                         C.POINTER(_Ev), _dp, _dp]
+        L.oracle_compute_nodef.argtypes = [C.POINTER(_State)]
+        L.oracle_nve_initial.argtypes = [C.POINTER(_State), C.c_double]
+        L.oracle_nve_final.argtypes = [C.POINTER(_State), C.c_double]
+        L.oracle_pbc.argtypes = [C.POINTER(_State)]
+        L.oracle_run_nve.argtypes = [C.POINTER(_State), C.c_int, C.c_double, C.c_double,
+                                     C.c_double, C.POINTER(_Eam), C.c_double, C.c_double,
+                                     C.c_int, C.c_int]
+        L.oracle_shape_array.argtypes = [_dp]
+        L.oracle_gauss_tables.argtypes = [C.POINTER(C.c_int), C.POINTER(C.c_int), _dp, _dp]
+        L.oracle_inverse_mass_hex.argtypes = [_dp]
+        _lib = L
+    return _lib
+
+
+def _ptr(a: np.ndarray):
+    return a.ctypes.data_as(_dp)
+
+
+class OracleState:
+    """Owns contiguous float64 copies of a system's arrays."""
+
+    def __init__(self, system):
+        self.x = np.ascontiguousarray(system.x, dtype=np.float64).copy()
+        self.v = np.ascontiguousarray(system.v, dtype=np.float64).copy()
+        self.nodex = np.ascontiguousarray(system.nodex, dtype=np.float64).copy()
+        self.nodev = np.ascontiguousarray(system.nodev, dtype=np.float64).copy()
+        self.f = np.zeros_like(self.x)
+        self.nodef = np.zeros_like(self.nodex)
+        self.gaussf = np.zeros_like(self.nodex)
+        self.boxlo = np.array(system.boxlo, dtype=np.float64)
+        self.boxhi = np.array(system.boxhi, dtype=np.float64)
+        self.mass = float(system.mass)
+        self._s = _State()
+        self._s.boxlo[:] = list(self.boxlo)
+        self._s.boxhi[:] = list(self.boxhi)
+        self._s.natoms = self.x.shape[0]
+        self._s.nelements = self.nodex.shape[0]
+        for name in ("x", "v", "f", "nodex", "nodev", "nodef", "gaussf"):
+            setattr(self._s, name, _ptr(getattr(self, name)))
+        self._s.mass = self.mass
+
+    @property
+    def ref(self):
+        return C.byref(self._s)
+
+
+class NeighList:
+    def __init__(self, offset, jkind, jidx, jsite, img):
+        self.offset, self.jkind, self.jidx, self.jsite, self.img = offset, jkind, jidx, jsite, img
+
+    @property
+    def nsites(self):
+        return len(self.offset) - 1
+
+    def canonical(self, natoms: int):
+        """Sorted int64 rows (i_site, kind, idx, site, sx, sy, sz)."""
+        counts = np.diff(self.offset)
+        isite = np.repeat(np.arange(self.nsites, dtype=np.int64), counts)
+        rows = np.stack([isite, self.jkind.astype(np.int64), self.jidx.astype(np.int64),
+                         self.jsite.astype(np.int64), self.img[:, 0].astype(np.int64),
+                         self.img[:, 1].astype(np.int64), self.img[:, 2].astype(np.int64)], axis=1)
+        order = np.lexsort(rows.T[::-1])
+        return rows[order]
+
+
+def build_list(state: OracleState, cutneigh: float, half: bool) -> NeighList:
+    L = _List()
+    rc = lib().oracle_build_list(state.ref, cutneigh, 1 if half else 0, C.byref(L))
+    if rc:
+        raise RuntimeError(f"oracle_build_list failed ({rc})")
+    n = L.nentries
+    ns = L.nsites
+    out = NeighList(
+        np.ctypeslib.as_array(L.offset, shape=(ns + 1,)).copy(),
+        np.ctypeslib.as_array(L.jkind, shape=(max(n, 1),))[:n].copy(),
+        np.ctypeslib.as_array(L.jidx, shape=(max(n, 1),))[:n].copy(),
+        np.ctypeslib.as_array(L.jsite, shape=(max(n, 1),))[:n].copy(),
+        np.ctypeslib.as_array(L.img, shape=(max(n, 1) * 3,))[:3 * n].reshape(n, 3).copy())
+    out._c = L
+    return out
+
+
+def _c_list(nl: NeighList) -> _List:
+    return nl._c
+
+
+def free_list(nl: NeighList) -> None:
+    if getattr(nl, "_c", None) is not None:
+        lib().oracle_free_list(C.byref(nl._c))
+        nl._c = None
+
+
+class EvResult:
+    def __init__(self, natoms, nelements):
+        self.eatom = np.zeros(natoms)
+        self.vatom = np.zeros((natoms, 6))
+        self.enode = np.zeros((nelements, 8))
+        self.vnode = np.zeros((nelements, 8, 6))
+        self._ev = _Ev()
+        self._ev.eatom = _ptr(self.eatom)
+        self._ev.vatom = _ptr(self.vatom)
+        self._ev.enode = _ptr(self.enode)
+        self._ev.vnode = _ptr(self.vnode)
+
+    @property
+    def energy(self):
+        return self._ev.energy
+
+    @property
+    def virial(self):
+        return np.array(list(self._ev.virial))
+
+
+def lj_forces(state: OracleState, half_list: NeighList, eps: float, sigma: float, cut: float):
+    ev = EvResult(state.x.shape[0], state.nodex.shape[0])
+    lib().oracle_lj_compute(state.ref, C.byref(half_list._c), eps, sigma, cut, C.byref(ev._ev))
+    lib().oracle_compute_nodef(state.ref)
+    return ev
+
+
+class Eam:
+    def __init__(self, path: str):
+        self._e = _Eam()
+        rc = lib().oracle_eam_load_setfl(path.encode(), C.byref(self._e))
+        if rc:
+            raise RuntimeError(f"cannot read setfl {path} ({rc})")
+
+    @property
+    def cut(self):
+        return self._e.cut
+
+    def __del__(self):
+        try:
+            lib().oracle_eam_free(C.byref(self._e))
+        except Exception:
+            pass
+
+
+def eam_forces(state: OracleState, half_list: NeighList, eam: Eam):
+    ev = EvResult(state.x.shape[0], state.nodex.shape[0])
+    rho_a = np.zeros(state.x.shape[0])
+    rho_n = np.zeros((state.nodex.shape[0], 8))
+    lib().oracle_eam_compute(state.ref, C.byref(half_list._c), C.byref(eam._e), C.byref(ev._ev),
+                             _ptr(rho_a), _ptr(rho_n))
+    lib().oracle_compute_nodef(state.ref)
+    ev.rho_atom, ev.rho_node = rho_a, rho_n
+    return ev
+
+
+def run_nve(state: OracleState, pair: str, *, lj=None, eam: Optional[Eam] = None,
+            skin: float = 1.0, dt: float = 0.001, nsteps: int = 10, every: int = 10) -> None:
+    if pair == "lj":
+        eps, sig, cut = lj
+        rc = lib().oracle_run_nve(state.ref, 0, eps, sig, cut, None, skin, dt, nsteps, every)
+    else:
+        rc = lib().oracle_run_nve(state.ref, 1, 0.0, 0.0, 0.0, C.byref(eam._e), skin, dt, nsteps, every)
+    if rc:
+        raise RuntimeError("oracle_run_nve failed")
+
+
+# ------------------------------------------------------- reference read-outs
+
+def read_dump(path: str) -> dict:
+    """Parse ``oracle_dump`` output: atoms sorted by tag, nodes by (tag, node)."""
+    out = {}
+    with open(path) as f:
+        lines = f.read().splitlines()
+    i = 0
+    while i < len(lines):
+        ln = lines[i]
+        if ln.startswith("#"):
+            i += 1
+            continue
+        w = ln.split()
+        if w[0] == "step":
+            out["step"] = int(w[1])
+        elif w[0] == "box":
+            out["box"] = np.array([float(t) for t in w[1:]])
+        elif w[0] == "natoms":
+            out["natoms"], out["nelements"] = int(w[1]), int(w[3])
+        elif w[0] == "energy":
+            out["energy"] = float(w[1])
+        elif w[0] == "virial":
+            out["virial"] = np.array([float(t) for t in w[1:]])
+        elif w[0] == "atoms":
+            n = out["natoms"]
+            a = np.array([[float(t) for t in lines[i + 1 + k].split()] for k in range(n)]).reshape(n, 17)
+            out["atoms"] = a
+            i += n
+        elif w[0] == "nodes":
+            n = out["nelements"] * 8
+            a = np.array([[float(t) for t in lines[i + 1 + k].split()] for k in range(n)]).reshape(n, 21)
+            out["nodes"] = a
+            i += n
+        i += 1
+    a = out["atoms"]
+    out["x"], out["v"], out["f"] = a[:, 1:4], a[:, 4:7], a[:, 7:10]
+    out["eatom"], out["vatom"] = a[:, 10], a[:, 11:17]
+    nd = out["nodes"]
+    ne = out["nelements"]
+    out["nodex"] = nd[:, 2:5].reshape(ne, 8, 3)
+    out["nodev"] = nd[:, 5:8].reshape(ne, 8, 3)
+    out["nodef"] = nd[:, 8:11].reshape(ne, 8, 3)
+    out["gaussf_at_node"] = nd[:, 11:14].reshape(ne, 8, 3)
+    out["enode"] = nd[:, 14].reshape(ne, 8)
+    out["vnode"] = nd[:, 15:21].reshape(ne, 8, 6)
+    return out
+
+
+def read_neigh(path: str, natoms: int) -> np.ndarray:
+    """Parse ``oracle_dump_neigh`` output into sorted int64 rows
+    (i_site, kind, idx, site, sx, sy, sz) in the restatement's numbering:
+    atoms by tag-1, Gauss points at natoms + 8*(etag-1) + igcell."""
+    rows = []
+    cur = None
+    with open(path) as f:
+        for ln in f:
+            if ln[0] == "I":
+                _, kind, tag, site, _n = ln.split()
+                kind, tag, site = int(kind), int(tag), int(site)
+                cur = tag - 1 if kind == 0 else natoms + 8 * (tag - 1) + site
+            elif ln[0] == "J":
+                _, kind, tag, site, sx, sy, sz = ln.split()
+                rows.append((cur, int(kind), int(tag) - 1, int(site), int(sx), int(sy), int(sz)))
+    a = np.array(rows, dtype=np.int64).reshape(-1, 7)
+    order = np.lexsort(a.T[::-1])
+    return a[order]
+
+
+def run_reference(workdir: str, script: str, exe: str = REF_EXE, timeout: float = 3600.0) -> str:
+    """Run the reference executable on ``script`` (a file in ``workdir``)."""
+    r = subprocess.run([exe, "-in", script], cwd=workdir, capture_output=True, text=True,
+                       timeout=timeout)
+    if r.returncode != 0:
+        raise RuntimeError(f"reference run failed ({r.returncode}):\n{r.stdout[-3000:]}\n{r.stderr[-3000:]}")
+    return r.stdout
