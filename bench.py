@@ -1,0 +1,342 @@
+#!/usr/bin/env python
+"""Benchmark of the CAC per-timestep force path on B200.
+
+Workload (default): the EAM system at scale -- 1,049,760 atoms (162 atomic
+layers) between two coarse regions of 20,000 8-node elements (9 lattice sites
+per edge, 2x2x2 Gauss points), 1,209,760 atom+IP sites; analytic EAM tabulated
+to 10,000 points, cutoff 5.0 A, skin 1.0 A, list rebuilt every 10 steps,
+velocity Verlet at dt = 1 fs from 300 K Maxwell-Boltzmann velocities; FP64.
+Seeded synthetic input (no dataset exists for this path).
+
+One step = one velocity-Verlet timestep of the whole system (force evaluation
+with both EAM passes, nodal assembly, integration; a list rebuild every 10th
+step).  value = atom+IP sites x steps / device time (max over ranks).
+
+``--gpus N`` (launched under torchrun) runs N independent replicas, one per
+GPU, with no collective on the data path ("replicas only"); value is the sum.
+
+``--impl reference`` times the CAC reference's own CPU path (oracle/_ref/cac,
+built from the reference sources with a single-rank MPI stand-in; one core)
+on the same workload: ``run W`` then ``run K``, rate from its "Loop time".
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "atom+IP-steps/s"
+UNIT = "atom+IP-steps/s"
+REF_EXE = os.path.join(ROOT, "oracle", "_ref", "cac")
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def build_workload(name: str, seed: int):
+    from cac_b200 import gen
+    if name == "eam_1m":
+        return gen.eam_1m(seed=seed), "eam"
+    if name == "lj_small":
+        return gen.lj_small(seed=seed), "lj"
+    if name == "eam_4m_strained":
+        return gen.eam_4m_strained(seed=seed), "eam"
+    raise SystemExit(f"unknown workload {name}")
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.samples = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.FIELDS,
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True,
+                                     timeout=5).stdout.strip()
+                if out:
+                    self.samples.append(out.split(", "))
+            except Exception:
+                pass
+            self._stop.wait(0.1)
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        sm = sorted(float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit())
+        mx = max(float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit())
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for s in self.samples for k in range(4)
+                          if len(s) > 5 + k and s[5 + k].strip().lower() == "active"})
+        return {"sm_mhz": sm[len(sm) // 2] if sm else None, "sm_max_mhz": mx, "reasons": reasons,
+                "samples": len(self.samples)}
+
+
+def dist_init():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    if ws <= 1:
+        return 0, 0, 1, None
+    import torch
+    import torch.distributed as dist
+    from datetime import timedelta
+    rank = int(os.environ["RANK"])
+    local = int(os.environ.get("LOCAL_RANK", rank))
+    torch.cuda.set_device(local)
+    dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
+    return rank, local, ws, dist
+
+
+# ----------------------------------------------------------------- reference arm
+
+def run_reference(workload: str, steps: int, warmup: int, seed: int = 2, timeout: float = 1800.0):
+    """Time the reference executable: `run warmup` then `run steps`; returns
+    (units per step, loop seconds of the timed run, log)."""
+    from cac_b200 import gen
+    s, pair = build_workload(workload, seed)
+    with tempfile.TemporaryDirectory() as d:
+        gen.write_data(s, os.path.join(d, "data.cac"))
+        lines = ["units metal", "dimension 3", "boundary p p p", "atom_style atomic",
+                 "element_style cac 8 1 wscale 1 1 1 1", "read_data data.cac"]
+        if pair == "eam":
+            gen.write_setfl(gen.EamParams(), os.path.join(d, "cu.setfl"))
+            lines += ["pair_style eam/alloy", "pair_coeff * * cu.setfl Cu"]
+        else:
+            lines += ["pair_style lj/cut 5.5", "pair_coeff 1 1 0.4093 2.338"]
+        lines += ["neighbor 1.0 bin", "neigh_modify every 10 delay 0 check no", "timestep 0.001",
+                  "fix 1 all nve", "thermo 1000000"]
+        if warmup > 0:
+            lines.append(f"run {warmup}")
+        lines.append(f"run {steps}")
+        with open(os.path.join(d, "in.cac"), "w") as f:
+            f.write("\n".join(lines) + "\n")
+        r = subprocess.run([REF_EXE, "-in", "in.cac"], cwd=d, capture_output=True, text=True, timeout=timeout)
+        if r.returncode != 0:
+            raise RuntimeError("reference run failed: " + r.stdout[-2000:] + r.stderr[-2000:])
+        loops = re.findall(r"Loop time of ([0-9.eE+-]+) on", r.stdout)
+        return s.nsites, float(loops[-1]), r.stdout
+
+
+def reference_arm(args, rank, ws):
+    if rank != 0:
+        return
+    if not os.path.exists(REF_EXE):
+        print(json.dumps({"impl": "reference", "unavailable": "reference executable oracle/_ref/cac was not built"}))
+        return
+    units, secs, _ = run_reference(args.workload, args.steps, args.warmup)
+    value = units * args.steps / secs
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * secs / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded generator)",
+        "config": {"workload": args.workload, "sites": units, "pair": "eam/alloy" if "eam" in args.workload else "lj/cut",
+                   "precision": "fp64", "parallelism": "1 core (reference CPU path, single MPI rank)"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "reference",
+                         "sample": f"full workload, run {args.warmup} then run {args.steps} steps; rate from Loop time"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+# ----------------------------------------------------------------- b200 arm
+
+def alg_bytes_per_site(kernel: str) -> int:
+    """Compulsory state traffic per site and launch (FP64): what the kernel
+    must read and write at minimum, independent of the list representation."""
+    return {
+        "eam_force": 24 + 8 + 24,     # read x, F'; write f
+        "eam_rho": 24 + 8,            # read x; write rho
+        "pair_lj": 24 + 24,           # read x; write f
+        "nve_initial": 72 + 48,       # read x, v, f; write x, v
+        "nve_final": 48 + 24,         # read v, f; write v
+    }.get(kernel, 0)
+
+
+def b200_arm(args, rank, local, ws, dist):
+    import numpy as np
+    import torch
+    from cac_b200 import api, gen
+
+    seed = 2 + rank
+    s, pair = build_workload(args.workload, seed)
+    units = s.nsites
+    eng = api.Engine(local)
+    eng.upload(s)
+    tmp = tempfile.mkdtemp()
+    if pair == "eam":
+        p = os.path.join(tmp, "cu.setfl")
+        gen.write_setfl(gen.EamParams(), p)
+        eng.pair_eam(p)
+    else:
+        eng.pair_lj(0.4093, 2.338, 5.5)
+    eng.set_precision(api.MIXED if args.form == "mixed" else api.FP64)
+    eng.neighbor(1.0, 10)
+    eng.setup()
+    stream = torch.cuda.ExternalStream(eng.stream, device=torch.device("cuda", local))
+
+    eng.run_nve(args.warmup, 0.001)
+    torch.cuda.synchronize(local)
+    if dist:
+        dist.barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        torch.cuda.synchronize(local)
+        if dist:
+            dist.barrier()
+        e0.record(stream)
+        eng.run_nve(args.steps, 0.001)
+        e1.record(stream)
+        torch.cuda.synchronize(local)
+        if dist:
+            dist.barrier()
+    ms = e0.elapsed_time(e1)
+    ms_max = ms
+    if dist:
+        t = torch.tensor([ms], device=torch.device("cuda", local))
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_max = float(t.item())
+    value = units * args.steps * ws / (ms_max / 1000.0)
+
+    # per-kernel device times (CUDA events around every launch) for the roofline
+    eng.profile(True)
+    eng.run_nve(max(20, min(args.steps, 100)), 0.001)
+    prof = eng.profile_read()
+    eng.profile(False)
+    timed = {k: v for k, v in prof.items() if alg_bytes_per_site(k) > 0}
+    top = max(prof.items(), key=lambda kv: kv[1][0])
+    dom = max(timed.items(), key=lambda kv: kv[1][0]) if timed else top
+    avg_ms = dom[1][0] / max(dom[1][1], 1)
+    nsi = units
+    alg = alg_bytes_per_site(dom[0]) * nsi
+    hbm, hbm_kind = peaks()
+    achieved = alg / (avg_ms / 1000.0) / 1e9
+    launches_per_step = sum(v[1] for v in prof.values()) / max(20, min(args.steps, 100))
+
+    # end to end through the C ABI with pinned host buffers: every step copies the
+    # state in (x, v, nodes), runs one step, and reads the state back
+    x_h = torch.empty((s.natoms, 3), dtype=torch.float64).pin_memory().numpy()
+    v_h = torch.empty((s.natoms, 3), dtype=torch.float64).pin_memory().numpy()
+    nx_h = torch.empty((s.nelements, 8, 3), dtype=torch.float64).pin_memory().numpy()
+    nv_h = torch.empty((s.nelements, 8, 3), dtype=torch.float64).pin_memory().numpy()
+    x0, v0, nx0, nv0 = eng.state()
+    x_h[:] = x0
+    v_h[:] = v0
+    nx_h[:] = nx0
+    nv_h[:] = nv0
+    k_e2e = max(5, min(args.steps, 50))
+    import ctypes as C
+    _p = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))
+    torch.cuda.synchronize(local)
+    t0 = time.perf_counter()
+    for _ in range(k_e2e):
+        eng._check(eng.lib.cacb200_set_state(eng.h, _p(x_h), _p(v_h), _p(nx_h), _p(nv_h)), "set_state")
+        eng.run_nve(1, 0.001)
+        eng._check(eng.lib.cacb200_get_state(eng.h, _p(x_h), _p(v_h), _p(nx_h), _p(nv_h)), "get_state")
+    e2e_s = time.perf_counter() - t0
+    if dist:
+        t = torch.tensor([e2e_s], device=torch.device("cuda", local))
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e_value = units * k_e2e * ws / e2e_s
+    bytes_state = 8 * (6 * s.natoms + 48 * s.nelements)
+
+    # CPU baseline: the reference on a bounded sample of the same workload
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        if os.path.exists(REF_EXE):
+            try:
+                cu, secs, _ = run_reference(args.workload, 10, 0)
+                cpu = {"value": cu * 10 / secs, "unit": UNIT, "cores": 1, "kind": "reference",
+                       "sample": "reference executable on the same workload, 10 steps incl. one list rebuild, "
+                                 "rate from its Loop time (setup excluded)"}
+            except Exception as ex:  # reported, not fatal
+                cpu = {"value": None, "unit": UNIT, "cores": 1, "kind": "reference", "sample": f"failed: {ex}"}
+        else:
+            cpu = {"value": None, "unit": UNIT, "cores": 1, "kind": "reference",
+                   "sample": "reference executable not built on this host"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.form == "fp64" else "f32/f64",
+            "data": "synthetic (seeded generator; no dataset exists for this path)",
+            "config": {"workload": args.workload, "sites": units, "atoms": s.natoms, "elements": s.nelements,
+                       "pair": "eam/alloy" if pair == "eam" else "lj/cut", "precision": args.form,
+                       "rebuild_every": 10, "parallelism": f"replicas x{ws} (no data-path collective)",
+                       "l2": "working set larger than L2 (site table + lists > 126 MB)"},
+            "roofline": {"bound": "hbm", "kernel": dom[0], "achieved": achieved, "peak": hbm,
+                         "peak_kind": hbm_kind, "unit": "GB/s", "frac": achieved / hbm, "traffic": None,
+                         "avg_launch_ms": avg_ms, "alg_bytes_per_launch": alg},
+            "kernels_ms_per_step": {k: v[0] / max(v[1], 1) for k, v in sorted(prof.items())},
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": bytes_state,
+                    "d2h_bytes_per_step": bytes_state, "steps": k_e2e},
+            "gpu_launches": int(round(launches_per_step * args.steps)),
+            "clocks": clk.summary(),
+        }
+        print(json.dumps(line))
+    eng.close()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=500)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--workload", default="eam_1m")
+    ap.add_argument("--form", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    rank, local, ws, dist = dist_init()
+    try:
+        if args.impl == "reference":
+            if args.steps > 50:
+                args.steps = 20     # ~2 s per reference step at this size
+            if args.warmup > 5:
+                args.warmup = 3
+            reference_arm(args, rank, ws)
+        else:
+            b200_arm(args, rank, local, ws, dist)
+    finally:
+        if dist:
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,284 @@
+"""Python host layer over the C ABI of ``libcacb200.so`` (declared in
+``include/cacb200.h``).
+
+It mirrors the reference's style commands for the per-timestep path:
+
+    pair_style lj/cut/b200 CUT ; pair_coeff 1 1 EPS SIGMA  -> Engine.pair_lj
+    pair_style eam/alloy/b200 ; pair_coeff * * FILE El     -> Engine.pair_eam
+    neighbor SKIN bin ; neigh_modify every N delay 0 check no -> Engine.neighbor
+    fix ID all nve/b200 ; run N                            -> Engine.run_nve
+
+There is no CPU fallback: without the library or a CUDA device every call
+raises ``CacB200Error``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Optional
+
+import numpy as np
+
+from . import build as _build
+
+ENERGY_GLOBAL = 1
+ENERGY_ATOM = 2
+VIRIAL_GLOBAL = 1
+VIRIAL_ATOM = 4
+FP64 = 0
+MIXED = 1
+
+_dp = C.POINTER(C.c_double)
+
+
+class CacB200Error(RuntimeError):
+    pass
+
+
+_lib = None
+
+# (name, restype, argtypes) of every entry point in include/cacb200.h
+SIGNATURES = [
+    ("cacb200_ctx_create", C.c_int, [C.c_int, C.POINTER(C.c_void_p)]),
+    ("cacb200_ctx_destroy", C.c_int, [C.c_void_p]),
+    ("cacb200_last_error", C.c_char_p, [C.c_void_p]),
+    ("cacb200_stream", C.c_void_p, [C.c_void_p]),
+    ("cacb200_set_precision", C.c_int, [C.c_void_p, C.c_int]),
+    ("cacb200_upload_system", C.c_int, [C.c_void_p, _dp, _dp, C.c_int, _dp, _dp, C.c_int, _dp, _dp, C.c_double]),
+    ("cacb200_set_state", C.c_int, [C.c_void_p, _dp, _dp, _dp, _dp]),
+    ("cacb200_get_state", C.c_int, [C.c_void_p, _dp, _dp, _dp, _dp]),
+    ("cacb200_get_forces", C.c_int, [C.c_void_p, _dp, _dp, _dp]),
+    ("cacb200_get_energy", C.c_int, [C.c_void_p, _dp, _dp, _dp, _dp, _dp, _dp]),
+    ("cacb200_counts", C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    ("cacb200_set_lj", C.c_int, [C.c_void_p, C.c_double, C.c_double, C.c_double]),
+    ("cacb200_set_eam", C.c_int, [C.c_void_p, C.c_int, C.c_double, C.c_int, C.c_double, C.c_double, _dp, _dp, _dp]),
+    ("cacb200_set_nodal_energy_weight", C.c_int, [C.c_void_p, C.c_double]),
+    ("cacb200_set_neighbor", C.c_int, [C.c_void_p, C.c_double, C.c_int]),
+    ("cacb200_build_lists", C.c_int, [C.c_void_p, C.c_int]),
+    ("cacb200_list_size", C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int64), C.POINTER(C.c_int)]),
+    ("cacb200_get_list", C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int64), C.POINTER(C.c_int8),
+                                   C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_int8)]),
+    ("cacb200_interpolate", C.c_int, [C.c_void_p]),
+    ("cacb200_compute_pair", C.c_int, [C.c_void_p, C.c_int, C.c_int]),
+    ("cacb200_assemble_nodef", C.c_int, [C.c_void_p]),
+    ("cacb200_compute_forces", C.c_int, [C.c_void_p, C.c_int, C.c_int]),
+    ("cacb200_nve_initial", C.c_int, [C.c_void_p, C.c_double]),
+    ("cacb200_nve_final", C.c_int, [C.c_void_p, C.c_double]),
+    ("cacb200_setup", C.c_int, [C.c_void_p]),
+    ("cacb200_run_nve", C.c_int, [C.c_void_p, C.c_int, C.c_double, C.c_int, C.c_int]),
+    ("cacb200_profile", C.c_int, [C.c_void_p, C.c_int]),
+    ("cacb200_profile_read", C.c_int, [C.c_void_p, C.c_int, C.c_char_p, _dp, C.POINTER(C.c_int64),
+                                       C.POINTER(C.c_int)]),
+]
+
+
+def library_path() -> str:
+    return _build.LIB
+
+
+def load(build_if_missing: bool = True):
+    """Load ``libcacb200.so`` (building it with nvcc when missing or stale)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if build_if_missing and _build.needs_build():
+        _build.build()
+    if not os.path.exists(_build.LIB):
+        raise CacB200Error("libcacb200.so is not built")
+    lib = C.CDLL(_build.LIB)
+    for name, res, args in SIGNATURES:
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def _p(a: Optional[np.ndarray]):
+    if a is None:
+        return None
+    assert a.dtype == np.float64 and a.flags.c_contiguous
+    return a.ctypes.data_as(_dp)
+
+
+def read_setfl(path: str):
+    """Parse a one-element setfl file (pair_eam_alloy.cpp:100-190)."""
+    with open(path) as f:
+        lines = f.read().split("\n")
+    nel = int(lines[3].split()[0])
+    if nel != 1:
+        raise CacB200Error("only one-element setfl files are supported")
+    w = lines[4].split()
+    nrho, drho, nr, dr, cut = int(w[0]), float(w[1]), int(w[2]), float(w[3]), float(w[4])
+    mass = float(lines[5].split()[1])
+    vals = np.array([float(t) for t in " ".join(lines[6:]).split()], dtype=np.float64)
+    need = nrho + 2 * nr
+    if vals.size < need:
+        raise CacB200Error("setfl file is truncated")
+    return dict(nrho=nrho, drho=drho, nr=nr, dr=dr, cut=cut, mass=mass,
+                frho=vals[:nrho].copy(), rhor=vals[nrho:nrho + nr].copy(),
+                z2r=vals[nrho + nr:nrho + 2 * nr].copy())
+
+
+class Engine:
+    """One device-resident CAC system (a ``cacb200_ctx``)."""
+
+    def __init__(self, device: int = 0):
+        self.lib = load()
+        h = C.c_void_p()
+        rc = self.lib.cacb200_ctx_create(device, C.byref(h))
+        if rc != 0:
+            raise CacB200Error(f"cacb200_ctx_create failed ({rc}): no usable CUDA device")
+        self.h = h
+        self.na = self.ne = 0
+        self._cut = None
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.cacb200_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc: int, what: str):
+        if rc != 0:
+            msg = self.lib.cacb200_last_error(self.h)
+            raise CacB200Error(f"{what} failed ({rc}): {msg.decode() if msg else ''}")
+
+    @property
+    def stream(self) -> int:
+        return int(self.lib.cacb200_stream(self.h) or 0)
+
+    # ------------------------------------------------------------- system
+    def upload(self, system) -> None:
+        x = np.ascontiguousarray(system.x, dtype=np.float64)
+        v = np.ascontiguousarray(system.v, dtype=np.float64)
+        nx = np.ascontiguousarray(system.nodex, dtype=np.float64)
+        nv = np.ascontiguousarray(system.nodev, dtype=np.float64)
+        lo = np.ascontiguousarray(system.boxlo, dtype=np.float64)
+        hi = np.ascontiguousarray(system.boxhi, dtype=np.float64)
+        self.na, self.ne = x.shape[0], nx.shape[0]
+        self._check(self.lib.cacb200_upload_system(self.h, _p(lo), _p(hi), self.na, _p(x), _p(v),
+                                                   self.ne, _p(nx), _p(nv), float(system.mass)),
+                    "upload_system")
+
+    def set_precision(self, form: int) -> None:
+        self._check(self.lib.cacb200_set_precision(self.h, form), "set_precision")
+
+    def pair_lj(self, epsilon: float, sigma: float, cut: float) -> None:
+        self._check(self.lib.cacb200_set_lj(self.h, epsilon, sigma, cut), "set_lj")
+
+    def pair_eam(self, setfl) -> None:
+        t = read_setfl(setfl) if isinstance(setfl, str) else setfl
+        self._check(self.lib.cacb200_set_eam(self.h, t["nrho"], t["drho"], t["nr"], t["dr"], t["cut"],
+                                             _p(t["frho"]), _p(t["rhor"]), _p(t["z2r"])), "set_eam")
+
+    def nodal_energy_weight(self, w: float) -> None:
+        self._check(self.lib.cacb200_set_nodal_energy_weight(self.h, w), "set_nodal_energy_weight")
+
+    def neighbor(self, skin: float, every: int) -> None:
+        self._check(self.lib.cacb200_set_neighbor(self.h, skin, every), "set_neighbor")
+
+    # ------------------------------------------------------------- lists
+    def build_lists(self, half: bool = False) -> None:
+        self._check(self.lib.cacb200_build_lists(self.h, 1 if half else 0), "build_lists")
+
+    def neighbor_list(self, half: bool = False) -> np.ndarray:
+        """Sorted int64 rows (i_site, kind, idx, site, sx, sy, sz)."""
+        n = C.c_int64()
+        ns = C.c_int()
+        self._check(self.lib.cacb200_list_size(self.h, 1 if half else 0, C.byref(n), C.byref(ns)), "list_size")
+        n, ns = n.value, ns.value
+        off = np.zeros(ns + 1, dtype=np.int64)
+        kind = np.zeros(max(n, 1), dtype=np.int8)
+        idx = np.zeros(max(n, 1), dtype=np.int32)
+        site = np.zeros(max(n, 1), dtype=np.int32)
+        img = np.zeros(max(n, 1) * 3, dtype=np.int8)
+        self._check(self.lib.cacb200_get_list(
+            self.h, 1 if half else 0, off.ctypes.data_as(C.POINTER(C.c_int64)),
+            kind.ctypes.data_as(C.POINTER(C.c_int8)), idx.ctypes.data_as(C.POINTER(C.c_int32)),
+            site.ctypes.data_as(C.POINTER(C.c_int32)), img.ctypes.data_as(C.POINTER(C.c_int8))), "get_list")
+        isite = np.repeat(np.arange(ns, dtype=np.int64), np.diff(off))
+        img = img[:3 * n].reshape(n, 3).astype(np.int64)
+        rows = np.stack([isite, kind[:n].astype(np.int64), idx[:n].astype(np.int64),
+                         site[:n].astype(np.int64), img[:, 0], img[:, 1], img[:, 2]], axis=1)
+        return rows[np.lexsort(rows.T[::-1])]
+
+    # ------------------------------------------------------------- steps
+    def compute(self, eflag: int = ENERGY_GLOBAL | ENERGY_ATOM, vflag: int = VIRIAL_GLOBAL | VIRIAL_ATOM) -> None:
+        self._check(self.lib.cacb200_compute_forces(self.h, eflag, vflag), "compute_forces")
+
+    def setup(self) -> None:
+        self._check(self.lib.cacb200_setup(self.h), "setup")
+
+    def run_nve(self, nsteps: int, dt: float = 0.001, eflag: int = 0, vflag: int = 0) -> None:
+        self._check(self.lib.cacb200_run_nve(self.h, nsteps, dt, eflag, vflag), "run_nve")
+
+    def counts(self):
+        a, e, s = C.c_int(), C.c_int(), C.c_int()
+        self._check(self.lib.cacb200_counts(self.h, C.byref(a), C.byref(e), C.byref(s)), "counts")
+        return a.value, e.value, s.value
+
+    # ------------------------------------------------------------- read-outs
+    def state(self):
+        x = np.zeros((self.na, 3))
+        v = np.zeros((self.na, 3))
+        nx = np.zeros((self.ne, 8, 3))
+        nv = np.zeros((self.ne, 8, 3))
+        self._check(self.lib.cacb200_get_state(self.h, _p(x), _p(v), _p(nx), _p(nv)), "get_state")
+        return x, v, nx, nv
+
+    def set_state(self, x=None, v=None, nodex=None, nodev=None) -> None:
+        conv = lambda a: None if a is None else np.ascontiguousarray(a, dtype=np.float64)
+        x, v, nodex, nodev = conv(x), conv(v), conv(nodex), conv(nodev)
+        self._check(self.lib.cacb200_set_state(self.h, _p(x), _p(v), _p(nodex), _p(nodev)), "set_state")
+
+    def forces(self):
+        f = np.zeros((self.na, 3))
+        nf = np.zeros((self.ne, 8, 3))
+        gf = np.zeros((self.ne, 8, 3))
+        self._check(self.lib.cacb200_get_forces(self.h, _p(f), _p(nf), _p(gf)), "get_forces")
+        return f, nf, gf
+
+    def energy(self, peratom: bool = True):
+        e = C.c_double()
+        vir = np.zeros(6)
+        out = {}
+        if peratom:
+            out["eatom"] = np.zeros(self.na)
+            out["vatom"] = np.zeros((self.na, 6))
+            out["enode"] = np.zeros((self.ne, 8))
+            out["vnode"] = np.zeros((self.ne, 8, 6))
+            self._check(self.lib.cacb200_get_energy(self.h, C.byref(e), _p(vir), _p(out["eatom"]),
+                                                    _p(out["vatom"]), _p(out["enode"]), _p(out["vnode"])),
+                        "get_energy")
+        else:
+            self._check(self.lib.cacb200_get_energy(self.h, C.byref(e), _p(vir), None, None, None, None),
+                        "get_energy")
+        out["energy"] = e.value
+        out["virial"] = vir
+        return out
+
+    # ------------------------------------------------------------- profiling
+    def profile(self, enable: bool) -> None:
+        self._check(self.lib.cacb200_profile(self.h, 1 if enable else 0), "profile")
+
+    def profile_read(self):
+        maxn = 64
+        names = C.create_string_buffer(32 * maxn)
+        ms = np.zeros(maxn)
+        la = np.zeros(maxn, dtype=np.int64)
+        cnt = C.c_int()
+        self._check(self.lib.cacb200_profile_read(self.h, maxn, names, _p(ms),
+                                                  la.ctypes.data_as(C.POINTER(C.c_int64)), C.byref(cnt)),
+                    "profile_read")
+        out = {}
+        raw = names.raw
+        for k in range(min(cnt.value, maxn)):
+            nm = raw[32 * k:32 * k + 32].split(b"\0", 1)[0].decode()
+            out[nm] = (float(ms[k]), int(la[k]))
+        return out

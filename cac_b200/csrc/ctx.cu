@@ -1,0 +1,513 @@
+// Context lifetime, host<->device transfer and the extern "C" entry points.
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "ctx.cuh"
+#include "device.cuh"
+
+struct cacb200_ctx {
+  cacb200::Ctx *impl;
+};
+
+namespace cacb200 {
+
+namespace {
+
+struct PendingTimer {
+  std::string name;
+  cudaEvent_t a, b;
+};
+
+void flush_profile(Ctx &c, std::vector<PendingTimer> &pend) {
+  if (pend.empty()) return;
+  cudaStreamSynchronize(c.stream);
+  for (auto &p : pend) {
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, p.a, p.b);
+    size_t k = 0;
+    for (; k < c.prof.names.size(); k++)
+      if (c.prof.names[k] == p.name) break;
+    if (k == c.prof.names.size()) {
+      c.prof.names.push_back(p.name);
+      c.prof.ms.push_back(0.0);
+      c.prof.launches.push_back(0);
+    }
+    c.prof.ms[k] += ms;
+    c.prof.launches[k] += 1;
+    cudaEventDestroy(p.a);
+    cudaEventDestroy(p.b);
+  }
+  pend.clear();
+}
+
+std::vector<PendingTimer> &pending_for(Ctx &c) {
+  static thread_local std::vector<std::pair<Ctx *, std::vector<PendingTimer>>> table;
+  for (auto &t : table)
+    if (t.first == &c) return t.second;
+  table.emplace_back(&c, std::vector<PendingTimer>());
+  return table.back().second;
+}
+
+}  // namespace
+
+Ctx::Ctx(int dev) : device(dev) {
+  CACB200_CUDA(cudaSetDevice(dev));
+  CACB200_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+}
+
+Ctx::~Ctx() {
+  if (stream) {
+    cudaStreamSynchronize(stream);
+    auto &pend = pending_for(*this);
+    flush_profile(*this, pend);
+    cudaStreamDestroy(stream);
+  }
+}
+
+KernelTimer::KernelTimer(Ctx &ctx, const char *n) : c(ctx), name(n) {
+  if (!c.prof.enabled) return;
+  PendingTimer p{name, nullptr, nullptr};
+  cudaEventCreate(&p.a);
+  cudaEventCreate(&p.b);
+  cudaEventRecord(p.a, c.stream);
+  pending_for(c).push_back(p);
+}
+
+KernelTimer::~KernelTimer() {
+  if (!c.prof.enabled) return;
+  auto &pend = pending_for(c);
+  if (!pend.empty()) cudaEventRecord(pend.back().b, c.stream);
+  if (pend.size() > 4096) flush_profile(c, pend);
+}
+
+namespace {
+
+void upload_system(Ctx &c, const double lo[3], const double hi[3], int na, const double *x,
+                   const double *v, int ne, const double *nodex, const double *nodev, double mass) {
+  if (na < 0 || ne < 0 || (na > 0 && (!x || !v)) || (ne > 0 && (!nodex || !nodev)))
+    throw Error(CACB200_EINVAL, "invalid system arrays");
+  if (!(mass > 0.0)) throw Error(CACB200_EINVAL, "mass must be positive");
+  if ((long)na + (long)NG * ne + (long)ne * NU >= (1L << 26))
+    throw Error(CACB200_EINVAL, "system too large for 26-bit site indices");
+  for (int d = 0; d < 3; d++) {
+    if (!(hi[d] > lo[d])) throw Error(CACB200_EINVAL, "empty box");
+    c.boxlo[d] = lo[d];
+    c.boxhi[d] = hi[d];
+    c.prd[d] = hi[d] - lo[d];
+  }
+  c.na = na;
+  c.ne = ne;
+  c.mass = mass;
+  c.nact = 0;
+  c.lists_valid = false;
+  c.have_half = false;
+  c.step = c.last_build_step = 0;
+  c.xs.release();
+  size_t ns = (size_t)na + NG * (size_t)ne;
+  c.xs.reserve(ns + ns / 8 + 64);
+  c.v.reserve(std::max(3 * na, 1));
+  c.f.reserve(std::max(3 * na, 1));
+  c.nodex.reserve(std::max(24 * ne, 1));
+  c.nodev.reserve(std::max(24 * ne, 1));
+  c.nodef.reserve(std::max(24 * ne, 1));
+  c.gaussf.reserve(std::max(24 * ne, 1));
+  CACB200_CUDA(cudaMemsetAsync(c.f.p, 0, sizeof(double) * std::max(3 * na, 1), c.stream));
+  CACB200_CUDA(cudaMemsetAsync(c.nodef.p, 0, sizeof(double) * std::max(24 * ne, 1), c.stream));
+  CACB200_CUDA(cudaMemsetAsync(c.gaussf.p, 0, sizeof(double) * std::max(24 * ne, 1), c.stream));
+  CACB200_CUDA(cudaMemsetAsync(c.xs.p, 0, sizeof(double4) * c.xs.n, c.stream));
+  c.have_system = true;
+  // positions/velocities
+  std::vector<double4> hx(std::max(na, 1));
+  for (int i = 0; i < na; i++) hx[i] = make_double4(x[3 * i], x[3 * i + 1], x[3 * i + 2], 0.0);
+  if (na) {
+    CACB200_CUDA(cudaMemcpy(c.xs.p, hx.data(), sizeof(double4) * na, cudaMemcpyHostToDevice));
+    CACB200_CUDA(cudaMemcpy(c.v.p, v, sizeof(double) * 3 * na, cudaMemcpyHostToDevice));
+  }
+  if (ne) {
+    CACB200_CUDA(cudaMemcpy(c.nodex.p, nodex, sizeof(double) * 24 * ne, cudaMemcpyHostToDevice));
+    CACB200_CUDA(cudaMemcpy(c.nodev.p, nodev, sizeof(double) * 24 * ne, cudaMemcpyHostToDevice));
+  }
+  CACB200_CUDA(cudaStreamSynchronize(c.stream));
+}
+
+__global__ void k_pack_x(const double *x, double4 *xs, int n) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double4 p = xs[i];
+  p.x = x[3 * i];
+  p.y = x[3 * i + 1];
+  p.z = x[3 * i + 2];
+  xs[i] = p;
+}
+
+__global__ void k_unpack_x(const double4 *xs, double *x, int n) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double4 p = xs[i];
+  x[3 * i] = p.x;
+  x[3 * i + 1] = p.y;
+  x[3 * i + 2] = p.z;
+}
+
+// Positions and velocities from host arrays.  Lists are kept, as the
+// reference keeps them between rebuilds while forward communication moves the
+// ghosts; rebuild when atoms moved further than half the skin.
+void set_state(Ctx &c, const double *x, const double *v, const double *nodex, const double *nodev) {
+  c.check_system();
+  if (x && c.na) {
+    c.stage.reserve(3 * (size_t)c.na);
+    CACB200_CUDA(cudaMemcpyAsync(c.stage.p, x, sizeof(double) * 3 * c.na, cudaMemcpyHostToDevice, c.stream));
+    k_pack_x<<<(c.na + 255) / 256, 256, 0, c.stream>>>(c.stage.p, c.xs.p, c.na);
+  }
+  if (v && c.na)
+    CACB200_CUDA(cudaMemcpyAsync(c.v.p, v, sizeof(double) * 3 * c.na, cudaMemcpyHostToDevice, c.stream));
+  if (nodex && c.ne)
+    CACB200_CUDA(cudaMemcpyAsync(c.nodex.p, nodex, sizeof(double) * 24 * c.ne, cudaMemcpyHostToDevice, c.stream));
+  if (nodev && c.ne)
+    CACB200_CUDA(cudaMemcpyAsync(c.nodev.p, nodev, sizeof(double) * 24 * c.ne, cudaMemcpyHostToDevice, c.stream));
+  CACB200_CUDA(cudaStreamSynchronize(c.stream));
+}
+
+void get_state(Ctx &c, double *x, double *v, double *nodex, double *nodev) {
+  c.check_system();
+  if (x && c.na) {
+    c.stage.reserve(3 * (size_t)c.na);
+    k_unpack_x<<<(c.na + 255) / 256, 256, 0, c.stream>>>(c.xs.p, c.stage.p, c.na);
+    CACB200_CUDA(cudaMemcpyAsync(x, c.stage.p, sizeof(double) * 3 * c.na, cudaMemcpyDeviceToHost, c.stream));
+  }
+  if (v && c.na)
+    CACB200_CUDA(cudaMemcpyAsync(v, c.v.p, sizeof(double) * 3 * c.na, cudaMemcpyDeviceToHost, c.stream));
+  if (nodex && c.ne)
+    CACB200_CUDA(cudaMemcpyAsync(nodex, c.nodex.p, sizeof(double) * 24 * c.ne, cudaMemcpyDeviceToHost, c.stream));
+  if (nodev && c.ne)
+    CACB200_CUDA(cudaMemcpyAsync(nodev, c.nodev.p, sizeof(double) * 24 * c.ne, cudaMemcpyDeviceToHost, c.stream));
+  CACB200_CUDA(cudaStreamSynchronize(c.stream));
+}
+
+void fetch_ev(Ctx &c) {
+  if (!c.ev_pending) return;
+  double h[7];
+  CACB200_CUDA(cudaMemcpyAsync(h, c.ev_out.p, sizeof(h), cudaMemcpyDeviceToHost, c.stream));
+  CACB200_CUDA(cudaStreamSynchronize(c.stream));
+  c.energy = h[0];
+  for (int k = 0; k < 6; k++) c.virial[k] = h[1 + k];
+  c.ev_pending = false;
+}
+
+void build(Ctx &c, bool want_half) {
+  neigh_build(c, want_half);
+  interpolate_sites(c);
+  c.last_build_step = c.step;
+}
+
+void forces(Ctx &c, int eflag, int vflag) {
+  interpolate_sites(c);
+  pair_compute(c, eflag, vflag);
+  assemble_nodef(c);
+}
+
+void setup(Ctx &c) {
+  c.check_system();
+  build(c, false);
+  forces(c, CACB200_ENERGY_GLOBAL, CACB200_VIRIAL_GLOBAL);
+}
+
+void run_nve(Ctx &c, int nsteps, double dt, int eflag, int vflag) {
+  c.check_system();
+  if (nsteps < 0) throw Error(CACB200_EINVAL, "negative step count");
+  if (!c.lists_valid) setup(c);
+  for (int s = 1; s <= nsteps; s++) {
+    nve_initial(c, dt);
+    c.step++;
+    if (c.every > 0 && (c.step - c.last_build_step) % c.every == 0) build(c, false);
+    bool last = (s == nsteps);
+    forces(c, last ? eflag : 0, last ? vflag : 0);
+    nve_final(c, dt);
+  }
+  CACB200_CUDA(cudaGetLastError());
+}
+
+}  // namespace
+}  // namespace cacb200
+
+using namespace cacb200;
+
+#define API_BEGIN                                                \
+  if (!ctx || !ctx->impl) return CACB200_EINVAL;                 \
+  Ctx &c = *ctx->impl;                                           \
+  try {
+#define API_END                                                  \
+  }                                                              \
+  catch (const Error &e) {                                       \
+    c.last_error = e.what();                                     \
+    return e.code;                                               \
+  }                                                              \
+  catch (const std::exception &e) {                              \
+    c.last_error = e.what();                                     \
+    return CACB200_EINVAL;                                       \
+  }                                                              \
+  return CACB200_OK;
+
+extern "C" {
+
+int cacb200_ctx_create(int device, cacb200_ctx **out) {
+  if (!out) return CACB200_EINVAL;
+  *out = nullptr;
+  try {
+    auto *h = new cacb200_ctx;
+    h->impl = new Ctx(device);
+    *out = h;
+  } catch (const Error &e) {
+    std::fprintf(stderr, "cacb200_ctx_create: %s\n", e.what());
+    return e.code;
+  }
+  return CACB200_OK;
+}
+
+int cacb200_ctx_destroy(cacb200_ctx *ctx) {
+  if (!ctx) return CACB200_EINVAL;
+  delete ctx->impl;
+  delete ctx;
+  return CACB200_OK;
+}
+
+const char *cacb200_last_error(const cacb200_ctx *ctx) {
+  if (!ctx || !ctx->impl) return "invalid context";
+  return ctx->impl->last_error.c_str();
+}
+
+void *cacb200_stream(cacb200_ctx *ctx) {
+  if (!ctx || !ctx->impl) return nullptr;
+  return (void *)ctx->impl->stream;
+}
+
+int cacb200_set_precision(cacb200_ctx *ctx, int form) {
+  API_BEGIN
+  if (form != CACB200_FP64 && form != CACB200_MIXED) throw Error(CACB200_EINVAL, "unknown precision form");
+  c.precision = form;
+  API_END
+}
+
+int cacb200_upload_system(cacb200_ctx *ctx, const double boxlo[3], const double boxhi[3], int natoms,
+                          const double *x, const double *v, int nelements, const double *nodex,
+                          const double *nodev, double mass) {
+  API_BEGIN
+  if (!boxlo || !boxhi) throw Error(CACB200_EINVAL, "box required");
+  upload_system(c, boxlo, boxhi, natoms, x, v, nelements, nodex, nodev, mass);
+  API_END
+}
+
+int cacb200_set_state(cacb200_ctx *ctx, const double *x, const double *v, const double *nodex,
+                      const double *nodev) {
+  API_BEGIN
+  set_state(c, x, v, nodex, nodev);
+  API_END
+}
+
+int cacb200_get_state(cacb200_ctx *ctx, double *x, double *v, double *nodex, double *nodev) {
+  API_BEGIN
+  get_state(c, x, v, nodex, nodev);
+  API_END
+}
+
+int cacb200_get_forces(cacb200_ctx *ctx, double *f, double *nodef, double *gaussf) {
+  API_BEGIN
+  c.check_system();
+  CACB200_CUDA(cudaStreamSynchronize(c.stream));
+  if (f && c.na) CACB200_CUDA(cudaMemcpy(f, c.f.p, sizeof(double) * 3 * c.na, cudaMemcpyDeviceToHost));
+  if (nodef && c.ne)
+    CACB200_CUDA(cudaMemcpy(nodef, c.nodef.p, sizeof(double) * 24 * c.ne, cudaMemcpyDeviceToHost));
+  if (gaussf && c.ne)
+    CACB200_CUDA(cudaMemcpy(gaussf, c.gaussf.p, sizeof(double) * 24 * c.ne, cudaMemcpyDeviceToHost));
+  API_END
+}
+
+int cacb200_get_energy(cacb200_ctx *ctx, double *energy, double virial[6], double *eatom, double *vatom,
+                       double *enode, double *vnode) {
+  API_BEGIN
+  c.check_system();
+  fetch_ev(c);
+  if (energy) *energy = c.energy;
+  if (virial)
+    for (int k = 0; k < 6; k++) virial[k] = c.virial[k];
+  if ((eatom || enode) && !c.have_peratom_e) throw Error(CACB200_ESTATE, "per-site energy not computed");
+  if ((vatom || vnode) && !c.have_peratom_v) throw Error(CACB200_ESTATE, "per-site virial not computed");
+  if (eatom && c.na) CACB200_CUDA(cudaMemcpy(eatom, c.eatom.p, sizeof(double) * c.na, cudaMemcpyDeviceToHost));
+  if (enode && c.ne) CACB200_CUDA(cudaMemcpy(enode, c.enode.p, sizeof(double) * 8 * c.ne, cudaMemcpyDeviceToHost));
+  if (vatom && c.na)
+    CACB200_CUDA(cudaMemcpy(vatom, c.vatom.p, sizeof(double) * 6 * c.na, cudaMemcpyDeviceToHost));
+  if (vnode && c.ne)
+    CACB200_CUDA(cudaMemcpy(vnode, c.vnode.p, sizeof(double) * 48 * c.ne, cudaMemcpyDeviceToHost));
+  API_END
+}
+
+int cacb200_counts(cacb200_ctx *ctx, int *natoms, int *nelements, int *nactive_sites) {
+  API_BEGIN
+  if (natoms) *natoms = c.na;
+  if (nelements) *nelements = c.ne;
+  if (nactive_sites) *nactive_sites = c.nact;
+  API_END
+}
+
+int cacb200_set_lj(cacb200_ctx *ctx, double epsilon, double sigma, double cut) {
+  API_BEGIN
+  if (!(cut > 0.0) || !(sigma > 0.0)) throw Error(CACB200_EINVAL, "invalid LJ parameters");
+  // PairLJCut::init_one (pair_lj_cut.cpp:142-160), no offset (pair_modify shift no)
+  c.pp = PairParams();
+  c.pp.style = CACB200_PAIR_LJ;
+  c.pp.cut = cut;
+  c.pp.lj1 = 48.0 * epsilon * std::pow(sigma, 12.0);
+  c.pp.lj2 = 24.0 * epsilon * std::pow(sigma, 6.0);
+  c.pp.lj3 = 4.0 * epsilon * std::pow(sigma, 12.0);
+  c.pp.lj4 = 4.0 * epsilon * std::pow(sigma, 6.0);
+  c.pp.offset = 0.0;
+  c.lists_valid = false;
+  API_END
+}
+
+int cacb200_set_eam(cacb200_ctx *ctx, int nrho, double drho, int nr, double dr, double cut,
+                    const double *frho, const double *rhor, const double *z2r) {
+  API_BEGIN
+  if (nrho < 5 || nr < 5 || !(drho > 0) || !(dr > 0) || !(cut > 0) || !frho || !rhor || !z2r)
+    throw Error(CACB200_EINVAL, "invalid EAM tables");
+  c.pp = PairParams();
+  c.pp.style = CACB200_PAIR_EAM;
+  c.pp.cut = cut;
+  c.pp.nrho = nrho;
+  c.pp.nr = nr;
+  c.pp.drho = drho;
+  c.pp.dr = dr;
+  c.pp.rdr = 1.0 / dr;
+  c.pp.rdrho = 1.0 / drho;
+  c.pp.rhomax = (nrho - 1) * drho;
+  eam_tables(c, frho, rhor, z2r);
+  c.lists_valid = false;
+  API_END
+}
+
+int cacb200_set_nodal_energy_weight(cacb200_ctx *ctx, double w) {
+  API_BEGIN
+  c.nodal_energy_weight = w;
+  API_END
+}
+
+int cacb200_set_neighbor(cacb200_ctx *ctx, double skin, int every) {
+  API_BEGIN
+  if (!(skin >= 0.0) || every < 0) throw Error(CACB200_EINVAL, "invalid neighbour settings");
+  c.skin = skin;
+  c.every = every;
+  c.lists_valid = false;
+  API_END
+}
+
+int cacb200_build_lists(cacb200_ctx *ctx, int want_half) {
+  API_BEGIN
+  build(c, want_half != 0);
+  API_END
+}
+
+int cacb200_list_size(cacb200_ctx *ctx, int half, int64_t *nentries, int *nsites) {
+  API_BEGIN
+  int64_t n = 0;
+  neigh_download(c, half != 0, nullptr, nullptr, nullptr, nullptr, nullptr, &n);
+  if (nentries) *nentries = n;
+  if (nsites) *nsites = c.nsite_i();
+  API_END
+}
+
+int cacb200_get_list(cacb200_ctx *ctx, int half, int64_t *offset, int8_t *kind, int32_t *idx, int32_t *site,
+                     int8_t *img) {
+  API_BEGIN
+  if (!offset || !kind || !idx || !site || !img) throw Error(CACB200_EINVAL, "null output array");
+  int64_t n = 0;
+  neigh_download(c, half != 0, offset, kind, idx, site, img, &n);
+  API_END
+}
+
+int cacb200_interpolate(cacb200_ctx *ctx) {
+  API_BEGIN
+  c.check_system();
+  interpolate_sites(c);
+  API_END
+}
+
+int cacb200_compute_pair(cacb200_ctx *ctx, int eflag, int vflag) {
+  API_BEGIN
+  pair_compute(c, eflag, vflag);
+  API_END
+}
+
+int cacb200_assemble_nodef(cacb200_ctx *ctx) {
+  API_BEGIN
+  c.check_system();
+  assemble_nodef(c);
+  API_END
+}
+
+int cacb200_compute_forces(cacb200_ctx *ctx, int eflag, int vflag) {
+  API_BEGIN
+  c.check_system();
+  if (!c.lists_valid) build(c, false);
+  forces(c, eflag, vflag);
+  API_END
+}
+
+int cacb200_nve_initial(cacb200_ctx *ctx, double dt) {
+  API_BEGIN
+  c.check_system();
+  nve_initial(c, dt);
+  API_END
+}
+
+int cacb200_nve_final(cacb200_ctx *ctx, double dt) {
+  API_BEGIN
+  c.check_system();
+  nve_final(c, dt);
+  API_END
+}
+
+int cacb200_setup(cacb200_ctx *ctx) {
+  API_BEGIN
+  setup(c);
+  API_END
+}
+
+int cacb200_run_nve(cacb200_ctx *ctx, int nsteps, double dt, int eflag, int vflag) {
+  API_BEGIN
+  run_nve(c, nsteps, dt, eflag, vflag);
+  API_END
+}
+
+int cacb200_profile(cacb200_ctx *ctx, int enable) {
+  API_BEGIN
+  auto &pend = pending_for(c);
+  flush_profile(c, pend);
+  c.prof.enabled = enable != 0;
+  c.prof.names.clear();
+  c.prof.ms.clear();
+  c.prof.launches.clear();
+  API_END
+}
+
+int cacb200_profile_read(cacb200_ctx *ctx, int max, char *names, double *total_ms, int64_t *launches,
+                         int *count) {
+  API_BEGIN
+  auto &pend = pending_for(c);
+  flush_profile(c, pend);
+  int n = (int)c.prof.names.size();
+  if (count) *count = n;
+  for (int k = 0; k < n && k < max; k++) {
+    if (names) {
+      std::memset(names + 32 * k, 0, 32);
+      std::strncpy(names + 32 * k, c.prof.names[k].c_str(), 31);
+    }
+    if (total_ms) total_ms[k] = c.prof.ms[k];
+    if (launches) launches[k] = c.prof.launches[k];
+  }
+  API_END
+}
+
+}  // extern "C"

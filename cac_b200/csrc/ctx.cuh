@@ -1,0 +1,192 @@
+// Internal state of a cacb200 context: device buffers, parameters and helpers.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/cacb200.h"
+
+namespace cacb200 {
+
+constexpr int NC = 9;           // lattice sites per element edge
+constexpr int NU = NC * NC * NC;  // lattice sites per element (729)
+constexpr int NPE = 8;          // nodes per element
+constexpr int NG = 8;           // Gauss points per element (the nodes)
+constexpr int IMG_BITS = 5;     // periodic image code 0..26 in the low bits of a list entry
+constexpr int IMG_ZERO = 13;    // image (0, 0, 0)
+
+struct Error : std::runtime_error {
+  int code;
+  Error(int c, const std::string &m) : std::runtime_error(m), code(c) {}
+};
+
+#define CACB200_CUDA(call)                                                             \
+  do {                                                                                 \
+    cudaError_t err_ = (call);                                                         \
+    if (err_ != cudaSuccess)                                                           \
+      throw ::cacb200::Error(CACB200_ECUDA, std::string(#call) + ": " +                \
+                                                cudaGetErrorString(err_));             \
+  } while (0)
+
+// Simple owning device buffer.
+template <class T>
+struct DBuf {
+  T *p = nullptr;
+  size_t n = 0;
+  DBuf() = default;
+  DBuf(const DBuf &) = delete;
+  DBuf &operator=(const DBuf &) = delete;
+  ~DBuf() { release(); }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  // grow to at least m elements (contents not preserved)
+  void reserve(size_t m) {
+    if (m <= n && p) return;
+    release();
+    size_t bytes = (m ? m : 1) * sizeof(T);
+    if (cudaMalloc(&p, bytes) != cudaSuccess) {
+      cudaGetLastError();
+      throw Error(CACB200_ENOMEM, "device allocation of " + std::to_string(bytes) + " bytes failed");
+    }
+    n = m ? m : 1;
+  }
+};
+
+// Atom bins of the reference (NBinStandard::setup_bins, nbin_standard.cpp:84-128):
+// used only for the half-list storage rule.
+struct RefBins {
+  double lo[3], hi[3], inv[3];
+  int nbin[3];
+};
+
+// Uniform periodic cell grid over wrapped coordinates (candidate search).
+struct Grid {
+  int nc[3];
+  double inv[3];   // 1 / cell size
+  int ncell;
+};
+
+struct PairParams {
+  int style = CACB200_PAIR_NONE;
+  double cut = 0.0;          // force cutoff
+  // LJ
+  double lj1 = 0, lj2 = 0, lj3 = 0, lj4 = 0, offset = 0;
+  // EAM
+  int nrho = 0, nr = 0;
+  double drho = 0, dr = 0, rdr = 0, rdrho = 0, rhomax = 0;
+};
+
+struct Profile {
+  bool enabled = false;
+  std::vector<std::string> names;
+  std::vector<double> ms;
+  std::vector<int64_t> launches;
+};
+
+struct Ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  std::string last_error;
+  int precision = CACB200_FP64;
+
+  // system
+  int na = 0, ne = 0;
+  double boxlo[3] = {0, 0, 0}, boxhi[3] = {0, 0, 0}, prd[3] = {0, 0, 0};
+  double mass = 1.0;
+  bool have_system = false;
+
+  // sites table S: [atoms | Gauss points (8 per element) | active lattice sites]
+  // xs[k] = (x, y, z, w) with w = F'(rho) for EAM
+  DBuf<double4> xs;
+  int nact = 0;                  // active non-Gauss lattice sites
+  DBuf<int> act_gid;             // [nact] e*729 + u
+  DBuf<int> act_off;             // [ne+1] CSR of active sites by element (into act_gid)
+  int nsite_i() const { return na + NG * ne; }
+  int nsite_s() const { return na + NG * ne + nact; }
+
+  DBuf<double> v, f;             // atoms [na*3]
+  DBuf<double> stage;            // [na*3] host-transfer staging for positions
+  DBuf<double> nodex, nodev, nodef, gaussf;  // [ne*8*3]
+  DBuf<double> rho;              // [na + 8*ne]: atoms then nodes (node order)
+  DBuf<double> phi_site;         // [nsite_i] embedding energy F(rho) per i-site (EAM, eflag)
+  // energy / virial
+  DBuf<double> eatom, vatom, enode, vnode;   // per-site outputs
+  DBuf<double> partial;          // per-block partial sums [nblocks*7]
+  DBuf<double> ev_out;           // [7]: energy, virial[6]
+  double energy = 0.0, virial[6] = {0, 0, 0, 0, 0, 0};
+  bool have_peratom_e = false, have_peratom_v = false;
+  bool ev_pending = false;       // ev_out holds a result not yet copied to energy/virial
+  long step = 0, last_build_step = 0;
+  double nodal_energy_weight = -1.0;
+
+  // element geometry (per rebuild)
+  DBuf<double4> ecenter;         // reference centre (x, y, z, R_e)
+  DBuf<double4> ewrap;           // wrapped centre, w = bitcast of packed wrap counts
+  DBuf<double> eframe;           // [ne*16]: n0(3) a(3) b(3) c(3) ... see neigh.cu
+  double emax_reach = 0.0;
+
+  // atom cell grid (candidate search)
+  Grid agrid{}, egrid{};
+  DBuf<int> acell_start;         // [ncell+1]
+  DBuf<int> acell_atoms;         // [na] atom ids sorted by cell
+  DBuf<double4> acell_pos;       // [na] wrapped positions sorted by cell, w = bitcast(id)
+  DBuf<int> ecell_start, ecell_elems;
+  DBuf<int> cell_key, cell_key2, idx_tmp, idx_tmp2;
+  DBuf<unsigned char> cub_tmp;
+  RefBins rbins{};
+
+  // neighbour lists: transposed [cap][nsite_i] packed entries (sidx << 5 | img)
+  double skin = 1.0, cutneigh = 0.0, cutneighsq = 0.0;
+  int every = 10;
+  int cap = 128;
+  DBuf<int> nbr_full, num_full;
+  DBuf<int> nbr_half, num_half;
+  bool have_half = false, lists_valid = false;
+  DBuf<int> raw_full, raw_half;  // build-time entries before compaction
+  DBuf<unsigned char> img_full, img_half;
+  DBuf<int> site_flag;           // [ne*729 + 1] marks
+  DBuf<int> site_pref;           // [ne*729 + 1] exclusive prefix of the marks
+  DBuf<int> overflow;            // [4] device flags
+  int build_count = 0;
+
+  PairParams pp;
+  DBuf<double4> rhor_val, rhor_der, z2r_val, z2r_der, frho_val, frho_der;
+
+  Profile prof;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+
+  Ctx(int dev);
+  ~Ctx();
+  void check_system() const {
+    if (!have_system) throw Error(CACB200_ESTATE, "no system uploaded");
+  }
+};
+
+// profiling helpers (host)
+struct KernelTimer {
+  Ctx &c;
+  const char *name;
+  KernelTimer(Ctx &ctx, const char *n);
+  ~KernelTimer();
+};
+
+// stages implemented in the .cu files
+void neigh_build(Ctx &c, bool want_half);
+void neigh_download(Ctx &c, bool half, int64_t *offset, int8_t *kind, int32_t *idx, int32_t *site,
+                    int8_t *img, int64_t *nentries);
+void interpolate_sites(Ctx &c);
+void pair_compute(Ctx &c, int eflag, int vflag);
+void assemble_nodef(Ctx &c);
+void nve_initial(Ctx &c, double dt);
+void nve_final(Ctx &c, double dt);
+void pbc_wrap(Ctx &c);
+void eam_tables(Ctx &c, const double *frho, const double *rhor, const double *z2r);
+
+}  // namespace cacb200

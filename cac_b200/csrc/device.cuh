@@ -1,0 +1,102 @@
+// Device helpers shared by the kernels: element-type tables computed on the
+// fly, periodic images, reductions.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "ctx.cuh"
+
+namespace cacb200 {
+
+struct BoxD {
+  double lo[3], hi[3], L[3];
+};
+
+inline BoxD make_box(const Ctx &c) {
+  BoxD b;
+  for (int d = 0; d < 3; d++) {
+    b.lo[d] = c.boxlo[d];
+    b.hi[d] = c.boxhi[d];
+    b.L[d] = c.prd[d];
+  }
+  return b;
+}
+
+// Hex node n sits at natural corner (xi, eta, zeta) in {0,1}^3 with the
+// reference's numbering (element_vec_cac.cpp:1740-1770):
+// 0 (0,0,0) 1 (1,0,0) 2 (1,1,0) 3 (0,1,0) 4 (0,0,1) 5 (1,0,1) 6 (1,1,1) 7 (0,1,1)
+__host__ __device__ __forceinline__ int node_xi(int n) { return (n == 1 || n == 2 || n == 5 || n == 6); }
+__host__ __device__ __forceinline__ int node_eta(int n) { return (n == 2 || n == 3 || n == 6 || n == 7); }
+__host__ __device__ __forceinline__ int node_zeta(int n) { return n >= 4; }
+__host__ __device__ __forceinline__ int corner_node(int xi, int eta, int zeta) {
+  return zeta * 4 + (eta ? (xi ? 2 : 3) : (xi ? 1 : 0));
+}
+
+// Gauss cell g = (i*2 + j)*2 + k at lattice indices {0, 8} (setup_integration_point,
+// element_vec_cac.cpp:2484-2553): its lattice site and node.
+__host__ __device__ __forceinline__ int gauss_site(int g) {
+  return ((g >> 2) & 1) * 8 * NC * NC + ((g >> 1) & 1) * 8 * NC + (g & 1) * 8;
+}
+__host__ __device__ __forceinline__ int gauss_node(int g) {
+  return corner_node((g >> 2) & 1, (g >> 1) & 1, g & 1);
+}
+__host__ __device__ __forceinline__ int node_gauss(int n) {
+  return node_xi(n) * 4 + node_eta(n) * 2 + node_zeta(n);
+}
+// lattice site u -> Gauss cell index, or -1 when u is not a corner
+__host__ __device__ __forceinline__ int site_gauss(int u) {
+  int i = u / (NC * NC), j = (u / NC) % NC, k = u % NC;
+  if ((i != 0 && i != NC - 1) || (j != 0 && j != NC - 1) || (k != 0 && k != NC - 1)) return -1;
+  return ((i ? 1 : 0) * 2 + (j ? 1 : 0)) * 2 + (k ? 1 : 0);
+}
+
+// Trilinear shape function of node n at lattice site u
+// (Element::shape_function Hex, element.cpp:2988-2997, at px = 0.25 i - 1).
+// Every factor is a multiple of 1/4 in [0, 2], so the product is exact in
+// binary64 and equals the reference's table entry bit for bit.
+__host__ __device__ __forceinline__ double shape_val(int u, int n) {
+  int i = u / (NC * NC), j = (u / NC) % NC, k = u % NC;
+  double px = 0.25 * i - 1.0, py = 0.25 * j - 1.0, pz = 0.25 * k - 1.0;
+  double a = node_xi(n) ? (1 + px) : (1 - px);
+  double b = node_eta(n) ? (1 + py) : (1 - py);
+  double c = node_zeta(n) ? (1 + pz) : (1 - pz);
+  return 0.125 * a * b * c;
+}
+
+__host__ __device__ __forceinline__ int img_code(int sx, int sy, int sz) {
+  return (sx + 1) + 3 * (sy + 1) + 9 * (sz + 1);
+}
+__host__ __device__ __forceinline__ void img_decode(int code, int &sx, int &sy, int &sz) {
+  sx = code % 3 - 1;
+  sy = (code / 3) % 3 - 1;
+  sz = code / 9 - 1;
+}
+
+__device__ __forceinline__ double warp_sum(double v) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Deterministic block reduction of NV doubles into out[blockIdx.x * NV + k].
+template <int NV>
+__device__ __forceinline__ void block_reduce_store(double (&vals)[NV], double *out) {
+  __shared__ double sh[32][NV];
+  int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int k = 0; k < NV; k++) vals[k] = warp_sum(vals[k]);
+  if (lane == 0)
+#pragma unroll
+    for (int k = 0; k < NV; k++) sh[warp][k] = vals[k];
+  __syncthreads();
+  if (warp == 0) {
+    int nw = (blockDim.x + 31) >> 5;
+#pragma unroll
+    for (int k = 0; k < NV; k++) {
+      double v = lane < nw ? sh[lane][k] : 0.0;
+      v = warp_sum(v);
+      if (lane == 0) out[blockIdx.x * NV + k] = v;
+    }
+  }
+}
+
+}  // namespace cacb200

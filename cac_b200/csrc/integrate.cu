@@ -1,0 +1,166 @@
+// Element interpolation, nodal-force assembly and velocity-Verlet updates.
+#include "ctx.cuh"
+#include "device.cuh"
+
+namespace cacb200 {
+
+namespace {
+
+inline int nblk(long n, int t) { return (int)((n + t - 1) / t); }
+
+// Positions of the Gauss points (their nodes) and of every active lattice
+// site from the current nodes: x_u = sum_n N_n(u) x_n, the interpolation the
+// reference repeats per pair (pair_lj_cut.cpp:364-368, pair_eam.cpp:959-964).
+__global__ void k_interpolate(double4 *xs, const double *nodex, int na, int ne, const int *act_gid,
+                              int nact) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  int ngp = NG * ne;
+  if (t < ngp) {
+    int e = t / NG, g = t % NG;
+    const double *nx = nodex + (size_t)e * 24 + 3 * gauss_node(g);
+    double4 p = xs[na + t];
+    p.x = nx[0];
+    p.y = nx[1];
+    p.z = nx[2];
+    xs[na + t] = p;
+    return;
+  }
+  int k = t - ngp;
+  if (k >= nact) return;
+  int gid = act_gid[k];
+  int e = gid / NU, u = gid % NU;
+  const double *nx = nodex + (size_t)e * 24;
+  double x = 0.0, y = 0.0, z = 0.0;
+#pragma unroll
+  for (int n = 0; n < NPE; n++) {
+    double N = shape_val(u, n);
+    x += N * nx[3 * n];
+    y += N * nx[3 * n + 1];
+    z += N * nx[3 * n + 2];
+  }
+  double4 p = xs[na + ngp + k];
+  p.x = x;
+  p.y = y;
+  p.z = z;
+  xs[na + ngp + k] = p;
+}
+
+// Element::compute_nodef, CONSISTENT (element.cpp:2178-2210): force columns
+// fc[n] = sum_g wsa[g][n] gaussf[g] with wsa = shape * weight / nucell, then
+// nodef[a] += sum_b Minv[a][b] fc[b] with the Hex inverse mass matrix
+// (element.cpp:1784-1850, the tensor product of [[4,-2],[-2,4]]).  With the
+// Gauss points on the nodes, wsa[g][n] = 1/8 when g sits on n, else 0; the
+// loops keep the reference's order of terms.  One thread per element.
+__global__ void k_assemble(const double *gaussf, double *nodef, int ne) {
+  int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= ne) return;
+  const double weight = (double)NU / (1.0 * 8) * 1.0;   // UNIFORM node weight
+  const double *gf = gaussf + (size_t)e * 24;
+  double fc[8][3];
+#pragma unroll
+  for (int n = 0; n < 8; n++) fc[n][0] = fc[n][1] = fc[n][2] = 0.0;
+#pragma unroll
+  for (int g = 0; g < NG; g++) {
+    int gn = gauss_node(g);
+#pragma unroll
+    for (int n = 0; n < NPE; n++) {
+      double w = (n == gn ? 1.0 : 0.0) * weight / NU;
+#pragma unroll
+      for (int d = 0; d < 3; d++) fc[n][d] += w * gf[3 * g + d];
+    }
+  }
+  double *nf = nodef + (size_t)e * 24;
+#pragma unroll
+  for (int a = 0; a < NPE; a++) {
+    double acc[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+    for (int b = 0; b < NPE; b++) {
+      double m = (node_xi(a) == node_xi(b) ? 4.0 : -2.0) * (node_eta(a) == node_eta(b) ? 4.0 : -2.0) *
+                 (node_zeta(a) == node_zeta(b) ? 4.0 : -2.0);
+#pragma unroll
+      for (int d = 0; d < 3; d++) acc[d] += m * fc[b][d];
+    }
+    nf[3 * a] = acc[0];
+    nf[3 * a + 1] = acc[1];
+    nf[3 * a + 2] = acc[2];
+  }
+}
+
+// FixNVE::initial_integrate (fix_nve.cpp:62-145): half kick and drift for
+// atoms (positions live in the site table) and nodes.
+__global__ void k_nve_initial(double4 *xs, double *v, const double *f, int na, double *nodex,
+                              double *nodev, const double *nodef, int nn3, double dtfm, double dtv) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < na) {
+    double4 p = xs[t];
+    double *vi = v + 3 * (size_t)t;
+    const double *fi = f + 3 * (size_t)t;
+    // separate roundings, as the reference's x86-64 build evaluates them
+    double vx = __dadd_rn(vi[0], __dmul_rn(dtfm, fi[0]));
+    double vy = __dadd_rn(vi[1], __dmul_rn(dtfm, fi[1]));
+    double vz = __dadd_rn(vi[2], __dmul_rn(dtfm, fi[2]));
+    vi[0] = vx;
+    vi[1] = vy;
+    vi[2] = vz;
+    p.x = __dadd_rn(p.x, __dmul_rn(dtv, vx));
+    p.y = __dadd_rn(p.y, __dmul_rn(dtv, vy));
+    p.z = __dadd_rn(p.z, __dmul_rn(dtv, vz));
+    xs[t] = p;
+    return;
+  }
+  int k = t - na;
+  if (k >= nn3) return;
+  double vn = __dadd_rn(nodev[k], __dmul_rn(dtfm, nodef[k]));
+  nodev[k] = vn;
+  nodex[k] = __dadd_rn(nodex[k], __dmul_rn(dtv, vn));
+}
+
+// FixNVE::final_integrate (fix_nve.cpp:148-219)
+__global__ void k_nve_final(double *v, const double *f, int n3, double *nodev, const double *nodef,
+                            int nn3, double dtfm) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < n3) {
+    v[t] = __dadd_rn(v[t], __dmul_rn(dtfm, f[t]));
+    return;
+  }
+  int k = t - n3;
+  if (k >= nn3) return;
+  nodev[k] = __dadd_rn(nodev[k], __dmul_rn(dtfm, nodef[k]));
+}
+
+}  // namespace
+
+void interpolate_sites(Ctx &c) {
+  int n = NG * c.ne + c.nact;
+  if (n == 0) return;
+  KernelTimer t(c, "interpolate");
+  k_interpolate<<<nblk(n, 256), 256, 0, c.stream>>>(c.xs.p, c.nodex.p, c.na, c.ne, c.act_gid.p, c.nact);
+}
+
+void assemble_nodef(Ctx &c) {
+  if (c.ne == 0) return;
+  KernelTimer t(c, "assemble");
+  k_assemble<<<nblk(c.ne, 128), 128, 0, c.stream>>>(c.gaussf.p, c.nodef.p, c.ne);
+}
+
+void nve_initial(Ctx &c, double dt) {
+  double dtf = 0.5 * dt * (1.0 / 1.0364269e-4);   // metal units, update.cpp:161-164
+  double dtfm = dtf / c.mass;
+  int n = c.na + 24 * c.ne;
+  if (n == 0) return;
+  KernelTimer t(c, "nve_initial");
+  k_nve_initial<<<nblk(n, 256), 256, 0, c.stream>>>(c.xs.p, c.v.p, c.f.p, c.na, c.nodex.p, c.nodev.p,
+                                                    c.nodef.p, 24 * c.ne, dtfm, dt);
+}
+
+void nve_final(Ctx &c, double dt) {
+  double dtf = 0.5 * dt * (1.0 / 1.0364269e-4);
+  double dtfm = dtf / c.mass;
+  int n = 3 * c.na + 24 * c.ne;
+  if (n == 0) return;
+  KernelTimer t(c, "nve_final");
+  k_nve_final<<<nblk(n, 256), 256, 0, c.stream>>>(c.v.p, c.f.p, 3 * c.na, c.nodev.p, c.nodef.p,
+                                                  24 * c.ne, dtfm);
+}
+
+}  // namespace cacb200

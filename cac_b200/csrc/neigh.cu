@@ -1,0 +1,817 @@
+// Periodic wrap, cell binning and neighbour-list construction.
+//
+// Lists hold, for every i-site (atoms, then the 8 Gauss points of each
+// element), the atoms and element lattice sites within cutneigh = cut + skin,
+// with the periodic image of each neighbour.  Membership is decided in the
+// reference's FP64 arithmetic, so the sets equal the reference's bit for bit:
+//   atom j:           rsq of xi - (xj + s*L)          (npair_half_bin_newton.cpp:116-120)
+//   lattice site j:   xi - sum_k N_k (xnode_k + s*L)  subtracted node by node
+//                                                     (npair_half_bin_newton.cpp:194-200)
+// with products and differences rounded separately (no FMA).
+//
+// Candidates come from two periodic cell grids instead of the reference's
+// bin/stencil/sub-element walk: atoms from a grid of cell >= cutneigh/2 with a
+// 5x5x5 stencil, element sites from a grid over element centres of cell
+// >= cutneigh + (centre-to-node radius + affine deviation), and for each
+// candidate element only the lattice sites whose affine position can lie
+// within cutneigh (a box in lattice-index space).  Both prunings are exact
+// supersets, so they change cost, not membership.
+//
+// Storage rules (the reference's, restated):
+//   full  (npair_full_bin.cpp:23-358): every neighbour except the site itself.
+//   half  (npair_half_bin_newton.cpp:25-392): an atom keeps atom j when j's
+//         reference bin is in its upper half stencil, or in the same bin when j
+//         is owned and later in order, or a ghost "above and to the right";
+//         it keeps every lattice site.  A Gauss point keeps no atoms, every
+//         non-Gauss lattice site, and a Gauss site once: owned (element i < j,
+//         or same element and igcell < jgcell) or ghost with its element
+//         centre above and to the right.
+#include <cub/cub.cuh>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <tuple>
+
+#include "ctx.cuh"
+#include "device.cuh"
+
+namespace cacb200 {
+
+namespace {
+
+constexpr int KIND_SITE = 1 << 30;  // build-time entry flag: lattice site (gid = e*729+u)
+
+// ------------------------------------------------------------------ pbc
+
+// Domain::pbc for owned atoms (domain.cpp:562-630)
+__global__ void k_pbc_atoms(double4 *xs, int na, BoxD b) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= na) return;
+  double4 p = xs[i];
+  double *q = &p.x;
+#pragma unroll
+  for (int d = 0; d < 3; d++) {
+    double x = q[d];
+    if (x < b.lo[d]) x += b.L[d];
+    if (x >= b.hi[d]) {
+      x -= b.L[d];
+      x = fmax(x, b.lo[d]);
+    }
+    q[d] = x;
+  }
+  xs[i] = p;
+}
+
+// Element centre (ElementVecCAC::update_center_coord, element_vec_cac.cpp:3740-3765),
+// Domain::pbc for elements (domain.cpp:645-720 with update_node_coord,
+// element_vec_cac.cpp:3772-3785), then the geometry used by the candidate
+// search: affine frame n0 + i a + j b + k c of the lattice sites, its inverse,
+// the largest deviation of the trilinear nodes from that frame, and the
+// centre-to-node radius.
+//   eframe[e*16 + 0..2]  n0
+//   eframe[e*16 + 3..11] rows of the inverse frame matrix
+//   eframe[e*16 + 12]    dmax
+__global__ void k_elem_geom(double *nodex, int ne, BoxD b, double4 *ecenter, double *eframe,
+                            unsigned long long *reach_bits) {
+  int e = blockIdx.x * blockDim.x + threadIdx.x;
+  double reach = 0.0;
+  if (e < ne) {
+    double *nx = nodex + (size_t)e * 24;
+    double c[3];
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+      double s = 0.0;
+      for (int k = 0; k < NPE; k++) s = __dadd_rn(s, nx[3 * k + d]);
+      c[d] = s / NPE / 1;
+    }
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+      bool moved = false;
+      if (c[d] < b.lo[d]) {
+        c[d] += b.L[d];
+        moved = true;
+      }
+      if (c[d] >= b.hi[d]) {
+        c[d] -= b.L[d];
+        c[d] = fmax(c[d], b.lo[d]);
+        moved = true;
+      }
+      if (moved) {
+        double s = 0.0;
+        for (int k = 0; k < NPE; k++) s = __dadd_rn(s, nx[3 * k + d]);
+        double sh = c[d] - s / NPE / 1;
+        for (int k = 0; k < NPE; k++) nx[3 * k + d] += sh;
+      }
+    }
+    double R = 0.0;
+    for (int k = 0; k < NPE; k++) {
+      double dx = nx[3 * k] - c[0], dy = nx[3 * k + 1] - c[1], dz = nx[3 * k + 2] - c[2];
+      R = fmax(R, sqrt(dx * dx + dy * dy + dz * dz));
+    }
+    double n0[3], A[3][3];  // columns a, b, c
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+      n0[d] = nx[d];
+      A[d][0] = (nx[3 * 1 + d] - n0[d]) / (NC - 1);
+      A[d][1] = (nx[3 * 3 + d] - n0[d]) / (NC - 1);
+      A[d][2] = (nx[3 * 4 + d] - n0[d]) / (NC - 1);
+    }
+    double dmax = 0.0;
+    for (int k = 0; k < NPE; k++) {
+      double dev2 = 0.0;
+#pragma unroll
+      for (int d = 0; d < 3; d++) {
+        double aff = n0[d] + (NC - 1) * (node_xi(k) * A[d][0] + node_eta(k) * A[d][1] +
+                                         node_zeta(k) * A[d][2]);
+        double t = nx[3 * k + d] - aff;
+        dev2 += t * t;
+      }
+      dmax = fmax(dmax, sqrt(dev2));
+    }
+    // inverse of the 3x3 frame
+    double det = A[0][0] * (A[1][1] * A[2][2] - A[1][2] * A[2][1]) -
+                 A[0][1] * (A[1][0] * A[2][2] - A[1][2] * A[2][0]) +
+                 A[0][2] * (A[1][0] * A[2][1] - A[1][1] * A[2][0]);
+    double id = 1.0 / det;
+    double inv[3][3];
+    inv[0][0] = (A[1][1] * A[2][2] - A[1][2] * A[2][1]) * id;
+    inv[0][1] = (A[0][2] * A[2][1] - A[0][1] * A[2][2]) * id;
+    inv[0][2] = (A[0][1] * A[1][2] - A[0][2] * A[1][1]) * id;
+    inv[1][0] = (A[1][2] * A[2][0] - A[1][0] * A[2][2]) * id;
+    inv[1][1] = (A[0][0] * A[2][2] - A[0][2] * A[2][0]) * id;
+    inv[1][2] = (A[0][2] * A[1][0] - A[0][0] * A[1][2]) * id;
+    inv[2][0] = (A[1][0] * A[2][1] - A[1][1] * A[2][0]) * id;
+    inv[2][1] = (A[0][1] * A[2][0] - A[0][0] * A[2][1]) * id;
+    inv[2][2] = (A[0][0] * A[1][1] - A[0][1] * A[1][0]) * id;
+    double *fr = eframe + (size_t)e * 16;
+    fr[0] = n0[0];
+    fr[1] = n0[1];
+    fr[2] = n0[2];
+#pragma unroll
+    for (int r = 0; r < 3; r++)
+#pragma unroll
+      for (int q = 0; q < 3; q++) fr[3 + 3 * r + q] = inv[r][q];
+    fr[12] = dmax;
+    ecenter[e] = make_double4(c[0], c[1], c[2], R);
+    reach = R + dmax;
+  }
+  // block max into reach_bits (non-negative doubles order like their bit patterns)
+  for (int o = 16; o > 0; o >>= 1) reach = fmax(reach, __shfl_down_sync(0xffffffffu, reach, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(reach_bits, (unsigned long long)__double_as_longlong(reach));
+}
+
+// ---------------------------------------------------------------- binning
+
+__device__ __forceinline__ int grid_cell(const Grid &g, const BoxD &b, const double *w) {
+  int c[3];
+#pragma unroll
+  for (int d = 0; d < 3; d++) {
+    int v = (int)((w[d] - b.lo[d]) * g.inv[d]);
+    c[d] = min(max(v, 0), g.nc[d] - 1);
+  }
+  return (c[2] * g.nc[1] + c[1]) * g.nc[0] + c[0];
+}
+
+__global__ void k_atom_keys(const double4 *xs, int na, Grid g, BoxD b, int *key, int *idx) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= na) return;
+  double4 p = xs[i];
+  double w[3] = {p.x, p.y, p.z};
+  key[i] = grid_cell(g, b, w);
+  idx[i] = i;
+}
+
+__global__ void k_elem_keys(const double4 *ecenter, int ne, Grid g, BoxD b, int *key, int *idx) {
+  int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= ne) return;
+  double4 p = ecenter[e];
+  double w[3] = {p.x, p.y, p.z};
+  key[e] = grid_cell(g, b, w);
+  idx[e] = e;
+}
+
+// cell_start[c] = first sorted position with key >= c, for c in [0, ncell]
+__global__ void k_cell_start(const int *skey, int n, int ncell, int *start) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k > n) return;
+  int prev = (k == 0) ? -1 : skey[k - 1];
+  int cur = (k == n) ? ncell : skey[k];
+  for (int c = prev + 1; c <= cur; c++) start[c] = k;
+}
+
+__global__ void k_gather_pos(const double4 *xs, const int *sidx, int n, double4 *out) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  int i = sidx[k];
+  double4 p = xs[i];
+  p.w = __longlong_as_double((long long)i);
+  out[k] = p;
+}
+
+// -------------------------------------------------------------- the build
+
+struct BuildArgs {
+  const double4 *xs;          // atom positions (first na entries)
+  const double *nodex;
+  const double4 *ecenter;
+  const double *eframe;
+  const int *acell_start;
+  const double4 *acell_pos;
+  const int *ecell_start;
+  const int *ecell_elems;
+  int na, ne, nsi, cap;
+  Grid ag, eg;
+  BoxD b;
+  RefBins rb;
+  double cutneigh, cutneighsq;
+  int want_half;
+  int *raw_full, *num_full;
+  unsigned char *img_full;
+  int *raw_half, *num_half;
+  unsigned char *img_half;
+  int *overflow;              // [0] flag, [1] max count, [2] bad image
+};
+
+__device__ __forceinline__ int ref_bin1(const RefBins &rb, int d, double x) {
+  int ix;
+  if (x >= rb.hi[d]) ix = (int)((x - rb.hi[d]) * rb.inv[d]) + rb.nbin[d];
+  else if (x >= rb.lo[d]) {
+    ix = (int)((x - rb.lo[d]) * rb.inv[d]);
+    ix = min(ix, rb.nbin[d] - 1);
+  } else ix = (int)((x - rb.lo[d]) * rb.inv[d]) - 1;
+  return ix;
+}
+
+// >0: q's reference bin is in p's upper half stencil; 0: same bin; <0 otherwise
+__device__ __forceinline__ int ref_bin_order(const RefBins &rb, const double *p, const double *q) {
+#pragma unroll
+  for (int d = 2; d >= 0; d--) {
+    int a = ref_bin1(rb, d, p[d]), c = ref_bin1(rb, d, q[d]);
+    if (c != a) return c > a ? 1 : -1;
+  }
+  return 0;
+}
+
+__device__ __forceinline__ bool above_right(const double *q, const double *p) {
+  if (q[2] < p[2]) return false;
+  if (q[2] == p[2]) {
+    if (q[1] < p[1]) return false;
+    if (q[1] == p[1] && q[0] < p[0]) return false;
+  }
+  return true;
+}
+
+__device__ __forceinline__ double rsq_rn(double dx, double dy, double dz) {
+  return __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
+}
+
+__device__ __forceinline__ void emit(const BuildArgs &A, int i, int &n, int *raw, unsigned char *img,
+                                     int val, int code) {
+  if (n < A.cap) {
+    raw[(size_t)n * A.nsi + i] = val;
+    img[(size_t)n * A.nsi + i] = (unsigned char)code;
+  }
+  n++;
+}
+
+__global__ void __launch_bounds__(128) k_build(BuildArgs A) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= A.nsi) return;
+  const bool iatom = i < A.na;
+  int ie = -1, ig = -1, iu = -1;
+  double xi[3];
+  if (iatom) {
+    double4 p = A.xs[i];
+    xi[0] = p.x;
+    xi[1] = p.y;
+    xi[2] = p.z;
+  } else {
+    ie = (i - A.na) / NG;
+    ig = (i - A.na) % NG;
+    iu = gauss_site(ig);
+    const double *nx = A.nodex + (size_t)ie * 24 + 3 * gauss_node(ig);
+    xi[0] = nx[0];
+    xi[1] = nx[1];
+    xi[2] = nx[2];
+  }
+  // wrapped query point: wi = xi + ti L inside the box
+  double wi[3];
+  int ti[3];
+#pragma unroll
+  for (int d = 0; d < 3; d++) {
+    double f = floor((xi[d] - A.b.lo[d]) / A.b.L[d]);
+    ti[d] = -(int)f;
+    wi[d] = xi[d] - f * A.b.L[d];
+    if (wi[d] >= A.b.hi[d]) {
+      wi[d] -= A.b.L[d];
+      ti[d] -= 1;
+    }
+    if (wi[d] < A.b.lo[d]) {
+      wi[d] += A.b.L[d];
+      ti[d] += 1;
+    }
+  }
+  const double pre = (A.cutneigh + 1e-6) * (A.cutneigh + 1e-6);
+  int nf = 0, nh = 0;
+
+  // ------------------------------------------------------------- atoms
+  if (A.na > 0) {
+    int ci[3];
+#pragma unroll
+    for (int d = 0; d < 3; d++)
+      ci[d] = min(max((int)((wi[d] - A.b.lo[d]) * A.ag.inv[d]), 0), A.ag.nc[d] - 1);
+    for (int oz = -2; oz <= 2; oz++) {
+      int cz = ci[2] + oz, Wz = 0;
+      while (cz < 0) { cz += A.ag.nc[2]; Wz--; }
+      while (cz >= A.ag.nc[2]) { cz -= A.ag.nc[2]; Wz++; }
+      for (int oy = -2; oy <= 2; oy++) {
+        int cy = ci[1] + oy, Wy = 0;
+        while (cy < 0) { cy += A.ag.nc[1]; Wy--; }
+        while (cy >= A.ag.nc[1]) { cy -= A.ag.nc[1]; Wy++; }
+        for (int ox = -2; ox <= 2; ox++) {
+          int cx = ci[0] + ox, Wx = 0;
+          while (cx < 0) { cx += A.ag.nc[0]; Wx--; }
+          while (cx >= A.ag.nc[0]) { cx -= A.ag.nc[0]; Wx++; }
+          int cell = (cz * A.ag.nc[1] + cy) * A.ag.nc[0] + cx;
+          int s[3] = {Wx - ti[0], Wy - ti[1], Wz - ti[2]};
+          double sh[3] = {Wx * A.b.L[0], Wy * A.b.L[1], Wz * A.b.L[2]};
+          int beg = A.acell_start[cell], end = A.acell_start[cell + 1];
+          for (int k = beg; k < end; k++) {
+            double4 pj = A.acell_pos[k];
+            double ex = wi[0] - (pj.x + sh[0]), ey = wi[1] - (pj.y + sh[1]), ez = wi[2] - (pj.z + sh[2]);
+            if (ex * ex + ey * ey + ez * ez > pre) continue;
+            int j = (int)__double_as_longlong(pj.w);
+            bool zero = (s[0] == 0 && s[1] == 0 && s[2] == 0);
+            if (iatom && j == i && zero) continue;
+            if (s[0] < -1 || s[0] > 1 || s[1] < -1 || s[1] > 1 || s[2] < -1 || s[2] > 1) {
+              atomicExch(&A.overflow[2], 1);
+              continue;
+            }
+            double4 xj = A.xs[j];
+            double q[3] = {xj.x, xj.y, xj.z};
+            if (!zero) {
+              q[0] = s[0] ? __dadd_rn(q[0], s[0] * A.b.L[0]) : q[0];
+              q[1] = s[1] ? __dadd_rn(q[1], s[1] * A.b.L[1]) : q[1];
+              q[2] = s[2] ? __dadd_rn(q[2], s[2] * A.b.L[2]) : q[2];
+            }
+            double rsq = rsq_rn(__dsub_rn(xi[0], q[0]), __dsub_rn(xi[1], q[1]), __dsub_rn(xi[2], q[2]));
+            if (!(rsq <= A.cutneighsq)) continue;
+            int code = img_code(s[0], s[1], s[2]);
+            emit(A, i, nf, A.raw_full, A.img_full, j, code);
+            if (A.want_half && iatom) {
+              int ord = ref_bin_order(A.rb, xi, q);
+              bool keep = ord > 0 || (ord == 0 && (zero ? (j > i) : above_right(q, xi)));
+              if (keep) emit(A, i, nh, A.raw_half, A.img_half, j, code);
+            }
+          }
+        }
+      }
+    }
+  }
+
+  // --------------------------------------------------- element lattice sites
+  if (A.ne > 0) {
+    int ci[3];
+#pragma unroll
+    for (int d = 0; d < 3; d++)
+      ci[d] = min(max((int)((wi[d] - A.b.lo[d]) * A.eg.inv[d]), 0), A.eg.nc[d] - 1);
+    double icen[3] = {0, 0, 0};
+    if (!iatom) {
+      double4 c = A.ecenter[ie];
+      icen[0] = c.x;
+      icen[1] = c.y;
+      icen[2] = c.z;
+    }
+    for (int oz = -1; oz <= 1; oz++) {
+      int cz = ci[2] + oz, Wz = 0;
+      while (cz < 0) { cz += A.eg.nc[2]; Wz--; }
+      while (cz >= A.eg.nc[2]) { cz -= A.eg.nc[2]; Wz++; }
+      for (int oy = -1; oy <= 1; oy++) {
+        int cy = ci[1] + oy, Wy = 0;
+        while (cy < 0) { cy += A.eg.nc[1]; Wy--; }
+        while (cy >= A.eg.nc[1]) { cy -= A.eg.nc[1]; Wy++; }
+        for (int ox = -1; ox <= 1; ox++) {
+          int cx = ci[0] + ox, Wx = 0;
+          while (cx < 0) { cx += A.eg.nc[0]; Wx--; }
+          while (cx >= A.eg.nc[0]) { cx -= A.eg.nc[0]; Wx++; }
+          int cell = (cz * A.eg.nc[1] + cy) * A.eg.nc[0] + cx;
+          int s[3] = {Wx - ti[0], Wy - ti[1], Wz - ti[2]};
+          bool zero = (s[0] == 0 && s[1] == 0 && s[2] == 0);
+          double sL[3] = {s[0] * A.b.L[0], s[1] * A.b.L[1], s[2] * A.b.L[2]};
+          int beg = A.ecell_start[cell], end = A.ecell_start[cell + 1];
+          for (int kk = beg; kk < end; kk++) {
+            int e = A.ecell_elems[kk];
+            double4 ce = A.ecenter[e];
+            // quick sphere test on the raw frame: |xi - s L - centre| <= cutneigh + R
+            double p[3] = {xi[0] - sL[0], xi[1] - sL[1], xi[2] - sL[2]};
+            const double *fr = A.eframe + (size_t)e * 16;
+            double dmax = fr[12];
+            double R = ce.w + dmax + A.cutneigh + 1e-6;
+            double dcx = p[0] - ce.x, dcy = p[1] - ce.y, dcz = p[2] - ce.z;
+            if (dcx * dcx + dcy * dcy + dcz * dcz > R * R) continue;
+            if (s[0] < -1 || s[0] > 1 || s[1] < -1 || s[1] > 1 || s[2] < -1 || s[2] > 1) {
+              atomicExch(&A.overflow[2], 1);
+              continue;
+            }
+            // lattice-index box of sites whose affine position is within cutneigh + dmax
+            double rel[3] = {p[0] - fr[0], p[1] - fr[1], p[2] - fr[2]};
+            int lo[3], hi[3];
+            bool empty = false;
+#pragma unroll
+            for (int r = 0; r < 3; r++) {
+              double a0 = fr[3 + 3 * r], a1 = fr[4 + 3 * r], a2 = fr[5 + 3 * r];
+              double fidx = a0 * rel[0] + a1 * rel[1] + a2 * rel[2];
+              double rho = (A.cutneigh + dmax + 1e-6) * sqrt(a0 * a0 + a1 * a1 + a2 * a2) + 1e-6;
+              lo[r] = max(0, (int)ceil(fidx - rho));
+              hi[r] = min(NC - 1, (int)floor(fidx + rho));
+              if (lo[r] > hi[r]) empty = true;
+            }
+            if (empty) continue;
+            const double *nx = A.nodex + (size_t)e * 24;
+            double g[24];  // ghost node coordinates nodex + s L
+#pragma unroll
+            for (int k = 0; k < 8; k++)
+#pragma unroll
+              for (int d = 0; d < 3; d++)
+                g[3 * k + d] = s[d] ? __dadd_rn(nx[3 * k + d], sL[d]) : nx[3 * k + d];
+            int code = img_code(s[0], s[1], s[2]);
+            double qcen[3] = {0, 0, 0};
+            if (!zero) {
+              qcen[0] = s[0] ? __dadd_rn(ce.x, sL[0]) : ce.x;
+              qcen[1] = s[1] ? __dadd_rn(ce.y, sL[1]) : ce.y;
+              qcen[2] = s[2] ? __dadd_rn(ce.z, sL[2]) : ce.z;
+            }
+            for (int a = lo[0]; a <= hi[0]; a++)
+              for (int bb = lo[1]; bb <= hi[1]; bb++)
+                for (int cc = lo[2]; cc <= hi[2]; cc++) {
+                  int u = (a * NC + bb) * NC + cc;
+                  if (!iatom && e == ie && u == iu && zero) continue;
+                  double dx = xi[0], dy = xi[1], dz = xi[2];
+#pragma unroll
+                  for (int k = 0; k < 8; k++) {
+                    double N = shape_val(u, k);
+                    dx = __dsub_rn(dx, __dmul_rn(N, g[3 * k]));
+                    dy = __dsub_rn(dy, __dmul_rn(N, g[3 * k + 1]));
+                    dz = __dsub_rn(dz, __dmul_rn(N, g[3 * k + 2]));
+                  }
+                  double rsq = rsq_rn(dx, dy, dz);
+                  if (!(rsq <= A.cutneighsq)) continue;
+                  int val = KIND_SITE | (e * NU + u);
+                  emit(A, i, nf, A.raw_full, A.img_full, val, code);
+                  if (A.want_half) {
+                    bool keep = true;
+                    if (!iatom) {
+                      int jg = site_gauss(u);
+                      if (jg >= 0) {
+                        if (zero) keep = (ie < e) || (ie == e && ig < jg);
+                        else keep = above_right(qcen, icen);
+                      }
+                    }
+                    if (keep) emit(A, i, nh, A.raw_half, A.img_half, val, code);
+                  }
+                }
+          }
+        }
+      }
+    }
+  }
+  A.num_full[i] = nf;
+  if (A.want_half) A.num_half[i] = nh;
+  int m = max(nf, nh);
+  if (m > A.cap) {
+    atomicExch(&A.overflow[0], 1);
+    atomicMax(&A.overflow[1], m);
+  }
+}
+
+// ------------------------------------------------------------- compaction
+
+__global__ void k_mark_sites(const int *raw, const int *num, int nsi, int cap, int *flag) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nsi) return;
+  int n = min(num[i], cap);
+  for (int k = 0; k < n; k++) {
+    int v = raw[(size_t)k * nsi + i];
+    if (v & KIND_SITE) {
+      int gid = v & ~KIND_SITE;
+      if (site_gauss(gid % NU) < 0) flag[gid] = 1;
+    }
+  }
+}
+
+__global__ void k_act_table(const int *flag, const int *pref, int ngid, int ne, int *act_gid,
+                            int *act_off, int nact) {
+  int gid = blockIdx.x * blockDim.x + threadIdx.x;
+  if (gid < ngid && flag[gid]) act_gid[pref[gid]] = gid;
+  if (gid < ne) act_off[gid] = pref[gid * NU];
+  if (gid == 0) act_off[ne] = nact;
+}
+
+__global__ void k_remap(const int *raw, const unsigned char *img, const int *num, int nsi, int cap,
+                        const int *pref, int na, int ne, int *out) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nsi) return;
+  int n = min(num[i], cap);
+  for (int k = 0; k < n; k++) {
+    size_t o = (size_t)k * nsi + i;
+    int v = raw[o];
+    int sidx;
+    if (v & KIND_SITE) {
+      int gid = v & ~KIND_SITE;
+      int e = gid / NU, u = gid % NU;
+      int g = site_gauss(u);
+      sidx = (g >= 0) ? na + NG * e + g : na + NG * ne + pref[gid];
+    } else {
+      sidx = v;
+    }
+    out[o] = (sidx << IMG_BITS) | img[o];
+  }
+}
+
+inline int nblk(long n, int t) { return (int)((n + t - 1) / t); }
+
+void setup_grids(Ctx &c, double ereach) {
+  // reference atom bins (nbin_standard.cpp:84-128), orthogonal box
+  double binsize_optimal = 0.5 * c.cutneigh;
+  double binsizeinv = 1.0 / binsize_optimal;
+  for (int d = 0; d < 3; d++) {
+    double bbox = c.boxhi[d] - c.boxlo[d];
+    c.rbins.lo[d] = c.boxlo[d];
+    c.rbins.hi[d] = c.boxhi[d];
+    int nb = (int)(bbox * binsizeinv);
+    if (nb == 0) nb = 1;
+    c.rbins.nbin[d] = nb;
+    double bs = bbox / nb;
+    c.rbins.inv[d] = 1.0 / bs;
+  }
+  // candidate grids
+  for (int d = 0; d < 3; d++) {
+    double L = c.prd[d];
+    int na_c = (int)(L / (0.5 * c.cutneigh));
+    if (na_c < 1) throw Error(CACB200_EINVAL, "box shorter than half the neighbour cutoff");
+    c.agrid.nc[d] = na_c;
+    c.agrid.inv[d] = na_c / L;
+    double reach = c.cutneigh + ereach + 1e-6;
+    if (c.ne > 0 && L < reach)
+      throw Error(CACB200_EINVAL, "box shorter than the cutoff plus the element radius in dimension " +
+                                      std::to_string(d));
+    int ne_c = std::max(1, (int)(L / reach));
+    c.egrid.nc[d] = ne_c;
+    c.egrid.inv[d] = ne_c / L;
+  }
+  c.agrid.ncell = c.agrid.nc[0] * c.agrid.nc[1] * c.agrid.nc[2];
+  c.egrid.ncell = c.egrid.nc[0] * c.egrid.nc[1] * c.egrid.nc[2];
+}
+
+template <class K>
+void sort_pairs(Ctx &c, int *keys_in, int *keys_out, int *vals_in, int *vals_out, int n, int maxkey) {
+  size_t bytes = 0;
+  int bits = 1;
+  while ((1 << bits) <= maxkey && bits < 31) bits++;
+  cub::DeviceRadixSort::SortPairs(nullptr, bytes, keys_in, keys_out, vals_in, vals_out, n, 0, bits,
+                                  c.stream);
+  c.cub_tmp.reserve(bytes);
+  CACB200_CUDA(cub::DeviceRadixSort::SortPairs(c.cub_tmp.p, bytes, keys_in, keys_out, vals_in,
+                                               vals_out, n, 0, bits, c.stream));
+}
+
+}  // namespace
+
+void pbc_wrap(Ctx &c) {
+  BoxD b = make_box(c);
+  if (c.na) k_pbc_atoms<<<nblk(c.na, 256), 256, 0, c.stream>>>(c.xs.p, c.na, b);
+}
+
+void neigh_build(Ctx &c, bool want_half) {
+  c.check_system();
+  if (c.pp.style == CACB200_PAIR_NONE) throw Error(CACB200_ESTATE, "no pair style set");
+  BoxD b = make_box(c);
+  double cutoff = std::sqrt(c.pp.cut * c.pp.cut);
+  c.cutneigh = cutoff + c.skin;
+  c.cutneighsq = c.cutneigh * c.cutneigh;
+
+  // periodic wrap, element geometry
+  {
+    KernelTimer t(c, "pbc_geom");
+    if (c.na) k_pbc_atoms<<<nblk(c.na, 256), 256, 0, c.stream>>>(c.xs.p, c.na, b);
+    c.ecenter.reserve(std::max(c.ne, 1));
+    c.eframe.reserve((size_t)std::max(c.ne, 1) * 16);
+    c.overflow.reserve(8);
+    CACB200_CUDA(cudaMemsetAsync(c.overflow.p, 0, 8 * sizeof(int), c.stream));
+    if (c.ne)
+      k_elem_geom<<<nblk(c.ne, 128), 128, 0, c.stream>>>(c.nodex.p, c.ne, b, c.ecenter.p, c.eframe.p,
+                                                         (unsigned long long *)(c.overflow.p + 4));
+  }
+  unsigned long long reach_bits = 0;
+  if (c.ne) {
+    CACB200_CUDA(cudaMemcpyAsync(&reach_bits, c.overflow.p + 4, sizeof(reach_bits),
+                                 cudaMemcpyDeviceToHost, c.stream));
+    CACB200_CUDA(cudaStreamSynchronize(c.stream));
+  }
+  double ereach;
+  std::memcpy(&ereach, &reach_bits, sizeof(double));
+  setup_grids(c, c.ne ? ereach : 0.0);
+
+  // binning: atoms and elements by cell, stable by index
+  {
+    KernelTimer t(c, "bin");
+    int nmax = std::max(std::max(c.na, c.ne), 1);
+    c.cell_key.reserve(nmax);
+    c.cell_key2.reserve(nmax);
+    c.idx_tmp.reserve(nmax);
+    c.idx_tmp2.reserve(nmax);
+    c.acell_start.reserve(c.agrid.ncell + 1);
+    c.acell_pos.reserve(std::max(c.na, 1));
+    c.ecell_start.reserve(c.egrid.ncell + 1);
+    c.ecell_elems.reserve(std::max(c.ne, 1));
+    if (c.na) {
+      k_atom_keys<<<nblk(c.na, 256), 256, 0, c.stream>>>(c.xs.p, c.na, c.agrid, b, c.cell_key.p,
+                                                         c.idx_tmp.p);
+      sort_pairs<int>(c, c.cell_key.p, c.cell_key2.p, c.idx_tmp.p, c.idx_tmp2.p, c.na, c.agrid.ncell);
+      k_cell_start<<<nblk(c.na + 1, 256), 256, 0, c.stream>>>(c.cell_key2.p, c.na, c.agrid.ncell,
+                                                              c.acell_start.p);
+      k_gather_pos<<<nblk(c.na, 256), 256, 0, c.stream>>>(c.xs.p, c.idx_tmp2.p, c.na, c.acell_pos.p);
+    } else {
+      CACB200_CUDA(cudaMemsetAsync(c.acell_start.p, 0, sizeof(int) * (c.agrid.ncell + 1), c.stream));
+    }
+    if (c.ne) {
+      k_elem_keys<<<nblk(c.ne, 256), 256, 0, c.stream>>>(c.ecenter.p, c.ne, c.egrid, b, c.cell_key.p,
+                                                         c.idx_tmp.p);
+      sort_pairs<int>(c, c.cell_key.p, c.cell_key2.p, c.idx_tmp.p, c.ecell_elems.p, c.ne, c.egrid.ncell);
+      k_cell_start<<<nblk(c.ne + 1, 256), 256, 0, c.stream>>>(c.cell_key2.p, c.ne, c.egrid.ncell,
+                                                              c.ecell_start.p);
+    } else {
+      CACB200_CUDA(cudaMemsetAsync(c.ecell_start.p, 0, sizeof(int) * (c.egrid.ncell + 1), c.stream));
+    }
+  }
+
+  const int nsi = c.nsite_i();
+  for (int attempt = 0; attempt < 3; attempt++) {
+    size_t slots = (size_t)c.cap * nsi;
+    c.raw_full.reserve(slots);
+    c.img_full.reserve(slots);
+    c.num_full.reserve(nsi);
+    if (want_half) {
+      c.raw_half.reserve(slots);
+      c.img_half.reserve(slots);
+      c.num_half.reserve(nsi);
+    }
+    CACB200_CUDA(cudaMemsetAsync(c.overflow.p, 0, 4 * sizeof(int), c.stream));
+    BuildArgs A;
+    A.xs = c.xs.p;
+    A.nodex = c.nodex.p;
+    A.ecenter = c.ecenter.p;
+    A.eframe = c.eframe.p;
+    A.acell_start = c.acell_start.p;
+    A.acell_pos = c.acell_pos.p;
+    A.ecell_start = c.ecell_start.p;
+    A.ecell_elems = c.ecell_elems.p;
+    A.na = c.na;
+    A.ne = c.ne;
+    A.nsi = nsi;
+    A.cap = c.cap;
+    A.ag = c.agrid;
+    A.eg = c.egrid;
+    A.b = b;
+    A.rb = c.rbins;
+    A.cutneigh = c.cutneigh;
+    A.cutneighsq = c.cutneighsq;
+    A.want_half = want_half ? 1 : 0;
+    A.raw_full = c.raw_full.p;
+    A.num_full = c.num_full.p;
+    A.img_full = c.img_full.p;
+    A.raw_half = want_half ? c.raw_half.p : nullptr;
+    A.num_half = want_half ? c.num_half.p : nullptr;
+    A.img_half = want_half ? c.img_half.p : nullptr;
+    A.overflow = c.overflow.p;
+    {
+      KernelTimer t(c, "build_list");
+      k_build<<<nblk(nsi, 128), 128, 0, c.stream>>>(A);
+    }
+    int ov[4];
+    CACB200_CUDA(cudaMemcpyAsync(ov, c.overflow.p, sizeof(ov), cudaMemcpyDeviceToHost, c.stream));
+    CACB200_CUDA(cudaStreamSynchronize(c.stream));
+    if (ov[2]) throw Error(CACB200_EINVAL, "neighbour image beyond the first periodic image (box too small)");
+    if (!ov[0]) break;
+    c.cap = ((ov[1] + 31) / 32) * 32;
+    if (attempt == 2) throw Error(CACB200_EOVERFLOW, "neighbour list capacity");
+  }
+
+  // compact referenced lattice sites into the site table
+  {
+    KernelTimer t(c, "compact");
+    size_t ngid = (size_t)c.ne * NU;
+    c.site_flag.reserve(ngid + 1);
+    c.site_pref.reserve(ngid + 1);
+    int *flag = c.site_flag.p;
+    int *pref = c.site_pref.p;
+    int nact = 0;
+    if (ngid) {
+      CACB200_CUDA(cudaMemsetAsync(flag, 0, sizeof(int) * (ngid + 1), c.stream));
+      k_mark_sites<<<nblk(nsi, 256), 256, 0, c.stream>>>(c.raw_full.p, c.num_full.p, nsi, c.cap, flag);
+      size_t bytes = 0;
+      cub::DeviceScan::ExclusiveSum(nullptr, bytes, flag, pref, (int)(ngid + 1), c.stream);
+      c.cub_tmp.reserve(bytes);
+      CACB200_CUDA(cub::DeviceScan::ExclusiveSum(c.cub_tmp.p, bytes, flag, pref, (int)(ngid + 1), c.stream));
+      CACB200_CUDA(cudaMemcpyAsync(&nact, pref + ngid, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+      CACB200_CUDA(cudaStreamSynchronize(c.stream));
+    }
+    c.nact = nact;
+    c.act_gid.reserve(std::max(nact, 1));
+    c.act_off.reserve(c.ne + 1);
+    if (ngid)
+      k_act_table<<<nblk((long)ngid, 256), 256, 0, c.stream>>>(flag, pref, (int)ngid, c.ne, c.act_gid.p,
+                                                              c.act_off.p, nact);
+    // grow the site table, keeping the atom positions it holds
+    size_t ns = (size_t)c.nsite_s();
+    if (ns > c.xs.n) {
+      double4 *np_ = nullptr;
+      size_t want = ns + ns / 8 + 64;
+      if (cudaMalloc(&np_, want * sizeof(double4)) != cudaSuccess) {
+        cudaGetLastError();
+        throw Error(CACB200_ENOMEM, "site table allocation failed");
+      }
+      if (c.na)
+        CACB200_CUDA(cudaMemcpyAsync(np_, c.xs.p, sizeof(double4) * c.na, cudaMemcpyDeviceToDevice, c.stream));
+      CACB200_CUDA(cudaStreamSynchronize(c.stream));
+      cudaFree(c.xs.p);
+      c.xs.p = np_;
+      c.xs.n = want;
+    }
+    size_t slots = (size_t)c.cap * nsi;
+    c.nbr_full.reserve(slots);
+    k_remap<<<nblk(nsi, 256), 256, 0, c.stream>>>(c.raw_full.p, c.img_full.p, c.num_full.p, nsi, c.cap,
+                                                   pref, c.na, c.ne, c.nbr_full.p);
+    if (want_half) {
+      c.nbr_half.reserve(slots);
+      k_remap<<<nblk(nsi, 256), 256, 0, c.stream>>>(c.raw_half.p, c.img_half.p, c.num_half.p, nsi, c.cap,
+                                                     pref, c.na, c.ne, c.nbr_half.p);
+    }
+  }
+  c.have_half = want_half;
+  c.lists_valid = true;
+  c.build_count++;
+  CACB200_CUDA(cudaGetLastError());
+}
+
+void neigh_download(Ctx &c, bool half, int64_t *offset, int8_t *kind, int32_t *idx, int32_t *site,
+                    int8_t *img, int64_t *nentries) {
+  if (!c.lists_valid || (half && !c.have_half)) throw Error(CACB200_ESTATE, "list not built");
+  const int nsi = c.nsite_i();
+  std::vector<int> num(nsi);
+  std::vector<int> ent((size_t)c.cap * nsi);
+  std::vector<int> act(std::max(c.nact, 1));
+  CACB200_CUDA(cudaStreamSynchronize(c.stream));
+  CACB200_CUDA(cudaMemcpy(num.data(), half ? c.num_half.p : c.num_full.p, sizeof(int) * nsi,
+                          cudaMemcpyDeviceToHost));
+  CACB200_CUDA(cudaMemcpy(ent.data(), half ? c.nbr_half.p : c.nbr_full.p, sizeof(int) * ent.size(),
+                          cudaMemcpyDeviceToHost));
+  if (c.nact)
+    CACB200_CUDA(cudaMemcpy(act.data(), c.act_gid.p, sizeof(int) * c.nact, cudaMemcpyDeviceToHost));
+  int64_t total = 0;
+  for (int i = 0; i < nsi; i++) total += num[i];
+  *nentries = total;
+  if (!offset) return;
+  int64_t pos = 0;
+  std::vector<std::tuple<int, int, int, int, int, int>> row;
+  for (int i = 0; i < nsi; i++) {
+    offset[i] = pos;
+    row.clear();
+    for (int k = 0; k < num[i]; k++) {
+      int v = ent[(size_t)k * nsi + i];
+      int sidx = v >> IMG_BITS, code = v & ((1 << IMG_BITS) - 1);
+      int sx, sy, sz;
+      img_decode(code, sx, sy, sz);
+      int kd, id, st;
+      if (sidx < c.na) {
+        kd = 0;
+        id = sidx;
+        st = -1;
+      } else if (sidx < c.na + NG * c.ne) {
+        kd = 1;
+        id = (sidx - c.na) / NG;
+        st = gauss_site((sidx - c.na) % NG);
+      } else {
+        int gid = act[sidx - c.na - NG * c.ne];
+        kd = 1;
+        id = gid / NU;
+        st = gid % NU;
+      }
+      row.emplace_back(kd, id, st, sx, sy, sz);
+    }
+    std::sort(row.begin(), row.end());
+    for (auto &t : row) {
+      kind[pos] = (int8_t)std::get<0>(t);
+      idx[pos] = std::get<1>(t);
+      site[pos] = std::get<2>(t);
+      img[3 * pos] = (int8_t)std::get<3>(t);
+      img[3 * pos + 1] = (int8_t)std::get<4>(t);
+      img[3 * pos + 2] = (int8_t)std::get<5>(t);
+      pos++;
+    }
+  }
+  offset[nsi] = pos;
+}
+
+}  // namespace cacb200

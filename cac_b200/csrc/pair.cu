@@ -1,0 +1,428 @@
+// Pair kernels: LJ 12-6 and two-pass EAM over the full neighbour list.
+//
+// Each i-site (atom or Gauss point) gathers over its own full list, so every
+// force, density and per-site energy is written once by one thread with no
+// atomics; the totals equal the reference's half-list sums with reactions
+// (pair_lj_cut.cpp:227-417, pair_eam.cpp:618-1031) up to summation order:
+//   * an atom's force is the sum over every neighbour; a Gauss point's force
+//     likewise (its atom neighbours are the reactions the reference applies
+//     from atom lists);
+//   * the global energy and virial are sum_i scale_i * sum_j term_ij with
+//     scale 1/2 for atoms and nodal_weight/2 for node Gauss points (the
+//     reference's iescale + jescale split over the two ends of a pair);
+//   * per-site energy and virial are half of each pair term (Pair::ev_tally,
+//     pair.cpp:428-482).
+// EAM evaluates F'(rho) once per site (atoms and nodes from their own
+// density, interpolated lattice sites from shape-weighted nodal density)
+// instead of once per pair, and keeps it in the w slot of the site table so
+// one 32-byte load brings a neighbour's position and F'.
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "ctx.cuh"
+#include "device.cuh"
+
+namespace cacb200 {
+
+namespace {
+
+inline int nblk(long n, int t) { return (int)((n + t - 1) / t); }
+
+struct PairArgs {
+  const double4 *xs;
+  const int *nbr;
+  const int *num;
+  int na, ne, nsi;
+  double L[3];
+  double *f, *gaussf;
+  double *eatom, *vatom, *enode, *vnode;
+  double *partial;
+  int eflag, vflag;
+  double escale_node, vscale_node;  // global scales of a node Gauss point
+};
+
+__device__ __forceinline__ void neighbour_pos(const PairArgs &A, int v, double4 &xj) {
+  int j = v >> IMG_BITS, code = v & ((1 << IMG_BITS) - 1);
+  xj = A.xs[j];
+  if (code != IMG_ZERO) {
+    int sx, sy, sz;
+    img_decode(code, sx, sy, sz);
+    xj.x += sx * A.L[0];
+    xj.y += sy * A.L[1];
+    xj.z += sz * A.L[2];
+  }
+}
+
+// Writes force and per-site energy/virial of i-site i and accumulates the
+// global sums (reduced per block in fixed order).
+__device__ __forceinline__ void finish_site(const PairArgs &A, int i, bool valid, const double fi[3],
+                                            double esum, const double vsum[6], double eextra_site,
+                                            double eextra_global) {
+  double red[7] = {0, 0, 0, 0, 0, 0, 0};
+  if (valid) {
+    bool atom = i < A.na;
+    int e = 0, g = 0, node = 0;
+    double *fo;
+    if (atom) {
+      fo = A.f + 3 * (size_t)i;
+    } else {
+      e = (i - A.na) / NG;
+      g = (i - A.na) % NG;
+      node = gauss_node(g);
+      fo = A.gaussf + (size_t)e * 24 + 3 * g;
+    }
+    fo[0] = fi[0];
+    fo[1] = fi[1];
+    fo[2] = fi[2];
+    double es = atom ? 0.5 : A.escale_node, vs = atom ? 0.5 : A.vscale_node;
+    if (A.eflag & CACB200_ENERGY_GLOBAL) red[0] = es * esum + eextra_global;
+    if (A.vflag & CACB200_VIRIAL_GLOBAL)
+#pragma unroll
+      for (int k = 0; k < 6; k++) red[1 + k] = vs * vsum[k];
+    if (A.eflag & CACB200_ENERGY_ATOM) {
+      double ev = 0.5 * esum + eextra_site;
+      if (atom) A.eatom[i] = ev;
+      else A.enode[(size_t)e * 8 + node] = ev;
+    }
+    if (A.vflag & CACB200_VIRIAL_ATOM) {
+      double *vo = atom ? A.vatom + 6 * (size_t)i : A.vnode + 48 * (size_t)e + 6 * node;
+#pragma unroll
+      for (int k = 0; k < 6; k++) vo[k] = 0.5 * vsum[k];
+    }
+  }
+  if (A.eflag || A.vflag) block_reduce_store<7>(red, A.partial);
+}
+
+// ------------------------------------------------------------------- LJ
+
+struct LjParams {
+  double cutsq, lj1, lj2, lj3, lj4, offset;
+};
+
+__global__ void __launch_bounds__(128) k_lj(PairArgs A, LjParams P) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  bool valid = i < A.nsi;
+  double fi[3] = {0, 0, 0}, esum = 0.0, vsum[6] = {0, 0, 0, 0, 0, 0};
+  if (valid) {
+    double4 xi = A.xs[i];
+    int n = A.num[i];
+    const int *nb = A.nbr + i;
+    for (int k = 0; k < n; k++) {
+      double4 xj;
+      neighbour_pos(A, nb[(size_t)k * A.nsi], xj);
+      double dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
+      double rsq = dx * dx + dy * dy + dz * dz;
+      if (rsq < P.cutsq) {
+        double r2inv = 1.0 / rsq;
+        double r6inv = r2inv * r2inv * r2inv;
+        double forcelj = r6inv * (P.lj1 * r6inv - P.lj2);
+        double fpair = forcelj * r2inv;
+        fi[0] += dx * fpair;
+        fi[1] += dy * fpair;
+        fi[2] += dz * fpair;
+        if (A.eflag) esum += r6inv * (P.lj3 * r6inv - P.lj4) - P.offset;
+        if (A.vflag) {
+          vsum[0] += dx * dx * fpair;
+          vsum[1] += dy * dy * fpair;
+          vsum[2] += dz * dz * fpair;
+          vsum[3] += dx * dy * fpair;
+          vsum[4] += dx * dz * fpair;
+          vsum[5] += dy * dz * fpair;
+        }
+      }
+    }
+  }
+  finish_site(A, i, valid, fi, esum, vsum, 0.0, 0.0);
+}
+
+// ------------------------------------------------------------------ EAM
+
+struct EamTables {
+  const double4 *rhor_val, *rhor_der, *z2r_val, *z2r_der, *frho_val, *frho_der;
+  double rdr, rdrho, rhomax, cutforcesq;
+  int nr, nrho;
+};
+
+// F'(rho) and F(rho) on the frho spline row (PairEAM::compute_fp,
+// pair_eam.cpp:1160-1169; the energy read on the same row, i.e. the
+// reference with its coefficient pointer returned to the caller)
+__device__ __forceinline__ double eam_fp(const EamTables &T, double rho, double *phi) {
+  double p = rho * T.rdrho + 1.0;
+  int m = (int)p;
+  m = max(1, min(m, T.nrho - 1));
+  p -= m;
+  p = fmin(p, 1.0);
+  double4 d = T.frho_der[m];
+  double fp = (d.x * p + d.y) * p + d.z;
+  if (phi) {
+    double4 v = T.frho_val[m];
+    double e = ((v.x * p + v.y) * p + v.z) * p + v.w;
+    if (rho > T.rhomax) e += fp * (rho - T.rhomax);
+    *phi = e;
+  }
+  return fp;
+}
+
+// pass 1: density at atoms and node Gauss points (pair_eam.cpp:707-812), then
+// F' at the site itself into xs[i].w (pair_eam.cpp:819-833 for atoms; for a
+// node the reference's rhoi = noderho at :901-903).
+__global__ void __launch_bounds__(128) k_eam_rho(PairArgs A, EamTables T, double *rho_out,
+                                                 double *phi_site) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= A.nsi) return;
+  double4 xi = A.xs[i];
+  int n = A.num[i];
+  const int *nb = A.nbr + i;
+  double rho = 0.0;
+  for (int k = 0; k < n; k++) {
+    double4 xj;
+    neighbour_pos(A, nb[(size_t)k * A.nsi], xj);
+    double dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
+    double rsq = dx * dx + dy * dy + dz * dz;
+    if (rsq < T.cutforcesq) {
+      double p = sqrt(rsq) * T.rdr + 1.0;
+      int m = (int)p;
+      m = max(1, min(m, T.nr - 1));
+      p -= m;
+      p = fmin(p, 1.0);
+      double4 c = T.rhor_val[m];
+      rho += ((c.x * p + c.y) * p + c.z) * p + c.w;
+    }
+  }
+  int slot = i;
+  if (i >= A.na) {
+    int e = (i - A.na) / NG, g = (i - A.na) % NG;
+    slot = A.na + 8 * e + gauss_node(g);
+  }
+  rho_out[slot] = rho;
+  double phi = 0.0;
+  double fp = eam_fp(T, rho, A.eflag ? &phi : nullptr);
+  ((double *)A.xs)[4 * (size_t)i + 3] = fp;
+  if (A.eflag) phi_site[i] = phi;
+}
+
+// F' at interpolated lattice sites from shape-weighted nodal density
+// (pair_eam.cpp:957-969)
+__global__ void k_eam_site_fp(double4 *xs, const int *act_gid, int nact, int base, int na,
+                              const double *rho, EamTables T) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nact) return;
+  int gid = act_gid[k];
+  int e = gid / NU, u = gid % NU;
+  const double *rn = rho + na + 8 * (size_t)e;
+  double r = 0.0;
+#pragma unroll
+  for (int n = 0; n < NPE; n++) r += shape_val(u, n) * rn[n];
+  xs[base + k].w = eam_fp(T, r, nullptr);
+}
+
+// pass 2: forces (pair_eam.cpp:845-1028)
+__global__ void __launch_bounds__(128) k_eam_force(PairArgs A, EamTables T, const double *phi_site) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  bool valid = i < A.nsi;
+  double fi[3] = {0, 0, 0}, esum = 0.0, vsum[6] = {0, 0, 0, 0, 0, 0};
+  double eemb_site = 0.0, eemb_global = 0.0;
+  if (valid) {
+    double4 xi = A.xs[i];
+    double fpi = xi.w;
+    int n = A.num[i];
+    const int *nb = A.nbr + i;
+    for (int k = 0; k < n; k++) {
+      double4 xj;
+      neighbour_pos(A, nb[(size_t)k * A.nsi], xj);
+      double dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
+      double rsq = dx * dx + dy * dy + dz * dz;
+      if (rsq < T.cutforcesq) {
+        double r = sqrt(rsq);
+        double p = r * T.rdr + 1.0;
+        int m = (int)p;
+        m = max(1, min(m, T.nr - 1));
+        p -= m;
+        p = fmin(p, 1.0);
+        double4 rd = T.rhor_der[m];
+        double rhop = (rd.x * p + rd.y) * p + rd.z;
+        double4 zd = T.z2r_der[m];
+        double4 zv = T.z2r_val[m];
+        double z2p = (zd.x * p + zd.y) * p + zd.z;
+        double z2 = ((zv.x * p + zv.y) * p + zv.z) * p + zv.w;
+        double recip = 1.0 / r;
+        double phi = z2 * recip;
+        double phip = z2p * recip - phi * recip;
+        double psip = fpi * rhop + xj.w * rhop + phip;
+        double fpair = -psip * recip;
+        fi[0] += dx * fpair;
+        fi[1] += dy * fpair;
+        fi[2] += dz * fpair;
+        if (A.eflag) esum += phi;
+        if (A.vflag) {
+          vsum[0] += dx * dx * fpair;
+          vsum[1] += dy * dy * fpair;
+          vsum[2] += dz * dz * fpair;
+          vsum[3] += dx * dy * fpair;
+          vsum[4] += dx * dz * fpair;
+          vsum[5] += dy * dz * fpair;
+        }
+      }
+    }
+    if (A.eflag) {
+      double phi = phi_site[i];
+      eemb_site = phi;
+      eemb_global = (i < A.na) ? phi : phi * A.escale_node * 2.0;
+    }
+  }
+  finish_site(A, i, valid, fi, esum, vsum, eemb_site, eemb_global);
+}
+
+__global__ void k_reduce_partials(const double *partial, int nblocks, double *out) {
+  // one warp per component, fixed order
+  int k = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (k >= 7) return;
+  double s = 0.0;
+  for (int b = lane; b < nblocks; b += 32) s += partial[b * 7 + k];
+  s = warp_sum(s);
+  if (lane == 0) out[k] = s;
+}
+
+// ---------------------------------------------------------- spline tables
+
+// PairEAM::interpolate (pair_eam.cpp:580-616): 7 coefficients per knot m = 1..n
+void spline7(int n, double delta, const std::vector<double> &f1, std::vector<double> &sp) {
+  sp.assign((size_t)(n + 1) * 7, 0.0);
+  auto S = [&](int m, int c) -> double & { return sp[(size_t)m * 7 + c]; };
+  for (int m = 1; m <= n; m++) S(m, 6) = f1[m];
+  S(1, 5) = S(2, 6) - S(1, 6);
+  S(2, 5) = 0.5 * (S(3, 6) - S(1, 6));
+  S(n - 1, 5) = 0.5 * (S(n, 6) - S(n - 2, 6));
+  S(n, 5) = S(n, 6) - S(n - 1, 6);
+  for (int m = 3; m <= n - 2; m++)
+    S(m, 5) = ((S(m - 2, 6) - S(m + 2, 6)) + 8.0 * (S(m + 1, 6) - S(m - 1, 6))) / 12.0;
+  for (int m = 1; m <= n - 1; m++) {
+    S(m, 4) = 3.0 * (S(m + 1, 6) - S(m, 6)) - 2.0 * S(m, 5) - S(m + 1, 5);
+    S(m, 3) = S(m, 5) + S(m + 1, 5) - 2.0 * (S(m + 1, 6) - S(m, 6));
+  }
+  S(n, 4) = 0.0;
+  S(n, 3) = 0.0;
+  for (int m = 1; m <= n; m++) {
+    S(m, 2) = S(m, 5) / delta;
+    S(m, 1) = 2.0 * S(m, 4) / delta;
+    S(m, 0) = 3.0 * S(m, 3) / delta;
+  }
+}
+
+void upload_split(Ctx &c, const std::vector<double> &sp, int n, DBuf<double4> &val, DBuf<double4> &der) {
+  std::vector<double4> hv(n + 1), hd(n + 1);
+  for (int m = 0; m <= n; m++) {
+    const double *r = &sp[(size_t)m * 7];
+    hv[m] = make_double4(r[3], r[4], r[5], r[6]);
+    hd[m] = make_double4(r[0], r[1], r[2], 0.0);
+  }
+  val.reserve(n + 1);
+  der.reserve(n + 1);
+  CACB200_CUDA(cudaMemcpy(val.p, hv.data(), sizeof(double4) * (n + 1), cudaMemcpyHostToDevice));
+  CACB200_CUDA(cudaMemcpy(der.p, hd.data(), sizeof(double4) * (n + 1), cudaMemcpyHostToDevice));
+}
+
+}  // namespace
+
+void eam_tables(Ctx &c, const double *frho, const double *rhor, const double *z2r) {
+  PairParams &p = c.pp;
+  std::vector<double> a(p.nrho + 1, 0.0), b(p.nr + 1, 0.0), z(p.nr + 1, 0.0), sp;
+  for (int m = 1; m <= p.nrho; m++) a[m] = frho[m - 1];
+  for (int m = 1; m <= p.nr; m++) {
+    b[m] = rhor[m - 1];
+    z[m] = z2r[m - 1];
+  }
+  spline7(p.nrho, p.drho, a, sp);
+  upload_split(c, sp, p.nrho, c.frho_val, c.frho_der);
+  spline7(p.nr, p.dr, b, sp);
+  upload_split(c, sp, p.nr, c.rhor_val, c.rhor_der);
+  spline7(p.nr, p.dr, z, sp);
+  upload_split(c, sp, p.nr, c.z2r_val, c.z2r_der);
+}
+
+void pair_compute(Ctx &c, int eflag, int vflag) {
+  c.check_system();
+  if (!c.lists_valid) throw Error(CACB200_ESTATE, "neighbour lists not built");
+  const int nsi = c.nsite_i();
+  const int T = 128;
+  const int nb = std::max(nblk(nsi, T), 1);
+  PairArgs A;
+  A.xs = c.xs.p;
+  A.nbr = c.nbr_full.p;
+  A.num = c.num_full.p;
+  A.na = c.na;
+  A.ne = c.ne;
+  A.nsi = nsi;
+  for (int d = 0; d < 3; d++) A.L[d] = c.prd[d];
+  A.f = c.f.p;
+  A.gaussf = c.gaussf.p;
+  if (eflag & CACB200_ENERGY_ATOM) {
+    c.eatom.reserve(std::max(c.na, 1));
+    c.enode.reserve(std::max(c.ne * 8, 1));
+  }
+  if (vflag & CACB200_VIRIAL_ATOM) {
+    c.vatom.reserve(std::max(c.na * 6, 1));
+    c.vnode.reserve(std::max(c.ne * 48, 1));
+  }
+  A.eatom = c.eatom.p;
+  A.enode = c.enode.p;
+  A.vatom = c.vatom.p;
+  A.vnode = c.vnode.p;
+  c.partial.reserve((size_t)nb * 7);
+  c.ev_out.reserve(7);
+  A.partial = c.partial.p;
+  A.eflag = eflag;
+  A.vflag = vflag;
+  double nodal_weight = (double)NU / (double)NPE;   // element_vec_cac.cpp:1732
+  A.vscale_node = nodal_weight / 2.0;
+  A.escale_node = nodal_weight / 2.0;
+  if (c.pp.style == CACB200_PAIR_EAM && c.nodal_energy_weight >= 0.0)
+    A.escale_node = c.nodal_energy_weight / 2.0;
+
+  if (c.pp.style == CACB200_PAIR_LJ) {
+    LjParams P{c.pp.cut * c.pp.cut, c.pp.lj1, c.pp.lj2, c.pp.lj3, c.pp.lj4, c.pp.offset};
+    KernelTimer t(c, "pair_lj");
+    k_lj<<<nb, T, 0, c.stream>>>(A, P);
+  } else if (c.pp.style == CACB200_PAIR_EAM) {
+    EamTables Tb;
+    Tb.rhor_val = c.rhor_val.p;
+    Tb.rhor_der = c.rhor_der.p;
+    Tb.z2r_val = c.z2r_val.p;
+    Tb.z2r_der = c.z2r_der.p;
+    Tb.frho_val = c.frho_val.p;
+    Tb.frho_der = c.frho_der.p;
+    Tb.rdr = c.pp.rdr;
+    Tb.rdrho = c.pp.rdrho;
+    Tb.rhomax = c.pp.rhomax;
+    Tb.cutforcesq = c.pp.cut * c.pp.cut;
+    Tb.nr = c.pp.nr;
+    Tb.nrho = c.pp.nrho;
+    c.rho.reserve(std::max(c.na + 8 * c.ne, 1));
+    c.phi_site.reserve(std::max(nsi, 1));
+    {
+      KernelTimer t(c, "eam_rho");
+      k_eam_rho<<<nb, T, 0, c.stream>>>(A, Tb, c.rho.p, c.phi_site.p);
+    }
+    if (c.nact) {
+      KernelTimer t(c, "eam_site_fp");
+      k_eam_site_fp<<<nblk(c.nact, 256), 256, 0, c.stream>>>(c.xs.p, c.act_gid.p, c.nact,
+                                                             c.na + NG * c.ne, c.na, c.rho.p, Tb);
+    }
+    {
+      KernelTimer t(c, "eam_force");
+      k_eam_force<<<nb, T, 0, c.stream>>>(A, Tb, c.phi_site.p);
+    }
+  } else {
+    throw Error(CACB200_ESTATE, "no pair style set");
+  }
+  if (eflag || vflag) {
+    k_reduce_partials<<<1, 256, 0, c.stream>>>(c.partial.p, nb, c.ev_out.p);
+    c.have_peratom_e = (eflag & CACB200_ENERGY_ATOM) != 0;
+    c.have_peratom_v = (vflag & CACB200_VIRIAL_ATOM) != 0;
+    c.ev_pending = true;
+  }
+  CACB200_CUDA(cudaGetLastError());
+}
+
+}  // namespace cacb200

@@ -1,0 +1,153 @@
+/*
+ * cacb200: B200 (sm_100a) implementation of the CAC per-timestep force path
+ * behind a C ABI.
+ *
+ * One context (cacb200_ctx) holds one system on one GPU: atoms, 8-node Hex
+ * elements (apc = 1, 9 lattice sites per edge, 2x2x2 Gauss points = nodes),
+ * a periodic orthogonal box, one pair style and the neighbour lists.  State is
+ * device-resident; the host copies in and out only through the calls below.
+ * All arrays are plain C arrays in the reference's own layouts:
+ *   atom x, v, f         [natoms][3]                        (atom.h:36-60)
+ *   node x, v, f          [nelements][8 nodes][3]            (element.h:94, apc = 1)
+ *   gaussf                [nelements][8 Gauss points][3]
+ * Atoms and elements keep the order in which they were uploaded; that order
+ * plays the role of the reference's local index order (it decides the
+ * "owned j after i" rule of the half list).
+ *
+ * Every call returns 0 on success or a negative CACB200_E* code; the message
+ * is available from cacb200_last_error().  Nothing aborts the process; the
+ * reference's styles turn a non-zero status into error->all().
+ * A context is driven by one host thread at a time (it owns one stream).
+ */
+#ifndef CACB200_H
+#define CACB200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CACB200_OK 0
+#define CACB200_EINVAL (-1)      /* bad argument */
+#define CACB200_ECUDA (-2)       /* CUDA runtime error */
+#define CACB200_ENOMEM (-3)      /* device allocation failed */
+#define CACB200_ESTATE (-4)      /* call out of order (e.g. no system yet) */
+#define CACB200_EOVERFLOW (-5)   /* a capacity was exceeded and could not grow */
+#define CACB200_ETIMEDOUT (-6)   /* a bounded device wait gave up */
+#define CACB200_EUNSTABLE (-7)   /* non-finite coordinates or forces */
+
+/* precision forms */
+#define CACB200_FP64 0           /* everything in FP64 */
+#define CACB200_MIXED 1          /* FP32 pair arithmetic on cell-relative positions */
+
+/* pair styles */
+#define CACB200_PAIR_NONE 0
+#define CACB200_PAIR_LJ 1
+#define CACB200_PAIR_EAM 2
+
+/* energy / virial request bits (force.h:11-20) */
+#define CACB200_ENERGY_GLOBAL 1
+#define CACB200_ENERGY_ATOM 2
+#define CACB200_VIRIAL_GLOBAL 1
+#define CACB200_VIRIAL_ATOM 4
+
+typedef struct cacb200_ctx cacb200_ctx;
+
+/* ---------------------------------------------------------------- context */
+
+/* Create a context on CUDA device `device` (replaces the per-run state that
+ * Atom/Element/Neighbor/Pair own in the reference, cac.cpp:36-197). */
+int cacb200_ctx_create(int device, cacb200_ctx **out);
+int cacb200_ctx_destroy(cacb200_ctx *ctx);
+const char *cacb200_last_error(const cacb200_ctx *ctx);
+/* cudaStream_t the context launches on, as void* */
+void *cacb200_stream(cacb200_ctx *ctx);
+int cacb200_set_precision(cacb200_ctx *ctx, int form);
+
+/* ----------------------------------------------------------------- system */
+
+/* Upload a system (replaces read_data + AtomVec/ElementVec data parsing,
+ * read_data.cpp:339-367, element_vec_cac.cpp:300-395).  Element nodes must be
+ * given unwrapped around their element centre; atoms inside the box. */
+int cacb200_upload_system(cacb200_ctx *ctx, const double boxlo[3], const double boxhi[3],
+                          int natoms, const double *x, const double *v,
+                          int nelements, const double *nodex, const double *nodev,
+                          double mass);
+/* Overwrite positions/velocities of the current system (same counts; NULL
+ * leaves an array unchanged).  Neighbour lists are kept, as the reference
+ * keeps them between rebuilds; call cacb200_build_lists after moves larger
+ * than half the skin. */
+int cacb200_set_state(cacb200_ctx *ctx, const double *x, const double *v,
+                      const double *nodex, const double *nodev);
+int cacb200_get_state(cacb200_ctx *ctx, double *x, double *v, double *nodex, double *nodev);
+/* Forces after the last force evaluation: atom f, nodal f (after assembly),
+ * Gauss-point f (before assembly).  Any pointer may be NULL. */
+int cacb200_get_forces(cacb200_ctx *ctx, double *f, double *nodef, double *gaussf);
+/* Energy and virial of the last evaluation that requested them
+ * (Pair::eng_vdwl, Pair::virial, eatom, vatom, enode, vnode). */
+int cacb200_get_energy(cacb200_ctx *ctx, double *energy, double virial[6], double *eatom,
+                       double *vatom, double *enode, double *vnode);
+int cacb200_counts(cacb200_ctx *ctx, int *natoms, int *nelements, int *nactive_sites);
+
+/* ------------------------------------------------------------- pair styles */
+
+/* pair_style lj/cut + pair_coeff 1 1 eps sigma (pair_lj_cut.cpp:142-215) */
+int cacb200_set_lj(cacb200_ctx *ctx, double epsilon, double sigma, double cut);
+/* pair_style eam/alloy with one element: the setfl arrays as read from the file
+ * (pair_eam_alloy.cpp:100-240): frho[nrho], rhor[nr], z2r[nr] (= r*phi). */
+int cacb200_set_eam(cacb200_ctx *ctx, int nrho, double drho, int nr, double dr, double cut,
+                    const double *frho, const double *rhor, const double *z2r);
+/* Pair::nodal_energy_weight (pair.cpp:38; minimize.cpp:37 sets 1.0): < 0 means
+ * the element's nodal weight. */
+int cacb200_set_nodal_energy_weight(cacb200_ctx *ctx, double w);
+
+/* --------------------------------------------------------------- neighbour */
+
+/* neighbor SKIN bin + neigh_modify every N delay 0 check no (neighbor.cpp:2043) */
+int cacb200_set_neighbor(cacb200_ctx *ctx, double skin, int every);
+/* Bin and build the lists now (Neighbor::build, neighbor.cpp:1704-1876).
+ * The full list (npair_full_bin.cpp) is always built; the half list
+ * (npair_half_bin_newton.cpp) only when want_half is non-zero. */
+int cacb200_build_lists(cacb200_ctx *ctx, int want_half);
+/* Copy a list out in canonical form: per i-site (atoms, then Gauss points
+ * natoms + 8*e + igcell) the neighbours (kind 0 atom / 1 lattice site, index,
+ * site = -1 or jucell, periodic image sx sy sz).  Call with NULL arrays to get
+ * the size; offset has nsites + 1 entries. */
+int cacb200_list_size(cacb200_ctx *ctx, int half, int64_t *nentries, int *nsites);
+int cacb200_get_list(cacb200_ctx *ctx, int half, int64_t *offset, int8_t *kind, int32_t *idx,
+                     int32_t *site, int8_t *img);
+
+/* ------------------------------------------------------------------ steps */
+
+/* Refresh interpolated lattice-site positions (and EAM embedding terms)
+ * from the current nodes: the implicit interpolation of
+ * npair_half_bin_newton.cpp:284-289 / pair_lj_cut.cpp:364-368 done once. */
+int cacb200_interpolate(cacb200_ctx *ctx);
+/* Evaluate the pair style (Pair::compute(eflag, vflag)): atom f and gaussf. */
+int cacb200_compute_pair(cacb200_ctx *ctx, int eflag, int vflag);
+/* Element::compute_nodef, CONSISTENT (element.cpp:2178-2210) */
+int cacb200_assemble_nodef(cacb200_ctx *ctx);
+/* One force evaluation: interpolate + pair + nodal assembly. */
+int cacb200_compute_forces(cacb200_ctx *ctx, int eflag, int vflag);
+/* FixNVE::initial_integrate / final_integrate (fix_nve.cpp:62-219) */
+int cacb200_nve_initial(cacb200_ctx *ctx, double dt);
+int cacb200_nve_final(cacb200_ctx *ctx, double dt);
+/* Verlet::setup + nsteps of Verlet::run with fix nve (verlet.cpp:64-360): lists
+ * rebuilt every `every` steps (set_neighbor); energy/virial of the final step
+ * when eflag/vflag are set.  Runs entirely on the device; returns when done. */
+int cacb200_setup(cacb200_ctx *ctx);
+int cacb200_run_nve(cacb200_ctx *ctx, int nsteps, double dt, int eflag, int vflag);
+
+/* Kernel timing: when enabled, every launch is bracketed by CUDA events and
+ * per-kernel totals accumulate (ms, launches) until reset. */
+int cacb200_profile(cacb200_ctx *ctx, int enable);
+int cacb200_profile_read(cacb200_ctx *ctx, int max, char *names /* max*32 */,
+                         double *total_ms, int64_t *launches, int *count);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

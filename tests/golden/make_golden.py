@@ -1,0 +1,123 @@
+"""Generate the golden fixtures of this directory by running the CAC reference
+(compiled by ``oracle/Makefile`` into ``oracle/_ref/``) on seeded systems from
+``cac_b200.gen``.
+
+Run from the repository root where the reference tree is available:
+
+    make -C oracle reference && python tests/golden/make_golden.py
+
+Each fixture ``<case>.npz`` holds the reference's own read-outs:
+  setup forces (atom f, nodal f, Gauss-point f), energy, virial and per-site
+  energy/virial (``oracle_dump compute``); the sha256 digest and per-site
+  counts of its half and full neighbour lists (``oracle_dump_neigh``); and for
+  trajectory cases the state after N velocity-Verlet steps.
+EAM energies come from the executable with the patched ``compute_fp``
+(``cac_eamfix``); the unpatched reference energy is kept as ``energy_unpatched``.
+"""
+from __future__ import annotations
+
+import hashlib
+import os
+import shutil
+import sys
+import tempfile
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+
+from cac_b200 import gen  # noqa: E402
+import oracle as O  # noqa: E402
+
+OUT = os.path.dirname(os.path.abspath(__file__))
+
+HEADER = """units metal
+dimension 3
+boundary p p p
+atom_style atomic
+element_style cac 8 1 wscale 1 1 1 1
+read_data data.cac
+"""
+
+
+def pair_lines(pair: str) -> str:
+    if pair == "lj":
+        return "pair_style lj/cut 5.5\npair_coeff 1 1 0.4093 2.338\n"
+    if pair == "lj_full":
+        return "pair_style lj/cut/fulllist 5.5\npair_coeff 1 1 0.4093 2.338\n"
+    if pair == "eam":
+        return "pair_style eam/alloy\npair_coeff * * cu.setfl Cu\n"
+    raise ValueError(pair)
+
+
+def digest(rows: np.ndarray) -> str:
+    return hashlib.sha256(np.ascontiguousarray(rows, dtype="<i8").tobytes()).hexdigest()
+
+
+def counts(rows: np.ndarray, nsites: int) -> np.ndarray:
+    return np.bincount(rows[:, 0], minlength=nsites).astype(np.int32)
+
+
+def run(work: str, script: str, exe: str) -> None:
+    with open(os.path.join(work, "in.cac"), "w") as f:
+        f.write(script)
+    O.run_reference(work, "in.cac", exe=exe)
+
+
+def make_case(name: str, system, pair: str, nsteps: int = 0, peratom_virial: bool = True) -> None:
+    work = tempfile.mkdtemp(prefix="cacgold_")
+    try:
+        gen.write_data(system, os.path.join(work, "data.cac"))
+        gen.write_setfl(gen.EamParams(), os.path.join(work, "cu.setfl"))
+        tail = "neighbor 1.0 bin\nneigh_modify every 10 delay 0 check no\ntimestep 0.001\nfix 1 all nve\n"
+        out = {}
+        exe_e = O.REF_EXE_EAMFIX if pair == "eam" else O.REF_EXE
+        run(work, HEADER + pair_lines(pair) + tail +
+            "run 0\noracle_dump setup.txt compute\noracle_dump_neigh half.txt\n", exe_e)
+        d = O.read_dump(os.path.join(work, "setup.txt"))
+        for k in ("f", "nodef", "gaussf_at_node", "eatom", "enode", "virial"):
+            out[k] = d[k]
+        if peratom_virial:
+            out["vatom"], out["vnode"] = d["vatom"], d["vnode"]
+        out["energy"] = np.float64(d["energy"])
+        if pair == "eam":
+            run(work, HEADER + pair_lines(pair) + tail + "run 0\noracle_dump unpatched.txt compute\n", O.REF_EXE)
+            out["energy_unpatched"] = np.float64(O.read_dump(os.path.join(work, "unpatched.txt"))["energy"])
+        nsites = system.natoms + 8 * system.nelements
+        half = O.read_neigh(os.path.join(work, "half.txt"), system.natoms)
+        full_pair = "lj_full" if pair.startswith("lj") else "lj_full"
+        fscript = HEADER + pair_lines(full_pair)
+        if pair == "eam":
+            fscript = fscript.replace("5.5", "5.0")
+        run(work, fscript + tail + "run 0\noracle_dump_neigh full.txt\n", O.REF_EXE)
+        full = O.read_neigh(os.path.join(work, "full.txt"), system.natoms)
+        out["half_digest"] = np.array(digest(half))
+        out["full_digest"] = np.array(digest(full))
+        out["half_counts"] = counts(half, nsites)
+        out["full_counts"] = counts(full, nsites)
+        if nsteps:
+            run(work, HEADER + pair_lines(pair) + tail + f"run {nsteps}\noracle_dump end.txt state\n", exe_e)
+            e = O.read_dump(os.path.join(work, "end.txt"))
+            out["nsteps"] = np.int64(nsteps)
+            for k in ("x", "v", "f", "nodex", "nodev", "nodef"):
+                out["end_" + k] = e[k]
+        meta = dict(system.meta)
+        out["meta"] = np.array(repr(sorted(meta.items())))
+        np.savez_compressed(os.path.join(OUT, name + ".npz"), **out)
+        print(name, "sites", nsites, "half", len(half), "full", len(full), "energy", out["energy"])
+    finally:
+        shutil.rmtree(work, ignore_errors=True)
+
+
+def main():
+    if not os.path.exists(O.REF_EXE):
+        raise SystemExit("build the reference first: make -C oracle reference")
+    make_case("tiny_lj", gen.tiny(seed=7, temperature=50.0), "lj", nsteps=100)
+    make_case("tiny_eam", gen.tiny(seed=11, temperature=300.0), "eam", nsteps=50)
+    make_case("lj_small", gen.lj_small(seed=1), "lj", nsteps=100, peratom_virial=False)
+
+
+if __name__ == "__main__":
+    main()

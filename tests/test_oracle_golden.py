@@ -1,0 +1,73 @@
+"""The CPU restatement in oracle/ against the reference's own read-outs
+(golden fixtures made by tests/golden/make_golden.py)."""
+import numpy as np
+import pytest
+
+from helpers import CASES, G2N, LJ, N2G, SKIN, counts, digest, rel_err, setfl_path
+
+
+@pytest.mark.parametrize("case", ["tiny_lj", "tiny_eam", "lj_small"])
+def test_lists_match_reference(case, oracle_mod, golden):
+    g = golden(case)
+    build, pair, cutneigh = CASES[case]
+    s = build()
+    st = oracle_mod.OracleState(s)
+    nsites = s.natoms + 8 * s.nelements
+    for half, key in ((True, "half"), (False, "full")):
+        L = oracle_mod.build_list(st, cutneigh, half)
+        rows = L.canonical(s.natoms)
+        oracle_mod.free_list(L)
+        assert np.array_equal(counts(rows, nsites), g[key + "_counts"])
+        assert digest(rows) == str(g[key + "_digest"])
+
+
+@pytest.mark.parametrize("case", ["tiny_lj", "tiny_eam", "lj_small"])
+def test_forces_energy_match_reference(case, oracle_mod, golden, tmp_path):
+    g = golden(case)
+    build, pair, cutneigh = CASES[case]
+    s = build()
+    st = oracle_mod.OracleState(s)
+    L = oracle_mod.build_list(st, cutneigh, True)
+    if pair == "lj":
+        ev = oracle_mod.lj_forces(st, L, *LJ)
+    else:
+        ev = oracle_mod.eam_forces(st, L, oracle_mod.Eam(setfl_path(tmp_path)))
+    oracle_mod.free_list(L)
+    fscale = max(np.abs(g["f"]).max(), np.abs(g["nodef"]).max())
+    assert np.abs(st.f - g["f"]).max() / fscale < 1e-12
+    assert np.abs(st.nodef - g["nodef"]).max() / fscale < 1e-12
+    assert np.abs(st.gaussf[:, N2G, :] - g["gaussf_at_node"]).max() / fscale < 1e-12
+    assert abs(ev.energy - float(g["energy"])) / abs(float(g["energy"])) < 1e-12
+    assert np.abs(ev.virial - g["virial"]).max() / np.abs(g["virial"]).max() < 1e-12
+    assert np.abs(ev.eatom - g["eatom"]).max() < 1e-11
+    assert np.abs(ev.enode - g["enode"]).max() < 1e-11
+    if "vatom" in g:
+        assert np.abs(ev.vatom - g["vatom"]).max() < 1e-11
+        assert np.abs(ev.vnode - g["vnode"]).max() < 1e-11
+
+
+def test_eam_reference_energy_quirk_is_real(golden):
+    """The unpatched reference reads the embedding energy from a stale spline
+    row (pair_eam.cpp:819-833 with compute_fp's coefficient pointer passed by
+    value); the fixture records both values and they differ grossly."""
+    g = golden("tiny_eam")
+    assert abs(float(g["energy_unpatched"]) - float(g["energy"])) > 1.0
+
+
+@pytest.mark.parametrize("case", ["tiny_lj", "tiny_eam", "lj_small"])
+def test_trajectory_matches_reference(case, oracle_mod, golden, tmp_path):
+    g = golden(case)
+    build, pair, cutneigh = CASES[case]
+    s = build()
+    st = oracle_mod.OracleState(s)
+    n = int(g["nsteps"])
+    if pair == "lj":
+        oracle_mod.run_nve(st, "lj", lj=LJ, skin=SKIN, nsteps=n, every=10)
+    else:
+        oracle_mod.run_nve(st, "eam", eam=oracle_mod.Eam(setfl_path(tmp_path)), skin=SKIN, nsteps=n, every=10)
+    assert np.abs(st.x - g["end_x"]).max() < 1e-10
+    assert np.abs(st.nodex - g["end_nodex"]).max() < 1e-10
+    assert rel_err(st.f, g["end_f"]) < 1e-10
+    assert rel_err(st.nodef, g["end_nodef"]) < 1e-10
+    assert rel_err(st.v, g["end_v"]) < 1e-10
+    assert rel_err(st.nodev, g["end_nodev"]) < 1e-10
