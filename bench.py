@@ -54,6 +54,8 @@ def build_workload(name: str, seed: int):
         return gen.eam_1m(seed=seed), "eam"
     if name == "lj_small":
         return gen.lj_small(seed=seed), "lj"
+    if name == "eam_small":
+        return gen.eam_small(seed=seed), "eam"
     if name == "eam_4m_strained":
         return gen.eam_4m_strained(seed=seed), "eam"
     raise SystemExit(f"unknown workload {name}")

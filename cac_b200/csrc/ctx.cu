@@ -123,12 +123,12 @@ void upload_system(Ctx &c, const double lo[3], const double hi[3], int na, const
   std::vector<double4> hx(std::max(na, 1));
   for (int i = 0; i < na; i++) hx[i] = make_double4(x[3 * i], x[3 * i + 1], x[3 * i + 2], 0.0);
   if (na) {
-    CACB200_CUDA(cudaMemcpy(c.xs.p, hx.data(), sizeof(double4) * na, cudaMemcpyHostToDevice));
-    CACB200_CUDA(cudaMemcpy(c.v.p, v, sizeof(double) * 3 * na, cudaMemcpyHostToDevice));
+    stream_copy(c, c.xs.p, hx.data(), sizeof(double4) * na, cudaMemcpyHostToDevice);
+    stream_copy(c, c.v.p, v, sizeof(double) * 3 * na, cudaMemcpyHostToDevice);
   }
   if (ne) {
-    CACB200_CUDA(cudaMemcpy(c.nodex.p, nodex, sizeof(double) * 24 * ne, cudaMemcpyHostToDevice));
-    CACB200_CUDA(cudaMemcpy(c.nodev.p, nodev, sizeof(double) * 24 * ne, cudaMemcpyHostToDevice));
+    stream_copy(c, c.nodex.p, nodex, sizeof(double) * 24 * ne, cudaMemcpyHostToDevice);
+    stream_copy(c, c.nodev.p, nodev, sizeof(double) * 24 * ne, cudaMemcpyHostToDevice);
   }
   CACB200_CUDA(cudaStreamSynchronize(c.stream));
 }
@@ -317,11 +317,11 @@ int cacb200_get_forces(cacb200_ctx *ctx, double *f, double *nodef, double *gauss
   API_BEGIN
   c.check_system();
   CACB200_CUDA(cudaStreamSynchronize(c.stream));
-  if (f && c.na) CACB200_CUDA(cudaMemcpy(f, c.f.p, sizeof(double) * 3 * c.na, cudaMemcpyDeviceToHost));
+  if (f && c.na) stream_copy(c, f, c.f.p, sizeof(double) * 3 * c.na, cudaMemcpyDeviceToHost);
   if (nodef && c.ne)
-    CACB200_CUDA(cudaMemcpy(nodef, c.nodef.p, sizeof(double) * 24 * c.ne, cudaMemcpyDeviceToHost));
+    stream_copy(c, nodef, c.nodef.p, sizeof(double) * 24 * c.ne, cudaMemcpyDeviceToHost);
   if (gaussf && c.ne)
-    CACB200_CUDA(cudaMemcpy(gaussf, c.gaussf.p, sizeof(double) * 24 * c.ne, cudaMemcpyDeviceToHost));
+    stream_copy(c, gaussf, c.gaussf.p, sizeof(double) * 24 * c.ne, cudaMemcpyDeviceToHost);
   API_END
 }
 
@@ -335,12 +335,12 @@ int cacb200_get_energy(cacb200_ctx *ctx, double *energy, double virial[6], doubl
     for (int k = 0; k < 6; k++) virial[k] = c.virial[k];
   if ((eatom || enode) && !c.have_peratom_e) throw Error(CACB200_ESTATE, "per-site energy not computed");
   if ((vatom || vnode) && !c.have_peratom_v) throw Error(CACB200_ESTATE, "per-site virial not computed");
-  if (eatom && c.na) CACB200_CUDA(cudaMemcpy(eatom, c.eatom.p, sizeof(double) * c.na, cudaMemcpyDeviceToHost));
-  if (enode && c.ne) CACB200_CUDA(cudaMemcpy(enode, c.enode.p, sizeof(double) * 8 * c.ne, cudaMemcpyDeviceToHost));
+  if (eatom && c.na) stream_copy(c, eatom, c.eatom.p, sizeof(double) * c.na, cudaMemcpyDeviceToHost);
+  if (enode && c.ne) stream_copy(c, enode, c.enode.p, sizeof(double) * 8 * c.ne, cudaMemcpyDeviceToHost);
   if (vatom && c.na)
-    CACB200_CUDA(cudaMemcpy(vatom, c.vatom.p, sizeof(double) * 6 * c.na, cudaMemcpyDeviceToHost));
+    stream_copy(c, vatom, c.vatom.p, sizeof(double) * 6 * c.na, cudaMemcpyDeviceToHost);
   if (vnode && c.ne)
-    CACB200_CUDA(cudaMemcpy(vnode, c.vnode.p, sizeof(double) * 48 * c.ne, cudaMemcpyDeviceToHost));
+    stream_copy(c, vnode, c.vnode.p, sizeof(double) * 48 * c.ne, cudaMemcpyDeviceToHost);
   API_END
 }
 

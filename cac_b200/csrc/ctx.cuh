@@ -169,6 +169,15 @@ struct Ctx {
   }
 };
 
+// Host<->device copy ordered on the context's stream and completed on return.
+// (The legacy default stream does not order against the context's non-blocking
+// stream, so every transfer goes through the stream.)
+inline void stream_copy(Ctx &c, void *dst, const void *src, size_t bytes, cudaMemcpyKind kind) {
+  if (bytes == 0) return;
+  CACB200_CUDA(cudaMemcpyAsync(dst, src, bytes, kind, c.stream));
+  CACB200_CUDA(cudaStreamSynchronize(c.stream));
+}
+
 // profiling helpers (host)
 struct KernelTimer {
   Ctx &c;

@@ -763,12 +763,12 @@ void neigh_download(Ctx &c, bool half, int64_t *offset, int8_t *kind, int32_t *i
   std::vector<int> ent((size_t)c.cap * nsi);
   std::vector<int> act(std::max(c.nact, 1));
   CACB200_CUDA(cudaStreamSynchronize(c.stream));
-  CACB200_CUDA(cudaMemcpy(num.data(), half ? c.num_half.p : c.num_full.p, sizeof(int) * nsi,
-                          cudaMemcpyDeviceToHost));
-  CACB200_CUDA(cudaMemcpy(ent.data(), half ? c.nbr_half.p : c.nbr_full.p, sizeof(int) * ent.size(),
-                          cudaMemcpyDeviceToHost));
+  stream_copy(c, num.data(), half ? c.num_half.p : c.num_full.p, sizeof(int) * nsi,
+                          cudaMemcpyDeviceToHost);
+  stream_copy(c, ent.data(), half ? c.nbr_half.p : c.nbr_full.p, sizeof(int) * ent.size(),
+                          cudaMemcpyDeviceToHost);
   if (c.nact)
-    CACB200_CUDA(cudaMemcpy(act.data(), c.act_gid.p, sizeof(int) * c.nact, cudaMemcpyDeviceToHost));
+    stream_copy(c, act.data(), c.act_gid.p, sizeof(int) * c.nact, cudaMemcpyDeviceToHost);
   int64_t total = 0;
   for (int i = 0; i < nsi; i++) total += num[i];
   *nentries = total;

@@ -319,8 +319,8 @@ void upload_split(Ctx &c, const std::vector<double> &sp, int n, DBuf<double4> &v
   }
   val.reserve(n + 1);
   der.reserve(n + 1);
-  CACB200_CUDA(cudaMemcpy(val.p, hv.data(), sizeof(double4) * (n + 1), cudaMemcpyHostToDevice));
-  CACB200_CUDA(cudaMemcpy(der.p, hd.data(), sizeof(double4) * (n + 1), cudaMemcpyHostToDevice));
+  stream_copy(c, val.p, hv.data(), sizeof(double4) * (n + 1), cudaMemcpyHostToDevice);
+  stream_copy(c, der.p, hd.data(), sizeof(double4) * (n + 1), cudaMemcpyHostToDevice);
 }
 
 }  // namespace

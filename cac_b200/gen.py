@@ -213,6 +213,13 @@ def eam_1m(seed: int = 2) -> System:
     return build_slab(8, 5, 125, 162, temperature=300.0, seed=seed)
 
 
+def eam_small(seed: int = 5) -> System:
+    """A quarter-height EAM slab for profiling captures: 272,160 atoms (42
+    layers of 6,480) plus 5,120 elements (2 regions x 32 layers x 80), 313,120
+    atom+IP sites, 300 K; still larger than the 126 MB L2 once lists exist."""
+    return build_slab(8, 5, 32, 42, temperature=300.0, seed=seed)
+
+
 def eam_4m_strained(seed: int = 3) -> System:
     """Mixed-precision workload: 4,179,600 atoms plus 100,000 elements under 3 %
     x-strain (nx=20, ny=10: 32,400 atoms per layer, 129 layers; 125 layers of

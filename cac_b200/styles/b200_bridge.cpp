@@ -1,0 +1,255 @@
+/*
+ * B200Bridge: the reference's host arrays <-> one cacb200 context.
+ * See b200_bridge.h.
+ */
+#include "b200_bridge.h"
+
+#include <algorithm>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include "atom.h"
+#include "comm.h"
+#include "domain.h"
+#include "element.h"
+#include "error.h"
+#include "force.h"
+#include "neighbor.h"
+#include "pair.h"
+#include "update.h"
+
+#include "cacb200.h"
+
+using namespace CAC_NS;
+
+B200Bridge::B200Bridge(CAC *cac) : Pointers(cac) {}
+
+B200Bridge::~B200Bridge()
+{
+  if (ctx) cacb200_ctx_destroy(ctx);
+}
+
+void B200Bridge::status(int rc, const char *what)
+{
+  if (rc == CACB200_OK) return;
+  std::string msg = std::string("b200: ") + what + " failed: " + (ctx ? cacb200_last_error(ctx) : "no context");
+  error->all(FLERR, msg.c_str());
+}
+
+void B200Bridge::set_lj(double epsilon, double sigma, double cut)
+{
+  pair_style = CACB200_PAIR_LJ;
+  lj = {epsilon, sigma, cut};
+  uploaded_na = uploaded_ne = -1;
+}
+
+void B200Bridge::set_eam(int nrho, double drho, int nr, double dr, double cut, const double *frho,
+                         const double *rhor, const double *z2r)
+{
+  pair_style = CACB200_PAIR_EAM;
+  eam_nrho = nrho;
+  eam_nr = nr;
+  eam_drho = drho;
+  eam_dr = dr;
+  eam_cut = cut;
+  eam_frho.assign(frho, frho + nrho);
+  eam_rhor.assign(rhor, rhor + nr);
+  eam_z2r.assign(z2r, z2r + nr);
+  uploaded_na = uploaded_ne = -1;
+}
+
+/* the subset of CAC this package implements: one rank, orthogonal fully
+   periodic box, one atom type, Hex elements with apc 1, 9 lattice sites per
+   edge, 2x2x2 Gauss points, UNIFORM weights and CONSISTENT nodal forces */
+void B200Bridge::check_system()
+{
+  if (comm->nprocs != 1) error->all(FLERR, "b200 styles run on one MPI rank");
+  if (domain->triclinic) error->all(FLERR, "b200 styles need an orthogonal box");
+  if (!domain->xperiodic || !domain->yperiodic || !domain->zperiodic)
+    error->all(FLERR, "b200 styles need a periodic box");
+  if (atom->ntypes != 1) error->all(FLERR, "b200 styles support one atom type");
+  if (element->nelements) {
+    if (element->maxapc != 1 || element->maxnpe != 8)
+      error->all(FLERR, "b200 styles need element_style cac 8 1");
+    if (element->nodal_force_style != Element::CONSISTENT)
+      error->all(FLERR, "b200 styles need CONSISTENT nodal forces");
+    if (element->weight_scale_flag != Element::UNIFORM)
+      error->all(FLERR, "b200 styles need element_style ... wscale (UNIFORM weights)");
+    for (int i = 0; i < element->nlocal; i++) {
+      int t = element->etype[i];
+      if (element->npe[t] != 8 || element->apc[t] != 1 || element->nucell[t] != 729 ||
+          element->ngcell[t] != 8)
+        error->all(FLERR, "b200 styles need Hex elements with 9x9x9 sites and 2x2x2 Gauss points");
+    }
+  }
+  if (!ctx) {
+    const char *dev = getenv("CACB200_DEVICE");
+    status(cacb200_ctx_create(dev ? atoi(dev) : 0, &ctx), "context creation");
+  }
+}
+
+void B200Bridge::configure_pair()
+{
+  if (pair_style == CACB200_PAIR_LJ) status(cacb200_set_lj(ctx, lj[0], lj[1], lj[2]), "set_lj");
+  else if (pair_style == CACB200_PAIR_EAM)
+    status(cacb200_set_eam(ctx, eam_nrho, eam_drho, eam_nr, eam_dr, eam_cut, eam_frho.data(),
+                           eam_rhor.data(), eam_z2r.data()),
+           "set_eam");
+  else error->all(FLERR, "b200: no pair style configured");
+}
+
+void B200Bridge::upload(bool with_velocities)
+{
+  int na = atom->nlocal, ne = element->nlocal;
+  const double *x = na ? &atom->x[0][0] : nullptr;
+  const double *nx = ne ? &element->nodex[0][0][0][0] : nullptr;
+  std::vector<double> zv;
+  const double *v = nullptr, *nv = nullptr;
+  if (with_velocities) {
+    v = na ? &atom->v[0][0] : nullptr;
+    nv = ne ? &element->nodev[0][0][0][0] : nullptr;
+  } else {
+    zv.assign(3 * (size_t)std::max(na, 1) + 24 * (size_t)std::max(ne, 1), 0.0);
+    v = zv.data();
+    nv = zv.data() + 3 * (size_t)std::max(na, 1);
+  }
+  status(cacb200_upload_system(ctx, domain->boxlo, domain->boxhi, na, x, v, ne, nx, nv, atom->mass[1]),
+         "upload_system");
+  configure_pair();
+  uploaded_na = na;
+  uploaded_ne = ne;
+}
+
+void B200Bridge::compute(Pair *pair)
+{
+  check_system();
+  int na = atom->nlocal, ne = element->nlocal;
+  bool rebuild = (uploaded_na != na || uploaded_ne != ne || neighbor->ago == 0);
+  if (rebuild) {
+    upload(false);
+    status(cacb200_set_neighbor(ctx, neighbor->skin, 0), "set_neighbor");
+    status(cacb200_build_lists(ctx, 0), "build_lists");
+  } else {
+    status(cacb200_set_state(ctx, na ? &atom->x[0][0] : nullptr, nullptr,
+                             ne ? &element->nodex[0][0][0][0] : nullptr, nullptr),
+           "set_state");
+  }
+  int ef = (pair->eflag_global ? CACB200_ENERGY_GLOBAL : 0) | (pair->eflag_atom ? CACB200_ENERGY_ATOM : 0);
+  int vf = (pair->vflag_global ? CACB200_VIRIAL_GLOBAL : 0) | (pair->vflag_atom ? CACB200_VIRIAL_ATOM : 0);
+  status(cacb200_compute_forces(ctx, ef, vf), "compute_forces");
+
+  fbuf.resize(3 * (size_t)std::max(na, 1));
+  gbuf.resize(24 * (size_t)std::max(ne, 1));
+  status(cacb200_get_forces(ctx, fbuf.data(), nullptr, gbuf.data()), "get_forces");
+  double **f = atom->f;
+  for (int i = 0; i < na; i++)
+    for (int d = 0; d < 3; d++) f[i][d] += fbuf[3 * (size_t)i + d];
+  double ****gf = element->gaussf;
+  for (int e = 0; e < ne; e++)
+    for (int g = 0; g < 8; g++)
+      for (int d = 0; d < 3; d++) gf[e][0][g][d] += gbuf[24 * (size_t)e + 3 * g + d];
+
+  if (ef || vf) {
+    double energy = 0.0, vir[6];
+    ebuf.resize(std::max(na, 1));
+    vbuf.resize(6 * (size_t)std::max(na, 1));
+    enbuf.resize(8 * (size_t)std::max(ne, 1));
+    vnbuf.resize(48 * (size_t)std::max(ne, 1));
+    status(cacb200_get_energy(ctx, &energy, vir, pair->eflag_atom ? ebuf.data() : nullptr,
+                              pair->vflag_atom ? vbuf.data() : nullptr,
+                              pair->eflag_atom ? enbuf.data() : nullptr,
+                              pair->vflag_atom ? vnbuf.data() : nullptr),
+           "get_energy");
+    if (pair->eflag_global) pair->eng_vdwl += energy;
+    if (pair->vflag_global)
+      for (int k = 0; k < 6; k++) pair->virial[k] += vir[k];
+    if (pair->eflag_atom) {
+      for (int i = 0; i < na; i++) pair->eatom[i] += ebuf[i];
+      for (int e = 0; e < ne; e++)
+        for (int n = 0; n < 8; n++) pair->enode[e][0][n] += enbuf[8 * (size_t)e + n];
+    }
+    if (pair->vflag_atom) {
+      for (int i = 0; i < na; i++)
+        for (int k = 0; k < 6; k++) pair->vatom[i][k] += vbuf[6 * (size_t)i + k];
+      for (int e = 0; e < ne; e++)
+        for (int n = 0; n < 8; n++)
+          for (int k = 0; k < 6; k++) pair->vnode[e][0][n][k] += vnbuf[48 * (size_t)e + 6 * n + k];
+    }
+  }
+}
+
+void B200Bridge::run_nve(int nsteps, double dt, int every)
+{
+  check_system();
+  upload(true);
+  status(cacb200_set_neighbor(ctx, neighbor->skin, every), "set_neighbor");
+  status(cacb200_setup(ctx), "setup");
+  status(cacb200_run_nve(ctx, nsteps, dt, 0, 0), "run_nve");
+  int na = atom->nlocal, ne = element->nlocal;
+  status(cacb200_get_state(ctx, na ? &atom->x[0][0] : nullptr, na ? &atom->v[0][0] : nullptr,
+                           ne ? &element->nodex[0][0][0][0] : nullptr,
+                           ne ? &element->nodev[0][0][0][0] : nullptr),
+         "get_state");
+  fbuf.resize(3 * (size_t)std::max(na, 1));
+  gbuf.resize(24 * (size_t)std::max(ne, 1));
+  std::vector<double> nf(24 * (size_t)std::max(ne, 1));
+  status(cacb200_get_forces(ctx, fbuf.data(), nf.data(), gbuf.data()), "get_forces");
+  for (int i = 0; i < na; i++)
+    for (int d = 0; d < 3; d++) atom->f[i][d] = fbuf[3 * (size_t)i + d];
+  for (int e = 0; e < ne; e++)
+    for (int n = 0; n < 8; n++)
+      for (int d = 0; d < 3; d++) {
+        element->nodef[e][0][n][d] = nf[24 * (size_t)e + 3 * n + d];
+        element->gaussf[e][0][n][d] = gbuf[24 * (size_t)e + 3 * n + d];
+      }
+  uploaded_na = uploaded_ne = -1;   // the reference must set up again (ghosts are stale)
+}
+
+void B200Bridge::dump_list(const char *file, int half)
+{
+  check_system();
+  upload(false);
+  status(cacb200_set_neighbor(ctx, neighbor->skin, 0), "set_neighbor");
+  status(cacb200_build_lists(ctx, half), "build_lists");
+  int64_t n = 0;
+  int nsites = 0;
+  status(cacb200_list_size(ctx, half, &n, &nsites), "list_size");
+  std::vector<int64_t> off(nsites + 1);
+  std::vector<int8_t> kind(std::max<int64_t>(n, 1)), img(3 * std::max<int64_t>(n, 1));
+  std::vector<int32_t> idx(std::max<int64_t>(n, 1)), site(std::max<int64_t>(n, 1));
+  status(cacb200_get_list(ctx, half, off.data(), kind.data(), idx.data(), site.data(), img.data()),
+         "get_list");
+  int na = atom->nlocal;
+  typedef std::tuple<int, int, int, int, int, int> Key;
+  std::vector<std::pair<Key, std::vector<Key>>> rows(nsites);
+  for (int i = 0; i < nsites; i++) {
+    Key ik = i < na ? Key(0, (int)atom->tag[i], -1, 0, 0, 0)
+                    : Key(1, (int)element->tag[(i - na) / 8], (i - na) % 8, 0, 0, 0);
+    rows[i].first = ik;
+    for (int64_t k = off[i]; k < off[i + 1]; k++) {
+      int t = kind[k] == 0 ? (int)atom->tag[idx[k]] : (int)element->tag[idx[k]];
+      rows[i].second.emplace_back(kind[k], t, site[k], img[3 * k], img[3 * k + 1], img[3 * k + 2]);
+    }
+    std::sort(rows[i].second.begin(), rows[i].second.end());
+  }
+  std::sort(rows.begin(), rows.end(),
+            [](const std::pair<Key, std::vector<Key>> &a, const std::pair<Key, std::vector<Key>> &b) {
+              return a.first < b.first;
+            });
+  FILE *fp = fopen(file, "w");
+  if (!fp) error->one(FLERR, "write_b200_neighbor: cannot open file");
+  fprintf(fp, "# cac b200 neighbour list v1: I kind tag site n / J kind tag site sx sy sz\n");
+  fprintf(fp, "inum %d\n", nsites);
+  for (auto &r : rows) {
+    fprintf(fp, "I %d %d %d %d\n", std::get<0>(r.first), std::get<1>(r.first), std::get<2>(r.first),
+            (int)r.second.size());
+    for (auto &k : r.second)
+      fprintf(fp, "J %d %d %d %d %d %d\n", std::get<0>(k), std::get<1>(k), std::get<2>(k), std::get<3>(k),
+              std::get<4>(k), std::get<5>(k));
+  }
+  fclose(fp);
+}

@@ -1,0 +1,62 @@
+/*
+ * Bridge between the CAC reference's host data (Atom, Element, Domain, Pair)
+ * and one cacb200 context (include/cacb200.h).  Used by the /b200 styles of
+ * this package; compiled into the reference executable together with them.
+ *
+ * The bridge owns the device context of one system.  Every force call copies
+ * the owned atoms' and elements' positions to the device (the whole system on
+ * the first call and whenever the reference has just rebuilt its neighbour
+ * lists, Neighbor::ago == 0, so that atom order and ghost images stay in step
+ * with the reference), evaluates the pair style there and adds the owned
+ * forces, Gauss-point forces, energies and virial back into the reference's
+ * arrays.  Ghost sites need nothing: on one rank every ghost is a periodic
+ * image, and the device applies the images itself, so owners receive their
+ * complete forces and the reference's reverse communication adds zeros.
+ */
+#ifndef CAC_B200_BRIDGE_H
+#define CAC_B200_BRIDGE_H
+
+#include <vector>
+
+#include "pointers.h"
+
+struct cacb200_ctx;
+
+namespace CAC_NS {
+
+class B200Bridge : protected Pointers {
+ public:
+  explicit B200Bridge(class CAC *);
+  ~B200Bridge();
+
+  void set_lj(double epsilon, double sigma, double cut);
+  void set_eam(int nrho, double drho, int nr, double dr, double cut, const double *frho,
+               const double *rhor, const double *z2r);
+  // Pair::compute body: fills atom->f, element->gaussf, eng_vdwl, virial and
+  // the per-site arrays of `pair` according to its ev flags.
+  void compute(class Pair *pair);
+  // run N velocity-Verlet steps on the device (run_b200 command)
+  void run_nve(int nsteps, double dt, int every);
+  // canonical neighbour-list dump (write_b200_neighbor command)
+  void dump_list(const char *file, int half);
+
+  cacb200_ctx *ctx = nullptr;
+
+ private:
+  int pair_style = 0;
+  std::vector<double> lj;                 // eps, sigma, cut
+  std::vector<double> eam_frho, eam_rhor, eam_z2r;
+  int eam_nrho = 0, eam_nr = 0;
+  double eam_drho = 0, eam_dr = 0, eam_cut = 0;
+  int uploaded_na = -1, uploaded_ne = -1;
+  std::vector<double> fbuf, gbuf, ebuf, vbuf, enbuf, vnbuf;
+
+  void check_system();
+  void upload(bool with_velocities);
+  void configure_pair();
+  void status(int rc, const char *what);
+};
+
+}  // namespace CAC_NS
+
+#endif

@@ -1,0 +1,93 @@
+"""The package's reference-side styles (cac_b200/styles) inside the reference's
+own executable: pair_style lj/cut/b200 and eam/alloy/b200 as drop-ins for
+lj/cut and eam/alloy, run_b200 and write_b200_neighbor.  The harness
+executable oracle/_ref/cac_b200 is built by ``make -C oracle app``."""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from cac_b200 import gen
+from helpers import CASES, N2G, counts, digest, rel_err
+
+pytestmark = pytest.mark.gpu
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+APP = os.path.join(ROOT, "oracle", "_ref", "cac_b200")
+TOL = 1e-10
+
+HEADER = """units metal
+dimension 3
+boundary p p p
+atom_style atomic
+element_style cac 8 1 wscale 1 1 1 1
+read_data data.cac
+"""
+TAIL = "neighbor 1.0 bin\nneigh_modify every 10 delay 0 check no\ntimestep 0.001\nfix 1 all nve\n"
+
+
+def pair_lines(pair):
+    if pair == "lj":
+        return "pair_style lj/cut/b200 5.5\npair_coeff 1 1 0.4093 2.338\n"
+    return "pair_style eam/alloy/b200\npair_coeff * * cu.setfl Cu\n"
+
+
+def run_app(tmp_path, case, body):
+    import oracle
+    build, pair, _ = CASES[case]
+    s = build()
+    gen.write_data(s, str(tmp_path / "data.cac"))
+    gen.write_setfl(gen.EamParams(), str(tmp_path / "cu.setfl"))
+    (tmp_path / "in.cac").write_text(HEADER + pair_lines(pair) + TAIL + body)
+    r = subprocess.run([APP, "-in", "in.cac"], cwd=tmp_path, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stdout[-3000:] + r.stderr[-3000:]
+    return s, oracle
+
+
+@pytest.fixture(scope="module", autouse=True)
+def app_present():
+    if not os.path.exists(APP):
+        pytest.fail("oracle/_ref/cac_b200 is missing: build it with make -C oracle app")
+
+
+@pytest.mark.parametrize("case", ["tiny_lj", "tiny_eam"])
+def test_pair_style_drop_in_setup_forces(case, golden, tmp_path):
+    g = golden(case)
+    s, O = run_app(tmp_path, case, "run 0\noracle_dump setup.txt compute\n")
+    d = O.read_dump(str(tmp_path / "setup.txt"))
+    assert rel_err(d["f"], g["f"]) < TOL
+    assert rel_err(d["nodef"], g["nodef"]) < TOL
+    assert rel_err(d["gaussf_at_node"], g["gaussf_at_node"]) < TOL
+    assert abs(d["energy"] - float(g["energy"])) / abs(float(g["energy"])) < TOL
+    assert np.abs(d["virial"] - g["virial"]).max() / np.abs(g["virial"]).max() < TOL
+    assert np.abs(d["eatom"] - g["eatom"]).max() / np.abs(g["eatom"]).max() < TOL
+    assert np.abs(d["enode"] - g["enode"]).max() / np.abs(g["eatom"]).max() < TOL
+
+
+@pytest.mark.parametrize("case", ["tiny_lj", "tiny_eam"])
+@pytest.mark.parametrize("mode", ["run", "run_b200"])
+def test_trajectory_in_reference_loop(case, mode, golden, tmp_path):
+    """`run N` (reference Verlet + fix nve, device forces) and `run_b200 N`
+    (whole loop on the device) both reproduce the reference trajectory."""
+    g = golden(case)
+    n = int(g["nsteps"])
+    s, O = run_app(tmp_path, case, f"{mode} {n}\noracle_dump end.txt state\n")
+    e = O.read_dump(str(tmp_path / "end.txt"))
+    assert np.abs(e["x"] - g["end_x"]).max() < 1e-10
+    assert np.abs(e["nodex"] - g["end_nodex"]).max() < 1e-10
+    assert rel_err(e["v"], g["end_v"]) < TOL
+    assert rel_err(e["nodev"], g["end_nodev"]) < TOL
+    assert rel_err(e["f"], g["end_f"]) < TOL
+    assert rel_err(e["nodef"], g["end_nodef"]) < TOL
+
+
+@pytest.mark.parametrize("case", ["tiny_lj", "tiny_eam"])
+def test_device_lists_written_by_the_style(case, golden, tmp_path):
+    g = golden(case)
+    s, O = run_app(tmp_path, case, "write_b200_neighbor half.txt half\nwrite_b200_neighbor full.txt full\n")
+    nsites = s.natoms + 8 * s.nelements
+    for key in ("half", "full"):
+        rows = O.read_neigh(str(tmp_path / f"{key}.txt"), s.natoms)
+        assert np.array_equal(counts(rows, nsites), g[key + "_counts"])
+        assert digest(rows) == str(g[key + "_digest"])
