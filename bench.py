@@ -12,6 +12,14 @@ One step = one velocity-Verlet timestep of the whole system (force evaluation
 with both EAM passes, nodal assembly, integration; a list rebuild every 10th
 step).  value = atom+IP sites x steps / device time (max over ranks).
 
+The K timed steps run as trajectories of at most ``--segment`` (50) steps,
+each restarted from the seeded initial state on the device (state restore,
+list build and a force evaluation, all inside the timed region).  The
+reference's own dynamics on these systems gain energy without bound (its
+total energy rises by thousands of eV within 300 steps, LJ and EAM alike), so
+long trajectories stop being physical; the restarts keep the timed work on
+physical configurations.
+
 ``--gpus N`` (launched under torchrun) runs N independent replicas, one per
 GPU, with no collective on the data path ("replicas only"); value is the sum.
 
@@ -62,48 +70,62 @@ def build_workload(name: str, seed: int):
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    """Clocks and throttle reasons during the timed region: one ``nvidia-smi
+    -lms`` process started before the region and stopped after it."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, gpu: int):
+    def __init__(self, gpu: int, period_ms: int = 100):
         self.gpu = gpu
+        self.period_ms = period_ms
         self.samples = []
-        self._stop = threading.Event()
-        self._t = None
-
-    def _run(self):
-        while not self._stop.is_set():
-            try:
-                out = subprocess.run(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.FIELDS,
-                                      "--format=csv,noheader,nounits"], capture_output=True, text=True,
-                                     timeout=5).stdout.strip()
-                if out:
-                    self.samples.append(out.split(", "))
-            except Exception:
-                pass
-            self._stop.wait(0.1)
+        self._proc = None
+        self._file = None
 
     def __enter__(self):
-        self._t = threading.Thread(target=self._run, daemon=True)
-        self._t.start()
+        self._file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        try:
+            self._proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.FIELDS,
+                                           "--format=csv,noheader,nounits", "-lms", str(self.period_ms)],
+                                          stdout=self._file, stderr=subprocess.DEVNULL)
+        except Exception:
+            self._proc = None
+        time.sleep(0.3)
         return self
 
     def __exit__(self, *a):
-        self._stop.set()
-        self._t.join(timeout=10)
+        time.sleep(0.25)
+        if self._proc is not None:
+            self._proc.terminate()
+            try:
+                self._proc.wait(timeout=10)
+            except Exception:
+                self._proc.kill()
+        self._file.flush()
+        self._file.seek(0)
+        for line in self._file.read().splitlines():
+            parts = [t.strip() for t in line.split(",")]
+            if len(parts) >= 9:
+                self.samples.append(parts)
+        self._file.close()
+        os.unlink(self._file.name)
 
     def summary(self):
-        if not self.samples:
+        def num(t):
+            try:
+                return float(t)
+            except ValueError:
+                return None
+        sm = sorted(v for v in (num(s[1]) for s in self.samples) if v is not None)
+        mx = [v for v in (num(s[2]) for s in self.samples) if v is not None]
+        if not sm:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
-        sm = sorted(float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit())
-        mx = max(float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit())
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         reasons = sorted({names[k] for s in self.samples for k in range(4)
-                          if len(s) > 5 + k and s[5 + k].strip().lower() == "active"})
-        return {"sm_mhz": sm[len(sm) // 2] if sm else None, "sm_max_mhz": mx, "reasons": reasons,
+                          if s[5 + k].lower() == "active"})
+        return {"sm_mhz": sm[len(sm) // 2], "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
                 "samples": len(self.samples)}
 
 
@@ -207,9 +229,23 @@ def b200_arm(args, rank, local, ws, dist):
     eng.set_precision(api.MIXED if args.form == "mixed" else api.FP64)
     eng.neighbor(1.0, 10)
     eng.setup()
+    eng.snapshot()
     stream = torch.cuda.ExternalStream(eng.stream, device=torch.device("cuda", local))
+    seg = max(1, min(args.segment, args.steps))
 
-    eng.run_nve(args.warmup, 0.001)
+    def trajectory(nsteps: int, first: bool):
+        """nsteps of velocity Verlet as segments of at most `seg` steps, each
+        from the seeded initial state (restore + list build + forces)."""
+        done = 0
+        while done < nsteps:
+            if not (first and done == 0):
+                eng.restore()
+                eng.setup()
+            k = min(seg, nsteps - done)
+            eng.run_nve(k, 0.001)
+            done += k
+
+    trajectory(args.warmup, True)
     torch.cuda.synchronize(local)
     if dist:
         dist.barrier()
@@ -220,7 +256,7 @@ def b200_arm(args, rank, local, ws, dist):
         if dist:
             dist.barrier()
         e0.record(stream)
-        eng.run_nve(args.steps, 0.001)
+        trajectory(args.steps, False)
         e1.record(stream)
         torch.cuda.synchronize(local)
         if dist:
@@ -234,8 +270,11 @@ def b200_arm(args, rank, local, ws, dist):
     value = units * args.steps * ws / (ms_max / 1000.0)
 
     # per-kernel device times (CUDA events around every launch) for the roofline
+    nprof = min(seg, 50)
+    eng.restore()
+    eng.setup()
     eng.profile(True)
-    eng.run_nve(max(20, min(args.steps, 100)), 0.001)
+    eng.run_nve(nprof, 0.001)
     prof = eng.profile_read()
     eng.profile(False)
     timed = {k: v for k, v in prof.items() if alg_bytes_per_site(k) > 0}
@@ -246,7 +285,9 @@ def b200_arm(args, rank, local, ws, dist):
     alg = alg_bytes_per_site(dom[0]) * nsi
     hbm, hbm_kind = peaks()
     achieved = alg / (avg_ms / 1000.0) / 1e9
-    launches_per_step = sum(v[1] for v in prof.values()) / max(20, min(args.steps, 100))
+    launches_per_step = sum(v[1] for v in prof.values()) / nprof
+    eng.restore()
+    eng.setup()
 
     # end to end through the C ABI with pinned host buffers: every step copies the
     # state in (x, v, nodes), runs one step, and reads the state back
@@ -259,7 +300,7 @@ def b200_arm(args, rank, local, ws, dist):
     v_h[:] = v0
     nx_h[:] = nx0
     nv_h[:] = nv0
-    k_e2e = max(5, min(args.steps, 50))
+    k_e2e = max(5, min(args.steps, seg))
     import ctypes as C
     _p = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))
     torch.cuda.synchronize(local)
@@ -304,7 +345,9 @@ def b200_arm(args, rank, local, ws, dist):
             "roofline": {"bound": "hbm", "kernel": dom[0], "achieved": achieved, "peak": hbm,
                          "peak_kind": hbm_kind, "unit": "GB/s", "frac": achieved / hbm, "traffic": None,
                          "avg_launch_ms": avg_ms, "alg_bytes_per_launch": alg},
-            "kernels_ms_per_step": {k: v[0] / max(v[1], 1) for k, v in sorted(prof.items())},
+            "kernels_ms_per_launch": {k: v[0] / max(v[1], 1) for k, v in sorted(prof.items())},
+            "kernels_ms_per_step": {k: v[0] / nprof for k, v in sorted(prof.items())},
+            "segment_steps": seg,
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": bytes_state,
                     "d2h_bytes_per_step": bytes_state, "steps": k_e2e},
@@ -324,6 +367,9 @@ def main():
     ap.add_argument("--workload", default="eam_1m")
     ap.add_argument("--form", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--segment", type=int, default=50,
+                    help="steps per trajectory from the seeded initial state (the reference's CAC "
+                         "dynamics heat up unboundedly after ~100 steps, so long runs restart)")
     args = ap.parse_args()
     rank, local, ws, dist = dist_init()
     try:

@@ -66,6 +66,8 @@ SIGNATURES = [
     ("cacb200_nve_final", C.c_int, [C.c_void_p, C.c_double]),
     ("cacb200_setup", C.c_int, [C.c_void_p]),
     ("cacb200_run_nve", C.c_int, [C.c_void_p, C.c_int, C.c_double, C.c_int, C.c_int]),
+    ("cacb200_snapshot", C.c_int, [C.c_void_p]),
+    ("cacb200_restore", C.c_int, [C.c_void_p]),
     ("cacb200_profile", C.c_int, [C.c_void_p, C.c_int]),
     ("cacb200_profile_read", C.c_int, [C.c_void_p, C.c_int, C.c_char_p, _dp, C.POINTER(C.c_int64),
                                        C.POINTER(C.c_int)]),
@@ -217,6 +219,12 @@ class Engine:
 
     def run_nve(self, nsteps: int, dt: float = 0.001, eflag: int = 0, vflag: int = 0) -> None:
         self._check(self.lib.cacb200_run_nve(self.h, nsteps, dt, eflag, vflag), "run_nve")
+
+    def snapshot(self) -> None:
+        self._check(self.lib.cacb200_snapshot(self.h), "snapshot")
+
+    def restore(self) -> None:
+        self._check(self.lib.cacb200_restore(self.h), "restore")
 
     def counts(self):
         a, e, s = C.c_int(), C.c_int(), C.c_int()

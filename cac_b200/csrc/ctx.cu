@@ -187,6 +187,36 @@ void get_state(Ctx &c, double *x, double *v, double *nodex, double *nodev) {
   CACB200_CUDA(cudaStreamSynchronize(c.stream));
 }
 
+void snapshot(Ctx &c) {
+  c.check_system();
+  size_t na = std::max(c.na, 1), ne = std::max(c.ne, 1);
+  c.snap_x.reserve(na);
+  c.snap_v.reserve(3 * na);
+  c.snap_nodex.reserve(24 * ne);
+  c.snap_nodev.reserve(24 * ne);
+  auto d2d = [&](void *dst, const void *src, size_t bytes) {
+    if (bytes) CACB200_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, c.stream));
+  };
+  d2d(c.snap_x.p, c.xs.p, sizeof(double4) * c.na);
+  d2d(c.snap_v.p, c.v.p, sizeof(double) * 3 * c.na);
+  d2d(c.snap_nodex.p, c.nodex.p, sizeof(double) * 24 * c.ne);
+  d2d(c.snap_nodev.p, c.nodev.p, sizeof(double) * 24 * c.ne);
+  c.have_snapshot = true;
+}
+
+void restore(Ctx &c) {
+  c.check_system();
+  if (!c.have_snapshot) throw Error(CACB200_ESTATE, "no snapshot taken");
+  auto d2d = [&](void *dst, const void *src, size_t bytes) {
+    if (bytes) CACB200_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, c.stream));
+  };
+  d2d(c.xs.p, c.snap_x.p, sizeof(double4) * c.na);
+  d2d(c.v.p, c.snap_v.p, sizeof(double) * 3 * c.na);
+  d2d(c.nodex.p, c.snap_nodex.p, sizeof(double) * 24 * c.ne);
+  d2d(c.nodev.p, c.snap_nodev.p, sizeof(double) * 24 * c.ne);
+  c.lists_valid = false;
+}
+
 void fetch_ev(Ctx &c) {
   if (!c.ev_pending) return;
   double h[7];
@@ -478,6 +508,18 @@ int cacb200_setup(cacb200_ctx *ctx) {
 int cacb200_run_nve(cacb200_ctx *ctx, int nsteps, double dt, int eflag, int vflag) {
   API_BEGIN
   run_nve(c, nsteps, dt, eflag, vflag);
+  API_END
+}
+
+int cacb200_snapshot(cacb200_ctx *ctx) {
+  API_BEGIN
+  snapshot(c);
+  API_END
+}
+
+int cacb200_restore(cacb200_ctx *ctx) {
+  API_BEGIN
+  restore(c);
   API_END
 }
 

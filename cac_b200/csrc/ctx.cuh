@@ -113,6 +113,9 @@ struct Ctx {
 
   DBuf<double> v, f;             // atoms [na*3]
   DBuf<double> stage;            // [na*3] host-transfer staging for positions
+  DBuf<double4> snap_x;          // device snapshot of the state (cacb200_snapshot)
+  DBuf<double> snap_v, snap_nodex, snap_nodev;
+  bool have_snapshot = false;
   DBuf<double> nodex, nodev, nodef, gaussf;  // [ne*8*3]
   DBuf<double> rho;              // [na + 8*ne]: atoms then nodes (node order)
   DBuf<double> phi_site;         // [nsite_i] embedding energy F(rho) per i-site (EAM, eflag)

@@ -10,12 +10,14 @@
 // with products and differences rounded separately (no FMA).
 //
 // Candidates come from two periodic cell grids instead of the reference's
-// bin/stencil/sub-element walk: atoms from a grid of cell >= cutneigh/2 with a
-// 5x5x5 stencil, element sites from a grid over element centres of cell
-// >= cutneigh + (centre-to-node radius + affine deviation), and for each
-// candidate element only the lattice sites whose affine position can lie
-// within cutneigh (a box in lattice-index space).  Both prunings are exact
-// supersets, so they change cost, not membership.
+// bin/stencil/sub-element walk: atoms from a grid of cell >= cutneigh with a
+// 3x3x3 stencil (atoms: one block per cell, the cell's atoms as lanes sharing
+// broadcast candidate loads; Gauss points: one thread each), element sites
+// from a grid over element centres of cell >= cutneigh + (centre-to-node
+// radius + affine deviation), and for each candidate element only the lattice
+// sites whose affine position can lie within cutneigh (a box in lattice-index
+// space).  Both prunings are exact supersets, so they change cost, not
+// membership.
 //
 // Storage rules (the reference's, restated):
 //   full  (npair_full_bin.cpp:23-358): every neighbour except the site itself.
@@ -192,12 +194,17 @@ __global__ void k_elem_keys(const double4 *ecenter, int ne, Grid g, BoxD b, int 
 }
 
 // cell_start[c] = first sorted position with key >= c, for c in [0, ncell]
+// (lower bound by binary search, one thread per cell)
 __global__ void k_cell_start(const int *skey, int n, int ncell, int *start) {
-  int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k > n) return;
-  int prev = (k == 0) ? -1 : skey[k - 1];
-  int cur = (k == n) ? ncell : skey[k];
-  for (int c = prev + 1; c <= cur; c++) start[c] = k;
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c > ncell) return;
+  int lo = 0, hi = n;
+  while (lo < hi) {
+    int mid = (lo + hi) >> 1;
+    if (skey[mid] < c) lo = mid + 1;
+    else hi = mid;
+  }
+  start[c] = lo;
 }
 
 __global__ void k_gather_pos(const double4 *xs, const int *sidx, int n, double4 *out) {
@@ -275,207 +282,198 @@ __device__ __forceinline__ void emit(const BuildArgs &A, int i, int &n, int *raw
   n++;
 }
 
-__global__ void __launch_bounds__(128) k_build(BuildArgs A) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= A.nsi) return;
-  const bool iatom = i < A.na;
-  int ie = -1, ig = -1, iu = -1;
-  double xi[3];
-  if (iatom) {
-    double4 p = A.xs[i];
-    xi[0] = p.x;
-    xi[1] = p.y;
-    xi[2] = p.z;
-  } else {
-    ie = (i - A.na) / NG;
-    ig = (i - A.na) % NG;
-    iu = gauss_site(ig);
-    const double *nx = A.nodex + (size_t)ie * 24 + 3 * gauss_node(ig);
-    xi[0] = nx[0];
-    xi[1] = nx[1];
-    xi[2] = nx[2];
-  }
-  // wrapped query point: wi = xi + ti L inside the box
-  double wi[3];
+// One query point (an i-site) of the build.
+struct Query {
+  int i;
+  bool iatom;
+  int ie, ig, iu;
+  double xi[3];   // raw position
+  double wi[3];   // wrapped into the box: wi = xi + ti L
   int ti[3];
+};
+
+__device__ __forceinline__ void make_query(const BuildArgs &A, int i, Query &q) {
+  q.i = i;
+  q.iatom = i < A.na;
+  q.ie = q.ig = q.iu = -1;
+  if (q.iatom) {
+    double4 p = A.xs[i];
+    q.xi[0] = p.x;
+    q.xi[1] = p.y;
+    q.xi[2] = p.z;
+  } else {
+    q.ie = (i - A.na) / NG;
+    q.ig = (i - A.na) % NG;
+    q.iu = gauss_site(q.ig);
+    const double *nx = A.nodex + (size_t)q.ie * 24 + 3 * gauss_node(q.ig);
+    q.xi[0] = nx[0];
+    q.xi[1] = nx[1];
+    q.xi[2] = nx[2];
+  }
 #pragma unroll
   for (int d = 0; d < 3; d++) {
-    double f = floor((xi[d] - A.b.lo[d]) / A.b.L[d]);
-    ti[d] = -(int)f;
-    wi[d] = xi[d] - f * A.b.L[d];
-    if (wi[d] >= A.b.hi[d]) {
-      wi[d] -= A.b.L[d];
-      ti[d] -= 1;
+    double f = floor((q.xi[d] - A.b.lo[d]) / A.b.L[d]);
+    q.ti[d] = -(int)f;
+    q.wi[d] = q.xi[d] - f * A.b.L[d];
+    if (q.wi[d] >= A.b.hi[d]) {
+      q.wi[d] -= A.b.L[d];
+      q.ti[d] -= 1;
     }
-    if (wi[d] < A.b.lo[d]) {
-      wi[d] += A.b.L[d];
-      ti[d] += 1;
+    if (q.wi[d] < A.b.lo[d]) {
+      q.wi[d] += A.b.L[d];
+      q.ti[d] += 1;
     }
   }
-  const double pre = (A.cutneigh + 1e-6) * (A.cutneigh + 1e-6);
-  int nf = 0, nh = 0;
+}
 
-  // ------------------------------------------------------------- atoms
-  if (A.na > 0) {
-    int ci[3];
+// A candidate atom j seen in a cell with wrap count W: exact test and storage
+// rules (atoms are inside the box after pbc, so their own wrap is zero).
+__device__ __forceinline__ void try_atom(const BuildArgs &A, const Query &q, int j, const int W[3],
+                                         int &nf, int &nh) {
+  int s[3] = {W[0] - q.ti[0], W[1] - q.ti[1], W[2] - q.ti[2]};
+  bool zero = (s[0] == 0 && s[1] == 0 && s[2] == 0);
+  if (q.iatom && j == q.i && zero) return;
+  if (s[0] < -1 || s[0] > 1 || s[1] < -1 || s[1] > 1 || s[2] < -1 || s[2] > 1) {
+    atomicExch(&A.overflow[2], 1);
+    return;
+  }
+  double4 xj = A.xs[j];
+  double qq[3] = {xj.x, xj.y, xj.z};
+  if (!zero) {
+    qq[0] = s[0] ? __dadd_rn(qq[0], s[0] * A.b.L[0]) : qq[0];
+    qq[1] = s[1] ? __dadd_rn(qq[1], s[1] * A.b.L[1]) : qq[1];
+    qq[2] = s[2] ? __dadd_rn(qq[2], s[2] * A.b.L[2]) : qq[2];
+  }
+  double rsq = rsq_rn(__dsub_rn(q.xi[0], qq[0]), __dsub_rn(q.xi[1], qq[1]), __dsub_rn(q.xi[2], qq[2]));
+  if (!(rsq <= A.cutneighsq)) return;
+  int code = img_code(s[0], s[1], s[2]);
+  emit(A, q.i, nf, A.raw_full, A.img_full, j, code);
+  if (A.want_half && q.iatom) {
+    int ord = ref_bin_order(A.rb, q.xi, qq);
+    bool keep = ord > 0 || (ord == 0 && (zero ? (j > q.i) : above_right(qq, q.xi)));
+    if (keep) emit(A, q.i, nh, A.raw_half, A.img_half, j, code);
+  }
+}
+
+__device__ __forceinline__ void wrap_cell(int v, int nc, int &cell, int &W) {
+  W = 0;
+  while (v < 0) {
+    v += nc;
+    W--;
+  }
+  while (v >= nc) {
+    v -= nc;
+    W++;
+  }
+  cell = v;
+}
+
+// Lattice sites of the elements near the query point.
+__device__ void element_candidates(const BuildArgs &A, const Query &q, int &nf, int &nh) {
+  int ci[3];
 #pragma unroll
-    for (int d = 0; d < 3; d++)
-      ci[d] = min(max((int)((wi[d] - A.b.lo[d]) * A.ag.inv[d]), 0), A.ag.nc[d] - 1);
-    for (int oz = -2; oz <= 2; oz++) {
-      int cz = ci[2] + oz, Wz = 0;
-      while (cz < 0) { cz += A.ag.nc[2]; Wz--; }
-      while (cz >= A.ag.nc[2]) { cz -= A.ag.nc[2]; Wz++; }
-      for (int oy = -2; oy <= 2; oy++) {
-        int cy = ci[1] + oy, Wy = 0;
-        while (cy < 0) { cy += A.ag.nc[1]; Wy--; }
-        while (cy >= A.ag.nc[1]) { cy -= A.ag.nc[1]; Wy++; }
-        for (int ox = -2; ox <= 2; ox++) {
-          int cx = ci[0] + ox, Wx = 0;
-          while (cx < 0) { cx += A.ag.nc[0]; Wx--; }
-          while (cx >= A.ag.nc[0]) { cx -= A.ag.nc[0]; Wx++; }
-          int cell = (cz * A.ag.nc[1] + cy) * A.ag.nc[0] + cx;
-          int s[3] = {Wx - ti[0], Wy - ti[1], Wz - ti[2]};
-          double sh[3] = {Wx * A.b.L[0], Wy * A.b.L[1], Wz * A.b.L[2]};
-          int beg = A.acell_start[cell], end = A.acell_start[cell + 1];
-          for (int k = beg; k < end; k++) {
-            double4 pj = A.acell_pos[k];
-            double ex = wi[0] - (pj.x + sh[0]), ey = wi[1] - (pj.y + sh[1]), ez = wi[2] - (pj.z + sh[2]);
-            if (ex * ex + ey * ey + ez * ez > pre) continue;
-            int j = (int)__double_as_longlong(pj.w);
-            bool zero = (s[0] == 0 && s[1] == 0 && s[2] == 0);
-            if (iatom && j == i && zero) continue;
-            if (s[0] < -1 || s[0] > 1 || s[1] < -1 || s[1] > 1 || s[2] < -1 || s[2] > 1) {
-              atomicExch(&A.overflow[2], 1);
-              continue;
-            }
-            double4 xj = A.xs[j];
-            double q[3] = {xj.x, xj.y, xj.z};
-            if (!zero) {
-              q[0] = s[0] ? __dadd_rn(q[0], s[0] * A.b.L[0]) : q[0];
-              q[1] = s[1] ? __dadd_rn(q[1], s[1] * A.b.L[1]) : q[1];
-              q[2] = s[2] ? __dadd_rn(q[2], s[2] * A.b.L[2]) : q[2];
-            }
-            double rsq = rsq_rn(__dsub_rn(xi[0], q[0]), __dsub_rn(xi[1], q[1]), __dsub_rn(xi[2], q[2]));
-            if (!(rsq <= A.cutneighsq)) continue;
-            int code = img_code(s[0], s[1], s[2]);
-            emit(A, i, nf, A.raw_full, A.img_full, j, code);
-            if (A.want_half && iatom) {
-              int ord = ref_bin_order(A.rb, xi, q);
-              bool keep = ord > 0 || (ord == 0 && (zero ? (j > i) : above_right(q, xi)));
-              if (keep) emit(A, i, nh, A.raw_half, A.img_half, j, code);
-            }
+  for (int d = 0; d < 3; d++)
+    ci[d] = min(max((int)((q.wi[d] - A.b.lo[d]) * A.eg.inv[d]), 0), A.eg.nc[d] - 1);
+  double icen[3] = {0, 0, 0};
+  if (!q.iatom) {
+    double4 c = A.ecenter[q.ie];
+    icen[0] = c.x;
+    icen[1] = c.y;
+    icen[2] = c.z;
+  }
+  for (int oz = -1; oz <= 1; oz++) {
+    int cz, Wz;
+    wrap_cell(ci[2] + oz, A.eg.nc[2], cz, Wz);
+    for (int oy = -1; oy <= 1; oy++) {
+      int cy, Wy;
+      wrap_cell(ci[1] + oy, A.eg.nc[1], cy, Wy);
+      for (int ox = -1; ox <= 1; ox++) {
+        int cx, Wx;
+        wrap_cell(ci[0] + ox, A.eg.nc[0], cx, Wx);
+        int cell = (cz * A.eg.nc[1] + cy) * A.eg.nc[0] + cx;
+        int beg = A.ecell_start[cell], end = A.ecell_start[cell + 1];
+        if (beg == end) continue;
+        int s[3] = {Wx - q.ti[0], Wy - q.ti[1], Wz - q.ti[2]};
+        bool zero = (s[0] == 0 && s[1] == 0 && s[2] == 0);
+        double sL[3] = {s[0] * A.b.L[0], s[1] * A.b.L[1], s[2] * A.b.L[2]};
+        for (int kk = beg; kk < end; kk++) {
+          int e = A.ecell_elems[kk];
+          double4 ce = A.ecenter[e];
+          // sphere test in the element's raw frame: |xi - s L - centre| <= cutneigh + R
+          double p[3] = {q.xi[0] - sL[0], q.xi[1] - sL[1], q.xi[2] - sL[2]};
+          const double *fr = A.eframe + (size_t)e * 16;
+          double dmax = fr[12];
+          double R = ce.w + dmax + A.cutneigh + 1e-6;
+          double dcx = p[0] - ce.x, dcy = p[1] - ce.y, dcz = p[2] - ce.z;
+          if (dcx * dcx + dcy * dcy + dcz * dcz > R * R) continue;
+          if (s[0] < -1 || s[0] > 1 || s[1] < -1 || s[1] > 1 || s[2] < -1 || s[2] > 1) {
+            atomicExch(&A.overflow[2], 1);
+            continue;
           }
-        }
-      }
-    }
-  }
-
-  // --------------------------------------------------- element lattice sites
-  if (A.ne > 0) {
-    int ci[3];
+          // lattice-index box of the sites whose affine position is within cutneigh + dmax
+          double rel[3] = {p[0] - fr[0], p[1] - fr[1], p[2] - fr[2]};
+          int lo[3], hi[3];
+          bool empty = false;
 #pragma unroll
-    for (int d = 0; d < 3; d++)
-      ci[d] = min(max((int)((wi[d] - A.b.lo[d]) * A.eg.inv[d]), 0), A.eg.nc[d] - 1);
-    double icen[3] = {0, 0, 0};
-    if (!iatom) {
-      double4 c = A.ecenter[ie];
-      icen[0] = c.x;
-      icen[1] = c.y;
-      icen[2] = c.z;
-    }
-    for (int oz = -1; oz <= 1; oz++) {
-      int cz = ci[2] + oz, Wz = 0;
-      while (cz < 0) { cz += A.eg.nc[2]; Wz--; }
-      while (cz >= A.eg.nc[2]) { cz -= A.eg.nc[2]; Wz++; }
-      for (int oy = -1; oy <= 1; oy++) {
-        int cy = ci[1] + oy, Wy = 0;
-        while (cy < 0) { cy += A.eg.nc[1]; Wy--; }
-        while (cy >= A.eg.nc[1]) { cy -= A.eg.nc[1]; Wy++; }
-        for (int ox = -1; ox <= 1; ox++) {
-          int cx = ci[0] + ox, Wx = 0;
-          while (cx < 0) { cx += A.eg.nc[0]; Wx--; }
-          while (cx >= A.eg.nc[0]) { cx -= A.eg.nc[0]; Wx++; }
-          int cell = (cz * A.eg.nc[1] + cy) * A.eg.nc[0] + cx;
-          int s[3] = {Wx - ti[0], Wy - ti[1], Wz - ti[2]};
-          bool zero = (s[0] == 0 && s[1] == 0 && s[2] == 0);
-          double sL[3] = {s[0] * A.b.L[0], s[1] * A.b.L[1], s[2] * A.b.L[2]};
-          int beg = A.ecell_start[cell], end = A.ecell_start[cell + 1];
-          for (int kk = beg; kk < end; kk++) {
-            int e = A.ecell_elems[kk];
-            double4 ce = A.ecenter[e];
-            // quick sphere test on the raw frame: |xi - s L - centre| <= cutneigh + R
-            double p[3] = {xi[0] - sL[0], xi[1] - sL[1], xi[2] - sL[2]};
-            const double *fr = A.eframe + (size_t)e * 16;
-            double dmax = fr[12];
-            double R = ce.w + dmax + A.cutneigh + 1e-6;
-            double dcx = p[0] - ce.x, dcy = p[1] - ce.y, dcz = p[2] - ce.z;
-            if (dcx * dcx + dcy * dcy + dcz * dcz > R * R) continue;
-            if (s[0] < -1 || s[0] > 1 || s[1] < -1 || s[1] > 1 || s[2] < -1 || s[2] > 1) {
-              atomicExch(&A.overflow[2], 1);
-              continue;
-            }
-            // lattice-index box of sites whose affine position is within cutneigh + dmax
-            double rel[3] = {p[0] - fr[0], p[1] - fr[1], p[2] - fr[2]};
-            int lo[3], hi[3];
-            bool empty = false;
+          for (int r = 0; r < 3; r++) {
+            double a0 = fr[3 + 3 * r], a1 = fr[4 + 3 * r], a2 = fr[5 + 3 * r];
+            double fidx = a0 * rel[0] + a1 * rel[1] + a2 * rel[2];
+            double rho = (A.cutneigh + dmax + 1e-6) * sqrt(a0 * a0 + a1 * a1 + a2 * a2) + 1e-6;
+            lo[r] = max(0, (int)ceil(fidx - rho));
+            hi[r] = min(NC - 1, (int)floor(fidx + rho));
+            if (lo[r] > hi[r]) empty = true;
+          }
+          if (empty) continue;
+          const double *nx = A.nodex + (size_t)e * 24;
+          double g[24];  // ghost node coordinates nodex + s L
 #pragma unroll
-            for (int r = 0; r < 3; r++) {
-              double a0 = fr[3 + 3 * r], a1 = fr[4 + 3 * r], a2 = fr[5 + 3 * r];
-              double fidx = a0 * rel[0] + a1 * rel[1] + a2 * rel[2];
-              double rho = (A.cutneigh + dmax + 1e-6) * sqrt(a0 * a0 + a1 * a1 + a2 * a2) + 1e-6;
-              lo[r] = max(0, (int)ceil(fidx - rho));
-              hi[r] = min(NC - 1, (int)floor(fidx + rho));
-              if (lo[r] > hi[r]) empty = true;
-            }
-            if (empty) continue;
-            const double *nx = A.nodex + (size_t)e * 24;
-            double g[24];  // ghost node coordinates nodex + s L
+          for (int k = 0; k < 8; k++)
 #pragma unroll
-            for (int k = 0; k < 8; k++)
+            for (int d = 0; d < 3; d++)
+              g[3 * k + d] = s[d] ? __dadd_rn(nx[3 * k + d], sL[d]) : nx[3 * k + d];
+          int code = img_code(s[0], s[1], s[2]);
+          double qcen[3] = {0, 0, 0};
+          if (!zero) {
+            qcen[0] = s[0] ? __dadd_rn(ce.x, sL[0]) : ce.x;
+            qcen[1] = s[1] ? __dadd_rn(ce.y, sL[1]) : ce.y;
+            qcen[2] = s[2] ? __dadd_rn(ce.z, sL[2]) : ce.z;
+          }
+          for (int a = lo[0]; a <= hi[0]; a++)
+            for (int bb = lo[1]; bb <= hi[1]; bb++)
+              for (int cc = lo[2]; cc <= hi[2]; cc++) {
+                int u = (a * NC + bb) * NC + cc;
+                if (!q.iatom && e == q.ie && u == q.iu && zero) continue;
+                double dx = q.xi[0], dy = q.xi[1], dz = q.xi[2];
 #pragma unroll
-              for (int d = 0; d < 3; d++)
-                g[3 * k + d] = s[d] ? __dadd_rn(nx[3 * k + d], sL[d]) : nx[3 * k + d];
-            int code = img_code(s[0], s[1], s[2]);
-            double qcen[3] = {0, 0, 0};
-            if (!zero) {
-              qcen[0] = s[0] ? __dadd_rn(ce.x, sL[0]) : ce.x;
-              qcen[1] = s[1] ? __dadd_rn(ce.y, sL[1]) : ce.y;
-              qcen[2] = s[2] ? __dadd_rn(ce.z, sL[2]) : ce.z;
-            }
-            for (int a = lo[0]; a <= hi[0]; a++)
-              for (int bb = lo[1]; bb <= hi[1]; bb++)
-                for (int cc = lo[2]; cc <= hi[2]; cc++) {
-                  int u = (a * NC + bb) * NC + cc;
-                  if (!iatom && e == ie && u == iu && zero) continue;
-                  double dx = xi[0], dy = xi[1], dz = xi[2];
-#pragma unroll
-                  for (int k = 0; k < 8; k++) {
-                    double N = shape_val(u, k);
-                    dx = __dsub_rn(dx, __dmul_rn(N, g[3 * k]));
-                    dy = __dsub_rn(dy, __dmul_rn(N, g[3 * k + 1]));
-                    dz = __dsub_rn(dz, __dmul_rn(N, g[3 * k + 2]));
-                  }
-                  double rsq = rsq_rn(dx, dy, dz);
-                  if (!(rsq <= A.cutneighsq)) continue;
-                  int val = KIND_SITE | (e * NU + u);
-                  emit(A, i, nf, A.raw_full, A.img_full, val, code);
-                  if (A.want_half) {
-                    bool keep = true;
-                    if (!iatom) {
-                      int jg = site_gauss(u);
-                      if (jg >= 0) {
-                        if (zero) keep = (ie < e) || (ie == e && ig < jg);
-                        else keep = above_right(qcen, icen);
-                      }
-                    }
-                    if (keep) emit(A, i, nh, A.raw_half, A.img_half, val, code);
-                  }
+                for (int k = 0; k < 8; k++) {
+                  double N = shape_val(u, k);
+                  dx = __dsub_rn(dx, __dmul_rn(N, g[3 * k]));
+                  dy = __dsub_rn(dy, __dmul_rn(N, g[3 * k + 1]));
+                  dz = __dsub_rn(dz, __dmul_rn(N, g[3 * k + 2]));
                 }
-          }
+                double rsq = rsq_rn(dx, dy, dz);
+                if (!(rsq <= A.cutneighsq)) continue;
+                int val = KIND_SITE | (e * NU + u);
+                emit(A, q.i, nf, A.raw_full, A.img_full, val, code);
+                if (A.want_half) {
+                  bool keep = true;
+                  if (!q.iatom) {
+                    int jg = site_gauss(u);
+                    if (jg >= 0) {
+                      if (zero) keep = (q.ie < e) || (q.ie == e && q.ig < jg);
+                      else keep = above_right(qcen, icen);
+                    }
+                  }
+                  if (keep) emit(A, q.i, nh, A.raw_half, A.img_half, val, code);
+                }
+              }
         }
       }
     }
   }
+}
+
+__device__ __forceinline__ void finish_counts(const BuildArgs &A, int i, int nf, int nh) {
   A.num_full[i] = nf;
   if (A.want_half) A.num_half[i] = nh;
   int m = max(nf, nh);
@@ -483,6 +481,93 @@ __global__ void __launch_bounds__(128) k_build(BuildArgs A) {
     atomicExch(&A.overflow[0], 1);
     atomicMax(&A.overflow[1], m);
   }
+}
+
+// Atoms: one block per cell of the atom grid (cell >= cutneigh); the lanes
+// are the cell's atoms and walk the 27 surrounding cells together, so every
+// candidate position is one broadcast load shared by the whole warp.
+__global__ void __launch_bounds__(64) k_build_atoms(BuildArgs A) {
+  const int home = blockIdx.x;
+  const int hbeg = A.acell_start[home], hend = A.acell_start[home + 1];
+  if (hbeg == hend) return;
+  const int nc0 = A.ag.nc[0], nc1 = A.ag.nc[1], nc2 = A.ag.nc[2];
+  const int hx = home % nc0, hy = (home / nc0) % nc1, hz = home / (nc0 * nc1);
+  const double pre = (A.cutneigh + 1e-6) * (A.cutneigh + 1e-6);
+  for (int base = hbeg; base < hend; base += blockDim.x) {
+    const int h = base + threadIdx.x;
+    const bool active = h < hend;
+    Query q;
+    int nf = 0, nh = 0;
+    if (active) make_query(A, (int)__double_as_longlong(A.acell_pos[h].w), q);
+    for (int oz = -1; oz <= 1; oz++) {
+      int cz, Wz;
+      wrap_cell(hz + oz, nc2, cz, Wz);
+      for (int oy = -1; oy <= 1; oy++) {
+        int cy, Wy;
+        wrap_cell(hy + oy, nc1, cy, Wy);
+        for (int ox = -1; ox <= 1; ox++) {
+          int cx, Wx;
+          wrap_cell(hx + ox, nc0, cx, Wx);
+          int cell = (cz * nc1 + cy) * nc0 + cx;
+          int W[3] = {Wx, Wy, Wz};
+          double sh[3] = {Wx * A.b.L[0], Wy * A.b.L[1], Wz * A.b.L[2]};
+          int beg = A.acell_start[cell], end = A.acell_start[cell + 1];
+          for (int k = beg; k < end; k++) {
+            double4 pj = A.acell_pos[k];
+            if (!active) continue;
+            double ex = q.wi[0] - (pj.x + sh[0]), ey = q.wi[1] - (pj.y + sh[1]), ez = q.wi[2] - (pj.z + sh[2]);
+            if (ex * ex + ey * ey + ez * ez > pre) continue;
+            try_atom(A, q, (int)__double_as_longlong(pj.w), W, nf, nh);
+          }
+        }
+      }
+    }
+    if (active) {
+      if (A.ne > 0) element_candidates(A, q, nf, nh);
+      finish_counts(A, q.i, nf, nh);
+    }
+  }
+}
+
+// Gauss points: one thread each; atoms from the 27 surrounding atom cells
+// (full list only), then element lattice sites.
+__global__ void __launch_bounds__(128) k_build_gauss(BuildArgs A) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= NG * A.ne) return;
+  Query q;
+  make_query(A, A.na + t, q);
+  int nf = 0, nh = 0;
+  if (A.na > 0) {
+    const double pre = (A.cutneigh + 1e-6) * (A.cutneigh + 1e-6);
+    int ci[3];
+#pragma unroll
+    for (int d = 0; d < 3; d++)
+      ci[d] = min(max((int)((q.wi[d] - A.b.lo[d]) * A.ag.inv[d]), 0), A.ag.nc[d] - 1);
+    for (int oz = -1; oz <= 1; oz++) {
+      int cz, Wz;
+      wrap_cell(ci[2] + oz, A.ag.nc[2], cz, Wz);
+      for (int oy = -1; oy <= 1; oy++) {
+        int cy, Wy;
+        wrap_cell(ci[1] + oy, A.ag.nc[1], cy, Wy);
+        for (int ox = -1; ox <= 1; ox++) {
+          int cx, Wx;
+          wrap_cell(ci[0] + ox, A.ag.nc[0], cx, Wx);
+          int cell = (cz * A.ag.nc[1] + cy) * A.ag.nc[0] + cx;
+          int W[3] = {Wx, Wy, Wz};
+          double sh[3] = {Wx * A.b.L[0], Wy * A.b.L[1], Wz * A.b.L[2]};
+          int beg = A.acell_start[cell], end = A.acell_start[cell + 1];
+          for (int k = beg; k < end; k++) {
+            double4 pj = A.acell_pos[k];
+            double ex = q.wi[0] - (pj.x + sh[0]), ey = q.wi[1] - (pj.y + sh[1]), ez = q.wi[2] - (pj.z + sh[2]);
+            if (ex * ex + ey * ey + ez * ez > pre) continue;
+            try_atom(A, q, (int)__double_as_longlong(pj.w), W, nf, nh);
+          }
+        }
+      }
+    }
+  }
+  element_candidates(A, q, nf, nh);
+  finish_counts(A, q.i, nf, nh);
 }
 
 // ------------------------------------------------------------- compaction
@@ -548,8 +633,8 @@ void setup_grids(Ctx &c, double ereach) {
   // candidate grids
   for (int d = 0; d < 3; d++) {
     double L = c.prd[d];
-    int na_c = (int)(L / (0.5 * c.cutneigh));
-    if (na_c < 1) throw Error(CACB200_EINVAL, "box shorter than half the neighbour cutoff");
+    int na_c = (int)(L / c.cutneigh);
+    if (na_c < 1) throw Error(CACB200_EINVAL, "box shorter than the neighbour cutoff");
     c.agrid.nc[d] = na_c;
     c.agrid.inv[d] = na_c / L;
     double reach = c.cutneigh + ereach + 1e-6;
@@ -629,7 +714,7 @@ void neigh_build(Ctx &c, bool want_half) {
       k_atom_keys<<<nblk(c.na, 256), 256, 0, c.stream>>>(c.xs.p, c.na, c.agrid, b, c.cell_key.p,
                                                          c.idx_tmp.p);
       sort_pairs<int>(c, c.cell_key.p, c.cell_key2.p, c.idx_tmp.p, c.idx_tmp2.p, c.na, c.agrid.ncell);
-      k_cell_start<<<nblk(c.na + 1, 256), 256, 0, c.stream>>>(c.cell_key2.p, c.na, c.agrid.ncell,
+      k_cell_start<<<nblk(c.agrid.ncell + 1, 256), 256, 0, c.stream>>>(c.cell_key2.p, c.na, c.agrid.ncell,
                                                               c.acell_start.p);
       k_gather_pos<<<nblk(c.na, 256), 256, 0, c.stream>>>(c.xs.p, c.idx_tmp2.p, c.na, c.acell_pos.p);
     } else {
@@ -639,7 +724,7 @@ void neigh_build(Ctx &c, bool want_half) {
       k_elem_keys<<<nblk(c.ne, 256), 256, 0, c.stream>>>(c.ecenter.p, c.ne, c.egrid, b, c.cell_key.p,
                                                          c.idx_tmp.p);
       sort_pairs<int>(c, c.cell_key.p, c.cell_key2.p, c.idx_tmp.p, c.ecell_elems.p, c.ne, c.egrid.ncell);
-      k_cell_start<<<nblk(c.ne + 1, 256), 256, 0, c.stream>>>(c.cell_key2.p, c.ne, c.egrid.ncell,
+      k_cell_start<<<nblk(c.egrid.ncell + 1, 256), 256, 0, c.stream>>>(c.cell_key2.p, c.ne, c.egrid.ncell,
                                                               c.ecell_start.p);
     } else {
       CACB200_CUDA(cudaMemsetAsync(c.ecell_start.p, 0, sizeof(int) * (c.egrid.ncell + 1), c.stream));
@@ -687,7 +772,8 @@ void neigh_build(Ctx &c, bool want_half) {
     A.overflow = c.overflow.p;
     {
       KernelTimer t(c, "build_list");
-      k_build<<<nblk(nsi, 128), 128, 0, c.stream>>>(A);
+      if (c.na) k_build_atoms<<<c.agrid.ncell, 64, 0, c.stream>>>(A);
+      if (c.ne) k_build_gauss<<<nblk(NG * c.ne, 128), 128, 0, c.stream>>>(A);
     }
     int ov[4];
     CACB200_CUDA(cudaMemcpyAsync(ov, c.overflow.p, sizeof(ov), cudaMemcpyDeviceToHost, c.stream));

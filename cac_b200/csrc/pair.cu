@@ -54,6 +54,33 @@ __device__ __forceinline__ void neighbour_pos(const PairArgs &A, int v, double4 
   }
 }
 
+// Walks a site's list four entries at a time: the four entry loads, then the
+// four position loads, are issued back to back before any of them is used, so
+// each thread keeps eight independent loads in flight instead of a chain of
+// dependent pairs.
+template <class F>
+__device__ __forceinline__ void for_each_neighbour(const PairArgs &A, const int *nb, int n, F &&f) {
+  int k = 0;
+  for (; k + 4 <= n; k += 4) {
+    int v0 = nb[(size_t)k * A.nsi], v1 = nb[(size_t)(k + 1) * A.nsi];
+    int v2 = nb[(size_t)(k + 2) * A.nsi], v3 = nb[(size_t)(k + 3) * A.nsi];
+    double4 p0, p1, p2, p3;
+    neighbour_pos(A, v0, p0);
+    neighbour_pos(A, v1, p1);
+    neighbour_pos(A, v2, p2);
+    neighbour_pos(A, v3, p3);
+    f(p0);
+    f(p1);
+    f(p2);
+    f(p3);
+  }
+  for (; k < n; k++) {
+    double4 p;
+    neighbour_pos(A, nb[(size_t)k * A.nsi], p);
+    f(p);
+  }
+}
+
 // Writes force and per-site energy/virial of i-site i and accumulates the
 // global sums (reduced per block in fixed order).
 __device__ __forceinline__ void finish_site(const PairArgs &A, int i, bool valid, const double fi[3],
@@ -108,9 +135,7 @@ __global__ void __launch_bounds__(128) k_lj(PairArgs A, LjParams P) {
     double4 xi = A.xs[i];
     int n = A.num[i];
     const int *nb = A.nbr + i;
-    for (int k = 0; k < n; k++) {
-      double4 xj;
-      neighbour_pos(A, nb[(size_t)k * A.nsi], xj);
+    auto pair = [&](const double4 &xj) {
       double dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
       double rsq = dx * dx + dy * dy + dz * dz;
       if (rsq < P.cutsq) {
@@ -131,7 +156,8 @@ __global__ void __launch_bounds__(128) k_lj(PairArgs A, LjParams P) {
           vsum[5] += dy * dz * fpair;
         }
       }
-    }
+    };
+    for_each_neighbour(A, nb, n, pair);
   }
   finish_site(A, i, valid, fi, esum, vsum, 0.0, 0.0);
 }
@@ -175,9 +201,7 @@ __global__ void __launch_bounds__(128) k_eam_rho(PairArgs A, EamTables T, double
   int n = A.num[i];
   const int *nb = A.nbr + i;
   double rho = 0.0;
-  for (int k = 0; k < n; k++) {
-    double4 xj;
-    neighbour_pos(A, nb[(size_t)k * A.nsi], xj);
+  auto pair = [&](const double4 &xj) {
     double dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
     double rsq = dx * dx + dy * dy + dz * dz;
     if (rsq < T.cutforcesq) {
@@ -189,7 +213,8 @@ __global__ void __launch_bounds__(128) k_eam_rho(PairArgs A, EamTables T, double
       double4 c = T.rhor_val[m];
       rho += ((c.x * p + c.y) * p + c.z) * p + c.w;
     }
-  }
+  };
+  for_each_neighbour(A, nb, n, pair);
   int slot = i;
   if (i >= A.na) {
     int e = (i - A.na) / NG, g = (i - A.na) % NG;
@@ -228,9 +253,7 @@ __global__ void __launch_bounds__(128) k_eam_force(PairArgs A, EamTables T, cons
     double fpi = xi.w;
     int n = A.num[i];
     const int *nb = A.nbr + i;
-    for (int k = 0; k < n; k++) {
-      double4 xj;
-      neighbour_pos(A, nb[(size_t)k * A.nsi], xj);
+    auto pair = [&](const double4 &xj) {
       double dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
       double rsq = dx * dx + dy * dy + dz * dz;
       if (rsq < T.cutforcesq) {
@@ -264,7 +287,8 @@ __global__ void __launch_bounds__(128) k_eam_force(PairArgs A, EamTables T, cons
           vsum[5] += dy * dz * fpair;
         }
       }
-    }
+    };
+    for_each_neighbour(A, nb, n, pair);
     if (A.eflag) {
       double phi = phi_site[i];
       eemb_site = phi;

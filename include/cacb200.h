@@ -136,9 +136,17 @@ int cacb200_nve_initial(cacb200_ctx *ctx, double dt);
 int cacb200_nve_final(cacb200_ctx *ctx, double dt);
 /* Verlet::setup + nsteps of Verlet::run with fix nve (verlet.cpp:64-360): lists
  * rebuilt every `every` steps (set_neighbor); energy/virial of the final step
- * when eflag/vflag are set.  Runs entirely on the device; returns when done. */
+ * when eflag/vflag are set.  Runs on the device; the call returns once every
+ * step is queued on the context's stream (list rebuilds synchronise). */
 int cacb200_setup(cacb200_ctx *ctx);
 int cacb200_run_nve(cacb200_ctx *ctx, int nsteps, double dt, int eflag, int vflag);
+
+/* Device-side copy of the state (x, v, nodex, nodev) and its restoration;
+ * restoring invalidates the lists (call cacb200_setup before stepping).
+ * Serves restarts of short trajectories and job preemption without host
+ * traffic. */
+int cacb200_snapshot(cacb200_ctx *ctx);
+int cacb200_restore(cacb200_ctx *ctx);
 
 /* Kernel timing: when enabled, every launch is bracketed by CUDA events and
  * per-kernel totals accumulate (ms, launches) until reset. */
