@@ -66,6 +66,11 @@ SIGNATURES = [
     ("cacb200_nve_final", C.c_int, [C.c_void_p, C.c_double]),
     ("cacb200_setup", C.c_int, [C.c_void_p]),
     ("cacb200_run_nve", C.c_int, [C.c_void_p, C.c_int, C.c_double, C.c_int, C.c_int]),
+    ("cacb200_set_fire_params", C.c_int, [C.c_void_p, C.c_int, C.c_double, C.c_double, C.c_double,
+                                          C.c_double, C.c_double, C.c_double, C.c_double, C.c_int,
+                                          C.c_int, C.c_int]),
+    ("cacb200_minimize_fire", C.c_int, [C.c_void_p, C.c_double, C.c_double, C.c_int, C.c_double, C.c_int,
+                                        C.POINTER(C.c_int), C.POINTER(C.c_int), _dp, _dp]),
     ("cacb200_snapshot", C.c_int, [C.c_void_p]),
     ("cacb200_restore", C.c_int, [C.c_void_p]),
     ("cacb200_profile", C.c_int, [C.c_void_p, C.c_int]),
@@ -219,6 +224,24 @@ class Engine:
 
     def run_nve(self, nsteps: int, dt: float = 0.001, eflag: int = 0, vflag: int = 0) -> None:
         self._check(self.lib.cacb200_run_nve(self.h, nsteps, dt, eflag, vflag), "run_nve")
+
+    def fire_params(self, delaystep=20, dtgrow=1.1, dtshrink=0.5, alpha0=0.25, alphashrink=0.99,
+                    tmax=10.0, tmin=0.02, dmax=0.1, halfstepback=True, delaystep_start=True,
+                    max_vdotf_negatif=2000) -> None:
+        self._check(self.lib.cacb200_set_fire_params(self.h, delaystep, dtgrow, dtshrink, alpha0, alphashrink,
+                                                     tmax, tmin, dmax, int(halfstepback), int(delaystep_start),
+                                                     max_vdotf_negatif), "set_fire_params")
+
+    def minimize_fire(self, etol: float = 0.0, ftol: float = 1e-6, maxiter: int = 5000, dt: float = 0.001,
+                      norm: str = "max"):
+        """min_style fire/b200; minimize etol ftol maxiter.  Returns
+        (stop_code, iterations, energy, fnorm)."""
+        ns = {"two": 0, "max": 1, "inf": 2}[norm]
+        code, it = C.c_int(), C.c_int()
+        e, fn = C.c_double(), C.c_double()
+        self._check(self.lib.cacb200_minimize_fire(self.h, etol, ftol, maxiter, dt, ns, C.byref(code),
+                                                   C.byref(it), C.byref(e), C.byref(fn)), "minimize_fire")
+        return code.value, it.value, e.value, fn.value
 
     def snapshot(self) -> None:
         self._check(self.lib.cacb200_snapshot(self.h), "snapshot")

@@ -260,6 +260,51 @@ void run_nve(Ctx &c, int nsteps, double dt, int eflag, int vflag) {
   CACB200_CUDA(cudaGetLastError());
 }
 
+// Minimize::command + Min::setup/run with a FIRE iterate (minimize.cpp:21-70,
+// min.cpp:182-463): nodal_energy_weight 1 for the duration (minimize.cpp:37),
+// lists rebuilt every `every` iterations, energy evaluated every iteration.
+void minimize_fire(Ctx &c, double etol, double ftol, int maxiter, double dt, int normstyle,
+                   int *stop_code, int *niter, double *energy, double *fnorm) {
+  c.check_system();
+  if (maxiter < 0 || !(dt > 0.0) || normstyle < 0 || normstyle > 2)
+    throw Error(CACB200_EINVAL, "invalid minimize arguments");
+  double saved_w = c.nodal_energy_weight;
+  c.nodal_energy_weight = 1.0;
+  c.fire.etol = etol;
+  c.fire.ftol = ftol;
+  c.fire.maxiter = maxiter;
+  c.fire.normstyle = normstyle;
+  try {
+    build(c, false);
+    fire_init(c, dt);
+    forces(c, CACB200_ENERGY_GLOBAL, 0);
+    FireState s{};
+    int done = 0;
+    const int chunk = 25;
+    while (true) {
+      for (int k = 0; k < chunk; k++) {
+        fire_step(c);
+        done++;
+        c.step++;
+        if (c.every > 0 && (c.step - c.last_build_step) % c.every == 0) build(c, false);
+        forces(c, CACB200_ENERGY_GLOBAL, 0);
+      }
+      s = fire_read(c);
+      if (s.status >= 0 || done > maxiter + chunk) break;
+    }
+    if (s.status < 0) s.status = 0;
+    *stop_code = s.status;
+    *niter = s.iter;
+    *energy = s.ecur;
+    *fnorm = s.fnorm;
+  } catch (...) {
+    c.nodal_energy_weight = saved_w;
+    throw;
+  }
+  c.nodal_energy_weight = saved_w;
+  fetch_ev(c);
+}
+
 }  // namespace
 }  // namespace cacb200
 
@@ -508,6 +553,36 @@ int cacb200_setup(cacb200_ctx *ctx) {
 int cacb200_run_nve(cacb200_ctx *ctx, int nsteps, double dt, int eflag, int vflag) {
   API_BEGIN
   run_nve(c, nsteps, dt, eflag, vflag);
+  API_END
+}
+
+int cacb200_set_fire_params(cacb200_ctx *ctx, int delaystep, double dtgrow, double dtshrink, double alpha0,
+                            double alphashrink, double tmax, double tmin, double dmax, int halfstepback,
+                            int delaystep_start, int max_vdotf_negatif) {
+  API_BEGIN
+  if (delaystep < 0 || !(dtgrow >= 1.0) || !(dtshrink > 0.0 && dtshrink <= 1.0) || !(alpha0 >= 0.0) ||
+      !(alphashrink > 0.0 && alphashrink <= 1.0) || !(tmax >= 1.0) || !(tmin > 0.0 && tmin <= 1.0) ||
+      !(dmax > 0.0))
+    throw Error(CACB200_EINVAL, "invalid FIRE parameters");
+  c.fire.delaystep = delaystep;
+  c.fire.dtgrow = dtgrow;
+  c.fire.dtshrink = dtshrink;
+  c.fire.alpha0 = alpha0;
+  c.fire.alphashrink = alphashrink;
+  c.fire.tmax = tmax;
+  c.fire.tmin = tmin;
+  c.fire.dmax = dmax;
+  c.fire.halfstepback = halfstepback ? 1 : 0;
+  c.fire.delaystep_start = delaystep_start ? 1 : 0;
+  c.fire.max_vdotf_negatif = max_vdotf_negatif;
+  API_END
+}
+
+int cacb200_minimize_fire(cacb200_ctx *ctx, double etol, double ftol, int maxiter, double dt, int normstyle,
+                          int *stop_code, int *niter, double *energy, double *fnorm) {
+  API_BEGIN
+  if (!stop_code || !niter || !energy || !fnorm) throw Error(CACB200_EINVAL, "null output");
+  minimize_fire(c, etol, ftol, maxiter, dt, normstyle, stop_code, niter, energy, fnorm);
   API_END
 }
 

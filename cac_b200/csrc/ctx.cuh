@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <functional>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -81,6 +82,24 @@ struct PairParams {
   // EAM
   int nrho = 0, nr = 0;
   double drho = 0, dr = 0, rdr = 0, rdrho = 0, rhomax = 0;
+};
+
+// FIRE parameters (Min defaults, min.cpp:33-47) and run settings
+struct FireParams {
+  int delaystep = 20;
+  double dtgrow = 1.1, dtshrink = 0.5, alpha0 = 0.25, alphashrink = 0.99;
+  double tmax = 10.0, tmin = 0.02, dmax = 0.1;
+  int halfstepback = 1, delaystep_start = 1, max_vdotf_negatif = 2000;
+  double etol = 0.0, ftol = 0.0;
+  int maxiter = 1000, normstyle = 0;  // 0 two-norm squared, 1 max per-site |f|^2, 2 inf (max component)^2
+  double dtmax = 0.0, dtmin = 0.0, mass = 1.0;
+};
+
+// FIRE iteration state, kept in device memory and advanced by the control kernel
+struct FireState {
+  double dt, alpha, dtv, halfback, s1, s2, vdotf, ecur, eprev, fnorm;
+  long long step, last_negative, start;
+  int vdotf_neg, reset, mix, apply, status, iter;
 };
 
 struct Profile {
@@ -161,6 +180,15 @@ struct Ctx {
 
   PairParams pp;
   DBuf<double4> rhor_val, rhor_der, z2r_val, z2r_der, frho_val, frho_der;
+  // mixed precision: FP32 tables, per-site FP32 offsets and packed anchor cells
+  DBuf<float4> rhor_val32, rhor_der32, z2r_val32, z2r_der32, frho_val32, frho_der32;
+  bool have_mixed_tables = false;
+  DBuf<float4> pos32;
+  DBuf<unsigned> anc32;
+
+  FireParams fire;
+  DBuf<FireState> fire_state;
+  DBuf<double> fire_partial;
 
   Profile prof;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -195,10 +223,14 @@ void neigh_download(Ctx &c, bool half, int64_t *offset, int8_t *kind, int32_t *i
                     int8_t *img, int64_t *nentries);
 void interpolate_sites(Ctx &c);
 void pair_compute(Ctx &c, int eflag, int vflag);
+void pair_compute_mixed(Ctx &c, int eflag, int vflag);
 void assemble_nodef(Ctx &c);
 void nve_initial(Ctx &c, double dt);
 void nve_final(Ctx &c, double dt);
 void pbc_wrap(Ctx &c);
 void eam_tables(Ctx &c, const double *frho, const double *rhor, const double *z2r);
+void fire_init(Ctx &c, double dt);
+void fire_step(Ctx &c);
+FireState fire_read(Ctx &c);
 
 }  // namespace cacb200

@@ -486,7 +486,7 @@ __device__ __forceinline__ void finish_counts(const BuildArgs &A, int i, int nf,
 // Atoms: one block per cell of the atom grid (cell >= cutneigh); the lanes
 // are the cell's atoms and walk the 27 surrounding cells together, so every
 // candidate position is one broadcast load shared by the whole warp.
-__global__ void __launch_bounds__(64) k_build_atoms(BuildArgs A) {
+__global__ void __launch_bounds__(32) k_build_atoms(BuildArgs A) {
   const int home = blockIdx.x;
   const int hbeg = A.acell_start[home], hend = A.acell_start[home + 1];
   if (hbeg == hend) return;
@@ -770,15 +770,19 @@ void neigh_build(Ctx &c, bool want_half) {
     A.num_half = want_half ? c.num_half.p : nullptr;
     A.img_half = want_half ? c.img_half.p : nullptr;
     A.overflow = c.overflow.p;
-    {
-      KernelTimer t(c, "build_list");
-      if (c.na) k_build_atoms<<<c.agrid.ncell, 64, 0, c.stream>>>(A);
-      if (c.ne) k_build_gauss<<<nblk(NG * c.ne, 128), 128, 0, c.stream>>>(A);
+    if (c.na) {
+      KernelTimer t(c, "build_atoms");
+      k_build_atoms<<<c.agrid.ncell, 32, 0, c.stream>>>(A);
     }
-    int ov[4];
+    if (c.ne) {
+      KernelTimer t(c, "build_gauss");
+      k_build_gauss<<<nblk(NG * c.ne, 128), 128, 0, c.stream>>>(A);
+    }
+    int ov[8];
     CACB200_CUDA(cudaMemcpyAsync(ov, c.overflow.p, sizeof(ov), cudaMemcpyDeviceToHost, c.stream));
     CACB200_CUDA(cudaStreamSynchronize(c.stream));
     if (ov[2]) throw Error(CACB200_EINVAL, "neighbour image beyond the first periodic image (box too small)");
+    if (ov[6]) throw Error(CACB200_EUNSTABLE, "a site moved more than 8 cells outside the box (unstable run)");
     if (!ov[0]) break;
     c.cap = ((ov[1] + 31) / 32) * 32;
     if (attempt == 2) throw Error(CACB200_EOVERFLOW, "neighbour list capacity");

@@ -121,13 +121,29 @@ __device__ __forceinline__ void finish_site(const PairArgs &A, int i, bool valid
   if (A.eflag || A.vflag) block_reduce_store<7>(red, A.partial);
 }
 
+// Force only (no energy or virial requested): one write per site.
+__device__ __forceinline__ void finish_force(const PairArgs &A, int i, bool valid, const double fi[3]) {
+  if (!valid) return;
+  double *fo;
+  if (i < A.na) {
+    fo = A.f + 3 * (size_t)i;
+  } else {
+    int e = (i - A.na) / NG, g = (i - A.na) % NG;
+    fo = A.gaussf + (size_t)e * 24 + 3 * g;
+  }
+  fo[0] = fi[0];
+  fo[1] = fi[1];
+  fo[2] = fi[2];
+}
+
 // ------------------------------------------------------------------- LJ
 
 struct LjParams {
   double cutsq, lj1, lj2, lj3, lj4, offset;
 };
 
-__global__ void __launch_bounds__(128) k_lj(PairArgs A, LjParams P) {
+template <bool EV>
+__global__ void __launch_bounds__(128, EV ? 4 : 8) k_lj(PairArgs A, LjParams P) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   bool valid = i < A.nsi;
   double fi[3] = {0, 0, 0}, esum = 0.0, vsum[6] = {0, 0, 0, 0, 0, 0};
@@ -146,8 +162,8 @@ __global__ void __launch_bounds__(128) k_lj(PairArgs A, LjParams P) {
         fi[0] += dx * fpair;
         fi[1] += dy * fpair;
         fi[2] += dz * fpair;
-        if (A.eflag) esum += r6inv * (P.lj3 * r6inv - P.lj4) - P.offset;
-        if (A.vflag) {
+        if (EV && A.eflag) esum += r6inv * (P.lj3 * r6inv - P.lj4) - P.offset;
+        if (EV && A.vflag) {
           vsum[0] += dx * dx * fpair;
           vsum[1] += dy * dy * fpair;
           vsum[2] += dz * dz * fpair;
@@ -159,7 +175,8 @@ __global__ void __launch_bounds__(128) k_lj(PairArgs A, LjParams P) {
     };
     for_each_neighbour(A, nb, n, pair);
   }
-  finish_site(A, i, valid, fi, esum, vsum, 0.0, 0.0);
+  if (EV) finish_site(A, i, valid, fi, esum, vsum, 0.0, 0.0);
+  else finish_force(A, i, valid, fi);
 }
 
 // ------------------------------------------------------------------ EAM
@@ -193,7 +210,7 @@ __device__ __forceinline__ double eam_fp(const EamTables &T, double rho, double 
 // pass 1: density at atoms and node Gauss points (pair_eam.cpp:707-812), then
 // F' at the site itself into xs[i].w (pair_eam.cpp:819-833 for atoms; for a
 // node the reference's rhoi = noderho at :901-903).
-__global__ void __launch_bounds__(128) k_eam_rho(PairArgs A, EamTables T, double *rho_out,
+__global__ void __launch_bounds__(128, 8) k_eam_rho(PairArgs A, EamTables T, double *rho_out,
                                                  double *phi_site) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= A.nsi) return;
@@ -243,7 +260,8 @@ __global__ void k_eam_site_fp(double4 *xs, const int *act_gid, int nact, int bas
 }
 
 // pass 2: forces (pair_eam.cpp:845-1028)
-__global__ void __launch_bounds__(128) k_eam_force(PairArgs A, EamTables T, const double *phi_site) {
+template <bool EV>
+__global__ void __launch_bounds__(128, EV ? 4 : 8) k_eam_force(PairArgs A, EamTables T, const double *phi_site) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   bool valid = i < A.nsi;
   double fi[3] = {0, 0, 0}, esum = 0.0, vsum[6] = {0, 0, 0, 0, 0, 0};
@@ -277,8 +295,8 @@ __global__ void __launch_bounds__(128) k_eam_force(PairArgs A, EamTables T, cons
         fi[0] += dx * fpair;
         fi[1] += dy * fpair;
         fi[2] += dz * fpair;
-        if (A.eflag) esum += phi;
-        if (A.vflag) {
+        if (EV && A.eflag) esum += phi;
+        if (EV && A.vflag) {
           vsum[0] += dx * dx * fpair;
           vsum[1] += dy * dy * fpair;
           vsum[2] += dz * dz * fpair;
@@ -289,13 +307,14 @@ __global__ void __launch_bounds__(128) k_eam_force(PairArgs A, EamTables T, cons
       }
     };
     for_each_neighbour(A, nb, n, pair);
-    if (A.eflag) {
+    if (EV && A.eflag) {
       double phi = phi_site[i];
       eemb_site = phi;
       eemb_global = (i < A.na) ? phi : phi * A.escale_node * 2.0;
     }
   }
-  finish_site(A, i, valid, fi, esum, vsum, eemb_site, eemb_global);
+  if (EV) finish_site(A, i, valid, fi, esum, vsum, eemb_site, eemb_global);
+  else finish_force(A, i, valid, fi);
 }
 
 __global__ void k_reduce_partials(const double *partial, int nblocks, double *out) {
@@ -357,6 +376,7 @@ void eam_tables(Ctx &c, const double *frho, const double *rhor, const double *z2
     b[m] = rhor[m - 1];
     z[m] = z2r[m - 1];
   }
+  c.have_mixed_tables = false;
   spline7(p.nrho, p.drho, a, sp);
   upload_split(c, sp, p.nrho, c.frho_val, c.frho_der);
   spline7(p.nr, p.dr, b, sp);
@@ -368,6 +388,10 @@ void eam_tables(Ctx &c, const double *frho, const double *rhor, const double *z2
 void pair_compute(Ctx &c, int eflag, int vflag) {
   c.check_system();
   if (!c.lists_valid) throw Error(CACB200_ESTATE, "neighbour lists not built");
+  if (c.precision == CACB200_MIXED) {
+    pair_compute_mixed(c, eflag, vflag);
+    return;
+  }
   const int nsi = c.nsite_i();
   const int T = 128;
   const int nb = std::max(nblk(nsi, T), 1);
@@ -407,7 +431,8 @@ void pair_compute(Ctx &c, int eflag, int vflag) {
   if (c.pp.style == CACB200_PAIR_LJ) {
     LjParams P{c.pp.cut * c.pp.cut, c.pp.lj1, c.pp.lj2, c.pp.lj3, c.pp.lj4, c.pp.offset};
     KernelTimer t(c, "pair_lj");
-    k_lj<<<nb, T, 0, c.stream>>>(A, P);
+    if (eflag || vflag) k_lj<true><<<nb, T, 0, c.stream>>>(A, P);
+    else k_lj<false><<<nb, T, 0, c.stream>>>(A, P);
   } else if (c.pp.style == CACB200_PAIR_EAM) {
     EamTables Tb;
     Tb.rhor_val = c.rhor_val.p;
@@ -435,7 +460,8 @@ void pair_compute(Ctx &c, int eflag, int vflag) {
     }
     {
       KernelTimer t(c, "eam_force");
-      k_eam_force<<<nb, T, 0, c.stream>>>(A, Tb, c.phi_site.p);
+      if (eflag || vflag) k_eam_force<true><<<nb, T, 0, c.stream>>>(A, Tb, c.phi_site.p);
+      else k_eam_force<false><<<nb, T, 0, c.stream>>>(A, Tb, c.phi_site.p);
     }
   } else {
     throw Error(CACB200_ESTATE, "no pair style set");

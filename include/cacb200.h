@@ -141,6 +141,26 @@ int cacb200_nve_final(cacb200_ctx *ctx, double dt);
 int cacb200_setup(cacb200_ctx *ctx);
 int cacb200_run_nve(cacb200_ctx *ctx, int nsteps, double dt, int eflag, int vflag);
 
+/* ------------------------------------------------------------- minimise */
+
+/* min_modify for FIRE: the parameters of Min (min.h:61-72) with the
+ * reference's defaults (min.cpp:33-47): delaystep 20, dtgrow 1.1,
+ * dtshrink 0.5, alpha0 0.25, alphashrink 0.99, tmax 10, tmin 0.02, dmax 0.1,
+ * halfstepback 1, delaystep_start 1, max_vdotf_negatif 2000. */
+int cacb200_set_fire_params(cacb200_ctx *ctx, int delaystep, double dtgrow, double dtshrink,
+                            double alpha0, double alphashrink, double tmax, double tmin,
+                            double dmax, int halfstepback, int delaystep_start,
+                            int max_vdotf_negatif);
+/* minimize etol ftol maxiter with min_style fire/b200 (Minimize::command,
+ * minimize.cpp:21-70; the reference itself has no FIRE: this is FIRE 2.0 of
+ * Guenole et al. 2020 over atoms + nodes).  normstyle: 0 two-norm, 1 max
+ * per-site norm, 2 inf norm (min_modify norm two|max|inf).  Returns the stop
+ * code of min.h:46-47 (0 MAXITER, 2 ETOL, 3 FTOL, 11 MAXVDOTF), iterations,
+ * final energy and force norm (squared, in the chosen style). */
+int cacb200_minimize_fire(cacb200_ctx *ctx, double etol, double ftol, int maxiter, double dt,
+                          int normstyle, int *stop_code, int *niter, double *energy,
+                          double *fnorm);
+
 /* Device-side copy of the state (x, v, nodex, nodev) and its restoration;
  * restoring invalidates the lists (call cacb200_setup before stepping).
  * Serves restarts of short trajectories and job preemption without host

@@ -92,6 +92,8 @@ void oracle_inverse_mass_hex(double *minv)
 static double g_shape[NU * 8];
 static int g_g2u[NG], g_g2n[NG], g_n2g[NPE], g_u2g[NU];
 static double g_wsa[NG * 8], g_nodal_weight, g_minv[64];
+/* Pair::nodal_energy_weight (pair.cpp:38); minimize sets it to 1 (minimize.cpp:37) */
+static double g_nodal_energy_weight = -1.0;
 static int g_tables_ready = 0;
 
 static void tables(void)
@@ -808,6 +810,7 @@ int oracle_eam_compute(oracle_state *s, const oracle_list *L, const oracle_eam *
       if (ev && ev->vnode) iv = ev->vnode + 48 * (size_t) e + 6 * node;
       const double *coeff;
       double p;
+      if (g_nodal_energy_weight >= 0.0) iescale = g_nodal_energy_weight / 2.0;
       fpi = compute_fp(eam, rhoi, &coeff, &p);
       double phi = ((coeff[3] * p + coeff[4]) * p + coeff[5]) * p + coeff[6];
       if (rhoi > eam->rhomax) phi += fpi * (rhoi - eam->rhomax);
@@ -837,7 +840,7 @@ int oracle_eam_compute(oracle_state *s, const oracle_list *L, const oracle_eam *
         if (g_u2g[site] >= 0) {
           int jg = g_u2g[site], jn = g_g2n[jg];
           fj = s->gaussf + (size_t) j * 24 + 3 * jg;
-          jescale = g_nodal_weight / 2.0;
+          jescale = g_nodal_energy_weight >= 0.0 ? g_nodal_energy_weight / 2.0 : g_nodal_weight / 2.0;
           if (ev && ev->enode) je = ev->enode + 8 * (size_t) j + jn;
           if (ev && ev->vnode) jv = ev->vnode + 48 * (size_t) j + 6 * jn;
         }
@@ -978,5 +981,150 @@ int oracle_run_nve(oracle_state *s, int pair, double p0, double p1, double p2,
   }
 #undef FORCE
   oracle_free_list(&L);
+  return 0;
+}
+
+
+/* ------------------------------------------------------------------ FIRE */
+
+/* FIRE 2.0 (Guenole et al., Comput. Mater. Sci. 175, 109584 (2020),
+ * Algorithm 2, semi-implicit Euler) over atoms then nodes, with the
+ * parameters of the reference's Min (min.h:61-72, defaults min.cpp:33-47) and
+ * its stopping tests; the reference has no FIRE iterate of its own.
+ * par: delaystep dtgrow dtshrink alpha0 alphashrink tmax tmin dmax halfstepback
+ *      delaystep_start max_vdotf_negatif. */
+static double fire_energy(oracle_state *s, const oracle_list *L, int pair, double p0, double p1,
+                          double p2, const oracle_eam *eam)
+{
+  oracle_ev ev;
+  memset(&ev, 0, sizeof ev);
+  if (pair == 0) oracle_lj_compute(s, L, p0, p1, p2, &ev);
+  else oracle_eam_compute(s, L, eam, &ev, NULL, NULL);
+  oracle_compute_nodef(s);
+  return ev.energy;
+}
+
+int oracle_minimize_fire(oracle_state *s, int pair, double p0, double p1, double p2,
+                         const oracle_eam *eam, double skin, double dt0, double etol, double ftol,
+                         int maxiter, int normstyle, int every, const double *par, int *code,
+                         int *niter, double *energy, double *fnorm)
+{
+  const double FTM2V = 1.0 / 1.0364269e-4, EPS_ENERGY = 1.0e-8;
+  int delaystep = (int) par[0];
+  double dtgrow = par[1], dtshrink = par[2], alpha0 = par[3], alphashrink = par[4];
+  double dtmax = par[5] * dt0, dtmin = par[6] * dt0, dmax = par[7];
+  int halfstepback = (int) par[8], delaystep_start = (int) par[9], max_vdotf_negatif = (int) par[10];
+  double cut = pair == 0 ? p2 : eam->cut;
+  double cutneigh = sqrt(cut * cut) + skin;
+  double saved_w = g_nodal_energy_weight;
+  g_nodal_energy_weight = 1.0;
+  oracle_list L;
+  oracle_pbc(s);
+  if (oracle_build_list(s, cutneigh, 1, &L)) return -1;
+  size_t na3 = 3 * (size_t) s->natoms, nn3 = 24 * (size_t) s->nelements;
+  memset(s->v, 0, sizeof(double) * na3);
+  memset(s->nodev, 0, sizeof(double) * nn3);
+  double ecur = fire_energy(s, &L, pair, p0, p1, p2, eam), eprev = ecur;
+  double dt = dt0, alpha = alpha0, dtv = dt0;
+  long long step = 0, last_negative = 0, start = 0, last_build = 0;
+  int vdotf_neg = 0, iter = 0, status = -1;
+  double fn = 0.0;
+  while (1) {
+    /* reductions over atoms then nodes */
+    double vdotf = 0, vdotv = 0, fdotf = 0, vmax = 0, fmaxd = 0, fmax2 = 0;
+    for (int pass = 0; pass < 2; pass++) {
+      size_t n = pass ? nn3 : na3;
+      const double *v = pass ? s->nodev : s->v, *f = pass ? s->nodef : s->f;
+      for (size_t k = 0; k < n; k += 3) {
+        double f2 = 0.0;
+        for (int d = 0; d < 3; d++) {
+          vdotf += v[k + d] * f[k + d];
+          vdotv += v[k + d] * v[k + d];
+          fdotf += f[k + d] * f[k + d];
+          if (fabs(v[k + d]) > vmax) vmax = fabs(v[k + d]);
+          if (fabs(f[k + d]) > fmaxd) fmaxd = fabs(f[k + d]);
+          f2 += f[k + d] * f[k + d];
+        }
+        if (f2 > fmax2) fmax2 = f2;
+      }
+    }
+    fn = normstyle == 1 ? fmax2 : (normstyle == 2 ? fmaxd * fmaxd : fdotf);
+    if (iter > 0) {
+      if (etol > 0.0 && step - last_negative > delaystep &&
+          fabs(ecur - eprev) < etol * 0.5 * (fabs(ecur) + fabs(eprev) + EPS_ENERGY)) {
+        status = 2;
+        break;
+      }
+      if (ftol > 0.0 && fn < ftol * ftol) {
+        status = 3;
+        break;
+      }
+    }
+    if (iter >= maxiter) {
+      status = 0;
+      break;
+    }
+    iter++;
+    step++;
+    int reset = 0;
+    if (vdotf > 0.0) {
+      vdotf_neg = 0;
+      if (step - last_negative > delaystep) {
+        dt = dt * dtgrow < dtmax ? dt * dtgrow : dtmax;
+        alpha *= alphashrink;
+      }
+    } else {
+      last_negative = step;
+      int delayed = !(delaystep_start && step - start < delaystep);
+      if (delayed) {
+        alpha = alpha0;
+        if (dt * dtshrink >= dtmin) dt *= dtshrink;
+      }
+      vdotf_neg++;
+      if (max_vdotf_negatif > 0 && vdotf_neg > max_vdotf_negatif) {
+        status = 11;
+        break;
+      }
+      reset = 1;
+    }
+    double vest = reset ? dt * FTM2V / s->mass * fmaxd : vmax;
+    double dtnew = dt;
+    if (dtnew * vest > dmax && vest > 0.0) dtnew = dmax / vest;
+    double hb = (reset && halfstepback) ? 0.5 * dtv : 0.0;
+    dtv = dtnew;
+    int mix = vdotf > 0.0;
+    double s1 = 1.0 - alpha, s2 = fdotf <= 1e-20 ? 0.0 : alpha * sqrt(vdotv / fdotf);
+    double dtfm = dtv * FTM2V / s->mass;
+    for (int pass = 0; pass < 2; pass++) {
+      size_t n = pass ? nn3 : na3;
+      double *x = pass ? s->nodex : s->x, *v = pass ? s->nodev : s->v;
+      const double *f = pass ? s->nodef : s->f;
+      for (size_t k = 0; k < n; k++) {
+        double vd = v[k];
+        if (reset) {
+          x[k] -= hb * vd;
+          vd = 0.0;
+        }
+        vd += dtfm * f[k];
+        if (mix) vd = s1 * vd + s2 * f[k];
+        x[k] += dtv * vd;
+        v[k] = vd;
+      }
+    }
+    if (every > 0 && (step - last_build) % every == 0) {
+      oracle_free_list(&L);
+      oracle_pbc(s);
+      if (oracle_build_list(s, cutneigh, 1, &L)) return -1;
+      last_build = step;
+    }
+    eprev = ecur;
+    ecur = fire_energy(s, &L, pair, p0, p1, p2, eam);
+  }
+  oracle_free_list(&L);
+  g_nodal_energy_weight = saved_w;
+  *code = status;
+  *niter = iter;
+  *energy = ecur;
+  *fnorm = fn;
   return 0;
 }

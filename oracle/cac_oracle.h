@@ -92,6 +92,12 @@ void oracle_pbc(oracle_state *s);
 int oracle_run_nve(oracle_state *s, int pair, double p0, double p1, double p2,
                    const oracle_eam *eam, double skin, double dt, int nsteps, int every);
 
+/* FIRE minimisation (see cac_oracle.c); par holds the 11 Min parameters */
+int oracle_minimize_fire(oracle_state *s, int pair, double p0, double p1, double p2,
+                         const oracle_eam *eam, double skin, double dt0, double etol, double ftol,
+                         int maxiter, int normstyle, int every, const double *par, int *code,
+                         int *niter, double *energy, double *fnorm);
+
 #ifdef __cplusplus
 }
 #endif
