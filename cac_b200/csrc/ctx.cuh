@@ -159,6 +159,7 @@ struct Ctx {
   DBuf<int> acell_start;         // [ncell+1]
   DBuf<int> acell_atoms;         // [na] atom ids sorted by cell
   DBuf<double4> acell_pos;       // [na] wrapped positions sorted by cell, w = bitcast(id)
+  DBuf<float4> acell_pos32;      // [na] the same as floats, w = bitcast(int id)
   DBuf<int> ecell_start, ecell_elems;
   DBuf<int> cell_key, cell_key2, idx_tmp, idx_tmp2;
   DBuf<unsigned char> cub_tmp;

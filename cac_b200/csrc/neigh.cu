@@ -71,9 +71,10 @@ __global__ void k_pbc_atoms(double4 *xs, int na, BoxD b) {
 // search: affine frame n0 + i a + j b + k c of the lattice sites, its inverse,
 // the largest deviation of the trilinear nodes from that frame, and the
 // centre-to-node radius.
-//   eframe[e*16 + 0..2]  n0
-//   eframe[e*16 + 3..11] rows of the inverse frame matrix
-//   eframe[e*16 + 12]    dmax
+//   eframe[e*24 + 0..2]   n0
+//   eframe[e*24 + 3..11]  rows of the inverse frame matrix
+//   eframe[e*24 + 12]     dmax
+//   eframe[e*24 + 13..21] frame vectors a, b, c (one lattice step each)
 __global__ void k_elem_geom(double *nodex, int ne, BoxD b, double4 *ecenter, double *eframe,
                             unsigned long long *reach_bits) {
   int e = blockIdx.x * blockDim.x + threadIdx.x;
@@ -146,7 +147,7 @@ __global__ void k_elem_geom(double *nodex, int ne, BoxD b, double4 *ecenter, dou
     inv[2][0] = (A[1][0] * A[2][1] - A[1][1] * A[2][0]) * id;
     inv[2][1] = (A[0][1] * A[2][0] - A[0][0] * A[2][1]) * id;
     inv[2][2] = (A[0][0] * A[1][1] - A[0][1] * A[1][0]) * id;
-    double *fr = eframe + (size_t)e * 16;
+    double *fr = eframe + (size_t)e * 24;
     fr[0] = n0[0];
     fr[1] = n0[1];
     fr[2] = n0[2];
@@ -155,6 +156,10 @@ __global__ void k_elem_geom(double *nodex, int ne, BoxD b, double4 *ecenter, dou
 #pragma unroll
       for (int q = 0; q < 3; q++) fr[3 + 3 * r + q] = inv[r][q];
     fr[12] = dmax;
+#pragma unroll
+    for (int q = 0; q < 3; q++)
+#pragma unroll
+      for (int d = 0; d < 3; d++) fr[13 + 3 * q + d] = A[d][q];
     ecenter[e] = make_double4(c[0], c[1], c[2], R);
     reach = R + dmax;
   }
@@ -207,11 +212,12 @@ __global__ void k_cell_start(const int *skey, int n, int ncell, int *start) {
   start[c] = lo;
 }
 
-__global__ void k_gather_pos(const double4 *xs, const int *sidx, int n, double4 *out) {
+__global__ void k_gather_pos(const double4 *xs, const int *sidx, int n, double4 *out, float4 *out32) {
   int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= n) return;
   int i = sidx[k];
   double4 p = xs[i];
+  out32[k] = make_float4((float)p.x, (float)p.y, (float)p.z, __int_as_float(i));
   p.w = __longlong_as_double((long long)i);
   out[k] = p;
 }
@@ -225,6 +231,7 @@ struct BuildArgs {
   const double *eframe;
   const int *acell_start;
   const double4 *acell_pos;
+  const float4 *acell_pos32;  // wrapped positions as floats, w = atom index bits
   const int *ecell_start;
   const int *ecell_elems;
   int na, ne, nsi, cap;
@@ -401,7 +408,7 @@ __device__ void element_candidates(const BuildArgs &A, const Query &q, int &nf, 
           double4 ce = A.ecenter[e];
           // sphere test in the element's raw frame: |xi - s L - centre| <= cutneigh + R
           double p[3] = {q.xi[0] - sL[0], q.xi[1] - sL[1], q.xi[2] - sL[2]};
-          const double *fr = A.eframe + (size_t)e * 16;
+          const double *fr = A.eframe + (size_t)e * 24;
           double dmax = fr[12];
           double R = ce.w + dmax + A.cutneigh + 1e-6;
           double dcx = p[0] - ce.x, dcy = p[1] - ce.y, dcz = p[2] - ce.z;
@@ -438,9 +445,22 @@ __device__ void element_candidates(const BuildArgs &A, const Query &q, int &nf, 
             qcen[1] = s[1] ? __dadd_rn(ce.y, sL[1]) : ce.y;
             qcen[2] = s[2] ? __dadd_rn(ce.z, sL[2]) : ce.z;
           }
+          // affine position of site (a, bb, cc) relative to the query, in FP32:
+          // a cheap superset test (radius cutneigh + dmax + margin) before the
+          // exact FP64 distance
+          const float fa0 = (float)fr[13], fa1 = (float)fr[14], fa2 = (float)fr[15];
+          const float fb0 = (float)fr[16], fb1 = (float)fr[17], fb2 = (float)fr[18];
+          const float fc0 = (float)fr[19], fc1 = (float)fr[20], fc2 = (float)fr[21];
+          const float r0 = (float)rel[0], r1 = (float)rel[1], r2 = (float)rel[2];
+          const float lim = (float)(A.cutneigh + dmax) + 1e-3f;
+          const float lim2 = lim * lim;
           for (int a = lo[0]; a <= hi[0]; a++)
             for (int bb = lo[1]; bb <= hi[1]; bb++)
               for (int cc = lo[2]; cc <= hi[2]; cc++) {
+                float ex = r0 - (a * fa0 + bb * fb0 + cc * fc0);
+                float ey = r1 - (a * fa1 + bb * fb1 + cc * fc1);
+                float ez = r2 - (a * fa2 + bb * fb2 + cc * fc2);
+                if (ex * ex + ey * ey + ez * ez > lim2) continue;
                 int u = (a * NC + bb) * NC + cc;
                 if (!q.iatom && e == q.ie && u == q.iu && zero) continue;
                 double dx = q.xi[0], dy = q.xi[1], dz = q.xi[2];
@@ -483,22 +503,32 @@ __device__ __forceinline__ void finish_counts(const BuildArgs &A, int i, int nf,
   }
 }
 
-// Atoms: one block per cell of the atom grid (cell >= cutneigh); the lanes
-// are the cell's atoms and walk the 27 surrounding cells together, so every
-// candidate position is one broadcast load shared by the whole warp.
+// Atoms, atom neighbours: one block (one warp) per cell of the atom grid
+// (cell >= cutneigh); the lanes are the cell's atoms and walk the 27
+// surrounding cells together, so every candidate is one broadcast load shared
+// by the warp.  A conservative FP32 distance test (from a float copy of the
+// wrapped positions) screens candidates before the exact FP64 test.
 __global__ void __launch_bounds__(32) k_build_atoms(BuildArgs A) {
   const int home = blockIdx.x;
   const int hbeg = A.acell_start[home], hend = A.acell_start[home + 1];
   if (hbeg == hend) return;
   const int nc0 = A.ag.nc[0], nc1 = A.ag.nc[1], nc2 = A.ag.nc[2];
   const int hx = home % nc0, hy = (home / nc0) % nc1, hz = home / (nc0 * nc1);
-  const double pre = (A.cutneigh + 1e-6) * (A.cutneigh + 1e-6);
+  const float pre = (float)(A.cutneigh + 1e-3);
+  const float pre2 = pre * pre;
   for (int base = hbeg; base < hend; base += blockDim.x) {
     const int h = base + threadIdx.x;
     const bool active = h < hend;
     Query q;
     int nf = 0, nh = 0;
-    if (active) make_query(A, (int)__double_as_longlong(A.acell_pos[h].w), q);
+    float wx = 0.f, wy = 0.f, wz = 0.f;
+    if (active) {
+      make_query(A, (int)__double_as_longlong(A.acell_pos[h].w), q);
+      float4 w = A.acell_pos32[h];
+      wx = w.x;
+      wy = w.y;
+      wz = w.z;
+    }
     for (int oz = -1; oz <= 1; oz++) {
       int cz, Wz;
       wrap_cell(hz + oz, nc2, cz, Wz);
@@ -510,23 +540,35 @@ __global__ void __launch_bounds__(32) k_build_atoms(BuildArgs A) {
           wrap_cell(hx + ox, nc0, cx, Wx);
           int cell = (cz * nc1 + cy) * nc0 + cx;
           int W[3] = {Wx, Wy, Wz};
-          double sh[3] = {Wx * A.b.L[0], Wy * A.b.L[1], Wz * A.b.L[2]};
+          const float sx = (float)(Wx * A.b.L[0]), sy = (float)(Wy * A.b.L[1]), sz = (float)(Wz * A.b.L[2]);
           int beg = A.acell_start[cell], end = A.acell_start[cell + 1];
           for (int k = beg; k < end; k++) {
-            double4 pj = A.acell_pos[k];
+            float4 pj = A.acell_pos32[k];
             if (!active) continue;
-            double ex = q.wi[0] - (pj.x + sh[0]), ey = q.wi[1] - (pj.y + sh[1]), ez = q.wi[2] - (pj.z + sh[2]);
-            if (ex * ex + ey * ey + ez * ez > pre) continue;
-            try_atom(A, q, (int)__double_as_longlong(pj.w), W, nf, nh);
+            float ex = wx - (pj.x + sx), ey = wy - (pj.y + sy), ez = wz - (pj.z + sz);
+            if (ex * ex + ey * ey + ez * ez > pre2) continue;
+            try_atom(A, q, __float_as_int(pj.w), W, nf, nh);
           }
         }
       }
     }
     if (active) {
-      if (A.ne > 0) element_candidates(A, q, nf, nh);
-      finish_counts(A, q.i, nf, nh);
+      A.num_full[q.i] = nf;
+      if (A.want_half) A.num_half[q.i] = nh;
     }
   }
+}
+
+// Atoms, element lattice sites: appended after the atom neighbours.  Atoms
+// whose 27 element cells hold no element leave at once.
+__global__ void __launch_bounds__(128) k_build_atom_sites(BuildArgs A) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= A.na) return;
+  Query q;
+  make_query(A, i, q);
+  int nf = A.num_full[i], nh = A.want_half ? A.num_half[i] : 0;
+  if (A.ne > 0) element_candidates(A, q, nf, nh);
+  finish_counts(A, i, nf, nh);
 }
 
 // Gauss points: one thread each; atoms from the 27 surrounding atom cells
@@ -681,7 +723,7 @@ void neigh_build(Ctx &c, bool want_half) {
     KernelTimer t(c, "pbc_geom");
     if (c.na) k_pbc_atoms<<<nblk(c.na, 256), 256, 0, c.stream>>>(c.xs.p, c.na, b);
     c.ecenter.reserve(std::max(c.ne, 1));
-    c.eframe.reserve((size_t)std::max(c.ne, 1) * 16);
+    c.eframe.reserve((size_t)std::max(c.ne, 1) * 24);
     c.overflow.reserve(8);
     CACB200_CUDA(cudaMemsetAsync(c.overflow.p, 0, 8 * sizeof(int), c.stream));
     if (c.ne)
@@ -708,6 +750,7 @@ void neigh_build(Ctx &c, bool want_half) {
     c.idx_tmp2.reserve(nmax);
     c.acell_start.reserve(c.agrid.ncell + 1);
     c.acell_pos.reserve(std::max(c.na, 1));
+    c.acell_pos32.reserve(std::max(c.na, 1));
     c.ecell_start.reserve(c.egrid.ncell + 1);
     c.ecell_elems.reserve(std::max(c.ne, 1));
     if (c.na) {
@@ -716,7 +759,8 @@ void neigh_build(Ctx &c, bool want_half) {
       sort_pairs<int>(c, c.cell_key.p, c.cell_key2.p, c.idx_tmp.p, c.idx_tmp2.p, c.na, c.agrid.ncell);
       k_cell_start<<<nblk(c.agrid.ncell + 1, 256), 256, 0, c.stream>>>(c.cell_key2.p, c.na, c.agrid.ncell,
                                                               c.acell_start.p);
-      k_gather_pos<<<nblk(c.na, 256), 256, 0, c.stream>>>(c.xs.p, c.idx_tmp2.p, c.na, c.acell_pos.p);
+      k_gather_pos<<<nblk(c.na, 256), 256, 0, c.stream>>>(c.xs.p, c.idx_tmp2.p, c.na, c.acell_pos.p,
+                                                          c.acell_pos32.p);
     } else {
       CACB200_CUDA(cudaMemsetAsync(c.acell_start.p, 0, sizeof(int) * (c.agrid.ncell + 1), c.stream));
     }
@@ -750,6 +794,7 @@ void neigh_build(Ctx &c, bool want_half) {
     A.eframe = c.eframe.p;
     A.acell_start = c.acell_start.p;
     A.acell_pos = c.acell_pos.p;
+    A.acell_pos32 = c.acell_pos32.p;
     A.ecell_start = c.ecell_start.p;
     A.ecell_elems = c.ecell_elems.p;
     A.na = c.na;
@@ -773,6 +818,10 @@ void neigh_build(Ctx &c, bool want_half) {
     if (c.na) {
       KernelTimer t(c, "build_atoms");
       k_build_atoms<<<c.agrid.ncell, 32, 0, c.stream>>>(A);
+    }
+    if (c.na) {
+      KernelTimer t(c, "build_atom_sites");
+      k_build_atom_sites<<<nblk(c.na, 128), 128, 0, c.stream>>>(A);
     }
     if (c.ne) {
       KernelTimer t(c, "build_gauss");
