@@ -204,9 +204,9 @@ def alg_bytes_per_site(kernel: str) -> int:
         "eam_force": 24 + 8 + 24,     # read x, F'; write f
         "eam_rho": 24 + 8,            # read x; write rho
         "pair_lj": 24 + 24,           # read x; write f
-        "eam_force32": 16 + 4 + 24,   # read FP32 offset + F', anchor; write f (FP64)
-        "eam_rho32": 16 + 4 + 8 + 4,  # read offset, anchor; write rho, F'
-        "pair_lj32": 16 + 4 + 24,     # read offset, anchor; write f
+        "eam_force32": 16 + 24,       # read fixed-point x + F'; write f (FP64)
+        "eam_rho32": 16 + 8 + 4,      # read fixed-point x; write rho, F'
+        "pair_lj32": 16 + 24,         # read fixed-point x; write f
         "nve_initial": 72 + 48,       # read x, v, f; write x, v
         "nve_final": 48 + 24,         # read v, f; write v
     }.get(kernel, 0)

@@ -102,12 +102,17 @@ void upload_system(Ctx &c, const double lo[3], const double hi[3], int na, const
   c.ne = ne;
   c.mass = mass;
   c.nact = 0;
+  c.nact_known = true;
   c.lists_valid = false;
   c.have_half = false;
+  c.planned = false;
   c.step = c.last_build_step = 0;
   c.xs.release();
-  size_t ns = (size_t)na + NG * (size_t)ne;
-  c.xs.reserve(ns + ns / 8 + 64);
+  // site table at full capacity: atoms, Gauss points and every lattice site
+  size_t ns = (size_t)na + NG * (size_t)ne + (size_t)ne * NU;
+  c.xs.reserve(ns);
+  c.dev_nact.reserve(1);
+  CACB200_CUDA(cudaMemsetAsync(c.dev_nact.p, 0, sizeof(int), c.stream));
   c.v.reserve(std::max(3 * na, 1));
   c.f.reserve(std::max(3 * na, 1));
   c.nodex.reserve(std::max(24 * ne, 1));
@@ -423,7 +428,7 @@ int cacb200_counts(cacb200_ctx *ctx, int *natoms, int *nelements, int *nactive_s
   API_BEGIN
   if (natoms) *natoms = c.na;
   if (nelements) *nelements = c.ne;
-  if (nactive_sites) *nactive_sites = c.nact;
+  if (nactive_sites) *nactive_sites = c.lists_valid ? device_nact(c) : 0;
   API_END
 }
 
@@ -440,6 +445,7 @@ int cacb200_set_lj(cacb200_ctx *ctx, double epsilon, double sigma, double cut) {
   c.pp.lj4 = 4.0 * epsilon * std::pow(sigma, 6.0);
   c.pp.offset = 0.0;
   c.lists_valid = false;
+  c.planned = false;
   API_END
 }
 
@@ -460,6 +466,7 @@ int cacb200_set_eam(cacb200_ctx *ctx, int nrho, double drho, int nr, double dr, 
   c.pp.rhomax = (nrho - 1) * drho;
   eam_tables(c, frho, rhor, z2r);
   c.lists_valid = false;
+  c.planned = false;
   API_END
 }
 
@@ -475,6 +482,7 @@ int cacb200_set_neighbor(cacb200_ctx *ctx, double skin, int every) {
   c.skin = skin;
   c.every = every;
   c.lists_valid = false;
+  c.planned = false;
   API_END
 }
 

@@ -124,11 +124,13 @@ struct Ctx {
   // sites table S: [atoms | Gauss points (8 per element) | active lattice sites]
   // xs[k] = (x, y, z, w) with w = F'(rho) for EAM
   DBuf<double4> xs;
-  int nact = 0;                  // active non-Gauss lattice sites
+  int nact = 0;                  // active non-Gauss lattice sites (host copy, valid if nact_known)
+  bool nact_known = true;
+  DBuf<int> dev_nact;            // device count written by each rebuild
+  size_t ns_cap = 0;             // site-table capacity (every lattice site active)
   DBuf<int> act_gid;             // [nact] e*729 + u
   DBuf<int> act_off;             // [ne+1] CSR of active sites by element (into act_gid)
   int nsite_i() const { return na + NG * ne; }
-  int nsite_s() const { return na + NG * ne + nact; }
 
   DBuf<double> v, f;             // atoms [na*3]
   DBuf<double> stage;            // [na*3] host-transfer staging for positions
@@ -163,12 +165,17 @@ struct Ctx {
   DBuf<int> ecell_start, ecell_elems;
   DBuf<int> cell_key, cell_key2, idx_tmp, idx_tmp2;
   DBuf<unsigned char> cub_tmp;
+  size_t cub_bytes = 0;
+  int sort_bits_a = 1, sort_bits_e = 1;
+  double reach_budget = 0.0;
+  bool planned = false, plan_half = false;
+  int plan_na = -1, plan_ne = -1;
   RefBins rbins{};
 
   // neighbour lists: transposed [cap][nsite_i] packed entries (sidx << 5 | img)
   double skin = 1.0, cutneigh = 0.0, cutneighsq = 0.0;
   int every = 10;
-  int cap = 128;
+  int cap = 160;
   DBuf<int> nbr_full, num_full;
   DBuf<int> nbr_half, num_half;
   bool have_half = false, lists_valid = false;
@@ -181,11 +188,14 @@ struct Ctx {
 
   PairParams pp;
   DBuf<double4> rhor_val, rhor_der, z2r_val, z2r_der, frho_val, frho_der;
+  // per r-knot m: [2m] rhor value coefficients, [2m+1] z2r value coefficients
+  // (one 64-byte record read by a pair; derivatives follow from them)
+  DBuf<double4> rz;
   // mixed precision: FP32 tables, per-site FP32 offsets and packed anchor cells
-  DBuf<float4> rhor_val32, rhor_der32, z2r_val32, z2r_der32, frho_val32, frho_der32;
+  DBuf<float4> frho_val32, frho_der32;
+  DBuf<float4> rz32;              // the same r-knot records in FP32 (32 bytes)
   bool have_mixed_tables = false;
-  DBuf<float4> pos32;
-  DBuf<unsigned> anc32;
+  DBuf<int4> pos32;              // mixed form: fixed-point site records (qx, qy, qz, F' bits)
 
   FireParams fire;
   DBuf<FireState> fire_state;
@@ -220,6 +230,10 @@ struct KernelTimer {
 
 // stages implemented in the .cu files
 void neigh_build(Ctx &c, bool want_half);
+void neigh_plan(Ctx &c, bool want_half);
+void neigh_build_async(Ctx &c, bool want_half);
+int neigh_check(Ctx &c);
+int device_nact(Ctx &c);
 void neigh_download(Ctx &c, bool half, int64_t *offset, int8_t *kind, int32_t *idx, int32_t *site,
                     int8_t *img, int64_t *nentries);
 void interpolate_sites(Ctx &c);

@@ -12,6 +12,15 @@ struct BoxD {
   double lo[3], hi[3], L[3];
 };
 
+// Grid for a kernel that strides over a count known only on the device:
+// enough blocks to fill the 148 SMs several times over, no more than the
+// capacity `n_max` needs.
+inline int stride_grid(long n_max, int threads) {
+  long b = (n_max + threads - 1) / threads;
+  if (b > 148L * 16) b = 148L * 16;
+  return (int)(b < 1 ? 1 : b);
+}
+
 inline BoxD make_box(const Ctx &c) {
   BoxD b;
   for (int d = 0; d < 3; d++) {
@@ -70,6 +79,24 @@ __host__ __device__ __forceinline__ void img_decode(int code, int &sx, int &sy, 
   sx = code % 3 - 1;
   sy = (code / 3) % 3 - 1;
   sz = code / 9 - 1;
+}
+
+// 256-bit loads through the read-only path (sm_100 and later; the address
+// must be 32-byte aligned).  One instruction brings a whole 32-byte record,
+// so a scattered gather costs one L1 wavefront per record instead of two.
+// Only for data that no thread of the same kernel writes, apart from fields
+// the reader ignores.
+__device__ __forceinline__ double4 ldg256(const double4 *p) {
+  double4 r;
+  asm("ld.global.nc.v4.f64 {%0, %1, %2, %3}, [%4];"
+      : "=d"(r.x), "=d"(r.y), "=d"(r.z), "=d"(r.w)
+      : "l"(p));
+  return r;
+}
+__device__ __forceinline__ void ldg256(const float4 *p, float4 &a, float4 &b) {
+  asm("ld.global.nc.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+      : "=f"(a.x), "=f"(a.y), "=f"(a.z), "=f"(a.w), "=f"(b.x), "=f"(b.y), "=f"(b.z), "=f"(b.w)
+      : "l"(p));
 }
 
 __device__ __forceinline__ double warp_sum(double v) {

@@ -11,38 +11,42 @@ inline int nblk(long n, int t) { return (int)((n + t - 1) / t); }
 // Positions of the Gauss points (their nodes) and of every active lattice
 // site from the current nodes: x_u = sum_n N_n(u) x_n, the interpolation the
 // reference repeats per pair (pair_lj_cut.cpp:364-368, pair_eam.cpp:959-964).
+// The number of active sites is read on the device (written by the last
+// rebuild), so the launch needs no host copy of it: a fixed grid strides
+// over [Gauss points | active sites].
 __global__ void k_interpolate(double4 *xs, const double *nodex, int na, int ne, const int *act_gid,
-                              int nact) {
-  int t = blockIdx.x * blockDim.x + threadIdx.x;
-  int ngp = NG * ne;
-  if (t < ngp) {
-    int e = t / NG, g = t % NG;
-    const double *nx = nodex + (size_t)e * 24 + 3 * gauss_node(g);
-    double4 p = xs[na + t];
-    p.x = nx[0];
-    p.y = nx[1];
-    p.z = nx[2];
-    xs[na + t] = p;
-    return;
-  }
-  int k = t - ngp;
-  if (k >= nact) return;
-  int gid = act_gid[k];
-  int e = gid / NU, u = gid % NU;
-  const double *nx = nodex + (size_t)e * 24;
-  double x = 0.0, y = 0.0, z = 0.0;
+                              const int *nact_dev) {
+  const int ngp = NG * ne;
+  const int n = ngp + *nact_dev;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+    if (t < ngp) {
+      int e = t / NG, g = t % NG;
+      const double *nx = nodex + (size_t)e * 24 + 3 * gauss_node(g);
+      double4 p = xs[na + t];
+      p.x = nx[0];
+      p.y = nx[1];
+      p.z = nx[2];
+      xs[na + t] = p;
+      continue;
+    }
+    int k = t - ngp;
+    int gid = act_gid[k];
+    int e = gid / NU, u = gid % NU;
+    const double *nx = nodex + (size_t)e * 24;
+    double x = 0.0, y = 0.0, z = 0.0;
 #pragma unroll
-  for (int n = 0; n < NPE; n++) {
-    double N = shape_val(u, n);
-    x += N * nx[3 * n];
-    y += N * nx[3 * n + 1];
-    z += N * nx[3 * n + 2];
+    for (int m = 0; m < NPE; m++) {
+      double N = shape_val(u, m);
+      x += N * nx[3 * m];
+      y += N * nx[3 * m + 1];
+      z += N * nx[3 * m + 2];
+    }
+    double4 p = xs[na + ngp + k];
+    p.x = x;
+    p.y = y;
+    p.z = z;
+    xs[na + ngp + k] = p;
   }
-  double4 p = xs[na + ngp + k];
-  p.x = x;
-  p.y = y;
-  p.z = z;
-  xs[na + ngp + k] = p;
 }
 
 // Element::compute_nodef, CONSISTENT (element.cpp:2178-2210): force columns
@@ -131,10 +135,10 @@ __global__ void k_nve_final(double *v, const double *f, int n3, double *nodev, c
 }  // namespace
 
 void interpolate_sites(Ctx &c) {
-  int n = NG * c.ne + c.nact;
-  if (n == 0) return;
+  if (c.ne == 0) return;
   KernelTimer t(c, "interpolate");
-  k_interpolate<<<nblk(n, 256), 256, 0, c.stream>>>(c.xs.p, c.nodex.p, c.na, c.ne, c.act_gid.p, c.nact);
+  k_interpolate<<<stride_grid((long)NG * c.ne + (long)c.ne * NU, 256), 256, 0, c.stream>>>(
+      c.xs.p, c.nodex.p, c.na, c.ne, c.act_gid.p, c.dev_nact.p);
 }
 
 void assemble_nodef(Ctx &c) {

@@ -76,7 +76,7 @@ __global__ void k_pbc_atoms(double4 *xs, int na, BoxD b) {
 //   eframe[e*24 + 12]     dmax
 //   eframe[e*24 + 13..21] frame vectors a, b, c (one lattice step each)
 __global__ void k_elem_geom(double *nodex, int ne, BoxD b, double4 *ecenter, double *eframe,
-                            unsigned long long *reach_bits) {
+                            unsigned long long *reach_bits, double reach_budget, int *grew) {
   int e = blockIdx.x * blockDim.x + threadIdx.x;
   double reach = 0.0;
   if (e < ne) {
@@ -162,6 +162,7 @@ __global__ void k_elem_geom(double *nodex, int ne, BoxD b, double4 *ecenter, dou
       for (int d = 0; d < 3; d++) fr[13 + 3 * q + d] = A[d][q];
     ecenter[e] = make_double4(c[0], c[1], c[2], R);
     reach = R + dmax;
+    if (!(reach <= reach_budget)) atomicExch(grew, 1);
   }
   // block max into reach_bits (non-negative doubles order like their bit patterns)
   for (int o = 16; o > 0; o >>= 1) reach = fmax(reach, __shfl_down_sync(0xffffffffu, reach, o));
@@ -628,11 +629,14 @@ __global__ void k_mark_sites(const int *raw, const int *num, int nsi, int cap, i
 }
 
 __global__ void k_act_table(const int *flag, const int *pref, int ngid, int ne, int *act_gid,
-                            int *act_off, int nact) {
+                            int *act_off, int *nact) {
   int gid = blockIdx.x * blockDim.x + threadIdx.x;
   if (gid < ngid && flag[gid]) act_gid[pref[gid]] = gid;
   if (gid < ne) act_off[gid] = pref[gid * NU];
-  if (gid == 0) act_off[ne] = nact;
+  if (gid == 0) {
+    act_off[ne] = pref[ngid];
+    *nact = pref[ngid];
+  }
 }
 
 __global__ void k_remap(const int *raw, const unsigned char *img, const int *num, int nsi, int cap,
@@ -691,18 +695,6 @@ void setup_grids(Ctx &c, double ereach) {
   c.egrid.ncell = c.egrid.nc[0] * c.egrid.nc[1] * c.egrid.nc[2];
 }
 
-template <class K>
-void sort_pairs(Ctx &c, int *keys_in, int *keys_out, int *vals_in, int *vals_out, int n, int maxkey) {
-  size_t bytes = 0;
-  int bits = 1;
-  while ((1 << bits) <= maxkey && bits < 31) bits++;
-  cub::DeviceRadixSort::SortPairs(nullptr, bytes, keys_in, keys_out, vals_in, vals_out, n, 0, bits,
-                                  c.stream);
-  c.cub_tmp.reserve(bytes);
-  CACB200_CUDA(cub::DeviceRadixSort::SortPairs(c.cub_tmp.p, bytes, keys_in, keys_out, vals_in,
-                                               vals_out, n, 0, bits, c.stream));
-}
-
 }  // namespace
 
 void pbc_wrap(Ctx &c) {
@@ -710,188 +702,261 @@ void pbc_wrap(Ctx &c) {
   if (c.na) k_pbc_atoms<<<nblk(c.na, 256), 256, 0, c.stream>>>(c.xs.p, c.na, b);
 }
 
-void neigh_build(Ctx &c, bool want_half) {
+// Capacity plan: sizes every buffer of a rebuild for the current system (site
+// table for the worst case of every lattice site active, candidate grids with
+// room for elements to grow, list slots of `cap` per site), so that rebuilds
+// afterwards neither allocate nor synchronise and can be queued or captured
+// in a CUDA graph.  Synchronises once to read the element radius.
+void neigh_plan(Ctx &c, bool want_half) {
   c.check_system();
   if (c.pp.style == CACB200_PAIR_NONE) throw Error(CACB200_ESTATE, "no pair style set");
   BoxD b = make_box(c);
   double cutoff = std::sqrt(c.pp.cut * c.pp.cut);
   c.cutneigh = cutoff + c.skin;
   c.cutneighsq = c.cutneigh * c.cutneigh;
+  c.ecenter.reserve(std::max(c.ne, 1));
+  c.eframe.reserve((size_t)std::max(c.ne, 1) * 24);
+  c.overflow.reserve(8);
+  c.dev_nact.reserve(1);
+  CACB200_CUDA(cudaMemsetAsync(c.overflow.p, 0, 8 * sizeof(int), c.stream));
+  CACB200_CUDA(cudaMemsetAsync(c.dev_nact.p, 0, sizeof(int), c.stream));
+  double ereach = 0.0;
+  if (c.ne) {
+    if (c.na) k_pbc_atoms<<<nblk(c.na, 256), 256, 0, c.stream>>>(c.xs.p, c.na, b);
+    k_elem_geom<<<nblk(c.ne, 128), 128, 0, c.stream>>>(c.nodex.p, c.ne, b, c.ecenter.p, c.eframe.p,
+                                                       (unsigned long long *)(c.overflow.p + 4), 1e300,
+                                                       c.overflow.p + 3);
+    unsigned long long bits = 0;
+    stream_copy(c, &bits, c.overflow.p + 4, sizeof(bits), cudaMemcpyDeviceToHost);
+    std::memcpy(&ereach, &bits, sizeof(double));
+    if (!(ereach < 1e30)) throw Error(CACB200_EUNSTABLE, "non-finite element geometry");
+  }
+  // elements may grow by 20 % (and 2 A) before the grid is planned again, as
+  // far as the box allows
+  c.reach_budget = 0.0;
+  if (c.ne) {
+    double room = std::min(c.prd[0], std::min(c.prd[1], c.prd[2])) - c.cutneigh - 2e-6;
+    c.reach_budget = std::max(ereach, std::min(std::max(1.2 * ereach, ereach + 2.0), room));
+  }
+  setup_grids(c, c.reach_budget);
 
-  // periodic wrap, element geometry
+  const int nsi = c.nsite_i();
+  const size_t ngid = (size_t)c.ne * NU;
+  int nmax = std::max(std::max(c.na, c.ne), 1);
+  c.cell_key.reserve(nmax);
+  c.cell_key2.reserve(nmax);
+  c.idx_tmp.reserve(nmax);
+  c.idx_tmp2.reserve(nmax);
+  c.acell_start.reserve(c.agrid.ncell + 1);
+  c.acell_pos.reserve(std::max(c.na, 1));
+  c.acell_pos32.reserve(std::max(c.na, 1));
+  c.ecell_start.reserve(c.egrid.ncell + 1);
+  c.ecell_elems.reserve(std::max(c.ne, 1));
+  size_t slots = (size_t)c.cap * std::max(nsi, 1);
+  c.raw_full.reserve(slots);
+  c.img_full.reserve(slots);
+  c.num_full.reserve(std::max(nsi, 1));
+  c.nbr_full.reserve(slots);
+  if (want_half) {
+    c.raw_half.reserve(slots);
+    c.img_half.reserve(slots);
+    c.num_half.reserve(std::max(nsi, 1));
+    c.nbr_half.reserve(slots);
+  }
+  c.site_flag.reserve(ngid + 1);
+  c.site_pref.reserve(ngid + 1);
+  c.act_gid.reserve(std::max<size_t>(ngid, 1));
+  c.act_off.reserve(c.ne + 1);
+  // site table for every lattice site active, keeping the atom positions
+  size_t ns_cap = (size_t)nsi + ngid;
+  if (ns_cap > c.xs.n) {
+    double4 *np_ = nullptr;
+    if (cudaMalloc(&np_, ns_cap * sizeof(double4)) != cudaSuccess) {
+      cudaGetLastError();
+      throw Error(CACB200_ENOMEM, "site table allocation failed");
+    }
+    if (c.na)
+      CACB200_CUDA(cudaMemcpyAsync(np_, c.xs.p, sizeof(double4) * c.na, cudaMemcpyDeviceToDevice, c.stream));
+    CACB200_CUDA(cudaStreamSynchronize(c.stream));
+    cudaFree(c.xs.p);
+    c.xs.p = np_;
+    c.xs.n = ns_cap;
+  }
+  c.ns_cap = ns_cap;
+  // CUB temporary storage for the largest sort and the scan
+  size_t need = 0, bytes = 0;
+  int bits_a = 1, bits_e = 1;
+  while ((1 << bits_a) <= c.agrid.ncell && bits_a < 31) bits_a++;
+  while ((1 << bits_e) <= c.egrid.ncell && bits_e < 31) bits_e++;
+  cub::DeviceRadixSort::SortPairs(nullptr, bytes, c.cell_key.p, c.cell_key2.p, c.idx_tmp.p, c.idx_tmp2.p,
+                                  std::max(c.na, 1), 0, bits_a, c.stream);
+  need = std::max(need, bytes);
+  cub::DeviceRadixSort::SortPairs(nullptr, bytes, c.cell_key.p, c.cell_key2.p, c.idx_tmp.p, c.ecell_elems.p,
+                                  std::max(c.ne, 1), 0, bits_e, c.stream);
+  need = std::max(need, bytes);
+  cub::DeviceScan::ExclusiveSum(nullptr, bytes, c.site_flag.p, c.site_pref.p, (int)(ngid + 1), c.stream);
+  need = std::max(need, bytes);
+  c.cub_tmp.reserve(need);
+  c.cub_bytes = need;
+  c.sort_bits_a = bits_a;
+  c.sort_bits_e = bits_e;
+  c.plan_half = want_half;
+  c.planned = true;
+  c.plan_na = c.na;
+  c.plan_ne = c.ne;
+}
+
+// Queue a rebuild: pbc, element geometry, binning, candidate search, storage
+// rules, compaction of the referenced lattice sites and packing of the list
+// entries.  Nothing here allocates or waits for the device; problems are
+// reported in the flag words (list overflow, distant image, element grown past
+// the grid plan) for neigh_check.
+void neigh_build_async(Ctx &c, bool want_half) {
+  if (!c.planned || c.plan_na != c.na || c.plan_ne != c.ne || (want_half && !c.plan_half))
+    throw Error(CACB200_ESTATE, "rebuild without a capacity plan");
+  BoxD b = make_box(c);
+  const int nsi = c.nsite_i();
+  const size_t ngid = (size_t)c.ne * NU;
+  CACB200_CUDA(cudaMemsetAsync(c.overflow.p, 0, 4 * sizeof(int), c.stream));
   {
     KernelTimer t(c, "pbc_geom");
     if (c.na) k_pbc_atoms<<<nblk(c.na, 256), 256, 0, c.stream>>>(c.xs.p, c.na, b);
-    c.ecenter.reserve(std::max(c.ne, 1));
-    c.eframe.reserve((size_t)std::max(c.ne, 1) * 24);
-    c.overflow.reserve(8);
-    CACB200_CUDA(cudaMemsetAsync(c.overflow.p, 0, 8 * sizeof(int), c.stream));
     if (c.ne)
       k_elem_geom<<<nblk(c.ne, 128), 128, 0, c.stream>>>(c.nodex.p, c.ne, b, c.ecenter.p, c.eframe.p,
-                                                         (unsigned long long *)(c.overflow.p + 4));
+                                                         (unsigned long long *)(c.overflow.p + 4),
+                                                         c.reach_budget, c.overflow.p + 3);
   }
-  unsigned long long reach_bits = 0;
-  if (c.ne) {
-    CACB200_CUDA(cudaMemcpyAsync(&reach_bits, c.overflow.p + 4, sizeof(reach_bits),
-                                 cudaMemcpyDeviceToHost, c.stream));
-    CACB200_CUDA(cudaStreamSynchronize(c.stream));
-  }
-  double ereach;
-  std::memcpy(&ereach, &reach_bits, sizeof(double));
-  setup_grids(c, c.ne ? ereach : 0.0);
-
-  // binning: atoms and elements by cell, stable by index
   {
     KernelTimer t(c, "bin");
-    int nmax = std::max(std::max(c.na, c.ne), 1);
-    c.cell_key.reserve(nmax);
-    c.cell_key2.reserve(nmax);
-    c.idx_tmp.reserve(nmax);
-    c.idx_tmp2.reserve(nmax);
-    c.acell_start.reserve(c.agrid.ncell + 1);
-    c.acell_pos.reserve(std::max(c.na, 1));
-    c.acell_pos32.reserve(std::max(c.na, 1));
-    c.ecell_start.reserve(c.egrid.ncell + 1);
-    c.ecell_elems.reserve(std::max(c.ne, 1));
+    size_t bytes = c.cub_bytes;
     if (c.na) {
-      k_atom_keys<<<nblk(c.na, 256), 256, 0, c.stream>>>(c.xs.p, c.na, c.agrid, b, c.cell_key.p,
-                                                         c.idx_tmp.p);
-      sort_pairs<int>(c, c.cell_key.p, c.cell_key2.p, c.idx_tmp.p, c.idx_tmp2.p, c.na, c.agrid.ncell);
+      k_atom_keys<<<nblk(c.na, 256), 256, 0, c.stream>>>(c.xs.p, c.na, c.agrid, b, c.cell_key.p, c.idx_tmp.p);
+      CACB200_CUDA(cub::DeviceRadixSort::SortPairs(c.cub_tmp.p, bytes, c.cell_key.p, c.cell_key2.p, c.idx_tmp.p,
+                                                   c.idx_tmp2.p, c.na, 0, c.sort_bits_a, c.stream));
       k_cell_start<<<nblk(c.agrid.ncell + 1, 256), 256, 0, c.stream>>>(c.cell_key2.p, c.na, c.agrid.ncell,
-                                                              c.acell_start.p);
+                                                                      c.acell_start.p);
       k_gather_pos<<<nblk(c.na, 256), 256, 0, c.stream>>>(c.xs.p, c.idx_tmp2.p, c.na, c.acell_pos.p,
                                                           c.acell_pos32.p);
     } else {
       CACB200_CUDA(cudaMemsetAsync(c.acell_start.p, 0, sizeof(int) * (c.agrid.ncell + 1), c.stream));
     }
     if (c.ne) {
+      bytes = c.cub_bytes;
       k_elem_keys<<<nblk(c.ne, 256), 256, 0, c.stream>>>(c.ecenter.p, c.ne, c.egrid, b, c.cell_key.p,
                                                          c.idx_tmp.p);
-      sort_pairs<int>(c, c.cell_key.p, c.cell_key2.p, c.idx_tmp.p, c.ecell_elems.p, c.ne, c.egrid.ncell);
+      CACB200_CUDA(cub::DeviceRadixSort::SortPairs(c.cub_tmp.p, bytes, c.cell_key.p, c.cell_key2.p, c.idx_tmp.p,
+                                                   c.ecell_elems.p, c.ne, 0, c.sort_bits_e, c.stream));
       k_cell_start<<<nblk(c.egrid.ncell + 1, 256), 256, 0, c.stream>>>(c.cell_key2.p, c.ne, c.egrid.ncell,
-                                                              c.ecell_start.p);
+                                                                      c.ecell_start.p);
     } else {
       CACB200_CUDA(cudaMemsetAsync(c.ecell_start.p, 0, sizeof(int) * (c.egrid.ncell + 1), c.stream));
     }
   }
-
-  const int nsi = c.nsite_i();
-  for (int attempt = 0; attempt < 3; attempt++) {
-    size_t slots = (size_t)c.cap * nsi;
-    c.raw_full.reserve(slots);
-    c.img_full.reserve(slots);
-    c.num_full.reserve(nsi);
-    if (want_half) {
-      c.raw_half.reserve(slots);
-      c.img_half.reserve(slots);
-      c.num_half.reserve(nsi);
-    }
-    CACB200_CUDA(cudaMemsetAsync(c.overflow.p, 0, 4 * sizeof(int), c.stream));
-    BuildArgs A;
-    A.xs = c.xs.p;
-    A.nodex = c.nodex.p;
-    A.ecenter = c.ecenter.p;
-    A.eframe = c.eframe.p;
-    A.acell_start = c.acell_start.p;
-    A.acell_pos = c.acell_pos.p;
-    A.acell_pos32 = c.acell_pos32.p;
-    A.ecell_start = c.ecell_start.p;
-    A.ecell_elems = c.ecell_elems.p;
-    A.na = c.na;
-    A.ne = c.ne;
-    A.nsi = nsi;
-    A.cap = c.cap;
-    A.ag = c.agrid;
-    A.eg = c.egrid;
-    A.b = b;
-    A.rb = c.rbins;
-    A.cutneigh = c.cutneigh;
-    A.cutneighsq = c.cutneighsq;
-    A.want_half = want_half ? 1 : 0;
-    A.raw_full = c.raw_full.p;
-    A.num_full = c.num_full.p;
-    A.img_full = c.img_full.p;
-    A.raw_half = want_half ? c.raw_half.p : nullptr;
-    A.num_half = want_half ? c.num_half.p : nullptr;
-    A.img_half = want_half ? c.img_half.p : nullptr;
-    A.overflow = c.overflow.p;
-    if (c.na) {
-      KernelTimer t(c, "build_atoms");
-      k_build_atoms<<<c.agrid.ncell, 32, 0, c.stream>>>(A);
-    }
-    if (c.na) {
-      KernelTimer t(c, "build_atom_sites");
-      k_build_atom_sites<<<nblk(c.na, 128), 128, 0, c.stream>>>(A);
-    }
-    if (c.ne) {
-      KernelTimer t(c, "build_gauss");
-      k_build_gauss<<<nblk(NG * c.ne, 128), 128, 0, c.stream>>>(A);
-    }
-    int ov[8];
-    CACB200_CUDA(cudaMemcpyAsync(ov, c.overflow.p, sizeof(ov), cudaMemcpyDeviceToHost, c.stream));
-    CACB200_CUDA(cudaStreamSynchronize(c.stream));
-    if (ov[2]) throw Error(CACB200_EINVAL, "neighbour image beyond the first periodic image (box too small)");
-    if (ov[6]) throw Error(CACB200_EUNSTABLE, "a site moved more than 8 cells outside the box (unstable run)");
-    if (!ov[0]) break;
-    c.cap = ((ov[1] + 31) / 32) * 32;
-    if (attempt == 2) throw Error(CACB200_EOVERFLOW, "neighbour list capacity");
+  BuildArgs A;
+  A.xs = c.xs.p;
+  A.nodex = c.nodex.p;
+  A.ecenter = c.ecenter.p;
+  A.eframe = c.eframe.p;
+  A.acell_start = c.acell_start.p;
+  A.acell_pos = c.acell_pos.p;
+  A.acell_pos32 = c.acell_pos32.p;
+  A.ecell_start = c.ecell_start.p;
+  A.ecell_elems = c.ecell_elems.p;
+  A.na = c.na;
+  A.ne = c.ne;
+  A.nsi = nsi;
+  A.cap = c.cap;
+  A.ag = c.agrid;
+  A.eg = c.egrid;
+  A.b = b;
+  A.rb = c.rbins;
+  A.cutneigh = c.cutneigh;
+  A.cutneighsq = c.cutneighsq;
+  A.want_half = want_half ? 1 : 0;
+  A.raw_full = c.raw_full.p;
+  A.num_full = c.num_full.p;
+  A.img_full = c.img_full.p;
+  A.raw_half = want_half ? c.raw_half.p : nullptr;
+  A.num_half = want_half ? c.num_half.p : nullptr;
+  A.img_half = want_half ? c.img_half.p : nullptr;
+  A.overflow = c.overflow.p;
+  if (c.na) {
+    KernelTimer t(c, "build_atoms");
+    k_build_atoms<<<c.agrid.ncell, 32, 0, c.stream>>>(A);
   }
-
-  // compact referenced lattice sites into the site table
+  if (c.na) {
+    KernelTimer t(c, "build_atom_sites");
+    k_build_atom_sites<<<nblk(c.na, 128), 128, 0, c.stream>>>(A);
+  }
+  if (c.ne) {
+    KernelTimer t(c, "build_gauss");
+    k_build_gauss<<<nblk(NG * c.ne, 128), 128, 0, c.stream>>>(A);
+  }
   {
     KernelTimer t(c, "compact");
-    size_t ngid = (size_t)c.ne * NU;
-    c.site_flag.reserve(ngid + 1);
-    c.site_pref.reserve(ngid + 1);
     int *flag = c.site_flag.p;
     int *pref = c.site_pref.p;
-    int nact = 0;
     if (ngid) {
       CACB200_CUDA(cudaMemsetAsync(flag, 0, sizeof(int) * (ngid + 1), c.stream));
       k_mark_sites<<<nblk(nsi, 256), 256, 0, c.stream>>>(c.raw_full.p, c.num_full.p, nsi, c.cap, flag);
-      size_t bytes = 0;
-      cub::DeviceScan::ExclusiveSum(nullptr, bytes, flag, pref, (int)(ngid + 1), c.stream);
-      c.cub_tmp.reserve(bytes);
+      size_t bytes = c.cub_bytes;
       CACB200_CUDA(cub::DeviceScan::ExclusiveSum(c.cub_tmp.p, bytes, flag, pref, (int)(ngid + 1), c.stream));
-      CACB200_CUDA(cudaMemcpyAsync(&nact, pref + ngid, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
-      CACB200_CUDA(cudaStreamSynchronize(c.stream));
-    }
-    c.nact = nact;
-    c.act_gid.reserve(std::max(nact, 1));
-    c.act_off.reserve(c.ne + 1);
-    if (ngid)
       k_act_table<<<nblk((long)ngid, 256), 256, 0, c.stream>>>(flag, pref, (int)ngid, c.ne, c.act_gid.p,
-                                                              c.act_off.p, nact);
-    // grow the site table, keeping the atom positions it holds
-    size_t ns = (size_t)c.nsite_s();
-    if (ns > c.xs.n) {
-      double4 *np_ = nullptr;
-      size_t want = ns + ns / 8 + 64;
-      if (cudaMalloc(&np_, want * sizeof(double4)) != cudaSuccess) {
-        cudaGetLastError();
-        throw Error(CACB200_ENOMEM, "site table allocation failed");
-      }
-      if (c.na)
-        CACB200_CUDA(cudaMemcpyAsync(np_, c.xs.p, sizeof(double4) * c.na, cudaMemcpyDeviceToDevice, c.stream));
-      CACB200_CUDA(cudaStreamSynchronize(c.stream));
-      cudaFree(c.xs.p);
-      c.xs.p = np_;
-      c.xs.n = want;
+                                                              c.act_off.p, c.dev_nact.p);
     }
-    size_t slots = (size_t)c.cap * nsi;
-    c.nbr_full.reserve(slots);
-    k_remap<<<nblk(nsi, 256), 256, 0, c.stream>>>(c.raw_full.p, c.img_full.p, c.num_full.p, nsi, c.cap,
-                                                   pref, c.na, c.ne, c.nbr_full.p);
-    if (want_half) {
-      c.nbr_half.reserve(slots);
-      k_remap<<<nblk(nsi, 256), 256, 0, c.stream>>>(c.raw_half.p, c.img_half.p, c.num_half.p, nsi, c.cap,
-                                                     pref, c.na, c.ne, c.nbr_half.p);
-    }
+    k_remap<<<nblk(nsi, 256), 256, 0, c.stream>>>(c.raw_full.p, c.img_full.p, c.num_full.p, nsi, c.cap, pref,
+                                                   c.na, c.ne, c.nbr_full.p);
+    if (want_half)
+      k_remap<<<nblk(nsi, 256), 256, 0, c.stream>>>(c.raw_half.p, c.img_half.p, c.num_half.p, nsi, c.cap, pref,
+                                                     c.na, c.ne, c.nbr_half.p);
   }
   c.have_half = want_half;
   c.lists_valid = true;
+  c.nact_known = false;
   c.build_count++;
   CACB200_CUDA(cudaGetLastError());
+}
+
+// Read the rebuild's flag words (synchronises).  Returns 0 when the lists are
+// good, 1 when a capacity must grow (the plan was updated: rebuild again).
+int neigh_check(Ctx &c) {
+  int ov[8];
+  stream_copy(c, ov, c.overflow.p, sizeof(ov), cudaMemcpyDeviceToHost);
+  if (ov[2]) throw Error(CACB200_EINVAL, "neighbour image beyond the first periodic image (box too small)");
+  if (ov[6]) throw Error(CACB200_EUNSTABLE, "a site left the fixed-point range around the box (unstable run)");
+  int again = 0;
+  if (ov[0]) {
+    c.cap = ((ov[1] + 31) / 32) * 32;
+    again = 1;
+  }
+  if (ov[3]) again = 1;   // an element outgrew the candidate grid
+  if (again) {
+    c.lists_valid = false;
+    neigh_plan(c, c.plan_half);
+  }
+  return again;
+}
+
+// Synchronous rebuild with retries (API calls, setup, tests).
+void neigh_build(Ctx &c, bool want_half) {
+  c.check_system();
+  if (!c.planned || c.plan_na != c.na || c.plan_ne != c.ne || (want_half && !c.plan_half))
+    neigh_plan(c, want_half || c.plan_half);
+  for (int attempt = 0; attempt < 4; attempt++) {
+    neigh_build_async(c, want_half);
+    if (!neigh_check(c)) return;
+  }
+  throw Error(CACB200_EOVERFLOW, "neighbour list capacity could not be settled");
+}
+
+int device_nact(Ctx &c) {
+  if (!c.nact_known) {
+    int n = 0;
+    if (c.ne) stream_copy(c, &n, c.dev_nact.p, sizeof(int), cudaMemcpyDeviceToHost);
+    c.nact = n;
+    c.nact_known = true;
+  }
+  return c.nact;
 }
 
 void neigh_download(Ctx &c, bool half, int64_t *offset, int8_t *kind, int32_t *idx, int32_t *site,
@@ -900,6 +965,7 @@ void neigh_download(Ctx &c, bool half, int64_t *offset, int8_t *kind, int32_t *i
   const int nsi = c.nsite_i();
   std::vector<int> num(nsi);
   std::vector<int> ent((size_t)c.cap * nsi);
+  device_nact(c);
   std::vector<int> act(std::max(c.nact, 1));
   CACB200_CUDA(cudaStreamSynchronize(c.stream));
   stream_copy(c, num.data(), half ? c.num_half.p : c.num_full.p, sizeof(int) * nsi,

@@ -44,7 +44,7 @@ struct PairArgs {
 
 __device__ __forceinline__ void neighbour_pos(const PairArgs &A, int v, double4 &xj) {
   int j = v >> IMG_BITS, code = v & ((1 << IMG_BITS) - 1);
-  xj = A.xs[j];
+  xj = ldg256(A.xs + j);
   if (code != IMG_ZERO) {
     int sx, sy, sz;
     img_decode(code, sx, sy, sz);
@@ -181,8 +181,13 @@ __global__ void __launch_bounds__(128, EV ? 4 : 8) k_lj(PairArgs A, LjParams P) 
 
 // ------------------------------------------------------------------ EAM
 
+// r-dependent splines as one 64-byte record per knot m: rz[2m] the rhor value
+// coefficients (S3, S4, S5, S6 of PairEAM::interpolate), rz[2m+1] those of
+// z2r.  A pair reads the record once; the derivative coefficients are the
+// reference's (S0, S1, S2) = (3 S3, 2 S4, S5) / dr (pair_eam.cpp:612-614),
+// applied as ((3 S3 p + 2 S4) p + S5) * (1/dr).
 struct EamTables {
-  const double4 *rhor_val, *rhor_der, *z2r_val, *z2r_der, *frho_val, *frho_der;
+  const double4 *rz, *frho_val, *frho_der;
   double rdr, rdrho, rhomax, cutforcesq;
   int nr, nrho;
 };
@@ -227,7 +232,7 @@ __global__ void __launch_bounds__(128, 8) k_eam_rho(PairArgs A, EamTables T, dou
       m = max(1, min(m, T.nr - 1));
       p -= m;
       p = fmin(p, 1.0);
-      double4 c = T.rhor_val[m];
+      double4 c = ldg256(T.rz + 2 * m);
       rho += ((c.x * p + c.y) * p + c.z) * p + c.w;
     }
   };
@@ -246,22 +251,23 @@ __global__ void __launch_bounds__(128, 8) k_eam_rho(PairArgs A, EamTables T, dou
 
 // F' at interpolated lattice sites from shape-weighted nodal density
 // (pair_eam.cpp:957-969)
-__global__ void k_eam_site_fp(double4 *xs, const int *act_gid, int nact, int base, int na,
+__global__ void k_eam_site_fp(double4 *xs, const int *act_gid, const int *nact_dev, int base, int na,
                               const double *rho, EamTables T) {
-  int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= nact) return;
-  int gid = act_gid[k];
-  int e = gid / NU, u = gid % NU;
-  const double *rn = rho + na + 8 * (size_t)e;
-  double r = 0.0;
+  const int nact = *nact_dev;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nact; k += gridDim.x * blockDim.x) {
+    int gid = act_gid[k];
+    int e = gid / NU, u = gid % NU;
+    const double *rn = rho + na + 8 * (size_t)e;
+    double r = 0.0;
 #pragma unroll
-  for (int n = 0; n < NPE; n++) r += shape_val(u, n) * rn[n];
-  xs[base + k].w = eam_fp(T, r, nullptr);
+    for (int n = 0; n < NPE; n++) r += shape_val(u, n) * rn[n];
+    xs[base + k].w = eam_fp(T, r, nullptr);
+  }
 }
 
 // pass 2: forces (pair_eam.cpp:845-1028)
 template <bool EV>
-__global__ void __launch_bounds__(128, EV ? 4 : 8) k_eam_force(PairArgs A, EamTables T, const double *phi_site) {
+__global__ void __launch_bounds__(128, EV ? 4 : 6) k_eam_force(PairArgs A, EamTables T, const double *phi_site) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   bool valid = i < A.nsi;
   double fi[3] = {0, 0, 0}, esum = 0.0, vsum[6] = {0, 0, 0, 0, 0, 0};
@@ -281,11 +287,10 @@ __global__ void __launch_bounds__(128, EV ? 4 : 8) k_eam_force(PairArgs A, EamTa
         m = max(1, min(m, T.nr - 1));
         p -= m;
         p = fmin(p, 1.0);
-        double4 rd = T.rhor_der[m];
-        double rhop = (rd.x * p + rd.y) * p + rd.z;
-        double4 zd = T.z2r_der[m];
-        double4 zv = T.z2r_val[m];
-        double z2p = (zd.x * p + zd.y) * p + zd.z;
+        double4 rv = ldg256(T.rz + 2 * m);
+        double4 zv = ldg256(T.rz + 2 * m + 1);
+        double rhop = ((3.0 * rv.x * p + 2.0 * rv.y) * p + rv.z) * T.rdr;
+        double z2p = ((3.0 * zv.x * p + 2.0 * zv.y) * p + zv.z) * T.rdr;
         double z2 = ((zv.x * p + zv.y) * p + zv.z) * p + zv.w;
         double recip = 1.0 / r;
         double phi = z2 * recip;
@@ -381,8 +386,19 @@ void eam_tables(Ctx &c, const double *frho, const double *rhor, const double *z2
   upload_split(c, sp, p.nrho, c.frho_val, c.frho_der);
   spline7(p.nr, p.dr, b, sp);
   upload_split(c, sp, p.nr, c.rhor_val, c.rhor_der);
+  std::vector<double4> rz((size_t)2 * (p.nr + 1));
+  for (int m = 0; m <= p.nr; m++) {
+    const double *r = &sp[(size_t)m * 7];
+    rz[2 * m] = make_double4(r[3], r[4], r[5], r[6]);
+  }
   spline7(p.nr, p.dr, z, sp);
   upload_split(c, sp, p.nr, c.z2r_val, c.z2r_der);
+  for (int m = 0; m <= p.nr; m++) {
+    const double *r = &sp[(size_t)m * 7];
+    rz[2 * m + 1] = make_double4(r[3], r[4], r[5], r[6]);
+  }
+  c.rz.reserve(rz.size());
+  stream_copy(c, c.rz.p, rz.data(), sizeof(double4) * rz.size(), cudaMemcpyHostToDevice);
 }
 
 void pair_compute(Ctx &c, int eflag, int vflag) {
@@ -435,10 +451,7 @@ void pair_compute(Ctx &c, int eflag, int vflag) {
     else k_lj<false><<<nb, T, 0, c.stream>>>(A, P);
   } else if (c.pp.style == CACB200_PAIR_EAM) {
     EamTables Tb;
-    Tb.rhor_val = c.rhor_val.p;
-    Tb.rhor_der = c.rhor_der.p;
-    Tb.z2r_val = c.z2r_val.p;
-    Tb.z2r_der = c.z2r_der.p;
+    Tb.rz = c.rz.p;
     Tb.frho_val = c.frho_val.p;
     Tb.frho_der = c.frho_der.p;
     Tb.rdr = c.pp.rdr;
@@ -453,10 +466,10 @@ void pair_compute(Ctx &c, int eflag, int vflag) {
       KernelTimer t(c, "eam_rho");
       k_eam_rho<<<nb, T, 0, c.stream>>>(A, Tb, c.rho.p, c.phi_site.p);
     }
-    if (c.nact) {
+    if (c.ne) {
       KernelTimer t(c, "eam_site_fp");
-      k_eam_site_fp<<<nblk(c.nact, 256), 256, 0, c.stream>>>(c.xs.p, c.act_gid.p, c.nact,
-                                                             c.na + NG * c.ne, c.na, c.rho.p, Tb);
+      k_eam_site_fp<<<stride_grid((long)c.ne * NU, 256), 256, 0, c.stream>>>(
+          c.xs.p, c.act_gid.p, c.dev_nact.p, c.na + NG * c.ne, c.na, c.rho.p, Tb);
     }
     {
       KernelTimer t(c, "eam_force");

@@ -1,16 +1,16 @@
 // Mixed-precision pair kernels: FP32 distances and force arithmetic on
-// positions stored relative to their cell, FP64 everywhere else.
+// fixed-point positions, FP64 everywhere else.
 //
-// Every site of the site table gets, each step, an anchor cell of an 8 A grid
-// fixed to the box (a = floor((x - lo) / 8), from its FP64 position, which may
-// lie outside the box for element sites) and its FP32 offset inside that cell
-// (x - lo - 8 a, at most 8 A, so one FP32 ulp is 4.8e-7 A).  A pair's
-// separation is then
-//     x_i - (x_j + s L) = (off_i - off_j) + (a_i - a_j - s n) * 8 - s r
-// per dimension, with n = ceil(L / 8) cells and r = L - 8 n: the cell term is
-// a small integer times 8 (exact in FP32), r is rounded once, and no FP32 sum
-// ever carries a box-sized coordinate.  Anchors are packed into one 32-bit
-// word with per-dimension bit fields sized from the box.
+// Every site of the site table gets, each step, a 32-bit fixed-point copy of
+// its FP64 position relative to the box corner, q = rint((x - lo) 2^k), with
+// k chosen from the box so that the box plus a 64 A margin (element sites may
+// lie outside the box) fits in an int.  A pair's separation is then
+//     x_i - (x_j + s L) = (q_i - q_j - s Lq) 2^-k,
+// an exact integer difference (wrap-around 32-bit arithmetic is exact while
+// the true difference is small) rounded once to FP32: no FP32 sum ever
+// carries a box-sized coordinate.  The quantum 2^-k is 2.4e-7 A for boxes up
+// to ~440 A.  A site's record is 16 bytes, (qx, qy, qz, F'), so one 128-bit
+// load brings everything a pair needs from its neighbour.
 //
 // What stays FP64 (as the mixed form specifies): positions and velocities and
 // their integration, element interpolation, nodal assembly over Gauss points,
@@ -30,56 +30,45 @@ namespace {
 
 inline int nblk(long n, int t) { return (int)((n + t - 1) / t); }
 
-constexpr double CELL = 8.0;   // anchor cell edge (A); exact in FP32
-constexpr int BIAS = 8;        // anchors may lie up to 8 cells outside the box
-
-struct AnchorGrid {
+struct FixGrid {
   double lo[3];
-  int n[3];        // cells per box length
-  float r[3];      // L - 8 n (rounded once)
-  int shift[3];    // bit offsets of the fields
-  int bits[3];
+  double scale;    // 2^k
+  float inv;       // 2^-k
+  int Lq[3];       // rint(L 2^k)
 };
 
-__device__ __forceinline__ void unpack_anchor(const AnchorGrid &G, unsigned w, int a[3]) {
-#pragma unroll
-  for (int d = 0; d < 3; d++) a[d] = (int)((w >> G.shift[d]) & ((1u << G.bits[d]) - 1u)) - BIAS;
-}
-
-// FP32 copy of every site's position relative to its anchor cell; w keeps F'
-// for EAM (written later in the step).
-__global__ void k_pack32(const double4 *xs, int n, AnchorGrid G, float4 *pos, unsigned *anc, int *bad) {
-  int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= n) return;
+__device__ __forceinline__ void pack_one(const double4 *xs, int k, const FixGrid &G, int4 *pos, int *bad) {
   double4 p = xs[k];
   double q[3] = {p.x, p.y, p.z};
-  unsigned w = 0;
-  float o[3];
+  int o[3];
 #pragma unroll
   for (int d = 0; d < 3; d++) {
-    double rel = q[d] - G.lo[d];
-    int a = (int)floor(rel / CELL);
-    int f = a + BIAS;
-    if (f < 0 || f >= (1 << G.bits[d])) {
+    double rel = (q[d] - G.lo[d]) * G.scale;
+    if (!(rel > -2147483000.0 && rel < 2147483000.0)) {
       atomicExch(bad, 1);
-      f = 0;
-      a = -BIAS;
+      rel = 0.0;
     }
-    o[d] = (float)(rel - CELL * a);
-    w |= (unsigned)f << G.shift[d];
+    o[d] = __double2int_rn(rel);
   }
-  float4 v = pos[k];
-  pos[k] = make_float4(o[0], o[1], o[2], v.w);
-  anc[k] = w;
+  int4 v = pos[k];
+  pos[k] = make_int4(o[0], o[1], o[2], v.w);
+}
+
+// Fixed-point copy of every site's position; w keeps F' for EAM (written
+// later in the step).  The active-site count is read on the device, so a
+// fixed grid strides over [atoms | Gauss points | active sites].
+__global__ void k_pack32(const double4 *xs, int nsi, const int *nact_dev, FixGrid G, int4 *pos, int *bad) {
+  const int n = nsi + *nact_dev;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x)
+    pack_one(xs, k, G, pos, bad);
 }
 
 struct Args32 {
-  const float4 *pos;
-  const unsigned *anc;
+  const int4 *pos;
   const int *nbr;
   const int *num;
   int na, ne, nsi;
-  AnchorGrid G;
+  FixGrid G;
   double *f, *gaussf;
   double *eatom, *vatom, *enode, *vnode;
   double *partial;
@@ -87,23 +76,26 @@ struct Args32 {
   double escale_node, vscale_node;
 };
 
-// separation of site i (offset oi, anchor ai) from neighbour entry v
-__device__ __forceinline__ void sep32(const Args32 &A, const float4 &oi, const int ai[3], int v,
-                                      float &dx, float &dy, float &dz, float &wj) {
+__device__ __forceinline__ float fix_delta(int qi, int qj, int s, int Lq, float inv) {
+  unsigned d = (unsigned)qi - (unsigned)qj - (unsigned)(s * Lq);
+  return (float)(int)d * inv;
+}
+
+// separation of site i (record oi) from neighbour entry v; wj = F'(j)
+__device__ __forceinline__ void sep32(const Args32 &A, const int4 &oi, int v, float &dx, float &dy, float &dz,
+                                      float &wj) {
   int j = v >> IMG_BITS, code = v & ((1 << IMG_BITS) - 1);
-  float4 oj = A.pos[j];
-  int aj[3];
-  unpack_anchor(A.G, A.anc[j], aj);
+  int4 oj = __ldg(A.pos + j);
   int s[3] = {0, 0, 0};
   if (code != IMG_ZERO) img_decode(code, s[0], s[1], s[2]);
-  dx = (oi.x - oj.x) + (float)(ai[0] - aj[0] - s[0] * A.G.n[0]) * (float)CELL - (float)s[0] * A.G.r[0];
-  dy = (oi.y - oj.y) + (float)(ai[1] - aj[1] - s[1] * A.G.n[1]) * (float)CELL - (float)s[1] * A.G.r[1];
-  dz = (oi.z - oj.z) + (float)(ai[2] - aj[2] - s[2] * A.G.n[2]) * (float)CELL - (float)s[2] * A.G.r[2];
-  wj = oj.w;
+  dx = fix_delta(oi.x, oj.x, s[0], A.G.Lq[0], A.G.inv);
+  dy = fix_delta(oi.y, oj.y, s[1], A.G.Lq[1], A.G.inv);
+  dz = fix_delta(oi.z, oj.z, s[2], A.G.Lq[2], A.G.inv);
+  wj = __int_as_float(oj.w);
 }
 
 template <class F>
-__device__ __forceinline__ void for_each32(const Args32 &A, int i, const float4 &oi, const int ai[3], F &&f) {
+__device__ __forceinline__ void for_each32(const Args32 &A, int i, const int4 &oi, F &&f) {
   int n = A.num[i];
   const int *nb = A.nbr + i;
   int k = 0;
@@ -111,16 +103,16 @@ __device__ __forceinline__ void for_each32(const Args32 &A, int i, const float4 
     int v0 = nb[(size_t)k * A.nsi], v1 = nb[(size_t)(k + 1) * A.nsi];
     int v2 = nb[(size_t)(k + 2) * A.nsi], v3 = nb[(size_t)(k + 3) * A.nsi];
     float d[4][4];
-    sep32(A, oi, ai, v0, d[0][0], d[0][1], d[0][2], d[0][3]);
-    sep32(A, oi, ai, v1, d[1][0], d[1][1], d[1][2], d[1][3]);
-    sep32(A, oi, ai, v2, d[2][0], d[2][1], d[2][2], d[2][3]);
-    sep32(A, oi, ai, v3, d[3][0], d[3][1], d[3][2], d[3][3]);
+    sep32(A, oi, v0, d[0][0], d[0][1], d[0][2], d[0][3]);
+    sep32(A, oi, v1, d[1][0], d[1][1], d[1][2], d[1][3]);
+    sep32(A, oi, v2, d[2][0], d[2][1], d[2][2], d[2][3]);
+    sep32(A, oi, v3, d[3][0], d[3][1], d[3][2], d[3][3]);
 #pragma unroll
     for (int u = 0; u < 4; u++) f(d[u][0], d[u][1], d[u][2], d[u][3]);
   }
   for (; k < n; k++) {
     float dx, dy, dz, wj;
-    sep32(A, oi, ai, nb[(size_t)k * A.nsi], dx, dy, dz, wj);
+    sep32(A, oi, nb[(size_t)k * A.nsi], dx, dy, dz, wj);
     f(dx, dy, dz, wj);
   }
 }
@@ -165,10 +157,7 @@ __device__ __forceinline__ void finish32(const Args32 &A, int i, bool valid, con
   if (ev) block_reduce_store<7>(red, A.partial);
 }
 
-__device__ __forceinline__ void site_frame(const Args32 &A, int i, float4 &oi, int ai[3]) {
-  oi = A.pos[i];
-  unpack_anchor(A.G, A.anc[i], ai);
-}
+__device__ __forceinline__ void site_frame(const Args32 &A, int i, int4 &oi) { oi = __ldg(A.pos + i); }
 
 // ---------------------------------------------------------------------- LJ
 
@@ -182,10 +171,9 @@ __global__ void __launch_bounds__(128, EV ? 4 : 8) k_lj32(Args32 A, Lj32 P) {
   bool valid = i < A.nsi;
   float fi[3] = {0, 0, 0}, esum = 0.f, vsum[6] = {0, 0, 0, 0, 0, 0};
   if (valid) {
-    float4 oi;
-    int ai[3];
-    site_frame(A, i, oi, ai);
-    for_each32(A, i, oi, ai, [&](float dx, float dy, float dz, float) {
+    int4 oi;
+    site_frame(A, i, oi);
+    for_each32(A, i, oi, [&](float dx, float dy, float dz, float) {
       float rsq = dx * dx + dy * dy + dz * dz;
       if (rsq < P.cutsq) {
         float r2inv = 1.0f / rsq;
@@ -211,8 +199,10 @@ __global__ void __launch_bounds__(128, EV ? 4 : 8) k_lj32(Args32 A, Lj32 P) {
 
 // --------------------------------------------------------------------- EAM
 
+// rz: per r-knot m the rhor value coefficients at [2m] and the z2r ones at
+// [2m+1], one 32-byte record; derivatives as in the FP64 kernels.
 struct Eam32 {
-  const float4 *rhor_val, *rhor_der, *z2r_val, *z2r_der, *frho_val, *frho_der;
+  const float4 *rz, *frho_val, *frho_der;
   float rdr, rdrho, rhomax, cutforcesq;
   int nr, nrho;
 };
@@ -235,14 +225,13 @@ __device__ __forceinline__ float fp32_of(const Eam32 &T, float rho, float *phi) 
 }
 
 __global__ void __launch_bounds__(128, 8) k_eam_rho32(Args32 A, Eam32 T, double *rho_out, double *phi_site,
-                                                      float4 *pos_w) {
+                                                      int4 *pos_w) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= A.nsi) return;
-  float4 oi;
-  int ai[3];
-  site_frame(A, i, oi, ai);
+  int4 oi;
+  site_frame(A, i, oi);
   float rho = 0.f;
-  for_each32(A, i, oi, ai, [&](float dx, float dy, float dz, float) {
+  for_each32(A, i, oi, [&](float dx, float dy, float dz, float) {
     float rsq = dx * dx + dy * dy + dz * dz;
     if (rsq < T.cutforcesq) {
       float p = sqrtf(rsq) * T.rdr + 1.0f;
@@ -250,7 +239,7 @@ __global__ void __launch_bounds__(128, 8) k_eam_rho32(Args32 A, Eam32 T, double 
       m = max(1, min(m, T.nr - 1));
       p -= (float)m;
       p = fminf(p, 1.0f);
-      float4 c = T.rhor_val[m];
+      float4 c = __ldg(T.rz + 2 * m);
       rho += ((c.x * p + c.y) * p + c.z) * p + c.w;
     }
   });
@@ -262,21 +251,22 @@ __global__ void __launch_bounds__(128, 8) k_eam_rho32(Args32 A, Eam32 T, double 
   rho_out[slot] = rho;
   float phi = 0.f;
   float fp = fp32_of(T, rho, A.eflag ? &phi : nullptr);
-  pos_w[i].w = fp;
+  pos_w[i].w = __float_as_int(fp);
   if (A.eflag) phi_site[i] = phi;
 }
 
-__global__ void k_eam_site_fp32(float4 *pos, const int *act_gid, int nact, int base, int na,
+__global__ void k_eam_site_fp32(int4 *pos, const int *act_gid, const int *nact_dev, int base, int na,
                                 const double *rho, Eam32 T) {
-  int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= nact) return;
-  int gid = act_gid[k];
-  int e = gid / NU, u = gid % NU;
-  const double *rn = rho + na + 8 * (size_t)e;
-  double r = 0.0;
+  const int nact = *nact_dev;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nact; k += gridDim.x * blockDim.x) {
+    int gid = act_gid[k];
+    int e = gid / NU, u = gid % NU;
+    const double *rn = rho + na + 8 * (size_t)e;
+    double r = 0.0;
 #pragma unroll
-  for (int n = 0; n < NPE; n++) r += shape_val(u, n) * rn[n];
-  pos[base + k].w = fp32_of(T, (float)r, nullptr);
+    for (int n = 0; n < NPE; n++) r += shape_val(u, n) * rn[n];
+    pos[base + k].w = __float_as_int(fp32_of(T, (float)r, nullptr));
+  }
 }
 
 template <bool EV>
@@ -286,11 +276,10 @@ __global__ void __launch_bounds__(128, EV ? 4 : 8) k_eam_force32(Args32 A, Eam32
   float fi[3] = {0, 0, 0}, esum = 0.f, vsum[6] = {0, 0, 0, 0, 0, 0};
   double eemb_site = 0.0, eemb_global = 0.0;
   if (valid) {
-    float4 oi;
-    int ai[3];
-    site_frame(A, i, oi, ai);
-    const float fpi = oi.w;
-    for_each32(A, i, oi, ai, [&](float dx, float dy, float dz, float fpj) {
+    int4 oi;
+    site_frame(A, i, oi);
+    const float fpi = __int_as_float(oi.w);
+    for_each32(A, i, oi, [&](float dx, float dy, float dz, float fpj) {
       float rsq = dx * dx + dy * dy + dz * dz;
       if (rsq < T.cutforcesq) {
         float recip = rsqrtf(rsq);
@@ -300,11 +289,10 @@ __global__ void __launch_bounds__(128, EV ? 4 : 8) k_eam_force32(Args32 A, Eam32
         m = max(1, min(m, T.nr - 1));
         p -= (float)m;
         p = fminf(p, 1.0f);
-        float4 rd = T.rhor_der[m];
-        float rhop = (rd.x * p + rd.y) * p + rd.z;
-        float4 zd = T.z2r_der[m];
-        float4 zv = T.z2r_val[m];
-        float z2p = (zd.x * p + zd.y) * p + zd.z;
+        float4 rv, zv;
+        ldg256(T.rz + 2 * m, rv, zv);
+        float rhop = ((3.0f * rv.x * p + 2.0f * rv.y) * p + rv.z) * T.rdr;
+        float z2p = ((3.0f * zv.x * p + 2.0f * zv.y) * p + zv.z) * T.rdr;
         float z2 = ((zv.x * p + zv.y) * p + zv.z) * p + zv.w;
         float phi = z2 * recip;
         float phip = z2p * recip - phi * recip;
@@ -342,20 +330,19 @@ __global__ void k_reduce_partials32(const double *partial, int nblocks, double *
   if (lane == 0) out[k] = s;
 }
 
-AnchorGrid make_anchor_grid(const Ctx &c) {
-  AnchorGrid G;
-  int off = 0;
+FixGrid make_fix_grid(const Ctx &c) {
+  FixGrid G;
+  double lmax = std::max(c.prd[0], std::max(c.prd[1], c.prd[2]));
+  int k = 24;
+  while (k > 8 && (lmax + 64.0) * std::ldexp(1.0, k) > 2147483000.0) k--;
+  if ((lmax + 64.0) * std::ldexp(1.0, k) > 2147483000.0)
+    throw Error(CACB200_EINVAL, "box too large for the mixed-precision fixed-point positions");
+  G.scale = std::ldexp(1.0, k);
+  G.inv = std::ldexp(1.0f, -k);
   for (int d = 0; d < 3; d++) {
     G.lo[d] = c.boxlo[d];
-    G.n[d] = (int)std::ceil(c.prd[d] / CELL);
-    G.r[d] = (float)(c.prd[d] - CELL * G.n[d]);
-    int need = G.n[d] + 2 * BIAS, bits = 1;
-    while ((1 << bits) < need) bits++;
-    G.bits[d] = bits;
-    G.shift[d] = off;
-    off += bits;
+    G.Lq[d] = (int)std::llround(c.prd[d] * G.scale);
   }
-  if (off > 32) throw Error(CACB200_EINVAL, "box too large for the mixed-precision anchor word");
   return G;
 }
 
@@ -370,30 +357,26 @@ void mixed_tables(Ctx &c) {
     dst.reserve(n + 1);
     stream_copy(c, dst.p, g.data(), sizeof(float4) * (n + 1), cudaMemcpyHostToDevice);
   };
-  conv(c.rhor_val, c.rhor_val32, c.pp.nr);
-  conv(c.rhor_der, c.rhor_der32, c.pp.nr);
-  conv(c.z2r_val, c.z2r_val32, c.pp.nr);
-  conv(c.z2r_der, c.z2r_der32, c.pp.nr);
+  conv(c.rz, c.rz32, 2 * c.pp.nr + 1);
   conv(c.frho_val, c.frho_val32, c.pp.nrho);
   conv(c.frho_der, c.frho_der32, c.pp.nrho);
 }
 
 void pair_compute_mixed(Ctx &c, int eflag, int vflag) {
   const int nsi = c.nsite_i();
-  const int ns = c.nsite_s();
+  const long ns = (long)nsi + (long)c.ne * NU;   // capacity: every lattice site active
   const int T = 128;
   const int nb = std::max(nblk(nsi, T), 1);
-  AnchorGrid G = make_anchor_grid(c);
-  c.pos32.reserve(std::max(ns, 1));
-  c.anc32.reserve(std::max(ns, 1));
+  FixGrid G = make_fix_grid(c);
+  c.pos32.reserve(std::max(ns, 1L));
   c.overflow.reserve(8);
   {
     KernelTimer t(c, "pack32");
-    k_pack32<<<nblk(ns, 256), 256, 0, c.stream>>>(c.xs.p, ns, G, c.pos32.p, c.anc32.p, c.overflow.p + 6);
+    k_pack32<<<stride_grid(ns, 256), 256, 0, c.stream>>>(c.xs.p, nsi, c.dev_nact.p, G, c.pos32.p,
+                                                         c.overflow.p + 6);
   }
   Args32 A;
   A.pos = c.pos32.p;
-  A.anc = c.anc32.p;
   A.nbr = c.nbr_full.p;
   A.num = c.num_full.p;
   A.na = c.na;
@@ -436,10 +419,7 @@ void pair_compute_mixed(Ctx &c, int eflag, int vflag) {
       c.have_mixed_tables = true;
     }
     Eam32 Tb;
-    Tb.rhor_val = c.rhor_val32.p;
-    Tb.rhor_der = c.rhor_der32.p;
-    Tb.z2r_val = c.z2r_val32.p;
-    Tb.z2r_der = c.z2r_der32.p;
+    Tb.rz = c.rz32.p;
     Tb.frho_val = c.frho_val32.p;
     Tb.frho_der = c.frho_der32.p;
     Tb.rdr = (float)c.pp.rdr;
@@ -454,10 +434,10 @@ void pair_compute_mixed(Ctx &c, int eflag, int vflag) {
       KernelTimer t(c, "eam_rho32");
       k_eam_rho32<<<nb, T, 0, c.stream>>>(A, Tb, c.rho.p, c.phi_site.p, c.pos32.p);
     }
-    if (c.nact) {
+    if (c.ne) {
       KernelTimer t(c, "eam_site_fp32");
-      k_eam_site_fp32<<<nblk(c.nact, 256), 256, 0, c.stream>>>(c.pos32.p, c.act_gid.p, c.nact, c.na + NG * c.ne,
-                                                               c.na, c.rho.p, Tb);
+      k_eam_site_fp32<<<stride_grid((long)c.ne * NU, 256), 256, 0, c.stream>>>(
+          c.pos32.p, c.act_gid.p, c.dev_nact.p, c.na + NG * c.ne, c.na, c.rho.p, Tb);
     }
     {
       KernelTimer t(c, "eam_force32");
