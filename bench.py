@@ -66,7 +66,15 @@ def build_workload(name: str, seed: int):
         return gen.eam_small(seed=seed), "eam"
     if name == "eam_4m_strained":
         return gen.eam_4m_strained(seed=seed), "eam"
+    if name == "batch256":
+        return gen.replica_set(256, seed=11 + seed), "eam"
     raise SystemExit(f"unknown workload {name}")
+
+
+def totals(s):
+    """(atom+IP sites, atoms, elements) of a system or a list of replicas."""
+    items = s if isinstance(s, list) else [s]
+    return (sum(r.nsites for r in items), sum(r.natoms for r in items), sum(r.nelements for r in items))
 
 
 class ClockSampler:
@@ -145,27 +153,58 @@ def dist_init():
 
 # ----------------------------------------------------------------- reference arm
 
+def reference_input(d: str, s, pair: str, steps: int, warmup: int) -> None:
+    from cac_b200 import gen
+    gen.write_data(s, os.path.join(d, "data.cac"))
+    lines = ["units metal", "dimension 3", "boundary p p p", "atom_style atomic",
+             "element_style cac 8 1 wscale 1 1 1 1", "read_data data.cac"]
+    if pair == "eam":
+        gen.write_setfl(gen.EamParams(), os.path.join(d, "cu.setfl"))
+        lines += ["pair_style eam/alloy", "pair_coeff * * cu.setfl Cu"]
+    else:
+        lines += ["pair_style lj/cut 5.5", "pair_coeff 1 1 0.4093 2.338"]
+    lines += ["neighbor 1.0 bin", "neigh_modify every 10 delay 0 check no", "timestep 0.001",
+              "fix 1 all nve", "thermo 1000000"]
+    if warmup > 0:
+        lines.append(f"run {warmup}")
+    lines.append(f"run {steps}")
+    with open(os.path.join(d, "in.cac"), "w") as f:
+        f.write("\n".join(lines) + "\n")
+
+
+def run_reference_many(systems, pair: str, steps: int, warmup: int, procs: int, timeout: float = 1800.0):
+    """Independent replicas as concurrent single-rank reference processes, at
+    most `procs` at a time; returns (sites x steps / s summed over the
+    processes, replicas timed)."""
+    rate = 0.0
+    with tempfile.TemporaryDirectory() as root:
+        pending = list(enumerate(systems))
+        running = []
+        while pending or running:
+            while pending and len(running) < procs:
+                k, s = pending.pop(0)
+                d = os.path.join(root, f"r{k}")
+                os.makedirs(d)
+                reference_input(d, s, pair, steps, warmup)
+                pr = subprocess.Popen([REF_EXE, "-in", "in.cac"], cwd=d, stdout=subprocess.PIPE,
+                                      stderr=subprocess.STDOUT, text=True)
+                running.append((s, pr))
+            s, pr = running.pop(0)
+            out, _ = pr.communicate(timeout=timeout)
+            if pr.returncode != 0:
+                raise RuntimeError("reference run failed: " + out[-2000:])
+            loops = re.findall(r"Loop time of ([0-9.eE+-]+) on", out)
+            rate += s.nsites * steps / float(loops[-1])
+    return rate, len(systems)
+
+
 def run_reference(workload: str, steps: int, warmup: int, seed: int = 2, timeout: float = 1800.0):
     """Time the reference executable: `run warmup` then `run steps`; returns
     (units per step, loop seconds of the timed run, log)."""
     from cac_b200 import gen
     s, pair = build_workload(workload, seed)
     with tempfile.TemporaryDirectory() as d:
-        gen.write_data(s, os.path.join(d, "data.cac"))
-        lines = ["units metal", "dimension 3", "boundary p p p", "atom_style atomic",
-                 "element_style cac 8 1 wscale 1 1 1 1", "read_data data.cac"]
-        if pair == "eam":
-            gen.write_setfl(gen.EamParams(), os.path.join(d, "cu.setfl"))
-            lines += ["pair_style eam/alloy", "pair_coeff * * cu.setfl Cu"]
-        else:
-            lines += ["pair_style lj/cut 5.5", "pair_coeff 1 1 0.4093 2.338"]
-        lines += ["neighbor 1.0 bin", "neigh_modify every 10 delay 0 check no", "timestep 0.001",
-                  "fix 1 all nve", "thermo 1000000"]
-        if warmup > 0:
-            lines.append(f"run {warmup}")
-        lines.append(f"run {steps}")
-        with open(os.path.join(d, "in.cac"), "w") as f:
-            f.write("\n".join(lines) + "\n")
+        reference_input(d, s, pair, steps, warmup)
         r = subprocess.run([REF_EXE, "-in", "in.cac"], cwd=d, capture_output=True, text=True, timeout=timeout)
         if r.returncode != 0:
             raise RuntimeError("reference run failed: " + r.stdout[-2000:] + r.stderr[-2000:])
@@ -179,17 +218,32 @@ def reference_arm(args, rank, ws):
     if not os.path.exists(REF_EXE):
         print(json.dumps({"impl": "reference", "unavailable": "reference executable oracle/_ref/cac was not built"}))
         return
-    units, secs, _ = run_reference(args.workload, args.steps, args.warmup)
-    value = units * args.steps / secs
+    cores, kind_sample = 1, f"full workload, run {args.warmup} then run {args.steps} steps; rate from Loop time"
+    par = "1 core (reference CPU path, single MPI rank)"
+    if args.workload.startswith("batch"):
+        systems, pair = build_workload(args.workload, 2)
+        cores = min(os.cpu_count() or 1, len(systems))
+        sample = systems[:cores]
+        value, nrep = run_reference_many(sample, pair, args.steps, args.warmup, cores)
+        units = totals(systems)[0]
+        secs = units * args.steps / value
+        kind_sample = (f"{nrep} of the {len(systems)} replicas as concurrent single-rank processes on {cores} "
+                       f"cores, run {args.warmup} then run {args.steps} steps each; rate = sum over processes "
+                       f"of sites x steps / Loop time")
+        par = f"{cores} concurrent single-rank reference processes (one replica each)"
+    else:
+        units, secs, _ = run_reference(args.workload, args.steps, args.warmup)
+        value = units * args.steps / secs
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * secs / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded generator)",
-        "config": {"workload": args.workload, "sites": units, "pair": "eam/alloy" if "eam" in args.workload else "lj/cut",
-                   "precision": "fp64", "parallelism": "1 core (reference CPU path, single MPI rank)"},
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "reference",
-                         "sample": f"full workload, run {args.warmup} then run {args.steps} steps; rate from Loop time"},
+        "config": {"workload": args.workload, "sites": units,
+                   "pair": "lj/cut" if args.workload.startswith("lj") else "eam/alloy",
+                   "precision": "fp64", "parallelism": par},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference",
+                         "sample": kind_sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
@@ -219,9 +273,13 @@ def b200_arm(args, rank, local, ws, dist):
 
     seed = 2 + rank
     s, pair = build_workload(args.workload, seed)
-    units = s.nsites
+    units, natoms, nelements = totals(s)
+    batch = isinstance(s, list)
     eng = api.Engine(local)
-    eng.upload(s)
+    if batch:
+        eng.upload_batch(s)
+    else:
+        eng.upload(s)
     tmp = tempfile.mkdtemp()
     if pair == "eam":
         p = os.path.join(tmp, "cu.setfl")
@@ -294,10 +352,10 @@ def b200_arm(args, rank, local, ws, dist):
 
     # end to end through the C ABI with pinned host buffers: every step copies the
     # state in (x, v, nodes), runs one step, and reads the state back
-    x_h = torch.empty((s.natoms, 3), dtype=torch.float64).pin_memory().numpy()
-    v_h = torch.empty((s.natoms, 3), dtype=torch.float64).pin_memory().numpy()
-    nx_h = torch.empty((s.nelements, 8, 3), dtype=torch.float64).pin_memory().numpy()
-    nv_h = torch.empty((s.nelements, 8, 3), dtype=torch.float64).pin_memory().numpy()
+    x_h = torch.empty((natoms, 3), dtype=torch.float64).pin_memory().numpy()
+    v_h = torch.empty((natoms, 3), dtype=torch.float64).pin_memory().numpy()
+    nx_h = torch.empty((nelements, 8, 3), dtype=torch.float64).pin_memory().numpy()
+    nv_h = torch.empty((nelements, 8, 3), dtype=torch.float64).pin_memory().numpy()
     x0, v0, nx0, nv0 = eng.state()
     x_h[:] = x0
     v_h[:] = v0
@@ -318,17 +376,25 @@ def b200_arm(args, rank, local, ws, dist):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_s = float(t.item())
     e2e_value = units * k_e2e * ws / e2e_s
-    bytes_state = 8 * (6 * s.natoms + 48 * s.nelements)
+    bytes_state = 8 * (6 * natoms + 48 * nelements)
 
     # CPU baseline: the reference on a bounded sample of the same workload
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
         if os.path.exists(REF_EXE):
             try:
-                cu, secs, _ = run_reference(args.workload, 10, 0)
-                cpu = {"value": cu * 10 / secs, "unit": UNIT, "cores": 1, "kind": "reference",
-                       "sample": "reference executable on the same workload, 10 steps incl. one list rebuild, "
-                                 "rate from its Loop time (setup excluded)"}
+                if batch:
+                    cores = min(os.cpu_count() or 1, len(s))
+                    rate, nrep = run_reference_many(s[:cores], pair, 10, 0, cores)
+                    cpu = {"value": rate, "unit": UNIT, "cores": cores, "kind": "reference",
+                           "sample": f"{nrep} of the {len(s)} replicas as concurrent single-rank reference "
+                                     f"processes, 10 steps each incl. one list rebuild; rate = sum of sites x "
+                                     f"steps / Loop time"}
+                else:
+                    cu, secs, _ = run_reference(args.workload, 10, 0)
+                    cpu = {"value": cu * 10 / secs, "unit": UNIT, "cores": 1, "kind": "reference",
+                           "sample": "reference executable on the same workload, 10 steps incl. one list "
+                                     "rebuild, rate from its Loop time (setup excluded)"}
             except Exception as ex:  # reported, not fatal
                 cpu = {"value": None, "unit": UNIT, "cores": 1, "kind": "reference", "sample": f"failed: {ex}"}
         else:
@@ -341,7 +407,8 @@ def b200_arm(args, rank, local, ws, dist):
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.form == "fp64" else "f32/f64",
             "data": "synthetic (seeded generator; no dataset exists for this path)",
-            "config": {"workload": args.workload, "sites": units, "atoms": s.natoms, "elements": s.nelements,
+            "config": {"workload": args.workload, "sites": units, "atoms": natoms, "elements": nelements,
+                       "replicas": len(s) if batch else 1,
                        "pair": "eam/alloy" if pair == "eam" else "lj/cut", "precision": args.form,
                        "rebuild_every": 10, "parallelism": f"replicas x{ws} (no data-path collective)",
                        "l2": "working set larger than L2 (site table + lists > 126 MB)"},

@@ -45,6 +45,11 @@ SIGNATURES = [
     ("cacb200_stream", C.c_void_p, [C.c_void_p]),
     ("cacb200_set_precision", C.c_int, [C.c_void_p, C.c_int]),
     ("cacb200_upload_system", C.c_int, [C.c_void_p, _dp, _dp, C.c_int, _dp, _dp, C.c_int, _dp, _dp, C.c_double]),
+    ("cacb200_upload_batch", C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int), _dp, _dp,
+                                       _dp, _dp, _dp, _dp, C.c_double]),
+    ("cacb200_replica_energy", C.c_int, [C.c_void_p, _dp]),
+    ("cacb200_set_graphs", C.c_int, [C.c_void_p, C.c_int]),
+    ("cacb200_graph_launches", C.c_int, [C.c_void_p, C.POINTER(C.c_longlong)]),
     ("cacb200_set_state", C.c_int, [C.c_void_p, _dp, _dp, _dp, _dp]),
     ("cacb200_get_state", C.c_int, [C.c_void_p, _dp, _dp, _dp, _dp]),
     ("cacb200_get_forces", C.c_int, [C.c_void_p, _dp, _dp, _dp]),
@@ -169,9 +174,46 @@ class Engine:
         lo = np.ascontiguousarray(system.boxlo, dtype=np.float64)
         hi = np.ascontiguousarray(system.boxhi, dtype=np.float64)
         self.na, self.ne = x.shape[0], nx.shape[0]
+        self.rep_na, self.rep_ne = np.array([self.na]), np.array([self.ne])
         self._check(self.lib.cacb200_upload_system(self.h, _p(lo), _p(hi), self.na, _p(x), _p(v),
                                                    self.ne, _p(nx), _p(nv), float(system.mass)),
                     "upload_system")
+
+    def upload_batch(self, systems) -> None:
+        """Upload independent replicas (one periodic box each) as one batch."""
+        if not systems:
+            raise CacB200Error("empty batch")
+        mass = float(systems[0].mass)
+        if any(float(s.mass) != mass for s in systems):
+            raise CacB200Error("replicas of a batch share one mass")
+        cat = lambda key, shape: np.ascontiguousarray(
+            np.concatenate([np.asarray(getattr(s, key), dtype=np.float64).reshape(shape) for s in systems]))
+        x, v = cat("x", (-1, 3)), cat("v", (-1, 3))
+        nx, nv = cat("nodex", (-1, 8, 3)), cat("nodev", (-1, 8, 3))
+        na = np.array([s.x.shape[0] for s in systems], dtype=np.int32)
+        ne = np.array([s.nodex.shape[0] for s in systems], dtype=np.int32)
+        lo = np.ascontiguousarray(np.stack([np.asarray(s.boxlo, dtype=np.float64) for s in systems]))
+        hi = np.ascontiguousarray(np.stack([np.asarray(s.boxhi, dtype=np.float64) for s in systems]))
+        self.na, self.ne = int(na.sum()), int(ne.sum())
+        self.rep_na, self.rep_ne = na.copy(), ne.copy()
+        ip = C.POINTER(C.c_int)
+        self._check(self.lib.cacb200_upload_batch(self.h, len(systems), na.ctypes.data_as(ip),
+                                                  ne.ctypes.data_as(ip), _p(lo), _p(hi), _p(x), _p(v),
+                                                  _p(nx), _p(nv), mass), "upload_batch")
+
+    def replica_energy(self) -> np.ndarray:
+        n = len(getattr(self, "rep_na", [0]))
+        out = np.zeros(n)
+        self._check(self.lib.cacb200_replica_energy(self.h, _p(out)), "replica_energy")
+        return out
+
+    def graphs(self, enable: bool) -> None:
+        self._check(self.lib.cacb200_set_graphs(self.h, 1 if enable else 0), "set_graphs")
+
+    def graph_launches(self) -> int:
+        n = C.c_longlong()
+        self._check(self.lib.cacb200_graph_launches(self.h, C.byref(n)), "graph_launches")
+        return n.value
 
     def set_precision(self, form: int) -> None:
         self._check(self.lib.cacb200_set_precision(self.h, form), "set_precision")

@@ -59,6 +59,8 @@ Ctx::Ctx(int dev) : device(dev) {
 }
 
 Ctx::~Ctx() {
+  if (g_build) cudaGraphExecDestroy(g_build);
+  if (g_steps) cudaGraphExecDestroy(g_steps);
   if (stream) {
     cudaStreamSynchronize(stream);
     auto &pend = pending_for(*this);
@@ -85,18 +87,50 @@ KernelTimer::~KernelTimer() {
 
 namespace {
 
-void upload_system(Ctx &c, const double lo[3], const double hi[3], int na, const double *x,
-                   const double *v, int ne, const double *nodex, const double *nodev, double mass) {
-  if (na < 0 || ne < 0 || (na > 0 && (!x || !v)) || (ne > 0 && (!nodex || !nodev)))
+// A system of nrep independent replicas stored one after another (a single
+// system is nrep = 1).  Each replica has its own periodic box; atoms and
+// elements keep the order of the input arrays.
+void upload_system(Ctx &c, int nrep, const int *rna, const int *rne, const double *lo, const double *hi,
+                   const double *x, const double *v, const double *nodex, const double *nodev, double mass) {
+  if (nrep < 1 || !rna || !rne || !lo || !hi) throw Error(CACB200_EINVAL, "invalid replica description");
+  long na_l = 0, ne_l = 0;
+  for (int r = 0; r < nrep; r++) {
+    if (rna[r] < 0 || rne[r] < 0) throw Error(CACB200_EINVAL, "negative atom or element count");
+    na_l += rna[r];
+    ne_l += rne[r];
+    for (int d = 0; d < 3; d++)
+      if (!(hi[3 * r + d] > lo[3 * r + d])) throw Error(CACB200_EINVAL, "empty box");
+  }
+  // list entries pack a site index in 26 bits: atoms and Gauss points must
+  // fit (referenced lattice sites are checked at each rebuild), and element
+  // lattice-site ids e * 729 + u must fit in 30 bits during the build
+  if (na_l + (long)NG * ne_l >= (1L << 26) || ne_l * NU >= (1L << 30))
+    throw Error(CACB200_EINVAL, "system too large for 26-bit site indices");
+  const int na = (int)na_l, ne = (int)ne_l;
+  if ((na > 0 && (!x || !v)) || (ne > 0 && (!nodex || !nodev)))
     throw Error(CACB200_EINVAL, "invalid system arrays");
   if (!(mass > 0.0)) throw Error(CACB200_EINVAL, "mass must be positive");
-  if ((long)na + (long)NG * ne + (long)ne * NU >= (1L << 26))
-    throw Error(CACB200_EINVAL, "system too large for 26-bit site indices");
   for (int d = 0; d < 3; d++) {
-    if (!(hi[d] > lo[d])) throw Error(CACB200_EINVAL, "empty box");
     c.boxlo[d] = lo[d];
     c.boxhi[d] = hi[d];
     c.prd[d] = hi[d] - lo[d];
+  }
+  c.nrep = nrep;
+  c.rep_na.assign(rna, rna + nrep);
+  c.rep_ne.assign(rne, rne + nrep);
+  c.rep_aoff.assign(nrep, 0);
+  c.rep_eoff.assign(nrep, 0);
+  c.rep_h.assign(nrep, Rep{});
+  for (int r = 0; r < nrep; r++) {
+    if (r) {
+      c.rep_aoff[r] = c.rep_aoff[r - 1] + rna[r - 1];
+      c.rep_eoff[r] = c.rep_eoff[r - 1] + rne[r - 1];
+    }
+    for (int d = 0; d < 3; d++) {
+      c.rep_h[r].b.lo[d] = lo[3 * r + d];
+      c.rep_h[r].b.hi[d] = hi[3 * r + d];
+      c.rep_h[r].b.L[d] = hi[3 * r + d] - lo[3 * r + d];
+    }
   }
   c.na = na;
   c.ne = ne;
@@ -106,6 +140,7 @@ void upload_system(Ctx &c, const double lo[3], const double hi[3], int na, const
   c.lists_valid = false;
   c.have_half = false;
   c.planned = false;
+  c.gen++;
   c.step = c.last_build_step = 0;
   c.xs.release();
   // site table at full capacity: atoms, Gauss points and every lattice site
@@ -124,6 +159,22 @@ void upload_system(Ctx &c, const double lo[3], const double hi[3], int na, const
   CACB200_CUDA(cudaMemsetAsync(c.gaussf.p, 0, sizeof(double) * std::max(24 * ne, 1), c.stream));
   CACB200_CUDA(cudaMemsetAsync(c.xs.p, 0, sizeof(double4) * c.xs.n, c.stream));
   c.have_system = true;
+  // replica of every i-site and element (batches)
+  if (nrep > 1) {
+    std::vector<int> sr(std::max(na + NG * ne, 1)), er(std::max(ne, 1));
+    for (int r = 0; r < nrep; r++) {
+      for (int i = 0; i < rna[r]; i++) sr[c.rep_aoff[r] + i] = r;
+      for (int e = 0; e < rne[r]; e++) {
+        int eg = c.rep_eoff[r] + e;
+        er[eg] = r;
+        for (int g = 0; g < NG; g++) sr[na + NG * eg + g] = r;
+      }
+    }
+    c.site_rep.reserve(sr.size());
+    c.elem_rep.reserve(er.size());
+    stream_copy(c, c.site_rep.p, sr.data(), sizeof(int) * sr.size(), cudaMemcpyHostToDevice);
+    stream_copy(c, c.elem_rep.p, er.data(), sizeof(int) * er.size(), cudaMemcpyHostToDevice);
+  }
   // positions/velocities
   std::vector<double4> hx(std::max(na, 1));
   for (int i = 0; i < na; i++) hx[i] = make_double4(x[3 * i], x[3 * i + 1], x[3 * i + 2], 0.0);
@@ -136,6 +187,20 @@ void upload_system(Ctx &c, const double lo[3], const double hi[3], int na, const
     stream_copy(c, c.nodev.p, nodev, sizeof(double) * 24 * ne, cudaMemcpyHostToDevice);
   }
   CACB200_CUDA(cudaStreamSynchronize(c.stream));
+}
+
+// Energy of each replica from the per-site energies of the last evaluation:
+// atoms count their own, node Gauss points theirs times the node weight (the
+// global sum's split, per replica).  One block per replica, fixed order.
+__global__ void k_replica_energy(const double *eatom, const double *enode, const int *aoff, const int *rna,
+                                 const int *eoff, const int *rne, double node_scale, double *out) {
+  int r = blockIdx.x;
+  double s = 0.0;
+  for (int i = threadIdx.x; i < rna[r]; i += blockDim.x) s += eatom[aoff[r] + i];
+  double t = 0.0;
+  for (int k = threadIdx.x; k < 8 * rne[r]; k += blockDim.x) t += enode[8 * (size_t)eoff[r] + k];
+  double v[1] = {s + node_scale * t};
+  block_reduce_store<1>(v, out);
 }
 
 __global__ void k_pack_x(const double *x, double4 *xs, int n) {
@@ -250,17 +315,108 @@ void setup(Ctx &c) {
   forces(c, CACB200_ENERGY_GLOBAL, CACB200_VIRIAL_GLOBAL);
 }
 
+void drop_graphs(Ctx &c) {
+  if (c.g_build) cudaGraphExecDestroy(c.g_build);
+  if (c.g_steps) cudaGraphExecDestroy(c.g_steps);
+  c.g_build = c.g_steps = nullptr;
+  c.graph_gen = -1;
+}
+
+// Record what `body` queues on the context stream as an executable graph.
+template <class F>
+cudaGraphExec_t capture(Ctx &c, F &&body) {
+  cudaGraph_t g = nullptr;
+  CACB200_CUDA(cudaStreamBeginCapture(c.stream, cudaStreamCaptureModeRelaxed));
+  try {
+    body();
+  } catch (...) {
+    cudaStreamEndCapture(c.stream, &g);
+    if (g) cudaGraphDestroy(g);
+    cudaGetLastError();
+    throw;
+  }
+  CACB200_CUDA(cudaStreamEndCapture(c.stream, &g));
+  cudaGraphExec_t x = nullptr;
+  cudaError_t e = cudaGraphInstantiate(&x, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) throw Error(CACB200_ECUDA, std::string("graph instantiation: ") + cudaGetErrorString(e));
+  return x;
+}
+
+// One rebuild cycle of `every` velocity-Verlet steps from two graph launches:
+// [half-kick + drift of the rebuild step, list rebuild], a check of the
+// rebuild's flag words (the one host wait of the cycle; an overflow is
+// repaired by a synchronous rebuild before any force uses the lists), then
+// [forces and second half-kick of that step, the every-1 steps that follow].
+void nve_cycle(Ctx &c, double dt) {
+  const int every = c.every;
+  if (c.graph_gen != c.gen || c.graph_dt != dt || c.graph_every != every || !c.g_build || !c.g_steps) {
+    drop_graphs(c);
+    // one eager evaluation first, so that every buffer and table the force
+    // path grows on first use exists before capture (it recomputes the
+    // forces of the current positions: the state does not change)
+    forces(c, 0, 0);
+    c.g_build = capture(c, [&] {
+      nve_initial(c, dt);
+      neigh_build_async(c, false);
+    });
+    c.g_steps = capture(c, [&] {
+      forces(c, 0, 0);
+      nve_final(c, dt);
+      for (int k = 1; k < every; k++) {
+        nve_initial(c, dt);
+        forces(c, 0, 0);
+        nve_final(c, dt);
+      }
+    });
+    c.graph_gen = c.gen;
+    c.graph_dt = dt;
+    c.graph_every = every;
+  }
+  CACB200_CUDA(cudaGraphLaunch(c.g_build, c.stream));
+  c.graph_launches++;
+  c.step++;
+  c.lists_valid = true;
+  c.nact_known = false;
+  if (neigh_check(c)) neigh_build(c, false);   // plan grew: rebuild once more, synchronously
+  c.last_build_step = c.step;
+  if (c.graph_gen == c.gen) {
+    CACB200_CUDA(cudaGraphLaunch(c.g_steps, c.stream));
+    c.graph_launches++;
+  } else {
+    forces(c, 0, 0);
+    nve_final(c, dt);
+    for (int k = 1; k < every; k++) {
+      nve_initial(c, dt);
+      forces(c, 0, 0);
+      nve_final(c, dt);
+    }
+  }
+  c.step += every - 1;
+}
+
 void run_nve(Ctx &c, int nsteps, double dt, int eflag, int vflag) {
   c.check_system();
   if (nsteps < 0) throw Error(CACB200_EINVAL, "negative step count");
   if (!c.lists_valid) setup(c);
-  for (int s = 1; s <= nsteps; s++) {
+  const bool graphs = c.graphs_enabled && c.every > 0 && !c.prof.enabled;
+  const bool want_ev = eflag || vflag;
+  int s = 1;
+  while (s <= nsteps) {
+    int left = nsteps - s + 1;
+    bool at_cycle = c.every > 0 && (c.step + 1 - c.last_build_step) % c.every == 0;
+    if (graphs && at_cycle && (left > c.every || (left == c.every && !want_ev))) {
+      nve_cycle(c, dt);
+      s += c.every;
+      continue;
+    }
     nve_initial(c, dt);
     c.step++;
     if (c.every > 0 && (c.step - c.last_build_step) % c.every == 0) build(c, false);
     bool last = (s == nsteps);
     forces(c, last ? eflag : 0, last ? vflag : 0);
     nve_final(c, dt);
+    s++;
   }
   CACB200_CUDA(cudaGetLastError());
 }
@@ -368,6 +524,7 @@ int cacb200_set_precision(cacb200_ctx *ctx, int form) {
   API_BEGIN
   if (form != CACB200_FP64 && form != CACB200_MIXED) throw Error(CACB200_EINVAL, "unknown precision form");
   c.precision = form;
+  c.gen++;
   API_END
 }
 
@@ -376,7 +533,51 @@ int cacb200_upload_system(cacb200_ctx *ctx, const double boxlo[3], const double 
                           const double *nodev, double mass) {
   API_BEGIN
   if (!boxlo || !boxhi) throw Error(CACB200_EINVAL, "box required");
-  upload_system(c, boxlo, boxhi, natoms, x, v, nelements, nodex, nodev, mass);
+  upload_system(c, 1, &natoms, &nelements, boxlo, boxhi, x, v, nodex, nodev, mass);
+  API_END
+}
+
+int cacb200_upload_batch(cacb200_ctx *ctx, int nreplicas, const int *natoms, const int *nelements,
+                         const double *boxlo, const double *boxhi, const double *x, const double *v,
+                         const double *nodex, const double *nodev, double mass) {
+  API_BEGIN
+  upload_system(c, nreplicas, natoms, nelements, boxlo, boxhi, x, v, nodex, nodev, mass);
+  API_END
+}
+
+int cacb200_replica_energy(cacb200_ctx *ctx, double *energy) {
+  API_BEGIN
+  c.check_system();
+  if (!energy) throw Error(CACB200_EINVAL, "null output array");
+  if (!c.have_peratom_e) throw Error(CACB200_ESTATE, "no per-site energies: evaluate with CACB200_ENERGY_ATOM");
+  std::vector<int> meta(4 * (size_t)c.nrep);
+  for (int r = 0; r < c.nrep; r++) {
+    meta[r] = c.rep_aoff[r];
+    meta[c.nrep + r] = c.rep_na[r];
+    meta[2 * c.nrep + r] = c.rep_eoff[r];
+    meta[3 * c.nrep + r] = c.rep_ne[r];
+  }
+  c.rep_meta.reserve(meta.size());
+  c.rep_energy.reserve(c.nrep);
+  stream_copy(c, c.rep_meta.p, meta.data(), sizeof(int) * meta.size(), cudaMemcpyHostToDevice);
+  k_replica_energy<<<c.nrep, 256, 0, c.stream>>>(c.eatom.p, c.enode.p, c.rep_meta.p, c.rep_meta.p + c.nrep,
+                                                 c.rep_meta.p + 2 * c.nrep, c.rep_meta.p + 3 * c.nrep,
+                                                 2.0 * c.escale_node_last, c.rep_energy.p);
+  CACB200_CUDA(cudaGetLastError());
+  stream_copy(c, energy, c.rep_energy.p, sizeof(double) * c.nrep, cudaMemcpyDeviceToHost);
+  API_END
+}
+
+int cacb200_set_graphs(cacb200_ctx *ctx, int enable) {
+  API_BEGIN
+  c.graphs_enabled = enable != 0;
+  if (!c.graphs_enabled) drop_graphs(c);
+  API_END
+}
+
+int cacb200_graph_launches(cacb200_ctx *ctx, long long *count) {
+  API_BEGIN
+  if (count) *count = c.graph_launches;
   API_END
 }
 
@@ -446,6 +647,7 @@ int cacb200_set_lj(cacb200_ctx *ctx, double epsilon, double sigma, double cut) {
   c.pp.offset = 0.0;
   c.lists_valid = false;
   c.planned = false;
+  c.gen++;
   API_END
 }
 
@@ -467,12 +669,14 @@ int cacb200_set_eam(cacb200_ctx *ctx, int nrho, double drho, int nr, double dr, 
   eam_tables(c, frho, rhor, z2r);
   c.lists_valid = false;
   c.planned = false;
+  c.gen++;
   API_END
 }
 
 int cacb200_set_nodal_energy_weight(cacb200_ctx *ctx, double w) {
   API_BEGIN
   c.nodal_energy_weight = w;
+  c.gen++;
   API_END
 }
 
@@ -483,6 +687,7 @@ int cacb200_set_neighbor(cacb200_ctx *ctx, double skin, int every) {
   c.every = every;
   c.lists_valid = false;
   c.planned = false;
+  c.gen++;
   API_END
 }
 

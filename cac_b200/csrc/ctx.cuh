@@ -74,6 +74,24 @@ struct Grid {
   int ncell;
 };
 
+// Orthogonal periodic box.
+struct BoxD {
+  double lo[3], hi[3], L[3];
+};
+
+// One replica of a batch (a single system is a batch of one): its box, its
+// two candidate grids and where their cells start in the batch-wide cell
+// numbering, and the element radius its grids were planned for.
+struct Rep {
+  BoxD b;
+  Grid ag, eg;
+  int abase, ebase;
+  double reach_budget;
+  double qscale[3];   // mixed form: fixed-point scale 2^k per dimension ...
+  float qinv[3];      // ... and 2^-k
+  int Lq[3];          // rint(L 2^k)
+};
+
 struct PairParams {
   int style = CACB200_PAIR_NONE;
   double cut = 0.0;          // force cutoff
@@ -115,8 +133,18 @@ struct Ctx {
   std::string last_error;
   int precision = CACB200_FP64;
 
-  // system
+  // system (a batch of nrep independent replicas, stored one after another:
+  // replica r owns atoms [rep_aoff[r], +rep_na[r]) and elements
+  // [rep_eoff[r], +rep_ne[r]); boxlo/boxhi/prd are replica 0's box)
   int na = 0, ne = 0;
+  int nrep = 1;
+  std::vector<int> rep_na, rep_ne, rep_aoff, rep_eoff;
+  std::vector<Rep> rep_h;        // descriptors as last planned
+  DBuf<Rep> rep_d;
+  DBuf<int> site_rep;            // [nsite_i] replica of each i-site (batches only)
+  DBuf<int> elem_rep;            // [ne] replica of each element (batches only)
+  DBuf<int> acell_rep;           // [atom cells] replica of each atom cell (batches only)
+  DBuf<unsigned long long> reach_bits;   // [nrep] element reach (double bits)
   double boxlo[3] = {0, 0, 0}, boxhi[3] = {0, 0, 0}, prd[3] = {0, 0, 0};
   double mass = 1.0;
   bool have_system = false;
@@ -202,6 +230,20 @@ struct Ctx {
   DBuf<double> fire_partial;
 
   Profile prof;
+
+  // CUDA graphs of the NVE cycle: [half-kick + drift, rebuild] then [forces,
+  // half-kick, every-1 more steps]; valid while `gen` (bumped by anything
+  // that moves buffers or changes baked-in parameters), dt and every match
+  long gen = 0;
+  bool graphs_enabled = true;
+  cudaGraphExec_t g_build = nullptr, g_steps = nullptr;
+  long graph_gen = -1;
+  double graph_dt = 0.0;
+  int graph_every = 0;
+  long graph_launches = 0;
+  double escale_node_last = 0.0;   // node energy scale of the last evaluation
+  DBuf<int> rep_meta;              // [4][nrep] aoff, na, eoff, ne (per-replica energy)
+  DBuf<double> rep_energy;         // [nrep]
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
 
   Ctx(int dev);
@@ -242,7 +284,6 @@ void pair_compute_mixed(Ctx &c, int eflag, int vflag);
 void assemble_nodef(Ctx &c);
 void nve_initial(Ctx &c, double dt);
 void nve_final(Ctx &c, double dt);
-void pbc_wrap(Ctx &c);
 void eam_tables(Ctx &c, const double *frho, const double *rhor, const double *z2r);
 void fire_init(Ctx &c, double dt);
 void fire_step(Ctx &c);

@@ -8,10 +8,6 @@
 
 namespace cacb200 {
 
-struct BoxD {
-  double lo[3], hi[3], L[3];
-};
-
 // Grid for a kernel that strides over a count known only on the device:
 // enough blocks to fill the 148 SMs several times over, no more than the
 // capacity `n_max` needs.

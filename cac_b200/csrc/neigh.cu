@@ -44,12 +44,35 @@ namespace {
 
 constexpr int KIND_SITE = 1 << 30;  // build-time entry flag: lattice site (gid = e*729+u)
 
+// Replica lookup.  A single system uses OneRep (its descriptor is a kernel
+// argument); a batch uses ManyRep (descriptor table plus per-site, per-element
+// and per-cell replica indices).  The kernels are written once for both.
+struct OneRep {
+  Rep r;
+  static constexpr bool many = false;
+  __device__ __forceinline__ Rep site(int) const { return r; }
+  __device__ __forceinline__ Rep elem(int) const { return r; }
+  __device__ __forceinline__ Rep acell(int) const { return r; }
+  __device__ __forceinline__ int elem_id(int) const { return 0; }
+};
+struct ManyRep {
+  const Rep *reps;
+  const int *site_rep, *elem_rep, *acell_rep;
+  static constexpr bool many = true;
+  __device__ __forceinline__ Rep site(int i) const { return reps[site_rep[i]]; }
+  __device__ __forceinline__ Rep elem(int e) const { return reps[elem_rep[e]]; }
+  __device__ __forceinline__ Rep acell(int c) const { return reps[acell_rep[c]]; }
+  __device__ __forceinline__ int elem_id(int e) const { return elem_rep[e]; }
+};
+
 // ------------------------------------------------------------------ pbc
 
 // Domain::pbc for owned atoms (domain.cpp:562-630)
-__global__ void k_pbc_atoms(double4 *xs, int na, BoxD b) {
+template <class RP>
+__global__ void k_pbc_atoms(double4 *xs, int na, RP P) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= na) return;
+  const BoxD b = P.site(i).b;
   double4 p = xs[i];
   double *q = &p.x;
 #pragma unroll
@@ -75,11 +98,14 @@ __global__ void k_pbc_atoms(double4 *xs, int na, BoxD b) {
 //   eframe[e*24 + 3..11]  rows of the inverse frame matrix
 //   eframe[e*24 + 12]     dmax
 //   eframe[e*24 + 13..21] frame vectors a, b, c (one lattice step each)
-__global__ void k_elem_geom(double *nodex, int ne, BoxD b, double4 *ecenter, double *eframe,
-                            unsigned long long *reach_bits, double reach_budget, int *grew) {
+template <class RP>
+__global__ void k_elem_geom(double *nodex, int ne, RP P, double4 *ecenter, double *eframe,
+                            unsigned long long *reach_bits, int *grew) {
   int e = blockIdx.x * blockDim.x + threadIdx.x;
   double reach = 0.0;
   if (e < ne) {
+    const Rep rp = P.elem(e);
+    const BoxD b = rp.b;
     double *nx = nodex + (size_t)e * 24;
     double c[3];
 #pragma unroll
@@ -162,11 +188,14 @@ __global__ void k_elem_geom(double *nodex, int ne, BoxD b, double4 *ecenter, dou
       for (int d = 0; d < 3; d++) fr[13 + 3 * q + d] = A[d][q];
     ecenter[e] = make_double4(c[0], c[1], c[2], R);
     reach = R + dmax;
-    if (!(reach <= reach_budget)) atomicExch(grew, 1);
+    if (!(reach <= rp.reach_budget)) atomicExch(grew, 1);
+    // per-replica maximum (non-negative doubles order like their bit patterns)
+    if (RP::many) atomicMax(reach_bits + P.elem_id(e), (unsigned long long)__double_as_longlong(reach));
   }
-  // block max into reach_bits (non-negative doubles order like their bit patterns)
-  for (int o = 16; o > 0; o >>= 1) reach = fmax(reach, __shfl_down_sync(0xffffffffu, reach, o));
-  if ((threadIdx.x & 31) == 0) atomicMax(reach_bits, (unsigned long long)__double_as_longlong(reach));
+  if (!RP::many) {
+    for (int o = 16; o > 0; o >>= 1) reach = fmax(reach, __shfl_down_sync(0xffffffffu, reach, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(reach_bits, (unsigned long long)__double_as_longlong(reach));
+  }
 }
 
 // ---------------------------------------------------------------- binning
@@ -181,21 +210,25 @@ __device__ __forceinline__ int grid_cell(const Grid &g, const BoxD &b, const dou
   return (c[2] * g.nc[1] + c[1]) * g.nc[0] + c[0];
 }
 
-__global__ void k_atom_keys(const double4 *xs, int na, Grid g, BoxD b, int *key, int *idx) {
+template <class RP>
+__global__ void k_atom_keys(const double4 *xs, int na, RP P, int *key, int *idx) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= na) return;
+  const Rep r = P.site(i);
   double4 p = xs[i];
   double w[3] = {p.x, p.y, p.z};
-  key[i] = grid_cell(g, b, w);
+  key[i] = r.abase + grid_cell(r.ag, r.b, w);
   idx[i] = i;
 }
 
-__global__ void k_elem_keys(const double4 *ecenter, int ne, Grid g, BoxD b, int *key, int *idx) {
+template <class RP>
+__global__ void k_elem_keys(const double4 *ecenter, int ne, RP P, int *key, int *idx) {
   int e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= ne) return;
+  const Rep r = P.elem(e);
   double4 p = ecenter[e];
   double w[3] = {p.x, p.y, p.z};
-  key[e] = grid_cell(g, b, w);
+  key[e] = r.ebase + grid_cell(r.eg, r.b, w);
   idx[e] = e;
 }
 
@@ -236,9 +269,7 @@ struct BuildArgs {
   const int *ecell_start;
   const int *ecell_elems;
   int na, ne, nsi, cap;
-  Grid ag, eg;
-  BoxD b;
-  RefBins rb;
+  RefBins rb;                 // single systems only (half lists)
   double cutneigh, cutneighsq;
   int want_half;
   int *raw_full, *num_full;
@@ -292,6 +323,7 @@ __device__ __forceinline__ void emit(const BuildArgs &A, int i, int &n, int *raw
 
 // One query point (an i-site) of the build.
 struct Query {
+  Rep r;          // its replica
   int i;
   bool iatom;
   int ie, ig, iu;
@@ -300,7 +332,9 @@ struct Query {
   int ti[3];
 };
 
-__device__ __forceinline__ void make_query(const BuildArgs &A, int i, Query &q) {
+template <class RP>
+__device__ __forceinline__ void make_query(const BuildArgs &A, const RP &P, int i, Query &q) {
+  q.r = P.site(i);
   q.i = i;
   q.iatom = i < A.na;
   q.ie = q.ig = q.iu = -1;
@@ -318,17 +352,18 @@ __device__ __forceinline__ void make_query(const BuildArgs &A, int i, Query &q) 
     q.xi[1] = nx[1];
     q.xi[2] = nx[2];
   }
+  const BoxD &b = q.r.b;
 #pragma unroll
   for (int d = 0; d < 3; d++) {
-    double f = floor((q.xi[d] - A.b.lo[d]) / A.b.L[d]);
+    double f = floor((q.xi[d] - b.lo[d]) / b.L[d]);
     q.ti[d] = -(int)f;
-    q.wi[d] = q.xi[d] - f * A.b.L[d];
-    if (q.wi[d] >= A.b.hi[d]) {
-      q.wi[d] -= A.b.L[d];
+    q.wi[d] = q.xi[d] - f * b.L[d];
+    if (q.wi[d] >= b.hi[d]) {
+      q.wi[d] -= b.L[d];
       q.ti[d] -= 1;
     }
-    if (q.wi[d] < A.b.lo[d]) {
-      q.wi[d] += A.b.L[d];
+    if (q.wi[d] < b.lo[d]) {
+      q.wi[d] += b.L[d];
       q.ti[d] += 1;
     }
   }
@@ -348,9 +383,9 @@ __device__ __forceinline__ void try_atom(const BuildArgs &A, const Query &q, int
   double4 xj = A.xs[j];
   double qq[3] = {xj.x, xj.y, xj.z};
   if (!zero) {
-    qq[0] = s[0] ? __dadd_rn(qq[0], s[0] * A.b.L[0]) : qq[0];
-    qq[1] = s[1] ? __dadd_rn(qq[1], s[1] * A.b.L[1]) : qq[1];
-    qq[2] = s[2] ? __dadd_rn(qq[2], s[2] * A.b.L[2]) : qq[2];
+    qq[0] = s[0] ? __dadd_rn(qq[0], s[0] * q.r.b.L[0]) : qq[0];
+    qq[1] = s[1] ? __dadd_rn(qq[1], s[1] * q.r.b.L[1]) : qq[1];
+    qq[2] = s[2] ? __dadd_rn(qq[2], s[2] * q.r.b.L[2]) : qq[2];
   }
   double rsq = rsq_rn(__dsub_rn(q.xi[0], qq[0]), __dsub_rn(q.xi[1], qq[1]), __dsub_rn(q.xi[2], qq[2]));
   if (!(rsq <= A.cutneighsq)) return;
@@ -378,10 +413,11 @@ __device__ __forceinline__ void wrap_cell(int v, int nc, int &cell, int &W) {
 
 // Lattice sites of the elements near the query point.
 __device__ void element_candidates(const BuildArgs &A, const Query &q, int &nf, int &nh) {
+  const Grid &eg = q.r.eg;
   int ci[3];
 #pragma unroll
   for (int d = 0; d < 3; d++)
-    ci[d] = min(max((int)((q.wi[d] - A.b.lo[d]) * A.eg.inv[d]), 0), A.eg.nc[d] - 1);
+    ci[d] = min(max((int)((q.wi[d] - q.r.b.lo[d]) * eg.inv[d]), 0), eg.nc[d] - 1);
   double icen[3] = {0, 0, 0};
   if (!q.iatom) {
     double4 c = A.ecenter[q.ie];
@@ -391,19 +427,19 @@ __device__ void element_candidates(const BuildArgs &A, const Query &q, int &nf, 
   }
   for (int oz = -1; oz <= 1; oz++) {
     int cz, Wz;
-    wrap_cell(ci[2] + oz, A.eg.nc[2], cz, Wz);
+    wrap_cell(ci[2] + oz, eg.nc[2], cz, Wz);
     for (int oy = -1; oy <= 1; oy++) {
       int cy, Wy;
-      wrap_cell(ci[1] + oy, A.eg.nc[1], cy, Wy);
+      wrap_cell(ci[1] + oy, eg.nc[1], cy, Wy);
       for (int ox = -1; ox <= 1; ox++) {
         int cx, Wx;
-        wrap_cell(ci[0] + ox, A.eg.nc[0], cx, Wx);
-        int cell = (cz * A.eg.nc[1] + cy) * A.eg.nc[0] + cx;
+        wrap_cell(ci[0] + ox, eg.nc[0], cx, Wx);
+        int cell = q.r.ebase + (cz * eg.nc[1] + cy) * eg.nc[0] + cx;
         int beg = A.ecell_start[cell], end = A.ecell_start[cell + 1];
         if (beg == end) continue;
         int s[3] = {Wx - q.ti[0], Wy - q.ti[1], Wz - q.ti[2]};
         bool zero = (s[0] == 0 && s[1] == 0 && s[2] == 0);
-        double sL[3] = {s[0] * A.b.L[0], s[1] * A.b.L[1], s[2] * A.b.L[2]};
+        double sL[3] = {s[0] * q.r.b.L[0], s[1] * q.r.b.L[1], s[2] * q.r.b.L[2]};
         for (int kk = beg; kk < end; kk++) {
           int e = A.ecell_elems[kk];
           double4 ce = A.ecenter[e];
@@ -509,12 +545,15 @@ __device__ __forceinline__ void finish_counts(const BuildArgs &A, int i, int nf,
 // surrounding cells together, so every candidate is one broadcast load shared
 // by the warp.  A conservative FP32 distance test (from a float copy of the
 // wrapped positions) screens candidates before the exact FP64 test.
-__global__ void __launch_bounds__(32) k_build_atoms(BuildArgs A) {
+template <class RP>
+__global__ void __launch_bounds__(32) k_build_atoms(BuildArgs A, RP P) {
   const int home = blockIdx.x;
   const int hbeg = A.acell_start[home], hend = A.acell_start[home + 1];
   if (hbeg == hend) return;
-  const int nc0 = A.ag.nc[0], nc1 = A.ag.nc[1], nc2 = A.ag.nc[2];
-  const int hx = home % nc0, hy = (home / nc0) % nc1, hz = home / (nc0 * nc1);
+  const Rep R = P.acell(home);
+  const int local = home - R.abase;
+  const int nc0 = R.ag.nc[0], nc1 = R.ag.nc[1], nc2 = R.ag.nc[2];
+  const int hx = local % nc0, hy = (local / nc0) % nc1, hz = local / (nc0 * nc1);
   const float pre = (float)(A.cutneigh + 1e-3);
   const float pre2 = pre * pre;
   for (int base = hbeg; base < hend; base += blockDim.x) {
@@ -524,7 +563,7 @@ __global__ void __launch_bounds__(32) k_build_atoms(BuildArgs A) {
     int nf = 0, nh = 0;
     float wx = 0.f, wy = 0.f, wz = 0.f;
     if (active) {
-      make_query(A, (int)__double_as_longlong(A.acell_pos[h].w), q);
+      make_query(A, P, (int)__double_as_longlong(A.acell_pos[h].w), q);
       float4 w = A.acell_pos32[h];
       wx = w.x;
       wy = w.y;
@@ -539,9 +578,9 @@ __global__ void __launch_bounds__(32) k_build_atoms(BuildArgs A) {
         for (int ox = -1; ox <= 1; ox++) {
           int cx, Wx;
           wrap_cell(hx + ox, nc0, cx, Wx);
-          int cell = (cz * nc1 + cy) * nc0 + cx;
+          int cell = R.abase + (cz * nc1 + cy) * nc0 + cx;
           int W[3] = {Wx, Wy, Wz};
-          const float sx = (float)(Wx * A.b.L[0]), sy = (float)(Wy * A.b.L[1]), sz = (float)(Wz * A.b.L[2]);
+          const float sx = (float)(Wx * R.b.L[0]), sy = (float)(Wy * R.b.L[1]), sz = (float)(Wz * R.b.L[2]);
           int beg = A.acell_start[cell], end = A.acell_start[cell + 1];
           for (int k = beg; k < end; k++) {
             float4 pj = A.acell_pos32[k];
@@ -562,11 +601,12 @@ __global__ void __launch_bounds__(32) k_build_atoms(BuildArgs A) {
 
 // Atoms, element lattice sites: appended after the atom neighbours.  Atoms
 // whose 27 element cells hold no element leave at once.
-__global__ void __launch_bounds__(128) k_build_atom_sites(BuildArgs A) {
+template <class RP>
+__global__ void __launch_bounds__(128) k_build_atom_sites(BuildArgs A, RP P) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= A.na) return;
   Query q;
-  make_query(A, i, q);
+  make_query(A, P, i, q);
   int nf = A.num_full[i], nh = A.want_half ? A.num_half[i] : 0;
   if (A.ne > 0) element_candidates(A, q, nf, nh);
   finish_counts(A, i, nf, nh);
@@ -574,30 +614,32 @@ __global__ void __launch_bounds__(128) k_build_atom_sites(BuildArgs A) {
 
 // Gauss points: one thread each; atoms from the 27 surrounding atom cells
 // (full list only), then element lattice sites.
-__global__ void __launch_bounds__(128) k_build_gauss(BuildArgs A) {
+template <class RP>
+__global__ void __launch_bounds__(128) k_build_gauss(BuildArgs A, RP P) {
   int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= NG * A.ne) return;
   Query q;
-  make_query(A, A.na + t, q);
+  make_query(A, P, A.na + t, q);
+  const Grid &ag = q.r.ag;
   int nf = 0, nh = 0;
   if (A.na > 0) {
     const double pre = (A.cutneigh + 1e-6) * (A.cutneigh + 1e-6);
     int ci[3];
 #pragma unroll
     for (int d = 0; d < 3; d++)
-      ci[d] = min(max((int)((q.wi[d] - A.b.lo[d]) * A.ag.inv[d]), 0), A.ag.nc[d] - 1);
+      ci[d] = min(max((int)((q.wi[d] - q.r.b.lo[d]) * ag.inv[d]), 0), ag.nc[d] - 1);
     for (int oz = -1; oz <= 1; oz++) {
       int cz, Wz;
-      wrap_cell(ci[2] + oz, A.ag.nc[2], cz, Wz);
+      wrap_cell(ci[2] + oz, ag.nc[2], cz, Wz);
       for (int oy = -1; oy <= 1; oy++) {
         int cy, Wy;
-        wrap_cell(ci[1] + oy, A.ag.nc[1], cy, Wy);
+        wrap_cell(ci[1] + oy, ag.nc[1], cy, Wy);
         for (int ox = -1; ox <= 1; ox++) {
           int cx, Wx;
-          wrap_cell(ci[0] + ox, A.ag.nc[0], cx, Wx);
-          int cell = (cz * A.ag.nc[1] + cy) * A.ag.nc[0] + cx;
+          wrap_cell(ci[0] + ox, ag.nc[0], cx, Wx);
+          int cell = q.r.abase + (cz * ag.nc[1] + cy) * ag.nc[0] + cx;
           int W[3] = {Wx, Wy, Wz};
-          double sh[3] = {Wx * A.b.L[0], Wy * A.b.L[1], Wz * A.b.L[2]};
+          double sh[3] = {Wx * q.r.b.L[0], Wy * q.r.b.L[1], Wz * q.r.b.L[2]};
           int beg = A.acell_start[cell], end = A.acell_start[cell + 1];
           for (int k = beg; k < end; k++) {
             double4 pj = A.acell_pos[k];
@@ -628,14 +670,15 @@ __global__ void k_mark_sites(const int *raw, const int *num, int nsi, int cap, i
   }
 }
 
-__global__ void k_act_table(const int *flag, const int *pref, int ngid, int ne, int *act_gid,
-                            int *act_off, int *nact) {
+__global__ void k_act_table(const int *flag, const int *pref, int ngid, int ne, int nsi, int *act_gid,
+                            int *act_off, int *nact, int *too_many) {
   int gid = blockIdx.x * blockDim.x + threadIdx.x;
   if (gid < ngid && flag[gid]) act_gid[pref[gid]] = gid;
   if (gid < ne) act_off[gid] = pref[gid * NU];
   if (gid == 0) {
     act_off[ne] = pref[ngid];
     *nact = pref[ngid];
+    if ((long)nsi + pref[ngid] >= (1L << (31 - IMG_BITS))) *too_many = 1;
   }
 }
 
@@ -662,8 +705,9 @@ __global__ void k_remap(const int *raw, const unsigned char *img, const int *num
 
 inline int nblk(long n, int t) { return (int)((n + t - 1) / t); }
 
-void setup_grids(Ctx &c, double ereach) {
-  // reference atom bins (nbin_standard.cpp:84-128), orthogonal box
+// Reference atom bins of a single system (nbin_standard.cpp:84-128),
+// orthogonal box: used only by the half-list storage rule.
+void setup_ref_bins(Ctx &c) {
   double binsize_optimal = 0.5 * c.cutneigh;
   double binsizeinv = 1.0 / binsize_optimal;
   for (int d = 0; d < 3; d++) {
@@ -676,41 +720,52 @@ void setup_grids(Ctx &c, double ereach) {
     double bs = bbox / nb;
     c.rbins.inv[d] = 1.0 / bs;
   }
-  // candidate grids
+}
+
+// Candidate grids of one replica: atoms in cells >= cutneigh, element
+// centres in cells >= cutneigh + element reach.
+void setup_grids(const Ctx &c, Rep &r, bool has_elements) {
   for (int d = 0; d < 3; d++) {
-    double L = c.prd[d];
+    double L = r.b.L[d];
     int na_c = (int)(L / c.cutneigh);
     if (na_c < 1) throw Error(CACB200_EINVAL, "box shorter than the neighbour cutoff");
-    c.agrid.nc[d] = na_c;
-    c.agrid.inv[d] = na_c / L;
-    double reach = c.cutneigh + ereach + 1e-6;
-    if (c.ne > 0 && L < reach)
+    r.ag.nc[d] = na_c;
+    r.ag.inv[d] = na_c / L;
+    double reach = c.cutneigh + r.reach_budget + 1e-6;
+    if (has_elements && L < reach)
       throw Error(CACB200_EINVAL, "box shorter than the cutoff plus the element radius in dimension " +
                                       std::to_string(d));
     int ne_c = std::max(1, (int)(L / reach));
-    c.egrid.nc[d] = ne_c;
-    c.egrid.inv[d] = ne_c / L;
+    r.eg.nc[d] = ne_c;
+    r.eg.inv[d] = ne_c / L;
   }
-  c.agrid.ncell = c.agrid.nc[0] * c.agrid.nc[1] * c.agrid.nc[2];
-  c.egrid.ncell = c.egrid.nc[0] * c.egrid.nc[1] * c.egrid.nc[2];
+  r.ag.ncell = r.ag.nc[0] * r.ag.nc[1] * r.ag.nc[2];
+  r.eg.ncell = r.eg.nc[0] * r.eg.nc[1] * r.eg.nc[2];
+}
+
+// Launch a rebuild kernel for a single system or a batch.
+template <class F>
+void with_reps(const Ctx &c, F &&f) {
+  if (c.nrep == 1) {
+    OneRep P{c.rep_h[0]};
+    f(P);
+  } else {
+    ManyRep P{c.rep_d.p, c.site_rep.p, c.elem_rep.p, c.acell_rep.p};
+    f(P);
+  }
 }
 
 }  // namespace
-
-void pbc_wrap(Ctx &c) {
-  BoxD b = make_box(c);
-  if (c.na) k_pbc_atoms<<<nblk(c.na, 256), 256, 0, c.stream>>>(c.xs.p, c.na, b);
-}
 
 // Capacity plan: sizes every buffer of a rebuild for the current system (site
 // table for the worst case of every lattice site active, candidate grids with
 // room for elements to grow, list slots of `cap` per site), so that rebuilds
 // afterwards neither allocate nor synchronise and can be queued or captured
-// in a CUDA graph.  Synchronises once to read the element radius.
+// in a CUDA graph.  Synchronises once to read the element radii.
 void neigh_plan(Ctx &c, bool want_half) {
   c.check_system();
   if (c.pp.style == CACB200_PAIR_NONE) throw Error(CACB200_ESTATE, "no pair style set");
-  BoxD b = make_box(c);
+  if (want_half && c.nrep > 1) throw Error(CACB200_EINVAL, "half lists are built for single systems only");
   double cutoff = std::sqrt(c.pp.cut * c.pp.cut);
   c.cutneigh = cutoff + c.skin;
   c.cutneighsq = c.cutneigh * c.cutneigh;
@@ -718,27 +773,65 @@ void neigh_plan(Ctx &c, bool want_half) {
   c.eframe.reserve((size_t)std::max(c.ne, 1) * 24);
   c.overflow.reserve(8);
   c.dev_nact.reserve(1);
+  c.reach_bits.reserve(c.nrep);
+  c.rep_d.reserve(c.nrep);
   CACB200_CUDA(cudaMemsetAsync(c.overflow.p, 0, 8 * sizeof(int), c.stream));
   CACB200_CUDA(cudaMemsetAsync(c.dev_nact.p, 0, sizeof(int), c.stream));
-  double ereach = 0.0;
+  CACB200_CUDA(cudaMemsetAsync(c.reach_bits.p, 0, sizeof(unsigned long long) * c.nrep, c.stream));
+  // element geometry with no reach limit, to measure each replica's radius
+  for (Rep &r : c.rep_h) r.reach_budget = 1e300;
+  stream_copy(c, c.rep_d.p, c.rep_h.data(), sizeof(Rep) * c.nrep, cudaMemcpyHostToDevice);
+  std::vector<unsigned long long> bits(c.nrep, 0);
   if (c.ne) {
-    if (c.na) k_pbc_atoms<<<nblk(c.na, 256), 256, 0, c.stream>>>(c.xs.p, c.na, b);
-    k_elem_geom<<<nblk(c.ne, 128), 128, 0, c.stream>>>(c.nodex.p, c.ne, b, c.ecenter.p, c.eframe.p,
-                                                       (unsigned long long *)(c.overflow.p + 4), 1e300,
-                                                       c.overflow.p + 3);
-    unsigned long long bits = 0;
-    stream_copy(c, &bits, c.overflow.p + 4, sizeof(bits), cudaMemcpyDeviceToHost);
-    std::memcpy(&ereach, &bits, sizeof(double));
+    with_reps(c, [&](auto P) {
+      if (c.na) k_pbc_atoms<<<nblk(c.na, 256), 256, 0, c.stream>>>(c.xs.p, c.na, P);
+      k_elem_geom<<<nblk(c.ne, 128), 128, 0, c.stream>>>(c.nodex.p, c.ne, P, c.ecenter.p, c.eframe.p,
+                                                         c.reach_bits.p, c.overflow.p + 3);
+    });
+    stream_copy(c, bits.data(), c.reach_bits.p, sizeof(unsigned long long) * c.nrep, cudaMemcpyDeviceToHost);
+  }
+  int abase = 0, ebase = 0;
+  for (int r = 0; r < c.nrep; r++) {
+    Rep &R = c.rep_h[r];
+    double ereach = 0.0;
+    std::memcpy(&ereach, &bits[r], sizeof(double));
     if (!(ereach < 1e30)) throw Error(CACB200_EUNSTABLE, "non-finite element geometry");
+    // elements may grow by 20 % (and 2 A) before the grid is planned again,
+    // as far as the box allows
+    R.reach_budget = 0.0;
+    if (c.rep_ne[r]) {
+      double room = std::min(R.b.L[0], std::min(R.b.L[1], R.b.L[2])) - c.cutneigh - 2e-6;
+      R.reach_budget = std::max(ereach, std::min(std::max(1.2 * ereach, ereach + 2.0), room));
+    }
+    setup_grids(c, R, c.rep_ne[r] > 0);
+    // fixed-point frame of the mixed form: the largest 2^k (k <= 24) with
+    // (L + 64 A) 2^k inside an int, per dimension
+    for (int d = 0; d < 3; d++) {
+      int k = 24;
+      while (k > 4 && (R.b.L[d] + 64.0) * std::ldexp(1.0, k) > 2147483000.0) k--;
+      if ((R.b.L[d] + 64.0) * std::ldexp(1.0, k) > 2147483000.0)
+        throw Error(CACB200_EINVAL, "box too large for the mixed-precision fixed-point positions");
+      R.qscale[d] = std::ldexp(1.0, k);
+      R.qinv[d] = std::ldexp(1.0f, -k);
+      R.Lq[d] = (int)std::nearbyint(R.b.L[d] * R.qscale[d]);
+    }
+    R.abase = abase;
+    R.ebase = ebase;
+    abase += R.ag.ncell;
+    ebase += R.eg.ncell;
   }
-  // elements may grow by 20 % (and 2 A) before the grid is planned again, as
-  // far as the box allows
-  c.reach_budget = 0.0;
-  if (c.ne) {
-    double room = std::min(c.prd[0], std::min(c.prd[1], c.prd[2])) - c.cutneigh - 2e-6;
-    c.reach_budget = std::max(ereach, std::min(std::max(1.2 * ereach, ereach + 2.0), room));
+  stream_copy(c, c.rep_d.p, c.rep_h.data(), sizeof(Rep) * c.nrep, cudaMemcpyHostToDevice);
+  c.agrid.ncell = abase;
+  c.egrid.ncell = ebase;
+  if (c.nrep > 1) {
+    std::vector<int> cr(abase);
+    for (int r = 0; r < c.nrep; r++)
+      std::fill(cr.begin() + c.rep_h[r].abase, cr.begin() + c.rep_h[r].abase + c.rep_h[r].ag.ncell, r);
+    c.acell_rep.reserve(abase);
+    stream_copy(c, c.acell_rep.p, cr.data(), sizeof(int) * abase, cudaMemcpyHostToDevice);
+  } else {
+    setup_ref_bins(c);
   }
-  setup_grids(c, c.reach_budget);
 
   const int nsi = c.nsite_i();
   const size_t ngid = (size_t)c.ne * NU;
@@ -802,6 +895,7 @@ void neigh_plan(Ctx &c, bool want_half) {
   c.sort_bits_e = bits_e;
   c.plan_half = want_half;
   c.planned = true;
+  c.gen++;
   c.plan_na = c.na;
   c.plan_ne = c.ne;
 }
@@ -814,84 +908,82 @@ void neigh_plan(Ctx &c, bool want_half) {
 void neigh_build_async(Ctx &c, bool want_half) {
   if (!c.planned || c.plan_na != c.na || c.plan_ne != c.ne || (want_half && !c.plan_half))
     throw Error(CACB200_ESTATE, "rebuild without a capacity plan");
-  BoxD b = make_box(c);
   const int nsi = c.nsite_i();
   const size_t ngid = (size_t)c.ne * NU;
   CACB200_CUDA(cudaMemsetAsync(c.overflow.p, 0, 4 * sizeof(int), c.stream));
-  {
-    KernelTimer t(c, "pbc_geom");
-    if (c.na) k_pbc_atoms<<<nblk(c.na, 256), 256, 0, c.stream>>>(c.xs.p, c.na, b);
-    if (c.ne)
-      k_elem_geom<<<nblk(c.ne, 128), 128, 0, c.stream>>>(c.nodex.p, c.ne, b, c.ecenter.p, c.eframe.p,
-                                                         (unsigned long long *)(c.overflow.p + 4),
-                                                         c.reach_budget, c.overflow.p + 3);
-  }
-  {
-    KernelTimer t(c, "bin");
-    size_t bytes = c.cub_bytes;
+  with_reps(c, [&](auto P) {
+    {
+      KernelTimer t(c, "pbc_geom");
+      if (c.na) k_pbc_atoms<<<nblk(c.na, 256), 256, 0, c.stream>>>(c.xs.p, c.na, P);
+      if (c.ne)
+        k_elem_geom<<<nblk(c.ne, 128), 128, 0, c.stream>>>(c.nodex.p, c.ne, P, c.ecenter.p, c.eframe.p,
+                                                           c.reach_bits.p, c.overflow.p + 3);
+    }
+    {
+      KernelTimer t(c, "bin");
+      size_t bytes = c.cub_bytes;
+      if (c.na) {
+        k_atom_keys<<<nblk(c.na, 256), 256, 0, c.stream>>>(c.xs.p, c.na, P, c.cell_key.p, c.idx_tmp.p);
+        CACB200_CUDA(cub::DeviceRadixSort::SortPairs(c.cub_tmp.p, bytes, c.cell_key.p, c.cell_key2.p,
+                                                     c.idx_tmp.p, c.idx_tmp2.p, c.na, 0, c.sort_bits_a,
+                                                     c.stream));
+        k_cell_start<<<nblk(c.agrid.ncell + 1, 256), 256, 0, c.stream>>>(c.cell_key2.p, c.na, c.agrid.ncell,
+                                                                        c.acell_start.p);
+        k_gather_pos<<<nblk(c.na, 256), 256, 0, c.stream>>>(c.xs.p, c.idx_tmp2.p, c.na, c.acell_pos.p,
+                                                            c.acell_pos32.p);
+      } else {
+        CACB200_CUDA(cudaMemsetAsync(c.acell_start.p, 0, sizeof(int) * (c.agrid.ncell + 1), c.stream));
+      }
+      if (c.ne) {
+        bytes = c.cub_bytes;
+        k_elem_keys<<<nblk(c.ne, 256), 256, 0, c.stream>>>(c.ecenter.p, c.ne, P, c.cell_key.p, c.idx_tmp.p);
+        CACB200_CUDA(cub::DeviceRadixSort::SortPairs(c.cub_tmp.p, bytes, c.cell_key.p, c.cell_key2.p,
+                                                     c.idx_tmp.p, c.ecell_elems.p, c.ne, 0, c.sort_bits_e,
+                                                     c.stream));
+        k_cell_start<<<nblk(c.egrid.ncell + 1, 256), 256, 0, c.stream>>>(c.cell_key2.p, c.ne, c.egrid.ncell,
+                                                                        c.ecell_start.p);
+      } else {
+        CACB200_CUDA(cudaMemsetAsync(c.ecell_start.p, 0, sizeof(int) * (c.egrid.ncell + 1), c.stream));
+      }
+    }
+    BuildArgs A;
+    A.xs = c.xs.p;
+    A.nodex = c.nodex.p;
+    A.ecenter = c.ecenter.p;
+    A.eframe = c.eframe.p;
+    A.acell_start = c.acell_start.p;
+    A.acell_pos = c.acell_pos.p;
+    A.acell_pos32 = c.acell_pos32.p;
+    A.ecell_start = c.ecell_start.p;
+    A.ecell_elems = c.ecell_elems.p;
+    A.na = c.na;
+    A.ne = c.ne;
+    A.nsi = nsi;
+    A.cap = c.cap;
+    A.rb = c.rbins;
+    A.cutneigh = c.cutneigh;
+    A.cutneighsq = c.cutneighsq;
+    A.want_half = want_half ? 1 : 0;
+    A.raw_full = c.raw_full.p;
+    A.num_full = c.num_full.p;
+    A.img_full = c.img_full.p;
+    A.raw_half = want_half ? c.raw_half.p : nullptr;
+    A.num_half = want_half ? c.num_half.p : nullptr;
+    A.img_half = want_half ? c.img_half.p : nullptr;
+    A.overflow = c.overflow.p;
     if (c.na) {
-      k_atom_keys<<<nblk(c.na, 256), 256, 0, c.stream>>>(c.xs.p, c.na, c.agrid, b, c.cell_key.p, c.idx_tmp.p);
-      CACB200_CUDA(cub::DeviceRadixSort::SortPairs(c.cub_tmp.p, bytes, c.cell_key.p, c.cell_key2.p, c.idx_tmp.p,
-                                                   c.idx_tmp2.p, c.na, 0, c.sort_bits_a, c.stream));
-      k_cell_start<<<nblk(c.agrid.ncell + 1, 256), 256, 0, c.stream>>>(c.cell_key2.p, c.na, c.agrid.ncell,
-                                                                      c.acell_start.p);
-      k_gather_pos<<<nblk(c.na, 256), 256, 0, c.stream>>>(c.xs.p, c.idx_tmp2.p, c.na, c.acell_pos.p,
-                                                          c.acell_pos32.p);
-    } else {
-      CACB200_CUDA(cudaMemsetAsync(c.acell_start.p, 0, sizeof(int) * (c.agrid.ncell + 1), c.stream));
+      KernelTimer t(c, "build_atoms");
+      k_build_atoms<<<c.agrid.ncell, 32, 0, c.stream>>>(A, P);
+    }
+    if (c.na) {
+      KernelTimer t(c, "build_atom_sites");
+      k_build_atom_sites<<<nblk(c.na, 128), 128, 0, c.stream>>>(A, P);
     }
     if (c.ne) {
-      bytes = c.cub_bytes;
-      k_elem_keys<<<nblk(c.ne, 256), 256, 0, c.stream>>>(c.ecenter.p, c.ne, c.egrid, b, c.cell_key.p,
-                                                         c.idx_tmp.p);
-      CACB200_CUDA(cub::DeviceRadixSort::SortPairs(c.cub_tmp.p, bytes, c.cell_key.p, c.cell_key2.p, c.idx_tmp.p,
-                                                   c.ecell_elems.p, c.ne, 0, c.sort_bits_e, c.stream));
-      k_cell_start<<<nblk(c.egrid.ncell + 1, 256), 256, 0, c.stream>>>(c.cell_key2.p, c.ne, c.egrid.ncell,
-                                                                      c.ecell_start.p);
-    } else {
-      CACB200_CUDA(cudaMemsetAsync(c.ecell_start.p, 0, sizeof(int) * (c.egrid.ncell + 1), c.stream));
+      KernelTimer t(c, "build_gauss");
+      k_build_gauss<<<nblk(NG * c.ne, 128), 128, 0, c.stream>>>(A, P);
     }
-  }
-  BuildArgs A;
-  A.xs = c.xs.p;
-  A.nodex = c.nodex.p;
-  A.ecenter = c.ecenter.p;
-  A.eframe = c.eframe.p;
-  A.acell_start = c.acell_start.p;
-  A.acell_pos = c.acell_pos.p;
-  A.acell_pos32 = c.acell_pos32.p;
-  A.ecell_start = c.ecell_start.p;
-  A.ecell_elems = c.ecell_elems.p;
-  A.na = c.na;
-  A.ne = c.ne;
-  A.nsi = nsi;
-  A.cap = c.cap;
-  A.ag = c.agrid;
-  A.eg = c.egrid;
-  A.b = b;
-  A.rb = c.rbins;
-  A.cutneigh = c.cutneigh;
-  A.cutneighsq = c.cutneighsq;
-  A.want_half = want_half ? 1 : 0;
-  A.raw_full = c.raw_full.p;
-  A.num_full = c.num_full.p;
-  A.img_full = c.img_full.p;
-  A.raw_half = want_half ? c.raw_half.p : nullptr;
-  A.num_half = want_half ? c.num_half.p : nullptr;
-  A.img_half = want_half ? c.img_half.p : nullptr;
-  A.overflow = c.overflow.p;
-  if (c.na) {
-    KernelTimer t(c, "build_atoms");
-    k_build_atoms<<<c.agrid.ncell, 32, 0, c.stream>>>(A);
-  }
-  if (c.na) {
-    KernelTimer t(c, "build_atom_sites");
-    k_build_atom_sites<<<nblk(c.na, 128), 128, 0, c.stream>>>(A);
-  }
-  if (c.ne) {
-    KernelTimer t(c, "build_gauss");
-    k_build_gauss<<<nblk(NG * c.ne, 128), 128, 0, c.stream>>>(A);
-  }
+  });
   {
     KernelTimer t(c, "compact");
     int *flag = c.site_flag.p;
@@ -901,8 +993,8 @@ void neigh_build_async(Ctx &c, bool want_half) {
       k_mark_sites<<<nblk(nsi, 256), 256, 0, c.stream>>>(c.raw_full.p, c.num_full.p, nsi, c.cap, flag);
       size_t bytes = c.cub_bytes;
       CACB200_CUDA(cub::DeviceScan::ExclusiveSum(c.cub_tmp.p, bytes, flag, pref, (int)(ngid + 1), c.stream));
-      k_act_table<<<nblk((long)ngid, 256), 256, 0, c.stream>>>(flag, pref, (int)ngid, c.ne, c.act_gid.p,
-                                                              c.act_off.p, c.dev_nact.p);
+      k_act_table<<<nblk((long)ngid, 256), 256, 0, c.stream>>>(flag, pref, (int)ngid, c.ne, nsi, c.act_gid.p,
+                                                              c.act_off.p, c.dev_nact.p, c.overflow.p + 7);
     }
     k_remap<<<nblk(nsi, 256), 256, 0, c.stream>>>(c.raw_full.p, c.img_full.p, c.num_full.p, nsi, c.cap, pref,
                                                    c.na, c.ne, c.nbr_full.p);
@@ -924,6 +1016,7 @@ int neigh_check(Ctx &c) {
   stream_copy(c, ov, c.overflow.p, sizeof(ov), cudaMemcpyDeviceToHost);
   if (ov[2]) throw Error(CACB200_EINVAL, "neighbour image beyond the first periodic image (box too small)");
   if (ov[6]) throw Error(CACB200_EUNSTABLE, "a site left the fixed-point range around the box (unstable run)");
+  if (ov[7]) throw Error(CACB200_EOVERFLOW, "more referenced sites than 26-bit list entries can address");
   int again = 0;
   if (ov[0]) {
     c.cap = ((ov[1] + 31) / 32) * 32;

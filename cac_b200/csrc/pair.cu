@@ -34,7 +34,9 @@ struct PairArgs {
   const int *nbr;
   const int *num;
   int na, ne, nsi;
-  double L[3];
+  double L[3];                      // box of a single system
+  const Rep *reps;                  // batches: replica descriptors ...
+  const int *site_rep;              // ... and the replica of each i-site (null for one system)
   double *f, *gaussf;
   double *eatom, *vatom, *enode, *vnode;
   double *partial;
@@ -42,33 +44,41 @@ struct PairArgs {
   double escale_node, vscale_node;  // global scales of a node Gauss point
 };
 
-__device__ __forceinline__ void neighbour_pos(const PairArgs &A, int v, double4 &xj) {
+__device__ __forceinline__ void neighbour_pos(const PairArgs &A, double Lx, double Ly, double Lz, int v,
+                                              double4 &xj) {
   int j = v >> IMG_BITS, code = v & ((1 << IMG_BITS) - 1);
   xj = ldg256(A.xs + j);
   if (code != IMG_ZERO) {
     int sx, sy, sz;
     img_decode(code, sx, sy, sz);
-    xj.x += sx * A.L[0];
-    xj.y += sy * A.L[1];
-    xj.z += sz * A.L[2];
+    xj.x += sx * Lx;
+    xj.y += sy * Ly;
+    xj.z += sz * Lz;
   }
 }
 
 // Walks a site's list four entries at a time: the four entry loads, then the
 // four position loads, are issued back to back before any of them is used, so
 // each thread keeps eight independent loads in flight instead of a chain of
-// dependent pairs.
-template <class F>
-__device__ __forceinline__ void for_each_neighbour(const PairArgs &A, const int *nb, int n, F &&f) {
+// dependent pairs.  MANY: the site belongs to a batch replica with its own box.
+template <bool MANY, class F>
+__device__ __forceinline__ void for_each_neighbour(const PairArgs &A, int i, const int *nb, int n, F &&f) {
+  double Lx = A.L[0], Ly = A.L[1], Lz = A.L[2];
+  if (MANY) {
+    const Rep *r = A.reps + A.site_rep[i];
+    Lx = r->b.L[0];
+    Ly = r->b.L[1];
+    Lz = r->b.L[2];
+  }
   int k = 0;
   for (; k + 4 <= n; k += 4) {
     int v0 = nb[(size_t)k * A.nsi], v1 = nb[(size_t)(k + 1) * A.nsi];
     int v2 = nb[(size_t)(k + 2) * A.nsi], v3 = nb[(size_t)(k + 3) * A.nsi];
     double4 p0, p1, p2, p3;
-    neighbour_pos(A, v0, p0);
-    neighbour_pos(A, v1, p1);
-    neighbour_pos(A, v2, p2);
-    neighbour_pos(A, v3, p3);
+    neighbour_pos(A, Lx, Ly, Lz, v0, p0);
+    neighbour_pos(A, Lx, Ly, Lz, v1, p1);
+    neighbour_pos(A, Lx, Ly, Lz, v2, p2);
+    neighbour_pos(A, Lx, Ly, Lz, v3, p3);
     f(p0);
     f(p1);
     f(p2);
@@ -76,7 +86,7 @@ __device__ __forceinline__ void for_each_neighbour(const PairArgs &A, const int 
   }
   for (; k < n; k++) {
     double4 p;
-    neighbour_pos(A, nb[(size_t)k * A.nsi], p);
+    neighbour_pos(A, Lx, Ly, Lz, nb[(size_t)k * A.nsi], p);
     f(p);
   }
 }
@@ -142,7 +152,7 @@ struct LjParams {
   double cutsq, lj1, lj2, lj3, lj4, offset;
 };
 
-template <bool EV>
+template <bool EV, bool MANY>
 __global__ void __launch_bounds__(128, EV ? 4 : 8) k_lj(PairArgs A, LjParams P) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   bool valid = i < A.nsi;
@@ -173,7 +183,7 @@ __global__ void __launch_bounds__(128, EV ? 4 : 8) k_lj(PairArgs A, LjParams P) 
         }
       }
     };
-    for_each_neighbour(A, nb, n, pair);
+    for_each_neighbour<MANY>(A, i, nb, n, pair);
   }
   if (EV) finish_site(A, i, valid, fi, esum, vsum, 0.0, 0.0);
   else finish_force(A, i, valid, fi);
@@ -215,6 +225,7 @@ __device__ __forceinline__ double eam_fp(const EamTables &T, double rho, double 
 // pass 1: density at atoms and node Gauss points (pair_eam.cpp:707-812), then
 // F' at the site itself into xs[i].w (pair_eam.cpp:819-833 for atoms; for a
 // node the reference's rhoi = noderho at :901-903).
+template <bool MANY>
 __global__ void __launch_bounds__(128, 8) k_eam_rho(PairArgs A, EamTables T, double *rho_out,
                                                  double *phi_site) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -236,7 +247,7 @@ __global__ void __launch_bounds__(128, 8) k_eam_rho(PairArgs A, EamTables T, dou
       rho += ((c.x * p + c.y) * p + c.z) * p + c.w;
     }
   };
-  for_each_neighbour(A, nb, n, pair);
+  for_each_neighbour<MANY>(A, i, nb, n, pair);
   int slot = i;
   if (i >= A.na) {
     int e = (i - A.na) / NG, g = (i - A.na) % NG;
@@ -266,7 +277,7 @@ __global__ void k_eam_site_fp(double4 *xs, const int *act_gid, const int *nact_d
 }
 
 // pass 2: forces (pair_eam.cpp:845-1028)
-template <bool EV>
+template <bool EV, bool MANY>
 __global__ void __launch_bounds__(128, EV ? 4 : 6) k_eam_force(PairArgs A, EamTables T, const double *phi_site) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   bool valid = i < A.nsi;
@@ -311,7 +322,7 @@ __global__ void __launch_bounds__(128, EV ? 4 : 6) k_eam_force(PairArgs A, EamTa
         }
       }
     };
-    for_each_neighbour(A, nb, n, pair);
+    for_each_neighbour<MANY>(A, i, nb, n, pair);
     if (EV && A.eflag) {
       double phi = phi_site[i];
       eemb_site = phi;
@@ -419,6 +430,8 @@ void pair_compute(Ctx &c, int eflag, int vflag) {
   A.ne = c.ne;
   A.nsi = nsi;
   for (int d = 0; d < 3; d++) A.L[d] = c.prd[d];
+  A.reps = c.rep_d.p;
+  A.site_rep = c.nrep > 1 ? c.site_rep.p : nullptr;
   A.f = c.f.p;
   A.gaussf = c.gaussf.p;
   if (eflag & CACB200_ENERGY_ATOM) {
@@ -443,12 +456,18 @@ void pair_compute(Ctx &c, int eflag, int vflag) {
   A.escale_node = nodal_weight / 2.0;
   if (c.pp.style == CACB200_PAIR_EAM && c.nodal_energy_weight >= 0.0)
     A.escale_node = c.nodal_energy_weight / 2.0;
+  c.escale_node_last = A.escale_node;
 
   if (c.pp.style == CACB200_PAIR_LJ) {
     LjParams P{c.pp.cut * c.pp.cut, c.pp.lj1, c.pp.lj2, c.pp.lj3, c.pp.lj4, c.pp.offset};
     KernelTimer t(c, "pair_lj");
-    if (eflag || vflag) k_lj<true><<<nb, T, 0, c.stream>>>(A, P);
-    else k_lj<false><<<nb, T, 0, c.stream>>>(A, P);
+    if (c.nrep > 1) {
+      if (eflag || vflag) k_lj<true, true><<<nb, T, 0, c.stream>>>(A, P);
+      else k_lj<false, true><<<nb, T, 0, c.stream>>>(A, P);
+    } else {
+      if (eflag || vflag) k_lj<true, false><<<nb, T, 0, c.stream>>>(A, P);
+      else k_lj<false, false><<<nb, T, 0, c.stream>>>(A, P);
+    }
   } else if (c.pp.style == CACB200_PAIR_EAM) {
     EamTables Tb;
     Tb.rz = c.rz.p;
@@ -464,7 +483,8 @@ void pair_compute(Ctx &c, int eflag, int vflag) {
     c.phi_site.reserve(std::max(nsi, 1));
     {
       KernelTimer t(c, "eam_rho");
-      k_eam_rho<<<nb, T, 0, c.stream>>>(A, Tb, c.rho.p, c.phi_site.p);
+      if (c.nrep > 1) k_eam_rho<true><<<nb, T, 0, c.stream>>>(A, Tb, c.rho.p, c.phi_site.p);
+      else k_eam_rho<false><<<nb, T, 0, c.stream>>>(A, Tb, c.rho.p, c.phi_site.p);
     }
     if (c.ne) {
       KernelTimer t(c, "eam_site_fp");
@@ -473,8 +493,13 @@ void pair_compute(Ctx &c, int eflag, int vflag) {
     }
     {
       KernelTimer t(c, "eam_force");
-      if (eflag || vflag) k_eam_force<true><<<nb, T, 0, c.stream>>>(A, Tb, c.phi_site.p);
-      else k_eam_force<false><<<nb, T, 0, c.stream>>>(A, Tb, c.phi_site.p);
+      if (c.nrep > 1) {
+        if (eflag || vflag) k_eam_force<true, true><<<nb, T, 0, c.stream>>>(A, Tb, c.phi_site.p);
+        else k_eam_force<false, true><<<nb, T, 0, c.stream>>>(A, Tb, c.phi_site.p);
+      } else {
+        if (eflag || vflag) k_eam_force<true, false><<<nb, T, 0, c.stream>>>(A, Tb, c.phi_site.p);
+        else k_eam_force<false, false><<<nb, T, 0, c.stream>>>(A, Tb, c.phi_site.p);
+      }
     }
   } else {
     throw Error(CACB200_ESTATE, "no pair style set");

@@ -3,13 +3,14 @@
 //
 // Every site of the site table gets, each step, a 32-bit fixed-point copy of
 // its FP64 position relative to the box corner, q = rint((x - lo) 2^k), with
-// k chosen from the box so that the box plus a 64 A margin (element sites may
-// lie outside the box) fits in an int.  A pair's separation is then
+// k chosen per box dimension so that the box length plus a 64 A margin
+// (element sites may lie outside the box) fits in an int.  A pair's
+// separation is then
 //     x_i - (x_j + s L) = (q_i - q_j - s Lq) 2^-k,
 // an exact integer difference (wrap-around 32-bit arithmetic is exact while
 // the true difference is small) rounded once to FP32: no FP32 sum ever
-// carries a box-sized coordinate.  The quantum 2^-k is 2.4e-7 A for boxes up
-// to ~440 A.  A site's record is 16 bytes, (qx, qy, qz, F'), so one 128-bit
+// carries a box-sized coordinate.  The quantum 2^-k is 2.4e-7 A for box
+// lengths up to ~440 A, 9.5e-7 A up to ~1.9e3 A.  A site's record is 16 bytes, (qx, qy, qz, F'), so one 128-bit
 // load brings everything a pair needs from its neighbour.
 //
 // What stays FP64 (as the mixed form specifies): positions and velocities and
@@ -30,20 +31,38 @@ namespace {
 
 inline int nblk(long n, int t) { return (int)((n + t - 1) / t); }
 
+// Fixed-point frame of a single system; batches read each replica's from its
+// descriptor.
 struct FixGrid {
   double lo[3];
-  double scale;    // 2^k
-  float inv;       // 2^-k
-  int Lq[3];       // rint(L 2^k)
+  double scale[3];
+  float inv[3];
+  int Lq[3];
+  const Rep *reps;          // batches (null for one system)
+  const int *site_rep;      // [nsite_i]
+  const int *elem_rep;      // [ne]
+  const int *act_gid;       // active lattice sites -> element * 729 + site
+  int nsi;
 };
 
 __device__ __forceinline__ void pack_one(const double4 *xs, int k, const FixGrid &G, int4 *pos, int *bad) {
   double4 p = xs[k];
   double q[3] = {p.x, p.y, p.z};
+  double lo[3] = {G.lo[0], G.lo[1], G.lo[2]};
+  double sc[3] = {G.scale[0], G.scale[1], G.scale[2]};
+  if (G.reps) {
+    int r = k < G.nsi ? G.site_rep[k] : G.elem_rep[G.act_gid[k - G.nsi] / NU];
+    const Rep *R = G.reps + r;
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+      lo[d] = R->b.lo[d];
+      sc[d] = R->qscale[d];
+    }
+  }
   int o[3];
 #pragma unroll
   for (int d = 0; d < 3; d++) {
-    double rel = (q[d] - G.lo[d]) * G.scale;
+    double rel = (q[d] - lo[d]) * sc[d];
     if (!(rel > -2147483000.0 && rel < 2147483000.0)) {
       atomicExch(bad, 1);
       rel = 0.0;
@@ -81,21 +100,46 @@ __device__ __forceinline__ float fix_delta(int qi, int qj, int s, int Lq, float 
   return (float)(int)d * inv;
 }
 
+// fixed-point frame (box lengths and quanta) of i-site i's replica
+struct SiteFix {
+  int Lq[3];
+  float inv[3];
+};
+__device__ __forceinline__ SiteFix site_fix(const Args32 &A, int i) {
+  SiteFix F;
+  if (A.G.reps) {
+    const Rep *R = A.G.reps + A.G.site_rep[i];
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+      F.Lq[d] = R->Lq[d];
+      F.inv[d] = R->qinv[d];
+    }
+  } else {
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+      F.Lq[d] = A.G.Lq[d];
+      F.inv[d] = A.G.inv[d];
+    }
+  }
+  return F;
+}
+
 // separation of site i (record oi) from neighbour entry v; wj = F'(j)
-__device__ __forceinline__ void sep32(const Args32 &A, const int4 &oi, int v, float &dx, float &dy, float &dz,
-                                      float &wj) {
+__device__ __forceinline__ void sep32(const Args32 &A, const SiteFix &F, const int4 &oi, int v, float &dx,
+                                      float &dy, float &dz, float &wj) {
   int j = v >> IMG_BITS, code = v & ((1 << IMG_BITS) - 1);
   int4 oj = __ldg(A.pos + j);
   int s[3] = {0, 0, 0};
   if (code != IMG_ZERO) img_decode(code, s[0], s[1], s[2]);
-  dx = fix_delta(oi.x, oj.x, s[0], A.G.Lq[0], A.G.inv);
-  dy = fix_delta(oi.y, oj.y, s[1], A.G.Lq[1], A.G.inv);
-  dz = fix_delta(oi.z, oj.z, s[2], A.G.Lq[2], A.G.inv);
+  dx = fix_delta(oi.x, oj.x, s[0], F.Lq[0], F.inv[0]);
+  dy = fix_delta(oi.y, oj.y, s[1], F.Lq[1], F.inv[1]);
+  dz = fix_delta(oi.z, oj.z, s[2], F.Lq[2], F.inv[2]);
   wj = __int_as_float(oj.w);
 }
 
 template <class F>
 __device__ __forceinline__ void for_each32(const Args32 &A, int i, const int4 &oi, F &&f) {
+  const SiteFix fx = site_fix(A, i);
   int n = A.num[i];
   const int *nb = A.nbr + i;
   int k = 0;
@@ -103,16 +147,16 @@ __device__ __forceinline__ void for_each32(const Args32 &A, int i, const int4 &o
     int v0 = nb[(size_t)k * A.nsi], v1 = nb[(size_t)(k + 1) * A.nsi];
     int v2 = nb[(size_t)(k + 2) * A.nsi], v3 = nb[(size_t)(k + 3) * A.nsi];
     float d[4][4];
-    sep32(A, oi, v0, d[0][0], d[0][1], d[0][2], d[0][3]);
-    sep32(A, oi, v1, d[1][0], d[1][1], d[1][2], d[1][3]);
-    sep32(A, oi, v2, d[2][0], d[2][1], d[2][2], d[2][3]);
-    sep32(A, oi, v3, d[3][0], d[3][1], d[3][2], d[3][3]);
+    sep32(A, fx, oi, v0, d[0][0], d[0][1], d[0][2], d[0][3]);
+    sep32(A, fx, oi, v1, d[1][0], d[1][1], d[1][2], d[1][3]);
+    sep32(A, fx, oi, v2, d[2][0], d[2][1], d[2][2], d[2][3]);
+    sep32(A, fx, oi, v3, d[3][0], d[3][1], d[3][2], d[3][3]);
 #pragma unroll
     for (int u = 0; u < 4; u++) f(d[u][0], d[u][1], d[u][2], d[u][3]);
   }
   for (; k < n; k++) {
     float dx, dy, dz, wj;
-    sep32(A, oi, nb[(size_t)k * A.nsi], dx, dy, dz, wj);
+    sep32(A, fx, oi, nb[(size_t)k * A.nsi], dx, dy, dz, wj);
     f(dx, dy, dz, wj);
   }
 }
@@ -332,17 +376,18 @@ __global__ void k_reduce_partials32(const double *partial, int nblocks, double *
 
 FixGrid make_fix_grid(const Ctx &c) {
   FixGrid G;
-  double lmax = std::max(c.prd[0], std::max(c.prd[1], c.prd[2]));
-  int k = 24;
-  while (k > 8 && (lmax + 64.0) * std::ldexp(1.0, k) > 2147483000.0) k--;
-  if ((lmax + 64.0) * std::ldexp(1.0, k) > 2147483000.0)
-    throw Error(CACB200_EINVAL, "box too large for the mixed-precision fixed-point positions");
-  G.scale = std::ldexp(1.0, k);
-  G.inv = std::ldexp(1.0f, -k);
+  const Rep &r0 = c.rep_h[0];
   for (int d = 0; d < 3; d++) {
-    G.lo[d] = c.boxlo[d];
-    G.Lq[d] = (int)std::llround(c.prd[d] * G.scale);
+    G.lo[d] = r0.b.lo[d];
+    G.scale[d] = r0.qscale[d];
+    G.inv[d] = r0.qinv[d];
+    G.Lq[d] = r0.Lq[d];
   }
+  G.reps = c.nrep > 1 ? c.rep_d.p : nullptr;
+  G.site_rep = c.site_rep.p;
+  G.elem_rep = c.elem_rep.p;
+  G.act_gid = c.act_gid.p;
+  G.nsi = c.nsite_i();
   return G;
 }
 
@@ -406,6 +451,7 @@ void pair_compute_mixed(Ctx &c, int eflag, int vflag) {
   A.vscale_node = nodal_weight / 2.0;
   A.escale_node = nodal_weight / 2.0;
   if (c.pp.style == CACB200_PAIR_EAM && c.nodal_energy_weight >= 0.0) A.escale_node = c.nodal_energy_weight / 2.0;
+  c.escale_node_last = A.escale_node;
   bool ev = eflag || vflag;
   if (c.pp.style == CACB200_PAIR_LJ) {
     Lj32 P{(float)(c.pp.cut * c.pp.cut), (float)c.pp.lj1, (float)c.pp.lj2, (float)c.pp.lj3, (float)c.pp.lj4,

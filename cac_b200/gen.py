@@ -40,7 +40,7 @@ from __future__ import annotations
 
 import dataclasses
 import math
-from typing import Optional
+from typing import List, Optional
 
 import numpy as np
 
@@ -225,6 +225,37 @@ def eam_4m_strained(seed: int = 3) -> System:
     x-strain (nx=20, ny=10: 32,400 atoms per layer, 129 layers; 125 layers of
     400 elements per region; 4,979,600 atom+IP sites), 300 K."""
     return build_slab(20, 10, 125, 129, temperature=300.0, strain=0.03, seed=seed)
+
+
+def replica(target_atoms: int, target_elements: int, *, temperature: float, strain: float,
+            seed: int) -> System:
+    """A slab with about ``target_atoms`` atoms and ``target_elements``
+    elements: the cross-section (nx, ny >= 2, 1) is chosen so that at least
+    3 atomic layers and 1 element layer per region fit both targets; the
+    realised counts are multiples of the layer sizes."""
+    nxy = max(2, min(target_atoms // 486, target_elements // 4))
+    nx = max(2, int(math.ceil(math.sqrt(nxy))))
+    ny = max(1, int(round(nxy / nx)))
+    per_layer = 162 * nx * ny
+    la = max(3, 3 * int(round(target_atoms / per_layer / 3.0)))
+    le = max(1, int(round(target_elements / (4.0 * nx * ny))))
+    return build_slab(nx, ny, le, la, temperature=temperature, strain=strain, seed=seed)
+
+
+def replica_set(n: int = 256, seed: int = 11, atoms=(2000, 64000), elements=(50, 2000),
+                temperature=(10.0, 500.0), strain=(0.0, 0.05)) -> List[System]:
+    """Independent replicas for batched runs: atom and element targets
+    log-uniform in the given ranges, temperature and x-strain uniform, every
+    draw from one seeded generator."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(n):
+        ta = int(round(math.exp(rng.uniform(math.log(atoms[0]), math.log(atoms[1])))))
+        te = int(round(math.exp(rng.uniform(math.log(elements[0]), math.log(elements[1])))))
+        t = float(rng.uniform(*temperature))
+        st = float(rng.uniform(*strain))
+        out.append(replica(ta, te, temperature=t, strain=st, seed=int(rng.integers(1 << 30))))
+    return out
 
 
 def tiny(seed: int = 7, temperature: float = 50.0) -> System:

@@ -75,6 +75,23 @@ int cacb200_upload_system(cacb200_ctx *ctx, const double boxlo[3], const double 
                           int natoms, const double *x, const double *v,
                           int nelements, const double *nodex, const double *nodev,
                           double mass);
+/* Upload a batch of independent replicas (no reference counterpart: the
+ * reference runs one system per process; a batch replaces nreplicas separate
+ * runs of the same pair style).  Replica r has natoms[r] atoms,
+ * nelements[r] elements and its own periodic box boxlo/boxhi[3r..3r+2];
+ * x, v, nodex, nodev concatenate the replicas in order.  Every other call
+ * (state, forces, stepping, snapshots) then acts on all replicas at once,
+ * arrays concatenated the same way.  Half lists are single-system only. */
+int cacb200_upload_batch(cacb200_ctx *ctx, int nreplicas, const int *natoms,
+                         const int *nelements, const double *boxlo, const double *boxhi,
+                         const double *x, const double *v, const double *nodex,
+                         const double *nodev, double mass);
+/* Potential energy of each replica (or of the single system) from the last
+ * evaluation made with CACB200_ENERGY_ATOM: per-atom energies plus node
+ * energies times the node weight, i.e. eng_vdwl split by replica
+ * (Pair::ev_tally, pair.cpp:428-482). */
+int cacb200_replica_energy(cacb200_ctx *ctx, double *energy /* [nreplicas] */);
+
 /* Overwrite positions/velocities of the current system (same counts; NULL
  * leaves an array unchanged).  Neighbour lists are kept, as the reference
  * keeps them between rebuilds; call cacb200_build_lists after moves larger
@@ -167,6 +184,15 @@ int cacb200_minimize_fire(cacb200_ctx *ctx, double etol, double ftol, int maxite
  * traffic. */
 int cacb200_snapshot(cacb200_ctx *ctx);
 int cacb200_restore(cacb200_ctx *ctx);
+
+/* cacb200_run_nve replays each rebuild cycle (every steps) as two CUDA
+ * graphs, with one host wait per cycle to read the rebuild's overflow flags.
+ * Enabled by default; disabling runs every launch eagerly (same kernels,
+ * same order, same results).  No reference counterpart (Verlet::run,
+ * verlet.cpp:192-360, calls the styles step by step). */
+int cacb200_set_graphs(cacb200_ctx *ctx, int enable);
+/* graph launches made so far by this context */
+int cacb200_graph_launches(cacb200_ctx *ctx, long long *count);
 
 /* Kernel timing: when enabled, every launch is bracketed by CUDA events and
  * per-kernel totals accumulate (ms, launches) until reset. */
