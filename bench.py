@@ -428,6 +428,126 @@ def b200_arm(args, rank, local, ws, dist):
     eng.close()
 
 
+def serve_jobs(n: int, seed: int):
+    """The serving stream: job sizes (atoms log-uniform 1k-200k, elements
+    20-5,000, x-strain U(0, 5 %)), kinds (70 % FIRE to fmax 1e-6 eV/A capped at
+    5,000 iterations, from rest; 30 % 2,000-step NVE at 300 K) and Poisson
+    arrival times at 50 jobs/s, all from one seeded generator."""
+    import numpy as np
+    from cac_b200 import gen
+    rng = np.random.default_rng(seed)
+    out, t = [], 0.0
+    for k in range(n):
+        ta = int(round(np.exp(rng.uniform(np.log(1000), np.log(200000)))))
+        te = int(round(np.exp(rng.uniform(np.log(20), np.log(5000)))))
+        st = float(rng.uniform(0.0, 0.05))
+        fire = bool(rng.uniform() < 0.7)
+        sys_ = gen.replica(ta, te, temperature=0.0 if fire else 300.0, strain=st, seed=int(rng.integers(1 << 30)))
+        t += float(rng.exponential(1.0 / 50.0))
+        out.append((t, sys_, fire))
+    return out
+
+
+def serve_arm(args):
+    """Serve a Poisson stream of jobs; report throughput, latency percentiles
+    and the same jobs run one after another in FP64 through the single-system
+    engine (on a bounded prefix of the stream).  NVE jobs run as restarted
+    trajectories of --segment steps (the reference's dynamics heat up without
+    bound on longer runs)."""
+    import numpy as np
+    from cac_b200 import api, gen
+    stream = serve_jobs(args.jobs, 101)
+    tmp = tempfile.mkdtemp()
+    setfl = os.path.join(tmp, "cu.setfl")
+    gen.write_setfl(gen.EamParams(), setfl)
+
+    def set_pair(obj):
+        if args.pair == "eam":
+            obj.pair_eam(setfl)
+        else:
+            obj.pair_lj(0.4093, 2.338, 5.5)
+
+    srv = api.Server(0, workers=args.workers, budget_gb=120.0,
+                     precision=api.MIXED if args.form == "mixed" else api.FP64)
+    set_pair(srv)
+    srv.neighbor(1.0, 10)
+    srv.segment(args.segment)
+    srv.start()
+    t0 = time.perf_counter()
+    ids = []
+    for t_arr, s, fire in stream:
+        delay = t_arr - (time.perf_counter() - t0)
+        if delay > 0:
+            time.sleep(delay)
+        if fire:
+            ids.append(srv.submit(s, api.JOB_FIRE, 5000, 0.001, 0.0, 1e-6))
+        else:
+            ids.append(srv.submit(s, api.JOB_NVE, 2000, 0.001))
+    lat, site_steps, codes, failed = [], 0.0, {}, {}
+    for j, (t_arr, s, fire) in zip(ids, stream):
+        rc = srv.wait(j)
+        if rc != 0:
+            msg = srv.last_error()
+            failed[msg] = failed.get(msg, 0) + 1
+            lat.append(srv.times(j)[2])
+            continue
+        _, _, _, _, _, it, code, times = srv.result(j)
+        lat.append(times[2])
+        site_steps += s.nsites * it
+        if fire:
+            codes[str(code)] = codes.get(str(code), 0) + 1
+        srv.release(j)
+    makespan = time.perf_counter() - t0
+    srv.close()
+    lat = np.array(lat)
+
+    # serial FP64: the same jobs one at a time through one context
+    serial_s, nser = 0.0, min(args.serial_jobs, len(stream))
+    e = api.Engine(0)
+    for t_arr, s, fire in stream[:nser]:
+        e.upload(s)
+        set_pair(e)
+        e.neighbor(1.0, 10)
+        e.set_precision(api.FP64)
+        a = time.perf_counter()
+        try:
+            if fire:
+                e.minimize_fire(0.0, 1e-6, 5000, 0.001, norm="max")
+            else:
+                e.snapshot()
+                done = 0
+                while done < 2000:
+                    if done:
+                        e.restore()
+                    e.setup()
+                    k = min(args.segment, 2000 - done)
+                    done += k
+                    e.run_nve(k, 0.001, eflag=api.ENERGY_GLOBAL if done == 2000 else 0)
+                e.energy(peratom=False)
+        except api.CacB200Error:
+            pass
+        serial_s += time.perf_counter() - a
+    e.close()
+    line = {
+        "metric": METRIC, "value": site_steps / makespan, "unit": UNIT, "n_gpus": 1, "steps": None,
+        "warmup": 0, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64" if args.form == "fp64" else "f32/f64",
+        "data": "synthetic (seeded generator; no dataset exists for this path)",
+        "config": {"workload": "serve", "jobs": len(stream), "arrivals": "Poisson 50/s",
+                   "pair": "eam/alloy" if args.pair == "eam" else "lj/cut",
+                   "mix": "70% FIRE (ftol 1e-6 max-norm, cap 5000), 30% NVE 2000 steps "
+                          f"(restarted every {args.segment})",
+                   "workers": args.workers, "budget_gb": 120.0, "precision": args.form},
+        "serving": {"jobs_per_s": len(stream) / makespan, "makespan_s": makespan,
+                    "latency_p50_s": float(np.percentile(lat, 50)),
+                    "latency_p99_s": float(np.percentile(lat, 99)), "fire_stop_codes": codes,
+                    "failed": failed,
+                    "serial_fp64_jobs_per_s": nser / serial_s if serial_s > 0 else None,
+                    "serial_fp64_sample_jobs": nser},
+    }
+    print(json.dumps(line))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -437,6 +557,11 @@ def main():
     ap.add_argument("--workload", default="eam_1m")
     ap.add_argument("--form", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--jobs", type=int, default=64, help="serve workload: jobs in the stream")
+    ap.add_argument("--workers", type=int, default=16, help="serve workload: worker contexts")
+    ap.add_argument("--serial-jobs", type=int, default=8,
+                    help="serve workload: jobs of the stream timed one at a time in FP64")
+    ap.add_argument("--pair", default="lj", choices=["lj", "eam"], help="serve workload: pair style")
     ap.add_argument("--segment", type=int, default=50,
                     help="steps per trajectory from the seeded initial state (the reference's CAC "
                          "dynamics heat up unboundedly after ~100 steps, so long runs restart)")
@@ -449,6 +574,9 @@ def main():
             if args.warmup > 5:
                 args.warmup = 3
             reference_arm(args, rank, ws)
+        elif args.workload == "serve":
+            if rank == 0:
+                serve_arm(args)
         else:
             b200_arm(args, rank, local, ws, dist)
     finally:

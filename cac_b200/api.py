@@ -49,6 +49,22 @@ SIGNATURES = [
                                        _dp, _dp, _dp, _dp, C.c_double]),
     ("cacb200_replica_energy", C.c_int, [C.c_void_p, _dp]),
     ("cacb200_set_graphs", C.c_int, [C.c_void_p, C.c_int]),
+    ("cacb200_server_create", C.c_int, [C.c_int, C.c_int, C.c_double, C.c_int, C.POINTER(C.c_void_p)]),
+    ("cacb200_server_set_lj", C.c_int, [C.c_void_p, C.c_double, C.c_double, C.c_double]),
+    ("cacb200_server_set_eam", C.c_int, [C.c_void_p, C.c_int, C.c_double, C.c_int, C.c_double, C.c_double,
+                                         _dp, _dp, _dp]),
+    ("cacb200_server_set_neighbor", C.c_int, [C.c_void_p, C.c_double, C.c_int]),
+    ("cacb200_server_set_segment", C.c_int, [C.c_void_p, C.c_int]),
+    ("cacb200_server_start", C.c_int, [C.c_void_p]),
+    ("cacb200_server_submit", C.c_int, [C.c_void_p, C.c_int, _dp, _dp, C.c_int, _dp, _dp, C.c_int, _dp, _dp,
+                                        C.c_double, C.c_int, C.c_double, C.c_double, C.c_double,
+                                        C.POINTER(C.c_int64)]),
+    ("cacb200_server_wait", C.c_int, [C.c_void_p, C.c_int64, C.c_double]),
+    ("cacb200_server_result", C.c_int, [C.c_void_p, C.c_int64, _dp, _dp, _dp, _dp, _dp, C.POINTER(C.c_int),
+                                        C.POINTER(C.c_int), _dp]),
+    ("cacb200_server_release", C.c_int, [C.c_void_p, C.c_int64]),
+    ("cacb200_server_last_error", C.c_char_p, [C.c_void_p]),
+    ("cacb200_server_destroy", C.c_int, [C.c_void_p]),
     ("cacb200_graph_launches", C.c_int, [C.c_void_p, C.POINTER(C.c_longlong)]),
     ("cacb200_set_state", C.c_int, [C.c_void_p, _dp, _dp, _dp, _dp]),
     ("cacb200_get_state", C.c_int, [C.c_void_p, _dp, _dp, _dp, _dp]),
@@ -355,3 +371,99 @@ class Engine:
             nm = raw[32 * k:32 * k + 32].split(b"\0", 1)[0].decode()
             out[nm] = (float(ms[k]), int(la[k]))
         return out
+
+
+JOB_NVE = 0
+JOB_FIRE = 1
+
+
+class Server:
+    """A ``cacb200_server``: jobs (one system each, ``run N`` under NVE or a
+    FIRE minimisation) served concurrently by worker threads that each own a
+    device context, admitted first come first served under a memory budget."""
+
+    def __init__(self, device: int = 0, workers: int = 8, budget_gb: float = 120.0, precision: int = FP64):
+        self.lib = load()
+        h = C.c_void_p()
+        rc = self.lib.cacb200_server_create(device, workers, budget_gb * 1e9, precision, C.byref(h))
+        if rc != 0:
+            raise CacB200Error(f"cacb200_server_create failed ({rc})")
+        self.h = h
+        self._shapes = {}
+
+    def _check(self, rc: int, what: str):
+        if rc != 0:
+            raise CacB200Error(f"{what} failed ({rc}): {self.last_error()}")
+
+    def last_error(self) -> str:
+        msg = self.lib.cacb200_server_last_error(self.h)
+        return msg.decode() if msg else ""
+
+    def pair_lj(self, epsilon: float, sigma: float, cut: float) -> None:
+        self._check(self.lib.cacb200_server_set_lj(self.h, epsilon, sigma, cut), "server_set_lj")
+
+    def pair_eam(self, setfl) -> None:
+        t = read_setfl(setfl) if isinstance(setfl, str) else setfl
+        self._check(self.lib.cacb200_server_set_eam(self.h, t["nrho"], t["drho"], t["nr"], t["dr"], t["cut"],
+                                                    _p(t["frho"]), _p(t["rhor"]), _p(t["z2r"])), "server_set_eam")
+
+    def neighbor(self, skin: float, every: int) -> None:
+        self._check(self.lib.cacb200_server_set_neighbor(self.h, skin, every), "server_set_neighbor")
+
+    def segment(self, steps: int) -> None:
+        self._check(self.lib.cacb200_server_set_segment(self.h, steps), "server_set_segment")
+
+    def start(self) -> None:
+        self._check(self.lib.cacb200_server_start(self.h), "server_start")
+
+    def submit(self, system, kind: int, steps: int, dt: float = 0.001, etol: float = 0.0,
+               ftol: float = 0.0) -> int:
+        x = np.ascontiguousarray(system.x, dtype=np.float64)
+        v = np.ascontiguousarray(system.v, dtype=np.float64)
+        nx = np.ascontiguousarray(system.nodex, dtype=np.float64)
+        nv = np.ascontiguousarray(system.nodev, dtype=np.float64)
+        lo = np.ascontiguousarray(system.boxlo, dtype=np.float64)
+        hi = np.ascontiguousarray(system.boxhi, dtype=np.float64)
+        job = C.c_int64()
+        self._check(self.lib.cacb200_server_submit(self.h, kind, _p(lo), _p(hi), x.shape[0], _p(x), _p(v),
+                                                   nx.shape[0], _p(nx), _p(nv), float(system.mass), steps, dt,
+                                                   etol, ftol, C.byref(job)), "server_submit")
+        self._shapes[job.value] = (x.shape[0], nx.shape[0])
+        return job.value
+
+    def wait(self, job: int, timeout: float = -1.0) -> int:
+        """The job's status once it ends (0 = done), or CACB200_ETIMEDOUT."""
+        return self.lib.cacb200_server_wait(self.h, job, timeout)
+
+    def times(self, job: int) -> np.ndarray:
+        """[queued, running, submit to end] seconds of an ended job, failed or not."""
+        t = np.zeros(3)
+        self.lib.cacb200_server_result(self.h, job, None, None, None, None, None, None, None, _p(t))
+        return t
+
+    def result(self, job: int):
+        """(x, v, nodex, nodev, energy, iterations, stop_code, times[queued, running, total])"""
+        na, ne = self._shapes[job]
+        x, v = np.zeros((na, 3)), np.zeros((na, 3))
+        nx, nv = np.zeros((ne, 8, 3)), np.zeros((ne, 8, 3))
+        e = np.zeros(1)
+        it, code = C.c_int(), C.c_int()
+        t = np.zeros(3)
+        self._check(self.lib.cacb200_server_result(self.h, job, _p(x), _p(v), _p(nx), _p(nv), _p(e),
+                                                   C.byref(it), C.byref(code), _p(t)), "server_result")
+        return x, v, nx, nv, float(e[0]), it.value, code.value, t
+
+    def release(self, job: int) -> None:
+        self._check(self.lib.cacb200_server_release(self.h, job), "server_release")
+        self._shapes.pop(job, None)
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self.lib.cacb200_server_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

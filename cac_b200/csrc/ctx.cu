@@ -142,8 +142,7 @@ void upload_system(Ctx &c, int nrep, const int *rna, const int *rne, const doubl
   c.planned = false;
   c.gen++;
   c.step = c.last_build_step = 0;
-  c.xs.release();
-  // site table at full capacity: atoms, Gauss points and every lattice site
+  // site table at full capacity (kept across uploads while large enough): atoms, Gauss points and every lattice site
   size_t ns = (size_t)na + NG * (size_t)ne + (size_t)ne * NU;
   c.xs.reserve(ns);
   c.dev_nact.reserve(1);

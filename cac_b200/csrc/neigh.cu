@@ -376,10 +376,6 @@ __device__ __forceinline__ void try_atom(const BuildArgs &A, const Query &q, int
   int s[3] = {W[0] - q.ti[0], W[1] - q.ti[1], W[2] - q.ti[2]};
   bool zero = (s[0] == 0 && s[1] == 0 && s[2] == 0);
   if (q.iatom && j == q.i && zero) return;
-  if (s[0] < -1 || s[0] > 1 || s[1] < -1 || s[1] > 1 || s[2] < -1 || s[2] > 1) {
-    atomicExch(&A.overflow[2], 1);
-    return;
-  }
   double4 xj = A.xs[j];
   double qq[3] = {xj.x, xj.y, xj.z};
   if (!zero) {
@@ -389,6 +385,12 @@ __device__ __forceinline__ void try_atom(const BuildArgs &A, const Query &q, int
   }
   double rsq = rsq_rn(__dsub_rn(q.xi[0], qq[0]), __dsub_rn(q.xi[1], qq[1]), __dsub_rn(q.xi[2], qq[2]));
   if (!(rsq <= A.cutneighsq)) return;
+  // a neighbour beyond the first periodic image cannot be stored (the box is
+  // shorter than twice the cutoff)
+  if (s[0] < -1 || s[0] > 1 || s[1] < -1 || s[1] > 1 || s[2] < -1 || s[2] > 1) {
+    atomicExch(&A.overflow[2], 1);
+    return;
+  }
   int code = img_code(s[0], s[1], s[2]);
   emit(A, q.i, nf, A.raw_full, A.img_full, j, code);
   if (A.want_half && q.iatom) {
@@ -450,10 +452,10 @@ __device__ void element_candidates(const BuildArgs &A, const Query &q, int &nf, 
           double R = ce.w + dmax + A.cutneigh + 1e-6;
           double dcx = p[0] - ce.x, dcy = p[1] - ce.y, dcz = p[2] - ce.z;
           if (dcx * dcx + dcy * dcy + dcz * dcz > R * R) continue;
-          if (s[0] < -1 || s[0] > 1 || s[1] < -1 || s[1] > 1 || s[2] < -1 || s[2] > 1) {
-            atomicExch(&A.overflow[2], 1);
-            continue;
-          }
+          // a box shorter than the candidate sphere's diameter shows an element
+          // under two images; only a site actually within the cutoff at an
+          // image beyond the first is an error (checked at the distance test)
+          const bool far_image = s[0] < -1 || s[0] > 1 || s[1] < -1 || s[1] > 1 || s[2] < -1 || s[2] > 1;
           // lattice-index box of the sites whose affine position is within cutneigh + dmax
           double rel[3] = {p[0] - fr[0], p[1] - fr[1], p[2] - fr[2]};
           int lo[3], hi[3];
@@ -475,7 +477,7 @@ __device__ void element_candidates(const BuildArgs &A, const Query &q, int &nf, 
 #pragma unroll
             for (int d = 0; d < 3; d++)
               g[3 * k + d] = s[d] ? __dadd_rn(nx[3 * k + d], sL[d]) : nx[3 * k + d];
-          int code = img_code(s[0], s[1], s[2]);
+          int code = far_image ? 0 : img_code(s[0], s[1], s[2]);
           double qcen[3] = {0, 0, 0};
           if (!zero) {
             qcen[0] = s[0] ? __dadd_rn(ce.x, sL[0]) : ce.x;
@@ -510,6 +512,10 @@ __device__ void element_candidates(const BuildArgs &A, const Query &q, int &nf, 
                 }
                 double rsq = rsq_rn(dx, dy, dz);
                 if (!(rsq <= A.cutneighsq)) continue;
+                if (far_image) {
+                  atomicExch(&A.overflow[2], 1);
+                  continue;
+                }
                 int val = KIND_SITE | (e * NU + u);
                 emit(A, q.i, nf, A.raw_full, A.img_full, val, code);
                 if (A.want_half) {

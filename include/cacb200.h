@@ -200,6 +200,54 @@ int cacb200_profile(cacb200_ctx *ctx, int enable);
 int cacb200_profile_read(cacb200_ctx *ctx, int max, char *names /* max*32 */,
                          double *total_ms, int64_t *launches, int *count);
 
+/* ---------------------------------------------------------------- serving */
+
+/* A job server (no reference counterpart: the reference runs one input deck
+ * per process).  Worker threads each own one context (own CUDA stream,
+ * buffers reused across jobs) and take jobs first come first served once the
+ * job's device-memory estimate fits the budget, so jobs of any size run
+ * concurrently and start as soon as room frees up.  A job is one system plus
+ * `run N` under fix nve (CACB200_JOB_NVE, steps = N) or `minimize etol ftol
+ * N` with the FIRE iterate and max-norm (CACB200_JOB_FIRE, steps = maxiter);
+ * it runs through the same context calls as a single run, so its results
+ * equal that run's bit for bit whatever else is being served.  Configure
+ * (pair style, neighbour settings) before cacb200_server_start.  Each worker
+ * keeps the buffers of the largest job it has run. */
+typedef struct cacb200_server cacb200_server;
+#define CACB200_JOB_NVE 0
+#define CACB200_JOB_FIRE 1
+int cacb200_server_create(int device, int nworkers, double budget_bytes, int precision,
+                          cacb200_server **out);
+int cacb200_server_set_lj(cacb200_server *s, double epsilon, double sigma, double cut);
+int cacb200_server_set_eam(cacb200_server *s, int nrho, double drho, int nr, double dr, double cut,
+                           const double *frho, const double *rhor, const double *z2r);
+int cacb200_server_set_neighbor(cacb200_server *s, double skin, int every);
+/* NVE jobs of more than `segment` steps run as trajectories of `segment`
+ * steps, each restarted from the job's initial state (device snapshot), the
+ * last one ending the job; 0 (default) runs one trajectory. */
+int cacb200_server_set_segment(cacb200_server *s, int segment);
+int cacb200_server_start(cacb200_server *s);
+/* Queue a job (arrays are copied).  CACB200_ENOMEM when the job alone
+ * exceeds the budget. */
+int cacb200_server_submit(cacb200_server *s, int kind, const double boxlo[3], const double boxhi[3],
+                          int natoms, const double *x, const double *v, int nelements,
+                          const double *nodex, const double *nodev, double mass, int steps,
+                          double dt, double etol, double ftol, int64_t *job);
+/* Block until the job ends (timeout_s < 0: no limit); returns its status
+ * (CACB200_OK, CACB200_ETIMEDOUT while still queued or running, or the
+ * job's error code). */
+int cacb200_server_wait(cacb200_server *s, int64_t job, double timeout_s);
+/* Final state, energy (eng_vdwl), iterations and FIRE stop code (-1 for
+ * NVE), and times in seconds: [queued, running, submit to end] (times are
+ * filled for failed jobs too, which return their error code). */
+int cacb200_server_result(cacb200_server *s, int64_t job, double *x, double *v, double *nodex,
+                          double *nodev, double *energy, int *niter, int *stop_code,
+                          double *times /* [3] */);
+int cacb200_server_release(cacb200_server *s, int64_t job);
+const char *cacb200_server_last_error(const cacb200_server *s);
+/* Finish running jobs, drop queued ones, join the workers. */
+int cacb200_server_destroy(cacb200_server *s);
+
 #ifdef __cplusplus
 }
 #endif
