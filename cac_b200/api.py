@@ -49,6 +49,8 @@ SIGNATURES = [
                                        _dp, _dp, _dp, _dp, C.c_double]),
     ("cacb200_replica_energy", C.c_int, [C.c_void_p, _dp]),
     ("cacb200_set_graphs", C.c_int, [C.c_void_p, C.c_int]),
+    ("cacb200_replica_energy_noalloc", C.c_int, [C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.POINTER(C.c_int),
+                                                 C.POINTER(C.c_int), C.c_double, _dp, C.c_void_p]),
     ("cacb200_server_create", C.c_int, [C.c_int, C.c_int, C.c_double, C.c_int, C.POINTER(C.c_void_p)]),
     ("cacb200_server_set_lj", C.c_int, [C.c_void_p, C.c_double, C.c_double, C.c_double]),
     ("cacb200_server_set_eam", C.c_int, [C.c_void_p, C.c_int, C.c_double, C.c_int, C.c_double, C.c_double,

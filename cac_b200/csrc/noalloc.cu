@@ -1,0 +1,114 @@
+// Per-replica potential energy without any device allocation.
+//
+// Some callers cannot allocate device memory: a host program that runs inside
+// another framework's memory pool (which has reserved the GPU's memory up
+// front and must stay the only allocator), or a serving loop whose other
+// streams must not be stalled, since cudaFree waits for the whole device.
+// This entry point is the same reduction as cacb200_replica_energy, but
+// its device scratch (the per-replica table of offsets and counts, and the
+// per-replica sums) lives in one fixed array of this file, set up once per
+// device, instead of buffers a context allocates.
+#include <cstdio>
+#include <mutex>
+#include <vector>
+
+#include "../../include/cacb200.h"
+#include "ctx.cuh"
+#include "device.cuh"
+
+namespace cacb200 {
+namespace {
+
+// Scratch for at most NOALLOC_MAX_REPLICAS replicas (96 KiB); every GPU that
+// loads the library holds it until the process exits.
+constexpr int NOALLOC_MAX_REPLICAS = CACB200_NOALLOC_MAX_REPLICAS;
+struct NoAllocScratch {
+  int meta[4][NOALLOC_MAX_REPLICAS];   // atom offset, atom count, element offset, element count
+  double sum[NOALLOC_MAX_REPLICAS];    // energy of each replica
+};
+static __device__ __align__(256) NoAllocScratch noalloc_scratch;
+
+// One block per replica: atoms' own energies plus node energies times the
+// node weight, summed in a fixed order (the kernel of cacb200_replica_energy
+// with its table and results in the fixed scratch).
+__global__ void k_replica_energy_fixed(const double *eatom, const double *enode, double node_weight,
+                                       NoAllocScratch *sc) {
+  const int r = blockIdx.x;
+  const int aoff = sc->meta[0][r], na = sc->meta[1][r], eoff = sc->meta[2][r], ne = sc->meta[3][r];
+  double s = 0.0;
+  for (int i = threadIdx.x; i < na; i += blockDim.x) s += eatom[aoff + i];
+  double t = 0.0;
+  for (int k = threadIdx.x; k < 8 * ne; k += blockDim.x) t += enode[8 * (size_t)eoff + k];
+  double v[1] = {s + node_weight * t};
+  block_reduce_store<1>(v, sc->sum);   // sum[r] for block r: every used slot is overwritten
+}
+
+// Device address of the scratch, looked up once per device with that device
+// current.  In host code `noalloc_scratch` only names a host-side stand-in.
+constexpr int MAX_DEVICES = 64;
+std::mutex scratch_mutex;
+NoAllocScratch *scratch_ptr[MAX_DEVICES] = {};
+
+cudaError_t scratch_for(int device, NoAllocScratch **out) {
+  std::lock_guard<std::mutex> g(scratch_mutex);
+  if (!scratch_ptr[device]) {
+    void *p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, noalloc_scratch);
+    if (e != cudaSuccess) return e;
+    scratch_ptr[device] = static_cast<NoAllocScratch *>(p);
+  }
+  *out = scratch_ptr[device];
+  return cudaSuccess;
+}
+
+}  // namespace
+}  // namespace cacb200
+
+extern "C" int cacb200_replica_energy_noalloc(int device, const double *eatom, const double *enode,
+                                              int nreplicas, const int *natoms, const int *nelements,
+                                              double node_weight, double *energy, void *stream) {
+  using namespace cacb200;
+  if (nreplicas < 1 || nreplicas > NOALLOC_MAX_REPLICAS) {
+    std::fprintf(stderr, "cacb200_replica_energy_noalloc: %d replicas; the fixed scratch holds 1 to %d\n",
+                 nreplicas, NOALLOC_MAX_REPLICAS);
+    return CACB200_EINVAL;
+  }
+  if (!natoms || !nelements || !energy || device < 0 || device >= MAX_DEVICES) return CACB200_EINVAL;
+  std::vector<int> meta(4 * (size_t)NOALLOC_MAX_REPLICAS, 0);
+  long a = 0, e = 0;
+  for (int r = 0; r < nreplicas; r++) {
+    if (natoms[r] < 0 || nelements[r] < 0) return CACB200_EINVAL;
+    meta[r] = (int)a;
+    meta[NOALLOC_MAX_REPLICAS + r] = natoms[r];
+    meta[2 * NOALLOC_MAX_REPLICAS + r] = (int)e;
+    meta[3 * NOALLOC_MAX_REPLICAS + r] = nelements[r];
+    a += natoms[r];
+    e += nelements[r];
+  }
+  if (a >= (1L << 31) || 8 * e >= (1L << 31)) return CACB200_EINVAL;
+  if ((a > 0 && !eatom) || (e > 0 && !enode)) return CACB200_EINVAL;
+  int prev = 0;
+  if (cudaGetDevice(&prev) != cudaSuccess) return CACB200_ECUDA;
+  if (cudaSetDevice(device) != cudaSuccess) {
+    cudaGetLastError();
+    return CACB200_ECUDA;
+  }
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  NoAllocScratch *sc = nullptr;
+  cudaError_t err = scratch_for(device, &sc);
+  if (err == cudaSuccess)
+    err = cudaMemcpyAsync(sc->meta, meta.data(), sizeof(int) * meta.size(), cudaMemcpyHostToDevice, st);
+  if (err == cudaSuccess) {
+    k_replica_energy_fixed<<<nreplicas, 256, 0, st>>>(eatom, enode, node_weight, sc);
+    err = cudaGetLastError();
+  }
+  if (err == cudaSuccess)
+    err = cudaMemcpyAsync(energy, sc->sum, sizeof(double) * nreplicas, cudaMemcpyDeviceToHost, st);
+  if (err == cudaSuccess) err = cudaStreamSynchronize(st);
+  cudaSetDevice(prev);
+  if (err != cudaSuccess) {
+    cudaGetLastError();
+    return CACB200_ECUDA;
+  }
+  return CACB200_OK;
+}

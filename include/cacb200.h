@@ -185,6 +185,28 @@ int cacb200_minimize_fire(cacb200_ctx *ctx, double etol, double ftol, int maxite
 int cacb200_snapshot(cacb200_ctx *ctx);
 int cacb200_restore(cacb200_ctx *ctx);
 
+/* The same per-replica energies from per-site energies the caller holds on
+ * the device, with no device allocation at all: no counterpart in the
+ * reference.  For callers that must not allocate device memory (a host
+ * program whose GPU memory belongs to another framework's pool, or a loop
+ * that cannot afford the device-wide wait of cudaFree beside running
+ * streams).  eatom [sum natoms] and enode [sum nelements][8] are device
+ * arrays, replicas one after another; natoms, nelements [nreplicas] and
+ * energy [nreplicas] are host arrays; node_weight multiplies node energies
+ * (729/8 for the UNIFORM Hex element; 1 for EAM during minimisation).  The
+ * scratch is one fixed device array of this library for at most
+ * CACB200_NOALLOC_MAX_REPLICAS replicas (more: CACB200_EINVAL and a message
+ * on stderr), held by every GPU that loads the library until exit.  The
+ * first call on a device looks up that array's device address; make it
+ * before any stream capture.  Every call shares the array, so calls that
+ * overlap on the GPU (other streams, other threads) race; each call waits
+ * for its stream before returning. */
+#define CACB200_NOALLOC_MAX_REPLICAS 4096
+int cacb200_replica_energy_noalloc(int device, const double *eatom, const double *enode,
+                                   int nreplicas, const int *natoms, const int *nelements,
+                                   double node_weight, double *energy /* [nreplicas] */,
+                                   void *stream /* cudaStream_t */);
+
 /* cacb200_run_nve replays each rebuild cycle (every steps) as two CUDA
  * graphs, with one host wait per cycle to read the rebuild's overflow flags.
  * Enabled by default; disabling runs every launch eagerly (same kernels,
