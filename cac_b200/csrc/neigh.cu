@@ -271,6 +271,7 @@ struct BuildArgs {
   int na, ne, nsi, cap;
   RefBins rb;                 // single systems only (half lists)
   double cutneigh, cutneighsq;
+  double cutforcesq;          // pairs inside the force cutoff at build time are stored first
   int want_half;
   int *raw_full, *num_full;
   unsigned char *img_full;
@@ -312,6 +313,9 @@ __device__ __forceinline__ double rsq_rn(double dx, double dy, double dz) {
   return __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
 }
 
+// Stores one entry; the image byte carries IN_CUT when the pair lies inside
+// the force cutoff at build time (the compaction puts those entries first).
+constexpr unsigned char IN_CUT = 0x80;
 __device__ __forceinline__ void emit(const BuildArgs &A, int i, int &n, int *raw, unsigned char *img,
                                      int val, int code) {
   if (n < A.cap) {
@@ -391,7 +395,7 @@ __device__ __forceinline__ void try_atom(const BuildArgs &A, const Query &q, int
     atomicExch(&A.overflow[2], 1);
     return;
   }
-  int code = img_code(s[0], s[1], s[2]);
+  int code = img_code(s[0], s[1], s[2]) | (rsq < A.cutforcesq ? IN_CUT : 0);
   emit(A, q.i, nf, A.raw_full, A.img_full, j, code);
   if (A.want_half && q.iatom) {
     int ord = ref_bin_order(A.rb, q.xi, qq);
@@ -517,7 +521,7 @@ __device__ void element_candidates(const BuildArgs &A, const Query &q, int &nf, 
                   continue;
                 }
                 int val = KIND_SITE | (e * NU + u);
-                emit(A, q.i, nf, A.raw_full, A.img_full, val, code);
+                emit(A, q.i, nf, A.raw_full, A.img_full, val, code | (rsq < A.cutforcesq ? IN_CUT : 0));
                 if (A.want_half) {
                   bool keep = true;
                   if (!q.iatom) {
@@ -688,24 +692,35 @@ __global__ void k_act_table(const int *flag, const int *pref, int ngid, int ne, 
   }
 }
 
+// Packs each entry as (site-table index << 5 | image code).  Entries inside
+// the force cutoff at build time go first, each group in build order, so that
+// the pair loops meet the in-cutoff neighbours of all lanes of a warp together
+// (the order of a site's terms changes, not the set).
 __global__ void k_remap(const int *raw, const unsigned char *img, const int *num, int nsi, int cap,
                         const int *pref, int na, int ne, int *out) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nsi) return;
   int n = min(num[i], cap);
-  for (int k = 0; k < n; k++) {
-    size_t o = (size_t)k * nsi + i;
-    int v = raw[o];
-    int sidx;
-    if (v & KIND_SITE) {
-      int gid = v & ~KIND_SITE;
-      int e = gid / NU, u = gid % NU;
-      int g = site_gauss(u);
-      sidx = (g >= 0) ? na + NG * e + g : na + NG * ne + pref[gid];
-    } else {
-      sidx = v;
+  int w = 0;
+  for (int pass = 0; pass < 2; pass++) {
+    const unsigned char want = pass == 0 ? IN_CUT : 0;
+    for (int k = 0; k < n; k++) {
+      size_t o = (size_t)k * nsi + i;
+      unsigned char im = img[o];
+      if ((im & IN_CUT) != want) continue;
+      int v = raw[o];
+      int sidx;
+      if (v & KIND_SITE) {
+        int gid = v & ~KIND_SITE;
+        int e = gid / NU, u = gid % NU;
+        int g = site_gauss(u);
+        sidx = (g >= 0) ? na + NG * e + g : na + NG * ne + pref[gid];
+      } else {
+        sidx = v;
+      }
+      out[(size_t)w * nsi + i] = (sidx << IMG_BITS) | (im & (IN_CUT - 1));
+      w++;
     }
-    out[o] = (sidx << IMG_BITS) | img[o];
   }
 }
 
@@ -969,6 +984,7 @@ void neigh_build_async(Ctx &c, bool want_half) {
     A.rb = c.rbins;
     A.cutneigh = c.cutneigh;
     A.cutneighsq = c.cutneighsq;
+    A.cutforcesq = c.pp.cut * c.pp.cut;
     A.want_half = want_half ? 1 : 0;
     A.raw_full = c.raw_full.p;
     A.num_full = c.num_full.p;
