@@ -266,6 +266,50 @@ def alg_bytes_per_site(kernel: str) -> int:
     }.get(kernel, 0)
 
 
+# DRAM bytes per site and launch of the dominant kernels, from one ncu capture
+# each (dram__bytes_read.sum + dram__bytes_write.sum) on the 313,120-site EAM
+# slab, where the whole working set exceeds L2; the list stream grows with the
+# sites, so the per-site figure carries over to larger systems of the same
+# lattice.
+TRAFFIC_PER_SITE = {"eam_force": 142.5e6 / 313120, "eam_force32": 122.8e6 / 313120}
+
+
+def alg_flops_per_site(kernel: str) -> int:
+    """FP operations per site counted on the reference algorithm's Verlet-list
+    candidates at the workloads' density: 78 candidates within cut + skin
+    (8 operations each for the separation and r^2) and 42 within the force
+    cutoff (12 operations for a density term, 42 for an EAM force term, 12 for
+    an LJ term; LJ: 86 and 54)."""
+    return {
+        "eam_force": 78 * 8 + 42 * 42, "eam_force32": 78 * 8 + 42 * 42,
+        "eam_rho": 78 * 8 + 42 * 12, "eam_rho32": 78 * 8 + 42 * 12,
+        "pair_lj": 86 * 8 + 54 * 12, "pair_lj32": 86 * 8 + 54 * 12,
+    }.get(kernel, 0)
+
+
+def pipe_peak(fp64: bool, device: int) -> float:
+    """Dense GEMM throughput (TFLOP/s) of this GPU in the kernel's arithmetic
+    type, measured here through cuBLAS (torch.matmul, TF32 off): the ceiling
+    for the pair kernels' FP64 or FP32 arithmetic."""
+    import torch
+    torch.backends.cuda.matmul.allow_tf32 = False
+    n = 4096 if fp64 else 8192
+    dt = torch.float64 if fp64 else torch.float32
+    a = torch.randn(n, n, dtype=dt, device=torch.device("cuda", device))
+    b = torch.randn(n, n, dtype=dt, device=torch.device("cuda", device))
+    best = 0.0
+    for _ in range(4):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        torch.cuda.synchronize(device)
+        best = max(best, 2.0 * n ** 3 / (e0.elapsed_time(e1) / 1000.0) / 1e12)
+    del a, b
+    return best
+
+
 def b200_arm(args, rank, local, ws, dist):
     import numpy as np
     import torch
@@ -347,6 +391,16 @@ def b200_arm(args, rank, local, ws, dist):
     hbm, hbm_kind = peaks()
     achieved = alg / (avg_ms / 1000.0) / 1e9
     launches_per_step = sum(v[1] for v in prof.values()) / nprof
+    traffic = TRAFFIC_PER_SITE[dom[0]] * nsi if dom[0] in TRAFFIC_PER_SITE else None
+    pipe = None
+    if alg_flops_per_site(dom[0]):
+        fp64 = not dom[0].endswith("32")
+        peak_tf = pipe_peak(fp64, local)
+        got_tf = alg_flops_per_site(dom[0]) * nsi / (avg_ms / 1000.0) / 1e12
+        pipe = {"bound": "fp64" if fp64 else "fp32", "kernel": dom[0], "achieved": got_tf, "peak": peak_tf,
+                "unit": "TFLOP/s", "frac": got_tf / peak_tf,
+                "peak_kind": "measured here: cuBLAS " + ("DGEMM" if fp64 else "SGEMM, TF32 off"),
+                "flops_per_site": alg_flops_per_site(dom[0])}
     eng.restore()
     eng.setup()
 
@@ -413,8 +467,11 @@ def b200_arm(args, rank, local, ws, dist):
                        "rebuild_every": 10, "parallelism": f"replicas x{ws} (no data-path collective)",
                        "l2": "working set larger than L2 (site table + lists > 126 MB)"},
             "roofline": {"bound": "hbm", "kernel": dom[0], "achieved": achieved, "peak": hbm,
-                         "peak_kind": hbm_kind, "unit": "GB/s", "frac": achieved / hbm, "traffic": None,
+                         "peak_kind": hbm_kind, "unit": "GB/s", "frac": achieved / hbm,
+                         "traffic": traffic, "traffic_note": "ncu dram read+write per launch, per-site figure "
+                                                             "of a 313,120-site capture scaled to this workload",
                          "avg_launch_ms": avg_ms, "alg_bytes_per_launch": alg},
+            "pipe_roofline": pipe,
             "kernels_ms_per_launch": {k: v[0] / max(v[1], 1) for k, v in sorted(prof.items())},
             "kernels_ms_per_step": {k: v[0] / nprof for k, v in sorted(prof.items())},
             "segment_steps": seg,

@@ -825,16 +825,12 @@ void neigh_plan(Ctx &c, bool want_half) {
       R.reach_budget = std::max(ereach, std::min(std::max(1.2 * ereach, ereach + 2.0), room));
     }
     setup_grids(c, R, c.rep_ne[r] > 0);
-    // fixed-point frame of the mixed form: the largest 2^k (k <= 24) with
-    // (L + 64 A) 2^k inside an int, per dimension
+    // fixed-point frame of the mixed form: quantum 2^-26 A, box length in
+    // quanta modulo 2^32 (pair separations are taken modulo 2^32 as well)
     for (int d = 0; d < 3; d++) {
-      int k = 24;
-      while (k > 4 && (R.b.L[d] + 64.0) * std::ldexp(1.0, k) > 2147483000.0) k--;
-      if ((R.b.L[d] + 64.0) * std::ldexp(1.0, k) > 2147483000.0)
-        throw Error(CACB200_EINVAL, "box too large for the mixed-precision fixed-point positions");
-      R.qscale[d] = std::ldexp(1.0, k);
-      R.qinv[d] = std::ldexp(1.0f, -k);
-      R.Lq[d] = (int)std::nearbyint(R.b.L[d] * R.qscale[d]);
+      R.qscale[d] = std::ldexp(1.0, 26);
+      R.qinv[d] = std::ldexp(1.0f, -26);
+      R.Lq[d] = (int)(uint32_t)(uint64_t)std::llrint(R.b.L[d] * R.qscale[d]);
     }
     R.abase = abase;
     R.ebase = ebase;
@@ -1037,7 +1033,7 @@ int neigh_check(Ctx &c) {
   int ov[8];
   stream_copy(c, ov, c.overflow.p, sizeof(ov), cudaMemcpyDeviceToHost);
   if (ov[2]) throw Error(CACB200_EINVAL, "neighbour image beyond the first periodic image (box too small)");
-  if (ov[6]) throw Error(CACB200_EUNSTABLE, "a site left the fixed-point range around the box (unstable run)");
+  if (ov[6]) throw Error(CACB200_EUNSTABLE, "a site position is not finite or absurdly far from the box (unstable run)");
   if (ov[7]) throw Error(CACB200_EOVERFLOW, "more referenced sites than 26-bit list entries can address");
   int again = 0;
   if (ov[0]) {

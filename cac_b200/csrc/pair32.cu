@@ -2,16 +2,15 @@
 // fixed-point positions, FP64 everywhere else.
 //
 // Every site of the site table gets, each step, a 32-bit fixed-point copy of
-// its FP64 position relative to the box corner, q = rint((x - lo) 2^k), with
-// k chosen per box dimension so that the box length plus a 64 A margin
-// (element sites may lie outside the box) fits in an int.  A pair's
-// separation is then
-//     x_i - (x_j + s L) = (q_i - q_j - s Lq) 2^-k,
-// an exact integer difference (wrap-around 32-bit arithmetic is exact while
-// the true difference is small) rounded once to FP32: no FP32 sum ever
-// carries a box-sized coordinate.  The quantum 2^-k is 2.4e-7 A for box
-// lengths up to ~440 A, 9.5e-7 A up to ~1.9e3 A.  A site's record is 16 bytes, (qx, qy, qz, F'), so one 128-bit
-// load brings everything a pair needs from its neighbour.
+// its FP64 position relative to the box corner, q = rint((x - lo) 2^26) taken
+// modulo 2^32.  A pair's separation is then
+//     x_i - (x_j + s L) = (q_i - q_j - s Lq) 2^-26   (mod 2^32 quanta),
+// an exact integer difference in wrap-around 32-bit arithmetic, which is the
+// true difference whenever that is shorter than 2^31 quanta = 32 A (pairs are
+// within the neighbour cutoff), rounded once to FP32: no FP32 sum ever
+// carries a box-sized coordinate, and the quantum (1.5e-8 A) does not depend
+// on the box size.  A site's record is 16 bytes, (qx, qy, qz, F'), so one
+// 128-bit load brings everything a pair needs from its neighbour.
 //
 // What stays FP64 (as the mixed form specifies): positions and velocities and
 // their integration, element interpolation, nodal assembly over Gauss points,
@@ -63,11 +62,13 @@ __device__ __forceinline__ void pack_one(const double4 *xs, int k, const FixGrid
 #pragma unroll
   for (int d = 0; d < 3; d++) {
     double rel = (q[d] - lo[d]) * sc[d];
-    if (!(rel > -2147483000.0 && rel < 2147483000.0)) {
+    // positions further than 2^62 quanta (~7e10 A) from the box, or not
+    // finite, only come from a run that has blown up
+    if (!(rel > -4.6e18 && rel < 4.6e18)) {
       atomicExch(bad, 1);
       rel = 0.0;
     }
-    o[d] = __double2int_rn(rel);
+    o[d] = (int)(unsigned)(unsigned long long)__double2ll_rn(rel);   // modulo 2^32
   }
   int4 v = pos[k];
   pos[k] = make_int4(o[0], o[1], o[2], v.w);
@@ -96,7 +97,8 @@ struct Args32 {
 };
 
 __device__ __forceinline__ float fix_delta(int qi, int qj, int s, int Lq, float inv) {
-  unsigned d = (unsigned)qi - (unsigned)qj - (unsigned)(s * Lq);
+  const unsigned sl = (unsigned)s * (unsigned)Lq;   // s in {-1, 0, 1}, modulo 2^32
+  unsigned d = (unsigned)qi - (unsigned)qj - sl;
   return (float)(int)d * inv;
 }
 
