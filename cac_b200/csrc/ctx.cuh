@@ -191,7 +191,12 @@ struct Ctx {
   DBuf<double4> acell_pos;       // [na] wrapped positions sorted by cell, w = bitcast(id)
   DBuf<float4> acell_pos32;      // [na] the same as floats, w = bitcast(int id)
   DBuf<int> ecell_start, ecell_elems;
-  DBuf<int> cell_key, cell_key2, idx_tmp, idx_tmp2;
+  DBuf<int> cell_key, cell_key2, idx_tmp;
+  // list slot -> atom (atoms sorted by cell at the last rebuild; slots past
+  // the atoms are Gauss points in site-table order).  Lists, counts and the
+  // pair kernels' threads are indexed by slot, so a warp covers a compact
+  // group of atoms.
+  DBuf<int> slot_atom;
   DBuf<unsigned char> cub_tmp;
   size_t cub_bytes = 0;
   int sort_bits_a = 1, sort_bits_e = 1;

@@ -268,6 +268,7 @@ struct BuildArgs {
   const float4 *acell_pos32;  // wrapped positions as floats, w = atom index bits
   const int *ecell_start;
   const int *ecell_elems;
+  const int *atom_of_slot;    // list slot (cell-sorted position) -> atom index
   int na, ne, nsi, cap;
   RefBins rb;                 // single systems only (half lists)
   double cutneigh, cutneighsq;
@@ -328,7 +329,8 @@ __device__ __forceinline__ void emit(const BuildArgs &A, int i, int &n, int *raw
 // One query point (an i-site) of the build.
 struct Query {
   Rep r;          // its replica
-  int i;
+  int i;          // site-table index (atoms: input order)
+  int slot;       // list slot: atoms in cell-sorted order, then Gauss points
   bool iatom;
   int ie, ig, iu;
   double xi[3];   // raw position
@@ -340,6 +342,7 @@ template <class RP>
 __device__ __forceinline__ void make_query(const BuildArgs &A, const RP &P, int i, Query &q) {
   q.r = P.site(i);
   q.i = i;
+  q.slot = i;
   q.iatom = i < A.na;
   q.ie = q.ig = q.iu = -1;
   if (q.iatom) {
@@ -396,11 +399,11 @@ __device__ __forceinline__ void try_atom(const BuildArgs &A, const Query &q, int
     return;
   }
   int code = img_code(s[0], s[1], s[2]) | (rsq < A.cutforcesq ? IN_CUT : 0);
-  emit(A, q.i, nf, A.raw_full, A.img_full, j, code);
+  emit(A, q.slot, nf, A.raw_full, A.img_full, j, code);
   if (A.want_half && q.iatom) {
     int ord = ref_bin_order(A.rb, q.xi, qq);
     bool keep = ord > 0 || (ord == 0 && (zero ? (j > q.i) : above_right(qq, q.xi)));
-    if (keep) emit(A, q.i, nh, A.raw_half, A.img_half, j, code);
+    if (keep) emit(A, q.slot, nh, A.raw_half, A.img_half, j, code);
   }
 }
 
@@ -521,7 +524,7 @@ __device__ void element_candidates(const BuildArgs &A, const Query &q, int &nf, 
                   continue;
                 }
                 int val = KIND_SITE | (e * NU + u);
-                emit(A, q.i, nf, A.raw_full, A.img_full, val, code | (rsq < A.cutforcesq ? IN_CUT : 0));
+                emit(A, q.slot, nf, A.raw_full, A.img_full, val, code | (rsq < A.cutforcesq ? IN_CUT : 0));
                 if (A.want_half) {
                   bool keep = true;
                   if (!q.iatom) {
@@ -531,7 +534,7 @@ __device__ void element_candidates(const BuildArgs &A, const Query &q, int &nf, 
                       else keep = above_right(qcen, icen);
                     }
                   }
-                  if (keep) emit(A, q.i, nh, A.raw_half, A.img_half, val, code);
+                  if (keep) emit(A, q.slot, nh, A.raw_half, A.img_half, val, code);
                 }
               }
         }
@@ -574,6 +577,7 @@ __global__ void __launch_bounds__(32) k_build_atoms(BuildArgs A, RP P) {
     float wx = 0.f, wy = 0.f, wz = 0.f;
     if (active) {
       make_query(A, P, (int)__double_as_longlong(A.acell_pos[h].w), q);
+      q.slot = h;
       float4 w = A.acell_pos32[h];
       wx = w.x;
       wy = w.y;
@@ -603,23 +607,25 @@ __global__ void __launch_bounds__(32) k_build_atoms(BuildArgs A, RP P) {
       }
     }
     if (active) {
-      A.num_full[q.i] = nf;
-      if (A.want_half) A.num_half[q.i] = nh;
+      A.num_full[q.slot] = nf;
+      if (A.want_half) A.num_half[q.slot] = nh;
     }
   }
 }
 
-// Atoms, element lattice sites: appended after the atom neighbours.  Atoms
-// whose 27 element cells hold no element leave at once.
+// Atoms, element lattice sites: appended after the atom neighbours, one
+// thread per list slot (cell-sorted order).  Atoms whose 27 element cells
+// hold no element leave at once.
 template <class RP>
 __global__ void __launch_bounds__(128) k_build_atom_sites(BuildArgs A, RP P) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= A.na) return;
+  int h = blockIdx.x * blockDim.x + threadIdx.x;
+  if (h >= A.na) return;
   Query q;
-  make_query(A, P, i, q);
-  int nf = A.num_full[i], nh = A.want_half ? A.num_half[i] : 0;
+  make_query(A, P, A.atom_of_slot[h], q);
+  q.slot = h;
+  int nf = A.num_full[h], nh = A.want_half ? A.num_half[h] : 0;
   if (A.ne > 0) element_candidates(A, q, nf, nh);
-  finish_counts(A, i, nf, nh);
+  finish_counts(A, h, nf, nh);
 }
 
 // Gauss points: one thread each; atoms from the 27 surrounding atom cells
@@ -662,7 +668,7 @@ __global__ void __launch_bounds__(128) k_build_gauss(BuildArgs A, RP P) {
     }
   }
   element_candidates(A, q, nf, nh);
-  finish_counts(A, q.i, nf, nh);
+  finish_counts(A, q.slot, nf, nh);
 }
 
 // ------------------------------------------------------------- compaction
@@ -856,7 +862,7 @@ void neigh_plan(Ctx &c, bool want_half) {
   c.cell_key.reserve(nmax);
   c.cell_key2.reserve(nmax);
   c.idx_tmp.reserve(nmax);
-  c.idx_tmp2.reserve(nmax);
+  c.slot_atom.reserve(nmax);
   c.acell_start.reserve(c.agrid.ncell + 1);
   c.acell_pos.reserve(std::max(c.na, 1));
   c.acell_pos32.reserve(std::max(c.na, 1));
@@ -898,7 +904,7 @@ void neigh_plan(Ctx &c, bool want_half) {
   int bits_a = 1, bits_e = 1;
   while ((1 << bits_a) <= c.agrid.ncell && bits_a < 31) bits_a++;
   while ((1 << bits_e) <= c.egrid.ncell && bits_e < 31) bits_e++;
-  cub::DeviceRadixSort::SortPairs(nullptr, bytes, c.cell_key.p, c.cell_key2.p, c.idx_tmp.p, c.idx_tmp2.p,
+  cub::DeviceRadixSort::SortPairs(nullptr, bytes, c.cell_key.p, c.cell_key2.p, c.idx_tmp.p, c.slot_atom.p,
                                   std::max(c.na, 1), 0, bits_a, c.stream);
   need = std::max(need, bytes);
   cub::DeviceRadixSort::SortPairs(nullptr, bytes, c.cell_key.p, c.cell_key2.p, c.idx_tmp.p, c.ecell_elems.p,
@@ -942,11 +948,11 @@ void neigh_build_async(Ctx &c, bool want_half) {
       if (c.na) {
         k_atom_keys<<<nblk(c.na, 256), 256, 0, c.stream>>>(c.xs.p, c.na, P, c.cell_key.p, c.idx_tmp.p);
         CACB200_CUDA(cub::DeviceRadixSort::SortPairs(c.cub_tmp.p, bytes, c.cell_key.p, c.cell_key2.p,
-                                                     c.idx_tmp.p, c.idx_tmp2.p, c.na, 0, c.sort_bits_a,
+                                                     c.idx_tmp.p, c.slot_atom.p, c.na, 0, c.sort_bits_a,
                                                      c.stream));
         k_cell_start<<<nblk(c.agrid.ncell + 1, 256), 256, 0, c.stream>>>(c.cell_key2.p, c.na, c.agrid.ncell,
                                                                         c.acell_start.p);
-        k_gather_pos<<<nblk(c.na, 256), 256, 0, c.stream>>>(c.xs.p, c.idx_tmp2.p, c.na, c.acell_pos.p,
+        k_gather_pos<<<nblk(c.na, 256), 256, 0, c.stream>>>(c.xs.p, c.slot_atom.p, c.na, c.acell_pos.p,
                                                             c.acell_pos32.p);
       } else {
         CACB200_CUDA(cudaMemsetAsync(c.acell_start.p, 0, sizeof(int) * (c.agrid.ncell + 1), c.stream));
@@ -973,6 +979,7 @@ void neigh_build_async(Ctx &c, bool want_half) {
     A.acell_pos32 = c.acell_pos32.p;
     A.ecell_start = c.ecell_start.p;
     A.ecell_elems = c.ecell_elems.p;
+    A.atom_of_slot = c.slot_atom.p;
     A.na = c.na;
     A.ne = c.ne;
     A.nsi = nsi;
@@ -1074,13 +1081,18 @@ void neigh_download(Ctx &c, bool half, int64_t *offset, int8_t *kind, int32_t *i
                     int8_t *img, int64_t *nentries) {
   if (!c.lists_valid || (half && !c.have_half)) throw Error(CACB200_ESTATE, "list not built");
   const int nsi = c.nsite_i();
-  std::vector<int> num(nsi);
+  std::vector<int> num_slot(nsi), num(nsi), slot_of(nsi);
   std::vector<int> ent((size_t)c.cap * nsi);
+  std::vector<int> atom_of(std::max(c.na, 1));
   device_nact(c);
   std::vector<int> act(std::max(c.nact, 1));
   CACB200_CUDA(cudaStreamSynchronize(c.stream));
-  stream_copy(c, num.data(), half ? c.num_half.p : c.num_full.p, sizeof(int) * nsi,
+  stream_copy(c, num_slot.data(), half ? c.num_half.p : c.num_full.p, sizeof(int) * nsi,
                           cudaMemcpyDeviceToHost);
+  if (c.na) stream_copy(c, atom_of.data(), c.slot_atom.p, sizeof(int) * c.na, cudaMemcpyDeviceToHost);
+  for (int k = 0; k < nsi; k++) slot_of[k] = k;
+  for (int h = 0; h < c.na; h++) slot_of[atom_of[h]] = h;
+  for (int i = 0; i < nsi; i++) num[i] = num_slot[slot_of[i]];
   stream_copy(c, ent.data(), half ? c.nbr_half.p : c.nbr_full.p, sizeof(int) * ent.size(),
                           cudaMemcpyDeviceToHost);
   if (c.nact)
@@ -1095,7 +1107,7 @@ void neigh_download(Ctx &c, bool half, int64_t *offset, int8_t *kind, int32_t *i
     offset[i] = pos;
     row.clear();
     for (int k = 0; k < num[i]; k++) {
-      int v = ent[(size_t)k * nsi + i];
+      int v = ent[(size_t)k * nsi + slot_of[i]];
       int sidx = v >> IMG_BITS, code = v & ((1 << IMG_BITS) - 1);
       int sx, sy, sz;
       img_decode(code, sx, sy, sz);

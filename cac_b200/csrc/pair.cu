@@ -31,8 +31,9 @@ inline int nblk(long n, int t) { return (int)((n + t - 1) / t); }
 
 struct PairArgs {
   const double4 *xs;
-  const int *nbr;
+  const int *nbr;                   // lists and counts indexed by list slot
   const int *num;
+  const int *slot_atom;             // list slot -> atom (slots past the atoms are Gauss points)
   int na, ne, nsi;
   double L[3];                      // box of a single system
   const Rep *reps;                  // batches: replica descriptors ...
@@ -43,6 +44,8 @@ struct PairArgs {
   int eflag, vflag;
   double escale_node, vscale_node;  // global scales of a node Gauss point
 };
+
+__device__ __forceinline__ int site_of_slot(const PairArgs &A, int t) { return t < A.na ? A.slot_atom[t] : t; }
 
 __device__ __forceinline__ void neighbour_pos(const PairArgs &A, double Lx, double Ly, double Lz, int v,
                                               double4 &xj) {
@@ -154,13 +157,14 @@ struct LjParams {
 
 template <bool EV, bool MANY>
 __global__ void __launch_bounds__(128, EV ? 4 : 8) k_lj(PairArgs A, LjParams P) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  bool valid = i < A.nsi;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;   // list slot
+  const bool valid = t < A.nsi;
+  const int i = valid ? site_of_slot(A, t) : 0;           // site-table index
   double fi[3] = {0, 0, 0}, esum = 0.0, vsum[6] = {0, 0, 0, 0, 0, 0};
   if (valid) {
     double4 xi = A.xs[i];
-    int n = A.num[i];
-    const int *nb = A.nbr + i;
+    int n = A.num[t];
+    const int *nb = A.nbr + t;
     auto pair = [&](const double4 &xj) {
       double dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
       double rsq = dx * dx + dy * dy + dz * dz;
@@ -228,11 +232,12 @@ __device__ __forceinline__ double eam_fp(const EamTables &T, double rho, double 
 template <bool MANY>
 __global__ void __launch_bounds__(128, 8) k_eam_rho(PairArgs A, EamTables T, double *rho_out,
                                                  double *phi_site) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= A.nsi) return;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;   // list slot
+  if (t >= A.nsi) return;
+  const int i = site_of_slot(A, t);                       // site-table index
   double4 xi = A.xs[i];
-  int n = A.num[i];
-  const int *nb = A.nbr + i;
+  int n = A.num[t];
+  const int *nb = A.nbr + t;
   double rho = 0.0;
   auto pair = [&](const double4 &xj) {
     double dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
@@ -279,15 +284,16 @@ __global__ void k_eam_site_fp(double4 *xs, const int *act_gid, const int *nact_d
 // pass 2: forces (pair_eam.cpp:845-1028)
 template <bool EV, bool MANY>
 __global__ void __launch_bounds__(128, EV ? 4 : 6) k_eam_force(PairArgs A, EamTables T, const double *phi_site) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  bool valid = i < A.nsi;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;   // list slot
+  const bool valid = t < A.nsi;
+  const int i = valid ? site_of_slot(A, t) : 0;           // site-table index
   double fi[3] = {0, 0, 0}, esum = 0.0, vsum[6] = {0, 0, 0, 0, 0, 0};
   double eemb_site = 0.0, eemb_global = 0.0;
   if (valid) {
     double4 xi = A.xs[i];
     double fpi = xi.w;
-    int n = A.num[i];
-    const int *nb = A.nbr + i;
+    int n = A.num[t];
+    const int *nb = A.nbr + t;
     auto pair = [&](const double4 &xj) {
       double dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
       double rsq = dx * dx + dy * dy + dz * dz;
@@ -426,6 +432,7 @@ void pair_compute(Ctx &c, int eflag, int vflag) {
   A.xs = c.xs.p;
   A.nbr = c.nbr_full.p;
   A.num = c.num_full.p;
+  A.slot_atom = c.slot_atom.p;
   A.na = c.na;
   A.ne = c.ne;
   A.nsi = nsi;

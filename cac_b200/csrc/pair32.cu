@@ -85,8 +85,9 @@ __global__ void k_pack32(const double4 *xs, int nsi, const int *nact_dev, FixGri
 
 struct Args32 {
   const int4 *pos;
-  const int *nbr;
+  const int *nbr;          // lists and counts indexed by list slot
   const int *num;
+  const int *slot_atom;    // list slot -> atom (slots past the atoms are Gauss points)
   int na, ne, nsi;
   FixGrid G;
   double *f, *gaussf;
@@ -126,6 +127,8 @@ __device__ __forceinline__ SiteFix site_fix(const Args32 &A, int i) {
   return F;
 }
 
+__device__ __forceinline__ int site_of_slot(const Args32 &A, int t) { return t < A.na ? A.slot_atom[t] : t; }
+
 // separation of site i (record oi) from neighbour entry v; wj = F'(j)
 __device__ __forceinline__ void sep32(const Args32 &A, const SiteFix &F, const int4 &oi, int v, float &dx,
                                       float &dy, float &dz, float &wj) {
@@ -140,10 +143,10 @@ __device__ __forceinline__ void sep32(const Args32 &A, const SiteFix &F, const i
 }
 
 template <class F>
-__device__ __forceinline__ void for_each32(const Args32 &A, int i, const int4 &oi, F &&f) {
+__device__ __forceinline__ void for_each32(const Args32 &A, int t, int i, const int4 &oi, F &&f) {
   const SiteFix fx = site_fix(A, i);
-  int n = A.num[i];
-  const int *nb = A.nbr + i;
+  int n = A.num[t];
+  const int *nb = A.nbr + t;
   int k = 0;
   for (; k + 4 <= n; k += 4) {
     int v0 = nb[(size_t)k * A.nsi], v1 = nb[(size_t)(k + 1) * A.nsi];
@@ -213,13 +216,14 @@ struct Lj32 {
 
 template <bool EV>
 __global__ void __launch_bounds__(128, EV ? 4 : 8) k_lj32(Args32 A, Lj32 P) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  bool valid = i < A.nsi;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;   // list slot
+  const bool valid = t < A.nsi;
+  const int i = valid ? site_of_slot(A, t) : 0;           // site-table index
   float fi[3] = {0, 0, 0}, esum = 0.f, vsum[6] = {0, 0, 0, 0, 0, 0};
   if (valid) {
     int4 oi;
     site_frame(A, i, oi);
-    for_each32(A, i, oi, [&](float dx, float dy, float dz, float) {
+    for_each32(A, t, i, oi, [&](float dx, float dy, float dz, float) {
       float rsq = dx * dx + dy * dy + dz * dz;
       if (rsq < P.cutsq) {
         float r2inv = 1.0f / rsq;
@@ -272,12 +276,13 @@ __device__ __forceinline__ float fp32_of(const Eam32 &T, float rho, float *phi) 
 
 __global__ void __launch_bounds__(128, 8) k_eam_rho32(Args32 A, Eam32 T, double *rho_out, double *phi_site,
                                                       int4 *pos_w) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= A.nsi) return;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;   // list slot
+  if (t >= A.nsi) return;
+  const int i = site_of_slot(A, t);                       // site-table index
   int4 oi;
   site_frame(A, i, oi);
   float rho = 0.f;
-  for_each32(A, i, oi, [&](float dx, float dy, float dz, float) {
+  for_each32(A, t, i, oi, [&](float dx, float dy, float dz, float) {
     float rsq = dx * dx + dy * dy + dz * dz;
     if (rsq < T.cutforcesq) {
       float p = sqrtf(rsq) * T.rdr + 1.0f;
@@ -317,15 +322,16 @@ __global__ void k_eam_site_fp32(int4 *pos, const int *act_gid, const int *nact_d
 
 template <bool EV>
 __global__ void __launch_bounds__(128, EV ? 4 : 8) k_eam_force32(Args32 A, Eam32 T, const double *phi_site) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  bool valid = i < A.nsi;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;   // list slot
+  const bool valid = t < A.nsi;
+  const int i = valid ? site_of_slot(A, t) : 0;           // site-table index
   float fi[3] = {0, 0, 0}, esum = 0.f, vsum[6] = {0, 0, 0, 0, 0, 0};
   double eemb_site = 0.0, eemb_global = 0.0;
   if (valid) {
     int4 oi;
     site_frame(A, i, oi);
     const float fpi = __int_as_float(oi.w);
-    for_each32(A, i, oi, [&](float dx, float dy, float dz, float fpj) {
+    for_each32(A, t, i, oi, [&](float dx, float dy, float dz, float fpj) {
       float rsq = dx * dx + dy * dy + dz * dz;
       if (rsq < T.cutforcesq) {
         float recip = rsqrtf(rsq);
@@ -426,6 +432,7 @@ void pair_compute_mixed(Ctx &c, int eflag, int vflag) {
   A.pos = c.pos32.p;
   A.nbr = c.nbr_full.p;
   A.num = c.num_full.p;
+  A.slot_atom = c.slot_atom.p;
   A.na = c.na;
   A.ne = c.ne;
   A.nsi = nsi;
