@@ -197,6 +197,12 @@ struct Ctx {
   // pair kernels' threads are indexed by slot, so a warp covers a compact
   // group of atoms.
   DBuf<int> slot_atom;
+  DBuf<int> atom_slot;           // atom -> list slot
+  // pair table: the site table in list-slot order, [atoms by slot | Gauss
+  // points | active lattice sites], refreshed each step before the pair
+  // kernels; list entries index it, so the neighbours a warp gathers lie in
+  // few cache lines.  w = F' for EAM.
+  DBuf<double4> xss;
   DBuf<unsigned char> cub_tmp;
   size_t cub_bytes = 0;
   int sort_bits_a = 1, sort_bits_e = 1;

@@ -8,29 +8,31 @@ namespace {
 
 inline int nblk(long n, int t) { return (int)((n + t - 1) / t); }
 
-// Positions of the Gauss points (their nodes) and of every active lattice
-// site from the current nodes: x_u = sum_n N_n(u) x_n, the interpolation the
-// reference repeats per pair (pair_lj_cut.cpp:364-368, pair_eam.cpp:959-964).
-// The number of active sites is read on the device (written by the last
-// rebuild), so the launch needs no host copy of it: a fixed grid strides
-// over [Gauss points | active sites].
-__global__ void k_interpolate(double4 *xs, const double *nodex, int na, int ne, const int *act_gid,
-                              const int *nact_dev) {
+// The pair table for this step: atoms in list-slot order (gathered from the
+// site table), then the positions of the Gauss points (their nodes) and of
+// every active lattice site from the current nodes, x_u = sum_n N_n(u) x_n,
+// the interpolation the reference repeats per pair (pair_lj_cut.cpp:364-368,
+// pair_eam.cpp:959-964).  The number of active sites is read on the device
+// (written by the last rebuild), so a fixed grid strides over the table.
+__global__ void k_pair_table(const double4 *xs, double4 *xss, const int *slot_atom, const double *nodex, int na,
+                             int ne, const int *act_gid, const int *nact_dev) {
   const int ngp = NG * ne;
-  const int n = ngp + *nact_dev;
+  const int n = na + ngp + *nact_dev;
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
-    if (t < ngp) {
-      int e = t / NG, g = t % NG;
-      const double *nx = nodex + (size_t)e * 24 + 3 * gauss_node(g);
-      double4 p = xs[na + t];
-      p.x = nx[0];
-      p.y = nx[1];
-      p.z = nx[2];
-      xs[na + t] = p;
+    if (t < na) {
+      double4 p = xs[slot_atom[t]];
+      p.w = 0.0;
+      xss[t] = p;
       continue;
     }
-    int k = t - ngp;
-    int gid = act_gid[k];
+    const int s = t - na;
+    if (s < ngp) {
+      int e = s / NG, g = s % NG;
+      const double *nx = nodex + (size_t)e * 24 + 3 * gauss_node(g);
+      xss[t] = make_double4(nx[0], nx[1], nx[2], 0.0);
+      continue;
+    }
+    int gid = act_gid[s - ngp];
     int e = gid / NU, u = gid % NU;
     const double *nx = nodex + (size_t)e * 24;
     double x = 0.0, y = 0.0, z = 0.0;
@@ -41,11 +43,7 @@ __global__ void k_interpolate(double4 *xs, const double *nodex, int na, int ne, 
       y += N * nx[3 * m + 1];
       z += N * nx[3 * m + 2];
     }
-    double4 p = xs[na + ngp + k];
-    p.x = x;
-    p.y = y;
-    p.z = z;
-    xs[na + ngp + k] = p;
+    xss[t] = make_double4(x, y, z, 0.0);
   }
 }
 
@@ -135,10 +133,10 @@ __global__ void k_nve_final(double *v, const double *f, int n3, double *nodev, c
 }  // namespace
 
 void interpolate_sites(Ctx &c) {
-  if (c.ne == 0) return;
+  if (c.na + c.ne == 0 || !c.lists_valid) return;
   KernelTimer t(c, "interpolate");
-  k_interpolate<<<stride_grid((long)NG * c.ne + (long)c.ne * NU, 256), 256, 0, c.stream>>>(
-      c.xs.p, c.nodex.p, c.na, c.ne, c.act_gid.p, c.dev_nact.p);
+  k_pair_table<<<stride_grid((long)c.na + (long)NG * c.ne + (long)c.ne * NU, 256), 256, 0, c.stream>>>(
+      c.xs.p, c.xss.p, c.slot_atom.p, c.nodex.p, c.na, c.ne, c.act_gid.p, c.dev_nact.p);
 }
 
 void assemble_nodef(Ctx &c) {

@@ -246,10 +246,12 @@ __global__ void k_cell_start(const int *skey, int n, int ncell, int *start) {
   start[c] = lo;
 }
 
-__global__ void k_gather_pos(const double4 *xs, const int *sidx, int n, double4 *out, float4 *out32) {
+__global__ void k_gather_pos(const double4 *xs, const int *sidx, int n, double4 *out, float4 *out32,
+                             int *atom_slot) {
   int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= n) return;
   int i = sidx[k];
+  atom_slot[i] = k;
   double4 p = xs[i];
   out32[k] = make_float4((float)p.x, (float)p.y, (float)p.z, __int_as_float(i));
   p.w = __longlong_as_double((long long)i);
@@ -698,12 +700,14 @@ __global__ void k_act_table(const int *flag, const int *pref, int ngid, int ne, 
   }
 }
 
-// Packs each entry as (site-table index << 5 | image code).  Entries inside
+// Packs each entry as (pair-table index << 5 | image code): atoms by their
+// list slot (the pair table holds atoms in cell-sorted order), element sites
+// after them as in the site table.  Entries inside
 // the force cutoff at build time go first, each group in build order, so that
 // the pair loops meet the in-cutoff neighbours of all lanes of a warp together
 // (the order of a site's terms changes, not the set).
 __global__ void k_remap(const int *raw, const unsigned char *img, const int *num, int nsi, int cap,
-                        const int *pref, int na, int ne, int *out) {
+                        const int *pref, const int *atom_slot, int na, int ne, int *out) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nsi) return;
   int n = min(num[i], cap);
@@ -722,7 +726,7 @@ __global__ void k_remap(const int *raw, const unsigned char *img, const int *num
         int g = site_gauss(u);
         sidx = (g >= 0) ? na + NG * e + g : na + NG * ne + pref[gid];
       } else {
-        sidx = v;
+        sidx = atom_slot[v];
       }
       out[(size_t)w * nsi + i] = (sidx << IMG_BITS) | (im & (IN_CUT - 1));
       w++;
@@ -863,6 +867,8 @@ void neigh_plan(Ctx &c, bool want_half) {
   c.cell_key2.reserve(nmax);
   c.idx_tmp.reserve(nmax);
   c.slot_atom.reserve(nmax);
+  c.atom_slot.reserve(std::max(c.na, 1));
+  c.xss.reserve(std::max(c.xs.n, (size_t)1));
   c.acell_start.reserve(c.agrid.ncell + 1);
   c.acell_pos.reserve(std::max(c.na, 1));
   c.acell_pos32.reserve(std::max(c.na, 1));
@@ -953,7 +959,7 @@ void neigh_build_async(Ctx &c, bool want_half) {
         k_cell_start<<<nblk(c.agrid.ncell + 1, 256), 256, 0, c.stream>>>(c.cell_key2.p, c.na, c.agrid.ncell,
                                                                         c.acell_start.p);
         k_gather_pos<<<nblk(c.na, 256), 256, 0, c.stream>>>(c.xs.p, c.slot_atom.p, c.na, c.acell_pos.p,
-                                                            c.acell_pos32.p);
+                                                            c.acell_pos32.p, c.atom_slot.p);
       } else {
         CACB200_CUDA(cudaMemsetAsync(c.acell_start.p, 0, sizeof(int) * (c.agrid.ncell + 1), c.stream));
       }
@@ -1022,10 +1028,10 @@ void neigh_build_async(Ctx &c, bool want_half) {
                                                               c.act_off.p, c.dev_nact.p, c.overflow.p + 7);
     }
     k_remap<<<nblk(nsi, 256), 256, 0, c.stream>>>(c.raw_full.p, c.img_full.p, c.num_full.p, nsi, c.cap, pref,
-                                                   c.na, c.ne, c.nbr_full.p);
+                                                   c.atom_slot.p, c.na, c.ne, c.nbr_full.p);
     if (want_half)
       k_remap<<<nblk(nsi, 256), 256, 0, c.stream>>>(c.raw_half.p, c.img_half.p, c.num_half.p, nsi, c.cap, pref,
-                                                     c.na, c.ne, c.nbr_half.p);
+                                                     c.atom_slot.p, c.na, c.ne, c.nbr_half.p);
   }
   c.have_half = want_half;
   c.lists_valid = true;
@@ -1112,9 +1118,9 @@ void neigh_download(Ctx &c, bool half, int64_t *offset, int8_t *kind, int32_t *i
       int sx, sy, sz;
       img_decode(code, sx, sy, sz);
       int kd, id, st;
-      if (sidx < c.na) {
+      if (sidx < c.na) {   // atoms are stored by list slot
         kd = 0;
-        id = sidx;
+        id = atom_of[sidx];
         st = -1;
       } else if (sidx < c.na + NG * c.ne) {
         kd = 1;

@@ -30,7 +30,7 @@ namespace {
 inline int nblk(long n, int t) { return (int)((n + t - 1) / t); }
 
 struct PairArgs {
-  const double4 *xs;
+  const double4 *xs;                // pair table (list-slot order; w = F')
   const int *nbr;                   // lists and counts indexed by list slot
   const int *num;
   const int *slot_atom;             // list slot -> atom (slots past the atoms are Gauss points)
@@ -162,7 +162,7 @@ __global__ void __launch_bounds__(128, EV ? 4 : 8) k_lj(PairArgs A, LjParams P) 
   const int i = valid ? site_of_slot(A, t) : 0;           // site-table index
   double fi[3] = {0, 0, 0}, esum = 0.0, vsum[6] = {0, 0, 0, 0, 0, 0};
   if (valid) {
-    double4 xi = A.xs[i];
+    double4 xi = A.xs[t];
     int n = A.num[t];
     const int *nb = A.nbr + t;
     auto pair = [&](const double4 &xj) {
@@ -235,7 +235,7 @@ __global__ void __launch_bounds__(128, 8) k_eam_rho(PairArgs A, EamTables T, dou
   const int t = blockIdx.x * blockDim.x + threadIdx.x;   // list slot
   if (t >= A.nsi) return;
   const int i = site_of_slot(A, t);                       // site-table index
-  double4 xi = A.xs[i];
+  double4 xi = A.xs[t];
   int n = A.num[t];
   const int *nb = A.nbr + t;
   double rho = 0.0;
@@ -261,7 +261,7 @@ __global__ void __launch_bounds__(128, 8) k_eam_rho(PairArgs A, EamTables T, dou
   rho_out[slot] = rho;
   double phi = 0.0;
   double fp = eam_fp(T, rho, A.eflag ? &phi : nullptr);
-  ((double *)A.xs)[4 * (size_t)i + 3] = fp;
+  ((double *)A.xs)[4 * (size_t)t + 3] = fp;
   if (A.eflag) phi_site[i] = phi;
 }
 
@@ -290,7 +290,7 @@ __global__ void __launch_bounds__(128, EV ? 4 : 6) k_eam_force(PairArgs A, EamTa
   double fi[3] = {0, 0, 0}, esum = 0.0, vsum[6] = {0, 0, 0, 0, 0, 0};
   double eemb_site = 0.0, eemb_global = 0.0;
   if (valid) {
-    double4 xi = A.xs[i];
+    double4 xi = A.xs[t];
     double fpi = xi.w;
     int n = A.num[t];
     const int *nb = A.nbr + t;
@@ -429,7 +429,7 @@ void pair_compute(Ctx &c, int eflag, int vflag) {
   const int T = 128;
   const int nb = std::max(nblk(nsi, T), 1);
   PairArgs A;
-  A.xs = c.xs.p;
+  A.xs = c.xss.p;
   A.nbr = c.nbr_full.p;
   A.num = c.num_full.p;
   A.slot_atom = c.slot_atom.p;
@@ -496,7 +496,7 @@ void pair_compute(Ctx &c, int eflag, int vflag) {
     if (c.ne) {
       KernelTimer t(c, "eam_site_fp");
       k_eam_site_fp<<<stride_grid((long)c.ne * NU, 256), 256, 0, c.stream>>>(
-          c.xs.p, c.act_gid.p, c.dev_nact.p, c.na + NG * c.ne, c.na, c.rho.p, Tb);
+          c.xss.p, c.act_gid.p, c.dev_nact.p, c.na + NG * c.ne, c.na, c.rho.p, Tb);
     }
     {
       KernelTimer t(c, "eam_force");

@@ -41,7 +41,8 @@ struct FixGrid {
   const int *site_rep;      // [nsite_i]
   const int *elem_rep;      // [ne]
   const int *act_gid;       // active lattice sites -> element * 729 + site
-  int nsi;
+  const int *slot_atom;     // list slot -> atom
+  int na, nsi;
 };
 
 __device__ __forceinline__ void pack_one(const double4 *xs, int k, const FixGrid &G, int4 *pos, int *bad) {
@@ -50,7 +51,8 @@ __device__ __forceinline__ void pack_one(const double4 *xs, int k, const FixGrid
   double lo[3] = {G.lo[0], G.lo[1], G.lo[2]};
   double sc[3] = {G.scale[0], G.scale[1], G.scale[2]};
   if (G.reps) {
-    int r = k < G.nsi ? G.site_rep[k] : G.elem_rep[G.act_gid[k - G.nsi] / NU];
+    int r = k < G.na ? G.site_rep[G.slot_atom[k]]
+                     : (k < G.nsi ? G.site_rep[k] : G.elem_rep[G.act_gid[k - G.nsi] / NU]);
     const Rep *R = G.reps + r;
 #pragma unroll
     for (int d = 0; d < 3; d++) {
@@ -74,8 +76,8 @@ __device__ __forceinline__ void pack_one(const double4 *xs, int k, const FixGrid
   pos[k] = make_int4(o[0], o[1], o[2], v.w);
 }
 
-// Fixed-point copy of every site's position; w keeps F' for EAM (written
-// later in the step).  The active-site count is read on the device, so a
+// Fixed-point copy of the pair table (list-slot order); w keeps F' for EAM
+// (written later in the step).  The active-site count is read on the device, so a
 // fixed grid strides over [atoms | Gauss points | active sites].
 __global__ void k_pack32(const double4 *xs, int nsi, const int *nact_dev, FixGrid G, int4 *pos, int *bad) {
   const int n = nsi + *nact_dev;
@@ -222,7 +224,7 @@ __global__ void __launch_bounds__(128, EV ? 4 : 8) k_lj32(Args32 A, Lj32 P) {
   float fi[3] = {0, 0, 0}, esum = 0.f, vsum[6] = {0, 0, 0, 0, 0, 0};
   if (valid) {
     int4 oi;
-    site_frame(A, i, oi);
+    site_frame(A, t, oi);
     for_each32(A, t, i, oi, [&](float dx, float dy, float dz, float) {
       float rsq = dx * dx + dy * dy + dz * dz;
       if (rsq < P.cutsq) {
@@ -280,7 +282,7 @@ __global__ void __launch_bounds__(128, 8) k_eam_rho32(Args32 A, Eam32 T, double 
   if (t >= A.nsi) return;
   const int i = site_of_slot(A, t);                       // site-table index
   int4 oi;
-  site_frame(A, i, oi);
+  site_frame(A, t, oi);
   float rho = 0.f;
   for_each32(A, t, i, oi, [&](float dx, float dy, float dz, float) {
     float rsq = dx * dx + dy * dy + dz * dz;
@@ -302,7 +304,7 @@ __global__ void __launch_bounds__(128, 8) k_eam_rho32(Args32 A, Eam32 T, double 
   rho_out[slot] = rho;
   float phi = 0.f;
   float fp = fp32_of(T, rho, A.eflag ? &phi : nullptr);
-  pos_w[i].w = __float_as_int(fp);
+  pos_w[t].w = __float_as_int(fp);
   if (A.eflag) phi_site[i] = phi;
 }
 
@@ -329,7 +331,7 @@ __global__ void __launch_bounds__(128, EV ? 4 : 8) k_eam_force32(Args32 A, Eam32
   double eemb_site = 0.0, eemb_global = 0.0;
   if (valid) {
     int4 oi;
-    site_frame(A, i, oi);
+    site_frame(A, t, oi);
     const float fpi = __int_as_float(oi.w);
     for_each32(A, t, i, oi, [&](float dx, float dy, float dz, float fpj) {
       float rsq = dx * dx + dy * dy + dz * dz;
@@ -395,6 +397,8 @@ FixGrid make_fix_grid(const Ctx &c) {
   G.site_rep = c.site_rep.p;
   G.elem_rep = c.elem_rep.p;
   G.act_gid = c.act_gid.p;
+  G.slot_atom = c.slot_atom.p;
+  G.na = c.na;
   G.nsi = c.nsite_i();
   return G;
 }
@@ -425,7 +429,7 @@ void pair_compute_mixed(Ctx &c, int eflag, int vflag) {
   c.overflow.reserve(8);
   {
     KernelTimer t(c, "pack32");
-    k_pack32<<<stride_grid(ns, 256), 256, 0, c.stream>>>(c.xs.p, nsi, c.dev_nact.p, G, c.pos32.p,
+    k_pack32<<<stride_grid(ns, 256), 256, 0, c.stream>>>(c.xss.p, nsi, c.dev_nact.p, G, c.pos32.p,
                                                          c.overflow.p + 6);
   }
   Args32 A;
