@@ -56,11 +56,20 @@ std::vector<PendingTimer> &pending_for(Ctx &c) {
 Ctx::Ctx(int dev) : device(dev) {
   CACB200_CUDA(cudaSetDevice(dev));
   CACB200_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+  CACB200_CUDA(cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking));
+  CACB200_CUDA(cudaEventCreateWithFlags(&fork_ev, cudaEventDisableTiming));
+  CACB200_CUDA(cudaEventCreateWithFlags(&join_ev, cudaEventDisableTiming));
 }
 
 Ctx::~Ctx() {
   if (g_build) cudaGraphExecDestroy(g_build);
   if (g_steps) cudaGraphExecDestroy(g_steps);
+  if (side) {
+    cudaStreamSynchronize(side);
+    cudaStreamDestroy(side);
+  }
+  if (fork_ev) cudaEventDestroy(fork_ev);
+  if (join_ev) cudaEventDestroy(join_ev);
   if (stream) {
     cudaStreamSynchronize(stream);
     auto &pend = pending_for(*this);

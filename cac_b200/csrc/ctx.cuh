@@ -130,6 +130,11 @@ struct Profile {
 struct Ctx {
   int device = 0;
   cudaStream_t stream = nullptr;
+  // second stream for work that overlaps inside one stage (the Gauss-point
+  // list build beside the atom list build), forked from and joined back to
+  // `stream` with events, so it is part of the same order and of graphs
+  cudaStream_t side = nullptr;
+  cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
   std::string last_error;
   int precision = CACB200_FP64;
 
