@@ -57,6 +57,7 @@ Ctx::Ctx(int dev) : device(dev) {
   CACB200_CUDA(cudaSetDevice(dev));
   CACB200_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
   CACB200_CUDA(cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking));
+  CACB200_CUDA(cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, dev));
   CACB200_CUDA(cudaEventCreateWithFlags(&fork_ev, cudaEventDisableTiming));
   CACB200_CUDA(cudaEventCreateWithFlags(&join_ev, cudaEventDisableTiming));
 }

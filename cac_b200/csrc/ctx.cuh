@@ -129,6 +129,7 @@ struct Profile {
 
 struct Ctx {
   int device = 0;
+  int num_sms = 148;             // multiprocessors of the device (persistent launches)
   cudaStream_t stream = nullptr;
   // second stream for work that overlaps inside one stage (the Gauss-point
   // list build beside the atom list build), forked from and joined back to
