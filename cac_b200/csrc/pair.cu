@@ -63,7 +63,10 @@ __device__ __forceinline__ void neighbour_pos(const PairArgs &A, double Lx, doub
 // Walks a site's list four entries at a time: the four entry loads, then the
 // four position loads, are issued back to back before any of them is used, so
 // each thread keeps eight independent loads in flight instead of a chain of
-// dependent pairs.  MANY: the site belongs to a batch replica with its own box.
+// dependent pairs.  List entries are read once per pass: they are loaded as
+// streaming (evict-first) so that L1 keeps the neighbour positions and spline
+// records, which are reused.  MANY: the site belongs to a batch replica with
+// its own box.
 template <bool MANY, class F>
 __device__ __forceinline__ void for_each_neighbour(const PairArgs &A, int i, const int *nb, int n, F &&f) {
   double Lx = A.L[0], Ly = A.L[1], Lz = A.L[2];
@@ -75,8 +78,8 @@ __device__ __forceinline__ void for_each_neighbour(const PairArgs &A, int i, con
   }
   int k = 0;
   for (; k + 4 <= n; k += 4) {
-    int v0 = nb[(size_t)k * A.nsi], v1 = nb[(size_t)(k + 1) * A.nsi];
-    int v2 = nb[(size_t)(k + 2) * A.nsi], v3 = nb[(size_t)(k + 3) * A.nsi];
+    int v0 = __ldcs(nb + (size_t)k * A.nsi), v1 = __ldcs(nb + (size_t)(k + 1) * A.nsi);
+    int v2 = __ldcs(nb + (size_t)(k + 2) * A.nsi), v3 = __ldcs(nb + (size_t)(k + 3) * A.nsi);
     double4 p0, p1, p2, p3;
     neighbour_pos(A, Lx, Ly, Lz, v0, p0);
     neighbour_pos(A, Lx, Ly, Lz, v1, p1);
@@ -89,7 +92,7 @@ __device__ __forceinline__ void for_each_neighbour(const PairArgs &A, int i, con
   }
   for (; k < n; k++) {
     double4 p;
-    neighbour_pos(A, Lx, Ly, Lz, nb[(size_t)k * A.nsi], p);
+    neighbour_pos(A, Lx, Ly, Lz, __ldcs(nb + (size_t)k * A.nsi), p);
     f(p);
   }
 }

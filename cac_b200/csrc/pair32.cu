@@ -151,8 +151,8 @@ __device__ __forceinline__ void for_each32(const Args32 &A, int t, int i, const 
   const int *nb = A.nbr + t;
   int k = 0;
   for (; k + 4 <= n; k += 4) {
-    int v0 = nb[(size_t)k * A.nsi], v1 = nb[(size_t)(k + 1) * A.nsi];
-    int v2 = nb[(size_t)(k + 2) * A.nsi], v3 = nb[(size_t)(k + 3) * A.nsi];
+    int v0 = __ldcs(nb + (size_t)k * A.nsi), v1 = __ldcs(nb + (size_t)(k + 1) * A.nsi);
+    int v2 = __ldcs(nb + (size_t)(k + 2) * A.nsi), v3 = __ldcs(nb + (size_t)(k + 3) * A.nsi);
     float d[4][4];
     sep32(A, fx, oi, v0, d[0][0], d[0][1], d[0][2], d[0][3]);
     sep32(A, fx, oi, v1, d[1][0], d[1][1], d[1][2], d[1][3]);
@@ -163,7 +163,7 @@ __device__ __forceinline__ void for_each32(const Args32 &A, int t, int i, const 
   }
   for (; k < n; k++) {
     float dx, dy, dz, wj;
-    sep32(A, fx, oi, nb[(size_t)k * A.nsi], dx, dy, dz, wj);
+    sep32(A, fx, oi, __ldcs(nb + (size_t)k * A.nsi), dx, dy, dz, wj);
     f(dx, dy, dz, wj);
   }
 }
