@@ -274,6 +274,22 @@ def alg_bytes_per_site(kernel: str) -> int:
 TRAFFIC_PER_SITE = {"eam_force": 142.5e6 / 313120, "eam_force32": 122.8e6 / 313120}
 
 
+def stream_bytes(kernel: str, na: int, ne: int, nact: int) -> int:
+    """Compulsory HBM bytes per launch of the streaming kernels (FP64 state):
+    what each must read and write once, with per-element node data counted
+    once per element."""
+    nsi = na + 8 * ne
+    return {
+        "nve_initial": 120 * nsi,                       # read x, v, f; write x, v (atoms and nodes)
+        "nve_final": 72 * nsi,                          # read v, f; write v
+        "interpolate": 68 * na + 56 * 8 * ne + 36 * nact + 192 * ne,   # pair table: atoms, Gauss points, sites
+        "assemble": 384 * ne,                           # read Gauss-point forces, write nodal forces
+        "pack32": 52 * (nsi + nact),                    # read the pair table, write fixed-point records
+        "eam_site_fp": 12 * nact + 64 * ne,             # site ids, nodal density, F'
+        "eam_site_fp32": 12 * nact + 64 * ne,
+    }.get(kernel, 0)
+
+
 def alg_flops_per_site(kernel: str) -> int:
     """FP operations per site counted on the reference algorithm's Verlet-list
     candidates at the workloads' density: 78 candidates within cut + skin
@@ -391,6 +407,13 @@ def b200_arm(args, rank, local, ws, dist):
     hbm, hbm_kind = peaks()
     achieved = alg / (avg_ms / 1000.0) / 1e9
     launches_per_step = sum(v[1] for v in prof.values()) / nprof
+    nact = eng.counts()[2]
+    hbm_by_kernel = {}
+    for k, (tot_ms, nl) in sorted(prof.items()):
+        b = stream_bytes(k, natoms, nelements, nact)
+        if b and nl:
+            gbs = b / (tot_ms / nl / 1000.0) / 1e9
+            hbm_by_kernel[k] = {"gbs": gbs, "frac": gbs / hbm, "bytes_per_launch": b}
     traffic = TRAFFIC_PER_SITE[dom[0]] * nsi if dom[0] in TRAFFIC_PER_SITE else None
     pipe = None
     if alg_flops_per_site(dom[0]):
@@ -474,6 +497,7 @@ def b200_arm(args, rank, local, ws, dist):
             "pipe_roofline": pipe,
             "kernels_ms_per_launch": {k: v[0] / max(v[1], 1) for k, v in sorted(prof.items())},
             "kernels_ms_per_step": {k: v[0] / nprof for k, v in sorted(prof.items())},
+            "hbm_by_kernel": hbm_by_kernel,
             "segment_steps": seg,
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": bytes_state,

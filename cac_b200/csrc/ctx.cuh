@@ -87,6 +87,7 @@ struct Rep {
   Grid ag, eg;
   int abase, ebase;
   double reach_budget;
+  float fmargin;      // bound on the error of FP32 separations in this box (A)
   double qscale[3];   // mixed form: fixed-point scale 2^k per dimension ...
   float qinv[3];      // ... and 2^-k
   int Lq[3];          // rint(L 2^k)

@@ -378,6 +378,22 @@ __device__ __forceinline__ void make_query(const BuildArgs &A, const RP &P, int 
   }
 }
 
+// A candidate atom j whose FP32 distance is below the cutoff by more than the
+// FP32 error bound: a neighbour for certain (the exact FP64 test would agree),
+// stored without that test.  Full lists only (the half rule needs the FP64
+// positions).
+__device__ __forceinline__ void accept_atom(const BuildArgs &A, const Query &q, int j, const int W[3], int &nf,
+                                            bool in_cut) {
+  int s[3] = {W[0] - q.ti[0], W[1] - q.ti[1], W[2] - q.ti[2]};
+  bool zero = (s[0] == 0 && s[1] == 0 && s[2] == 0);
+  if (q.iatom && j == q.i && zero) return;
+  if (s[0] < -1 || s[0] > 1 || s[1] < -1 || s[1] > 1 || s[2] < -1 || s[2] > 1) {
+    atomicExch(&A.overflow[2], 1);
+    return;
+  }
+  emit(A, q.slot, nf, A.raw_full, A.img_full, j, img_code(s[0], s[1], s[2]) | (in_cut ? IN_CUT : 0));
+}
+
 // A candidate atom j seen in a cell with wrap count W: exact test and storage
 // rules (atoms are inside the box after pbc, so their own wrap is zero).
 __device__ __forceinline__ void try_atom(const BuildArgs &A, const Query &q, int j, const int W[3],
@@ -569,8 +585,11 @@ __global__ void __launch_bounds__(32) k_build_atoms(BuildArgs A, RP P) {
   const int local = home - R.abase;
   const int nc0 = R.ag.nc[0], nc1 = R.ag.nc[1], nc2 = R.ag.nc[2];
   const int hx = local % nc0, hy = (local / nc0) % nc1, hz = local / (nc0 * nc1);
-  const float pre = (float)(A.cutneigh + 1e-3);
-  const float pre2 = pre * pre;
+  // FP32 screen: beyond cutneigh + margin never a neighbour, within
+  // cutneigh - margin always one; only the band between takes the FP64 test
+  const float pre = (float)A.cutneigh + R.fmargin, sure = (float)A.cutneigh - R.fmargin;
+  const float pre2 = pre * pre, sure2 = sure * sure;
+  const float fcut2 = (float)A.cutforcesq;
   for (int base = hbeg; base < hend; base += blockDim.x) {
     const int h = base + threadIdx.x;
     const bool active = h < hend;
@@ -602,8 +621,10 @@ __global__ void __launch_bounds__(32) k_build_atoms(BuildArgs A, RP P) {
             float4 pj = A.acell_pos32[k];
             if (!active) continue;
             float ex = wx - (pj.x + sx), ey = wy - (pj.y + sy), ez = wz - (pj.z + sz);
-            if (ex * ex + ey * ey + ez * ez > pre2) continue;
-            try_atom(A, q, __float_as_int(pj.w), W, nf, nh);
+            const float r2 = ex * ex + ey * ey + ez * ez;
+            if (r2 > pre2) continue;
+            if (r2 < sure2 && !A.want_half) accept_atom(A, q, __float_as_int(pj.w), W, nf, r2 < fcut2);
+            else try_atom(A, q, __float_as_int(pj.w), W, nf, nh);
           }
         }
       }
@@ -835,6 +856,14 @@ void neigh_plan(Ctx &c, bool want_half) {
       R.reach_budget = std::max(ereach, std::min(std::max(1.2 * ereach, ereach + 2.0), room));
     }
     setup_grids(c, R, c.rep_ne[r] > 0);
+    // FP32 separations of wrapped positions and shifted candidates (|x| <=
+    // X = |lo| + |hi| + L) carry at most ~4 ulp(X) of rounding per distance;
+    // 16 ulp of 2X bounds it with room to spare
+    {
+      double X = 1.0;
+      for (int d = 0; d < 3; d++) X = std::max(X, std::fabs(R.b.lo[d]) + std::fabs(R.b.hi[d]) + R.b.L[d]);
+      R.fmargin = (float)(16.0 * std::ldexp(1.0, std::ilogb(2.0 * X) - 23));
+    }
     // fixed-point frame of the mixed form: quantum 2^-26 A, box length in
     // quanta modulo 2^32 (pair separations are taken modulo 2^32 as well)
     for (int d = 0; d < 3; d++) {
