@@ -111,6 +111,33 @@ def test_seeded_vs_oracle(seed, pair, T, oracle_mod, tmp_path):
     e.close()
 
 
+@pytest.mark.parametrize("shift", [0.0, 4000.0])
+def test_tall_and_offset_boxes_vs_oracle(shift, oracle_mod, tmp_path):
+    """A 1,434 A tall box, and the same box moved 4,000 A from the origin:
+    the FP32 screens of the list build must stay exact where coordinates are
+    large (lists bit-exact, forces within the FP64 tolerance)."""
+    s = gen.replica(1500, 600, temperature=100.0, strain=0.02, seed=5)
+    if shift:
+        for a in (s.x, s.nodex):
+            a[..., 2] += shift
+        s.boxlo[2] += shift
+        s.boxhi[2] += shift
+    st = oracle_mod.OracleState(s)
+    e = make_engine(s, "eam", tmp_path)
+    e.build_lists(half=True)
+    for half in (True, False):
+        L = oracle_mod.build_list(st, 6.0, half)
+        assert np.array_equal(e.neighbor_list(half), L.canonical(s.natoms))
+        if half:
+            oracle_mod.eam_forces(st, L, oracle_mod.Eam(setfl_path(tmp_path)))
+        oracle_mod.free_list(L)
+    e.compute()
+    f, nf, _ = e.forces()
+    assert rel_err(f, st.f) < TOL
+    assert rel_err(nf, st.nodef) < TOL
+    e.close()
+
+
 def test_empty_and_atoms_only_and_elements_only(tmp_path, oracle_mod):
     """Edge cases: no elements; no atoms."""
     s = gen.build_slab(3, 1, 0, 6, temperature=20.0, seed=5)
