@@ -271,6 +271,7 @@ struct BuildArgs {
   const int *ecell_start;
   const int *ecell_elems;
   const int *atom_of_slot;    // list slot (cell-sorted position) -> atom index
+  int *site_flag;             // [ne * 729] marks the lattice sites some full list references
   int na, ne, nsi, cap;
   RefBins rb;                 // single systems only (half lists)
   double cutneigh, cutneighsq;
@@ -543,6 +544,7 @@ __device__ void element_candidates(const BuildArgs &A, const Query &q, int &nf, 
                 }
                 int val = KIND_SITE | (e * NU + u);
                 emit(A, q.slot, nf, A.raw_full, A.img_full, val, code | (rsq < A.cutforcesq ? IN_CUT : 0));
+                if (site_gauss(u) < 0) A.site_flag[e * NU + u] = 1;   // to be interpolated
                 if (A.want_half) {
                   bool keep = true;
                   if (!q.iatom) {
@@ -696,19 +698,6 @@ __global__ void __launch_bounds__(128) k_build_gauss(BuildArgs A, RP P) {
 
 // ------------------------------------------------------------- compaction
 
-__global__ void k_mark_sites(const int *raw, const int *num, int nsi, int cap, int *flag) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= nsi) return;
-  int n = min(num[i], cap);
-  for (int k = 0; k < n; k++) {
-    int v = raw[(size_t)k * nsi + i];
-    if (v & KIND_SITE) {
-      int gid = v & ~KIND_SITE;
-      if (site_gauss(gid % NU) < 0) flag[gid] = 1;
-    }
-  }
-}
-
 __global__ void k_act_table(const int *flag, const int *pref, int ngid, int ne, int nsi, int *act_gid,
                             int *act_off, int *nact, int *too_many) {
   int gid = blockIdx.x * blockDim.x + threadIdx.x;
@@ -732,26 +721,24 @@ __global__ void k_remap(const int *raw, const unsigned char *img, const int *num
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nsi) return;
   int n = min(num[i], cap);
-  int w = 0;
-  for (int pass = 0; pass < 2; pass++) {
-    const unsigned char want = pass == 0 ? IN_CUT : 0;
-    for (int k = 0; k < n; k++) {
-      size_t o = (size_t)k * nsi + i;
-      unsigned char im = img[o];
-      if ((im & IN_CUT) != want) continue;
-      int v = raw[o];
-      int sidx;
-      if (v & KIND_SITE) {
-        int gid = v & ~KIND_SITE;
-        int e = gid / NU, u = gid % NU;
-        int g = site_gauss(u);
-        sidx = (g >= 0) ? na + NG * e + g : na + NG * ne + pref[gid];
-      } else {
-        sidx = atom_slot[v];
-      }
-      out[(size_t)w * nsi + i] = (sidx << IMG_BITS) | (im & (IN_CUT - 1));
-      w++;
+  int nin = 0;
+  for (int k = 0; k < n; k++) nin += (img[(size_t)k * nsi + i] & IN_CUT) != 0;
+  int a = 0, b = nin;   // next in-cutoff and next other position
+  for (int k = 0; k < n; k++) {
+    size_t o = (size_t)k * nsi + i;
+    unsigned char im = img[o];
+    int v = raw[o];
+    int sidx;
+    if (v & KIND_SITE) {
+      int gid = v & ~KIND_SITE;
+      int e = gid / NU, u = gid % NU;
+      int g = site_gauss(u);
+      sidx = (g >= 0) ? na + NG * e + g : na + NG * ne + pref[gid];
+    } else {
+      sidx = atom_slot[v];
     }
+    const int w = (im & IN_CUT) ? a++ : b++;
+    out[(size_t)w * nsi + i] = (sidx << IMG_BITS) | (im & (IN_CUT - 1));
   }
 }
 
@@ -1015,6 +1002,8 @@ void neigh_build_async(Ctx &c, bool want_half) {
     A.ecell_start = c.ecell_start.p;
     A.ecell_elems = c.ecell_elems.p;
     A.atom_of_slot = c.slot_atom.p;
+    A.site_flag = c.site_flag.p;
+    if (ngid) CACB200_CUDA(cudaMemsetAsync(c.site_flag.p, 0, sizeof(int) * (ngid + 1), c.stream));
     A.na = c.na;
     A.ne = c.ne;
     A.nsi = nsi;
@@ -1060,8 +1049,6 @@ void neigh_build_async(Ctx &c, bool want_half) {
     int *flag = c.site_flag.p;
     int *pref = c.site_pref.p;
     if (ngid) {
-      CACB200_CUDA(cudaMemsetAsync(flag, 0, sizeof(int) * (ngid + 1), c.stream));
-      k_mark_sites<<<nblk(nsi, 256), 256, 0, c.stream>>>(c.raw_full.p, c.num_full.p, nsi, c.cap, flag);
       size_t bytes = c.cub_bytes;
       CACB200_CUDA(cub::DeviceScan::ExclusiveSum(c.cub_tmp.p, bytes, flag, pref, (int)(ngid + 1), c.stream));
       k_act_table<<<nblk((long)ngid, 256), 256, 0, c.stream>>>(flag, pref, (int)ngid, c.ne, nsi, c.act_gid.p,
