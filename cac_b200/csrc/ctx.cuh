@@ -199,6 +199,10 @@ struct Ctx {
   DBuf<float4> acell_pos32;      // [na] the same as floats, w = bitcast(int id)
   DBuf<int> ecell_start, ecell_elems;
   DBuf<int> cell_key, cell_key2, idx_tmp;
+  DBuf<int> atom_work, atom_nwork;   // atoms with element sites in reach (rebuild work list)
+  DBuf<int2> items;                  // [slots][item_cap] element boxes to test, per query
+  DBuf<int> nitems;                  // [slots]
+  int item_cap = 48;
   // list slot -> atom (atoms sorted by cell at the last rebuild; slots past
   // the atoms are Gauss points in site-table order).  Lists, counts and the
   // pair kernels' threads are indexed by slot, so a warp covers a compact
@@ -229,7 +233,7 @@ struct Ctx {
   DBuf<unsigned char> img_full, img_half;
   DBuf<int> site_flag;           // [ne*729 + 1] marks
   DBuf<int> site_pref;           // [ne*729 + 1] exclusive prefix of the marks
-  DBuf<int> overflow;            // [4] device flags
+  DBuf<int> overflow;            // [16] device flags (see neigh_check)
   int build_count = 0;
 
   PairParams pp;

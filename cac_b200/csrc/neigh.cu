@@ -439,20 +439,43 @@ __device__ __forceinline__ void wrap_cell(int v, int nc, int &cell, int &W) {
   cell = v;
 }
 
-// Lattice sites of the elements near the query point.
-__device__ void element_candidates(const BuildArgs &A, const Query &q, int &nf, int &nh) {
+// Element lattice sites are found in two phases.  Phase A (one thread per
+// query) walks the element cells around the query and, for every element
+// whose site box in lattice-index space is not empty, writes a work item:
+// the element, the periodic image and the box.  Phase B (one warp per query)
+// tests the sites of each item with the lanes splitting the box, emitting in
+// box order, so the list is the one a serial walk would write.
+
+// work item: x = element | (image + 4 per dimension, 3 bits each) << 21,
+// y = box lo/hi in lattice indices (4 bits each)
+__device__ __forceinline__ int2 pack_item(int e, const int s[3], const int lo[3], const int hi[3]) {
+  int x = e | ((s[0] + 4) << 21) | ((s[1] + 4) << 24) | ((s[2] + 4) << 27);
+  int y = lo[0] | (lo[1] << 4) | (lo[2] << 8) | (hi[0] << 12) | (hi[1] << 16) | (hi[2] << 20);
+  return make_int2(x, y);
+}
+__device__ __forceinline__ void unpack_item(int2 it, int &e, int s[3], int lo[3], int hi[3]) {
+  e = it.x & ((1 << 21) - 1);
+  s[0] = ((it.x >> 21) & 7) - 4;
+  s[1] = ((it.x >> 24) & 7) - 4;
+  s[2] = ((it.x >> 27) & 7) - 4;
+#pragma unroll
+  for (int d = 0; d < 3; d++) {
+    lo[d] = (it.y >> (4 * d)) & 15;
+    hi[d] = (it.y >> (12 + 4 * d)) & 15;
+  }
+}
+
+// Phase A for one query: the element walk (candidate sphere test, then the
+// lattice-index box of the sites whose affine position can lie within
+// cutneigh + the element's deviation from affine).  Returns the number of
+// items; at most cap are stored.
+__device__ int element_items(const BuildArgs &A, const Query &q, int2 *out, int cap) {
   const Grid &eg = q.r.eg;
   int ci[3];
 #pragma unroll
   for (int d = 0; d < 3; d++)
     ci[d] = min(max((int)((q.wi[d] - q.r.b.lo[d]) * eg.inv[d]), 0), eg.nc[d] - 1);
-  double icen[3] = {0, 0, 0};
-  if (!q.iatom) {
-    double4 c = A.ecenter[q.ie];
-    icen[0] = c.x;
-    icen[1] = c.y;
-    icen[2] = c.z;
-  }
+  int n = 0;
   for (int oz = -1; oz <= 1; oz++) {
     int cz, Wz;
     wrap_cell(ci[2] + oz, eg.nc[2], cz, Wz);
@@ -466,7 +489,6 @@ __device__ void element_candidates(const BuildArgs &A, const Query &q, int &nf, 
         int beg = A.ecell_start[cell], end = A.ecell_start[cell + 1];
         if (beg == end) continue;
         int s[3] = {Wx - q.ti[0], Wy - q.ti[1], Wz - q.ti[2]};
-        bool zero = (s[0] == 0 && s[1] == 0 && s[2] == 0);
         double sL[3] = {s[0] * q.r.b.L[0], s[1] * q.r.b.L[1], s[2] * q.r.b.L[2]};
         for (int kk = beg; kk < end; kk++) {
           int e = A.ecell_elems[kk];
@@ -478,11 +500,6 @@ __device__ void element_candidates(const BuildArgs &A, const Query &q, int &nf, 
           double R = ce.w + dmax + A.cutneigh + 1e-6;
           double dcx = p[0] - ce.x, dcy = p[1] - ce.y, dcz = p[2] - ce.z;
           if (dcx * dcx + dcy * dcy + dcz * dcz > R * R) continue;
-          // a box shorter than the candidate sphere's diameter shows an element
-          // under two images; only a site actually within the cutoff at an
-          // image beyond the first is an error (checked at the distance test)
-          const bool far_image = s[0] < -1 || s[0] > 1 || s[1] < -1 || s[1] > 1 || s[2] < -1 || s[2] > 1;
-          // lattice-index box of the sites whose affine position is within cutneigh + dmax
           double rel[3] = {p[0] - fr[0], p[1] - fr[1], p[2] - fr[2]};
           int lo[3], hi[3];
           bool empty = false;
@@ -496,71 +513,152 @@ __device__ void element_candidates(const BuildArgs &A, const Query &q, int &nf, 
             if (lo[r] > hi[r]) empty = true;
           }
           if (empty) continue;
-          const double *nx = A.nodex + (size_t)e * 24;
-          double g[24];  // ghost node coordinates nodex + s L
-#pragma unroll
-          for (int k = 0; k < 8; k++)
-#pragma unroll
-            for (int d = 0; d < 3; d++)
-              g[3 * k + d] = s[d] ? __dadd_rn(nx[3 * k + d], sL[d]) : nx[3 * k + d];
-          int code = far_image ? 0 : img_code(s[0], s[1], s[2]);
-          double qcen[3] = {0, 0, 0};
-          if (!zero) {
-            qcen[0] = s[0] ? __dadd_rn(ce.x, sL[0]) : ce.x;
-            qcen[1] = s[1] ? __dadd_rn(ce.y, sL[1]) : ce.y;
-            qcen[2] = s[2] ? __dadd_rn(ce.z, sL[2]) : ce.z;
+          // a box shorter than the candidate sphere's diameter shows an element
+          // under two images; images beyond +-2 cannot be encoded (and are far
+          // beyond any cutoff in such a box)
+          if (s[0] < -3 || s[0] > 3 || s[1] < -3 || s[1] > 3 || s[2] < -3 || s[2] > 3) {
+            atomicExch(&A.overflow[2], 1);
+            continue;
           }
-          // affine position of site (a, bb, cc) relative to the query, in FP32:
-          // a cheap superset test (radius cutneigh + dmax + margin) before the
-          // exact FP64 distance
-          const float fa0 = (float)fr[13], fa1 = (float)fr[14], fa2 = (float)fr[15];
-          const float fb0 = (float)fr[16], fb1 = (float)fr[17], fb2 = (float)fr[18];
-          const float fc0 = (float)fr[19], fc1 = (float)fr[20], fc2 = (float)fr[21];
-          const float r0 = (float)rel[0], r1 = (float)rel[1], r2 = (float)rel[2];
-          const float lim = (float)(A.cutneigh + dmax) + 1e-3f;
-          const float lim2 = lim * lim;
-          for (int a = lo[0]; a <= hi[0]; a++)
-            for (int bb = lo[1]; bb <= hi[1]; bb++)
-              for (int cc = lo[2]; cc <= hi[2]; cc++) {
-                float ex = r0 - (a * fa0 + bb * fb0 + cc * fc0);
-                float ey = r1 - (a * fa1 + bb * fb1 + cc * fc1);
-                float ez = r2 - (a * fa2 + bb * fb2 + cc * fc2);
-                if (ex * ex + ey * ey + ez * ez > lim2) continue;
-                int u = (a * NC + bb) * NC + cc;
-                if (!q.iatom && e == q.ie && u == q.iu && zero) continue;
-                double dx = q.xi[0], dy = q.xi[1], dz = q.xi[2];
-#pragma unroll
-                for (int k = 0; k < 8; k++) {
-                  double N = shape_val(u, k);
-                  dx = __dsub_rn(dx, __dmul_rn(N, g[3 * k]));
-                  dy = __dsub_rn(dy, __dmul_rn(N, g[3 * k + 1]));
-                  dz = __dsub_rn(dz, __dmul_rn(N, g[3 * k + 2]));
-                }
-                double rsq = rsq_rn(dx, dy, dz);
-                if (!(rsq <= A.cutneighsq)) continue;
-                if (far_image) {
-                  atomicExch(&A.overflow[2], 1);
-                  continue;
-                }
-                int val = KIND_SITE | (e * NU + u);
-                emit(A, q.slot, nf, A.raw_full, A.img_full, val, code | (rsq < A.cutforcesq ? IN_CUT : 0));
-                if (site_gauss(u) < 0) A.site_flag[e * NU + u] = 1;   // to be interpolated
-                if (A.want_half) {
-                  bool keep = true;
-                  if (!q.iatom) {
-                    int jg = site_gauss(u);
-                    if (jg >= 0) {
-                      if (zero) keep = (q.ie < e) || (q.ie == e && q.ig < jg);
-                      else keep = above_right(qcen, icen);
-                    }
-                  }
-                  if (keep) emit(A, q.slot, nh, A.raw_half, A.img_half, val, code);
-                }
-              }
+          if (n < cap) out[n] = pack_item(e, s, lo, hi);
+          n++;
         }
       }
     }
   }
+  return n;
+}
+
+__device__ __forceinline__ unsigned lanemask_lt() {
+  unsigned m;
+  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+  return m;
+}
+
+// Warp-wide emission: the lanes' accepted candidates are stored in lane
+// order after the entries already written, so a warp walking candidates in
+// chunks of 32 writes exactly the order of a serial walk.  Every lane keeps
+// the same count n.
+__device__ __forceinline__ void warp_emit(const BuildArgs &A, int slot, int &n, int *raw, unsigned char *img,
+                                          bool pass, int val, int code) {
+  const unsigned m = __ballot_sync(0xffffffffu, pass);
+  if (pass) {
+    const int at = n + __popc(m & lanemask_lt());
+    if (at < A.cap) {
+      raw[(size_t)at * A.nsi + slot] = val;
+      img[(size_t)at * A.nsi + slot] = (unsigned char)code;
+    }
+  }
+  n += __popc(m);
+}
+
+// Phase B for one item of a query: the lanes split the site box (a outer, cc
+// inner, the serial order); each site takes the FP32 affine screen, then the
+// reference's exact FP64 distance.  g: the warp's shared scratch for the 24
+// ghost node coordinates.
+__device__ void item_sites(const BuildArgs &A, const Query &q, int2 item, double *g, int &nf, int &nh) {
+  const int lane = threadIdx.x & 31;
+  int e, s[3], lo[3], hi[3];
+  unpack_item(item, e, s, lo, hi);
+  const bool zero = (s[0] == 0 && s[1] == 0 && s[2] == 0);
+  const bool far_image = s[0] < -1 || s[0] > 1 || s[1] < -1 || s[1] > 1 || s[2] < -1 || s[2] > 1;
+  const double sL[3] = {s[0] * q.r.b.L[0], s[1] * q.r.b.L[1], s[2] * q.r.b.L[2]};
+  const double *nx = A.nodex + (size_t)e * 24;
+  __syncwarp();
+  if (lane < 24) {
+    const int d = lane % 3;
+    g[lane] = s[d] ? __dadd_rn(nx[lane], sL[d]) : nx[lane];
+  }
+  __syncwarp();
+  const double *fr = A.eframe + (size_t)e * 24;
+  const double dmax = fr[12];
+  const double4 ce = A.ecenter[e];
+  const int code = far_image ? 0 : img_code(s[0], s[1], s[2]);
+  double qcen[3] = {0, 0, 0}, icen[3] = {0, 0, 0};
+  if (A.want_half && !q.iatom) {
+    if (!zero) {
+      qcen[0] = s[0] ? __dadd_rn(ce.x, sL[0]) : ce.x;
+      qcen[1] = s[1] ? __dadd_rn(ce.y, sL[1]) : ce.y;
+      qcen[2] = s[2] ? __dadd_rn(ce.z, sL[2]) : ce.z;
+    }
+    double4 c = A.ecenter[q.ie];
+    icen[0] = c.x;
+    icen[1] = c.y;
+    icen[2] = c.z;
+  }
+  const float fa0 = (float)fr[13], fa1 = (float)fr[14], fa2 = (float)fr[15];
+  const float fb0 = (float)fr[16], fb1 = (float)fr[17], fb2 = (float)fr[18];
+  const float fc0 = (float)fr[19], fc1 = (float)fr[20], fc2 = (float)fr[21];
+  const float r0 = (float)(q.xi[0] - sL[0] - fr[0]), r1 = (float)(q.xi[1] - sL[1] - fr[1]),
+              r2 = (float)(q.xi[2] - sL[2] - fr[2]);
+  const float lim = (float)(A.cutneigh + dmax) + 1e-3f;
+  const float lim2 = lim * lim;
+  const int n1 = hi[1] - lo[1] + 1, n2 = hi[2] - lo[2] + 1;
+  const int nbox = (hi[0] - lo[0] + 1) * n1 * n2;
+  for (int base = 0; base < nbox; base += 32) {
+    const int t = base + lane;
+    bool pf = false, ph = false;
+    int val = 0, codef = 0;
+    if (t < nbox) {
+      const int cc = lo[2] + t % n2, bb = lo[1] + (t / n2) % n1, a = lo[0] + t / (n1 * n2);
+      const float ex = r0 - (a * fa0 + bb * fb0 + cc * fc0);
+      const float ey = r1 - (a * fa1 + bb * fb1 + cc * fc1);
+      const float ez = r2 - (a * fa2 + bb * fb2 + cc * fc2);
+      const int u = (a * NC + bb) * NC + cc;
+      if (ex * ex + ey * ey + ez * ez <= lim2 && !(!q.iatom && e == q.ie && u == q.iu && zero)) {
+        double dx = q.xi[0], dy = q.xi[1], dz = q.xi[2];
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+          double N = shape_val(u, k);
+          dx = __dsub_rn(dx, __dmul_rn(N, g[3 * k]));
+          dy = __dsub_rn(dy, __dmul_rn(N, g[3 * k + 1]));
+          dz = __dsub_rn(dz, __dmul_rn(N, g[3 * k + 2]));
+        }
+        double rsq = rsq_rn(dx, dy, dz);
+        if (rsq <= A.cutneighsq) {
+          if (far_image) {
+            atomicExch(&A.overflow[2], 1);
+          } else {
+            pf = true;
+            val = KIND_SITE | (e * NU + u);
+            codef = code | (rsq < A.cutforcesq ? IN_CUT : 0);
+            if (site_gauss(u) < 0) A.site_flag[e * NU + u] = 1;   // to be interpolated
+            ph = true;
+            if (!q.iatom) {
+              int jg = site_gauss(u);
+              if (jg >= 0) {
+                if (zero) ph = (q.ie < e) || (q.ie == e && q.ig < jg);
+                else ph = above_right(qcen, icen);
+              }
+            }
+          }
+        }
+      }
+    }
+    warp_emit(A, q.slot, nf, A.raw_full, A.img_full, pf, val, codef);
+    if (A.want_half) warp_emit(A, q.slot, nh, A.raw_half, A.img_half, ph, val, code);
+  }
+}
+
+// An atom candidate j of a Gauss point seen in a cell with wrap count W:
+// the exact distance test; code gets the image and the in-cutoff mark
+// (Gauss points keep no atoms in half lists).
+__device__ __forceinline__ bool gauss_atom_test(const BuildArgs &A, const Query &q, int j, const int W[3],
+                                                int &code) {
+  int s[3] = {W[0] - q.ti[0], W[1] - q.ti[1], W[2] - q.ti[2]};
+  double4 xj = A.xs[j];
+  double qq[3] = {xj.x, xj.y, xj.z};
+  qq[0] = s[0] ? __dadd_rn(qq[0], s[0] * q.r.b.L[0]) : qq[0];
+  qq[1] = s[1] ? __dadd_rn(qq[1], s[1] * q.r.b.L[1]) : qq[1];
+  qq[2] = s[2] ? __dadd_rn(qq[2], s[2] * q.r.b.L[2]) : qq[2];
+  double rsq = rsq_rn(__dsub_rn(q.xi[0], qq[0]), __dsub_rn(q.xi[1], qq[1]), __dsub_rn(q.xi[2], qq[2]));
+  if (!(rsq <= A.cutneighsq)) return false;
+  if (s[0] < -1 || s[0] > 1 || s[1] < -1 || s[1] > 1 || s[2] < -1 || s[2] > 1) {
+    atomicExch(&A.overflow[2], 1);
+    return false;
+  }
+  code = img_code(s[0], s[1], s[2]) | (rsq < A.cutforcesq ? IN_CUT : 0);
+  return true;
 }
 
 __device__ __forceinline__ void finish_counts(const BuildArgs &A, int i, int nf, int nh) {
@@ -638,27 +736,62 @@ __global__ void __launch_bounds__(32) k_build_atoms(BuildArgs A, RP P) {
   }
 }
 
-// Atoms, element lattice sites: appended after the atom neighbours, one
-// thread per list slot (cell-sorted order).  Atoms whose 27 element cells
-// hold no element leave at once.
+// Phase A over every list slot: the element walk of each atom and Gauss
+// point; atoms with at least one item go on the work list of phase B (its
+// order does not matter: an atom's entries depend on that atom alone).
 template <class RP>
-__global__ void __launch_bounds__(128) k_build_atom_sites(BuildArgs A, RP P) {
-  int h = blockIdx.x * blockDim.x + threadIdx.x;
-  if (h >= A.na) return;
+__global__ void __launch_bounds__(128) k_elem_items(BuildArgs A, RP P, int2 *items, int *nitems, int icap,
+                                                    int *work, int *nwork) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= A.nsi) return;
   Query q;
-  make_query(A, P, A.atom_of_slot[h], q);
-  q.slot = h;
-  int nf = A.num_full[h], nh = A.want_half ? A.num_half[h] : 0;
-  if (A.ne > 0) element_candidates(A, q, nf, nh);
-  finish_counts(A, h, nf, nh);
+  if (t < A.na) {
+    make_query(A, P, A.atom_of_slot[t], q);
+    q.slot = t;
+  } else {
+    make_query(A, P, t, q);
+  }
+  const int n = element_items(A, q, items + (size_t)t * icap, icap);
+  nitems[t] = n;
+  if (n > icap) {
+    atomicExch(&A.overflow[8], 1);
+    atomicMax(&A.overflow[9], n);
+  }
+  if (t < A.na && n > 0) work[atomicAdd(nwork, 1)] = t;
 }
 
-// Gauss points: one thread each; atoms from the 27 surrounding atom cells
-// (full list only), then element lattice sites.
+// Phase B for atoms: one warp per listed atom, its element sites appended
+// after its atom neighbours.
 template <class RP>
-__global__ void __launch_bounds__(128) k_build_gauss(BuildArgs A, RP P) {
-  int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= NG * A.ne) return;
+__global__ void __launch_bounds__(128) k_build_atom_sites(BuildArgs A, RP P, const int2 *items, const int *nitems,
+                                                          int icap, const int *work, const int *nwork) {
+  __shared__ double gsm[4][24];
+  double *g = gsm[threadIdx.x >> 5];
+  const int lane = threadIdx.x & 31;
+  const int nw = *nwork;
+  for (int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < nw; w += (gridDim.x * blockDim.x) >> 5) {
+    const int h = work[w];
+    Query q;
+    make_query(A, P, A.atom_of_slot[h], q);
+    q.slot = h;
+    int nf = A.num_full[h], nh = A.want_half ? A.num_half[h] : 0;
+    const int n = min(nitems[h], icap);
+    for (int k = 0; k < n; k++) item_sites(A, q, items[(size_t)h * icap + k], g, nf, nh);
+    if (lane == 0) finish_counts(A, h, nf, nh);
+    __syncwarp();
+  }
+}
+
+// Phase B for Gauss points: one warp each; atoms from the 27 surrounding atom
+// cells (full list only), 32 candidates at a time, then the element sites.
+template <class RP>
+__global__ void __launch_bounds__(128) k_build_gauss(BuildArgs A, RP P, const int2 *items, const int *nitems,
+                                                     int icap) {
+  __shared__ double gsm[4][24];
+  double *g = gsm[threadIdx.x >> 5];
+  const int t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (t >= NG * A.ne) return;   // whole warps
   Query q;
   make_query(A, P, A.na + t, q);
   const Grid &ag = q.r.ag;
@@ -682,18 +815,28 @@ __global__ void __launch_bounds__(128) k_build_gauss(BuildArgs A, RP P) {
           int W[3] = {Wx, Wy, Wz};
           double sh[3] = {Wx * q.r.b.L[0], Wy * q.r.b.L[1], Wz * q.r.b.L[2]};
           int beg = A.acell_start[cell], end = A.acell_start[cell + 1];
-          for (int k = beg; k < end; k++) {
-            double4 pj = A.acell_pos[k];
-            double ex = q.wi[0] - (pj.x + sh[0]), ey = q.wi[1] - (pj.y + sh[1]), ez = q.wi[2] - (pj.z + sh[2]);
-            if (ex * ex + ey * ey + ez * ez > pre) continue;
-            try_atom(A, q, (int)__double_as_longlong(pj.w), W, nf, nh);
+          for (int base = beg; base < end; base += 32) {
+            const int k = base + lane;
+            bool pass = false;
+            int j = 0, code = 0;
+            if (k < end) {
+              double4 pj = A.acell_pos[k];
+              double ex = q.wi[0] - (pj.x + sh[0]), ey = q.wi[1] - (pj.y + sh[1]), ez = q.wi[2] - (pj.z + sh[2]);
+              if (ex * ex + ey * ey + ez * ez <= pre) {
+                j = (int)__double_as_longlong(pj.w);
+                pass = gauss_atom_test(A, q, j, W, code);
+              }
+            }
+            warp_emit(A, q.slot, nf, A.raw_full, A.img_full, pass, j, code);
           }
         }
       }
     }
   }
-  element_candidates(A, q, nf, nh);
-  finish_counts(A, q.slot, nf, nh);
+  const int slot = A.na + t;
+  const int n = min(nitems[slot], icap);
+  for (int k = 0; k < n; k++) item_sites(A, q, items[(size_t)slot * icap + k], g, nf, nh);
+  if (lane == 0) finish_counts(A, q.slot, nf, nh);
 }
 
 // ------------------------------------------------------------- compaction
@@ -810,11 +953,11 @@ void neigh_plan(Ctx &c, bool want_half) {
   c.cutneighsq = c.cutneigh * c.cutneigh;
   c.ecenter.reserve(std::max(c.ne, 1));
   c.eframe.reserve((size_t)std::max(c.ne, 1) * 24);
-  c.overflow.reserve(8);
+  c.overflow.reserve(16);
   c.dev_nact.reserve(1);
   c.reach_bits.reserve(c.nrep);
   c.rep_d.reserve(c.nrep);
-  CACB200_CUDA(cudaMemsetAsync(c.overflow.p, 0, 8 * sizeof(int), c.stream));
+  CACB200_CUDA(cudaMemsetAsync(c.overflow.p, 0, 16 * sizeof(int), c.stream));
   CACB200_CUDA(cudaMemsetAsync(c.dev_nact.p, 0, sizeof(int), c.stream));
   CACB200_CUDA(cudaMemsetAsync(c.reach_bits.p, 0, sizeof(unsigned long long) * c.nrep, c.stream));
   // element geometry with no reach limit, to measure each replica's radius
@@ -901,6 +1044,10 @@ void neigh_plan(Ctx &c, bool want_half) {
     c.num_half.reserve(std::max(nsi, 1));
     c.nbr_half.reserve(slots);
   }
+  c.items.reserve((size_t)std::max(nsi, 1) * c.item_cap);
+  c.nitems.reserve(std::max(nsi, 1));
+  c.atom_work.reserve(std::max(c.na, 1));
+  c.atom_nwork.reserve(1);
   c.site_flag.reserve(ngid + 1);
   c.site_pref.reserve(ngid + 1);
   c.act_gid.reserve(std::max<size_t>(ngid, 1));
@@ -956,6 +1103,7 @@ void neigh_build_async(Ctx &c, bool want_half) {
   const int nsi = c.nsite_i();
   const size_t ngid = (size_t)c.ne * NU;
   CACB200_CUDA(cudaMemsetAsync(c.overflow.p, 0, 4 * sizeof(int), c.stream));
+  CACB200_CUDA(cudaMemsetAsync(c.overflow.p + 8, 0, 2 * sizeof(int), c.stream));
   with_reps(c, [&](auto P) {
     {
       KernelTimer t(c, "pbc_geom");
@@ -1020,27 +1168,35 @@ void neigh_build_async(Ctx &c, bool want_half) {
     A.num_half = want_half ? c.num_half.p : nullptr;
     A.img_half = want_half ? c.img_half.p : nullptr;
     A.overflow = c.overflow.p;
-    // The Gauss-point lists and the atom lists touch disjoint slots: unless
-    // kernels are being timed one by one, the Gauss-point build runs on the
-    // side stream beside the atom build (both are latency-bound walks).
+    // Phase A for every slot, then the Gauss-point lists (phase B) beside
+    // the atom lists: they touch disjoint slots, so unless kernels are being
+    // timed one by one the Gauss-point build runs on the side stream.
+    if (c.ne) {
+      KernelTimer t(c, "build_items");
+      CACB200_CUDA(cudaMemsetAsync(c.atom_nwork.p, 0, sizeof(int), c.stream));
+      k_elem_items<<<nblk(nsi, 128), 128, 0, c.stream>>>(A, P, c.items.p, c.nitems.p, c.item_cap, c.atom_work.p,
+                                                        c.atom_nwork.p);
+    }
     const bool split = c.na && c.ne && !c.prof.enabled;
     if (split) {
       CACB200_CUDA(cudaEventRecord(c.fork_ev, c.stream));
       CACB200_CUDA(cudaStreamWaitEvent(c.side, c.fork_ev, 0));
-      k_build_gauss<<<nblk(NG * c.ne, 128), 128, 0, c.side>>>(A, P);
+      k_build_gauss<<<nblk(32L * NG * c.ne, 128), 128, 0, c.side>>>(A, P, c.items.p, c.nitems.p, c.item_cap);
       CACB200_CUDA(cudaEventRecord(c.join_ev, c.side));
     }
     if (c.na) {
       KernelTimer t(c, "build_atoms");
       k_build_atoms<<<c.agrid.ncell, 32, 0, c.stream>>>(A, P);
     }
-    if (c.na) {
+    if (c.na && c.ne) {
       KernelTimer t(c, "build_atom_sites");
-      k_build_atom_sites<<<nblk(c.na, 128), 128, 0, c.stream>>>(A, P);
+      k_build_atom_sites<<<stride_grid(32L * c.na, 128), 128, 0, c.stream>>>(A, P, c.items.p, c.nitems.p,
+                                                                            c.item_cap, c.atom_work.p,
+                                                                            c.atom_nwork.p);
     }
     if (c.ne && !split) {
       KernelTimer t(c, "build_gauss");
-      k_build_gauss<<<nblk(NG * c.ne, 128), 128, 0, c.stream>>>(A, P);
+      k_build_gauss<<<nblk(32L * NG * c.ne, 128), 128, 0, c.stream>>>(A, P, c.items.p, c.nitems.p, c.item_cap);
     }
     if (split) CACB200_CUDA(cudaStreamWaitEvent(c.stream, c.join_ev, 0));
   });
@@ -1070,7 +1226,7 @@ void neigh_build_async(Ctx &c, bool want_half) {
 // Read the rebuild's flag words (synchronises).  Returns 0 when the lists are
 // good, 1 when a capacity must grow (the plan was updated: rebuild again).
 int neigh_check(Ctx &c) {
-  int ov[8];
+  int ov[16];
   stream_copy(c, ov, c.overflow.p, sizeof(ov), cudaMemcpyDeviceToHost);
   if (ov[2]) throw Error(CACB200_EINVAL, "neighbour image beyond the first periodic image (box too small)");
   if (ov[6]) throw Error(CACB200_EUNSTABLE, "a site position is not finite or absurdly far from the box (unstable run)");
@@ -1081,6 +1237,10 @@ int neigh_check(Ctx &c) {
     again = 1;
   }
   if (ov[3]) again = 1;   // an element outgrew the candidate grid
+  if (ov[8]) {            // a query met more element boxes than its item slots
+    c.item_cap = ((ov[9] + 15) / 16) * 16;
+    again = 1;
+  }
   if (again) {
     c.lists_valid = false;
     neigh_plan(c, c.plan_half);

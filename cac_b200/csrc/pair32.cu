@@ -426,7 +426,7 @@ void pair_compute_mixed(Ctx &c, int eflag, int vflag) {
   const int nb = std::max(nblk(nsi, T), 1);
   FixGrid G = make_fix_grid(c);
   c.pos32.reserve(std::max(ns, 1L));
-  c.overflow.reserve(8);
+  c.overflow.reserve(16);
   {
     KernelTimer t(c, "pack32");
     k_pack32<<<stride_grid(ns, 256), 256, 0, c.stream>>>(c.xss.p, nsi, c.dev_nact.p, G, c.pos32.p,
