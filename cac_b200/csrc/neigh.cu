@@ -552,91 +552,123 @@ __device__ __forceinline__ void warp_emit(const BuildArgs &A, int slot, int &n, 
   n += __popc(m);
 }
 
-// Phase B for one item of a query: the lanes split the site box (a outer, cc
-// inner, the serial order); each site takes the FP32 affine screen, then the
-// reference's exact FP64 distance.  g: the warp's shared scratch for the 24
-// ghost node coordinates.
-__device__ void item_sites(const BuildArgs &A, const Query &q, int2 item, double *g, int &nf, int &nh) {
+// Phase B for one query: its items in groups of up to 32.  Lane k stages
+// item k of a group in the warp's shared scratch (the 24 ghost node
+// coordinates and the FP32 affine frame relative to the query), then the
+// lanes walk the group's sites flattened in (item, a, bb, cc) order -- the
+// serial order -- so small boxes do not leave lanes idle.  Each site takes the
+// FP32 affine screen, then the reference's exact FP64 distance.
+struct ItemStage {
+  double g[32][24];   // ghost node coordinates nodex + s L
+  float fr[32][13];   // frame columns a, b, c; query minus frame origin; screen radius^2
+};
+
+__device__ void items_warp(const BuildArgs &A, const Query &q, const int2 *items, int n, ItemStage &st, int &nf,
+                           int &nh) {
   const int lane = threadIdx.x & 31;
-  int e, s[3], lo[3], hi[3];
-  unpack_item(item, e, s, lo, hi);
-  const bool zero = (s[0] == 0 && s[1] == 0 && s[2] == 0);
-  const bool far_image = s[0] < -1 || s[0] > 1 || s[1] < -1 || s[1] > 1 || s[2] < -1 || s[2] > 1;
-  const double sL[3] = {s[0] * q.r.b.L[0], s[1] * q.r.b.L[1], s[2] * q.r.b.L[2]};
-  const double *nx = A.nodex + (size_t)e * 24;
-  __syncwarp();
-  if (lane < 24) {
-    const int d = lane % 3;
-    g[lane] = s[d] ? __dadd_rn(nx[lane], sL[d]) : nx[lane];
-  }
-  __syncwarp();
-  const double *fr = A.eframe + (size_t)e * 24;
-  const double dmax = fr[12];
-  const double4 ce = A.ecenter[e];
-  const int code = far_image ? 0 : img_code(s[0], s[1], s[2]);
-  double qcen[3] = {0, 0, 0}, icen[3] = {0, 0, 0};
-  if (A.want_half && !q.iatom) {
-    if (!zero) {
-      qcen[0] = s[0] ? __dadd_rn(ce.x, sL[0]) : ce.x;
-      qcen[1] = s[1] ? __dadd_rn(ce.y, sL[1]) : ce.y;
-      qcen[2] = s[2] ? __dadd_rn(ce.z, sL[2]) : ce.z;
-    }
-    double4 c = A.ecenter[q.ie];
-    icen[0] = c.x;
-    icen[1] = c.y;
-    icen[2] = c.z;
-  }
-  const float fa0 = (float)fr[13], fa1 = (float)fr[14], fa2 = (float)fr[15];
-  const float fb0 = (float)fr[16], fb1 = (float)fr[17], fb2 = (float)fr[18];
-  const float fc0 = (float)fr[19], fc1 = (float)fr[20], fc2 = (float)fr[21];
-  const float r0 = (float)(q.xi[0] - sL[0] - fr[0]), r1 = (float)(q.xi[1] - sL[1] - fr[1]),
-              r2 = (float)(q.xi[2] - sL[2] - fr[2]);
-  const float lim = (float)(A.cutneigh + dmax) + 1e-3f;
-  const float lim2 = lim * lim;
-  const int n1 = hi[1] - lo[1] + 1, n2 = hi[2] - lo[2] + 1;
-  const int nbox = (hi[0] - lo[0] + 1) * n1 * n2;
-  for (int base = 0; base < nbox; base += 32) {
-    const int t = base + lane;
-    bool pf = false, ph = false;
-    int val = 0, codef = 0;
-    if (t < nbox) {
-      const int cc = lo[2] + t % n2, bb = lo[1] + (t / n2) % n1, a = lo[0] + t / (n1 * n2);
-      const float ex = r0 - (a * fa0 + bb * fb0 + cc * fc0);
-      const float ey = r1 - (a * fa1 + bb * fb1 + cc * fc1);
-      const float ez = r2 - (a * fa2 + bb * fb2 + cc * fc2);
-      const int u = (a * NC + bb) * NC + cc;
-      if (ex * ex + ey * ey + ez * ez <= lim2 && !(!q.iatom && e == q.ie && u == q.iu && zero)) {
-        double dx = q.xi[0], dy = q.xi[1], dz = q.xi[2];
+  for (int g0 = 0; g0 < n; g0 += 32) {
+    const int gi = g0 + lane;
+    int2 it = make_int2(0, 0);
+    int nbox = 0;
+    __syncwarp();
+    if (gi < n) {
+      it = items[gi];
+      int e, sv[3], lo[3], hi[3];
+      unpack_item(it, e, sv, lo, hi);
+      nbox = (hi[0] - lo[0] + 1) * (hi[1] - lo[1] + 1) * (hi[2] - lo[2] + 1);
+      const double sL[3] = {sv[0] * q.r.b.L[0], sv[1] * q.r.b.L[1], sv[2] * q.r.b.L[2]};
+      const double *nx = A.nodex + (size_t)e * 24;
 #pragma unroll
-        for (int k = 0; k < 8; k++) {
-          double N = shape_val(u, k);
-          dx = __dsub_rn(dx, __dmul_rn(N, g[3 * k]));
-          dy = __dsub_rn(dy, __dmul_rn(N, g[3 * k + 1]));
-          dz = __dsub_rn(dz, __dmul_rn(N, g[3 * k + 2]));
-        }
-        double rsq = rsq_rn(dx, dy, dz);
-        if (rsq <= A.cutneighsq) {
-          if (far_image) {
-            atomicExch(&A.overflow[2], 1);
-          } else {
-            pf = true;
-            val = KIND_SITE | (e * NU + u);
-            codef = code | (rsq < A.cutforcesq ? IN_CUT : 0);
-            if (site_gauss(u) < 0) A.site_flag[e * NU + u] = 1;   // to be interpolated
-            ph = true;
-            if (!q.iatom) {
-              int jg = site_gauss(u);
-              if (jg >= 0) {
-                if (zero) ph = (q.ie < e) || (q.ie == e && q.ig < jg);
-                else ph = above_right(qcen, icen);
+      for (int k = 0; k < 24; k++) st.g[lane][k] = sv[k % 3] ? __dadd_rn(nx[k], sL[k % 3]) : nx[k];
+      const double *fr = A.eframe + (size_t)e * 24;
+#pragma unroll
+      for (int k = 0; k < 9; k++) st.fr[lane][k] = (float)fr[13 + k];
+#pragma unroll
+      for (int d = 0; d < 3; d++) st.fr[lane][9 + d] = (float)(q.xi[d] - sL[d] - fr[d]);
+      const float lim = (float)(A.cutneigh + fr[12]) + 1e-3f;
+      st.fr[lane][12] = lim * lim;
+    }
+    __syncwarp();
+    // exclusive prefix of the box sizes over the group's lanes
+    int incl = nbox;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      int v = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += v;
+    }
+    const int excl = incl - nbox;
+    const int total = __shfl_sync(0xffffffffu, incl, 31);
+    const int ng = min(32, n - g0);
+    for (int base = 0; base < total; base += 32) {
+      const int f = base + lane;
+      // item of flattened site f: the last lane m < ng with excl[m] <= f
+      int m = 0;
+#pragma unroll
+      for (int step = 16; step > 0; step >>= 1) {
+        const int cand = m + step;
+        const int v = __shfl_sync(0xffffffffu, excl, cand & 31);
+        if (cand < ng && v <= f) m = cand;
+      }
+      const int2 itm = make_int2(__shfl_sync(0xffffffffu, it.x, m), __shfl_sync(0xffffffffu, it.y, m));
+      const int exm = __shfl_sync(0xffffffffu, excl, m);
+      bool pf = false, ph = false;
+      int val = 0, codef = 0, code = 0;
+      if (f < total) {
+        int e, sv[3], lo[3], hi[3];
+        unpack_item(itm, e, sv, lo, hi);
+        const bool zero = (sv[0] == 0 && sv[1] == 0 && sv[2] == 0);
+        const bool far_image = sv[0] < -1 || sv[0] > 1 || sv[1] < -1 || sv[1] > 1 || sv[2] < -1 || sv[2] > 1;
+        code = far_image ? 0 : img_code(sv[0], sv[1], sv[2]);
+        const int n1 = hi[1] - lo[1] + 1, n2 = hi[2] - lo[2] + 1;
+        const int t = f - exm;
+        const int cc = lo[2] + t % n2, bb = lo[1] + (t / n2) % n1, a = lo[0] + t / (n1 * n2);
+        const float *F = st.fr[m];
+        const float ex = F[9] - (a * F[0] + bb * F[3] + cc * F[6]);
+        const float ey = F[10] - (a * F[1] + bb * F[4] + cc * F[7]);
+        const float ez = F[11] - (a * F[2] + bb * F[5] + cc * F[8]);
+        const int u = (a * NC + bb) * NC + cc;
+        if (ex * ex + ey * ey + ez * ez <= F[12] && !(!q.iatom && e == q.ie && u == q.iu && zero)) {
+          const double *g = st.g[m];
+          double dx = q.xi[0], dy = q.xi[1], dz = q.xi[2];
+#pragma unroll
+          for (int k = 0; k < 8; k++) {
+            double N = shape_val(u, k);
+            dx = __dsub_rn(dx, __dmul_rn(N, g[3 * k]));
+            dy = __dsub_rn(dy, __dmul_rn(N, g[3 * k + 1]));
+            dz = __dsub_rn(dz, __dmul_rn(N, g[3 * k + 2]));
+          }
+          double rsq = rsq_rn(dx, dy, dz);
+          if (rsq <= A.cutneighsq) {
+            if (far_image) {
+              atomicExch(&A.overflow[2], 1);
+            } else {
+              pf = true;
+              val = KIND_SITE | (e * NU + u);
+              codef = code | (rsq < A.cutforcesq ? IN_CUT : 0);
+              if (site_gauss(u) < 0) A.site_flag[e * NU + u] = 1;   // to be interpolated
+              ph = true;
+              if (A.want_half && !q.iatom) {
+                int jg = site_gauss(u);
+                if (jg >= 0) {
+                  if (zero) {
+                    ph = (q.ie < e) || (q.ie == e && q.ig < jg);
+                  } else {
+                    const double4 ce = A.ecenter[e], ci = A.ecenter[q.ie];
+                    const double sL[3] = {sv[0] * q.r.b.L[0], sv[1] * q.r.b.L[1], sv[2] * q.r.b.L[2]};
+                    double qcen[3] = {sv[0] ? __dadd_rn(ce.x, sL[0]) : ce.x, sv[1] ? __dadd_rn(ce.y, sL[1]) : ce.y,
+                                      sv[2] ? __dadd_rn(ce.z, sL[2]) : ce.z};
+                    double icen[3] = {ci.x, ci.y, ci.z};
+                    ph = above_right(qcen, icen);
+                  }
+                }
               }
             }
           }
         }
       }
+      warp_emit(A, q.slot, nf, A.raw_full, A.img_full, pf, val, codef);
+      if (A.want_half) warp_emit(A, q.slot, nh, A.raw_half, A.img_half, ph, val, code);
     }
-    warp_emit(A, q.slot, nf, A.raw_full, A.img_full, pf, val, codef);
-    if (A.want_half) warp_emit(A, q.slot, nh, A.raw_half, A.img_half, ph, val, code);
   }
 }
 
@@ -765,8 +797,8 @@ __global__ void __launch_bounds__(128) k_elem_items(BuildArgs A, RP P, int2 *ite
 template <class RP>
 __global__ void __launch_bounds__(128) k_build_atom_sites(BuildArgs A, RP P, const int2 *items, const int *nitems,
                                                           int icap, const int *work, const int *nwork) {
-  __shared__ double gsm[4][24];
-  double *g = gsm[threadIdx.x >> 5];
+  __shared__ ItemStage stage[4];
+  ItemStage &st = stage[threadIdx.x >> 5];
   const int lane = threadIdx.x & 31;
   const int nw = *nwork;
   for (int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < nw; w += (gridDim.x * blockDim.x) >> 5) {
@@ -775,8 +807,7 @@ __global__ void __launch_bounds__(128) k_build_atom_sites(BuildArgs A, RP P, con
     make_query(A, P, A.atom_of_slot[h], q);
     q.slot = h;
     int nf = A.num_full[h], nh = A.want_half ? A.num_half[h] : 0;
-    const int n = min(nitems[h], icap);
-    for (int k = 0; k < n; k++) item_sites(A, q, items[(size_t)h * icap + k], g, nf, nh);
+    items_warp(A, q, items + (size_t)h * icap, min(nitems[h], icap), st, nf, nh);
     if (lane == 0) finish_counts(A, h, nf, nh);
     __syncwarp();
   }
@@ -787,8 +818,8 @@ __global__ void __launch_bounds__(128) k_build_atom_sites(BuildArgs A, RP P, con
 template <class RP>
 __global__ void __launch_bounds__(128) k_build_gauss(BuildArgs A, RP P, const int2 *items, const int *nitems,
                                                      int icap) {
-  __shared__ double gsm[4][24];
-  double *g = gsm[threadIdx.x >> 5];
+  __shared__ ItemStage stage[4];
+  ItemStage &st = stage[threadIdx.x >> 5];
   const int t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (t >= NG * A.ne) return;   // whole warps
@@ -834,8 +865,7 @@ __global__ void __launch_bounds__(128) k_build_gauss(BuildArgs A, RP P, const in
     }
   }
   const int slot = A.na + t;
-  const int n = min(nitems[slot], icap);
-  for (int k = 0; k < n; k++) item_sites(A, q, items[(size_t)slot * icap + k], g, nf, nh);
+  items_warp(A, q, items + (size_t)slot * icap, min(nitems[slot], icap), st, nf, nh);
   if (lane == 0) finish_counts(A, q.slot, nf, nh);
 }
 
