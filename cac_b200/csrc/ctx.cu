@@ -60,6 +60,7 @@ Ctx::Ctx(int dev) : device(dev) {
   CACB200_CUDA(cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, dev));
   CACB200_CUDA(cudaEventCreateWithFlags(&fork_ev, cudaEventDisableTiming));
   CACB200_CUDA(cudaEventCreateWithFlags(&join_ev, cudaEventDisableTiming));
+  CACB200_CUDA(cudaEventCreateWithFlags(&items_ev, cudaEventDisableTiming));
 }
 
 Ctx::~Ctx() {
@@ -71,6 +72,7 @@ Ctx::~Ctx() {
   }
   if (fork_ev) cudaEventDestroy(fork_ev);
   if (join_ev) cudaEventDestroy(join_ev);
+  if (items_ev) cudaEventDestroy(items_ev);
   if (stream) {
     cudaStreamSynchronize(stream);
     auto &pend = pending_for(*this);

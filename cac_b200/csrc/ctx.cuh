@@ -136,7 +136,7 @@ struct Ctx {
   // list build beside the atom list build), forked from and joined back to
   // `stream` with events, so it is part of the same order and of graphs
   cudaStream_t side = nullptr;
-  cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
+  cudaEvent_t fork_ev = nullptr, join_ev = nullptr, items_ev = nullptr;
   std::string last_error;
   int precision = CACB200_FP64;
 

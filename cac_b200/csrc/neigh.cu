@@ -1198,35 +1198,41 @@ void neigh_build_async(Ctx &c, bool want_half) {
     A.num_half = want_half ? c.num_half.p : nullptr;
     A.img_half = want_half ? c.img_half.p : nullptr;
     A.overflow = c.overflow.p;
-    // Phase A for every slot, then the Gauss-point lists (phase B) beside
-    // the atom lists: they touch disjoint slots, so unless kernels are being
-    // timed one by one the Gauss-point build runs on the side stream.
-    if (c.ne) {
-      KernelTimer t(c, "build_items");
-      CACB200_CUDA(cudaMemsetAsync(c.atom_nwork.p, 0, sizeof(int), c.stream));
-      k_elem_items<<<nblk(nsi, 128), 128, 0, c.stream>>>(A, P, c.items.p, c.nitems.p, c.item_cap, c.atom_work.p,
-                                                        c.atom_nwork.p);
-    }
+    // The atom-atom lists need no element work: they run on the context
+    // stream while the side stream does phase A for every slot and then the
+    // Gauss-point lists (disjoint slots); the atoms' element sites follow the
+    // atom-atom lists once phase A is done.  Timed one kernel at a time when
+    // profiling.
     const bool split = c.na && c.ne && !c.prof.enabled;
+    cudaStream_t es = split ? c.side : c.stream;
     if (split) {
       CACB200_CUDA(cudaEventRecord(c.fork_ev, c.stream));
       CACB200_CUDA(cudaStreamWaitEvent(c.side, c.fork_ev, 0));
-      k_build_gauss<<<nblk(32L * NG * c.ne, 128), 128, 0, c.side>>>(A, P, c.items.p, c.nitems.p, c.item_cap);
-      CACB200_CUDA(cudaEventRecord(c.join_ev, c.side));
+    }
+    if (c.ne) {
+      {
+        KernelTimer t(c, "build_items");
+        CACB200_CUDA(cudaMemsetAsync(c.atom_nwork.p, 0, sizeof(int), es));
+        k_elem_items<<<nblk(nsi, 128), 128, 0, es>>>(A, P, c.items.p, c.nitems.p, c.item_cap, c.atom_work.p,
+                                                    c.atom_nwork.p);
+      }
+      if (split) CACB200_CUDA(cudaEventRecord(c.items_ev, c.side));
+      {
+        KernelTimer t(c, "build_gauss");
+        k_build_gauss<<<nblk(32L * NG * c.ne, 128), 128, 0, es>>>(A, P, c.items.p, c.nitems.p, c.item_cap);
+      }
+      if (split) CACB200_CUDA(cudaEventRecord(c.join_ev, c.side));
     }
     if (c.na) {
       KernelTimer t(c, "build_atoms");
       k_build_atoms<<<c.agrid.ncell, 32, 0, c.stream>>>(A, P);
     }
     if (c.na && c.ne) {
+      if (split) CACB200_CUDA(cudaStreamWaitEvent(c.stream, c.items_ev, 0));
       KernelTimer t(c, "build_atom_sites");
       k_build_atom_sites<<<stride_grid(32L * c.na, 128), 128, 0, c.stream>>>(A, P, c.items.p, c.nitems.p,
                                                                             c.item_cap, c.atom_work.p,
                                                                             c.atom_nwork.p);
-    }
-    if (c.ne && !split) {
-      KernelTimer t(c, "build_gauss");
-      k_build_gauss<<<nblk(32L * NG * c.ne, 128), 128, 0, c.stream>>>(A, P, c.items.p, c.nitems.p, c.item_cap);
     }
     if (split) CACB200_CUDA(cudaStreamWaitEvent(c.stream, c.join_ev, 0));
   });
