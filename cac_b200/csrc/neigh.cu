@@ -379,22 +379,6 @@ __device__ __forceinline__ void make_query(const BuildArgs &A, const RP &P, int 
   }
 }
 
-// A candidate atom j whose FP32 distance is below the cutoff by more than the
-// FP32 error bound: a neighbour for certain (the exact FP64 test would agree),
-// stored without that test.  Full lists only (the half rule needs the FP64
-// positions).
-__device__ __forceinline__ void accept_atom(const BuildArgs &A, const Query &q, int j, const int W[3], int &nf,
-                                            bool in_cut) {
-  int s[3] = {W[0] - q.ti[0], W[1] - q.ti[1], W[2] - q.ti[2]};
-  bool zero = (s[0] == 0 && s[1] == 0 && s[2] == 0);
-  if (q.iatom && j == q.i && zero) return;
-  if (s[0] < -1 || s[0] > 1 || s[1] < -1 || s[1] > 1 || s[2] < -1 || s[2] > 1) {
-    atomicExch(&A.overflow[2], 1);
-    return;
-  }
-  emit(A, q.slot, nf, A.raw_full, A.img_full, j, img_code(s[0], s[1], s[2]) | (in_cut ? IN_CUT : 0));
-}
-
 // A candidate atom j seen in a cell with wrap count W: exact test and storage
 // rules (atoms are inside the box after pbc, so their own wrap is zero).
 __device__ __forceinline__ void try_atom(const BuildArgs &A, const Query &q, int j, const int W[3],
@@ -704,66 +688,87 @@ __device__ __forceinline__ void finish_counts(const BuildArgs &A, int i, int nf,
 }
 
 // Atoms, atom neighbours: one block (one warp) per cell of the atom grid
-// (cell >= cutneigh); the lanes are the cell's atoms and walk the 27
-// surrounding cells together, so every candidate is one broadcast load shared
-// by the warp.  A conservative FP32 distance test (from a float copy of the
-// wrapped positions) screens candidates before the exact FP64 test.
+// (cell >= cutneigh); the lanes are the cell's
+// atoms and walk the 27 surrounding cells together, so every candidate is one
+// broadcast load shared by the warp.  A conservative FP32 distance test (from
+// a float copy of the wrapped positions) decides all but the candidates near
+// the cutoff, which take the exact FP64 test.  The image of a candidate cell
+// relative to each lane's atom is fixed per cell.
 template <class RP>
-__global__ void __launch_bounds__(32) k_build_atoms(BuildArgs A, RP P) {
-  const int home = blockIdx.x;
-  const int hbeg = A.acell_start[home], hend = A.acell_start[home + 1];
-  if (hbeg == hend) return;
-  const Rep R = P.acell(home);
-  const int local = home - R.abase;
-  const int nc0 = R.ag.nc[0], nc1 = R.ag.nc[1], nc2 = R.ag.nc[2];
-  const int hx = local % nc0, hy = (local / nc0) % nc1, hz = local / (nc0 * nc1);
-  // FP32 screen: beyond cutneigh + margin never a neighbour, within
-  // cutneigh - margin always one; only the band between takes the FP64 test
-  const float pre = (float)A.cutneigh + R.fmargin, sure = (float)A.cutneigh - R.fmargin;
-  const float pre2 = pre * pre, sure2 = sure * sure;
+__global__ void __launch_bounds__(32) k_build_atoms(BuildArgs A, RP P, int ncell) {
+  const int lane = threadIdx.x & 31;
   const float fcut2 = (float)A.cutforcesq;
-  for (int base = hbeg; base < hend; base += blockDim.x) {
-    const int h = base + threadIdx.x;
-    const bool active = h < hend;
-    Query q;
-    int nf = 0, nh = 0;
-    float wx = 0.f, wy = 0.f, wz = 0.f;
-    if (active) {
-      make_query(A, P, (int)__double_as_longlong(A.acell_pos[h].w), q);
-      q.slot = h;
-      float4 w = A.acell_pos32[h];
-      wx = w.x;
-      wy = w.y;
-      wz = w.z;
-    }
-    for (int oz = -1; oz <= 1; oz++) {
-      int cz, Wz;
-      wrap_cell(hz + oz, nc2, cz, Wz);
-      for (int oy = -1; oy <= 1; oy++) {
-        int cy, Wy;
-        wrap_cell(hy + oy, nc1, cy, Wy);
-        for (int ox = -1; ox <= 1; ox++) {
-          int cx, Wx;
-          wrap_cell(hx + ox, nc0, cx, Wx);
-          int cell = R.abase + (cz * nc1 + cy) * nc0 + cx;
-          int W[3] = {Wx, Wy, Wz};
-          const float sx = (float)(Wx * R.b.L[0]), sy = (float)(Wy * R.b.L[1]), sz = (float)(Wz * R.b.L[2]);
-          int beg = A.acell_start[cell], end = A.acell_start[cell + 1];
-          for (int k = beg; k < end; k++) {
-            float4 pj = A.acell_pos32[k];
-            if (!active) continue;
-            float ex = wx - (pj.x + sx), ey = wy - (pj.y + sy), ez = wz - (pj.z + sz);
-            const float r2 = ex * ex + ey * ey + ez * ez;
-            if (r2 > pre2) continue;
-            if (r2 < sure2 && !A.want_half) accept_atom(A, q, __float_as_int(pj.w), W, nf, r2 < fcut2);
-            else try_atom(A, q, __float_as_int(pj.w), W, nf, nh);
+  {
+    const int home = blockIdx.x;
+    const int hbeg = A.acell_start[home], hend = A.acell_start[home + 1];
+    if (hbeg == hend) return;
+    const Rep R = P.acell(home);
+    const int local = home - R.abase;
+    const int nc0 = R.ag.nc[0], nc1 = R.ag.nc[1], nc2 = R.ag.nc[2];
+    const int hx = local % nc0, hy = (local / nc0) % nc1, hz = local / (nc0 * nc1);
+    // FP32 screen: beyond cutneigh + margin never a neighbour, within
+    // cutneigh - margin always one; only the band between takes the FP64 test
+    const float pre = (float)A.cutneigh + R.fmargin, sure = (float)A.cutneigh - R.fmargin;
+    const float pre2 = pre * pre, sure2 = sure * sure;
+    for (int base = hbeg; base < hend; base += 32) {
+      const int h = base + lane;
+      const bool active = h < hend;
+      Query q;
+      int nf = 0, nh = 0;
+      float wx = 0.f, wy = 0.f, wz = 0.f;
+      if (active) {
+        make_query(A, P, (int)__double_as_longlong(A.acell_pos[h].w), q);
+        q.slot = h;
+        float4 w = A.acell_pos32[h];
+        wx = w.x;
+        wy = w.y;
+        wz = w.z;
+      }
+      for (int oz = -1; oz <= 1; oz++) {
+        int cz, Wz;
+        wrap_cell(hz + oz, nc2, cz, Wz);
+        for (int oy = -1; oy <= 1; oy++) {
+          int cy, Wy;
+          wrap_cell(hy + oy, nc1, cy, Wy);
+          for (int ox = -1; ox <= 1; ox++) {
+            int cx, Wx;
+            wrap_cell(hx + ox, nc0, cx, Wx);
+            int cell = R.abase + (cz * nc1 + cy) * nc0 + cx;
+            int W[3] = {Wx, Wy, Wz};
+            const float sx = (float)(Wx * R.b.L[0]), sy = (float)(Wy * R.b.L[1]), sz = (float)(Wz * R.b.L[2]);
+            // this cell's image relative to the lane's atom
+            const int s0 = Wx - q.ti[0], s1 = Wy - q.ti[1], s2 = Wz - q.ti[2];
+            const bool zero = (s0 == 0 && s1 == 0 && s2 == 0);
+            const bool far = s0 < -1 || s0 > 1 || s1 < -1 || s1 > 1 || s2 < -1 || s2 > 1;
+            const int code = far ? 0 : img_code(s0, s1, s2);
+            int beg = A.acell_start[cell], end = A.acell_start[cell + 1];
+            auto consider = [&](const float4 &pj) {
+              float ex = wx - (pj.x + sx), ey = wy - (pj.y + sy), ez = wz - (pj.z + sz);
+              const float r2 = ex * ex + ey * ey + ez * ez;
+              if (r2 > pre2) return;
+              const int j = __float_as_int(pj.w);
+              if (r2 < sure2 && !A.want_half) {
+                if (zero && j == q.i) return;
+                if (far) {
+                  atomicExch(&A.overflow[2], 1);
+                  return;
+                }
+                emit(A, q.slot, nf, A.raw_full, A.img_full, j, code | (r2 < fcut2 ? IN_CUT : 0));
+              } else {
+                try_atom(A, q, j, W, nf, nh);
+              }
+            };
+            for (int k = beg; k < end; k++) {
+              const float4 pj = A.acell_pos32[k];
+              if (active) consider(pj);
+            }
           }
         }
       }
-    }
-    if (active) {
-      A.num_full[q.slot] = nf;
-      if (A.want_half) A.num_half[q.slot] = nh;
+      if (active) {
+        A.num_full[q.slot] = nf;
+        if (A.want_half) A.num_half[q.slot] = nh;
+      }
     }
   }
 }
@@ -1225,7 +1230,7 @@ void neigh_build_async(Ctx &c, bool want_half) {
     }
     if (c.na) {
       KernelTimer t(c, "build_atoms");
-      k_build_atoms<<<c.agrid.ncell, 32, 0, c.stream>>>(A, P);
+      k_build_atoms<<<c.agrid.ncell, 32, 0, c.stream>>>(A, P, c.agrid.ncell);
     }
     if (c.na && c.ne) {
       if (split) CACB200_CUDA(cudaStreamWaitEvent(c.stream, c.items_ev, 0));
