@@ -137,6 +137,29 @@ class ClockSampler:
                 "samples": len(self.samples)}
 
 
+def max_over_ranks(value: float, dist, device=None) -> float:
+    """The largest value over the ranks (the slowest rank's time); the value
+    itself without a process group.  `device`: where the collective's tensor
+    lives (a CUDA device for NCCL, None for gloo)."""
+    if not dist:
+        return value
+    import torch
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(units_per_rank: int, steps: int, ws: int, seconds: float) -> float:
+    """Units all ranks processed (each rank runs its own replica of the same
+    size) per second of the slowest rank."""
+    return units_per_rank * steps * ws / seconds
+
+
+def rank_seed(base: int, rank: int) -> int:
+    """Seed of a rank's replica: replicas differ, the work per rank does not."""
+    return base + rank
+
+
 def dist_init():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     if ws <= 1:
@@ -331,7 +354,7 @@ def b200_arm(args, rank, local, ws, dist):
     import torch
     from cac_b200 import api, gen
 
-    seed = 2 + rank
+    seed = rank_seed(2, rank)
     s, pair = build_workload(args.workload, seed)
     units, natoms, nelements = totals(s)
     batch = isinstance(s, list)
@@ -383,12 +406,8 @@ def b200_arm(args, rank, local, ws, dist):
         if dist:
             dist.barrier()
     ms = e0.elapsed_time(e1)
-    ms_max = ms
-    if dist:
-        t = torch.tensor([ms], device=torch.device("cuda", local))
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_max = float(t.item())
-    value = units * args.steps * ws / (ms_max / 1000.0)
+    ms_max = max_over_ranks(ms, dist, torch.device("cuda", local))
+    value = whole_job_rate(units, args.steps, ws, ms_max / 1000.0)
 
     # per-kernel device times (CUDA events around every launch) for the roofline
     nprof = min(seg, 50)
@@ -447,12 +466,8 @@ def b200_arm(args, rank, local, ws, dist):
         eng._check(eng.lib.cacb200_set_state(eng.h, _p(x_h), _p(v_h), _p(nx_h), _p(nv_h)), "set_state")
         eng.run_nve(1, 0.001)
         eng._check(eng.lib.cacb200_get_state(eng.h, _p(x_h), _p(v_h), _p(nx_h), _p(nv_h)), "get_state")
-    e2e_s = time.perf_counter() - t0
-    if dist:
-        t = torch.tensor([e2e_s], device=torch.device("cuda", local))
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
-    e2e_value = units * k_e2e * ws / e2e_s
+    e2e_s = max_over_ranks(time.perf_counter() - t0, dist, torch.device("cuda", local))
+    e2e_value = whole_job_rate(units, k_e2e, ws, e2e_s)
     bytes_state = 8 * (6 * natoms + 48 * nelements)
 
     # CPU baseline: the reference on a bounded sample of the same workload
