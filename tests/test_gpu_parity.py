@@ -179,3 +179,27 @@ def test_errors_are_reported_not_fatal(tmp_path):
     e.neighbor(SKIN, 10)
     e.compute()                   # context still usable
     e.close()
+
+
+def test_size_limits_refused_before_any_work():
+    """List entries address sites with 26 bits: a system whose atoms and Gauss
+    points reach 2^26, or whose lattice-site ids reach 2^30, is refused with
+    EINVAL (checked before any array is read, so none is passed here); the
+    context stays usable."""
+    import ctypes as C
+    import numpy as np
+    from cac_b200.api import Engine
+    e = Engine(0)
+    lo = np.zeros(3)
+    hi = np.full(3, 100.0)
+    dp = C.POINTER(C.c_double)
+    for na, ne in [(1 << 26, 0), (0, (1 << 23)), ((1 << 26) - 8, 1), (0, (1 << 30) // 729 + 1)]:
+        rc = e.lib.cacb200_upload_system(e.h, lo.ctypes.data_as(dp), hi.ctypes.data_as(dp), na, None, None,
+                                         ne, None, None, 1.0)
+        assert rc == -1, (na, ne, rc)
+        assert b"too large" in e.lib.cacb200_last_error(e.h)
+    e.upload(gen.tiny())
+    e.pair_lj(*LJ)
+    e.neighbor(SKIN, 10)
+    e.compute()
+    e.close()
