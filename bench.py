@@ -654,7 +654,7 @@ def main():
     ap.add_argument("--form", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--jobs", type=int, default=64, help="serve workload: jobs in the stream")
-    ap.add_argument("--workers", type=int, default=16, help="serve workload: worker contexts")
+    ap.add_argument("--workers", type=int, default=8, help="serve workload: worker contexts")
     ap.add_argument("--serial-jobs", type=int, default=8,
                     help="serve workload: jobs of the stream timed one at a time in FP64")
     ap.add_argument("--pair", default="lj", choices=["lj", "eam"], help="serve workload: pair style")
