@@ -443,6 +443,7 @@ def b200_arm(args, rank, local, ws, dist):
                 "unit": "TFLOP/s", "frac": got_tf / peak_tf,
                 "peak_kind": "measured here: cuBLAS " + ("DGEMM" if fp64 else "SGEMM, TF32 off"),
                 "flops_per_site": alg_flops_per_site(dom[0])}
+    tuned = eng.pair_blocks()
     eng.restore()
     eng.setup()
 
@@ -518,6 +519,7 @@ def b200_arm(args, rank, local, ws, dist):
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": bytes_state,
                     "d2h_bytes_per_step": bytes_state, "steps": k_e2e},
             "gpu_launches": int(round(launches_per_step * args.steps)),
+            "tuned_blocks": dict(zip(("rho", "force"), tuned)),
             "clocks": clk.summary(),
         }
         print(json.dumps(line))

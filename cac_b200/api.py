@@ -68,6 +68,7 @@ SIGNATURES = [
     ("cacb200_server_last_error", C.c_char_p, [C.c_void_p]),
     ("cacb200_server_destroy", C.c_int, [C.c_void_p]),
     ("cacb200_graph_launches", C.c_int, [C.c_void_p, C.POINTER(C.c_longlong)]),
+    ("cacb200_pair_blocks", C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     ("cacb200_set_state", C.c_int, [C.c_void_p, _dp, _dp, _dp, _dp]),
     ("cacb200_get_state", C.c_int, [C.c_void_p, _dp, _dp, _dp, _dp]),
     ("cacb200_get_forces", C.c_int, [C.c_void_p, _dp, _dp, _dp]),
@@ -227,6 +228,12 @@ class Engine:
 
     def graphs(self, enable: bool) -> None:
         self._check(self.lib.cacb200_set_graphs(self.h, 1 if enable else 0), "set_graphs")
+
+    def pair_blocks(self):
+        """(rho, force) block sizes the context chose for its force-only EAM passes."""
+        r, f = C.c_int(), C.c_int()
+        self._check(self.lib.cacb200_pair_blocks(self.h, C.byref(r), C.byref(f)), "pair_blocks")
+        return r.value, f.value
 
     def graph_launches(self) -> int:
         n = C.c_longlong()

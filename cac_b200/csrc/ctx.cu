@@ -586,6 +586,14 @@ int cacb200_set_graphs(cacb200_ctx *ctx, int enable) {
   API_END
 }
 
+int cacb200_pair_blocks(cacb200_ctx *ctx, int *rho_threads, int *force_threads) {
+  API_BEGIN
+  const bool mixed = c.precision == CACB200_MIXED;
+  if (rho_threads) *rho_threads = mixed ? c.tb_rho32 : c.tb_rho;
+  if (force_threads) *force_threads = mixed ? c.tb_force32 : c.tb_force;
+  API_END
+}
+
 int cacb200_graph_launches(cacb200_ctx *ctx, long long *count) {
   API_BEGIN
   if (count) *count = c.graph_launches;

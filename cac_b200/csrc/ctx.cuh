@@ -263,6 +263,10 @@ struct Ctx {
   double graph_dt = 0.0;
   int graph_every = 0;
   long graph_launches = 0;
+  // block sizes of the force-only pair passes, chosen by timing (valid for
+  // tune_gen == gen); FP64 and mixed forms
+  long tune_gen = -1, tune_gen32 = -1;
+  int tb_rho = 128, tb_force = 128, tb_rho32 = 128, tb_force32 = 128;
   double escale_node_last = 0.0;   // node energy scale of the last evaluation
   DBuf<int> rep_meta;              // [4][nrep] aoff, na, eoff, ne (per-replica energy)
   DBuf<double> rep_energy;         // [nrep]

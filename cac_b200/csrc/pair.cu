@@ -232,9 +232,9 @@ __device__ __forceinline__ double eam_fp(const EamTables &T, double rho, double 
 // pass 1: density at atoms and node Gauss points (pair_eam.cpp:707-812), then
 // F' at the site itself into xs[i].w (pair_eam.cpp:819-833 for atoms; for a
 // node the reference's rhoi = noderho at :901-903).
-template <bool MANY>
-__global__ void __launch_bounds__(128, 8) k_eam_rho(PairArgs A, EamTables T, double *rho_out,
-                                                 double *phi_site) {
+template <int TB, bool MANY>
+__global__ void __launch_bounds__(TB, 1024 / TB) k_eam_rho(PairArgs A, EamTables T, double *rho_out,
+                                                       double *phi_site) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;   // list slot
   if (t >= A.nsi) return;
   const int i = site_of_slot(A, t);                       // site-table index
@@ -285,8 +285,9 @@ __global__ void k_eam_site_fp(double4 *xs, const int *act_gid, const int *nact_d
 }
 
 // pass 2: forces (pair_eam.cpp:845-1028)
-template <bool EV, bool MANY>
-__global__ void __launch_bounds__(128, EV ? 4 : 6) k_eam_force(PairArgs A, EamTables T, const double *phi_site) {
+template <int TB, bool EV, bool MANY>
+__global__ void __launch_bounds__(TB, (EV ? 512 : 768) / TB) k_eam_force(PairArgs A, EamTables T,
+                                                                       const double *phi_site) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;   // list slot
   const bool valid = t < A.nsi;
   const int i = valid ? site_of_slot(A, t) : 0;           // site-table index
@@ -421,6 +422,51 @@ void eam_tables(Ctx &c, const double *frho, const double *rhor, const double *z2
   stream_copy(c, c.rz.p, rz.data(), sizeof(double4) * rz.size(), cudaMemcpyHostToDevice);
 }
 
+// Block size of the force-only pair passes, chosen per context by timing 64,
+// 128 and 256 threads (best of three launches each; 128 unless another is at
+// least 3 % faster) on the context's own lists the first time they run
+// (every thread owns one list slot, so results do not depend on the choice;
+// the passes are idempotent, so the trial launches change nothing).  Not
+// during stream capture: there the default stays.
+template <bool MANY>
+void launch_rho(int tb, int nsi, cudaStream_t st, const PairArgs &A, const EamTables &T, double *rho, double *phi) {
+  if (tb == 64) k_eam_rho<64, MANY><<<std::max(nblk(nsi, 64), 1), 64, 0, st>>>(A, T, rho, phi);
+  else if (tb == 256) k_eam_rho<256, MANY><<<std::max(nblk(nsi, 256), 1), 256, 0, st>>>(A, T, rho, phi);
+  else k_eam_rho<128, MANY><<<std::max(nblk(nsi, 128), 1), 128, 0, st>>>(A, T, rho, phi);
+}
+template <bool MANY>
+void launch_force(int tb, int nsi, cudaStream_t st, const PairArgs &A, const EamTables &T, const double *phi) {
+  if (tb == 64) k_eam_force<64, false, MANY><<<std::max(nblk(nsi, 64), 1), 64, 0, st>>>(A, T, phi);
+  else if (tb == 256) k_eam_force<256, false, MANY><<<std::max(nblk(nsi, 256), 1), 256, 0, st>>>(A, T, phi);
+  else k_eam_force<128, false, MANY><<<std::max(nblk(nsi, 128), 1), 128, 0, st>>>(A, T, phi);
+}
+
+template <class F>
+float time_launch(cudaStream_t st, F &&launch) {
+  cudaEvent_t a, b;
+  CACB200_CUDA(cudaEventCreate(&a));
+  CACB200_CUDA(cudaEventCreate(&b));
+  float best = 1e30f;
+  for (int rep = 0; rep < 3; rep++) {
+    CACB200_CUDA(cudaEventRecord(a, st));
+    launch();
+    CACB200_CUDA(cudaEventRecord(b, st));
+    CACB200_CUDA(cudaEventSynchronize(b));
+    float ms = 0.f;
+    CACB200_CUDA(cudaEventElapsedTime(&ms, a, b));
+    best = std::min(best, ms);
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  return best;
+}
+
+bool capturing(cudaStream_t st) {
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  CACB200_CUDA(cudaStreamIsCapturing(st, &cs));
+  return cs != cudaStreamCaptureStatusNone;
+}
+
 void pair_compute(Ctx &c, int eflag, int vflag) {
   c.check_system();
   if (!c.lists_valid) throw Error(CACB200_ESTATE, "neighbour lists not built");
@@ -491,24 +537,52 @@ void pair_compute(Ctx &c, int eflag, int vflag) {
     Tb.nrho = c.pp.nrho;
     c.rho.reserve(std::max(c.na + 8 * c.ne, 1));
     c.phi_site.reserve(std::max(nsi, 1));
+    const bool many = c.nrep > 1;
+    auto site_fp = [&] {
+      if (c.ne)
+        k_eam_site_fp<<<stride_grid((long)c.ne * NU, 256), 256, 0, c.stream>>>(
+            c.xss.p, c.act_gid.p, c.dev_nact.p, c.na + NG * c.ne, c.na, c.rho.p, Tb);
+    };
+    auto rho = [&](int tb) {
+      if (many) launch_rho<true>(tb, nsi, c.stream, A, Tb, c.rho.p, c.phi_site.p);
+      else launch_rho<false>(tb, nsi, c.stream, A, Tb, c.rho.p, c.phi_site.p);
+    };
+    auto force = [&](int tb) {
+      if (many) launch_force<true>(tb, nsi, c.stream, A, Tb, c.phi_site.p);
+      else launch_force<false>(tb, nsi, c.stream, A, Tb, c.phi_site.p);
+    };
+    if (c.tune_gen != c.gen && !eflag && !vflag && !capturing(c.stream)) {
+      // another size replaces 128 only when it is at least 3 % faster
+      const int cand[3] = {128, 64, 256};
+      float best = 1e30f;
+      for (int tb : cand) {
+        float ms = time_launch(c.stream, [&] { rho(tb); });
+        if (tb == 128 || ms < 0.97f * best) best = ms, c.tb_rho = tb;
+      }
+      rho(c.tb_rho);
+      site_fp();
+      best = 1e30f;
+      for (int tb : cand) {
+        float ms = time_launch(c.stream, [&] { force(tb); });
+        if (tb == 128 || ms < 0.97f * best) best = ms, c.tb_force = tb;
+      }
+      c.tune_gen = c.gen;
+    }
     {
       KernelTimer t(c, "eam_rho");
-      if (c.nrep > 1) k_eam_rho<true><<<nb, T, 0, c.stream>>>(A, Tb, c.rho.p, c.phi_site.p);
-      else k_eam_rho<false><<<nb, T, 0, c.stream>>>(A, Tb, c.rho.p, c.phi_site.p);
+      rho(c.tb_rho);
     }
-    if (c.ne) {
+    {
       KernelTimer t(c, "eam_site_fp");
-      k_eam_site_fp<<<stride_grid((long)c.ne * NU, 256), 256, 0, c.stream>>>(
-          c.xss.p, c.act_gid.p, c.dev_nact.p, c.na + NG * c.ne, c.na, c.rho.p, Tb);
+      site_fp();
     }
     {
       KernelTimer t(c, "eam_force");
-      if (c.nrep > 1) {
-        if (eflag || vflag) k_eam_force<true, true><<<nb, T, 0, c.stream>>>(A, Tb, c.phi_site.p);
-        else k_eam_force<false, true><<<nb, T, 0, c.stream>>>(A, Tb, c.phi_site.p);
+      if (eflag || vflag) {
+        if (many) k_eam_force<128, true, true><<<nb, T, 0, c.stream>>>(A, Tb, c.phi_site.p);
+        else k_eam_force<128, true, false><<<nb, T, 0, c.stream>>>(A, Tb, c.phi_site.p);
       } else {
-        if (eflag || vflag) k_eam_force<true, false><<<nb, T, 0, c.stream>>>(A, Tb, c.phi_site.p);
-        else k_eam_force<false, false><<<nb, T, 0, c.stream>>>(A, Tb, c.phi_site.p);
+        force(c.tb_force);
       }
     }
   } else {

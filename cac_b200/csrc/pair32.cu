@@ -276,7 +276,8 @@ __device__ __forceinline__ float fp32_of(const Eam32 &T, float rho, float *phi) 
   return fp;
 }
 
-__global__ void __launch_bounds__(128, 8) k_eam_rho32(Args32 A, Eam32 T, double *rho_out, double *phi_site,
+template <int TB>
+__global__ void __launch_bounds__(TB, 1024 / TB) k_eam_rho32(Args32 A, Eam32 T, double *rho_out, double *phi_site,
                                                       int4 *pos_w) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;   // list slot
   if (t >= A.nsi) return;
@@ -322,8 +323,9 @@ __global__ void k_eam_site_fp32(int4 *pos, const int *act_gid, const int *nact_d
   }
 }
 
-template <bool EV>
-__global__ void __launch_bounds__(128, EV ? 4 : 8) k_eam_force32(Args32 A, Eam32 T, const double *phi_site) {
+template <int TB, bool EV>
+__global__ void __launch_bounds__(TB, (EV ? 512 : 1024) / TB) k_eam_force32(Args32 A, Eam32 T,
+                                                                          const double *phi_site) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;   // list slot
   const bool valid = t < A.nsi;
   const int i = valid ? site_of_slot(A, t) : 0;           // site-table index
@@ -489,19 +491,71 @@ void pair_compute_mixed(Ctx &c, int eflag, int vflag) {
     Tb.nrho = c.pp.nrho;
     c.rho.reserve(std::max(c.na + 8 * c.ne, 1));
     c.phi_site.reserve(std::max(nsi, 1));
+    auto rho = [&](int tb) {
+      if (tb == 64) k_eam_rho32<64><<<std::max(nblk(nsi, 64), 1), 64, 0, c.stream>>>(A, Tb, c.rho.p, c.phi_site.p, c.pos32.p);
+      else if (tb == 256) k_eam_rho32<256><<<std::max(nblk(nsi, 256), 1), 256, 0, c.stream>>>(A, Tb, c.rho.p, c.phi_site.p, c.pos32.p);
+      else k_eam_rho32<128><<<nb, 128, 0, c.stream>>>(A, Tb, c.rho.p, c.phi_site.p, c.pos32.p);
+    };
+    auto site_fp = [&] {
+      if (c.ne)
+        k_eam_site_fp32<<<stride_grid((long)c.ne * NU, 256), 256, 0, c.stream>>>(
+            c.pos32.p, c.act_gid.p, c.dev_nact.p, c.na + NG * c.ne, c.na, c.rho.p, Tb);
+    };
+    auto force = [&](int tb) {
+      if (tb == 64) k_eam_force32<64, false><<<std::max(nblk(nsi, 64), 1), 64, 0, c.stream>>>(A, Tb, c.phi_site.p);
+      else if (tb == 256) k_eam_force32<256, false><<<std::max(nblk(nsi, 256), 1), 256, 0, c.stream>>>(A, Tb, c.phi_site.p);
+      else k_eam_force32<128, false><<<nb, 128, 0, c.stream>>>(A, Tb, c.phi_site.p);
+    };
+    // block sizes of the force-only passes chosen by timing on first use (as
+    // in the FP64 form; results do not depend on them)
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    CACB200_CUDA(cudaStreamIsCapturing(c.stream, &cs));
+    if (c.tune_gen32 != c.gen && !ev && cs == cudaStreamCaptureStatusNone) {
+      const int cand[3] = {128, 64, 256};   // another size replaces 128 only when >= 3 % faster
+      cudaEvent_t e0, e1;
+      CACB200_CUDA(cudaEventCreate(&e0));
+      CACB200_CUDA(cudaEventCreate(&e1));
+      auto timed = [&](auto &&launch) {
+        float best = 1e30f;
+        for (int rep = 0; rep < 3; rep++) {
+          CACB200_CUDA(cudaEventRecord(e0, c.stream));
+          launch();
+          CACB200_CUDA(cudaEventRecord(e1, c.stream));
+          CACB200_CUDA(cudaEventSynchronize(e1));
+          float ms = 0.f;
+          CACB200_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+          best = std::min(best, ms);
+        }
+        return best;
+      };
+      float best = 1e30f;
+      for (int tb : cand) {
+        float ms = timed([&] { rho(tb); });
+        if (tb == 128 || ms < 0.97f * best) best = ms, c.tb_rho32 = tb;
+      }
+      rho(c.tb_rho32);
+      site_fp();
+      best = 1e30f;
+      for (int tb : cand) {
+        float ms = timed([&] { force(tb); });
+        if (tb == 128 || ms < 0.97f * best) best = ms, c.tb_force32 = tb;
+      }
+      cudaEventDestroy(e0);
+      cudaEventDestroy(e1);
+      c.tune_gen32 = c.gen;
+    }
     {
       KernelTimer t(c, "eam_rho32");
-      k_eam_rho32<<<nb, T, 0, c.stream>>>(A, Tb, c.rho.p, c.phi_site.p, c.pos32.p);
+      rho(c.tb_rho32);
     }
     if (c.ne) {
       KernelTimer t(c, "eam_site_fp32");
-      k_eam_site_fp32<<<stride_grid((long)c.ne * NU, 256), 256, 0, c.stream>>>(
-          c.pos32.p, c.act_gid.p, c.dev_nact.p, c.na + NG * c.ne, c.na, c.rho.p, Tb);
+      site_fp();
     }
     {
       KernelTimer t(c, "eam_force32");
-      if (ev) k_eam_force32<true><<<nb, T, 0, c.stream>>>(A, Tb, c.phi_site.p);
-      else k_eam_force32<false><<<nb, T, 0, c.stream>>>(A, Tb, c.phi_site.p);
+      if (ev) k_eam_force32<128, true><<<nb, T, 0, c.stream>>>(A, Tb, c.phi_site.p);
+      else force(c.tb_force32);
     }
   }
   if (ev) {

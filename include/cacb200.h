@@ -215,6 +215,11 @@ int cacb200_replica_energy_noalloc(int device, const double *eatom, const double
 int cacb200_set_graphs(cacb200_ctx *ctx, int enable);
 /* graph launches made so far by this context */
 int cacb200_graph_launches(cacb200_ctx *ctx, long long *count);
+/* Block sizes (threads) of the force-only EAM passes of the current precision
+ * form: chosen per context by timing 64, 128 and 256 threads on the
+ * context's own lists the first time they run (results do not depend on the
+ * choice); 128 before that.  No reference counterpart. */
+int cacb200_pair_blocks(cacb200_ctx *ctx, int *rho_threads, int *force_threads);
 
 /* Kernel timing: when enabled, every launch is bracketed by CUDA events and
  * per-kernel totals accumulate (ms, launches) until reset. */
