@@ -45,6 +45,13 @@ SIGNATURES = [
     ("cacb200_stream", C.c_void_p, [C.c_void_p]),
     ("cacb200_set_precision", C.c_int, [C.c_void_p, C.c_int]),
     ("cacb200_upload_system", C.c_int, [C.c_void_p, _dp, _dp, C.c_int, _dp, _dp, C.c_int, _dp, _dp, C.c_double]),
+    ("cacb200_get_box", C.c_int, [C.c_void_p, _dp, _dp, _dp]),
+    ("cacb200_data_last_error", C.c_char_p, []),
+    ("cacb200_data_counts", C.c_int, [C.c_char_p, C.POINTER(C.c_int), C.POINTER(C.c_int), _dp, _dp, _dp]),
+    ("cacb200_data_read", C.c_int, [C.c_char_p, _dp, _dp, _dp, _dp]),
+    ("cacb200_data_write", C.c_int, [C.c_char_p, C.c_int, C.c_int, _dp, _dp, C.c_double, _dp, _dp, _dp, _dp]),
+    ("cacb200_read_data", C.c_int, [C.c_void_p, C.c_char_p]),
+    ("cacb200_write_data", C.c_int, [C.c_void_p, C.c_char_p]),
     ("cacb200_upload_batch", C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int), _dp, _dp,
                                        _dp, _dp, _dp, _dp, C.c_double]),
     ("cacb200_replica_energy", C.c_int, [C.c_void_p, _dp]),
@@ -239,6 +246,18 @@ class Engine:
         n = C.c_longlong()
         self._check(self.lib.cacb200_graph_launches(self.h, C.byref(n)), "graph_launches")
         return n.value
+
+    def read_data(self, path: str) -> None:
+        """Upload a data file in the reference's format (read_data)."""
+        na, ne = C.c_int(), C.c_int()
+        self._check(self.lib.cacb200_read_data(self.h, path.encode()), "read_data")
+        self._check(self.lib.cacb200_counts(self.h, C.byref(na), C.byref(ne), None), "counts")
+        self.na, self.ne = na.value, ne.value
+        self.rep_na, self.rep_ne = np.array([self.na]), np.array([self.ne])
+
+    def write_data(self, path: str) -> None:
+        """Write the current state as a data file in the reference's format."""
+        self._check(self.lib.cacb200_write_data(self.h, path.encode()), "write_data")
 
     def set_precision(self, form: int) -> None:
         self._check(self.lib.cacb200_set_precision(self.h, form), "set_precision")
@@ -476,3 +495,35 @@ class Server:
             self.close()
         except Exception:
             pass
+
+
+def _data_check(lib, rc: int, what: str):
+    if rc != 0:
+        msg = lib.cacb200_data_last_error()
+        raise CacB200Error(f"{what} failed ({rc}): {msg.decode() if msg else ''}")
+
+
+def read_data_file(path: str):
+    """Host-only read of a data file in the reference's format: a ``gen.System``
+    with the file's box, mass and state (tags in file order)."""
+    from cac_b200 import gen
+    lib = load()
+    na, ne = C.c_int(), C.c_int()
+    lo, hi, m = np.zeros(3), np.zeros(3), np.zeros(1)
+    _data_check(lib, lib.cacb200_data_counts(path.encode(), C.byref(na), C.byref(ne), _p(lo), _p(hi), _p(m)),
+                "data_counts")
+    x, v = np.zeros((na.value, 3)), np.zeros((na.value, 3))
+    nx, nv = np.zeros((ne.value, 8, 3)), np.zeros((ne.value, 8, 3))
+    _data_check(lib, lib.cacb200_data_read(path.encode(), _p(x), _p(v), _p(nx), _p(nv)), "data_read")
+    return gen.System(boxlo=lo, boxhi=hi, x=x, v=v, nodex=nx, nodev=nv, mass=float(m[0]), lattice_a=0.0, meta={})
+
+
+def write_data_file(path: str, system) -> None:
+    """Host-only write of ``system`` in the reference's data-file format."""
+    lib = load()
+    arr = lambda a, shape: np.ascontiguousarray(np.asarray(a, dtype=np.float64).reshape(shape))
+    x, v = arr(system.x, (-1, 3)), arr(system.v, (-1, 3))
+    nx, nv = arr(system.nodex, (-1, 8, 3)), arr(system.nodev, (-1, 8, 3))
+    lo, hi = arr(system.boxlo, (3,)), arr(system.boxhi, (3,))
+    _data_check(lib, lib.cacb200_data_write(path.encode(), x.shape[0], nx.shape[0], _p(lo), _p(hi),
+                                            float(system.mass), _p(x), _p(v), _p(nx), _p(nv)), "data_write")

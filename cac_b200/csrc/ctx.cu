@@ -644,6 +644,18 @@ int cacb200_get_energy(cacb200_ctx *ctx, double *energy, double virial[6], doubl
   API_END
 }
 
+int cacb200_get_box(cacb200_ctx *ctx, double boxlo[3], double boxhi[3], double *mass) {
+  API_BEGIN
+  c.check_system();
+  if (c.nrep != 1) throw Error(CACB200_ESTATE, "a batch has one box per replica");
+  for (int d = 0; d < 3; d++) {
+    if (boxlo) boxlo[d] = c.boxlo[d];
+    if (boxhi) boxhi[d] = c.boxhi[d];
+  }
+  if (mass) *mass = c.mass;
+  API_END
+}
+
 int cacb200_counts(cacb200_ctx *ctx, int *natoms, int *nelements, int *nactive_sites) {
   API_BEGIN
   if (natoms) *natoms = c.na;

@@ -92,6 +92,31 @@ int cacb200_upload_batch(cacb200_ctx *ctx, int nreplicas, const int *natoms,
  * (Pair::ev_tally, pair.cpp:428-482). */
 int cacb200_replica_energy(cacb200_ctx *ctx, double *energy /* [nreplicas] */);
 
+/* Box and mass of a single system (not a batch). */
+int cacb200_get_box(cacb200_ctx *ctx, double boxlo[3], double boxhi[3], double *mass);
+
+/* ------------------------------------------------------------- data files */
+
+/* The reference's data-file format (ReadData::command, read_data.cpp:339-367,
+ * and the element data parsers, element_vec_cac.cpp:300-470; written as by
+ * write_data, element_vec_cac.cpp:1177-1300), restricted to the force path's
+ * systems: one atom type, one Hex element type with one atom per cell, 9x9x9
+ * lattice sites and 2x2x2 integration points; sections Masses, Element
+ * Types, Atoms, Velocities, Elements, Nodes, Node Velocities.  Host-only
+ * functions (no device needed) parse and write; cacb200_read_data uploads a
+ * file into a context, cacb200_write_data writes a context's state.  Errors
+ * return CACB200_EINVAL with the message in cacb200_data_last_error() (a
+ * context's own calls report through cacb200_last_error). */
+const char *cacb200_data_last_error(void);
+int cacb200_data_counts(const char *path, int *natoms, int *nelements, double boxlo[3],
+                        double boxhi[3], double *mass);
+int cacb200_data_read(const char *path, double *x, double *v, double *nodex, double *nodev);
+int cacb200_data_write(const char *path, int natoms, int nelements, const double boxlo[3],
+                       const double boxhi[3], double mass, const double *x, const double *v,
+                       const double *nodex, const double *nodev);
+int cacb200_read_data(cacb200_ctx *ctx, const char *path);
+int cacb200_write_data(cacb200_ctx *ctx, const char *path);
+
 /* Overwrite positions/velocities of the current system (same counts; NULL
  * leaves an array unchanged).  Neighbour lists are kept, as the reference
  * keeps them between rebuilds; call cacb200_build_lists after moves larger
