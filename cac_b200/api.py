@@ -55,6 +55,7 @@ SIGNATURES = [
     ("cacb200_upload_batch", C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int), _dp, _dp,
                                        _dp, _dp, _dp, _dp, C.c_double]),
     ("cacb200_replica_energy", C.c_int, [C.c_void_p, _dp]),
+    ("cacb200_thermo", C.c_int, [C.c_void_p, C.c_int, _dp]),
     ("cacb200_set_graphs", C.c_int, [C.c_void_p, C.c_int]),
     ("cacb200_replica_energy_noalloc", C.c_int, [C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.POINTER(C.c_int),
                                                  C.POINTER(C.c_int), C.c_double, _dp, C.c_void_p]),
@@ -232,6 +233,24 @@ class Engine:
         out = np.zeros(n)
         self._check(self.lib.cacb200_replica_energy(self.h, _p(out)), "replica_energy")
         return out
+
+    THERMO_FIELDS = ("temp", "ke", "pe", "etotal", "press", "pxx", "pyy", "pzz", "pxy", "pxz", "pyz", "vol")
+
+    def thermo(self, units: str = "metal"):
+        """Thermo read-out reduced on the device (``thermo_style custom temp ke
+        pe etotal press pxx pyy pzz pxy pxz pyz vol``, norm no): a dict of
+        floats for one system (or a batch of one), of arrays (one entry per
+        replica) for a batch.  ``units`` is ``metal`` (bar) or ``metalgpa`` (GPa).  Energies
+        and pressures not tallied at the current step read NaN."""
+        u = {"metal": 0, "metalgpa": 1}.get(units)
+        if u is None:
+            raise ValueError(f"unknown unit style {units!r}")
+        n = len(getattr(self, "rep_na", [0]))
+        out = np.zeros((n, len(self.THERMO_FIELDS)))
+        self._check(self.lib.cacb200_thermo(self.h, u, _p(out)), "thermo")
+        if n == 1:
+            return {k: float(out[0, i]) for i, k in enumerate(self.THERMO_FIELDS)}
+        return {k: out[:, i].copy() for i, k in enumerate(self.THERMO_FIELDS)}
 
     def graphs(self, enable: bool) -> None:
         self._check(self.lib.cacb200_set_graphs(self.h, 1 if enable else 0), "set_graphs")

@@ -102,6 +102,10 @@ namespace {
 // A system of nrep independent replicas stored one after another (a single
 // system is nrep = 1).  Each replica has its own periodic box; atoms and
 // elements keep the order of the input arrays.
+// Energies and virials tallied before the positions changed no longer
+// describe the system.
+void forget_tallies(Ctx &c) { c.tally_step_e = c.tally_step_v = c.tally_step_ae = c.tally_step_av = -1; }
+
 void upload_system(Ctx &c, int nrep, const int *rna, const int *rne, const double *lo, const double *hi,
                    const double *x, const double *v, const double *nodex, const double *nodev, double mass) {
   if (nrep < 1 || !rna || !rne || !lo || !hi) throw Error(CACB200_EINVAL, "invalid replica description");
@@ -154,6 +158,7 @@ void upload_system(Ctx &c, int nrep, const int *rna, const int *rne, const doubl
   c.planned = false;
   c.gen++;
   c.step = c.last_build_step = 0;
+  forget_tallies(c);
   // site table at full capacity (kept across uploads while large enough): atoms, Gauss points and every lattice site
   size_t ns = (size_t)na + NG * (size_t)ne + (size_t)ne * NU;
   c.xs.reserve(ns);
@@ -250,6 +255,7 @@ void set_state(Ctx &c, const double *x, const double *v, const double *nodex, co
   if (nodev && c.ne)
     CACB200_CUDA(cudaMemcpyAsync(c.nodev.p, nodev, sizeof(double) * 24 * c.ne, cudaMemcpyHostToDevice, c.stream));
   CACB200_CUDA(cudaStreamSynchronize(c.stream));
+  if ((x && c.na) || (nodex && c.ne)) forget_tallies(c);
 }
 
 void get_state(Ctx &c, double *x, double *v, double *nodex, double *nodev) {
@@ -296,6 +302,7 @@ void restore(Ctx &c) {
   d2d(c.nodex.p, c.snap_nodex.p, sizeof(double) * 24 * c.ne);
   d2d(c.nodev.p, c.snap_nodev.p, sizeof(double) * 24 * c.ne);
   c.lists_valid = false;
+  forget_tallies(c);
 }
 
 void fetch_ev(Ctx &c) {
@@ -576,6 +583,12 @@ int cacb200_replica_energy(cacb200_ctx *ctx, double *energy) {
                                                  2.0 * c.escale_node_last, c.rep_energy.p);
   CACB200_CUDA(cudaGetLastError());
   stream_copy(c, energy, c.rep_energy.p, sizeof(double) * c.nrep, cudaMemcpyDeviceToHost);
+  API_END
+}
+
+int cacb200_thermo(cacb200_ctx *ctx, int units, double *out) {
+  API_BEGIN
+  thermo(c, units, out);
   API_END
 }
 

@@ -182,6 +182,9 @@ struct Ctx {
   double energy = 0.0, virial[6] = {0, 0, 0, 0, 0, 0};
   bool have_peratom_e = false, have_peratom_v = false;
   bool ev_pending = false;       // ev_out holds a result not yet copied to energy/virial
+  // step of the last evaluation that tallied the global energy / virial and
+  // the per-site energy / virial (-1: none since the system was set)
+  long tally_step_e = -1, tally_step_v = -1, tally_step_ae = -1, tally_step_av = -1;
   long step = 0, last_build_step = 0;
   double nodal_energy_weight = -1.0;
 
@@ -270,6 +273,11 @@ struct Ctx {
   double escale_node_last = 0.0;   // node energy scale of the last evaluation
   DBuf<int> rep_meta;              // [4][nrep] aoff, na, eoff, ne (per-replica energy)
   DBuf<double> rep_energy;         // [nrep]
+  // thermo read-outs: per-replica offsets and volumes (valid for thermo_gen == gen),
+  // block partial sums and results
+  long thermo_gen = -1;
+  DBuf<int4> thermo_meta;
+  DBuf<double> thermo_vol, thermo_part, thermo_out;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
 
   Ctx(int dev);
@@ -314,5 +322,6 @@ void eam_tables(Ctx &c, const double *frho, const double *rhor, const double *z2
 void fire_init(Ctx &c, double dt);
 void fire_step(Ctx &c);
 FireState fire_read(Ctx &c);
+void thermo(Ctx &c, int units, double *out);
 
 }  // namespace cacb200

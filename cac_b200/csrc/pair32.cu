@@ -563,6 +563,10 @@ void pair_compute_mixed(Ctx &c, int eflag, int vflag) {
     c.have_peratom_e = (eflag & CACB200_ENERGY_ATOM) != 0;
     c.have_peratom_v = (vflag & CACB200_VIRIAL_ATOM) != 0;
     c.ev_pending = true;
+    if (eflag & CACB200_ENERGY_GLOBAL) c.tally_step_e = c.step;
+    if (vflag & CACB200_VIRIAL_GLOBAL) c.tally_step_v = c.step;
+    if (eflag & CACB200_ENERGY_ATOM) c.tally_step_ae = c.step;
+    if (vflag & CACB200_VIRIAL_ATOM) c.tally_step_av = c.step;
   }
   CACB200_CUDA(cudaGetLastError());
 }

@@ -92,6 +92,35 @@ int cacb200_upload_batch(cacb200_ctx *ctx, int nreplicas, const int *natoms,
  * (Pair::ev_tally, pair.cpp:428-482). */
 int cacb200_replica_energy(cacb200_ctx *ctx, double *energy /* [nreplicas] */);
 
+/* Thermo read-out reduced on the device, CACB200_THERMO_N doubles per replica
+ * in the order below: thermo_style custom temp ke pe etotal press pxx pyy pzz
+ * pxy pxz pyz vol with thermo_modify norm no (Thermo::compute_*,
+ * thermo.cpp:1642-1936; ComputeTemp, compute_temp.cpp:74-243, CONSISTENT
+ * element mass matrix; ComputePressure, compute_pressure.cpp:140-220).
+ * Temperature, kinetic energy and volume always come from the current
+ * velocities; PotEng and TotEng need the global energy, Press and the tensor
+ * the global virial tallied at the current step (per-site energy / virial for
+ * a batch).  A quantity not tallied at this step reads NaN, where the
+ * reference stops with "Energy (Virial) was not tallied on needed timestep".
+ * units: CACB200_UNITS_METAL (pressure in bar) or CACB200_UNITS_METALGPA
+ * (GPa), the two pressure units of update.cpp:160-172. */
+#define CACB200_UNITS_METAL 0
+#define CACB200_UNITS_METALGPA 1
+#define CACB200_THERMO_TEMP 0
+#define CACB200_THERMO_KE 1
+#define CACB200_THERMO_PE 2
+#define CACB200_THERMO_ETOTAL 3
+#define CACB200_THERMO_PRESS 4
+#define CACB200_THERMO_PXX 5
+#define CACB200_THERMO_PYY 6
+#define CACB200_THERMO_PZZ 7
+#define CACB200_THERMO_PXY 8
+#define CACB200_THERMO_PXZ 9
+#define CACB200_THERMO_PYZ 10
+#define CACB200_THERMO_VOL 11
+#define CACB200_THERMO_N 12
+int cacb200_thermo(cacb200_ctx *ctx, int units, double *out /* [nreplicas][CACB200_THERMO_N] */);
+
 /* Box and mass of a single system (not a batch). */
 int cacb200_get_box(cacb200_ctx *ctx, double boxlo[3], double boxhi[3], double *mass);
 

@@ -259,6 +259,90 @@ def minimize_fire(state: OracleState, pair: str, *, lj=None, eam: Optional[Eam] 
     return code.value, it.value, e.value, fn.value
 
 
+# ------------------------------------------------------------------ thermo
+
+THERMO_FIELDS = ("temp", "ke", "pe", "etotal", "press", "pxx", "pyy", "pzz", "pxy", "pxz", "pyz", "vol")
+THERMO_COLUMNS = ("Temp", "KinEng", "PotEng", "TotEng", "Press", "Pxx", "Pyy", "Pzz", "Pxy", "Pxz", "Pyz",
+                  "Volume")
+BOLTZ, MVV2E = 8.617343e-5, 1.0364269e-4          # update.cpp:160-164 (metal)
+NKTV2P = {"metal": 1.6021765e6, "metalgpa": 1.6021765e2}   # update.cpp:166-170
+
+
+def hex_mass_matrix() -> np.ndarray:
+    """Element::define_mass_matrices, HEXAHEDRON (element.cpp:1993-2056), as
+    the listed literals: 1/27, 1/54, 1/108, 1/216 by the number of natural
+    coordinates in which two nodes differ."""
+    corner = np.array([(0, 0, 0), (1, 0, 0), (1, 1, 0), (0, 1, 0), (0, 0, 1), (1, 0, 1), (1, 1, 1), (0, 1, 1)])
+    d = (corner[:, None, :] != corner[None, :, :]).sum(-1)
+    return np.array([1.0 / 27.0, 1.0 / 54.0, 1.0 / 108.0, 1.0 / 216.0])[d]
+
+
+def thermo(v, nodev, mass, boxlo, boxhi, energy, virial, units: str = "metal", nucell: int = 729) -> dict:
+    """Thermo keywords temp ke pe etotal press pxx..pyz vol (norm no) of one
+    system, restated with Python loops in the reference's order of terms:
+    ComputeTemp::dof_compute / compute_scalar / compute_vector
+    (compute_temp.cpp:74-158, 160-243; CONSISTENT branch, apc 1), virtual
+    atoms nucell per element (group.cpp:1160-1175), ComputePressure
+    (compute_pressure.cpp:140-220), Thermo::compute_ke / compute_etotal
+    (thermo.cpp:1913-1936).  ``energy`` / ``virial`` are the pair's tallies."""
+    v = np.asarray(v, dtype=np.float64).reshape(-1, 3)
+    nodev = np.asarray(nodev, dtype=np.float64).reshape(-1, 8, 3)
+    M = hex_mass_matrix()
+    t = 0.0
+    tv = [0.0] * 6
+    for i in range(v.shape[0]):
+        vx, vy, vz = v[i]
+        t += mass * (vx * vx + vy * vy + vz * vz)
+        for q, (a, b) in enumerate(((0, 0), (1, 1), (2, 2), (0, 1), (0, 2), (1, 2))):
+            tv[q] += mass * v[i, a] * v[i, b]
+    for e in range(nodev.shape[0]):
+        nv = nodev[e]
+        s = 0.0
+        for k in range(8):
+            for l in range(8):
+                s += M[k, l] * (nv[k, 0] * nv[l, 0] + nv[k, 1] * nv[l, 1] + nv[k, 2] * nv[l, 2])
+        t += s * mass * nucell
+        massone = mass * nucell
+        for k in range(8):
+            for l in range(8):
+                for q, (a, b) in enumerate(((0, 0), (1, 1), (2, 2), (0, 1), (0, 2), (1, 2))):
+                    tv[q] += massone * M[k, l] * nv[k, a] * nv[l, b]
+    dof = 3.0 * (v.shape[0] + nucell * nodev.shape[0])
+    tfactor = MVV2E / (dof * BOLTZ) if dof > 0 else 0.0
+    temp = t * tfactor
+    ke = temp * (0.5 * dof * BOLTZ)
+    prd = np.asarray(boxhi, dtype=np.float64) - np.asarray(boxlo, dtype=np.float64)
+    vol = prd[0] * prd[1] * prd[2]
+    inv_volume = 1.0 / vol
+    nk = NKTV2P[units]
+    w = np.asarray(virial, dtype=np.float64)
+    out = {"temp": temp, "ke": ke, "pe": float(energy), "etotal": float(energy) + ke,
+           "press": (dof * BOLTZ * temp + w[0] + w[1] + w[2]) / 3.0 * inv_volume * nk, "vol": vol}
+    for q, k in enumerate(("pxx", "pyy", "pzz", "pxy", "pxz", "pyz")):
+        out[k] = (tv[q] * MVV2E + w[q]) * inv_volume * nk
+    return out
+
+
+def read_thermo(log: str, columns=THERMO_COLUMNS) -> np.ndarray:
+    """Rows of the reference's thermo output (``Step`` plus ``columns``) from
+    a run's screen log, one row per printed step."""
+    rows = []
+    lines = log.splitlines()
+    for n, line in enumerate(lines):
+        head = line.split()
+        if head[:1] != ["Step"] or tuple(head[1:]) != tuple(columns):
+            continue
+        for row in lines[n + 1:]:
+            parts = row.split()
+            if len(parts) != len(columns) + 1:
+                break
+            try:
+                rows.append([float(p) for p in parts])
+            except ValueError:
+                break
+    return np.array(rows, dtype=np.float64).reshape(-1, len(columns) + 1)
+
+
 # ------------------------------------------------------- reference read-outs
 
 def read_dump(path: str) -> dict:

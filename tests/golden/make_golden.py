@@ -9,8 +9,10 @@ Run from the repository root where the reference tree is available:
 Each fixture ``<case>.npz`` holds the reference's own read-outs:
   setup forces (atom f, nodal f, Gauss-point f), energy, virial and per-site
   energy/virial (``oracle_dump compute``); the sha256 digest and per-site
-  counts of its half and full neighbour lists (``oracle_dump_neigh``); and for
-  trajectory cases the state after N velocity-Verlet steps.
+  counts of its half and full neighbour lists (``oracle_dump_neigh``); for
+  trajectory cases the state after N velocity-Verlet steps; and its thermo
+  lines (``thermo_style custom step temp ke pe etotal press pxx pyy pzz pxy
+  pxz pyz vol``, printed with ``%.17g``) at step 0 and step N.
 EAM energies come from the executable with the patched ``compute_fp``
 (``cac_eamfix``); the unpatched reference energy is kept as ``energy_unpatched``.
 """
@@ -66,6 +68,39 @@ def run(work: str, script: str, exe: str) -> None:
     O.run_reference(work, "in.cac", exe=exe)
 
 
+THERMO = ("thermo_style custom step temp ke pe etotal press pxx pyy pzz pxy pxz pyz vol\n"
+          "thermo_modify format float %.17g\n")
+
+
+def thermo_rows(work: str, pair: str, nsteps: int, exe: str) -> dict:
+    """The reference's thermo lines (full precision) at step 0 and step
+    ``nsteps``: columns Step, then ``O.THERMO_COLUMNS``."""
+    tail = "neighbor 1.0 bin\nneigh_modify every 10 delay 0 check no\ntimestep 0.001\nfix 1 all nve\n"
+    with open(os.path.join(work, "in.cac"), "w") as f:
+        f.write(HEADER + pair_lines(pair) + tail + THERMO + f"thermo {max(nsteps, 1)}\nrun {nsteps}\n")
+    rows = O.read_thermo(O.run_reference(work, "in.cac", exe=exe))
+    if rows.shape[0] != (2 if nsteps else 1):
+        raise RuntimeError(f"unexpected thermo output: {rows.shape[0]} rows")
+    return {"thermo_rows": rows, "thermo_columns": np.array(("Step",) + O.THERMO_COLUMNS)}
+
+
+def add_thermo(name: str, system, pair: str) -> None:
+    """Add the thermo rows to an existing fixture, leaving its other arrays as they are."""
+    path = os.path.join(OUT, name + ".npz")
+    with np.load(path) as z:
+        out = {k: z[k] for k in z.files}
+    nsteps = int(out.get("nsteps", 0))
+    work = tempfile.mkdtemp(prefix="cacgold_")
+    try:
+        gen.write_data(system, os.path.join(work, "data.cac"))
+        gen.write_setfl(gen.EamParams(), os.path.join(work, "cu.setfl"))
+        out.update(thermo_rows(work, pair, nsteps, O.REF_EXE_EAMFIX if pair == "eam" else O.REF_EXE))
+    finally:
+        shutil.rmtree(work, ignore_errors=True)
+    np.savez_compressed(path, **out)
+    print(name, "thermo", out["thermo_rows"][:, :3].tolist())
+
+
 def make_case(name: str, system, pair: str, nsteps: int = 0, peratom_virial: bool = True) -> None:
     work = tempfile.mkdtemp(prefix="cacgold_")
     try:
@@ -103,6 +138,7 @@ def make_case(name: str, system, pair: str, nsteps: int = 0, peratom_virial: boo
             out["nsteps"] = np.int64(nsteps)
             for k in ("x", "v", "f", "nodex", "nodev", "nodef"):
                 out["end_" + k] = e[k]
+        out.update(thermo_rows(work, pair, nsteps, exe_e))
         meta = dict(system.meta)
         out["meta"] = np.array(repr(sorted(meta.items())))
         np.savez_compressed(os.path.join(OUT, name + ".npz"), **out)
@@ -111,12 +147,24 @@ def make_case(name: str, system, pair: str, nsteps: int = 0, peratom_virial: boo
         shutil.rmtree(work, ignore_errors=True)
 
 
+CASES = (
+    ("tiny_lj", lambda: gen.tiny(seed=7, temperature=50.0), "lj", dict(nsteps=100)),
+    ("tiny_eam", lambda: gen.tiny(seed=11, temperature=300.0), "eam", dict(nsteps=50)),
+    ("lj_small", lambda: gen.lj_small(seed=1), "lj", dict(nsteps=100, peratom_virial=False)),
+)
+
+
 def main():
+    """``make_golden.py`` writes every fixture; ``make_golden.py thermo``
+    only adds the thermo rows to the fixtures already here."""
     if not os.path.exists(O.REF_EXE):
         raise SystemExit("build the reference first: make -C oracle reference")
-    make_case("tiny_lj", gen.tiny(seed=7, temperature=50.0), "lj", nsteps=100)
-    make_case("tiny_eam", gen.tiny(seed=11, temperature=300.0), "eam", nsteps=50)
-    make_case("lj_small", gen.lj_small(seed=1), "lj", nsteps=100, peratom_virial=False)
+    thermo_only = sys.argv[1:] == ["thermo"]
+    for name, system, pair, kw in CASES:
+        if thermo_only:
+            add_thermo(name, system(), pair)
+        else:
+            make_case(name, system(), pair, **kw)
 
 
 if __name__ == "__main__":

@@ -71,3 +71,48 @@ def test_trajectory_matches_reference(case, oracle_mod, golden, tmp_path):
     assert rel_err(st.nodef, g["end_nodef"]) < 1e-10
     assert rel_err(st.v, g["end_v"]) < 1e-10
     assert rel_err(st.nodev, g["end_nodev"]) < 1e-10
+
+
+def thermo_err(got: dict, ref_row, fields) -> float:
+    """Largest error over thermo fields: energies and temperature relative to
+    their own size, pressures relative to the largest pressure component."""
+    ref = dict(zip(fields, ref_row))
+    pk = ("press", "pxx", "pyy", "pzz", "pxy", "pxz", "pyz")
+    pscale = max(abs(ref[k]) for k in pk if k in ref) if any(k in ref for k in pk) else 1.0
+    err = 0.0
+    for k, r in ref.items():
+        scale = pscale if k in pk else abs(r)
+        err = max(err, abs(got[k] - r) / scale)
+    return err
+
+
+@pytest.mark.parametrize("case", ["tiny_lj", "tiny_eam", "lj_small"])
+def test_thermo_matches_reference(case, oracle_mod, golden):
+    """The thermo restatement against the reference's own thermo lines: at
+    step 0 from the setup tallies (every field), at the last step from the
+    reference's end velocities (temperature, kinetic energy, volume)."""
+    g = golden(case)
+    build, _, _ = CASES[case]
+    s = build()
+    rows = g["thermo_rows"]
+    fields = oracle_mod.THERMO_FIELDS
+    assert tuple(g["thermo_columns"][1:]) == oracle_mod.THERMO_COLUMNS
+    t0 = oracle_mod.thermo(s.v, s.nodev, s.mass, s.boxlo, s.boxhi, g["energy"], g["virial"])
+    assert rows[0, 0] == 0
+    assert thermo_err(t0, rows[0, 1:], fields) < 1e-14
+    tn = oracle_mod.thermo(g["end_v"], g["end_nodev"], s.mass, s.boxlo, s.boxhi, 0.0, np.zeros(6))
+    assert rows[1, 0] == int(g["nsteps"])
+    keep = [fields.index(k) for k in ("temp", "ke", "vol")]
+    assert thermo_err(tn, rows[1, 1:][keep], [fields[i] for i in keep]) < 1e-12
+
+
+def test_thermo_units_and_empty(oracle_mod):
+    """metalgpa pressures are metal's divided by 1e4; a system with no sites
+    has zero temperature (ComputeTemp::dof_compute sets tfactor 0)."""
+    s = CASES["tiny_lj"][0]()
+    w = np.arange(1.0, 7.0)
+    a = oracle_mod.thermo(s.v, s.nodev, s.mass, s.boxlo, s.boxhi, -1.0, w, units="metal")
+    b = oracle_mod.thermo(s.v, s.nodev, s.mass, s.boxlo, s.boxhi, -1.0, w, units="metalgpa")
+    assert abs(a["press"] / 1e4 - b["press"]) < 1e-12 * abs(a["press"])
+    e = oracle_mod.thermo(np.zeros((0, 3)), np.zeros((0, 8, 3)), 1.0, [0, 0, 0], [1, 1, 1], 0.0, np.zeros(6))
+    assert e["temp"] == 0.0 and e["ke"] == 0.0 and e["press"] == 0.0
