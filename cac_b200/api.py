@@ -56,6 +56,8 @@ SIGNATURES = [
                                        _dp, _dp, _dp, _dp, C.c_double]),
     ("cacb200_replica_energy", C.c_int, [C.c_void_p, _dp]),
     ("cacb200_thermo", C.c_int, [C.c_void_p, C.c_int, _dp]),
+    ("cacb200_set_langevin", C.c_int, [C.c_void_p, C.c_double, C.c_double, C.c_double, C.c_int, C.c_int]),
+    ("cacb200_unset_langevin", C.c_int, [C.c_void_p]),
     ("cacb200_set_graphs", C.c_int, [C.c_void_p, C.c_int]),
     ("cacb200_replica_energy_noalloc", C.c_int, [C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.POINTER(C.c_int),
                                                  C.POINTER(C.c_int), C.c_double, _dp, C.c_void_p]),
@@ -326,6 +328,14 @@ class Engine:
 
     def setup(self) -> None:
         self._check(self.lib.cacb200_setup(self.h), "setup")
+
+    def langevin(self, t_start: float, t_stop: float, t_period: float, seed: int, zero: bool = False) -> None:
+        """``fix ID all langevin t_start t_stop t_period seed [zero yes]``, applied by run_nve."""
+        self._check(self.lib.cacb200_set_langevin(self.h, t_start, t_stop, t_period, seed, 1 if zero else 0),
+                    "set_langevin")
+
+    def unset_langevin(self) -> None:
+        self._check(self.lib.cacb200_unset_langevin(self.h), "unset_langevin")
 
     def run_nve(self, nsteps: int, dt: float = 0.001, eflag: int = 0, vflag: int = 0) -> None:
         self._check(self.lib.cacb200_run_nve(self.h, nsteps, dt, eflag, vflag), "run_nve")

@@ -159,6 +159,7 @@ void upload_system(Ctx &c, int nrep, const int *rna, const int *rne, const doubl
   c.gen++;
   c.step = c.last_build_step = 0;
   forget_tallies(c);
+  c.lgv.on = false;   // a thermostat is set for the system it acts on
   // site table at full capacity (kept across uploads while large enough): atoms, Gauss points and every lattice site
   size_t ns = (size_t)na + NG * (size_t)ne + (size_t)ne * NU;
   c.xs.reserve(ns);
@@ -372,18 +373,35 @@ void nve_cycle(Ctx &c, double dt) {
     drop_graphs(c);
     // one eager evaluation first, so that every buffer and table the force
     // path grows on first use exists before capture (it recomputes the
-    // forces of the current positions: the state does not change)
+    // forces of the current positions: the state does not change; forces
+    // that hold a thermostat's last draws are kept aside and put back)
+    const size_t n3 = 3 * (size_t)c.na, n24 = 24 * (size_t)c.ne;
+    if (c.lgv.on) {
+      c.lgv_save.reserve(n3 + n24 + 1);
+      if (n3) CACB200_CUDA(cudaMemcpyAsync(c.lgv_save.p, c.f.p, sizeof(double) * n3, cudaMemcpyDeviceToDevice, c.stream));
+      if (n24)
+        CACB200_CUDA(cudaMemcpyAsync(c.lgv_save.p + n3, c.nodef.p, sizeof(double) * n24, cudaMemcpyDeviceToDevice,
+                                     c.stream));
+    }
     forces(c, 0, 0);
+    if (c.lgv.on) {
+      if (n3) CACB200_CUDA(cudaMemcpyAsync(c.f.p, c.lgv_save.p, sizeof(double) * n3, cudaMemcpyDeviceToDevice, c.stream));
+      if (n24)
+        CACB200_CUDA(cudaMemcpyAsync(c.nodef.p, c.lgv_save.p + n3, sizeof(double) * n24, cudaMemcpyDeviceToDevice,
+                                     c.stream));
+    }
     c.g_build = capture(c, [&] {
       nve_initial(c, dt);
       neigh_build_async(c, false);
     });
     c.g_steps = capture(c, [&] {
       forces(c, 0, 0);
+      langevin_post_force(c, dt);
       nve_final(c, dt);
       for (int k = 1; k < every; k++) {
         nve_initial(c, dt);
         forces(c, 0, 0);
+        langevin_post_force(c, dt);
         nve_final(c, dt);
       }
     });
@@ -403,10 +421,12 @@ void nve_cycle(Ctx &c, double dt) {
     c.graph_launches++;
   } else {
     forces(c, 0, 0);
+    langevin_post_force(c, dt);
     nve_final(c, dt);
     for (int k = 1; k < every; k++) {
       nve_initial(c, dt);
       forces(c, 0, 0);
+      langevin_post_force(c, dt);
       nve_final(c, dt);
     }
   }
@@ -416,7 +436,16 @@ void nve_cycle(Ctx &c, double dt) {
 void run_nve(Ctx &c, int nsteps, double dt, int eflag, int vflag) {
   c.check_system();
   if (nsteps < 0) throw Error(CACB200_EINVAL, "negative step count");
-  if (!c.lists_valid) setup(c);
+  if (c.lgv.on) {
+    // Verlet::setup: forces of the current positions, then the fixes'
+    // setup, which for fix langevin is its first post_force of the run
+    if (!c.lists_valid) setup(c);
+    else forces(c, 0, 0);
+    langevin_begin(c, nsteps);
+    langevin_post_force(c, dt);
+  } else if (!c.lists_valid) {
+    setup(c);
+  }
   const bool graphs = c.graphs_enabled && c.every > 0 && !c.prof.enabled;
   const bool want_ev = eflag || vflag;
   int s = 1;
@@ -433,6 +462,7 @@ void run_nve(Ctx &c, int nsteps, double dt, int eflag, int vflag) {
     if (c.every > 0 && (c.step - c.last_build_step) % c.every == 0) build(c, false);
     bool last = (s == nsteps);
     forces(c, last ? eflag : 0, last ? vflag : 0);
+    langevin_post_force(c, dt);
     nve_final(c, dt);
     s++;
   }
@@ -589,6 +619,18 @@ int cacb200_replica_energy(cacb200_ctx *ctx, double *energy) {
 int cacb200_thermo(cacb200_ctx *ctx, int units, double *out) {
   API_BEGIN
   thermo(c, units, out);
+  API_END
+}
+
+int cacb200_set_langevin(cacb200_ctx *ctx, double t_start, double t_stop, double t_period, int seed, int zero) {
+  API_BEGIN
+  langevin_set(c, t_start, t_stop, t_period, seed, zero);
+  API_END
+}
+
+int cacb200_unset_langevin(cacb200_ctx *ctx) {
+  API_BEGIN
+  langevin_unset(c);
   API_END
 }
 

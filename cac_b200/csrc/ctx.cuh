@@ -121,6 +121,14 @@ struct FireState {
   int vdotf_neg, reset, mix, apply, status, iter;
 };
 
+// fix langevin parameters (FixLangevin, fix_langevin.cpp:40-214), CONSTANT style
+struct LangevinParams {
+  bool on = false;
+  double t_start = 0, t_stop = 0, t_period = 1;
+  int seed = 0;
+  bool zero = false;
+};
+
 struct Profile {
   bool enabled = false;
   std::vector<std::string> names;
@@ -276,6 +284,17 @@ struct Ctx {
   // thermo read-outs: per-replica offsets and volumes (valid for thermo_gen == gen),
   // block partial sums and results
   long thermo_gen = -1;
+  // fix langevin: per-replica random streams (window of the last 97 values
+  // and the 96 after it, draws made), the run's step counter, chunk layout
+  // and jump coefficients
+  LangevinParams lgv;
+  DBuf<unsigned> lgv_base, lgv_next, lgv_poly;
+  DBuf<unsigned long long> lgv_m;
+  DBuf<long long> lgv_ctl;
+  DBuf<int2> lgv_chunks, lgv_rchunk;
+  DBuf<int4> lgv_meta;
+  DBuf<double> lgv_part, lgv_mean, lgv_save;
+  int lgv_nchunks = 0, lgv_poly_n = 0;
   DBuf<int4> thermo_meta;
   DBuf<double> thermo_vol, thermo_part, thermo_out;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -323,5 +342,9 @@ void fire_init(Ctx &c, double dt);
 void fire_step(Ctx &c);
 FireState fire_read(Ctx &c);
 void thermo(Ctx &c, int units, double *out);
+void langevin_set(Ctx &c, double t_start, double t_stop, double t_period, int seed, int zero);
+void langevin_unset(Ctx &c);
+void langevin_begin(Ctx &c, long nsteps);
+void langevin_post_force(Ctx &c, double dt);
 
 }  // namespace cacb200

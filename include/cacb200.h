@@ -212,6 +212,22 @@ int cacb200_nve_final(cacb200_ctx *ctx, double dt);
 int cacb200_setup(cacb200_ctx *ctx);
 int cacb200_run_nve(cacb200_ctx *ctx, int nsteps, double dt, int eflag, int vflag);
 
+/* fix ID all langevin t_start t_stop t_period seed [zero yes]
+ * (FixLangevin, fix_langevin.cpp:40-214, 266-273, 455-694): drag plus random
+ * force on atoms and element nodes (node noise scaled by 1/sqrt(nodal
+ * weight)) after each force evaluation of cacb200_run_nve and at the start of
+ * each run (the fix's setup), target temperature ramped from t_start to t_stop
+ * over each run.  The random numbers are the reference's own RanMars stream
+ * (random_mars.cpp:23-90) for `seed`, drawn in its order, so trajectories
+ * follow the reference's; replica r of a batch uses seed + r.  The stream
+ * starts at this call and continues across runs; a new system (upload) or
+ * cacb200_unset_langevin removes the fix.  Snapshots do not rewind the
+ * stream.  Not applied during minimisation (the reference's fix has no
+ * min_post_force). */
+int cacb200_set_langevin(cacb200_ctx *ctx, double t_start, double t_stop, double t_period, int seed,
+                         int zero);
+int cacb200_unset_langevin(cacb200_ctx *ctx);
+
 /* ------------------------------------------------------------- minimise */
 
 /* min_modify for FIRE: the parameters of Min (min.h:61-72) with the

@@ -7,6 +7,7 @@ the benchmark's CPU-baseline leg import this module, and only as the checker.
 from __future__ import annotations
 
 import ctypes as C
+import math
 import os
 import subprocess
 from typing import Optional
@@ -321,6 +322,101 @@ def thermo(v, nodev, mass, boxlo, boxhi, energy, virial, units: str = "metal", n
     for q, k in enumerate(("pxx", "pyy", "pzz", "pxy", "pxz", "pyz")):
         out[k] = (tv[q] * MVV2E + w[q]) * inv_volume * nk
     return out
+
+
+# ------------------------------------------------------------------ langevin
+
+FTM2V = 1.0 / 1.0364269e-4    # update.cpp:164 (metal)
+
+
+class RanMars:
+    """The reference's uniform generator (random_mars.cpp:23-90): F. James's
+    RANMAR (Comp. Phys. Comm. 60, 329 (1990)), a lagged subtractive Fibonacci
+    sequence (lags 97 and 33) combined with an arithmetic sequence, restated
+    in integers: every value the reference handles is a multiple of 2^-24,
+    so u[] holds 24-bit integers and ``uniform`` returns integer / 2^24, the
+    same doubles exactly.  The constructor's warm-up draw is kept."""
+
+    C0, CD, CM = 362436, 7654321, 16777213
+    MASK = (1 << 24) - 1
+
+    def __init__(self, seed: int):
+        if seed <= 0 or seed > 900000000:
+            raise ValueError("Invalid seed for Marsaglia random # generator")
+        ij = (seed - 1) // 30082
+        kl = (seed - 1) - 30082 * ij
+        i = (ij // 177) % 177 + 2
+        j = ij % 177 + 2
+        k = (kl // 169) % 178 + 1
+        l = kl % 169
+        self.u = [0] * 98
+        for ii in range(1, 98):
+            s = 0
+            for jj in range(1, 25):
+                m = ((i * j) % 179) * k % 179
+                i, j, k = j, k, m
+                l = (53 * l + 1) % 169
+                if (l * m) % 64 >= 32:
+                    s += 1 << (24 - jj)
+            self.u[ii] = s
+        self.c = self.C0
+        self.i97, self.j97 = 97, 33
+        self.uniform()
+
+    def uniform_int(self) -> int:
+        uni = (self.u[self.i97] - self.u[self.j97]) & self.MASK
+        self.u[self.i97] = uni
+        self.i97 = 97 if self.i97 == 1 else self.i97 - 1
+        self.j97 = 97 if self.j97 == 1 else self.j97 - 1
+        self.c -= self.CD
+        if self.c < 0:
+            self.c += self.CM
+        return (uni - self.c) & self.MASK
+
+    def uniform(self) -> float:
+        return self.uniform_int() / 16777216.0
+
+
+def langevin_post_force(f, nodef, v, nodev, rng: RanMars, mass: float, t_target: float, t_period: float,
+                        dt: float, zero: bool, nucell: int = 729, npe: int = 8) -> None:
+    """FixLangevin::post_force on one system, in place (fix_langevin.cpp:
+    gfactors 266-273, atoms 538-612, element nodes 614-646, zero 650-672),
+    with the reference's order of draws (atoms x y z, then each element's
+    nodes x y z) and of floating-point operations.  ``count`` for ``zero``
+    is atoms + elements (group.cpp:1068-1104), as in the reference."""
+    gfactor1 = -mass / t_period / FTM2V
+    gfactor2 = math.sqrt(mass) * math.sqrt(24.0 * BOLTZ / t_period / dt / MVV2E) / FTM2V
+    gfactor1 *= 1.0 / 1.0
+    gfactor2 *= 1.0 / math.sqrt(1.0)
+    tsqrt = math.sqrt(t_target)
+    fsum = [0.0, 0.0, 0.0]
+    gamma1, gamma2 = gfactor1, gfactor2 * tsqrt
+    for i in range(f.shape[0]):
+        fran = [gamma2 * (rng.uniform() - 0.5) for _ in range(3)]
+        for d in range(3):
+            f[i, d] += gamma1 * v[i, d] + fran[d]
+            fsum[d] += fran[d]
+    gamma2 = gfactor2 * tsqrt / math.sqrt(nucell / npe)
+    for e in range(nodef.shape[0]):
+        for k in range(npe):
+            fran = [gamma2 * (rng.uniform() - 0.5) for _ in range(3)]
+            for d in range(3):
+                nodef[e, k, d] += gamma1 * nodev[e, k, d] + fran[d]
+                fsum[d] += fran[d]
+    if zero:
+        count = f.shape[0] + nodef.shape[0]
+        fs = [s / count for s in fsum]
+        for d in range(3):
+            f[:, d] -= fs[d]
+            nodef[:, :, d] -= fs[d]
+
+
+def langevin_target(t_start: float, t_stop: float, step: int, begin: int, end: int) -> float:
+    """FixLangevin::compute_target, CONSTANT style (fix_langevin.cpp:683-694)."""
+    delta = float(step - begin)
+    if delta != 0.0:
+        delta /= end - begin
+    return t_start + delta * (t_stop - t_start)
 
 
 def read_thermo(log: str, columns=THERMO_COLUMNS) -> np.ndarray:

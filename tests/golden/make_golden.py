@@ -12,7 +12,9 @@ Each fixture ``<case>.npz`` holds the reference's own read-outs:
   counts of its half and full neighbour lists (``oracle_dump_neigh``); for
   trajectory cases the state after N velocity-Verlet steps; and its thermo
   lines (``thermo_style custom step temp ke pe etotal press pxx pyy pzz pxy
-  pxz pyz vol``, printed with ``%.17g``) at step 0 and step N.
+  pxz pyz vol``, printed with ``%.17g``) at step 0 and step N; and with
+  ``fix langevin`` (the ``LANGEVIN`` cases) its setup forces and the state
+  after consecutive runs.
 EAM energies come from the executable with the patched ``compute_fp``
 (``cac_eamfix``); the unpatched reference energy is kept as ``energy_unpatched``.
 """
@@ -84,6 +86,50 @@ def thermo_rows(work: str, pair: str, nsteps: int, exe: str) -> dict:
     return {"thermo_rows": rows, "thermo_columns": np.array(("Step",) + O.THERMO_COLUMNS)}
 
 
+# fix langevin cases: t_start, t_stop, t_period, seed, zero; the run lengths
+LANGEVIN = {
+    "tiny_lj": ((50.0, 150.0, 0.05, 48279, 1), (20, 20)),
+    "tiny_eam": ((300.0, 300.0, 0.1, 9173, 0), (30,)),
+    "lj_small": ((80.0, 20.0, 0.2, 5501, 1), (15, 10)),
+}
+
+
+def langevin_rows(work: str, pair: str, exe: str, params, runs) -> dict:
+    """The reference with ``fix langevin`` after ``fix nve``: the forces of
+    its setup (``run 0``: pair forces plus the fix's first draws), and the
+    state after the given consecutive runs (each run draws again at its
+    setup and ramps the target over its own steps)."""
+    t0, t1, damp, seed, zero = params
+    tail = "neighbor 1.0 bin\nneigh_modify every 10 delay 0 check no\ntimestep 0.001\nfix 1 all nve\n"
+    fix = f"fix 2 all langevin {t0!r} {t1!r} {damp!r} {seed} zero {'yes' if zero else 'no'}\n"
+    out = {"lgv_params": np.array(params, dtype=np.float64), "lgv_runs": np.array(runs, dtype=np.int64)}
+    run(work, HEADER + pair_lines(pair) + tail + fix + "run 0\noracle_dump lgv0.txt state\n", exe)
+    d = O.read_dump(os.path.join(work, "lgv0.txt"))
+    out["lgv_setup_f"], out["lgv_setup_nodef"] = d["f"], d["nodef"]
+    script = HEADER + pair_lines(pair) + tail + fix + "".join(f"run {n}\n" for n in runs)
+    run(work, script + "oracle_dump lgv1.txt state\n", exe)
+    e = O.read_dump(os.path.join(work, "lgv1.txt"))
+    for k in ("x", "v", "f", "nodex", "nodev", "nodef"):
+        out["lgv_end_" + k] = e[k]
+    return out
+
+
+def add_langevin(name: str, system, pair: str) -> None:
+    """Add the fix langevin read-outs to an existing fixture."""
+    path = os.path.join(OUT, name + ".npz")
+    with np.load(path) as z:
+        out = {k: z[k] for k in z.files}
+    work = tempfile.mkdtemp(prefix="cacgold_")
+    try:
+        gen.write_data(system, os.path.join(work, "data.cac"))
+        gen.write_setfl(gen.EamParams(), os.path.join(work, "cu.setfl"))
+        out.update(langevin_rows(work, pair, O.REF_EXE, *LANGEVIN[name]))
+    finally:
+        shutil.rmtree(work, ignore_errors=True)
+    np.savez_compressed(path, **out)
+    print(name, "langevin", float(np.abs(out["lgv_end_v"]).max()))
+
+
 def add_thermo(name: str, system, pair: str) -> None:
     """Add the thermo rows to an existing fixture, leaving its other arrays as they are."""
     path = os.path.join(OUT, name + ".npz")
@@ -139,6 +185,7 @@ def make_case(name: str, system, pair: str, nsteps: int = 0, peratom_virial: boo
             for k in ("x", "v", "f", "nodex", "nodev", "nodef"):
                 out["end_" + k] = e[k]
         out.update(thermo_rows(work, pair, nsteps, exe_e))
+        out.update(langevin_rows(work, pair, O.REF_EXE, *LANGEVIN[name]))
         meta = dict(system.meta)
         out["meta"] = np.array(repr(sorted(meta.items())))
         np.savez_compressed(os.path.join(OUT, name + ".npz"), **out)
@@ -156,13 +203,16 @@ CASES = (
 
 def main():
     """``make_golden.py`` writes every fixture; ``make_golden.py thermo``
-    only adds the thermo rows to the fixtures already here."""
+    or ``make_golden.py langevin`` only adds those read-outs to the fixtures
+    already here."""
     if not os.path.exists(O.REF_EXE):
         raise SystemExit("build the reference first: make -C oracle reference")
-    thermo_only = sys.argv[1:] == ["thermo"]
+    only = sys.argv[1] if sys.argv[1:] else None
     for name, system, pair, kw in CASES:
-        if thermo_only:
+        if only == "thermo":
             add_thermo(name, system(), pair)
+        elif only == "langevin":
+            add_langevin(name, system(), pair)
         else:
             make_case(name, system(), pair, **kw)
 

@@ -116,3 +116,34 @@ def test_thermo_units_and_empty(oracle_mod):
     assert abs(a["press"] / 1e4 - b["press"]) < 1e-12 * abs(a["press"])
     e = oracle_mod.thermo(np.zeros((0, 3)), np.zeros((0, 8, 3)), 1.0, [0, 0, 0], [1, 1, 1], 0.0, np.zeros(6))
     assert e["temp"] == 0.0 and e["ke"] == 0.0 and e["press"] == 0.0
+
+
+@pytest.mark.parametrize("case", ["tiny_lj", "tiny_eam", "lj_small"])
+def test_langevin_setup_matches_reference(case, oracle_mod, golden):
+    """The RanMars and FixLangevin restatement against the reference's setup
+    forces with fix langevin: its pair forces plus the first draws, bit for
+    bit with zero no (the same operations in the same order), and with zero
+    yes (the mean is summed in the same sequential order)."""
+    g = golden(case)
+    s = CASES[case][0]()
+    t0, _, damp, seed, zero = g["lgv_params"]
+    f, nf = g["f"].copy(), g["nodef"].copy()
+    rng = oracle_mod.RanMars(int(seed))
+    oracle_mod.langevin_post_force(f, nf, np.asarray(s.v), np.asarray(s.nodev), rng, s.mass,
+                                   oracle_mod.langevin_target(t0, 0.0, 0, 0, 1), damp, 0.001, bool(zero))
+    assert np.array_equal(f, g["lgv_setup_f"])
+    assert np.array_equal(nf, g["lgv_setup_nodef"])
+
+
+def test_ranmars_restatement_properties(oracle_mod):
+    """RanMars values are multiples of 2^-24 in [0, 1); different seeds give
+    different streams; the reference's seed bounds are enforced."""
+    a, b = oracle_mod.RanMars(1), oracle_mod.RanMars(2)
+    xa = [a.uniform() for _ in range(1000)]
+    xb = [b.uniform() for _ in range(1000)]
+    assert all(0.0 <= x < 1.0 and x * 16777216.0 == int(x * 16777216.0) for x in xa)
+    assert xa != xb
+    assert abs(np.mean(xa) - 0.5) < 0.05
+    for bad in (0, 900000001):
+        with pytest.raises(ValueError):
+            oracle_mod.RanMars(bad)
