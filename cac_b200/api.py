@@ -58,6 +58,8 @@ SIGNATURES = [
     ("cacb200_thermo", C.c_int, [C.c_void_p, C.c_int, _dp]),
     ("cacb200_set_langevin", C.c_int, [C.c_void_p, C.c_double, C.c_double, C.c_double, C.c_int, C.c_int]),
     ("cacb200_unset_langevin", C.c_int, [C.c_void_p]),
+    ("cacb200_set_deform", C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int), _dp, _dp, C.c_int]),
+    ("cacb200_unset_deform", C.c_int, [C.c_void_p]),
     ("cacb200_set_graphs", C.c_int, [C.c_void_p, C.c_int]),
     ("cacb200_replica_energy_noalloc", C.c_int, [C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.POINTER(C.c_int),
                                                  C.POINTER(C.c_int), C.c_double, _dp, C.c_void_p]),
@@ -333,6 +335,35 @@ class Engine:
         """``fix ID all langevin t_start t_stop t_period seed [zero yes]``, applied by run_nve."""
         self._check(self.lib.cacb200_set_langevin(self.h, t_start, t_stop, t_period, seed, 1 if zero else 0),
                     "set_langevin")
+
+    DEFORM_STYLES = {"none": 0, "final": 1, "delta": 2, "scale": 3, "vel": 4, "erate": 5, "trate": 6,
+                     "wiggle": 7, "volume": 8}
+
+    def deform(self, nevery: int, remap: str = "x", **dims) -> None:
+        """``fix ID all deform N dim style args ... remap x|none units box``:
+        ``deform(1, x=("erate", 0.5), y=("volume",), z=("final", lo, hi))``."""
+        style = (C.c_int * 3)()
+        a, b = np.zeros(3), np.zeros(3)
+        for d, name in enumerate("xyz"):
+            spec = dims.pop(name, ("none",))
+            style[d] = self.DEFORM_STYLES[spec[0]]
+            args = list(spec[1:]) + [0.0, 0.0]
+            a[d], b[d] = float(args[0]), float(args[1])
+        if dims:
+            raise ValueError(f"unknown dimensions {sorted(dims)}")
+        if remap not in ("x", "none"):
+            raise ValueError("remap must be x or none")
+        self._check(self.lib.cacb200_set_deform(self.h, nevery, style, _p(a), _p(b), 1 if remap == "x" else 0),
+                    "set_deform")
+
+    def unset_deform(self) -> None:
+        self._check(self.lib.cacb200_unset_deform(self.h), "unset_deform")
+
+    def box(self):
+        """(boxlo, boxhi) of a single system."""
+        lo, hi, m = np.zeros(3), np.zeros(3), C.c_double()
+        self._check(self.lib.cacb200_get_box(self.h, _p(lo), _p(hi), C.byref(m)), "get_box")
+        return lo, hi
 
     def unset_langevin(self) -> None:
         self._check(self.lib.cacb200_unset_langevin(self.h), "unset_langevin")

@@ -159,7 +159,10 @@ void upload_system(Ctx &c, int nrep, const int *rna, const int *rne, const doubl
   c.gen++;
   c.step = c.last_build_step = 0;
   forget_tallies(c);
-  c.lgv.on = false;   // a thermostat is set for the system it acts on
+  c.forces_current = false;
+  c.lgv.on = false;   // a thermostat or deformation is set for the system it acts on
+  c.dfm.on = false;
+  c.box_replan = false;
   // site table at full capacity (kept across uploads while large enough): atoms, Gauss points and every lattice site
   size_t ns = (size_t)na + NG * (size_t)ne + (size_t)ne * NU;
   c.xs.reserve(ns);
@@ -256,7 +259,10 @@ void set_state(Ctx &c, const double *x, const double *v, const double *nodex, co
   if (nodev && c.ne)
     CACB200_CUDA(cudaMemcpyAsync(c.nodev.p, nodev, sizeof(double) * 24 * c.ne, cudaMemcpyHostToDevice, c.stream));
   CACB200_CUDA(cudaStreamSynchronize(c.stream));
-  if ((x && c.na) || (nodex && c.ne)) forget_tallies(c);
+  if ((x && c.na) || (nodex && c.ne)) {
+    forget_tallies(c);
+    c.forces_current = false;
+  }
 }
 
 void get_state(Ctx &c, double *x, double *v, double *nodex, double *nodev) {
@@ -303,6 +309,7 @@ void restore(Ctx &c) {
   d2d(c.nodex.p, c.snap_nodex.p, sizeof(double) * 24 * c.ne);
   d2d(c.nodev.p, c.snap_nodev.p, sizeof(double) * 24 * c.ne);
   c.lists_valid = false;
+  c.forces_current = false;
   forget_tallies(c);
 }
 
@@ -326,6 +333,7 @@ void forces(Ctx &c, int eflag, int vflag) {
   interpolate_sites(c);
   pair_compute(c, eflag, vflag);
   assemble_nodef(c);
+  c.forces_current = true;
 }
 
 void setup(Ctx &c) {
@@ -445,8 +453,14 @@ void run_nve(Ctx &c, int nsteps, double dt, int eflag, int vflag) {
     langevin_post_force(c, dt);
   } else if (!c.lists_valid) {
     setup(c);
+  } else if (!c.forces_current) {
+    // Verlet::setup evaluates the forces of the positions a run starts from;
+    // they differ from the last evaluation after a box change or new positions
+    forces(c, 0, 0);
   }
-  const bool graphs = c.graphs_enabled && c.every > 0 && !c.prof.enabled;
+  deform_begin(c, nsteps, dt);
+  // a deforming box changes launch arguments every step: no graph replay
+  const bool graphs = c.graphs_enabled && c.every > 0 && !c.prof.enabled && !c.dfm.on;
   const bool want_ev = eflag || vflag;
   int s = 1;
   while (s <= nsteps) {
@@ -464,6 +478,7 @@ void run_nve(Ctx &c, int nsteps, double dt, int eflag, int vflag) {
     forces(c, last ? eflag : 0, last ? vflag : 0);
     langevin_post_force(c, dt);
     nve_final(c, dt);
+    deform_end_of_step(c, dt);
     s++;
   }
   CACB200_CUDA(cudaGetLastError());
@@ -631,6 +646,19 @@ int cacb200_set_langevin(cacb200_ctx *ctx, double t_start, double t_stop, double
 int cacb200_unset_langevin(cacb200_ctx *ctx) {
   API_BEGIN
   langevin_unset(c);
+  API_END
+}
+
+int cacb200_set_deform(cacb200_ctx *ctx, int nevery, const int style[3], const double a[3], const double b[3],
+                       int remap_x) {
+  API_BEGIN
+  deform_set(c, nevery, style, a, b, remap_x);
+  API_END
+}
+
+int cacb200_unset_deform(cacb200_ctx *ctx) {
+  API_BEGIN
+  deform_unset(c);
   API_END
 }
 

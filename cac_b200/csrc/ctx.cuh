@@ -129,6 +129,27 @@ struct LangevinParams {
   bool zero = false;
 };
 
+// fix deform, orthogonal box (FixDeform, fix_deform.cpp:40-372): per
+// dimension a style with its arguments (box units) and, for volume, the
+// dimensions it is linked to
+struct DeformDim {
+  enum { ONE_FROM_ONE, ONE_FROM_TWO, TWO_FROM_ONE };
+  int style = CACB200_DEFORM_NONE;
+  double a = 0, b = 0;
+  int substyle = 0, fixed = 0, dynamic1 = 0, dynamic2 = 0;
+};
+struct DeformParams {
+  bool on = false;
+  int nevery = 1;
+  bool remap_x = true;
+  DeformDim dim[3];
+  long begin = 0, end = 0;   // the current run's first and last step
+};
+// per replica: the run's start and stop boxes (FixDeform::Set)
+struct DeformRep {
+  double lo_start[3], hi_start[3], lo_stop[3], hi_stop[3], vol_start[3];
+};
+
 struct Profile {
   bool enabled = false;
   std::vector<std::string> names;
@@ -295,6 +316,12 @@ struct Ctx {
   DBuf<int4> lgv_meta;
   DBuf<double> lgv_part, lgv_mean, lgv_save;
   int lgv_nchunks = 0, lgv_poly_n = 0;
+  // fix deform: parameters, per-replica start/stop boxes, device remap table
+  DeformParams dfm;
+  std::vector<DeformRep> dfm_rep;
+  DBuf<double> dfm_maps;
+  bool box_replan = false;        // the next plan follows a box change only
+  bool forces_current = false;    // f / nodef belong to the current positions and box
   DBuf<int4> thermo_meta;
   DBuf<double> thermo_vol, thermo_part, thermo_out;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -346,5 +373,9 @@ void langevin_set(Ctx &c, double t_start, double t_stop, double t_period, int se
 void langevin_unset(Ctx &c);
 void langevin_begin(Ctx &c, long nsteps);
 void langevin_post_force(Ctx &c, double dt);
+void deform_set(Ctx &c, int nevery, const int *style, const double *a, const double *b, int remap_x);
+void deform_unset(Ctx &c);
+void deform_begin(Ctx &c, long nsteps, double dt);
+void deform_end_of_step(Ctx &c, double dt);
 
 }  // namespace cacb200

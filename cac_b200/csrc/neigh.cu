@@ -1122,7 +1122,15 @@ void neigh_plan(Ctx &c, bool want_half) {
   c.sort_bits_e = bits_e;
   c.plan_half = want_half;
   c.planned = true;
+  const long gen_before = c.gen;
   c.gen++;
+  if (c.box_replan) {
+    // only the box moved (fix deform): the block sizes chosen for this
+    // system stay valid
+    if (c.tune_gen == gen_before) c.tune_gen = c.gen;
+    if (c.tune_gen32 == gen_before) c.tune_gen32 = c.gen;
+    c.box_replan = false;
+  }
   c.plan_na = c.na;
   c.plan_ne = c.ne;
 }

@@ -228,6 +228,39 @@ int cacb200_set_langevin(cacb200_ctx *ctx, double t_start, double t_stop, double
                          int zero);
 int cacb200_unset_langevin(cacb200_ctx *ctx);
 
+/* fix ID all deform N x|y|z style args ... remap x|none units box on an
+ * orthogonal periodic box (FixDeform, fix_deform.cpp:40-487, 698-707,
+ * 1020-1240): every N-th step, after the second half-kick, each dimension's
+ * box edges move to the style's target for that step of the run (run start
+ * box -> stop box, per run as the reference's init does), and with remap x
+ * the atoms and nodes follow affinely.  style[d] and its arguments a[d], b[d]
+ * (box units):
+ *   CACB200_DEFORM_NONE    unchanged
+ *   CACB200_DEFORM_FINAL   a = lo, b = hi at the end of the run
+ *   CACB200_DEFORM_DELTA   a = dlo, b = dhi added over the run
+ *   CACB200_DEFORM_SCALE   a = factor about the centre
+ *   CACB200_DEFORM_VEL     a = velocity of the length (distance/time)
+ *   CACB200_DEFORM_ERATE   a = engineering strain rate (1/time)
+ *   CACB200_DEFORM_TRATE   a = true strain rate (1/time)
+ *   CACB200_DEFORM_WIGGLE  a = amplitude, b = period (time)
+ *   CACB200_DEFORM_VOLUME  keeps the volume, linked to the other dimensions
+ * Replicas of a batch deform alike, each from its own box.  Runs with a
+ * deforming box queue their steps without graph replay; the neighbour grids
+ * follow the box at each rebuild.  A new system or cacb200_unset_deform
+ * removes the fix.  remap v and tilt (triclinic) styles are not offered. */
+#define CACB200_DEFORM_NONE 0
+#define CACB200_DEFORM_FINAL 1
+#define CACB200_DEFORM_DELTA 2
+#define CACB200_DEFORM_SCALE 3
+#define CACB200_DEFORM_VEL 4
+#define CACB200_DEFORM_ERATE 5
+#define CACB200_DEFORM_TRATE 6
+#define CACB200_DEFORM_WIGGLE 7
+#define CACB200_DEFORM_VOLUME 8
+int cacb200_set_deform(cacb200_ctx *ctx, int nevery, const int style[3], const double a[3],
+                       const double b[3], int remap_x);
+int cacb200_unset_deform(cacb200_ctx *ctx);
+
 /* ------------------------------------------------------------- minimise */
 
 /* min_modify for FIRE: the parameters of Min (min.h:61-72) with the

@@ -419,6 +419,93 @@ def langevin_target(t_start: float, t_stop: float, step: int, begin: int, end: i
     return t_start + delta * (t_stop - t_start)
 
 
+# ------------------------------------------------------------------ deform
+
+DEFORM_STYLES = ("none", "final", "delta", "scale", "vel", "erate", "trate", "wiggle", "volume")
+MY_2PI = 6.28318530717958647692
+
+
+def deform_boxes(boxlo, boxhi, nevery: int, style, a, b, runs, dt: float = 0.001, first_step: int = 0):
+    """Box edges under ``fix deform`` (orthogonal, units box) after the given
+    consecutive runs, in the reference's order of operations: FixDeform::init
+    per run (fix_deform.cpp:417-487), apply_strain / apply_volume /
+    update_domain on steps divisible by N (fix_deform.cpp:698-707,
+    1020-1240).  Returns (lo, hi) as lists."""
+    lo, hi = [float(v) for v in boxlo], [float(v) for v in boxhi]
+    st = [DEFORM_STYLES[int(s)] for s in style]
+    link = {}
+    for i in range(3):
+        if st[i] != "volume":
+            continue
+        o1, o2 = (i + 1) % 3, (i + 2) % 3
+        if st[o1] == "none":
+            link[i] = ("one_from_one", o1, o2, None)
+        elif st[o2] == "none":
+            link[i] = ("one_from_one", o2, o1, None)
+        elif st[o1] == "volume":
+            link[i] = ("two_from_one", o1, o2, None)
+        elif st[o2] == "volume":
+            link[i] = ("two_from_one", o2, o1, None)
+        else:
+            link[i] = ("one_from_two", None, o1, o2)
+    step = first_step
+    for n in runs:
+        begin, end = step, step + n
+        delt = (end - begin) * dt
+        los, his = lo[:], hi[:]
+        vol0 = (hi[0] - lo[0]) * (hi[1] - lo[1]) * (hi[2] - lo[2])
+        lstop, hstop = lo[:], hi[:]
+        for i in range(3):
+            s, x, y = st[i], float(a[i]), float(b[i])
+            if s == "final":
+                lstop[i], hstop[i] = x, y
+            elif s == "delta":
+                lstop[i], hstop[i] = los[i] + x, his[i] + y
+            elif s == "scale":
+                lstop[i] = 0.5 * (los[i] + his[i]) - 0.5 * x * (his[i] - los[i])
+                hstop[i] = 0.5 * (los[i] + his[i]) + 0.5 * x * (his[i] - los[i])
+            elif s == "vel":
+                lstop[i], hstop[i] = los[i] - 0.5 * delt * x, his[i] + 0.5 * delt * x
+            elif s == "erate":
+                lstop[i] = los[i] - 0.5 * delt * x * (his[i] - los[i])
+                hstop[i] = his[i] + 0.5 * delt * x * (his[i] - los[i])
+        for _ in range(n):
+            step += 1
+            if step % nevery:
+                continue
+            delta = float(step - begin)
+            if delta != 0.0:
+                delta /= end - begin
+            t = (step - begin) * dt
+            lt, ht = lo[:], hi[:]
+            for i in range(3):
+                s, x, y = st[i], float(a[i]), float(b[i])
+                if s == "trate":
+                    shift = 0.5 * ((his[i] - los[i]) * math.exp(x * t))
+                    lt[i], ht[i] = 0.5 * (los[i] + his[i]) - shift, 0.5 * (los[i] + his[i]) + shift
+                elif s == "wiggle":
+                    shift = 0.5 * x * math.sin(MY_2PI * t / y)
+                    lt[i], ht[i] = los[i] - shift, his[i] + shift
+                elif s in ("final", "delta", "scale", "vel", "erate"):
+                    lt[i] = los[i] + delta * (lstop[i] - los[i])
+                    ht[i] = his[i] + delta * (hstop[i] - his[i])
+            for i in range(3):
+                if i not in link:
+                    continue
+                kind, fixed, d1, d2 = link[i]
+                if kind == "one_from_one":
+                    shift = 0.5 * (vol0 / (ht[d1] - lt[d1]) / (his[fixed] - los[fixed]))
+                elif kind == "one_from_two":
+                    shift = 0.5 * (vol0 / (ht[d1] - lt[d1]) / (ht[d2] - lt[d2]))
+                else:
+                    shift = 0.5 * math.sqrt(vol0 * (his[i] - los[i]) / (ht[d1] - lt[d1]) / (his[fixed] - los[fixed]))
+                lt[i], ht[i] = 0.5 * (los[i] + his[i]) - shift, 0.5 * (los[i] + his[i]) + shift
+            for i in range(3):
+                if st[i] != "none":
+                    lo[i], hi[i] = lt[i], ht[i]
+    return lo, hi
+
+
 def read_thermo(log: str, columns=THERMO_COLUMNS) -> np.ndarray:
     """Rows of the reference's thermo output (``Step`` plus ``columns``) from
     a run's screen log, one row per printed step."""

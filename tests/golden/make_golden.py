@@ -14,7 +14,8 @@ Each fixture ``<case>.npz`` holds the reference's own read-outs:
   lines (``thermo_style custom step temp ke pe etotal press pxx pyy pzz pxy
   pxz pyz vol``, printed with ``%.17g``) at step 0 and step N; and with
   ``fix langevin`` (the ``LANGEVIN`` cases) its setup forces and the state
-  after consecutive runs.
+  after consecutive runs; with ``fix deform`` (the ``DEFORM`` cases) the
+  state and box after consecutive runs.
 EAM energies come from the executable with the patched ``compute_fp``
 (``cac_eamfix``); the unpatched reference energy is kept as ``energy_unpatched``.
 """
@@ -130,6 +131,69 @@ def add_langevin(name: str, system, pair: str) -> None:
     print(name, "langevin", float(np.abs(out["lgv_end_v"]).max()))
 
 
+# fix deform cases: N, per-dimension (style, a, b) in box units, the run lengths;
+# "final" edges are offsets from the case's own box
+DEFORM_STYLES = ("none", "final", "delta", "scale", "vel", "erate", "trate", "wiggle", "volume")
+DEFORM = {
+    "tiny_lj": (1, (("erate", 0.5, 0.0), ("volume", 0.0, 0.0), ("vel", 0.4, 0.0)), (20, 20)),
+    "tiny_eam": (2, (("trate", 0.2, 0.0), ("none", 0.0, 0.0), ("wiggle", 0.3, 0.01)), (30,)),
+    "lj_small": (1, (("final", -0.05, 0.05), ("scale", 0.995, 0.0), ("delta", -0.02, 0.03)), (25,)),
+}
+
+
+def deform_spec(name: str, system):
+    """(N, styles, a, b, runs) with final edges made absolute for this system."""
+    nevery, dims, runs = DEFORM[name]
+    style, a, b = [], [], []
+    for d, (st, x, y) in enumerate(dims):
+        if st == "final":
+            x, y = float(system.boxlo[d]) + x, float(system.boxhi[d]) + y
+        style.append(DEFORM_STYLES.index(st))
+        a.append(float(x))
+        b.append(float(y))
+    return nevery, style, a, b, runs
+
+
+def deform_rows(work: str, pair: str, exe: str, system, name: str) -> dict:
+    """The reference with ``fix deform ... units box remap x`` after ``fix
+    nve``: the state and box after the given consecutive runs."""
+    nevery, style, a, b, runs = deform_spec(name, system)
+    args = []
+    for d in range(3):
+        st = DEFORM_STYLES[style[d]]
+        if st == "none":
+            continue
+        n = {"final": 2, "delta": 2, "wiggle": 2, "scale": 1, "vel": 1, "erate": 1, "trate": 1, "volume": 0}[st]
+        args.append(" ".join(["xyz"[d], st] + [repr(v) for v in (a[d], b[d])[:n]]))
+    tail = "neighbor 1.0 bin\nneigh_modify every 10 delay 0 check no\ntimestep 0.001\nfix 1 all nve\n"
+    fix = f"fix 3 all deform {nevery} {' '.join(args)} units box remap x\n"
+    script = HEADER + pair_lines(pair) + tail + fix + "".join(f"run {n}\n" for n in runs)
+    run(work, script + "oracle_dump dfm1.txt state\n", exe)
+    e = O.read_dump(os.path.join(work, "dfm1.txt"))
+    out = {"dfm_nevery": np.int64(nevery), "dfm_style": np.array(style, dtype=np.int64),
+           "dfm_a": np.array(a), "dfm_b": np.array(b), "dfm_runs": np.array(runs, dtype=np.int64),
+           "dfm_end_box": e["box"]}
+    for k in ("x", "v", "f", "nodex", "nodev", "nodef"):
+        out["dfm_end_" + k] = e[k]
+    return out
+
+
+def add_deform(name: str, system, pair: str) -> None:
+    """Add the fix deform read-outs to an existing fixture."""
+    path = os.path.join(OUT, name + ".npz")
+    with np.load(path) as z:
+        out = {k: z[k] for k in z.files}
+    work = tempfile.mkdtemp(prefix="cacgold_")
+    try:
+        gen.write_data(system, os.path.join(work, "data.cac"))
+        gen.write_setfl(gen.EamParams(), os.path.join(work, "cu.setfl"))
+        out.update(deform_rows(work, pair, O.REF_EXE, system, name))
+    finally:
+        shutil.rmtree(work, ignore_errors=True)
+    np.savez_compressed(path, **out)
+    print(name, "deform box", out["dfm_end_box"].tolist())
+
+
 def add_thermo(name: str, system, pair: str) -> None:
     """Add the thermo rows to an existing fixture, leaving its other arrays as they are."""
     path = os.path.join(OUT, name + ".npz")
@@ -186,6 +250,7 @@ def make_case(name: str, system, pair: str, nsteps: int = 0, peratom_virial: boo
                 out["end_" + k] = e[k]
         out.update(thermo_rows(work, pair, nsteps, exe_e))
         out.update(langevin_rows(work, pair, O.REF_EXE, *LANGEVIN[name]))
+        out.update(deform_rows(work, pair, O.REF_EXE, system, name))
         meta = dict(system.meta)
         out["meta"] = np.array(repr(sorted(meta.items())))
         np.savez_compressed(os.path.join(OUT, name + ".npz"), **out)
@@ -202,17 +267,21 @@ CASES = (
 
 
 def main():
-    """``make_golden.py`` writes every fixture; ``make_golden.py thermo``
-    or ``make_golden.py langevin`` only adds those read-outs to the fixtures
+    """``make_golden.py`` writes every fixture; ``make_golden.py thermo``,
+    ``langevin`` or ``deform`` only adds those read-outs to the fixtures
     already here."""
     if not os.path.exists(O.REF_EXE):
         raise SystemExit("build the reference first: make -C oracle reference")
     only = sys.argv[1] if sys.argv[1:] else None
+    if only not in (None, "thermo", "langevin", "deform"):
+        raise SystemExit(f"unknown mode {only!r}")
     for name, system, pair, kw in CASES:
         if only == "thermo":
             add_thermo(name, system(), pair)
         elif only == "langevin":
             add_langevin(name, system(), pair)
+        elif only == "deform":
+            add_deform(name, system(), pair)
         else:
             make_case(name, system(), pair, **kw)
 

@@ -147,3 +147,17 @@ def test_ranmars_restatement_properties(oracle_mod):
     for bad in (0, 900000001):
         with pytest.raises(ValueError):
             oracle_mod.RanMars(bad)
+
+
+@pytest.mark.parametrize("case", ["tiny_lj", "tiny_eam", "lj_small"])
+def test_deform_box_matches_reference(case, oracle_mod, golden):
+    """The fix deform box arithmetic restated against the reference's box
+    after consecutive runs (every style of the cases: erate, volume, vel,
+    trate, wiggle, final, scale, delta), bit for bit."""
+    g = golden(case)
+    s = CASES[case][0]()
+    lo, hi = oracle_mod.deform_boxes(s.boxlo, s.boxhi, int(g["dfm_nevery"]), g["dfm_style"], g["dfm_a"],
+                                     g["dfm_b"], [int(n) for n in g["dfm_runs"]])
+    box = g["dfm_end_box"]
+    assert lo == [box[0], box[2], box[4]]
+    assert hi == [box[1], box[3], box[5]]
