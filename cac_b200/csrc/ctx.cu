@@ -223,14 +223,30 @@ __global__ void k_replica_energy(const double *eatom, const double *enode, const
   block_reduce_store<1>(v, out);
 }
 
-__global__ void k_pack_x(const double *x, double4 *xs, int n) {
+__device__ __forceinline__ bool same_bits(double a, double b) {
+  return __double_as_longlong(a) == __double_as_longlong(b);
+}
+
+// New positions into the site table; *changed is set when any differs
+// from the one it replaces (bit for bit).
+__global__ void k_pack_x(const double *x, double4 *xs, int n, int *changed) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   double4 p = xs[i];
-  p.x = x[3 * i];
-  p.y = x[3 * i + 1];
-  p.z = x[3 * i + 2];
+  const double a = x[3 * i], b = x[3 * i + 1], d = x[3 * i + 2];
+  if (!same_bits(p.x, a) || !same_bits(p.y, b) || !same_bits(p.z, d)) atomicOr(changed, 1);
+  p.x = a;
+  p.y = b;
+  p.z = d;
   xs[i] = p;
+}
+
+__global__ void k_copy_cmp(const double *src, double *dst, long n, int *changed) {
+  long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double v = src[i];
+  if (!same_bits(dst[i], v)) atomicOr(changed, 1);
+  dst[i] = v;
 }
 
 __global__ void k_unpack_x(const double4 *xs, double *x, int n) {
@@ -247,21 +263,36 @@ __global__ void k_unpack_x(const double4 *xs, double *x, int n) {
 // ghosts; rebuild when atoms moved further than half the skin.
 void set_state(Ctx &c, const double *x, const double *v, const double *nodex, const double *nodev) {
   c.check_system();
+  const bool moves = (x && c.na) || (nodex && c.ne);
+  if (moves) {
+    c.state_changed.reserve(1);
+    CACB200_CUDA(cudaMemsetAsync(c.state_changed.p, 0, sizeof(int), c.stream));
+  }
   if (x && c.na) {
     c.stage.reserve(3 * (size_t)c.na);
     CACB200_CUDA(cudaMemcpyAsync(c.stage.p, x, sizeof(double) * 3 * c.na, cudaMemcpyHostToDevice, c.stream));
-    k_pack_x<<<(c.na + 255) / 256, 256, 0, c.stream>>>(c.stage.p, c.xs.p, c.na);
+    k_pack_x<<<(c.na + 255) / 256, 256, 0, c.stream>>>(c.stage.p, c.xs.p, c.na, c.state_changed.p);
   }
   if (v && c.na)
     CACB200_CUDA(cudaMemcpyAsync(c.v.p, v, sizeof(double) * 3 * c.na, cudaMemcpyHostToDevice, c.stream));
-  if (nodex && c.ne)
-    CACB200_CUDA(cudaMemcpyAsync(c.nodex.p, nodex, sizeof(double) * 24 * c.ne, cudaMemcpyHostToDevice, c.stream));
+  if (nodex && c.ne) {
+    const long n = 24L * c.ne;
+    c.stage_nodes.reserve(n);
+    CACB200_CUDA(cudaMemcpyAsync(c.stage_nodes.p, nodex, sizeof(double) * n, cudaMemcpyHostToDevice, c.stream));
+    k_copy_cmp<<<(int)((n + 255) / 256), 256, 0, c.stream>>>(c.stage_nodes.p, c.nodex.p, n, c.state_changed.p);
+  }
   if (nodev && c.ne)
     CACB200_CUDA(cudaMemcpyAsync(c.nodev.p, nodev, sizeof(double) * 24 * c.ne, cudaMemcpyHostToDevice, c.stream));
+  CACB200_CUDA(cudaGetLastError());
   CACB200_CUDA(cudaStreamSynchronize(c.stream));
-  if ((x && c.na) || (nodex && c.ne)) {
-    forget_tallies(c);
-    c.forces_current = false;
+  if (moves) {
+    // positions written back unchanged keep the forces and tallies they had
+    int changed = 1;
+    stream_copy(c, &changed, c.state_changed.p, sizeof(int), cudaMemcpyDeviceToHost);
+    if (changed) {
+      forget_tallies(c);
+      c.forces_current = false;
+    }
   }
 }
 

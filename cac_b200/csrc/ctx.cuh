@@ -198,6 +198,8 @@ struct Ctx {
 
   DBuf<double> v, f;             // atoms [na*3]
   DBuf<double> stage;            // [na*3] host-transfer staging for positions
+  DBuf<double> stage_nodes;      // [ne*24] the same for node positions
+  DBuf<int> state_changed;       // set_state: did any position change
   DBuf<double4> snap_x;          // device snapshot of the state (cacb200_snapshot)
   DBuf<double> snap_v, snap_nodex, snap_nodev;
   bool have_snapshot = false;

@@ -146,6 +146,7 @@ void assemble_nodef(Ctx &c) {
 }
 
 void nve_initial(Ctx &c, double dt) {
+  c.forces_current = false;   // the drift moves every site
   double dtf = 0.5 * dt * (1.0 / 1.0364269e-4);   // metal units, update.cpp:161-164
   double dtfm = dtf / c.mass;
   int n = c.na + 24 * c.ne;

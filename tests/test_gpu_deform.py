@@ -126,3 +126,28 @@ def test_deform_arguments_and_unset(tmp_path):
     lo, hi = e.box()
     assert np.array_equal(lo, lo0) and np.array_equal(hi, hi0)
     e.close()
+
+
+def test_run_starts_from_forces_of_current_positions(tmp_path):
+    """Like Verlet::setup, a run starts from the forces of the positions it
+    is given: new positions through set_state are evaluated first, positions
+    written back unchanged keep their forces (the same values either way)."""
+    s = CASES["tiny_lj"][0]()
+    e = make_engine(s, "lj", tmp_path)
+    e.setup()
+    x, v, nx, nv = e.state()
+    e.set_state(x, v, nx, nv)          # unchanged
+    f0, nf0, _ = e.forces()
+    x2 = x.copy()
+    x2[0, 0] += 0.01
+    e.set_state(x2, v, nx, nv)
+    e.run_nve(0)
+    f1, _, _ = e.forces()
+    e.close()
+    r = make_engine(s, "lj", tmp_path)
+    r.set_state(x2, v, nx, nv)
+    r.setup()
+    fr, _, _ = r.forces()
+    r.close()
+    assert not np.array_equal(f0, f1)
+    assert rel_err(f1, fr) < 1e-13   # lists built from other positions: summation order may differ
