@@ -46,6 +46,7 @@ SIGNATURES = [
     ("cacb200_set_precision", C.c_int, [C.c_void_p, C.c_int]),
     ("cacb200_upload_system", C.c_int, [C.c_void_p, _dp, _dp, C.c_int, _dp, _dp, C.c_int, _dp, _dp, C.c_double]),
     ("cacb200_get_box", C.c_int, [C.c_void_p, _dp, _dp, _dp]),
+    ("cacb200_set_box", C.c_int, [C.c_void_p, _dp, _dp]),
     ("cacb200_data_last_error", C.c_char_p, []),
     ("cacb200_data_counts", C.c_int, [C.c_char_p, C.POINTER(C.c_int), C.POINTER(C.c_int), _dp, _dp, _dp]),
     ("cacb200_data_read", C.c_int, [C.c_char_p, _dp, _dp, _dp, _dp]),
@@ -57,6 +58,7 @@ SIGNATURES = [
     ("cacb200_replica_energy", C.c_int, [C.c_void_p, _dp]),
     ("cacb200_thermo", C.c_int, [C.c_void_p, C.c_int, _dp]),
     ("cacb200_set_langevin", C.c_int, [C.c_void_p, C.c_double, C.c_double, C.c_double, C.c_int, C.c_int]),
+    ("cacb200_set_langevin_stream", C.c_int, [C.c_void_p, C.c_longlong]),
     ("cacb200_unset_langevin", C.c_int, [C.c_void_p]),
     ("cacb200_set_deform", C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int), _dp, _dp, C.c_int]),
     ("cacb200_unset_deform", C.c_int, [C.c_void_p]),
@@ -356,6 +358,12 @@ class Engine:
         self._check(self.lib.cacb200_set_deform(self.h, nevery, style, _p(a), _p(b), 1 if remap == "x" else 0),
                     "set_deform")
 
+    def set_box(self, boxlo, boxhi) -> None:
+        """New periodic box of a single system, sites left where they are."""
+        lo = np.ascontiguousarray(boxlo, dtype=np.float64)
+        hi = np.ascontiguousarray(boxhi, dtype=np.float64)
+        self._check(self.lib.cacb200_set_box(self.h, _p(lo), _p(hi)), "set_box")
+
     def unset_deform(self) -> None:
         self._check(self.lib.cacb200_unset_deform(self.h), "unset_deform")
 
@@ -364,6 +372,10 @@ class Engine:
         lo, hi, m = np.zeros(3), np.zeros(3), C.c_double()
         self._check(self.lib.cacb200_get_box(self.h, _p(lo), _p(hi), C.byref(m)), "get_box")
         return lo, hi
+
+    def langevin_stream(self, draws: int) -> None:
+        """Continue the thermostat's RanMars streams after ``draws`` uniform() calls."""
+        self._check(self.lib.cacb200_set_langevin_stream(self.h, int(draws)), "set_langevin_stream")
 
     def unset_langevin(self) -> None:
         self._check(self.lib.cacb200_unset_langevin(self.h), "unset_langevin")

@@ -674,6 +674,12 @@ int cacb200_set_langevin(cacb200_ctx *ctx, double t_start, double t_stop, double
   API_END
 }
 
+int cacb200_set_langevin_stream(cacb200_ctx *ctx, long long draws) {
+  API_BEGIN
+  langevin_stream(c, draws);
+  API_END
+}
+
 int cacb200_unset_langevin(cacb200_ctx *ctx) {
   API_BEGIN
   langevin_unset(c);
@@ -684,6 +690,12 @@ int cacb200_set_deform(cacb200_ctx *ctx, int nevery, const int style[3], const d
                        int remap_x) {
   API_BEGIN
   deform_set(c, nevery, style, a, b, remap_x);
+  API_END
+}
+
+int cacb200_set_box(cacb200_ctx *ctx, const double boxlo[3], const double boxhi[3]) {
+  API_BEGIN
+  set_box(c, boxlo, boxhi);
   API_END
 }
 

@@ -373,11 +373,13 @@ FireState fire_read(Ctx &c);
 void thermo(Ctx &c, int units, double *out);
 void langevin_set(Ctx &c, double t_start, double t_stop, double t_period, int seed, int zero);
 void langevin_unset(Ctx &c);
+void langevin_stream(Ctx &c, long long draws);
 void langevin_begin(Ctx &c, long nsteps);
 void langevin_post_force(Ctx &c, double dt);
 void deform_set(Ctx &c, int nevery, const int *style, const double *a, const double *b, int remap_x);
 void deform_unset(Ctx &c);
 void deform_begin(Ctx &c, long nsteps, double dt);
 void deform_end_of_step(Ctx &c, double dt);
+void set_box(Ctx &c, const double *lo, const double *hi);
 
 }  // namespace cacb200

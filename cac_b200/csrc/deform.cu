@@ -178,6 +178,8 @@ void deform_begin(Ctx &c, long nsteps, double dt) {
   }
 }
 
+void box_changed(Ctx &c);
+
 // FixDeform::end_of_step on the steps it applies to (Modify::end_of_step,
 // modify.cpp:910-915): new targets, remap, new box.
 void deform_end_of_step(Ctx &c, double dt) {
@@ -250,13 +252,6 @@ void deform_end_of_step(Ctx &c, double dt) {
       M.lo1[i] = B.lo[i];
       M.h1[i] = B.L[i];
     }
-    Rep &P = c.rep_h[r];
-    for (int i = 0; i < 3; i++) P.Lq[i] = (int)(uint32_t)(uint64_t)std::llrint(B.L[i] * P.qscale[i]);
-  }
-  for (int i = 0; i < 3; i++) {
-    c.boxlo[i] = c.rep_h[0].b.lo[i];
-    c.boxhi[i] = c.rep_h[0].b.hi[i];
-    c.prd[i] = c.rep_h[0].b.L[i];
   }
   if (c.dfm.remap_x && (c.na || c.ne)) {
     const Remap *many = nullptr;
@@ -272,16 +267,50 @@ void deform_end_of_step(Ctx &c, double dt) {
         c.nrep > 1 ? c.elem_rep.p : nullptr);
     CACB200_CUDA(cudaGetLastError());
   }
+  // energies tallied this step stay (the reference's thermo output after
+  // end_of_step reports them with the new volume)
+  box_changed(c);
+}
+
+// The replica boxes in rep_h changed: the fixed-point box lengths, the
+// context box, the device descriptors; grids and reference bins are replanned
+// at the next rebuild, read-outs see the new volume, and a run starts from
+// forces of the new box.
+void box_changed(Ctx &c) {
+  for (Rep &P : c.rep_h)
+    for (int i = 0; i < 3; i++) P.Lq[i] = (int)(uint32_t)(uint64_t)std::llrint(P.b.L[i] * P.qscale[i]);
+  for (int i = 0; i < 3; i++) {
+    c.boxlo[i] = c.rep_h[0].b.lo[i];
+    c.boxhi[i] = c.rep_h[0].b.hi[i];
+    c.prd[i] = c.rep_h[0].b.L[i];
+  }
   if (c.rep_d.p && c.rep_d.n >= (size_t)c.nrep)
     CACB200_CUDA(cudaMemcpyAsync(c.rep_d.p, c.rep_h.data(), sizeof(Rep) * c.nrep, cudaMemcpyHostToDevice, c.stream));
-  // the grids follow the box at the next rebuild; read-outs see the new volume
   c.planned = false;
   c.box_replan = true;
   c.thermo_gen = -1;
-  // energies tallied this step stay (the reference's thermo output after
-  // end_of_step reports them with the new volume); forces are recomputed
-  // before the next run starts
   c.forces_current = false;
+}
+
+// A new box for a single system without moving its sites (the box a host
+// loop has just changed, e.g. the reference's own fix deform; the positions
+// follow with the next set_state).
+void set_box(Ctx &c, const double *lo, const double *hi) {
+  c.check_system();
+  if (c.nrep != 1) throw Error(CACB200_ESTATE, "a batch has one box per replica");
+  if (!lo || !hi) throw Error(CACB200_EINVAL, "box required");
+  BoxD &B = c.rep_h[0].b;
+  for (int i = 0; i < 3; i++)
+    if (!(hi[i] > lo[i])) throw Error(CACB200_EINVAL, "empty box");
+  bool same = true;
+  for (int i = 0; i < 3; i++) same = same && B.lo[i] == lo[i] && B.hi[i] == hi[i];
+  if (same) return;
+  for (int i = 0; i < 3; i++) {
+    B.lo[i] = lo[i];
+    B.hi[i] = hi[i];
+    B.L[i] = hi[i] - lo[i];
+  }
+  box_changed(c);
 }
 
 }  // namespace cacb200

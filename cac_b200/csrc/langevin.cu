@@ -109,6 +109,38 @@ std::vector<unsigned> jump_table(int n) {
   return out;
 }
 
+// x^n mod P by squaring.
+std::vector<unsigned> xpow(unsigned long long n) {
+  std::vector<unsigned> r(WIN, 0), b(WIN, 0);
+  r[0] = 1;
+  b[1] = 1;
+  while (n) {
+    if (n & 1) r = polymul(r, b);
+    n >>= 1;
+    if (n) b = polymul(b, b);
+  }
+  return r;
+}
+
+// The 193 values Y_{B-96} .. Y_{B+96} of a stream after `draws` uniform()
+// calls (the constructor's warm-up included), B = 97 + draws the last value
+// used: Y_{1+draws+s} = sum_i c_i Y_{1+s+i} with c = x^draws mod P, from the
+// seeded values extended to Y_193.
+std::vector<unsigned> stream_window(int seed, unsigned long long draws) {
+  std::vector<unsigned> y = seed_window(seed);   // Y_1 .. Y_97
+  y.resize(EXT);
+  for (int n = WIN; n < EXT; n++) y[n] = (y[n - WIN] - y[n - 33]) & MASK24;
+  const std::vector<unsigned> c = xpow(draws);
+  std::vector<unsigned> w(EXT);
+  for (int s = 0; s < WIN; s++) {
+    unsigned long long acc = 0;
+    for (int i = 0; i < WIN; i++) acc += (unsigned long long)c[i] * y[s + i];
+    w[s] = (unsigned)(acc & MASK24);
+  }
+  for (int n = WIN; n < EXT; n++) w[n] = (w[n - WIN] - w[n - 33]) & MASK24;
+  return w;
+}
+
 // ---------------------------------------------------------- device kernels
 
 struct LgvArgs {
@@ -294,11 +326,9 @@ void langevin_set(Ctx &c, double t_start, double t_stop, double t_period, int se
   std::vector<int4> meta(c.nrep);
   int maxj = 1;
   for (int r = 0; r < c.nrep; r++) {
-    std::vector<unsigned> y = seed_window(seed + r);   // Y_1 .. Y_97
-    y.resize(WIN + 1 + EXT);
-    for (size_t n = WIN; n < y.size(); n++) y[n] = (y[n - WIN] - y[n - 33]) & MASK24;   // Y_98 ...
-    // after the warm-up draw the last value is Y_98: window Y_2 .. Y_98, then Y_99 .. Y_194
-    for (int i = 0; i < EXT; i++) base[(size_t)r * EXT + i] = y[1 + i];
+    // after the constructor's warm-up draw: window Y_2 .. Y_98, then Y_99 .. Y_194
+    const std::vector<unsigned> w = stream_window(seed + r, 1);
+    std::copy(w.begin(), w.end(), base.begin() + (size_t)r * EXT);
     const long long N = 3LL * c.rep_na[r] + 24LL * c.rep_ne[r];
     const int nj = (int)((N + CHUNK - 1) / CHUNK);
     rchunk[r] = make_int2((int)chunks.size(), nj);
@@ -335,6 +365,22 @@ void langevin_set(Ctx &c, double t_start, double t_stop, double t_period, int se
   c.lgv.zero = zero != 0;
   c.lgv_nchunks = (int)chunks.size();
   c.gen++;
+}
+
+// Every replica's stream positioned after `draws` uniform() calls of its
+// RanMars (the constructor's warm-up is draw 1), e.g. to continue a stream
+// the reference's own loop has been drawing from.
+void langevin_stream(Ctx &c, long long draws) {
+  if (!c.lgv.on) throw Error(CACB200_ESTATE, "no fix langevin set");
+  if (draws < 1) throw Error(CACB200_EINVAL, "a RanMars stream has made at least its warm-up draw");
+  std::vector<unsigned> base((size_t)c.nrep * EXT);
+  for (int r = 0; r < c.nrep; r++) {
+    const std::vector<unsigned> w = stream_window(c.lgv.seed + r, (unsigned long long)draws);
+    std::copy(w.begin(), w.end(), base.begin() + (size_t)r * EXT);
+  }
+  std::vector<unsigned long long> m(c.nrep, (unsigned long long)draws);
+  stream_copy(c, c.lgv_base.p, base.data(), sizeof(unsigned) * base.size(), cudaMemcpyHostToDevice);
+  stream_copy(c, c.lgv_m.p, m.data(), sizeof(unsigned long long) * m.size(), cudaMemcpyHostToDevice);
 }
 
 void langevin_unset(Ctx &c) {

@@ -16,6 +16,7 @@
 #include "comm.h"
 #include "domain.h"
 #include "element.h"
+#include "element_vec.h"
 #include "error.h"
 #include "force.h"
 #include "neighbor.h"
@@ -122,6 +123,10 @@ void B200Bridge::upload(bool with_velocities)
   configure_pair();
   uploaded_na = na;
   uploaded_ne = ne;
+  for (int d = 0; d < 3; d++) {
+    uploaded_lo[d] = domain->boxlo[d];
+    uploaded_hi[d] = domain->boxhi[d];
+  }
 }
 
 void B200Bridge::compute(Pair *pair)
@@ -134,6 +139,18 @@ void B200Bridge::compute(Pair *pair)
     status(cacb200_set_neighbor(ctx, neighbor->skin, 0), "set_neighbor");
     status(cacb200_build_lists(ctx, 0), "build_lists");
   } else {
+    // a box the reference changed since the last rebuild (fix deform): the
+    // device's periodic images follow it
+    bool moved = false;
+    for (int d = 0; d < 3; d++)
+      moved = moved || domain->boxlo[d] != uploaded_lo[d] || domain->boxhi[d] != uploaded_hi[d];
+    if (moved) {
+      status(cacb200_set_box(ctx, domain->boxlo, domain->boxhi), "set_box");
+      for (int d = 0; d < 3; d++) {
+        uploaded_lo[d] = domain->boxlo[d];
+        uploaded_hi[d] = domain->boxhi[d];
+      }
+    }
     status(cacb200_set_state(ctx, na ? &atom->x[0][0] : nullptr, nullptr,
                              ne ? &element->nodex[0][0][0][0] : nullptr, nullptr),
            "set_state");
@@ -182,11 +199,19 @@ void B200Bridge::compute(Pair *pair)
   }
 }
 
-void B200Bridge::run_nve(int nsteps, double dt, int every)
+void B200Bridge::run_nve(int nsteps, double dt, int every, const B200Fixes &fx)
 {
   check_system();
   upload(true);
   status(cacb200_set_neighbor(ctx, neighbor->skin, every), "set_neighbor");
+  if (fx.langevin) {
+    status(cacb200_set_langevin(ctx, fx.t_start, fx.t_stop, fx.t_period, fx.seed, fx.zero), "set_langevin");
+    status(cacb200_set_langevin_stream(ctx, fx.draws), "set_langevin_stream");
+  }
+  if (fx.deform)
+    status(cacb200_set_deform(ctx, fx.deform_every, fx.deform_style, fx.deform_a, fx.deform_b,
+                              fx.deform_remap_x),
+           "set_deform");
   status(cacb200_setup(ctx), "setup");
   status(cacb200_run_nve(ctx, nsteps, dt, 0, 0), "run_nve");
   int na = atom->nlocal, ne = element->nlocal;
@@ -206,6 +231,20 @@ void B200Bridge::run_nve(int nsteps, double dt, int every)
         element->nodef[e][0][n][d] = nf[24 * (size_t)e + 3 * n + d];
         element->gaussf[e][0][n][d] = gbuf[24 * (size_t)e + 3 * n + d];
       }
+  // element centres follow the nodes, as after FixNVE::initial_integrate
+  // (fix_nve.cpp:143)
+  if (ne) element->evec->update_center_coord();
+  if (fx.deform) {
+    // the box the device ended with (FixDeform::update_domain)
+    double lo[3], hi[3], m = 0.0;
+    status(cacb200_get_box(ctx, lo, hi, &m), "get_box");
+    for (int d = 0; d < 3; d++) {
+      domain->boxlo[d] = lo[d];
+      domain->boxhi[d] = hi[d];
+    }
+    domain->set_global_box();
+    domain->set_local_box();
+  }
   uploaded_na = uploaded_ne = -1;   // the reference must set up again (ghosts are stale)
 }
 

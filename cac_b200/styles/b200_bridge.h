@@ -24,6 +24,19 @@ struct cacb200_ctx;
 
 namespace CAC_NS {
 
+// Fixes run_b200 applies on the device besides fix nve (settings read from
+// the langevin/b200 and deform/b200 styles)
+struct B200Fixes {
+  bool langevin = false;
+  double t_start = 0, t_stop = 0, t_period = 1;
+  int seed = 1, zero = 0;
+  long long draws = 1;          // uniform() calls the host generator has made
+  bool deform = false;
+  int deform_every = 1, deform_remap_x = 1;
+  int deform_style[3] = {0, 0, 0};
+  double deform_a[3] = {0, 0, 0}, deform_b[3] = {0, 0, 0};
+};
+
 class B200Bridge : protected Pointers {
  public:
   explicit B200Bridge(class CAC *);
@@ -35,8 +48,9 @@ class B200Bridge : protected Pointers {
   // Pair::compute body: fills atom->f, element->gaussf, eng_vdwl, virial and
   // the per-site arrays of `pair` according to its ev flags.
   void compute(class Pair *pair);
-  // run N velocity-Verlet steps on the device (run_b200 command)
-  void run_nve(int nsteps, double dt, int every);
+  // run N velocity-Verlet steps on the device (run_b200 command), with the
+  // given thermostat / deformation
+  void run_nve(int nsteps, double dt, int every, const B200Fixes &fixes);
   // canonical neighbour-list dump (write_b200_neighbor command)
   void dump_list(const char *file, int half);
 
@@ -49,6 +63,7 @@ class B200Bridge : protected Pointers {
   int eam_nrho = 0, eam_nr = 0;
   double eam_drho = 0, eam_dr = 0, eam_cut = 0;
   int uploaded_na = -1, uploaded_ne = -1;
+  double uploaded_lo[3] = {0, 0, 0}, uploaded_hi[3] = {0, 0, 0};   // box the device holds
   std::vector<double> fbuf, gbuf, ebuf, vbuf, enbuf, vnbuf;
 
   void check_system();

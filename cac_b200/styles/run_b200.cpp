@@ -5,6 +5,8 @@
 #include "cac.h"
 #include "error.h"
 #include "fix.h"
+#include "fix_deform_b200.h"
+#include "fix_langevin_b200.h"
 #include "force.h"
 #include "modify.h"
 #include "neighbor.h"
@@ -34,13 +36,52 @@ void RunB200::command(int narg, char **arg)
   B200Bridge *b = bridge_of(force->pair);
   if (!b) error->all(FLERR, "run_b200 needs pair style lj/cut/b200 or eam/alloy/b200");
   int nve = 0;
+  FixLangevinB200 *lgv = nullptr;
+  FixDeformB200 *dfm = nullptr;
   for (int i = 0; i < modify->nfix; i++) {
-    if (strcmp(modify->fix[i]->style, "nve") == 0) nve++;
-    else error->all(FLERR, "run_b200 integrates fix nve only; remove other fixes");
+    Fix *f = modify->fix[i];
+    if (strcmp(f->style, "nve") == 0) {
+      nve++;
+    } else if (auto *l = dynamic_cast<FixLangevinB200 *>(f)) {
+      if (lgv) error->all(FLERR, "run_b200 takes one fix langevin/b200");
+      lgv = l;
+    } else if (auto *d = dynamic_cast<FixDeformB200 *>(f)) {
+      if (dfm) error->all(FLERR, "run_b200 takes one fix deform/b200");
+      dfm = d;
+    } else {
+      error->all(FLERR, "run_b200 integrates fix nve with fix langevin/b200 and fix deform/b200 only; "
+                        "remove other fixes (use the /b200 forms of langevin and deform)");
+    }
   }
   if (nve != 1) error->all(FLERR, "run_b200 needs exactly one fix nve");
   cac->init();   // pair init_style/init_one push the tables to the bridge
-  b->run_nve(nsteps, update->dt, neighbor->every);
+  B200Fixes fx;
+  if (lgv) {
+    if (!lgv->device_ok())
+      error->all(FLERR, "run_b200: fix langevin/b200 needs group all and constant temperatures");
+    fx.langevin = true;
+    fx.t_start = lgv->start();
+    fx.t_stop = lgv->stop();
+    fx.t_period = lgv->damp();
+    fx.seed = lgv->seed_value();
+    fx.zero = lgv->zero();
+    fx.draws = lgv->draws;
+  }
+  if (dfm) {
+    if (!dfm->device_ok())
+      error->all(FLERR, "run_b200: fix deform/b200 needs group all, an orthogonal box, no tilt and remap x or none");
+    fx.deform = true;
+    fx.deform_every = dfm->every();
+    fx.deform_remap_x = dfm->remap_x();
+    for (int d = 0; d < 3; d++) {
+      fx.deform_style[d] = dfm->device_style(d, fx.deform_a[d], fx.deform_b[d]);
+      if (fx.deform_style[d] < 0) error->all(FLERR, "run_b200: fix deform/b200 variable styles are not offered");
+    }
+  }
+  b->run_nve(nsteps, update->dt, neighbor->every, fx);
+  // the host generator continues after the device's draws: the run's setup
+  // call and one call per step
+  if (lgv) lgv->advance((long long)(nsteps + 1) * lgv->draws_per_call());
   update->ntimestep += nsteps;
 }
 

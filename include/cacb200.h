@@ -123,6 +123,12 @@ int cacb200_thermo(cacb200_ctx *ctx, int units, double *out /* [nreplicas][CACB2
 
 /* Box and mass of a single system (not a batch). */
 int cacb200_get_box(cacb200_ctx *ctx, double boxlo[3], double boxhi[3], double *mass);
+/* A new periodic box for a single system, sites left where they are (the
+ * device side of Domain::set_global_box after a host loop changed the box,
+ * domain.cpp:227-238, e.g. the reference's own fix deform between list
+ * rebuilds; new positions follow through cacb200_set_state).  Lists are kept;
+ * the next rebuild plans its grids for the new box. */
+int cacb200_set_box(cacb200_ctx *ctx, const double boxlo[3], const double boxhi[3]);
 
 /* ------------------------------------------------------------- data files */
 
@@ -226,6 +232,11 @@ int cacb200_run_nve(cacb200_ctx *ctx, int nsteps, double dt, int eflag, int vfla
  * min_post_force). */
 int cacb200_set_langevin(cacb200_ctx *ctx, double t_start, double t_stop, double t_period, int seed,
                          int zero);
+/* Position every replica's stream after `draws` uniform() calls of its
+ * RanMars (the constructor's warm-up is draw 1; FixLangevin draws 3 per atom
+ * and 24 per element each post_force), so that a run continues a stream the
+ * reference's own loop has been drawing from (the fix langevin/b200 style). */
+int cacb200_set_langevin_stream(cacb200_ctx *ctx, long long draws);
 int cacb200_unset_langevin(cacb200_ctx *ctx);
 
 /* fix ID all deform N x|y|z style args ... remap x|none units box on an

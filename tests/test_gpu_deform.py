@@ -151,3 +151,29 @@ def test_run_starts_from_forces_of_current_positions(tmp_path):
     r.close()
     assert not np.array_equal(f0, f1)
     assert rel_err(f1, fr) < 1e-13   # lists built from other positions: summation order may differ
+
+
+def test_set_box_matches_fresh_upload(tmp_path):
+    """A new box through cacb200_set_box (lists kept) gives the forces of the
+    same positions uploaded in that box (lists built for it)."""
+    from cac_b200.api import ENERGY_GLOBAL, VIRIAL_GLOBAL
+    s = CASES["tiny_lj"][0]()
+    lo = np.asarray(s.boxlo, dtype=np.float64)
+    hi = np.asarray(s.boxhi, dtype=np.float64) + np.array([0.03, -0.02, 0.01])
+    e = make_engine(s, "lj", tmp_path)
+    e.setup()
+    e.set_box(lo, hi)
+    e.compute(ENERGY_GLOBAL, VIRIAL_GLOBAL)
+    f1, nf1, _ = e.forces()
+    ev1 = e.energy(peratom=False)
+    e.close()
+    s2 = CASES["tiny_lj"][0]()
+    s2.boxhi = hi
+    r = make_engine(s2, "lj", tmp_path)
+    r.compute(ENERGY_GLOBAL, VIRIAL_GLOBAL)
+    f2, nf2, _ = r.forces()
+    ev2 = r.energy(peratom=False)
+    r.close()
+    assert rel_err(f1, f2) < 1e-13
+    assert rel_err(nf1, nf2) < 1e-13
+    assert abs(ev1["energy"] - ev2["energy"]) < 1e-12 * abs(ev2["energy"])

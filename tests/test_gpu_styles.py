@@ -91,3 +91,76 @@ def test_device_lists_written_by_the_style(case, golden, tmp_path):
         rows = O.read_neigh(str(tmp_path / f"{key}.txt"), s.natoms)
         assert np.array_equal(counts(rows, nsites), g[key + "_counts"])
         assert digest(rows) == str(g[key + "_digest"])
+
+
+def lgv_fix(g):
+    t0, t1, damp, seed, zero = (float(v) for v in g["lgv_params"])
+    return f"fix 2 all langevin/b200 {t0!r} {t1!r} {damp!r} {int(seed)} zero {'yes' if zero else 'no'}\n"
+
+
+def dfm_fix(g):
+    names = ("none", "final", "delta", "scale", "vel", "erate", "trate", "wiggle", "volume")
+    nargs = {"final": 2, "delta": 2, "wiggle": 2, "scale": 1, "vel": 1, "erate": 1, "trate": 1, "volume": 0}
+    parts = []
+    for d in range(3):
+        st = names[int(g["dfm_style"][d])]
+        if st == "none":
+            continue
+        vals = (float(g["dfm_a"][d]), float(g["dfm_b"][d]))[:nargs[st]]
+        parts.append(" ".join(["xyz"[d], st] + [repr(v) for v in vals]))
+    return f"fix 3 all deform/b200 {int(g['dfm_nevery'])} {' '.join(parts)} units box remap x\n"
+
+
+def assert_state(e, g, prefix):
+    assert np.abs(e["x"] - g[prefix + "x"]).max() < 1e-10
+    assert np.abs(e["nodex"] - g[prefix + "nodex"]).max() < 1e-10
+    assert rel_err(e["v"], g[prefix + "v"]) < TOL
+    assert rel_err(e["nodev"], g[prefix + "nodev"]) < TOL
+    assert rel_err(e["f"], g[prefix + "f"]) < TOL
+    assert rel_err(e["nodef"], g[prefix + "nodef"]) < TOL
+
+
+@pytest.mark.parametrize("order", [("run", "run_b200"), ("run_b200", "run")])
+def test_langevin_style_mixes_reference_loop_and_device(order, golden, tmp_path):
+    """fix langevin/b200 draws the reference's RanMars stream in both loops:
+    20 steps in one and 20 in the other reproduce the reference's own
+    fix langevin over two runs (the device continues the host generator, and
+    the host generator is advanced past the device's draws)."""
+    g = golden("tiny_lj")
+    runs = [int(n) for n in g["lgv_runs"]]
+    body = lgv_fix(g) + f"{order[0]} {runs[0]}\n{order[1]} {runs[1]}\noracle_dump end.txt state\n"
+    s, O = run_app(tmp_path, "tiny_lj", body)
+    assert_state(O.read_dump(str(tmp_path / "end.txt")), g, "lgv_end_")
+
+
+def test_langevin_style_run_b200_eam(golden, tmp_path):
+    g = golden("tiny_eam")
+    body = lgv_fix(g) + f"run_b200 {int(g['lgv_runs'][0])}\noracle_dump end.txt state\n"
+    s, O = run_app(tmp_path, "tiny_eam", body)
+    assert_state(O.read_dump(str(tmp_path / "end.txt")), g, "lgv_end_")
+
+
+@pytest.mark.parametrize("case,order", [("tiny_lj", ("run", "run_b200")), ("tiny_lj", ("run_b200", "run")),
+                                        ("tiny_eam", ("run_b200",))])
+def test_deform_style_mixes_reference_loop_and_device(case, order, golden, tmp_path):
+    """fix deform/b200 in the reference loop and on the device: the box and
+    the state equal the reference's own fix deform over the same runs."""
+    g = golden(case)
+    runs = [int(n) for n in g["dfm_runs"]]
+    body = dfm_fix(g) + "".join(f"{m} {n}\n" for m, n in zip(order, runs)) + "oracle_dump end.txt state\n"
+    s, O = run_app(tmp_path, case, body)
+    e = O.read_dump(str(tmp_path / "end.txt"))
+    assert np.array_equal(e["box"], g["dfm_end_box"])
+    assert_state(e, g, "dfm_end_")
+
+
+def test_run_b200_refuses_plain_langevin(tmp_path):
+    import oracle  # noqa: F401
+    build, pair, _ = CASES["tiny_lj"]
+    s = build()
+    gen.write_data(s, str(tmp_path / "data.cac"))
+    (tmp_path / "in.cac").write_text(HEADER + pair_lines("lj") + TAIL +
+                                     "fix 2 all langevin 10.0 10.0 0.1 5\nrun_b200 5\n")
+    r = subprocess.run([APP, "-in", "in.cac"], cwd=tmp_path, capture_output=True, text=True, timeout=600)
+    assert r.returncode != 0
+    assert "langevin/b200" in r.stdout + r.stderr
