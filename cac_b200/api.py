@@ -75,6 +75,10 @@ SIGNATURES = [
     ("cacb200_server_submit", C.c_int, [C.c_void_p, C.c_int, _dp, _dp, C.c_int, _dp, _dp, C.c_int, _dp, _dp,
                                         C.c_double, C.c_int, C.c_double, C.c_double, C.c_double,
                                         C.POINTER(C.c_int64)]),
+    ("cacb200_server_submit_nvt", C.c_int, [C.c_void_p, _dp, _dp, C.c_int, _dp, _dp, C.c_int, _dp, _dp,
+                                            C.c_double, C.c_int, C.c_double, C.c_double, C.c_double, C.c_double,
+                                            C.c_int, C.c_int, C.POINTER(C.c_int64)]),
+    ("cacb200_server_thermo", C.c_int, [C.c_void_p, C.c_int64, _dp]),
     ("cacb200_server_wait", C.c_int, [C.c_void_p, C.c_int64, C.c_double]),
     ("cacb200_server_result", C.c_int, [C.c_void_p, C.c_int64, _dp, _dp, _dp, _dp, _dp, C.POINTER(C.c_int),
                                         C.POINTER(C.c_int), _dp]),
@@ -530,6 +534,29 @@ class Server:
                                                    etol, ftol, C.byref(job)), "server_submit")
         self._shapes[job.value] = (x.shape[0], nx.shape[0])
         return job.value
+
+    def submit_nvt(self, system, steps: int, dt: float, t_start: float, t_stop: float, damp: float, seed: int,
+                   zero: bool = False) -> int:
+        """An NVE job under ``fix langevin t_start t_stop damp seed [zero yes]``."""
+        x = np.ascontiguousarray(system.x, dtype=np.float64)
+        v = np.ascontiguousarray(system.v, dtype=np.float64)
+        nx = np.ascontiguousarray(system.nodex, dtype=np.float64)
+        nv = np.ascontiguousarray(system.nodev, dtype=np.float64)
+        lo = np.ascontiguousarray(system.boxlo, dtype=np.float64)
+        hi = np.ascontiguousarray(system.boxhi, dtype=np.float64)
+        job = C.c_int64()
+        self._check(self.lib.cacb200_server_submit_nvt(self.h, _p(lo), _p(hi), x.shape[0], _p(x), _p(v),
+                                                       nx.shape[0], _p(nx), _p(nv), float(system.mass), steps, dt,
+                                                       t_start, t_stop, damp, seed, 1 if zero else 0,
+                                                       C.byref(job)), "server_submit_nvt")
+        self._shapes[job.value] = (x.shape[0], nx.shape[0])
+        return job.value
+
+    def thermo(self, job: int) -> dict:
+        """The job's thermo line at its end (Engine.THERMO_FIELDS, metal units)."""
+        out = np.zeros(len(Engine.THERMO_FIELDS))
+        self._check(self.lib.cacb200_server_thermo(self.h, job, _p(out)), "server_thermo")
+        return {k: float(out[i]) for i, k in enumerate(Engine.THERMO_FIELDS)}
 
     def wait(self, job: int, timeout: float = -1.0) -> int:
         """The job's status once it ends (0 = done), or CACB200_ETIMEDOUT."""

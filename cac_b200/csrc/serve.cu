@@ -34,11 +34,16 @@ struct Job {
   double mass = 1.0;
   int steps = 0;          // NVE steps or FIRE iteration cap
   double dt = 0.001, etol = 0.0, ftol = 0.0;
+  // NVE under fix langevin (cacb200_server_submit_nvt)
+  bool langevin = false;
+  double lgv_t0 = 0, lgv_t1 = 0, lgv_damp = 1;
+  int lgv_seed = 1, lgv_zero = 0;
   size_t bytes = 0;       // device-memory estimate used for admission
   // results
   int status = 1;         // 1 queued, 2 running, then a CACB200_* code
   std::string error;
   double energy = 0.0;
+  double thermo[CACB200_THERMO_N] = {};   // the job's last state, metal units
   int niter = 0, stop_code = -1;
   Clock::time_point t_submit, t_start, t_end;
 };
@@ -102,7 +107,8 @@ int execute(cacb200_ctx *c, Job &j, int segment) {
   if (rc) return rc;
   if (j.kind == CACB200_JOB_NVE) {
     const int seg = (segment > 0 && segment < j.steps) ? segment : j.steps;
-    if (seg < j.steps) rc = cacb200_snapshot(c);
+    if (j.langevin) rc = cacb200_set_langevin(c, j.lgv_t0, j.lgv_t1, j.lgv_damp, j.lgv_seed, j.lgv_zero);
+    if (!rc && seg < j.steps) rc = cacb200_snapshot(c);
     if (!rc) rc = cacb200_setup(c);
     for (int done = 0; !rc && done < j.steps;) {
       if (done > 0) {
@@ -112,15 +118,21 @@ int execute(cacb200_ctx *c, Job &j, int segment) {
       }
       int k = std::min(seg, j.steps - done);
       done += k;
-      rc = cacb200_run_nve(c, k, j.dt, done == j.steps ? CACB200_ENERGY_GLOBAL : 0, 0);
+      const bool last = done == j.steps;
+      rc = cacb200_run_nve(c, k, j.dt, last ? CACB200_ENERGY_GLOBAL : 0, last ? CACB200_VIRIAL_GLOBAL : 0);
     }
+    // a run of 0 steps ends on the setup evaluation, which tallied both
     double vir[6];
     if (!rc) rc = cacb200_get_energy(c, &j.energy, vir, nullptr, nullptr, nullptr, nullptr);
     j.niter = j.steps;
   } else {
     double fnorm = 0.0;
     rc = cacb200_minimize_fire(c, j.etol, j.ftol, j.steps, j.dt, 1, &j.stop_code, &j.niter, &j.energy, &fnorm);
+    // the minimiser tallies energies only: one more evaluation of the final
+    // positions for the pressure (forces and energy unchanged)
+    if (!rc) rc = cacb200_compute_forces(c, CACB200_ENERGY_GLOBAL, CACB200_VIRIAL_GLOBAL);
   }
+  if (!rc) rc = cacb200_thermo(c, CACB200_UNITS_METAL, j.thermo);
   if (!rc) rc = cacb200_get_state(c, j.x.data(), j.v.data(), j.nodex.data(), j.nodev.data());
   return rc;
 }
@@ -245,10 +257,12 @@ int cacb200_server_start(cacb200_server *s) {
   return CACB200_OK;
 }
 
-int cacb200_server_submit(cacb200_server *s, int kind, const double boxlo[3], const double boxhi[3], int natoms,
-                          const double *x, const double *v, int nelements, const double *nodex,
-                          const double *nodev, double mass, int steps, double dt, double etol, double ftol,
-                          int64_t *job) {
+namespace {
+
+int submit_job(cacb200_server *s, int kind, const double boxlo[3], const double boxhi[3], int natoms,
+               const double *x, const double *v, int nelements, const double *nodex, const double *nodev,
+               double mass, int steps, double dt, double etol, double ftol, const Job *thermostat,
+               int64_t *job) {
   if (!s || !job) return CACB200_EINVAL;
   if ((kind != CACB200_JOB_NVE && kind != CACB200_JOB_FIRE) || !boxlo || !boxhi || natoms < 0 || nelements < 0 ||
       (natoms && (!x || !v)) || (nelements && (!nodex || !nodev)) || steps < 0 || !(dt > 0.0)) {
@@ -275,6 +289,14 @@ int cacb200_server_submit(cacb200_server *s, int kind, const double boxlo[3], co
   j->dt = dt;
   j->etol = etol;
   j->ftol = ftol;
+  if (thermostat) {
+    j->langevin = true;
+    j->lgv_t0 = thermostat->lgv_t0;
+    j->lgv_t1 = thermostat->lgv_t1;
+    j->lgv_damp = thermostat->lgv_damp;
+    j->lgv_seed = thermostat->lgv_seed;
+    j->lgv_zero = thermostat->lgv_zero;
+  }
   j->bytes = job_bytes(natoms, nelements);
   std::lock_guard<std::mutex> g(s->m);
   if (!s->started || s->stopping) {
@@ -291,6 +313,56 @@ int cacb200_server_submit(cacb200_server *s, int kind, const double boxlo[3], co
   s->queue.push_back(j.get());
   s->jobs[j->id] = std::move(j);
   s->cv_work.notify_all();
+  return CACB200_OK;
+}
+
+}  // namespace
+
+int cacb200_server_submit(cacb200_server *s, int kind, const double boxlo[3], const double boxhi[3], int natoms,
+                          const double *x, const double *v, int nelements, const double *nodex,
+                          const double *nodev, double mass, int steps, double dt, double etol, double ftol,
+                          int64_t *job) {
+  return submit_job(s, kind, boxlo, boxhi, natoms, x, v, nelements, nodex, nodev, mass, steps, dt, etol, ftol,
+                    nullptr, job);
+}
+
+int cacb200_server_submit_nvt(cacb200_server *s, const double boxlo[3], const double boxhi[3], int natoms,
+                              const double *x, const double *v, int nelements, const double *nodex,
+                              const double *nodev, double mass, int steps, double dt, double t_start,
+                              double t_stop, double damp, int seed, int zero, int64_t *job) {
+  // the fix's own checks up front (FixLangevin::FixLangevin, fix_langevin.cpp:40-60)
+  if (!(damp > 0.0) || seed <= 0 || seed > 900000000 || !(t_start >= 0.0) || !(t_stop >= 0.0)) {
+    if (s) {
+      std::lock_guard<std::mutex> g(s->m);
+      s->last_error = "invalid fix langevin settings";
+    }
+    return CACB200_EINVAL;
+  }
+  Job t;
+  t.lgv_t0 = t_start;
+  t.lgv_t1 = t_stop;
+  t.lgv_damp = damp;
+  t.lgv_seed = seed;
+  t.lgv_zero = zero;
+  return submit_job(s, CACB200_JOB_NVE, boxlo, boxhi, natoms, x, v, nelements, nodex, nodev, mass, steps, dt, 0.0,
+                    0.0, &t, job);
+}
+
+int cacb200_server_thermo(cacb200_server *s, int64_t job, double *out) {
+  if (!s || !out) return CACB200_EINVAL;
+  std::lock_guard<std::mutex> g(s->m);
+  auto it = s->jobs.find(job);
+  if (it == s->jobs.end()) {
+    s->last_error = "unknown job";
+    return CACB200_EINVAL;
+  }
+  Job *j = it->second.get();
+  if (j->status > 0) return CACB200_ESTATE;
+  if (j->status < 0) {
+    s->last_error = j->error;
+    return j->status;
+  }
+  std::memcpy(out, j->thermo, sizeof(j->thermo));
   return CACB200_OK;
 }
 

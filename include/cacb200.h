@@ -378,6 +378,20 @@ int cacb200_server_submit(cacb200_server *s, int kind, const double boxlo[3], co
  * (CACB200_OK, CACB200_ETIMEDOUT while still queued or running, or the
  * job's error code). */
 int cacb200_server_wait(cacb200_server *s, int64_t job, double timeout_s);
+/* An NVE job under fix langevin t_start t_stop damp seed [zero yes]
+ * (cacb200_set_langevin semantics: the reference's RanMars stream for `seed`,
+ * started with the job; with segmented NVE the stream runs on across the
+ * restarts).  Its results equal the same run on one context bit for bit. */
+int cacb200_server_submit_nvt(cacb200_server *s, const double boxlo[3], const double boxhi[3],
+                              int natoms, const double *x, const double *v, int nelements,
+                              const double *nodex, const double *nodev, double mass, int steps,
+                              double dt, double t_start, double t_stop, double damp, int seed,
+                              int zero, int64_t *job);
+/* The job's thermo line at its end (cacb200_thermo, metal units:
+ * CACB200_THERMO_N doubles), reduced on the device before the state is read
+ * back.  NVE jobs tally energy and virial on their last step; FIRE jobs
+ * evaluate their final positions once more for the virial. */
+int cacb200_server_thermo(cacb200_server *s, int64_t job, double *out /* [CACB200_THERMO_N] */);
 /* Final state, energy (eng_vdwl), iterations and FIRE stop code (-1 for
  * NVE), and times in seconds: [queued, running, submit to end] (times are
  * filled for failed jobs too, which return their error code). */

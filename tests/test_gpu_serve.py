@@ -86,3 +86,50 @@ def test_budget_admission(tmp_path):
     for j in ids:
         assert srv.wait(j) == 0, srv.last_error()
     srv.close()
+
+
+def test_served_nvt_and_thermo_equal_alone(tmp_path):
+    """NVT jobs (fix langevin) served beside NVE and FIRE jobs equal the same
+    run on one context bit for bit, and each job's device thermo line equals
+    the context's read-out after that run."""
+    from cac_b200.api import ENERGY_GLOBAL, VIRIAL_GLOBAL, Engine, Server
+    setfl = setfl_path(tmp_path)
+    js = jobs()[:4]
+    lgv = (150.0, 250.0, 0.05, 8811, True)
+    srv = Server(0, workers=3, budget_gb=8.0, precision=0)
+    srv.pair_eam(setfl)
+    srv.neighbor(SKIN, 10)
+    srv.start()
+    ids = []
+    for k, (s, kind) in enumerate(js):
+        if k % 2 == 0:
+            ids.append((srv.submit_nvt(s, NVE_STEPS, 0.001, *lgv), "nvt"))
+        else:
+            ids.append((srv.submit(s, kind, NVE_STEPS if kind == 0 else FIRE_ITERS, 0.001, 0.0, FTOL),
+                        "nve" if kind == 0 else "fire"))
+    for j, _ in ids:
+        assert srv.wait(j) == 0, srv.last_error()
+    for (s, kind), (j, what) in zip(js, ids):
+        x, v, nx, nv, energy, _, _, _ = srv.result(j)
+        th = srv.thermo(j)
+        e = Engine(0)
+        e.upload(s)
+        e.pair_eam(setfl)
+        e.neighbor(SKIN, 10)
+        if what == "fire":
+            e.minimize_fire(0.0, FTOL, FIRE_ITERS, 0.001, norm="max")
+            e.compute(ENERGY_GLOBAL, VIRIAL_GLOBAL)
+        else:
+            if what == "nvt":
+                e.langevin(*lgv)
+            e.setup()
+            e.run_nve(NVE_STEPS, 0.001, ENERGY_GLOBAL, VIRIAL_GLOBAL)
+        ref = e.thermo()
+        xr, vr, nxr, nvr = e.state()
+        e.close()
+        assert np.array_equal(x, xr) and np.array_equal(v, vr), what
+        assert np.array_equal(nx, nxr) and np.array_equal(nv, nvr), what
+        for key, val in ref.items():
+            assert th[key] == val, (what, key)
+        srv.release(j)
+    srv.close()
