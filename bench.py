@@ -20,6 +20,11 @@ total energy rises by thousands of eV within 300 steps, LJ and EAM alike), so
 long trajectories stop being physical; the restarts keep the timed work on
 physical configurations.
 
+``--fix langevin`` / ``--fix deform`` time the same trajectories under the
+reference's fix langevin (300 K, damp 0.1 ps) or fix deform (x erate 0.1/ps,
+y volume; each restart also restores the seeded box); the default is fix nve
+alone.  ``thermo_readout_ms`` is the host time of one device thermo read-out.
+
 ``--gpus N`` (launched under torchrun) runs N independent replicas, one per
 GPU, with no collective on the data path ("replicas only"); value is the sum.
 
@@ -372,6 +377,13 @@ def b200_arm(args, rank, local, ws, dist):
         eng.pair_lj(0.4093, 2.338, 5.5)
     eng.set_precision(api.MIXED if args.form == "mixed" else api.FP64)
     eng.neighbor(1.0, 10)
+    if args.fix == "langevin":
+        eng.langevin(300.0, 300.0, 0.1, 4928459)
+    elif args.fix == "deform":
+        if batch:
+            raise SystemExit("--fix deform times a single system")
+        box0 = (np.asarray(s.boxlo, dtype=np.float64), np.asarray(s.boxhi, dtype=np.float64))
+        eng.deform(1, x=("erate", 0.1), y=("volume",))
     eng.setup()
     eng.snapshot()
     stream = torch.cuda.ExternalStream(eng.stream, device=torch.device("cuda", local))
@@ -379,11 +391,14 @@ def b200_arm(args, rank, local, ws, dist):
 
     def trajectory(nsteps: int, first: bool):
         """nsteps of velocity Verlet as segments of at most `seg` steps, each
-        from the seeded initial state (restore + list build + forces)."""
+        from the seeded initial state (restore + list build + forces; with a
+        deforming box, the seeded box too)."""
         done = 0
         while done < nsteps:
             if not (first and done == 0):
                 eng.restore()
+                if args.fix == "deform":
+                    eng.set_box(*box0)
                 eng.setup()
             k = min(seg, nsteps - done)
             eng.run_nve(k, 0.001)
@@ -417,6 +432,12 @@ def b200_arm(args, rank, local, ws, dist):
     eng.run_nve(nprof, 0.001)
     prof = eng.profile_read()
     eng.profile(False)
+    # thermo read-out on the device: reduction plus one small copy, host wall time
+    eng.thermo()
+    t_th = time.perf_counter()
+    for _ in range(20):
+        eng.thermo()
+    thermo_ms = (time.perf_counter() - t_th) / 20 * 1000.0
     timed = {k: v for k, v in prof.items() if alg_bytes_per_site(k) > 0}
     top = max(prof.items(), key=lambda kv: kv[1][0])
     dom = max(timed.items(), key=lambda kv: kv[1][0]) if timed else top
@@ -504,6 +525,8 @@ def b200_arm(args, rank, local, ws, dist):
                        "replicas": len(s) if batch else 1,
                        "pair": "eam/alloy" if pair == "eam" else "lj/cut", "precision": args.form,
                        "rebuild_every": 10, "parallelism": f"replicas x{ws} (no data-path collective)",
+                       "fix": {"none": "nve", "langevin": "nve + langevin 300 300 0.1",
+                               "deform": "nve + deform 1 x erate 0.1 y volume"}[args.fix],
                        "l2": "working set larger than L2 (site table + lists > 126 MB)"},
             "roofline": {"bound": "hbm", "kernel": dom[0], "achieved": achieved, "peak": hbm,
                          "peak_kind": hbm_kind, "unit": "GB/s", "frac": achieved / hbm,
@@ -520,6 +543,7 @@ def b200_arm(args, rank, local, ws, dist):
                     "d2h_bytes_per_step": bytes_state, "steps": k_e2e},
             "gpu_launches": int(round(launches_per_step * args.steps)),
             "tuned_blocks": dict(zip(("rho", "force"), tuned)),
+            "thermo_readout_ms": thermo_ms,
             "clocks": clk.summary(),
         }
         print(json.dumps(line))
@@ -655,6 +679,8 @@ def main():
     ap.add_argument("--workload", default="eam_1m")
     ap.add_argument("--form", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--fix", default="none", choices=["none", "langevin", "deform"],
+                    help="integrate with fix langevin or fix deform besides fix nve")
     ap.add_argument("--jobs", type=int, default=64, help="serve workload: jobs in the stream")
     ap.add_argument("--workers", type=int, default=8, help="serve workload: worker contexts")
     ap.add_argument("--serial-jobs", type=int, default=8,

@@ -34,7 +34,7 @@ namespace {
 constexpr unsigned MASK24 = (1u << 24) - 1;
 constexpr int WIN = 97;          // window of the long lag
 constexpr int EXT = 2 * WIN - 1; // window plus the 96 values after it
-constexpr int CHUNK = 2048;      // draws per warp
+constexpr int CHUNK = 512;       // draws per warp
 constexpr int WARPS = 4;         // warps (chunks) per block
 constexpr long long C0 = 362436, CD = 7654321, CM = 16777213;
 constexpr double FTM2V = 1.0 / 1.0364269e-4;   // update.cpp:160-164 (metal)
@@ -169,7 +169,7 @@ __device__ __forceinline__ double target_sqrt(const LgvArgs &A) {
 __global__ void __launch_bounds__(32 * WARPS) k_langevin(LgvArgs A) {
   __shared__ unsigned sb[WARPS][EXT];
   __shared__ unsigned sp[WARPS][WIN];
-  __shared__ unsigned ring[WARPS][128];
+  __shared__ unsigned seq[WARPS][WIN + CHUNK];   // seq[rho] = Y_{B-96+jC+rho}
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int ci = blockIdx.x * WARPS + w;
   if (ci >= A.nchunks) return;   // the whole warp leaves; only warp barriers follow
@@ -181,11 +181,21 @@ __global__ void __launch_bounds__(32 * WARPS) k_langevin(LgvArgs A) {
   for (int i = lane; i < EXT; i += 32) sb[w][i] = A.base[(size_t)r * EXT + i];
   for (int i = lane; i < WIN; i += 32) sp[w][i] = A.poly[(size_t)j * WIN + i];
   __syncwarp();
-  // window at the chunk's offset: ring[s] = Y_{B-96+jC+s}
+  // window at the chunk's offset
   for (int s = lane; s < WIN; s += 32) {
     unsigned long long acc = 0;
     for (int i = 0; i < WIN; i++) acc += (unsigned long long)sp[w][i] * sb[w][s + i];
-    ring[w][s] = (unsigned)(acc & MASK24);
+    seq[w][s] = (unsigned)(acc & MASK24);
+  }
+  const long long qbase = (long long)j * CHUNK;
+  const int len = (int)min((long long)CHUNK, N - qbase);
+  // the chunk's values, 32 per step (the short lag is 33), all in shared
+  // memory before any force is touched
+  for (int t0 = 0; t0 < len; t0 += 32) {
+    __syncwarp();
+    const int t = t0 + lane;
+    const unsigned y = (seq[w][t] - seq[w][t + 64]) & MASK24;
+    seq[w][WIN + t] = y;
   }
   __syncwarp();
 
@@ -193,8 +203,6 @@ __global__ void __launch_bounds__(32 * WARPS) k_langevin(LgvArgs A) {
   const double g1 = A.gfactor1;
   const double g2a = __dmul_rn(A.gfactor2, tsqrt);
   const double g2n = __ddiv_rn(__dmul_rn(A.gfactor2, tsqrt), A.sqrt_nodal_weight);
-  const long long qbase = (long long)j * CHUNK;
-  const int len = (int)min((long long)CHUNK, N - qbase);
   // C of this lane's first draw, then 32 draws further on per step
   const unsigned long long first = A.m[r] + 1 + qbase + lane;
   long long cm = (C0 - (long long)((first % CM) * CD % CM) + CM) % CM;
@@ -205,32 +213,28 @@ __global__ void __launch_bounds__(32 * WARPS) k_langevin(LgvArgs A) {
   double *fn = A.nodef + 24LL * mt.z;
   const double *vn = A.nodev + 24LL * mt.z;
   unsigned *nx = A.next + (size_t)r * WIN;
-  for (int t0 = 0; t0 < len; t0 += 32) {
-    const int t = t0 + lane;
-    const int rho = WIN + t;   // ring position of Y_{B+jC+1+t}
-    const unsigned y = (ring[w][(rho - WIN) & 127] - ring[w][(rho - 33) & 127]) & MASK24;
-    __syncwarp();
-    ring[w][rho & 127] = y;
-    __syncwarp();
-    if (t < len) {
-      const long long q = qbase + t;
-      const unsigned u = (y - (unsigned)cm) & MASK24;
-      const double uni = (double)u * (1.0 / 16777216.0);
-      double fran;
-      if (q < na3) {
-        fran = __dmul_rn(g2a, uni - 0.5);
-        fa[q] = __dadd_rn(fa[q], __dadd_rn(__dmul_rn(g1, va[q]), fran));
-      } else {
-        const long long k = q - na3;
-        fran = __dmul_rn(g2n, uni - 0.5);
-        fn[k] = __dadd_rn(fn[k], __dadd_rn(__dmul_rn(g1, vn[k]), fran));
-      }
-      const int d = (int)(q % 3);
-      fs[0] += d == 0 ? fran : 0.0;
-      fs[1] += d == 1 ? fran : 0.0;
-      fs[2] += d == 2 ? fran : 0.0;
-      if (q >= N - WIN && N >= WIN) nx[q - (N - WIN)] = y;
+  // draw q = qbase + t on force component q of the atoms, then of the nodes;
+  // no barrier in this loop, so the loads of successive steps overlap
+#pragma unroll 4
+  for (int t = lane; t < len; t += 32) {
+    const unsigned y = seq[w][WIN + t];
+    const long long q = qbase + t;
+    const unsigned u = (y - (unsigned)cm) & MASK24;
+    const double uni = (double)u * (1.0 / 16777216.0);
+    double fran;
+    if (q < na3) {
+      fran = __dmul_rn(g2a, uni - 0.5);
+      fa[q] = __dadd_rn(fa[q], __dadd_rn(__dmul_rn(g1, va[q]), fran));
+    } else {
+      const long long k = q - na3;
+      fran = __dmul_rn(g2n, uni - 0.5);
+      fn[k] = __dadd_rn(fn[k], __dadd_rn(__dmul_rn(g1, vn[k]), fran));
     }
+    const int d = (int)(q % 3);
+    fs[0] += d == 0 ? fran : 0.0;
+    fs[1] += d == 1 ? fran : 0.0;
+    fs[2] += d == 2 ? fran : 0.0;
+    if (q >= N - WIN && N >= WIN) nx[q - (N - WIN)] = y;
     cm -= cstep;
     if (cm < 0) cm += CM;
   }
