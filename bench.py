@@ -61,8 +61,20 @@ def peaks():
         return 6650.0, "fallback"
 
 
-def build_workload(name: str, seed: int):
-    from cac_b200 import gen
+def batch_share(specs, rank: int, ws: int):
+    """Indices of a rank's replicas: greedy split by size (atoms + 8 x elements)."""
+    from cac_b200 import shard
+    return shard.balanced_partition([ta + 8 * te for ta, te, _, _, _ in specs], ws)[rank]
+
+
+def build_workload(name: str, seed: int, rank: int = 0, ws: int = 1):
+    """A rank's workload.  Single systems: one replica per rank (seeded by
+    rank).  Batches: one global set of 256 replicas per GPU, split over the
+    ranks by the size-balanced greedy rule (each rank builds its own share)."""
+    from cac_b200 import gen, shard
+    if name == "batch256" and ws > 1:
+        specs = gen.replica_specs(256 * ws, seed=13)
+        return [gen.replica_from_spec(specs[i]) for i in batch_share(specs, rank, ws)], "eam"
     if name == "eam_1m":
         return gen.eam_1m(seed=seed), "eam"
     if name == "lj_small":
@@ -359,9 +371,12 @@ def b200_arm(args, rank, local, ws, dist):
     import torch
     from cac_b200 import api, gen
 
+    from cac_b200 import shard
     seed = rank_seed(2, rank)
-    s, pair = build_workload(args.workload, seed)
+    s, pair = build_workload(args.workload, seed, rank, ws)
     units, natoms, nelements = totals(s)
+    dev = torch.device("cuda", local)
+    units_all = shard.sum_over_ranks(units, dist, dev)
     batch = isinstance(s, list)
     eng = api.Engine(local)
     if batch:
@@ -422,7 +437,7 @@ def b200_arm(args, rank, local, ws, dist):
             dist.barrier()
     ms = e0.elapsed_time(e1)
     ms_max = max_over_ranks(ms, dist, torch.device("cuda", local))
-    value = whole_job_rate(units, args.steps, ws, ms_max / 1000.0)
+    value = units_all * args.steps / (ms_max / 1000.0)
 
     # per-kernel device times (CUDA events around every launch) for the roofline
     nprof = min(seg, 50)
@@ -489,7 +504,7 @@ def b200_arm(args, rank, local, ws, dist):
         eng.run_nve(1, 0.001)
         eng._check(eng.lib.cacb200_get_state(eng.h, _p(x_h), _p(v_h), _p(nx_h), _p(nv_h)), "get_state")
     e2e_s = max_over_ranks(time.perf_counter() - t0, dist, torch.device("cuda", local))
-    e2e_value = whole_job_rate(units, k_e2e, ws, e2e_s)
+    e2e_value = units_all * k_e2e / e2e_s
     bytes_state = 8 * (6 * natoms + 48 * nelements)
 
     # CPU baseline: the reference on a bounded sample of the same workload
@@ -521,10 +536,13 @@ def b200_arm(args, rank, local, ws, dist):
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.form == "fp64" else "f32/f64",
             "data": "synthetic (seeded generator; no dataset exists for this path)",
-            "config": {"workload": args.workload, "sites": units, "atoms": natoms, "elements": nelements,
-                       "replicas": len(s) if batch else 1,
+            "config": {"workload": args.workload, "sites": int(units_all), "sites_rank0": units,
+                       "atoms_rank0": natoms, "elements_rank0": nelements,
+                       "replicas_rank0": len(s) if batch else 1,
                        "pair": "eam/alloy" if pair == "eam" else "lj/cut", "precision": args.form,
-                       "rebuild_every": 10, "parallelism": f"replicas x{ws} (no data-path collective)",
+                       "rebuild_every": 10,
+                       "parallelism": (f"{ws} ranks, replicas split by size (greedy), no data-path collective"
+                                       if batch and ws > 1 else f"replicas x{ws} (no data-path collective)"),
                        "fix": {"none": "nve", "langevin": "nve + langevin 300 300 0.1",
                                "deform": "nve + deform 1 x erate 0.1 y volume"}[args.fix],
                        "l2": "working set larger than L2 (site table + lists > 126 MB)"},
@@ -550,13 +568,13 @@ def b200_arm(args, rank, local, ws, dist):
     eng.close()
 
 
-def serve_jobs(n: int, seed: int):
+def serve_specs(n: int, seed: int):
     """The serving stream: job sizes (atoms log-uniform 1k-200k, elements
     20-5,000, x-strain U(0, 5 %)), kinds (70 % FIRE to fmax 1e-6 eV/A capped at
     5,000 iterations, from rest; 30 % 2,000-step NVE at 300 K) and Poisson
-    arrival times at 50 jobs/s, all from one seeded generator."""
+    arrival times at 50 jobs/s per GPU, all from one seeded generator:
+    (arrival, atoms, elements, strain, fire, seed) per job."""
     import numpy as np
-    from cac_b200 import gen
     rng = np.random.default_rng(seed)
     out, t = [], 0.0
     for k in range(n):
@@ -564,21 +582,49 @@ def serve_jobs(n: int, seed: int):
         te = int(round(np.exp(rng.uniform(np.log(20), np.log(5000)))))
         st = float(rng.uniform(0.0, 0.05))
         fire = bool(rng.uniform() < 0.7)
-        sys_ = gen.replica(ta, te, temperature=0.0 if fire else 300.0, strain=st, seed=int(rng.integers(1 << 30)))
+        js = int(rng.integers(1 << 30))
         t += float(rng.exponential(1.0 / 50.0))
-        out.append((t, sys_, fire))
+        out.append((t, ta, te, st, fire, js))
     return out
 
 
-def serve_arm(args):
+def serve_jobs(n: int, seed: int, rank: int = 0, ws: int = 1):
+    """A rank's share of a stream of n x ws jobs (arrival rate scaled by the
+    ranks), split by the size-balanced greedy rule: (arrival, system, fire)."""
+    from cac_b200 import gen, shard
+    specs = serve_specs(n * ws, seed)
+    if ws > 1:
+        specs = [(sp[0] / ws,) + tuple(sp[1:]) for sp in specs]
+        own = shard.balanced_partition([ta + 8 * te for _, ta, te, _, _, _ in specs], ws)[rank]
+        specs = [specs[i] for i in own]
+    return [(t, gen.replica(ta, te, temperature=0.0 if fire else 300.0, strain=st, seed=js), fire)
+            for t, ta, te, st, fire, js in specs]
+
+
+def merge_serving(parts):
+    """Rank records (latencies, site-steps, FIRE stop codes, failures,
+    makespan) merged: sums, the longest makespan, all latencies."""
+    lat, site_steps, codes, failed, makespan = [], 0.0, {}, {}, 0.0
+    for p in parts:
+        lat += list(p["lat"])
+        site_steps += p["site_steps"]
+        makespan = max(makespan, p["makespan"])
+        for k, v in p["codes"].items():
+            codes[k] = codes.get(k, 0) + v
+        for k, v in p["failed"].items():
+            failed[k] = failed.get(k, 0) + v
+    return lat, site_steps, codes, failed, makespan
+
+
+def serve_arm(args, rank: int = 0, local: int = 0, ws: int = 1, dist=None):
     """Serve a Poisson stream of jobs; report throughput, latency percentiles
     and the same jobs run one after another in FP64 through the single-system
     engine (on a bounded prefix of the stream).  NVE jobs run as restarted
     trajectories of --segment steps (the reference's dynamics heat up without
     bound on longer runs)."""
     import numpy as np
-    from cac_b200 import api, gen
-    stream = serve_jobs(args.jobs, 101)
+    from cac_b200 import api, gen, shard
+    stream = serve_jobs(args.jobs, 101, rank, ws)
     tmp = tempfile.mkdtemp()
     setfl = os.path.join(tmp, "cu.setfl")
     gen.write_setfl(gen.EamParams(), setfl)
@@ -589,12 +635,14 @@ def serve_arm(args):
         else:
             obj.pair_lj(0.4093, 2.338, 5.5)
 
-    srv = api.Server(0, workers=args.workers, budget_gb=120.0,
+    srv = api.Server(local, workers=args.workers, budget_gb=120.0,
                      precision=api.MIXED if args.form == "mixed" else api.FP64)
     set_pair(srv)
     srv.neighbor(1.0, 10)
     srv.segment(args.segment)
     srv.start()
+    if dist:
+        dist.barrier()
     t0 = time.perf_counter()
     ids = []
     for t_arr, s, fire in stream:
@@ -621,11 +669,17 @@ def serve_arm(args):
         srv.release(j)
     makespan = time.perf_counter() - t0
     srv.close()
+    parts = shard.gather_objects({"lat": lat, "site_steps": site_steps, "codes": codes, "failed": failed,
+                                  "makespan": makespan, "jobs": len(stream)}, dist)
+    njobs = sum(p["jobs"] for p in parts)
+    lat, site_steps, codes, failed, makespan = merge_serving(parts)
     lat = np.array(lat)
+    if rank != 0:
+        return
 
     # serial FP64: the same jobs one at a time through one context
     serial_s, nser = 0.0, min(args.serial_jobs, len(stream))
-    e = api.Engine(0)
+    e = api.Engine(local)
     for t_arr, s, fire in stream[:nser]:
         e.upload(s)
         set_pair(e)
@@ -651,16 +705,17 @@ def serve_arm(args):
         serial_s += time.perf_counter() - a
     e.close()
     line = {
-        "metric": METRIC, "value": site_steps / makespan, "unit": UNIT, "n_gpus": 1, "steps": None,
+        "metric": METRIC, "value": site_steps / makespan, "unit": UNIT, "n_gpus": ws, "steps": None,
         "warmup": 0, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64" if args.form == "fp64" else "f32/f64",
         "data": "synthetic (seeded generator; no dataset exists for this path)",
-        "config": {"workload": "serve", "jobs": len(stream), "arrivals": "Poisson 50/s",
+        "config": {"workload": "serve", "jobs": njobs, "arrivals": f"Poisson {50 * ws}/s",
+                   "parallelism": f"{ws} ranks, jobs split by size (greedy), one server per GPU",
                    "pair": "eam/alloy" if args.pair == "eam" else "lj/cut",
                    "mix": "70% FIRE (ftol 1e-6 max-norm, cap 5000), 30% NVE 2000 steps "
                           f"(restarted every {args.segment})",
                    "workers": args.workers, "budget_gb": 120.0, "precision": args.form},
-        "serving": {"jobs_per_s": len(stream) / makespan, "makespan_s": makespan,
+        "serving": {"jobs_per_s": njobs / makespan, "makespan_s": makespan,
                     "latency_p50_s": float(np.percentile(lat, 50)),
                     "latency_p99_s": float(np.percentile(lat, 99)), "fire_stop_codes": codes,
                     "failed": failed,
@@ -699,8 +754,7 @@ def main():
                 args.warmup = 3
             reference_arm(args, rank, ws)
         elif args.workload == "serve":
-            if rank == 0:
-                serve_arm(args)
+            serve_arm(args, rank, local, ws, dist)
         else:
             b200_arm(args, rank, local, ws, dist)
     finally:

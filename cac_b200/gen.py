@@ -242,11 +242,12 @@ def replica(target_atoms: int, target_elements: int, *, temperature: float, stra
     return build_slab(nx, ny, le, la, temperature=temperature, strain=strain, seed=seed)
 
 
-def replica_set(n: int = 256, seed: int = 11, atoms=(2000, 64000), elements=(50, 2000),
-                temperature=(10.0, 500.0), strain=(0.0, 0.05)) -> List[System]:
-    """Independent replicas for batched runs: atom and element targets
-    log-uniform in the given ranges, temperature and x-strain uniform, every
-    draw from one seeded generator."""
+def replica_specs(n: int = 256, seed: int = 11, atoms=(2000, 64000), elements=(50, 2000),
+                  temperature=(10.0, 500.0), strain=(0.0, 0.05)) -> List[tuple]:
+    """(atom target, element target, temperature, x-strain, seed) of the
+    replicas of ``replica_set``: targets log-uniform in the given ranges,
+    temperature and strain uniform, every draw from one seeded generator in
+    replica order (the first k specs of a longer set are the k of a shorter)."""
     rng = np.random.default_rng(seed)
     out = []
     for k in range(n):
@@ -254,8 +255,18 @@ def replica_set(n: int = 256, seed: int = 11, atoms=(2000, 64000), elements=(50,
         te = int(round(math.exp(rng.uniform(math.log(elements[0]), math.log(elements[1])))))
         t = float(rng.uniform(*temperature))
         st = float(rng.uniform(*strain))
-        out.append(replica(ta, te, temperature=t, strain=st, seed=int(rng.integers(1 << 30))))
+        out.append((ta, te, t, st, int(rng.integers(1 << 30))))
     return out
+
+
+def replica_from_spec(spec: tuple) -> System:
+    ta, te, t, st, s = spec
+    return replica(ta, te, temperature=t, strain=st, seed=s)
+
+
+def replica_set(n: int = 256, seed: int = 11, **ranges) -> List[System]:
+    """Independent replicas for batched runs (``replica_specs``)."""
+    return [replica_from_spec(sp) for sp in replica_specs(n, seed, **ranges)]
 
 
 def tiny(seed: int = 7, temperature: float = 50.0) -> System:
