@@ -63,6 +63,7 @@ SIGNATURES = [
     ("cacb200_set_deform", C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int), _dp, _dp, C.c_int]),
     ("cacb200_unset_deform", C.c_int, [C.c_void_p]),
     ("cacb200_set_graphs", C.c_int, [C.c_void_p, C.c_int]),
+    ("cacb200_set_list_prefix", C.c_int, [C.c_void_p, C.c_double]),
     ("cacb200_replica_energy_noalloc", C.c_int, [C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.POINTER(C.c_int),
                                                  C.POINTER(C.c_int), C.c_double, _dp, C.c_void_p]),
     ("cacb200_server_create", C.c_int, [C.c_int, C.c_int, C.c_double, C.c_int, C.POINTER(C.c_void_p)]),
@@ -261,6 +262,10 @@ class Engine:
         if n == 1:
             return {k: float(out[0, i]) for i, k in enumerate(self.THERMO_FIELDS)}
         return {k: out[:, i].copy() for i, k in enumerate(self.THERMO_FIELDS)}
+
+    def list_prefix(self, margin: float) -> None:
+        """Inner-prefix margin of the lists (< 0: default 0.4 x skin, 0: off)."""
+        self._check(self.lib.cacb200_set_list_prefix(self.h, margin), "set_list_prefix")
 
     def graphs(self, enable: bool) -> None:
         self._check(self.lib.cacb200_set_graphs(self.h, 1 if enable else 0), "set_graphs")

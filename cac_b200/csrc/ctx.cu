@@ -292,6 +292,7 @@ void set_state(Ctx &c, const double *x, const double *v, const double *nodex, co
     if (changed) {
       forget_tallies(c);
       c.forces_current = false;
+      inner_off(c);
     }
   }
 }
@@ -341,6 +342,7 @@ void restore(Ctx &c) {
   d2d(c.nodev.p, c.snap_nodev.p, sizeof(double) * 24 * c.ne);
   c.lists_valid = false;
   c.forces_current = false;
+  inner_off(c);
   forget_tallies(c);
 }
 
@@ -702,6 +704,14 @@ int cacb200_set_box(cacb200_ctx *ctx, const double boxlo[3], const double boxhi[
 int cacb200_unset_deform(cacb200_ctx *ctx) {
   API_BEGIN
   deform_unset(c);
+  API_END
+}
+
+int cacb200_set_list_prefix(cacb200_ctx *ctx, double margin) {
+  API_BEGIN
+  c.inner_margin_set = margin;
+  c.planned = false;
+  c.lists_valid = false;
   API_END
 }
 

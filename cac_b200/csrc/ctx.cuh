@@ -261,6 +261,15 @@ struct Ctx {
   int every = 10;
   int cap = 160;
   DBuf<int> nbr_full, num_full;
+  // inner prefix of the full lists: entries within cut + inner_margin at the
+  // build come first, num_in of them; inner_ok (device) is nonzero while no
+  // site has moved inner_limit() since the build (positions in xbuild /
+  // nodex_build), and the pair loops then stop at num_in
+  double inner_margin = 0.4;
+  double inner_margin_set = -1.0;   // cacb200_set_list_prefix (< 0: 0.4 x skin)
+  DBuf<int> num_in, inner_ok;
+  DBuf<double4> xbuild;
+  DBuf<double> nodex_build;
   DBuf<int> nbr_half, num_half;
   bool have_half = false, lists_valid = false;
   DBuf<int> raw_full, raw_half;  // build-time entries before compaction
@@ -334,6 +343,17 @@ struct Ctx {
     if (!have_system) throw Error(CACB200_ESTATE, "no system uploaded");
   }
 };
+
+// Largest displacement since the build for which the inner prefix still
+// holds every pair inside the cutoff: half the margin, less an allowance for
+// the FP32 screen of the build's classification.
+inline double inner_limit(const Ctx &c) { return 0.5 * (c.inner_margin - 1e-3); }
+
+// Positions moved by something other than the checked drift: the pair loops
+// use the whole lists until the next build.
+inline void inner_off(Ctx &c) {
+  if (c.inner_ok.p) cudaMemsetAsync(c.inner_ok.p, 0, sizeof(int), c.stream);
+}
 
 // Host<->device copy ordered on the context's stream and completed on return.
 // (The legacy default stream does not order against the context's non-blocking

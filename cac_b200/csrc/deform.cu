@@ -290,6 +290,7 @@ void box_changed(Ctx &c) {
   c.box_replan = true;
   c.thermo_gen = -1;
   c.forces_current = false;
+  inner_off(c);   // distances changed by more than the sites' own motion
 }
 
 // A new box for a single system without moving its sites (the box a host

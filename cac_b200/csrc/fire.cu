@@ -259,6 +259,7 @@ void fire_init(Ctx &c, double dt) {
 // the velocity/position update (the force evaluation follows, after the
 // caller's list-rebuild decision, as in Min::energy_force).
 void fire_step(Ctx &c) {
+  inner_off(c);   // the FIRE update moves sites without the displacement test
   int nsite = c.na + 8 * c.ne;
   int nb = std::max(nblk(nsite, 256), 1);
   c.fire_partial.reserve((size_t)6 * nb);

@@ -89,9 +89,13 @@ __global__ void k_assemble(const double *gaussf, double *nodef, int ne) {
 }
 
 // FixNVE::initial_integrate (fix_nve.cpp:62-145): half kick and drift for
-// atoms (positions live in the site table) and nodes.
+// atoms (positions live in the site table) and nodes.  The drift also tests
+// the displacement since the last list build: an atom farther than `lim`
+// (a node component farther than lim / sqrt 3, which bounds every lattice
+// site of its element) ends the inner-prefix shortcut until the next build.
 __global__ void k_nve_initial(double4 *xs, double *v, const double *f, int na, double *nodex,
-                              double *nodev, const double *nodef, int nn3, double dtfm, double dtv) {
+                              double *nodev, const double *nodef, int nn3, double dtfm, double dtv,
+                              const double4 *xb, const double *nxb, int *inner_ok, double lim2, double limc) {
   int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t < na) {
     double4 p = xs[t];
@@ -108,13 +112,20 @@ __global__ void k_nve_initial(double4 *xs, double *v, const double *f, int na, d
     p.y = __dadd_rn(p.y, __dmul_rn(dtv, vy));
     p.z = __dadd_rn(p.z, __dmul_rn(dtv, vz));
     xs[t] = p;
+    if (xb) {
+      const double4 b = xb[t];
+      const double dx = p.x - b.x, dy = p.y - b.y, dz = p.z - b.z;
+      if (dx * dx + dy * dy + dz * dz > lim2) *inner_ok = 0;
+    }
     return;
   }
   int k = t - na;
   if (k >= nn3) return;
   double vn = __dadd_rn(nodev[k], __dmul_rn(dtfm, nodef[k]));
   nodev[k] = vn;
-  nodex[k] = __dadd_rn(nodex[k], __dmul_rn(dtv, vn));
+  const double xn = __dadd_rn(nodex[k], __dmul_rn(dtv, vn));
+  nodex[k] = xn;
+  if (nxb && fabs(xn - nxb[k]) > limc) *inner_ok = 0;
 }
 
 // FixNVE::final_integrate (fix_nve.cpp:148-219)
@@ -152,8 +163,12 @@ void nve_initial(Ctx &c, double dt) {
   int n = c.na + 24 * c.ne;
   if (n == 0) return;
   KernelTimer t(c, "nve_initial");
-  k_nve_initial<<<nblk(n, 256), 256, 0, c.stream>>>(c.xs.p, c.v.p, c.f.p, c.na, c.nodex.p, c.nodev.p,
-                                                    c.nodef.p, 24 * c.ne, dtfm, dt);
+  const bool check = c.lists_valid && c.inner_ok.p && c.xbuild.p;
+  const double lim = inner_limit(c);
+  k_nve_initial<<<nblk(n, 256), 256, 0, c.stream>>>(
+      c.xs.p, c.v.p, c.f.p, c.na, c.nodex.p, c.nodev.p, c.nodef.p, 24 * c.ne, dtfm, dt,
+      check ? c.xbuild.p : nullptr, check ? c.nodex_build.p : nullptr, c.inner_ok.p, lim * lim,
+      lim / 1.7320508075688772);
 }
 
 void nve_final(Ctx &c, double dt) {

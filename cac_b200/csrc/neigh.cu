@@ -275,7 +275,7 @@ struct BuildArgs {
   int na, ne, nsi, cap;
   RefBins rb;                 // single systems only (half lists)
   double cutneigh, cutneighsq;
-  double cutforcesq;          // pairs inside the force cutoff at build time are stored first
+  double cutforcesq;          // pairs inside the inner radius (force cutoff + margin) at build time go first
   int want_half;
   int *raw_full, *num_full;
   unsigned char *img_full;
@@ -890,17 +890,19 @@ __global__ void k_act_table(const int *flag, const int *pref, int ngid, int ne, 
 
 // Packs each entry as (pair-table index << 5 | image code): atoms by their
 // list slot (the pair table holds atoms in cell-sorted order), element sites
-// after them as in the site table.  Entries inside
-// the force cutoff at build time go first, each group in build order, so that
-// the pair loops meet the in-cutoff neighbours of all lanes of a warp together
-// (the order of a site's terms changes, not the set).
+// after them as in the site table.  Entries inside the inner radius (the
+// force cutoff plus a margin) at build time go first, each group in build
+// order, and their number is kept (num_in): while no site has moved half the
+// margin since the build, every pair inside the cutoff lies in that prefix,
+// in the same order, so the pair loops may stop there with identical sums.
 __global__ void k_remap(const int *raw, const unsigned char *img, const int *num, int nsi, int cap,
-                        const int *pref, const int *atom_slot, int na, int ne, int *out) {
+                        const int *pref, const int *atom_slot, int na, int ne, int *out, int *num_in) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nsi) return;
   int n = min(num[i], cap);
   int nin = 0;
   for (int k = 0; k < n; k++) nin += (img[(size_t)k * nsi + i] & IN_CUT) != 0;
+  if (num_in) num_in[i] = nin;
   int a = 0, b = nin;   // next in-cutoff and next other position
   for (int k = 0; k < n; k++) {
     size_t o = (size_t)k * nsi + i;
@@ -990,6 +992,11 @@ void neigh_plan(Ctx &c, bool want_half) {
   c.eframe.reserve((size_t)std::max(c.ne, 1) * 24);
   c.overflow.reserve(16);
   c.dev_nact.reserve(1);
+  c.inner_margin = c.inner_margin_set >= 0.0 ? c.inner_margin_set : 0.4 * c.skin;
+  c.inner_ok.reserve(1);
+  c.xbuild.reserve(std::max(c.na, 1));
+  c.nodex_build.reserve(24 * (size_t)std::max(c.ne, 1));
+  c.num_in.reserve(std::max(c.nsite_i(), 1));
   c.reach_bits.reserve(c.nrep);
   c.rep_d.reserve(c.nrep);
   CACB200_CUDA(cudaMemsetAsync(c.overflow.p, 0, 16 * sizeof(int), c.stream));
@@ -1155,6 +1162,14 @@ void neigh_build_async(Ctx &c, bool want_half) {
         k_elem_geom<<<nblk(c.ne, 128), 128, 0, c.stream>>>(c.nodex.p, c.ne, P, c.ecenter.p, c.eframe.p,
                                                            c.reach_bits.p, c.overflow.p + 3);
     }
+    // the positions these lists are built from, for the displacement test of
+    // the inner prefix; the prefix is usable until a site moves half the margin
+    if (c.na)
+      CACB200_CUDA(cudaMemcpyAsync(c.xbuild.p, c.xs.p, sizeof(double4) * c.na, cudaMemcpyDeviceToDevice, c.stream));
+    if (c.ne)
+      CACB200_CUDA(cudaMemcpyAsync(c.nodex_build.p, c.nodex.p, sizeof(double) * 24 * c.ne,
+                                   cudaMemcpyDeviceToDevice, c.stream));
+    CACB200_CUDA(cudaMemsetAsync(c.inner_ok.p, inner_limit(c) > 0.0 ? 1 : 0, sizeof(int), c.stream));
     {
       KernelTimer t(c, "bin");
       size_t bytes = c.cub_bytes;
@@ -1202,7 +1217,7 @@ void neigh_build_async(Ctx &c, bool want_half) {
     A.rb = c.rbins;
     A.cutneigh = c.cutneigh;
     A.cutneighsq = c.cutneighsq;
-    A.cutforcesq = c.pp.cut * c.pp.cut;
+    A.cutforcesq = (c.pp.cut + c.inner_margin) * (c.pp.cut + c.inner_margin);
     A.want_half = want_half ? 1 : 0;
     A.raw_full = c.raw_full.p;
     A.num_full = c.num_full.p;
@@ -1260,10 +1275,10 @@ void neigh_build_async(Ctx &c, bool want_half) {
                                                               c.act_off.p, c.dev_nact.p, c.overflow.p + 7);
     }
     k_remap<<<nblk(nsi, 256), 256, 0, c.stream>>>(c.raw_full.p, c.img_full.p, c.num_full.p, nsi, c.cap, pref,
-                                                   c.atom_slot.p, c.na, c.ne, c.nbr_full.p);
+                                                   c.atom_slot.p, c.na, c.ne, c.nbr_full.p, c.num_in.p);
     if (want_half)
       k_remap<<<nblk(nsi, 256), 256, 0, c.stream>>>(c.raw_half.p, c.img_half.p, c.num_half.p, nsi, c.cap, pref,
-                                                     c.atom_slot.p, c.na, c.ne, c.nbr_half.p);
+                                                     c.atom_slot.p, c.na, c.ne, c.nbr_half.p, nullptr);
   }
   c.have_half = want_half;
   c.lists_valid = true;

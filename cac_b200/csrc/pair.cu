@@ -33,6 +33,8 @@ struct PairArgs {
   const double4 *xs;                // pair table (list-slot order; w = F')
   const int *nbr;                   // lists and counts indexed by list slot
   const int *num;
+  const int *num_in;                // inner prefix length of each list ...
+  const int *inner_ok;              // ... usable while this is nonzero
   const int *slot_atom;             // list slot -> atom (slots past the atoms are Gauss points)
   int na, ne, nsi;
   double L[3];                      // box of a single system
@@ -95,6 +97,18 @@ __device__ __forceinline__ void for_each_neighbour(const PairArgs &A, int i, con
     neighbour_pos(A, Lx, Ly, Lz, __ldcs(nb + (size_t)k * A.nsi), p);
     f(p);
   }
+}
+
+// A site's list in two walks: the inner prefix (entries within the cutoff
+// plus a margin at the build), then, unless no site has moved half the margin
+// since the build, the rest.  Each entry's arithmetic depends on its place in
+// the walk (the compiler may fuse multiply-adds differently in the grouped and
+// the remainder loop), so the prefix is always walked on its own: the sums are
+// the same whether the rest is walked or not.
+template <bool MANY, class F>
+__device__ __forceinline__ void walk_list(const PairArgs &A, int i, const int *nb, int n_in, int n, F &&f) {
+  for_each_neighbour<MANY>(A, i, nb, n_in, f);
+  if (!*A.inner_ok && n > n_in) for_each_neighbour<MANY>(A, i, nb + (size_t)n_in * A.nsi, n - n_in, f);
 }
 
 // Writes force and per-site energy/virial of i-site i and accumulates the
@@ -166,7 +180,7 @@ __global__ void __launch_bounds__(128, EV ? 4 : 8) k_lj(PairArgs A, LjParams P) 
   double fi[3] = {0, 0, 0}, esum = 0.0, vsum[6] = {0, 0, 0, 0, 0, 0};
   if (valid) {
     double4 xi = A.xs[t];
-    int n = A.num[t];
+    const int n_in = A.num_in[t], n = A.num[t];
     const int *nb = A.nbr + t;
     auto pair = [&](const double4 &xj) {
       double dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
@@ -190,7 +204,7 @@ __global__ void __launch_bounds__(128, EV ? 4 : 8) k_lj(PairArgs A, LjParams P) 
         }
       }
     };
-    for_each_neighbour<MANY>(A, i, nb, n, pair);
+    walk_list<MANY>(A, i, nb, n_in, n, pair);
   }
   if (EV) finish_site(A, i, valid, fi, esum, vsum, 0.0, 0.0);
   else finish_force(A, i, valid, fi);
@@ -239,7 +253,7 @@ __global__ void __launch_bounds__(TB, 1024 / TB) k_eam_rho(PairArgs A, EamTables
   if (t >= A.nsi) return;
   const int i = site_of_slot(A, t);                       // site-table index
   double4 xi = A.xs[t];
-  int n = A.num[t];
+  const int n_in = A.num_in[t], n = A.num[t];
   const int *nb = A.nbr + t;
   double rho = 0.0;
   auto pair = [&](const double4 &xj) {
@@ -255,7 +269,7 @@ __global__ void __launch_bounds__(TB, 1024 / TB) k_eam_rho(PairArgs A, EamTables
       rho += ((c.x * p + c.y) * p + c.z) * p + c.w;
     }
   };
-  for_each_neighbour<MANY>(A, i, nb, n, pair);
+  walk_list<MANY>(A, i, nb, n_in, n, pair);
   int slot = i;
   if (i >= A.na) {
     int e = (i - A.na) / NG, g = (i - A.na) % NG;
@@ -296,7 +310,7 @@ __global__ void __launch_bounds__(TB, (EV ? 512 : 768) / TB) k_eam_force(PairArg
   if (valid) {
     double4 xi = A.xs[t];
     double fpi = xi.w;
-    int n = A.num[t];
+    const int n_in = A.num_in[t], n = A.num[t];
     const int *nb = A.nbr + t;
     auto pair = [&](const double4 &xj) {
       double dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
@@ -332,7 +346,7 @@ __global__ void __launch_bounds__(TB, (EV ? 512 : 768) / TB) k_eam_force(PairArg
         }
       }
     };
-    for_each_neighbour<MANY>(A, i, nb, n, pair);
+    walk_list<MANY>(A, i, nb, n_in, n, pair);
     if (EV && A.eflag) {
       double phi = phi_site[i];
       eemb_site = phi;
@@ -481,6 +495,8 @@ void pair_compute(Ctx &c, int eflag, int vflag) {
   A.xs = c.xss.p;
   A.nbr = c.nbr_full.p;
   A.num = c.num_full.p;
+  A.num_in = c.num_in.p;
+  A.inner_ok = c.inner_ok.p;
   A.slot_atom = c.slot_atom.p;
   A.na = c.na;
   A.ne = c.ne;

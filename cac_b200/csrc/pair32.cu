@@ -89,6 +89,8 @@ struct Args32 {
   const int4 *pos;
   const int *nbr;          // lists and counts indexed by list slot
   const int *num;
+  const int *num_in;                // inner prefix length of each list ...
+  const int *inner_ok;              // ... usable while this is nonzero
   const int *slot_atom;    // list slot -> atom (slots past the atoms are Gauss points)
   int na, ne, nsi;
   FixGrid G;
@@ -145,10 +147,8 @@ __device__ __forceinline__ void sep32(const Args32 &A, const SiteFix &F, const i
 }
 
 template <class F>
-__device__ __forceinline__ void for_each32(const Args32 &A, int t, int i, const int4 &oi, F &&f) {
-  const SiteFix fx = site_fix(A, i);
-  int n = A.num[t];
-  const int *nb = A.nbr + t;
+__device__ __forceinline__ void walk32(const Args32 &A, const SiteFix &fx, const int4 &oi, const int *nb, int n,
+                                       F &&f) {
   int k = 0;
   for (; k + 4 <= n; k += 4) {
     int v0 = __ldcs(nb + (size_t)k * A.nsi), v1 = __ldcs(nb + (size_t)(k + 1) * A.nsi);
@@ -166,6 +166,18 @@ __device__ __forceinline__ void for_each32(const Args32 &A, int t, int i, const 
     sep32(A, fx, oi, __ldcs(nb + (size_t)k * A.nsi), dx, dy, dz, wj);
     f(dx, dy, dz, wj);
   }
+}
+
+// A site's list: the inner prefix on its own, then the rest unless the
+// prefix still holds every pair inside the cutoff (an entry's arithmetic
+// depends on its place in a walk, so the prefix is always walked alone).
+template <class F>
+__device__ __forceinline__ void for_each32(const Args32 &A, int t, int i, const int4 &oi, F &&f) {
+  const SiteFix fx = site_fix(A, i);
+  const int n_in = A.num_in[t], n = A.num[t];
+  const int *nb = A.nbr + t;
+  walk32(A, fx, oi, nb, n_in, f);
+  if (!*A.inner_ok && n > n_in) walk32(A, fx, oi, nb + (size_t)n_in * A.nsi, n - n_in, f);
 }
 
 __device__ __forceinline__ void finish32(const Args32 &A, int i, bool valid, const float fi[3], bool ev,
@@ -438,6 +450,8 @@ void pair_compute_mixed(Ctx &c, int eflag, int vflag) {
   A.pos = c.pos32.p;
   A.nbr = c.nbr_full.p;
   A.num = c.num_full.p;
+  A.num_in = c.num_in.p;
+  A.inner_ok = c.inner_ok.p;
   A.slot_atom = c.slot_atom.p;
   A.na = c.na;
   A.ne = c.ne;

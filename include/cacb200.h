@@ -184,6 +184,14 @@ int cacb200_set_nodal_energy_weight(cacb200_ctx *ctx, double w);
 
 /* neighbor SKIN bin + neigh_modify every N delay 0 check no (neighbor.cpp:2043) */
 int cacb200_set_neighbor(cacb200_ctx *ctx, double skin, int every);
+/* The inner prefix of the lists (no reference counterpart; an evaluation
+ * order, not a different result): entries within cutoff + margin at the
+ * build are stored first, and while no site has moved half the margin since
+ * the build the pair loops stop after them; every pair inside the cutoff is
+ * in the prefix in the same order, so forces and energies are those of the
+ * whole lists bit for bit.  margin < 0: 0.4 x skin (default); 0: always the
+ * whole lists.  Takes effect at the next list build. */
+int cacb200_set_list_prefix(cacb200_ctx *ctx, double margin);
 /* Bin and build the lists now (Neighbor::build, neighbor.cpp:1704-1876).
  * The full list (npair_full_bin.cpp) is always built; the half list
  * (npair_half_bin_newton.cpp) only when want_half is non-zero. */
