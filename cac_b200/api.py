@@ -64,6 +64,7 @@ SIGNATURES = [
     ("cacb200_unset_deform", C.c_int, [C.c_void_p]),
     ("cacb200_set_graphs", C.c_int, [C.c_void_p, C.c_int]),
     ("cacb200_set_list_prefix", C.c_int, [C.c_void_p, C.c_double]),
+    ("cacb200_device_array", C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_void_p), C.POINTER(C.c_int64)]),
     ("cacb200_replica_energy_noalloc", C.c_int, [C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.POINTER(C.c_int),
                                                  C.POINTER(C.c_int), C.c_double, _dp, C.c_void_p]),
     ("cacb200_server_create", C.c_int, [C.c_int, C.c_int, C.c_double, C.c_int, C.POINTER(C.c_void_p)]),
@@ -180,6 +181,7 @@ class Engine:
         if rc != 0:
             raise CacB200Error(f"cacb200_ctx_create failed ({rc}): no usable CUDA device")
         self.h = h
+        self.device = device
         self.na = self.ne = 0
         self._cut = None
 
@@ -262,6 +264,27 @@ class Engine:
         if n == 1:
             return {k: float(out[0, i]) for i, k in enumerate(self.THERMO_FIELDS)}
         return {k: out[:, i].copy() for i, k in enumerate(self.THERMO_FIELDS)}
+
+    ARRAYS = {"x": (0, 4), "v": (1, 3), "f": (2, 3), "nodex": (3, 3), "nodev": (4, 3), "nodef": (5, 3),
+              "eatom": (6, 1), "enode": (7, 1), "vatom": (8, 6), "vnode": (9, 6)}
+
+    def device_array(self, name: str):
+        """A context array as a torch CUDA tensor sharing the device memory
+        (no copy): ``x`` (natoms, 4), ``v``/``f`` (natoms, 3), ``nodex``/
+        ``nodev``/``nodef`` (nelements*8, 3), ``eatom`` (natoms,), ``enode``
+        (nelements*8,), ``vatom``/``vnode`` (n, 6).  Synchronises the
+        context's stream first; valid until the next upload or list plan."""
+        import torch
+        which, width = self.ARRAYS[name]
+        ptr, n = C.c_void_p(), C.c_int64()
+        self._check(self.lib.cacb200_device_array(self.h, which, C.byref(ptr), C.byref(n)), "device_array")
+        torch.cuda.ExternalStream(self.stream, device=torch.device("cuda", self.device)).synchronize()
+        shape = (n.value // width, width) if width > 1 else (n.value,)
+
+        class _View:
+            __cuda_array_interface__ = {"shape": shape, "typestr": "<f8", "data": (ptr.value or 0, False),
+                                        "version": 3, "strides": None}
+        return torch.as_tensor(_View(), device=torch.device("cuda", self.device))
 
     def list_prefix(self, margin: float) -> None:
         """Inner-prefix margin of the lists (< 0: default 0.4 x skin, 0: off)."""

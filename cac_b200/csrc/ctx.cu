@@ -792,6 +792,40 @@ int cacb200_get_box(cacb200_ctx *ctx, double boxlo[3], double boxhi[3], double *
   API_END
 }
 
+int cacb200_device_array(cacb200_ctx *ctx, int which, void **ptr, int64_t *count) {
+  API_BEGIN
+  c.check_system();
+  if (!ptr || !count) throw Error(CACB200_EINVAL, "null output");
+  const int64_t na = c.na, ne = c.ne;
+  void *p = nullptr;
+  int64_t n = 0;
+  switch (which) {
+    case CACB200_ARRAY_X: p = c.xs.p, n = 4 * na; break;
+    case CACB200_ARRAY_V: p = c.v.p, n = 3 * na; break;
+    case CACB200_ARRAY_F: p = c.f.p, n = 3 * na; break;
+    case CACB200_ARRAY_NODEX: p = c.nodex.p, n = 24 * ne; break;
+    case CACB200_ARRAY_NODEV: p = c.nodev.p, n = 24 * ne; break;
+    case CACB200_ARRAY_NODEF: p = c.nodef.p, n = 24 * ne; break;
+    case CACB200_ARRAY_EATOM:
+    case CACB200_ARRAY_ENODE:
+      if (!c.have_peratom_e) throw Error(CACB200_ESTATE, "per-site energy not computed");
+      if (which == CACB200_ARRAY_EATOM) p = c.eatom.p, n = na;
+      else p = c.enode.p, n = 8 * ne;
+      break;
+    case CACB200_ARRAY_VATOM:
+    case CACB200_ARRAY_VNODE:
+      if (!c.have_peratom_v) throw Error(CACB200_ESTATE, "per-site virial not computed");
+      if (which == CACB200_ARRAY_VATOM) p = c.vatom.p, n = 6 * na;
+      else p = c.vnode.p, n = 48 * ne;
+      break;
+    default:
+      throw Error(CACB200_EINVAL, "unknown array");
+  }
+  *ptr = p;
+  *count = n;
+  API_END
+}
+
 int cacb200_counts(cacb200_ctx *ctx, int *natoms, int *nelements, int *nactive_sites) {
   API_BEGIN
   if (natoms) *natoms = c.na;

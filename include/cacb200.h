@@ -166,6 +166,33 @@ int cacb200_get_forces(cacb200_ctx *ctx, double *f, double *nodef, double *gauss
  * (Pair::eng_vdwl, Pair::virial, eatom, vatom, enode, vnode). */
 int cacb200_get_energy(cacb200_ctx *ctx, double *energy, double virial[6], double *eatom,
                        double *vatom, double *enode, double *vnode);
+/* Device address of one of the context's arrays, for consumers on the same
+ * GPU (analysis, dumps, another framework's tensors) that should not copy it
+ * to the host: compute pe/atom is CACB200_ARRAY_EATOM / ENODE
+ * (compute_pe_atom.cpp), compute stress/atom is -nktv2p times
+ * CACB200_ARRAY_VATOM / VNODE (compute_stress_atom.cpp:112-330; this
+ * reference adds no kinetic term).  *count is the number of doubles.
+ * Layouts (atom and element order of the upload):
+ *   X      [natoms][4]  x, y, z and a scratch word (positions in the site table)
+ *   V, F   [natoms][3]
+ *   NODEX, NODEV, NODEF  [nelements][8][3]
+ *   EATOM  [natoms], ENODE [nelements][8]      (last evaluation with ENERGY_ATOM)
+ *   VATOM  [natoms][6], VNODE [nelements][8][6] (last evaluation with VIRIAL_ATOM)
+ * Per-site energies and virials are CACB200_ESTATE until an evaluation has
+ * produced them.  The address stays valid until the next upload, list plan
+ * or destroy; reads are ordered after the context's stream only once that
+ * stream has been synchronised (cacb200_stream gives it). */
+#define CACB200_ARRAY_X 0
+#define CACB200_ARRAY_V 1
+#define CACB200_ARRAY_F 2
+#define CACB200_ARRAY_NODEX 3
+#define CACB200_ARRAY_NODEV 4
+#define CACB200_ARRAY_NODEF 5
+#define CACB200_ARRAY_EATOM 6
+#define CACB200_ARRAY_ENODE 7
+#define CACB200_ARRAY_VATOM 8
+#define CACB200_ARRAY_VNODE 9
+int cacb200_device_array(cacb200_ctx *ctx, int which, void **ptr, int64_t *count);
 int cacb200_counts(cacb200_ctx *ctx, int *natoms, int *nelements, int *nactive_sites);
 
 /* ------------------------------------------------------------- pair styles */
