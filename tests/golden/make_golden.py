@@ -15,7 +15,7 @@ Each fixture ``<case>.npz`` holds the reference's own read-outs:
   pxz pyz vol``, printed with ``%.17g``) at step 0 and step N; and with
   ``fix langevin`` (the ``LANGEVIN`` cases) its setup forces and the state
   after consecutive runs; with ``fix deform`` (the ``DEFORM`` cases) the
-  state and box after consecutive runs.
+  state and box after consecutive runs; and with both fixes together.
 EAM energies come from the executable with the patched ``compute_fp``
 (``cac_eamfix``); the unpatched reference energy is kept as ``energy_unpatched``.
 """
@@ -178,6 +178,47 @@ def deform_rows(work: str, pair: str, exe: str, system, name: str) -> dict:
     return out
 
 
+def both_rows(work: str, pair: str, exe: str, system, name: str) -> dict:
+    """The reference with fix langevin (post_force) and fix deform
+    (end_of_step) together after fix nve, over the langevin case's runs."""
+    nevery, style, a, b, _ = deform_spec(name, system)
+    t0, t1, damp, seed, zero = LANGEVIN[name][0]
+    runs = LANGEVIN[name][1]
+    args = []
+    for d in range(3):
+        st = DEFORM_STYLES[style[d]]
+        if st == "none":
+            continue
+        n = {"final": 2, "delta": 2, "wiggle": 2, "scale": 1, "vel": 1, "erate": 1, "trate": 1, "volume": 0}[st]
+        args.append(" ".join(["xyz"[d], st] + [repr(v) for v in (a[d], b[d])[:n]]))
+    tail = "neighbor 1.0 bin\nneigh_modify every 10 delay 0 check no\ntimestep 0.001\nfix 1 all nve\n"
+    fixes = (f"fix 2 all langevin {t0!r} {t1!r} {damp!r} {seed} zero {'yes' if zero else 'no'}\n"
+             f"fix 3 all deform {nevery} {' '.join(args)} units box remap x\n")
+    run(work, HEADER + pair_lines(pair) + tail + fixes + "".join(f"run {n}\n" for n in runs) +
+        "oracle_dump both.txt state\n", exe)
+    e = O.read_dump(os.path.join(work, "both.txt"))
+    out = {"both_end_box": e["box"]}
+    for k in ("x", "v", "f", "nodex", "nodev", "nodef"):
+        out["both_end_" + k] = e[k]
+    return out
+
+
+def add_both(name: str, system, pair: str) -> None:
+    """Add the langevin + deform read-outs to an existing fixture."""
+    path = os.path.join(OUT, name + ".npz")
+    with np.load(path) as z:
+        out = {k: z[k] for k in z.files}
+    work = tempfile.mkdtemp(prefix="cacgold_")
+    try:
+        gen.write_data(system, os.path.join(work, "data.cac"))
+        gen.write_setfl(gen.EamParams(), os.path.join(work, "cu.setfl"))
+        out.update(both_rows(work, pair, O.REF_EXE, system, name))
+    finally:
+        shutil.rmtree(work, ignore_errors=True)
+    np.savez_compressed(path, **out)
+    print(name, "langevin + deform box", out["both_end_box"].tolist())
+
+
 def add_deform(name: str, system, pair: str) -> None:
     """Add the fix deform read-outs to an existing fixture."""
     path = os.path.join(OUT, name + ".npz")
@@ -251,6 +292,7 @@ def make_case(name: str, system, pair: str, nsteps: int = 0, peratom_virial: boo
         out.update(thermo_rows(work, pair, nsteps, exe_e))
         out.update(langevin_rows(work, pair, O.REF_EXE, *LANGEVIN[name]))
         out.update(deform_rows(work, pair, O.REF_EXE, system, name))
+        out.update(both_rows(work, pair, O.REF_EXE, system, name))
         meta = dict(system.meta)
         out["meta"] = np.array(repr(sorted(meta.items())))
         np.savez_compressed(os.path.join(OUT, name + ".npz"), **out)
@@ -268,12 +310,12 @@ CASES = (
 
 def main():
     """``make_golden.py`` writes every fixture; ``make_golden.py thermo``,
-    ``langevin`` or ``deform`` only adds those read-outs to the fixtures
+    ``langevin``, ``deform`` or ``both`` only adds those read-outs to the fixtures
     already here."""
     if not os.path.exists(O.REF_EXE):
         raise SystemExit("build the reference first: make -C oracle reference")
     only = sys.argv[1] if sys.argv[1:] else None
-    if only not in (None, "thermo", "langevin", "deform"):
+    if only not in (None, "thermo", "langevin", "deform", "both"):
         raise SystemExit(f"unknown mode {only!r}")
     for name, system, pair, kw in CASES:
         if only == "thermo":
@@ -282,6 +324,8 @@ def main():
             add_langevin(name, system(), pair)
         elif only == "deform":
             add_deform(name, system(), pair)
+        elif only == "both":
+            add_both(name, system(), pair)
         else:
             make_case(name, system(), pair, **kw)
 

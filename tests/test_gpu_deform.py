@@ -177,3 +177,30 @@ def test_set_box_matches_fresh_upload(tmp_path):
     assert rel_err(f1, f2) < 1e-13
     assert rel_err(nf1, nf2) < 1e-13
     assert abs(ev1["energy"] - ev2["energy"]) < 1e-12 * abs(ev2["energy"])
+
+
+@pytest.mark.parametrize("case", ["tiny_lj", "tiny_eam", "lj_small"])
+def test_langevin_and_deform_together_vs_reference(case, golden, tmp_path):
+    """fix langevin (after the forces) and fix deform (at the end of the step)
+    together, over the langevin case's runs: the reference's box bit for bit,
+    its state within 1e-10."""
+    g = golden(case)
+    build, pair, _ = CASES[case]
+    e = make_engine(build(), pair, tmp_path)
+    t0, t1, damp, seed, zero = (float(v) for v in g["lgv_params"])
+    e.langevin(t0, t1, damp, int(seed), bool(zero))
+    apply_deform(e, g)
+    for n in g["lgv_runs"]:
+        e.run_nve(int(n))
+    lo, hi = e.box()
+    x, v, nx, nv = e.state()
+    f, nf, _ = e.forces()
+    e.close()
+    box = g["both_end_box"]
+    assert list(lo) == [box[0], box[2], box[4]] and list(hi) == [box[1], box[3], box[5]]
+    assert np.abs(x - g["both_end_x"]).max() < TOL_TRAJ
+    assert np.abs(nx - g["both_end_nodex"]).max() < TOL_TRAJ
+    assert rel_err(v, g["both_end_v"]) < TOL_TRAJ
+    assert rel_err(nv, g["both_end_nodev"]) < TOL_TRAJ
+    assert rel_err(f, g["both_end_f"]) < TOL_TRAJ
+    assert rel_err(nf, g["both_end_nodef"]) < TOL_TRAJ
