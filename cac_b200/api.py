@@ -64,6 +64,8 @@ SIGNATURES = [
     ("cacb200_unset_deform", C.c_int, [C.c_void_p]),
     ("cacb200_set_graphs", C.c_int, [C.c_void_p, C.c_int]),
     ("cacb200_set_list_prefix", C.c_int, [C.c_void_p, C.c_double]),
+    ("cacb200_run_begin", C.c_int, [C.c_void_p, C.c_int, C.c_double, C.c_int, C.c_int]),
+    ("cacb200_run_steps", C.c_int, [C.c_void_p, C.c_int, C.c_double, C.c_int, C.c_int]),
     ("cacb200_device_array", C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_void_p), C.POINTER(C.c_int64)]),
     ("cacb200_replica_energy_noalloc", C.c_int, [C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.POINTER(C.c_int),
                                                  C.POINTER(C.c_int), C.c_double, _dp, C.c_void_p]),
@@ -411,6 +413,14 @@ class Engine:
 
     def unset_langevin(self) -> None:
         self._check(self.lib.cacb200_unset_langevin(self.h), "unset_langevin")
+
+    def run_begin(self, nsteps: int, dt: float = 0.001, eflag: int = 0, vflag: int = 0) -> None:
+        """Verlet::setup of a run of ``nsteps`` (see run_steps)."""
+        self._check(self.lib.cacb200_run_begin(self.h, nsteps, dt, eflag, vflag), "run_begin")
+
+    def run_steps(self, nsteps: int, dt: float = 0.001, eflag: int = 0, vflag: int = 0) -> None:
+        """Advance the run begun by run_begin by ``nsteps`` of its steps."""
+        self._check(self.lib.cacb200_run_steps(self.h, nsteps, dt, eflag, vflag), "run_steps")
 
     def run_nve(self, nsteps: int, dt: float = 0.001, eflag: int = 0, vflag: int = 0) -> None:
         self._check(self.lib.cacb200_run_nve(self.h, nsteps, dt, eflag, vflag), "run_nve")

@@ -474,24 +474,41 @@ void nve_cycle(Ctx &c, double dt) {
   c.step += every - 1;
 }
 
-void run_nve(Ctx &c, int nsteps, double dt, int eflag, int vflag) {
+// Verlet::setup for a run of nsteps (verlet.cpp:64-190): the forces of the
+// positions the run starts from (evaluated again only when they are not
+// current or when the requested tallies are missing), the thermostat's setup
+// draws, the deformation's start and stop boxes.  eflag / vflag: tallies of
+// the setup evaluation (the reference tallies them for its step-0 output).
+void run_begin(Ctx &c, long nsteps, double dt, int eflag, int vflag) {
   c.check_system();
   if (nsteps < 0) throw Error(CACB200_EINVAL, "negative step count");
+  const bool need_tally = ((eflag & CACB200_ENERGY_GLOBAL) && c.tally_step_e != c.step) ||
+                          ((vflag & CACB200_VIRIAL_GLOBAL) && c.tally_step_v != c.step) ||
+                          ((eflag & CACB200_ENERGY_ATOM) && c.tally_step_ae != c.step) ||
+                          ((vflag & CACB200_VIRIAL_ATOM) && c.tally_step_av != c.step);
+  if (!c.lists_valid) {
+    setup(c);   // lists, then forces with the global tallies
+    if ((eflag & CACB200_ENERGY_ATOM) || (vflag & CACB200_VIRIAL_ATOM)) forces(c, eflag, vflag);
+  } else if (c.lgv.on || !c.forces_current || need_tally) {
+    // forces of the positions the run starts from: they differ from the last
+    // evaluation after a box change, new positions or a thermostat's draws
+    forces(c, eflag, vflag);
+  }
   if (c.lgv.on) {
-    // Verlet::setup: forces of the current positions, then the fixes'
-    // setup, which for fix langevin is its first post_force of the run
-    if (!c.lists_valid) setup(c);
-    else forces(c, 0, 0);
+    // the fixes' setup, which for fix langevin is its first post_force of the run
     langevin_begin(c, nsteps);
     langevin_post_force(c, dt);
-  } else if (!c.lists_valid) {
-    setup(c);
-  } else if (!c.forces_current) {
-    // Verlet::setup evaluates the forces of the positions a run starts from;
-    // they differ from the last evaluation after a box change or new positions
-    forces(c, 0, 0);
   }
   deform_begin(c, nsteps, dt);
+  c.run_left = nsteps;
+}
+
+// nsteps of the run begun by run_begin (Verlet::run, verlet.cpp:218-360);
+// energy / virial tallied on the last of them when eflag / vflag are set.
+void run_steps(Ctx &c, int nsteps, double dt, int eflag, int vflag) {
+  c.check_system();
+  if (nsteps < 0) throw Error(CACB200_EINVAL, "negative step count");
+  if (nsteps > c.run_left) throw Error(CACB200_ESTATE, "more steps than the run begun has left");
   // a deforming box changes launch arguments every step: no graph replay
   const bool graphs = c.graphs_enabled && c.every > 0 && !c.prof.enabled && !c.dfm.on;
   const bool want_ev = eflag || vflag;
@@ -514,7 +531,13 @@ void run_nve(Ctx &c, int nsteps, double dt, int eflag, int vflag) {
     deform_end_of_step(c, dt);
     s++;
   }
+  c.run_left -= nsteps;
   CACB200_CUDA(cudaGetLastError());
+}
+
+void run_nve(Ctx &c, int nsteps, double dt, int eflag, int vflag) {
+  run_begin(c, nsteps, dt, 0, 0);
+  run_steps(c, nsteps, dt, eflag, vflag);
 }
 
 // Minimize::command + Min::setup/run with a FIRE iterate (minimize.cpp:21-70,
@@ -961,6 +984,18 @@ int cacb200_nve_final(cacb200_ctx *ctx, double dt) {
 int cacb200_setup(cacb200_ctx *ctx) {
   API_BEGIN
   setup(c);
+  API_END
+}
+
+int cacb200_run_begin(cacb200_ctx *ctx, int nsteps, double dt, int eflag, int vflag) {
+  API_BEGIN
+  run_begin(c, nsteps, dt, eflag, vflag);
+  API_END
+}
+
+int cacb200_run_steps(cacb200_ctx *ctx, int nsteps, double dt, int eflag, int vflag) {
+  API_BEGIN
+  run_steps(c, nsteps, dt, eflag, vflag);
   API_END
 }
 

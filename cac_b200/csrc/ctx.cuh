@@ -332,7 +332,8 @@ struct Ctx {
   std::vector<DeformRep> dfm_rep;
   DBuf<double> dfm_maps;
   bool box_replan = false;        // the next plan follows a box change only
-  bool forces_current = false;    // f / nodef belong to the current positions and box
+  bool forces_current = false;    // f / nodef are the pair forces of the current positions and box
+  long run_left = 0;              // steps left in the run begun by run_begin
   DBuf<int4> thermo_meta;
   DBuf<double> thermo_vol, thermo_part, thermo_out;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;

@@ -402,6 +402,7 @@ void langevin_begin(Ctx &c, long nsteps) {
 // FixLangevin::post_force for the step the device counter holds.
 void langevin_post_force(Ctx &c, double dt) {
   if (!c.lgv.on) return;
+  c.forces_current = false;   // f and nodef now hold the draws as well
   LgvArgs A{};
   A.f = c.f.p;
   A.nodef = c.nodef.p;

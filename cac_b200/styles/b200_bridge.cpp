@@ -19,8 +19,11 @@
 #include "element_vec.h"
 #include "error.h"
 #include "force.h"
+#include "modify.h"
 #include "neighbor.h"
+#include "output.h"
 #include "pair.h"
+#include "thermo.h"
 #include "update.h"
 
 #include "cacb200.h"
@@ -199,7 +202,7 @@ void B200Bridge::compute(Pair *pair)
   }
 }
 
-void B200Bridge::run_nve(int nsteps, double dt, int every, const B200Fixes &fx)
+void B200Bridge::run_nve(int nsteps, double dt, int every, const B200Fixes &fx, bool thermo_output)
 {
   check_system();
   upload(true);
@@ -212,13 +215,29 @@ void B200Bridge::run_nve(int nsteps, double dt, int every, const B200Fixes &fx)
     status(cacb200_set_deform(ctx, fx.deform_every, fx.deform_style, fx.deform_a, fx.deform_b,
                               fx.deform_remap_x),
            "set_deform");
-  status(cacb200_setup(ctx), "setup");
-  status(cacb200_run_nve(ctx, nsteps, dt, 0, 0), "run_nve");
+  // thermo output on the reference's schedule (Output::setup / Output::write,
+  // output.cpp:264-284, 378-392): step 0 with the header, every
+  // thermo_every steps, and the last step of the run
+  const int ev = thermo_output ? CACB200_ENERGY_GLOBAL : 0, vv = thermo_output ? CACB200_VIRIAL_GLOBAL : 0;
+  const bigint step0 = update->ntimestep;
+  status(cacb200_run_begin(ctx, nsteps, dt, ev, vv), "run_begin");
+  if (thermo_output) thermo_line(step0, true, fx.deform);
+  const bigint every_t = output->thermo_every;
+  int done = 0;
+  while (done < nsteps) {
+    int k = nsteps - done;
+    if (thermo_output && every_t > 0) {
+      const bigint now = step0 + done;
+      const bigint next = (now / every_t) * every_t + every_t;
+      k = (int)std::min<bigint>(next - now, (bigint)(nsteps - done));
+    }
+    const bool out = thermo_output && (every_t > 0 || k == nsteps - done);
+    status(cacb200_run_steps(ctx, k, dt, out ? ev : 0, out ? vv : 0), "run_steps");
+    done += k;
+    if (out) thermo_line(step0 + done, false, fx.deform);
+  }
+  download_state(fx.deform);
   int na = atom->nlocal, ne = element->nlocal;
-  status(cacb200_get_state(ctx, na ? &atom->x[0][0] : nullptr, na ? &atom->v[0][0] : nullptr,
-                           ne ? &element->nodex[0][0][0][0] : nullptr,
-                           ne ? &element->nodev[0][0][0][0] : nullptr),
-         "get_state");
   fbuf.resize(3 * (size_t)std::max(na, 1));
   gbuf.resize(24 * (size_t)std::max(ne, 1));
   std::vector<double> nf(24 * (size_t)std::max(ne, 1));
@@ -231,10 +250,22 @@ void B200Bridge::run_nve(int nsteps, double dt, int every, const B200Fixes &fx)
         element->nodef[e][0][n][d] = nf[24 * (size_t)e + 3 * n + d];
         element->gaussf[e][0][n][d] = gbuf[24 * (size_t)e + 3 * n + d];
       }
+  uploaded_na = uploaded_ne = -1;   // the reference must set up again (ghosts are stale)
+}
+
+// Positions and velocities (and the box, when it deforms) from the device
+// into the reference's arrays.
+void B200Bridge::download_state(bool box)
+{
+  int na = atom->nlocal, ne = element->nlocal;
+  status(cacb200_get_state(ctx, na ? &atom->x[0][0] : nullptr, na ? &atom->v[0][0] : nullptr,
+                           ne ? &element->nodex[0][0][0][0] : nullptr,
+                           ne ? &element->nodev[0][0][0][0] : nullptr),
+         "get_state");
   // element centres follow the nodes, as after FixNVE::initial_integrate
   // (fix_nve.cpp:143)
   if (ne) element->evec->update_center_coord();
-  if (fx.deform) {
+  if (box) {
     // the box the device ended with (FixDeform::update_domain)
     double lo[3], hi[3], m = 0.0;
     status(cacb200_get_box(ctx, lo, hi, &m), "get_box");
@@ -245,7 +276,25 @@ void B200Bridge::run_nve(int nsteps, double dt, int every, const B200Fixes &fx)
     domain->set_global_box();
     domain->set_local_box();
   }
-  uploaded_na = uploaded_ne = -1;   // the reference must set up again (ghosts are stale)
+}
+
+// One thermo line of the reference (Thermo::header / Thermo::compute) at
+// `step`: the state and the pair's global tallies of that step go into the
+// reference's arrays, and its own Thermo evaluates and prints every keyword.
+void B200Bridge::thermo_line(bigint step, bool first, bool box)
+{
+  download_state(box);
+  double e = 0.0, vir[6];
+  status(cacb200_get_energy(ctx, &e, vir, nullptr, nullptr, nullptr, nullptr), "get_energy");
+  Pair *pair = force->pair;
+  pair->eng_vdwl = e;
+  pair->eng_coul = 0.0;
+  for (int k = 0; k < 6; k++) pair->virial[k] = vir[k];
+  update->ntimestep = step;
+  update->eflag_global = update->vflag_global = step;
+  modify->clearstep_compute();
+  if (first) output->thermo->header();
+  output->thermo->compute(first ? 0 : 1);
 }
 
 void B200Bridge::dump_list(const char *file, int half)

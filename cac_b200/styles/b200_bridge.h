@@ -49,8 +49,8 @@ class B200Bridge : protected Pointers {
   // the per-site arrays of `pair` according to its ev flags.
   void compute(class Pair *pair);
   // run N velocity-Verlet steps on the device (run_b200 command), with the
-  // given thermostat / deformation
-  void run_nve(int nsteps, double dt, int every, const B200Fixes &fixes);
+  // given thermostat / deformation; thermo lines on the reference's schedule
+  void run_nve(int nsteps, double dt, int every, const B200Fixes &fixes, bool thermo_output);
   // canonical neighbour-list dump (write_b200_neighbor command)
   void dump_list(const char *file, int half);
 
@@ -67,6 +67,8 @@ class B200Bridge : protected Pointers {
   std::vector<double> fbuf, gbuf, ebuf, vbuf, enbuf, vnbuf;
 
   void check_system();
+  void download_state(bool box);
+  void thermo_line(bigint step, bool first, bool box);
   void upload(bool with_velocities);
   void configure_pair();
   void status(int rc, const char *what);

@@ -10,6 +10,7 @@
 #include "force.h"
 #include "modify.h"
 #include "neighbor.h"
+#include "output.h"
 #include "pair_eam_alloy_b200.h"
 #include "pair_lj_cut_b200.h"
 #include "universe.h"
@@ -78,11 +79,12 @@ void RunB200::command(int narg, char **arg)
       if (fx.deform_style[d] < 0) error->all(FLERR, "run_b200: fix deform/b200 variable styles are not offered");
     }
   }
-  b->run_nve(nsteps, update->dt, neighbor->every, fx);
+  const bigint step0 = update->ntimestep;
+  b->run_nve(nsteps, update->dt, neighbor->every, fx, output->thermo != nullptr);
   // the host generator continues after the device's draws: the run's setup
   // call and one call per step
   if (lgv) lgv->advance((long long)(nsteps + 1) * lgv->draws_per_call());
-  update->ntimestep += nsteps;
+  update->ntimestep = step0 + nsteps;
 }
 
 void WriteB200Neighbor::command(int narg, char **arg)

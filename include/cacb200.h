@@ -252,6 +252,16 @@ int cacb200_nve_final(cacb200_ctx *ctx, double dt);
  * step is queued on the context's stream (list rebuilds synchronise). */
 int cacb200_setup(cacb200_ctx *ctx);
 int cacb200_run_nve(cacb200_ctx *ctx, int nsteps, double dt, int eflag, int vflag);
+/* cacb200_run_nve in two parts, so that a host can act between steps of one
+ * run (e.g. print the reference's thermo lines): cacb200_run_begin is
+ * Verlet::setup for a run of nsteps (forces of the starting positions, with
+ * the tallies eflag / vflag for step-0 output; the thermostat's setup draws;
+ * the deformation's start and stop boxes over nsteps), cacb200_run_steps
+ * advances that run by some of its steps (tallies on the last of them).
+ * cacb200_run_nve(n) = cacb200_run_begin(n, 0, 0) + cacb200_run_steps(n).
+ * CACB200_ESTATE when more steps are asked than the run begun has left. */
+int cacb200_run_begin(cacb200_ctx *ctx, int nsteps, double dt, int eflag, int vflag);
+int cacb200_run_steps(cacb200_ctx *ctx, int nsteps, double dt, int eflag, int vflag);
 
 /* fix ID all langevin t_start t_stop t_period seed [zero yes]
  * (FixLangevin, fix_langevin.cpp:40-214, 266-273, 455-694): drag plus random

@@ -164,3 +164,67 @@ def test_run_b200_refuses_plain_langevin(tmp_path):
     r = subprocess.run([APP, "-in", "in.cac"], cwd=tmp_path, capture_output=True, text=True, timeout=600)
     assert r.returncode != 0
     assert "langevin/b200" in r.stdout + r.stderr
+
+
+THERMO = ("thermo_style custom step temp ke pe etotal press pxx pyy pzz pxy pxz pyz vol\n"
+          "thermo_modify format float %.17g\nthermo 10\n")
+
+
+def app_log(tmp_path, case, body):
+    """The harness executable's screen output for the /b200 deck."""
+    build, pair, _ = CASES[case]
+    gen.write_data(build(), str(tmp_path / "data.cac"))
+    gen.write_setfl(gen.EamParams(), str(tmp_path / "cu.setfl"))
+    (tmp_path / "in.cac").write_text(HEADER + pair_lines(pair) + TAIL + body)
+    r = subprocess.run([APP, "-in", "in.cac"], cwd=tmp_path, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stdout[-3000:] + r.stderr[-3000:]
+    return r.stdout
+
+
+def reference_log(tmp_path, case, body, exe):
+    import oracle
+    build, pair, _ = CASES[case]
+    work = tmp_path / "ref"
+    work.mkdir()
+    gen.write_data(build(), str(work / "data.cac"))
+    gen.write_setfl(gen.EamParams(), str(work / "cu.setfl"))
+    plain = ("pair_style lj/cut 5.5\npair_coeff 1 1 0.4093 2.338\n" if pair == "lj"
+             else "pair_style eam/alloy\npair_coeff * * cu.setfl Cu\n")
+    (work / "in.cac").write_text(HEADER + plain + TAIL + body)
+    return oracle.run_reference(str(work), "in.cac", exe=exe)
+
+
+def assert_thermo_rows(ours, ref, O):
+    assert ours.shape == ref.shape and ours.shape[0] >= 3
+    assert np.array_equal(ours[:, 0], ref[:, 0])               # the same steps
+    cols = ("step",) + O.THERMO_FIELDS
+    p = [cols.index(k) for k in ("press", "pxx", "pyy", "pzz", "pxy", "pxz", "pyz")]
+    pscale = np.abs(ref[:, p]).max()
+    for c in range(1, ours.shape[1]):
+        scale = pscale if c in p else np.abs(ref[:, c]).max()
+        assert np.abs(ours[:, c] - ref[:, c]).max() <= 1e-9 * scale, cols[c]
+
+
+@pytest.mark.parametrize("case", ["tiny_lj", "tiny_eam"])
+def test_run_b200_prints_the_reference_thermo(case, tmp_path):
+    """run_b200 under `thermo 10` prints the reference's thermo lines (its own
+    Thermo, fed with the device state and tallies at each output step): step
+    0, every 10 steps and the last step, equal to the reference's run."""
+    import oracle as O
+    pair = CASES[case][1]
+    ours = O.read_thermo(app_log(tmp_path, case, THERMO + "run_b200 25\n"))
+    exe = O.REF_EXE_EAMFIX if pair == "eam" else O.REF_EXE
+    ref = O.read_thermo(reference_log(tmp_path, case, THERMO + "run 25\n", exe))
+    assert list(ours[:, 0]) == [0, 10, 20, 25]
+    assert_thermo_rows(ours, ref, O)
+
+
+def test_run_b200_thermo_with_both_fixes(golden, tmp_path):
+    import oracle as O
+    g = golden("tiny_lj")
+    fixes_b200 = lgv_fix(g) + dfm_fix(g)
+    fixes_ref = fixes_b200.replace("langevin/b200", "langevin").replace("deform/b200", "deform")
+    ours = O.read_thermo(app_log(tmp_path, "tiny_lj", fixes_b200 + THERMO + "run_b200 20\n"))
+    ref = O.read_thermo(reference_log(tmp_path, "tiny_lj", fixes_ref + THERMO + "run 20\n", O.REF_EXE))
+    assert list(ours[:, 0]) == [0, 10, 20]
+    assert_thermo_rows(ours, ref, O)
