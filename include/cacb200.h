@@ -327,9 +327,11 @@ int cacb200_set_fire_params(cacb200_ctx *ctx, int delaystep, double dtgrow, doub
                             double alpha0, double alphashrink, double tmax, double tmin,
                             double dmax, int halfstepback, int delaystep_start,
                             int max_vdotf_negatif);
-/* minimize etol ftol maxiter with min_style fire/b200 (Minimize::command,
- * minimize.cpp:21-70; the reference itself has no FIRE: this is FIRE 2.0 of
- * Guenole et al. 2020 over atoms + nodes).  normstyle: 0 two-norm, 1 max
+/* minimize etol ftol maxiter (Minimize::command, minimize.cpp:21-70, with
+ * nodal/weight 1) by a device FIRE iterate over atoms + nodes: FIRE 2.0 of
+ * Guenole et al. 2020 with the FIRE parameters and defaults the reference's
+ * Min carries (its own min styles are cg and sd; it has no FIRE style, so
+ * this minimiser has no input-deck form here).  normstyle: 0 two-norm, 1 max
  * per-site norm, 2 inf norm (min_modify norm two|max|inf).  Returns the stop
  * code of min.h:46-47 (0 MAXITER, 2 ETOL, 3 FTOL, 11 MAXVDOTF), iterations,
  * final energy and force norm (squared, in the chosen style). */
