@@ -262,9 +262,9 @@ struct Ctx {
   int cap = 160;
   DBuf<int> nbr_full, num_full;
   // inner prefix of the full lists: entries within cut + inner_margin at the
-  // build come first, num_in of them; inner_ok (device) is nonzero while no
-  // site has moved inner_limit() since the build (positions in xbuild /
-  // nodex_build), and the pair loops then stop at num_in
+  // build come first, num_in of them; inner_ok[replica] (device) is nonzero
+  // while no site of the replica has moved inner_limit() since the build
+  // (positions in xbuild / nodex_build), and the pair loops then stop at num_in
   double inner_margin = 0.4;
   double inner_margin_set = -1.0;   // cacb200_set_list_prefix (< 0: 0.4 x skin)
   DBuf<int> num_in, inner_ok;
@@ -353,7 +353,7 @@ inline double inner_limit(const Ctx &c) { return 0.5 * (c.inner_margin - 1e-3); 
 // Positions moved by something other than the checked drift: the pair loops
 // use the whole lists until the next build.
 inline void inner_off(Ctx &c) {
-  if (c.inner_ok.p) cudaMemsetAsync(c.inner_ok.p, 0, sizeof(int), c.stream);
+  if (c.inner_ok.p) cudaMemsetAsync(c.inner_ok.p, 0, sizeof(int) * c.inner_ok.n, c.stream);
 }
 
 // Host<->device copy ordered on the context's stream and completed on return.

@@ -178,9 +178,12 @@ __global__ void k_fire_control(const double *partial, int nb, const double *ev_o
 
 // Semi-implicit Euler step with FIRE mixing (Algorithm 2 of the paper):
 // optional half step back and velocity reset, v += dt F/m, mixing, x += dt v.
+// The FIRE move; like the velocity-Verlet drift it tests each site's
+// displacement since the list build (the inner-prefix flag of its replica).
 __global__ void k_fire_update(double4 *xs, double *v, const double *f, int na, double *nodex,
                               double *nodev, const double *nodef, int nn3, const FireState *S,
-                              double mass) {
+                              double mass, const double4 *xb, const double *nxb, int *inner_ok, double lim2,
+                              double limc, const int *site_rep, const int *elem_rep) {
   if (!S->apply) return;
   int t = blockIdx.x * blockDim.x + threadIdx.x;
   const double dtv = S->dtv, dtfm = dtv * FTM2V / mass, hb = S->halfback;
@@ -204,6 +207,11 @@ __global__ void k_fire_update(double4 *xs, double *v, const double *f, int na, d
       vi[d] = vd;
     }
     xs[t] = p;
+    if (xb) {
+      const double4 b = xb[t];
+      const double dx = p.x - b.x, dy = p.y - b.y, dz = p.z - b.z;
+      if (dx * dx + dy * dy + dz * dz > lim2) inner_ok[site_rep ? site_rep[t] : 0] = 0;
+    }
     return;
   }
   int k = t - na;
@@ -216,8 +224,10 @@ __global__ void k_fire_update(double4 *xs, double *v, const double *f, int na, d
   }
   vd += dtfm * nodef[k];
   if (mix) vd = s1 * vd + s2 * nodef[k];
-  nodex[k] = x + dtv * vd;
+  const double xn = x + dtv * vd;
+  nodex[k] = xn;
   nodev[k] = vd;
+  if (nxb && fabs(xn - nxb[k]) > limc) inner_ok[elem_rep ? elem_rep[k / 24] : 0] = 0;
 }
 
 __global__ void k_zero(double *a, size_t n) {
@@ -259,7 +269,6 @@ void fire_init(Ctx &c, double dt) {
 // the velocity/position update (the force evaluation follows, after the
 // caller's list-rebuild decision, as in Min::energy_force).
 void fire_step(Ctx &c) {
-  inner_off(c);   // the FIRE update moves sites without the displacement test
   int nsite = c.na + 8 * c.ne;
   int nb = std::max(nblk(nsite, 256), 1);
   c.fire_partial.reserve((size_t)6 * nb);
@@ -276,8 +285,12 @@ void fire_step(Ctx &c) {
   int n = c.na + 24 * c.ne;
   if (n) {
     KernelTimer t(c, "fire_update");
-    k_fire_update<<<nblk(n, 256), 256, 0, c.stream>>>(c.xs.p, c.v.p, c.f.p, c.na, c.nodex.p, c.nodev.p,
-                                                      c.nodef.p, 24 * c.ne, c.fire_state.p, c.mass);
+    const bool check = c.lists_valid && c.inner_ok.p && c.xbuild.p;
+    const double lim = inner_limit(c);
+    k_fire_update<<<nblk(n, 256), 256, 0, c.stream>>>(
+        c.xs.p, c.v.p, c.f.p, c.na, c.nodex.p, c.nodev.p, c.nodef.p, 24 * c.ne, c.fire_state.p, c.mass,
+        check ? c.xbuild.p : nullptr, check ? c.nodex_build.p : nullptr, c.inner_ok.p, lim * lim,
+        lim / 1.7320508075688772, c.nrep > 1 ? c.site_rep.p : nullptr, c.nrep > 1 ? c.elem_rep.p : nullptr);
   }
 }
 

@@ -95,7 +95,8 @@ __global__ void k_assemble(const double *gaussf, double *nodef, int ne) {
 // site of its element) ends the inner-prefix shortcut until the next build.
 __global__ void k_nve_initial(double4 *xs, double *v, const double *f, int na, double *nodex,
                               double *nodev, const double *nodef, int nn3, double dtfm, double dtv,
-                              const double4 *xb, const double *nxb, int *inner_ok, double lim2, double limc) {
+                              const double4 *xb, const double *nxb, int *inner_ok, double lim2, double limc,
+                              const int *site_rep, const int *elem_rep) {
   int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t < na) {
     double4 p = xs[t];
@@ -115,7 +116,7 @@ __global__ void k_nve_initial(double4 *xs, double *v, const double *f, int na, d
     if (xb) {
       const double4 b = xb[t];
       const double dx = p.x - b.x, dy = p.y - b.y, dz = p.z - b.z;
-      if (dx * dx + dy * dy + dz * dz > lim2) *inner_ok = 0;
+      if (dx * dx + dy * dy + dz * dz > lim2) inner_ok[site_rep ? site_rep[t] : 0] = 0;
     }
     return;
   }
@@ -125,7 +126,7 @@ __global__ void k_nve_initial(double4 *xs, double *v, const double *f, int na, d
   nodev[k] = vn;
   const double xn = __dadd_rn(nodex[k], __dmul_rn(dtv, vn));
   nodex[k] = xn;
-  if (nxb && fabs(xn - nxb[k]) > limc) *inner_ok = 0;
+  if (nxb && fabs(xn - nxb[k]) > limc) inner_ok[elem_rep ? elem_rep[k / 24] : 0] = 0;
 }
 
 // FixNVE::final_integrate (fix_nve.cpp:148-219)
@@ -168,7 +169,7 @@ void nve_initial(Ctx &c, double dt) {
   k_nve_initial<<<nblk(n, 256), 256, 0, c.stream>>>(
       c.xs.p, c.v.p, c.f.p, c.na, c.nodex.p, c.nodev.p, c.nodef.p, 24 * c.ne, dtfm, dt,
       check ? c.xbuild.p : nullptr, check ? c.nodex_build.p : nullptr, c.inner_ok.p, lim * lim,
-      lim / 1.7320508075688772);
+      lim / 1.7320508075688772, c.nrep > 1 ? c.site_rep.p : nullptr, c.nrep > 1 ? c.elem_rep.p : nullptr);
 }
 
 void nve_final(Ctx &c, double dt) {

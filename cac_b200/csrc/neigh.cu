@@ -993,7 +993,7 @@ void neigh_plan(Ctx &c, bool want_half) {
   c.overflow.reserve(16);
   c.dev_nact.reserve(1);
   c.inner_margin = c.inner_margin_set >= 0.0 ? c.inner_margin_set : 0.4 * c.skin;
-  c.inner_ok.reserve(1);
+  c.inner_ok.reserve(c.nrep);
   c.xbuild.reserve(std::max(c.na, 1));
   c.nodex_build.reserve(24 * (size_t)std::max(c.ne, 1));
   c.num_in.reserve(std::max(c.nsite_i(), 1));
@@ -1169,7 +1169,7 @@ void neigh_build_async(Ctx &c, bool want_half) {
     if (c.ne)
       CACB200_CUDA(cudaMemcpyAsync(c.nodex_build.p, c.nodex.p, sizeof(double) * 24 * c.ne,
                                    cudaMemcpyDeviceToDevice, c.stream));
-    CACB200_CUDA(cudaMemsetAsync(c.inner_ok.p, inner_limit(c) > 0.0 ? 1 : 0, sizeof(int), c.stream));
+    CACB200_CUDA(cudaMemsetAsync(c.inner_ok.p, inner_limit(c) > 0.0 ? 1 : 0, sizeof(int) * c.nrep, c.stream));
     {
       KernelTimer t(c, "bin");
       size_t bytes = c.cub_bytes;

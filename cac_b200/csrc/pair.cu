@@ -34,7 +34,7 @@ struct PairArgs {
   const int *nbr;                   // lists and counts indexed by list slot
   const int *num;
   const int *num_in;                // inner prefix length of each list ...
-  const int *inner_ok;              // ... usable while this is nonzero
+  const int *inner_ok;              // ... usable while this is nonzero (per replica)
   const int *slot_atom;             // list slot -> atom (slots past the atoms are Gauss points)
   int na, ne, nsi;
   double L[3];                      // box of a single system
@@ -105,10 +105,15 @@ __device__ __forceinline__ void for_each_neighbour(const PairArgs &A, int i, con
 // the walk (the compiler may fuse multiply-adds differently in the grouped and
 // the remainder loop), so the prefix is always walked on its own: the sums are
 // the same whether the rest is walked or not.
+// The prefix flag belongs to the site's replica (one hot replica of a batch
+// does not end the shortcut for the others); one copy of the walk serves both
+// segments, which keeps the register count of the unrolled body.
 template <bool MANY, class F>
 __device__ __forceinline__ void walk_list(const PairArgs &A, int i, const int *nb, int n_in, int n, F &&f) {
-  for_each_neighbour<MANY>(A, i, nb, n_in, f);
-  if (!*A.inner_ok && n > n_in) for_each_neighbour<MANY>(A, i, nb + (size_t)n_in * A.nsi, n - n_in, f);
+  const bool rest = n > n_in && !A.inner_ok[MANY ? A.site_rep[i] : 0];
+#pragma unroll 1
+  for (int seg = 0; seg < (rest ? 2 : 1); seg++)
+    for_each_neighbour<MANY>(A, i, seg ? nb + (size_t)n_in * A.nsi : nb, seg ? n - n_in : n_in, f);
 }
 
 // Writes force and per-site energy/virial of i-site i and accumulates the

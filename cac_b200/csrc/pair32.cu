@@ -90,7 +90,7 @@ struct Args32 {
   const int *nbr;          // lists and counts indexed by list slot
   const int *num;
   const int *num_in;                // inner prefix length of each list ...
-  const int *inner_ok;              // ... usable while this is nonzero
+  const int *inner_ok;              // ... usable while this is nonzero (per replica)
   const int *slot_atom;    // list slot -> atom (slots past the atoms are Gauss points)
   int na, ne, nsi;
   FixGrid G;
@@ -176,8 +176,10 @@ __device__ __forceinline__ void for_each32(const Args32 &A, int t, int i, const 
   const SiteFix fx = site_fix(A, i);
   const int n_in = A.num_in[t], n = A.num[t];
   const int *nb = A.nbr + t;
-  walk32(A, fx, oi, nb, n_in, f);
-  if (!*A.inner_ok && n > n_in) walk32(A, fx, oi, nb + (size_t)n_in * A.nsi, n - n_in, f);
+  const bool rest = n > n_in && !A.inner_ok[A.G.reps ? A.G.site_rep[i] : 0];
+#pragma unroll 1
+  for (int seg = 0; seg < (rest ? 2 : 1); seg++)
+    walk32(A, fx, oi, seg ? nb + (size_t)n_in * A.nsi : nb, seg ? n - n_in : n_in, f);
 }
 
 __device__ __forceinline__ void finish32(const Args32 &A, int i, bool valid, const float fi[3], bool ev,
