@@ -222,7 +222,7 @@ struct Ctx {
   // element geometry (per rebuild)
   DBuf<double4> ecenter;         // reference centre (x, y, z, R_e)
   DBuf<double4> ewrap;           // wrapped centre, w = bitcast of packed wrap counts
-  DBuf<double> eframe;           // [ne*16]: n0(3) a(3) b(3) c(3) ... see neigh.cu
+  DBuf<double> eframe;           // [ne*28]: element frame (layout at k_elem_geom, neigh.cu)
   double emax_reach = 0.0;
 
   // atom cell grid (candidate search)

@@ -285,7 +285,7 @@ void fire_step(Ctx &c) {
   int n = c.na + 24 * c.ne;
   if (n) {
     KernelTimer t(c, "fire_update");
-    const bool check = c.lists_valid && c.inner_ok.p && c.xbuild.p;
+    const bool check = c.lists_valid && c.inner_ok.p && c.xbuild.p && inner_limit(c) > 0.0;
     const double lim = inner_limit(c);
     k_fire_update<<<nblk(n, 256), 256, 0, c.stream>>>(
         c.xs.p, c.v.p, c.f.p, c.na, c.nodex.p, c.nodev.p, c.nodef.p, 24 * c.ne, c.fire_state.p, c.mass,

@@ -164,7 +164,7 @@ void nve_initial(Ctx &c, double dt) {
   int n = c.na + 24 * c.ne;
   if (n == 0) return;
   KernelTimer t(c, "nve_initial");
-  const bool check = c.lists_valid && c.inner_ok.p && c.xbuild.p;
+  const bool check = c.lists_valid && c.inner_ok.p && c.xbuild.p && inner_limit(c) > 0.0;
   const double lim = inner_limit(c);
   k_nve_initial<<<nblk(n, 256), 256, 0, c.stream>>>(
       c.xs.p, c.v.p, c.f.p, c.na, c.nodex.p, c.nodev.p, c.nodef.p, 24 * c.ne, dtfm, dt,

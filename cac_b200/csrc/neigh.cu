@@ -94,10 +94,14 @@ __global__ void k_pbc_atoms(double4 *xs, int na, RP P) {
 // search: affine frame n0 + i a + j b + k c of the lattice sites, its inverse,
 // the largest deviation of the trilinear nodes from that frame, and the
 // centre-to-node radius.
-//   eframe[e*24 + 0..2]   n0
-//   eframe[e*24 + 3..11]  rows of the inverse frame matrix
-//   eframe[e*24 + 12]     dmax
-//   eframe[e*24 + 13..21] frame vectors a, b, c (one lattice step each)
+//   eframe[e*EFR + 0..2]  n0
+//   eframe[e*EFR + 3..11] rows of the inverse frame matrix
+//   eframe[e*EFR + 12]    dmax
+//   eframe[e*EFR + 13..21] frame vectors a, b, c (one lattice step each)
+//   eframe[e*EFR + 22..24] norms of the inverse frame's rows (lattice steps
+//                         per unit length along each index)
+constexpr int EFR = 28;
+
 template <class RP>
 __global__ void k_elem_geom(double *nodex, int ne, RP P, double4 *ecenter, double *eframe,
                             unsigned long long *reach_bits, int *grew) {
@@ -173,7 +177,7 @@ __global__ void k_elem_geom(double *nodex, int ne, RP P, double4 *ecenter, doubl
     inv[2][0] = (A[1][0] * A[2][1] - A[1][1] * A[2][0]) * id;
     inv[2][1] = (A[0][1] * A[2][0] - A[0][0] * A[2][1]) * id;
     inv[2][2] = (A[0][0] * A[1][1] - A[0][1] * A[1][0]) * id;
-    double *fr = eframe + (size_t)e * 24;
+    double *fr = eframe + (size_t)e * EFR;
     fr[0] = n0[0];
     fr[1] = n0[1];
     fr[2] = n0[2];
@@ -181,6 +185,9 @@ __global__ void k_elem_geom(double *nodex, int ne, RP P, double4 *ecenter, doubl
     for (int r = 0; r < 3; r++)
 #pragma unroll
       for (int q = 0; q < 3; q++) fr[3 + 3 * r + q] = inv[r][q];
+#pragma unroll
+    for (int r = 0; r < 3; r++)
+      fr[22 + r] = sqrt(inv[r][0] * inv[r][0] + inv[r][1] * inv[r][1] + inv[r][2] * inv[r][2]);
     fr[12] = dmax;
 #pragma unroll
     for (int q = 0; q < 3; q++)
@@ -479,7 +486,7 @@ __device__ int element_items(const BuildArgs &A, const Query &q, int2 *out, int 
           double4 ce = A.ecenter[e];
           // sphere test in the element's raw frame: |xi - s L - centre| <= cutneigh + R
           double p[3] = {q.xi[0] - sL[0], q.xi[1] - sL[1], q.xi[2] - sL[2]};
-          const double *fr = A.eframe + (size_t)e * 24;
+          const double *fr = A.eframe + (size_t)e * EFR;
           double dmax = fr[12];
           double R = ce.w + dmax + A.cutneigh + 1e-6;
           double dcx = p[0] - ce.x, dcy = p[1] - ce.y, dcz = p[2] - ce.z;
@@ -491,7 +498,7 @@ __device__ int element_items(const BuildArgs &A, const Query &q, int2 *out, int 
           for (int r = 0; r < 3; r++) {
             double a0 = fr[3 + 3 * r], a1 = fr[4 + 3 * r], a2 = fr[5 + 3 * r];
             double fidx = a0 * rel[0] + a1 * rel[1] + a2 * rel[2];
-            double rho = (A.cutneigh + dmax + 1e-6) * sqrt(a0 * a0 + a1 * a1 + a2 * a2) + 1e-6;
+            double rho = (A.cutneigh + dmax + 1e-6) * fr[22 + r] + 1e-6;
             lo[r] = max(0, (int)ceil(fidx - rho));
             hi[r] = min(NC - 1, (int)floor(fidx + rho));
             if (lo[r] > hi[r]) empty = true;
@@ -541,11 +548,70 @@ __device__ __forceinline__ void warp_emit(const BuildArgs &A, int slot, int &n, 
 // coordinates and the FP32 affine frame relative to the query), then the
 // lanes walk the group's sites flattened in (item, a, bb, cc) order -- the
 // serial order -- so small boxes do not leave lanes idle.  Each site takes the
-// FP32 affine screen, then the reference's exact FP64 distance.
+// FP32 affine screen; the sites that pass are queued in that order and take
+// the reference's exact FP64 distance 32 at a time, so the FP64 work runs on
+// full warps and the entries are emitted in the serial order.
 struct ItemStage {
   double g[32][24];   // ghost node coordinates nodex + s L
   float fr[32][13];   // frame columns a, b, c; query minus frame origin; screen radius^2
+  int mg[32][2];      // ceil(2^16 / n) of the box's z and y extents (division by multiply-shift)
+  int2 item[32];      // the group's items
+  int queue[64];      // screened sites: item lane << 10 | lattice site
 };
+
+// The exact test of one queued site (active lanes only) and the warp's
+// emission of the accepted ones.
+__device__ __forceinline__ void items_exact(const BuildArgs &A, const Query &q, const ItemStage &st, bool active,
+                                            int entry, int &nf, int &nh) {
+  bool pf = false, ph = false;
+  int val = 0, codef = 0, code = 0;
+  if (active) {
+    const int m = entry >> 10, u = entry & 1023;
+    int e, sv[3], lo[3], hi[3];
+    unpack_item(st.item[m], e, sv, lo, hi);
+    const bool zero = (sv[0] == 0 && sv[1] == 0 && sv[2] == 0);
+    const bool far_image = sv[0] < -1 || sv[0] > 1 || sv[1] < -1 || sv[1] > 1 || sv[2] < -1 || sv[2] > 1;
+    code = far_image ? 0 : img_code(sv[0], sv[1], sv[2]);
+    const double *g = st.g[m];
+    double dx = q.xi[0], dy = q.xi[1], dz = q.xi[2];
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+      double N = shape_val(u, k);
+      dx = __dsub_rn(dx, __dmul_rn(N, g[3 * k]));
+      dy = __dsub_rn(dy, __dmul_rn(N, g[3 * k + 1]));
+      dz = __dsub_rn(dz, __dmul_rn(N, g[3 * k + 2]));
+    }
+    double rsq = rsq_rn(dx, dy, dz);
+    if (rsq <= A.cutneighsq) {
+      if (far_image) {
+        atomicExch(&A.overflow[2], 1);
+      } else {
+        pf = true;
+        val = KIND_SITE | (e * NU + u);
+        codef = code | (rsq < A.cutforcesq ? IN_CUT : 0);
+        if (site_gauss(u) < 0) A.site_flag[e * NU + u] = 1;   // to be interpolated
+        ph = true;
+        if (A.want_half && !q.iatom) {
+          int jg = site_gauss(u);
+          if (jg >= 0) {
+            if (zero) {
+              ph = (q.ie < e) || (q.ie == e && q.ig < jg);
+            } else {
+              const double4 ce = A.ecenter[e], ci = A.ecenter[q.ie];
+              const double sL[3] = {sv[0] * q.r.b.L[0], sv[1] * q.r.b.L[1], sv[2] * q.r.b.L[2]};
+              double qcen[3] = {sv[0] ? __dadd_rn(ce.x, sL[0]) : ce.x, sv[1] ? __dadd_rn(ce.y, sL[1]) : ce.y,
+                                sv[2] ? __dadd_rn(ce.z, sL[2]) : ce.z};
+              double icen[3] = {ci.x, ci.y, ci.z};
+              ph = above_right(qcen, icen);
+            }
+          }
+        }
+      }
+    }
+  }
+  warp_emit(A, q.slot, nf, A.raw_full, A.img_full, pf, val, codef);
+  if (A.want_half) warp_emit(A, q.slot, nh, A.raw_half, A.img_half, ph, val, code);
+}
 
 __device__ void items_warp(const BuildArgs &A, const Query &q, const int2 *items, int n, ItemStage &st, int &nf,
                            int &nh) {
@@ -557,6 +623,7 @@ __device__ void items_warp(const BuildArgs &A, const Query &q, const int2 *items
     __syncwarp();
     if (gi < n) {
       it = items[gi];
+      st.item[lane] = it;
       int e, sv[3], lo[3], hi[3];
       unpack_item(it, e, sv, lo, hi);
       nbox = (hi[0] - lo[0] + 1) * (hi[1] - lo[1] + 1) * (hi[2] - lo[2] + 1);
@@ -564,13 +631,16 @@ __device__ void items_warp(const BuildArgs &A, const Query &q, const int2 *items
       const double *nx = A.nodex + (size_t)e * 24;
 #pragma unroll
       for (int k = 0; k < 24; k++) st.g[lane][k] = sv[k % 3] ? __dadd_rn(nx[k], sL[k % 3]) : nx[k];
-      const double *fr = A.eframe + (size_t)e * 24;
+      const double *fr = A.eframe + (size_t)e * EFR;
 #pragma unroll
       for (int k = 0; k < 9; k++) st.fr[lane][k] = (float)fr[13 + k];
 #pragma unroll
       for (int d = 0; d < 3; d++) st.fr[lane][9 + d] = (float)(q.xi[d] - sL[d] - fr[d]);
       const float lim = (float)(A.cutneigh + fr[12]) + 1e-3f;
       st.fr[lane][12] = lim * lim;
+      const int n1s = hi[1] - lo[1] + 1, n2s = hi[2] - lo[2] + 1;
+      st.mg[lane][0] = (65536 + n2s - 1) / n2s;
+      st.mg[lane][1] = (65536 + n1s - 1) / n1s;
     }
     __syncwarp();
     // exclusive prefix of the box sizes over the group's lanes
@@ -583,6 +653,7 @@ __device__ void items_warp(const BuildArgs &A, const Query &q, const int2 *items
     const int excl = incl - nbox;
     const int total = __shfl_sync(0xffffffffu, incl, 31);
     const int ng = min(32, n - g0);
+    int qn = 0;   // queued sites (warp-uniform)
     for (int base = 0; base < total; base += 32) {
       const int f = base + lane;
       // item of flattened site f: the last lane m < ng with excl[m] <= f
@@ -593,66 +664,44 @@ __device__ void items_warp(const BuildArgs &A, const Query &q, const int2 *items
         const int v = __shfl_sync(0xffffffffu, excl, cand & 31);
         if (cand < ng && v <= f) m = cand;
       }
-      const int2 itm = make_int2(__shfl_sync(0xffffffffu, it.x, m), __shfl_sync(0xffffffffu, it.y, m));
       const int exm = __shfl_sync(0xffffffffu, excl, m);
-      bool pf = false, ph = false;
-      int val = 0, codef = 0, code = 0;
+      bool pass = false;
+      int u = 0;
       if (f < total) {
-        int e, sv[3], lo[3], hi[3];
-        unpack_item(itm, e, sv, lo, hi);
-        const bool zero = (sv[0] == 0 && sv[1] == 0 && sv[2] == 0);
-        const bool far_image = sv[0] < -1 || sv[0] > 1 || sv[1] < -1 || sv[1] > 1 || sv[2] < -1 || sv[2] > 1;
-        code = far_image ? 0 : img_code(sv[0], sv[1], sv[2]);
-        const int n1 = hi[1] - lo[1] + 1, n2 = hi[2] - lo[2] + 1;
+        const int y = st.item[m].y;
+        const int lo0 = y & 15, lo1 = (y >> 4) & 15, lo2 = (y >> 8) & 15;
+        const int n1 = ((y >> 16) & 15) - lo1 + 1, n2 = ((y >> 20) & 15) - lo2 + 1;
+        // (a, bb, cc) of the t-th site of the box in (a, bb, cc) order; the
+        // multiply-shift quotients are exact for t < 729 and extents <= 9
         const int t = f - exm;
-        const int cc = lo[2] + t % n2, bb = lo[1] + (t / n2) % n1, a = lo[0] + t / (n1 * n2);
+        const int q2 = (t * st.mg[m][0]) >> 16, q12 = (q2 * st.mg[m][1]) >> 16;
+        const int cc = lo2 + (t - q2 * n2), bb = lo1 + (q2 - q12 * n1), a = lo0 + q12;
         const float *F = st.fr[m];
         const float ex = F[9] - (a * F[0] + bb * F[3] + cc * F[6]);
         const float ey = F[10] - (a * F[1] + bb * F[4] + cc * F[7]);
         const float ez = F[11] - (a * F[2] + bb * F[5] + cc * F[8]);
-        const int u = (a * NC + bb) * NC + cc;
-        if (ex * ex + ey * ey + ez * ez <= F[12] && !(!q.iatom && e == q.ie && u == q.iu && zero)) {
-          const double *g = st.g[m];
-          double dx = q.xi[0], dy = q.xi[1], dz = q.xi[2];
-#pragma unroll
-          for (int k = 0; k < 8; k++) {
-            double N = shape_val(u, k);
-            dx = __dsub_rn(dx, __dmul_rn(N, g[3 * k]));
-            dy = __dsub_rn(dy, __dmul_rn(N, g[3 * k + 1]));
-            dz = __dsub_rn(dz, __dmul_rn(N, g[3 * k + 2]));
-          }
-          double rsq = rsq_rn(dx, dy, dz);
-          if (rsq <= A.cutneighsq) {
-            if (far_image) {
-              atomicExch(&A.overflow[2], 1);
-            } else {
-              pf = true;
-              val = KIND_SITE | (e * NU + u);
-              codef = code | (rsq < A.cutforcesq ? IN_CUT : 0);
-              if (site_gauss(u) < 0) A.site_flag[e * NU + u] = 1;   // to be interpolated
-              ph = true;
-              if (A.want_half && !q.iatom) {
-                int jg = site_gauss(u);
-                if (jg >= 0) {
-                  if (zero) {
-                    ph = (q.ie < e) || (q.ie == e && q.ig < jg);
-                  } else {
-                    const double4 ce = A.ecenter[e], ci = A.ecenter[q.ie];
-                    const double sL[3] = {sv[0] * q.r.b.L[0], sv[1] * q.r.b.L[1], sv[2] * q.r.b.L[2]};
-                    double qcen[3] = {sv[0] ? __dadd_rn(ce.x, sL[0]) : ce.x, sv[1] ? __dadd_rn(ce.y, sL[1]) : ce.y,
-                                      sv[2] ? __dadd_rn(ce.z, sL[2]) : ce.z};
-                    double icen[3] = {ci.x, ci.y, ci.z};
-                    ph = above_right(qcen, icen);
-                  }
-                }
-              }
-            }
-          }
+        u = (a * NC + bb) * NC + cc;
+        pass = ex * ex + ey * ey + ez * ez <= F[12];
+        if (pass && !q.iatom && u == q.iu) {
+          // the query's own site (same element, zero image)
+          const int x = st.item[m].x;
+          pass = !((x & ((1 << 21) - 1)) == q.ie && (x >> 21) == ((4 << 6) | (4 << 3) | 4));
         }
       }
-      warp_emit(A, q.slot, nf, A.raw_full, A.img_full, pf, val, codef);
-      if (A.want_half) warp_emit(A, q.slot, nh, A.raw_half, A.img_half, ph, val, code);
+      const unsigned mask = __ballot_sync(0xffffffffu, pass);
+      if (pass) st.queue[qn + __popc(mask & lanemask_lt())] = (m << 10) | u;
+      qn += __popc(mask);
+      __syncwarp();
+      if (qn >= 32) {
+        items_exact(A, q, st, true, st.queue[lane], nf, nh);
+        qn -= 32;
+        const int rest = lane < qn ? st.queue[32 + lane] : 0;
+        __syncwarp();
+        if (lane < qn) st.queue[lane] = rest;
+        __syncwarp();
+      }
     }
+    if (qn > 0) items_exact(A, q, st, lane < qn, lane < qn ? st.queue[lane] : 0, nf, nh);
   }
 }
 
@@ -989,7 +1038,7 @@ void neigh_plan(Ctx &c, bool want_half) {
   c.cutneigh = cutoff + c.skin;
   c.cutneighsq = c.cutneigh * c.cutneigh;
   c.ecenter.reserve(std::max(c.ne, 1));
-  c.eframe.reserve((size_t)std::max(c.ne, 1) * 24);
+  c.eframe.reserve((size_t)std::max(c.ne, 1) * EFR);
   c.overflow.reserve(16);
   c.dev_nact.reserve(1);
   c.inner_margin = c.inner_margin_set >= 0.0 ? c.inner_margin_set : 0.4 * c.skin;
@@ -1258,9 +1307,15 @@ void neigh_build_async(Ctx &c, bool want_half) {
     if (c.na && c.ne) {
       if (split) CACB200_CUDA(cudaStreamWaitEvent(c.stream, c.items_ev, 0));
       KernelTimer t(c, "build_atom_sites");
-      k_build_atom_sites<<<stride_grid(32L * c.na, 128), 128, 0, c.stream>>>(A, P, c.items.p, c.nitems.p,
-                                                                            c.item_cap, c.atom_work.p,
-                                                                            c.atom_nwork.p);
+      // the warps stride over the work list: one wave of resident blocks
+      static const int per_sm = [] {
+        int b = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_build_atom_sites<decltype(P)>, 128, 0);
+        return b > 0 ? b : 1;
+      }();
+      const int grid = (int)std::min<long>(stride_grid(32L * c.na, 128), (long)per_sm * c.num_sms);
+      k_build_atom_sites<<<grid, 128, 0, c.stream>>>(A, P, c.items.p, c.nitems.p, c.item_cap, c.atom_work.p,
+                                                     c.atom_nwork.p);
     }
     if (split) CACB200_CUDA(cudaStreamWaitEvent(c.stream, c.join_ev, 0));
   });
