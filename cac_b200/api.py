@@ -64,6 +64,7 @@ SIGNATURES = [
     ("cacb200_unset_deform", C.c_int, [C.c_void_p]),
     ("cacb200_set_graphs", C.c_int, [C.c_void_p, C.c_int]),
     ("cacb200_set_list_prefix", C.c_int, [C.c_void_p, C.c_double]),
+    ("cacb200_set_neighbor_modify", C.c_int, [C.c_void_p, C.c_int, C.c_int]),
     ("cacb200_run_begin", C.c_int, [C.c_void_p, C.c_int, C.c_double, C.c_int, C.c_int]),
     ("cacb200_run_steps", C.c_int, [C.c_void_p, C.c_int, C.c_double, C.c_int, C.c_int]),
     ("cacb200_device_array", C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_void_p), C.POINTER(C.c_int64)]),
@@ -287,6 +288,11 @@ class Engine:
             __cuda_array_interface__ = {"shape": shape, "typestr": "<f8", "data": (ptr.value or 0, False),
                                         "version": 3, "strides": None}
         return torch.as_tensor(_View(), device=torch.device("cuda", self.device))
+
+    def neighbor_modify(self, delay: int = 0, check: bool = False) -> None:
+        """neigh_modify delay D check yes|no (the every of ``neighbor`` stays)."""
+        self._check(self.lib.cacb200_set_neighbor_modify(self.h, delay, 1 if check else 0),
+                    "set_neighbor_modify")
 
     def list_prefix(self, margin: float) -> None:
         """Inner-prefix margin of the lists (< 0: default 0.4 x skin, 0: off)."""

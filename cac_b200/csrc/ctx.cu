@@ -362,6 +362,16 @@ void build(Ctx &c, bool want_half) {
   c.last_build_step = c.step;
 }
 
+// Neighbor::decide (neighbor.cpp:1584-1604): a rebuild is due when at least
+// `delay` steps have passed since the last one and their count is a multiple
+// of `every`; with check yes it happens only when a site has moved past the
+// trigger (otherwise the next one is due `every` steps later).
+bool rebuild_due(Ctx &c) {
+  const long ago = c.step - c.last_build_step;
+  if (c.every <= 0 || ago < c.delay || ago % c.every != 0) return false;
+  return !c.dist_check || moved_past_trigger(c);
+}
+
 void forces(Ctx &c, int eflag, int vflag) {
   interpolate_sites(c);
   pair_compute(c, eflag, vflag);
@@ -456,6 +466,7 @@ void nve_cycle(Ctx &c, double dt) {
   c.lists_valid = true;
   c.nact_known = false;
   if (neigh_check(c)) neigh_build(c, false);   // plan grew: rebuild once more, synchronously
+  note_build_box(c);
   c.last_build_step = c.step;
   if (c.graph_gen == c.gen) {
     CACB200_CUDA(cudaGraphLaunch(c.g_steps, c.stream));
@@ -509,8 +520,11 @@ void run_steps(Ctx &c, int nsteps, double dt, int eflag, int vflag) {
   c.check_system();
   if (nsteps < 0) throw Error(CACB200_EINVAL, "negative step count");
   if (nsteps > c.run_left) throw Error(CACB200_ESTATE, "more steps than the run begun has left");
-  // a deforming box changes launch arguments every step: no graph replay
-  const bool graphs = c.graphs_enabled && c.every > 0 && !c.prof.enabled && !c.dfm.on;
+  // a deforming box changes launch arguments every step, and the check of
+  // check yes decides on the host: no graph replay for either (nor for a
+  // delay that moves the rebuilds off the multiples of every)
+  const bool graphs = c.graphs_enabled && c.every > 0 && !c.prof.enabled && !c.dfm.on && !c.dist_check &&
+                      c.delay <= c.every;
   const bool want_ev = eflag || vflag;
   int s = 1;
   while (s <= nsteps) {
@@ -523,7 +537,7 @@ void run_steps(Ctx &c, int nsteps, double dt, int eflag, int vflag) {
     }
     nve_initial(c, dt);
     c.step++;
-    if (c.every > 0 && (c.step - c.last_build_step) % c.every == 0) build(c, false);
+    if (rebuild_due(c)) build(c, false);
     bool last = (s == nsteps);
     forces(c, last ? eflag : 0, last ? vflag : 0);
     langevin_post_force(c, dt);
@@ -566,7 +580,7 @@ void minimize_fire(Ctx &c, double etol, double ftol, int maxiter, double dt, int
         fire_step(c);
         done++;
         c.step++;
-        if (c.every > 0 && (c.step - c.last_build_step) % c.every == 0) build(c, false);
+        if (rebuild_due(c)) build(c, false);
         forces(c, CACB200_ENERGY_GLOBAL, 0);
       }
       s = fire_read(c);
@@ -912,6 +926,14 @@ int cacb200_set_neighbor(cacb200_ctx *ctx, double skin, int every) {
   c.lists_valid = false;
   c.planned = false;
   c.gen++;
+  API_END
+}
+
+int cacb200_set_neighbor_modify(cacb200_ctx *ctx, int delay, int check) {
+  API_BEGIN
+  if (delay < 0 || (check != 0 && check != 1)) throw Error(CACB200_EINVAL, "invalid delay or check");
+  c.delay = delay;
+  c.dist_check = check;
   API_END
 }
 

@@ -259,6 +259,10 @@ struct Ctx {
   // neighbour lists: transposed [cap][nsite_i] packed entries (sidx << 5 | img)
   double skin = 1.0, cutneigh = 0.0, cutneighsq = 0.0;
   int every = 10;
+  int delay = 0;                 // neigh_modify delay: no rebuild before this many steps
+  int dist_check = 0;            // neigh_modify check yes: a due rebuild only after a move > trigger
+  std::vector<double> build_box; // [nrep*6] replica boxes (lo, hi) at the last build
+  DBuf<int> moved;               // flag of the displacement check
   int cap = 160;
   DBuf<int> nbr_full, num_full;
   // inner prefix of the full lists: entries within cut + inner_margin at the
@@ -373,6 +377,17 @@ struct KernelTimer {
   ~KernelTimer();
 };
 
+// The replica boxes the lists are built in (the trigger of the displacement
+// check shrinks by the box corners' movement since then).
+inline void note_build_box(Ctx &c) {
+  c.build_box.resize(6 * (size_t)c.rep_h.size());
+  for (size_t r = 0; r < c.rep_h.size(); r++)
+    for (int d = 0; d < 3; d++) {
+      c.build_box[6 * r + d] = c.rep_h[r].b.lo[d];
+      c.build_box[6 * r + 3 + d] = c.rep_h[r].b.hi[d];
+    }
+}
+
 // stages implemented in the .cu files
 void neigh_build(Ctx &c, bool want_half);
 void neigh_plan(Ctx &c, bool want_half);
@@ -386,6 +401,7 @@ void pair_compute(Ctx &c, int eflag, int vflag);
 void pair_compute_mixed(Ctx &c, int eflag, int vflag);
 void assemble_nodef(Ctx &c);
 void nve_initial(Ctx &c, double dt);
+bool moved_past_trigger(Ctx &c);
 void nve_final(Ctx &c, double dt);
 void eam_tables(Ctx &c, const double *frho, const double *rhor, const double *z2r);
 void fire_init(Ctx &c, double dt);

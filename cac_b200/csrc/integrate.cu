@@ -172,6 +172,62 @@ void nve_initial(Ctx &c, double dt) {
       lim / 1.7320508075688772, c.nrep > 1 ? c.site_rep.p : nullptr, c.nrep > 1 ? c.elem_rep.p : nullptr);
 }
 
+// Neighbor::check_distance (neighbor.cpp:1617-1683): does any atom or node
+// lie farther than the trigger distance from where the lists were built?
+// (the reference's operation order, without fused multiply-adds)
+__global__ void k_moved(const double4 *xs, const double4 *xb, int na, const double *nodex, const double *nxb,
+                        int nnode, double deltasq, int *flag) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  double dx, dy, dz;
+  if (t < na) {
+    const double4 p = xs[t], b = xb[t];
+    dx = p.x - b.x;
+    dy = p.y - b.y;
+    dz = p.z - b.z;
+  } else if (t < na + nnode) {
+    const double *p = nodex + 3 * (size_t)(t - na), *b = nxb + 3 * (size_t)(t - na);
+    dx = p[0] - b[0];
+    dy = p[1] - b[1];
+    dz = p[2] - b[2];
+  } else {
+    return;
+  }
+  const double rsq = __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
+  if (rsq > deltasq) *flag = 1;
+}
+
+// The check of neigh_modify check yes.  Trigger: half the skin
+// (triggersq, neighbor.cpp:240); while the box changes, half of the skin
+// less the movement of the box's lo and hi corners since the build
+// (orthogonal boxes; for a batch the smallest over its replicas).  Reads one
+// flag back (synchronises).
+bool moved_past_trigger(Ctx &c) {
+  double deltasq = 0.25 * c.skin * c.skin;
+  if (c.dfm.on && c.build_box.size() == 6 * c.rep_h.size()) {
+    bool first = true;
+    for (size_t r = 0; r < c.rep_h.size(); r++) {
+      const BoxD &B = c.rep_h[r].b;
+      const double *h = c.build_box.data() + 6 * r;
+      const double lx = B.lo[0] - h[0], ly = B.lo[1] - h[1], lz = B.lo[2] - h[2];
+      const double delta1 = sqrt(lx * lx + ly * ly + lz * lz);
+      const double ux = B.hi[0] - h[3], uy = B.hi[1] - h[4], uz = B.hi[2] - h[5];
+      const double delta2 = sqrt(ux * ux + uy * uy + uz * uz);
+      const double delta = 0.5 * (c.skin - (delta1 + delta2));
+      if (first || delta * delta < deltasq) deltasq = delta * delta;
+      first = false;
+    }
+  }
+  c.moved.reserve(1);
+  CACB200_CUDA(cudaMemsetAsync(c.moved.p, 0, sizeof(int), c.stream));
+  const int n = c.na + 8 * c.ne;
+  if (n)
+    k_moved<<<nblk(n, 256), 256, 0, c.stream>>>(c.xs.p, c.xbuild.p, c.na, c.nodex.p, c.nodex_build.p, 8 * c.ne,
+                                                deltasq, c.moved.p);
+  int h = 0;
+  stream_copy(c, &h, c.moved.p, sizeof(int), cudaMemcpyDeviceToHost);
+  return h != 0;
+}
+
 void nve_final(Ctx &c, double dt) {
   double dtf = 0.5 * dt * (1.0 / 1.0364269e-4);
   double dtfm = dtf / c.mass;

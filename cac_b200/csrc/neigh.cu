@@ -1374,7 +1374,10 @@ void neigh_build(Ctx &c, bool want_half) {
     neigh_plan(c, want_half || c.plan_half);
   for (int attempt = 0; attempt < 4; attempt++) {
     neigh_build_async(c, want_half);
-    if (!neigh_check(c)) return;
+    if (!neigh_check(c)) {
+      note_build_box(c);
+      return;
+    }
   }
   throw Error(CACB200_EOVERFLOW, "neighbour list capacity could not be settled");
 }

@@ -27,6 +27,8 @@
 #include "update.h"
 
 #include "cacb200.h"
+#include "pair_eam_alloy_b200.h"
+#include "pair_lj_cut_b200.h"
 
 using namespace CAC_NS;
 
@@ -207,6 +209,7 @@ void B200Bridge::run_nve(int nsteps, double dt, int every, const B200Fixes &fx, 
   check_system();
   upload(true);
   status(cacb200_set_neighbor(ctx, neighbor->skin, every), "set_neighbor");
+  status(cacb200_set_neighbor_modify(ctx, neighbor->delay, neighbor->dist_check), "set_neighbor_modify");
   if (fx.langevin) {
     status(cacb200_set_langevin(ctx, fx.t_start, fx.t_stop, fx.t_period, fx.seed, fx.zero), "set_langevin");
     status(cacb200_set_langevin_stream(ctx, fx.draws), "set_langevin_stream");
@@ -251,6 +254,34 @@ void B200Bridge::run_nve(int nsteps, double dt, int every, const B200Fixes &fx, 
         element->gaussf[e][0][n][d] = gbuf[24 * (size_t)e + 3 * n + d];
       }
   uploaded_na = uploaded_ne = -1;   // the reference must set up again (ghosts are stale)
+}
+
+void B200Bridge::minimize_fire(double etol, double ftol, int maxiter, double dt, int normstyle,
+                               const B200Fire &p, int &stop, int &niter, double &energy, double &fnorm)
+{
+  check_system();
+  upload(false);
+  status(cacb200_set_neighbor(ctx, neighbor->skin, neighbor->every), "set_neighbor");
+  status(cacb200_set_neighbor_modify(ctx, neighbor->delay, neighbor->dist_check), "set_neighbor_modify");
+  status(cacb200_set_fire_params(ctx, p.delaystep, p.dtgrow, p.dtshrink, p.alpha0, p.alphashrink, p.tmax,
+                                 p.tmin, p.dmax, p.halfstepback, p.delaystep_start, p.max_vdotf_negatif),
+         "set_fire_params");
+  status(cacb200_minimize_fire(ctx, etol, ftol, maxiter, dt, normstyle, &stop, &niter, &energy, &fnorm),
+         "minimize_fire");
+  int na = atom->nlocal, ne = element->nlocal;
+  status(cacb200_get_state(ctx, na ? &atom->x[0][0] : nullptr, nullptr, ne ? &element->nodex[0][0][0][0] : nullptr,
+                           nullptr),
+         "get_state");
+  // element centres follow the nodes (ElementVecCAC::update_center_coord)
+  if (ne) element->evec->update_center_coord();
+  uploaded_na = uploaded_ne = -1;   // the reference sets up again (ghosts are stale)
+}
+
+B200Bridge *CAC_NS::b200_bridge_of(Pair *pair)
+{
+  if (auto *p = dynamic_cast<PairLJCutB200 *>(pair)) return p->bridge;
+  if (auto *p = dynamic_cast<PairEAMAlloyB200 *>(pair)) return p->bridge;
+  return nullptr;
 }
 
 // Positions and velocities (and the box, when it deforms) from the device

@@ -37,6 +37,15 @@ struct B200Fixes {
   double deform_a[3] = {0, 0, 0}, deform_b[3] = {0, 0, 0};
 };
 
+// min_style fire/b200: the FIRE parameters of Min (min.h:61-72) with the
+// reference's defaults (min.cpp:33-47)
+struct B200Fire {
+  int delaystep = 20;
+  double dtgrow = 1.1, dtshrink = 0.5, alpha0 = 0.25, alphashrink = 0.99;
+  double tmax = 10.0, tmin = 0.02, dmax = 0.1;
+  int halfstepback = 1, delaystep_start = 1, max_vdotf_negatif = 2000;
+};
+
 class B200Bridge : protected Pointers {
  public:
   explicit B200Bridge(class CAC *);
@@ -51,6 +60,12 @@ class B200Bridge : protected Pointers {
   // run N velocity-Verlet steps on the device (run_b200 command), with the
   // given thermostat / deformation; thermo lines on the reference's schedule
   void run_nve(int nsteps, double dt, int every, const B200Fixes &fixes, bool thermo_output);
+  // minimise on the device from the reference's current state (min_style
+  // fire/b200) under the reference's current neighbour rule; the final
+  // positions come back into atom->x / element->nodex (velocities are left
+  // as they are, as by the reference's minimisers)
+  void minimize_fire(double etol, double ftol, int maxiter, double dt, int normstyle, const B200Fire &p,
+                     int &stop, int &niter, double &energy, double &fnorm);
   // canonical neighbour-list dump (write_b200_neighbor command)
   void dump_list(const char *file, int half);
 
@@ -73,6 +88,9 @@ class B200Bridge : protected Pointers {
   void configure_pair();
   void status(int rc, const char *what);
 };
+
+// The bridge of a /b200 pair style (lj/cut/b200, eam/alloy/b200), else null.
+B200Bridge *b200_bridge_of(class Pair *pair);
 
 }  // namespace CAC_NS
 

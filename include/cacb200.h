@@ -211,6 +211,18 @@ int cacb200_set_nodal_energy_weight(cacb200_ctx *ctx, double w);
 
 /* neighbor SKIN bin + neigh_modify every N delay 0 check no (neighbor.cpp:2043) */
 int cacb200_set_neighbor(cacb200_ctx *ctx, double skin, int every);
+/* neigh_modify delay D check yes|no (check 1|0; defaults 0 and 0, the
+ * settings of cacb200_set_neighbor alone).  A rebuild is due when at least
+ * `delay` steps have passed since the last one and their count is a multiple
+ * of `every`; with check yes it then happens only when an atom or node has
+ * moved more than half the skin since the last build, less the box corners'
+ * movement while the box deforms, and otherwise the next one is due `every`
+ * steps later (Neighbor::decide / check_distance, neighbor.cpp:1584-1683).
+ * The reference's minimiser runs with every 1 delay 0 check yes (Min::init,
+ * min.cpp:155-169).  Honoured by cacb200_run_nve / cacb200_run_steps (which
+ * replay no graphs under check yes or a delay above every) and
+ * cacb200_minimize_fire. */
+int cacb200_set_neighbor_modify(cacb200_ctx *ctx, int delay, int check);
 /* The inner prefix of the lists (no reference counterpart; an evaluation
  * order, not a different result): entries within cutoff + margin at the
  * build are stored first, and while no site has moved half the margin since
@@ -330,8 +342,10 @@ int cacb200_set_fire_params(cacb200_ctx *ctx, int delaystep, double dtgrow, doub
 /* minimize etol ftol maxiter (Minimize::command, minimize.cpp:21-70, with
  * nodal/weight 1) by a device FIRE iterate over atoms + nodes: FIRE 2.0 of
  * Guenole et al. 2020 with the FIRE parameters and defaults the reference's
- * Min carries (its own min styles are cg and sd; it has no FIRE style, so
- * this minimiser has no input-deck form here).  normstyle: 0 two-norm, 1 max
+ * Min carries (its own min styles are cg and sd, with no FIRE style; the
+ * input-deck form is the package's min_style fire/b200, a Min subclass that
+ * calls this with the rule Min::init sets, cacb200_set_neighbor_modify).
+ * The lists follow cacb200_set_neighbor / _modify.  normstyle: 0 two-norm, 1 max
  * per-site norm, 2 inf norm (min_modify norm two|max|inf).  Returns the stop
  * code of min.h:46-47 (0 MAXITER, 2 ETOL, 3 FTOL, 11 MAXVDOTF), iterations,
  * final energy and force norm (squared, in the chosen style). */

@@ -95,6 +95,32 @@ static double g_wsa[NG * 8], g_nodal_weight, g_minv[64];
 /* Pair::nodal_energy_weight (pair.cpp:38); minimize sets it to 1 (minimize.cpp:37) */
 static double g_nodal_energy_weight = -1.0;
 static int g_tables_ready = 0;
+/* neigh_modify check yes for the minimiser: a due rebuild only after a move
+ * past half the skin (Neighbor::decide / check_distance, neighbor.cpp:1584-1683) */
+static int g_neigh_check = 0;
+
+void oracle_set_neighbor_check(int check) { g_neigh_check = check != 0; }
+
+/* Neighbor::check_distance for a fixed box (neighbor.cpp:1617-1683):
+ * 1 when an atom or node lies farther than sqrt(triggersq) from its position
+ * at the last build, triggersq = 0.25 skin^2 (neighbor.cpp:240). */
+static int moved_past_trigger(const oracle_state *s, const double *xhold, const double *nodexhold,
+                              double skin)
+{
+  const double triggersq = 0.25 * skin * skin;
+  int flag = 0;
+  for (int i = 0; i < s->natoms; i++) {
+    double delx = s->x[3 * i] - xhold[3 * i], dely = s->x[3 * i + 1] - xhold[3 * i + 1];
+    double delz = s->x[3 * i + 2] - xhold[3 * i + 2];
+    if (delx * delx + dely * dely + delz * delz > triggersq) flag = 1;
+  }
+  for (int k = 0; k < 8 * s->nelements; k++) {
+    double delx = s->nodex[3 * k] - nodexhold[3 * k], dely = s->nodex[3 * k + 1] - nodexhold[3 * k + 1];
+    double delz = s->nodex[3 * k + 2] - nodexhold[3 * k + 2];
+    if (delx * delx + dely * dely + delz * delz > triggersq) flag = 1;
+  }
+  return flag;
+}
 
 static void tables(void)
 {
@@ -1022,6 +1048,17 @@ int oracle_minimize_fire(oracle_state *s, int pair, double p0, double p1, double
   oracle_pbc(s);
   if (oracle_build_list(s, cutneigh, 1, &L)) return -1;
   size_t na3 = 3 * (size_t) s->natoms, nn3 = 24 * (size_t) s->nelements;
+  /* positions at the last build (Neighbor::build keeps xhold / nodexhold) */
+  double *xhold = malloc(sizeof(double) * (na3 ? na3 : 1));
+  double *nodexhold = malloc(sizeof(double) * (nn3 ? nn3 : 1));
+  if (!xhold || !nodexhold) {
+    free(xhold);
+    free(nodexhold);
+    oracle_free_list(&L);
+    return -1;
+  }
+  memcpy(xhold, s->x, sizeof(double) * na3);
+  memcpy(nodexhold, s->nodex, sizeof(double) * nn3);
   memset(s->v, 0, sizeof(double) * na3);
   memset(s->nodev, 0, sizeof(double) * nn3);
   double ecur = fire_energy(s, &L, pair, p0, p1, p2, eam), eprev = ecur;
@@ -1111,15 +1148,24 @@ int oracle_minimize_fire(oracle_state *s, int pair, double p0, double p1, double
         v[k] = vd;
       }
     }
-    if (every > 0 && (step - last_build) % every == 0) {
+    if (every > 0 && (step - last_build) % every == 0 &&
+        (!g_neigh_check || moved_past_trigger(s, xhold, nodexhold, skin))) {
       oracle_free_list(&L);
       oracle_pbc(s);
-      if (oracle_build_list(s, cutneigh, 1, &L)) return -1;
+      if (oracle_build_list(s, cutneigh, 1, &L)) {
+        free(xhold);
+        free(nodexhold);
+        return -1;
+      }
       last_build = step;
+      memcpy(xhold, s->x, sizeof(double) * na3);
+      memcpy(nodexhold, s->nodex, sizeof(double) * nn3);
     }
     eprev = ecur;
     ecur = fire_energy(s, &L, pair, p0, p1, p2, eam);
   }
+  free(xhold);
+  free(nodexhold);
   oracle_free_list(&L);
   g_nodal_energy_weight = saved_w;
   *code = status;

@@ -92,6 +92,10 @@ void oracle_pbc(oracle_state *s);
 int oracle_run_nve(oracle_state *s, int pair, double p0, double p1, double p2,
                    const oracle_eam *eam, double skin, double dt, int nsteps, int every);
 
+/* neigh_modify check yes|no for oracle_minimize_fire (default no): a rebuild
+ * due by `every` happens only after an atom or node moved past half the skin */
+void oracle_set_neighbor_check(int check);
+
 /* FIRE minimisation (see cac_oracle.c); par holds the 11 Min parameters */
 int oracle_minimize_fire(oracle_state *s, int pair, double p0, double p1, double p2,
                          const oracle_eam *eam, double skin, double dt0, double etol, double ftol,

@@ -83,6 +83,7 @@ def lib():
                                            C.POINTER(_Eam), C.c_double, C.c_double, C.c_double, C.c_double,
                                            C.c_int, C.c_int, C.c_int, _dp, C.POINTER(C.c_int),
                                            C.POINTER(C.c_int), _dp, _dp]
+        L.oracle_set_neighbor_check.argtypes = [C.c_int]
         L.oracle_shape_array.argtypes = [_dp]
         L.oracle_gauss_tables.argtypes = [C.POINTER(C.c_int), C.POINTER(C.c_int), _dp, _dp]
         L.oracle_inverse_mass_hex.argtypes = [_dp]
@@ -241,9 +242,13 @@ FIRE_DEFAULTS = (20, 1.1, 0.5, 0.25, 0.99, 10.0, 0.02, 0.1, 1, 1, 2000)
 
 def minimize_fire(state: OracleState, pair: str, *, lj=None, eam: Optional[Eam] = None,
                   skin: float = 1.0, dt: float = 0.001, etol: float = 0.0, ftol: float = 1e-6,
-                  maxiter: int = 5000, norm: str = "max", every: int = 10, params=FIRE_DEFAULTS):
-    """FIRE restated in C; returns (stop_code, iterations, energy, fnorm)."""
+                  maxiter: int = 5000, norm: str = "max", every: int = 10, check: bool = False,
+                  params=FIRE_DEFAULTS):
+    """FIRE restated in C; returns (stop_code, iterations, energy, fnorm).
+    check: neigh_modify check yes (a rebuild due by ``every`` only after a
+    move past half the skin, as the reference's Min runs its lists)."""
     par = np.array(params, dtype=np.float64)
+    lib().oracle_set_neighbor_check(1 if check else 0)
     code, it = C.c_int(), C.c_int()
     e, fn = C.c_double(), C.c_double()
     ns = {"two": 0, "max": 1, "inf": 2}[norm]
@@ -255,6 +260,7 @@ def minimize_fire(state: OracleState, pair: str, *, lj=None, eam: Optional[Eam] 
         rc = lib().oracle_minimize_fire(state.ref, 1, 0.0, 0.0, 0.0, C.byref(eam._e), skin, dt, etol, ftol,
                                         maxiter, ns, every, _ptr(par), C.byref(code), C.byref(it), C.byref(e),
                                         C.byref(fn))
+    lib().oracle_set_neighbor_check(0)
     if rc:
         raise RuntimeError("oracle_minimize_fire failed")
     return code.value, it.value, e.value, fn.value

@@ -103,3 +103,37 @@ def test_fire_short_run_bitwise_close(pair, oracle_mod, tmp_path):
     assert np.abs(x - st.x).max() < 1e-10
     assert np.abs(nx - st.nodex).max() < 1e-10
     e.close()
+
+
+@pytest.mark.parametrize("pair", ["lj", "eam"])
+def test_fire_check_yes_matches_restatement(pair, oracle_mod, tmp_path):
+    """The reference Min's neighbour rule (every 1 delay 0 check yes) on the
+    device and in the C restatement: 20 iterations agree to 1e-10, and a
+    converged run stops like the restatement."""
+    s = gen.tiny(seed=12, temperature=0.0)
+    eam = oracle_mod.Eam(setfl_path(tmp_path)) if pair == "eam" else None
+    e = engine(s, pair, tmp_path, 0)
+    e.neighbor(SKIN, 1)
+    e.neighbor_modify(0, True)
+    e.minimize_fire(ftol=0.0, maxiter=20, norm="two")
+    x, _, nx, _ = e.state()
+    e.close()
+    st = oracle_mod.OracleState(s)
+    oracle_mod.minimize_fire(st, pair, lj=LJ, eam=eam, ftol=0.0, maxiter=20, norm="two", every=1, check=True)
+    assert np.abs(x - st.x).max() < 1e-10
+    assert np.abs(nx - st.nodex).max() < 1e-10
+    if pair == "lj":
+        e = engine(s, pair, tmp_path, 0)
+        e.neighbor(SKIN, 1)
+        e.neighbor_modify(0, True)
+        code, it, en, fn = e.minimize_fire(ftol=1e-6, maxiter=2500, norm="max")
+        x, _, nx, _ = e.state()
+        e.close()
+        st = oracle_mod.OracleState(s)
+        ocode, oit, oen, ofn = oracle_mod.minimize_fire(st, pair, lj=LJ, ftol=1e-6, maxiter=2500, norm="max",
+                                                        every=1, check=True)
+        assert code == ocode == 3
+        assert abs(it - oit) <= max(2, oit // 50)
+        assert abs(en - oen) / abs(oen) < 1e-8
+        assert np.abs(x - st.x).max() < 1e-5
+        assert np.abs(nx - st.nodex).max() < 1e-5

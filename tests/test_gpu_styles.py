@@ -228,3 +228,51 @@ def test_run_b200_thermo_with_both_fixes(golden, tmp_path):
     ref = O.read_thermo(reference_log(tmp_path, "tiny_lj", fixes_ref + THERMO + "run 20\n", O.REF_EXE))
     assert list(ours[:, 0]) == [0, 10, 20]
     assert_thermo_rows(ours, ref, O)
+
+
+# EAM FIRE on these systems does not converge (it ends with elements grown
+# past the box, in the C restatement as on the device): EAM takes the
+# fixed-iteration case only
+@pytest.mark.parametrize("case,stop", [("tiny_lj", "ftol"), ("tiny_lj", "maxiter"), ("tiny_eam", "maxiter")])
+def test_min_style_fire_b200_under_reference_minimize(case, stop, tmp_path):
+    """min_style fire/b200 under the reference's own minimize command: the
+    configuration it ends in is the device minimiser's run through the C ABI
+    with the neighbour rule Min::init sets (every 1 delay 0 check yes), and
+    the reference's Finish reports its stop reason and iteration count."""
+    import oracle
+    from cac_b200.api import Engine
+    build, pair, _ = CASES[case]
+    s = build()
+    gen.write_data(s, str(tmp_path / "data.cac"))
+    gen.write_setfl(gen.EamParams(), str(tmp_path / "cu.setfl"))
+    ftol, maxiter = (1e-6, 3000) if stop == "ftol" else (0.0, 60)
+    body = (f"min_style fire/b200\nmin_modify norm max\nminimize 0.0 {ftol} {maxiter} 100000\n"
+            "oracle_dump end.txt state\n")
+    (tmp_path / "in.cac").write_text(HEADER + pair_lines(pair) + TAIL + body)
+    r = subprocess.run([APP, "-in", "in.cac"], cwd=tmp_path, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stdout[-3000:] + r.stderr[-3000:]
+    d = oracle.read_dump(str(tmp_path / "end.txt"))
+    e = Engine(0)
+    e.upload(s)
+    if pair == "lj":
+        e.pair_lj(0.4093, 2.338, 5.5)
+    else:
+        e.pair_eam(str(tmp_path / "cu.setfl"))
+    e.neighbor(1.0, 1)
+    e.neighbor_modify(0, True)
+    code, it, en, fn = e.minimize_fire(ftol=ftol, maxiter=maxiter, norm="max")
+    x, _, nx, _ = e.state()
+    e.close()
+    assert code == (3 if stop == "ftol" else 0)
+    reason = {3: "force tolerance", 0: "max iterations"}[code]
+    assert f"Stopping criterion = {reason}" in r.stdout
+    if stop == "maxiter":
+        assert f"Iterations, force evaluations = {it} {it}" in r.stdout
+        assert np.abs(d["x"] - x).max() < 1e-10
+        assert np.abs(d["nodex"] - nx).max() < 1e-10
+    else:
+        # converged: the same minimum, the iteration count within 2 %
+        got = int(r.stdout.split("Iterations, force evaluations = ")[1].split()[0])
+        assert abs(got - it) <= max(2, it // 50)
+        assert np.abs(d["x"] - x).max() < 1e-5
+        assert np.abs(d["nodex"] - nx).max() < 1e-5

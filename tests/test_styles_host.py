@@ -50,3 +50,21 @@ def test_fix_styles_equal_reference_fixes_in_reference_loop(fix, oracle_mod, tmp
     ours = run(APP, tmp_path, fix.format(s="/b200"))
     ref = run(oracle_mod.REF_EXE, tmp_path, fix.format(s=""))
     assert ours == ref
+
+
+def test_min_style_fire_b200_registered_and_needs_a_b200_pair(tmp_path):
+    """min_style fire/b200 is a min style of the harness executable (the
+    reference has no FIRE style); with a CPU pair style its setup stops with
+    the style's own message, before any device is touched."""
+    if not os.path.exists(APP):
+        pytest.skip("harness executable not built (make -C oracle app)")
+    gen.write_data(CASES["tiny_lj"][0](), str(tmp_path / "data.cac"))
+    (tmp_path / "in.cac").write_text(HEADER.replace("fix 1 all nve\n", "") +
+                                     "min_style fire/b200\nminimize 0.0 1e-6 10 100\n")
+    r = subprocess.run([APP, "-in", "in.cac"], cwd=tmp_path, capture_output=True, text=True, timeout=600)
+    out = r.stdout + r.stderr
+    assert r.returncode != 0
+    assert "min_style fire/b200 needs pair style lj/cut/b200 or eam/alloy/b200" in out
+    (tmp_path / "in2.cac").write_text(HEADER + "min_style fire\n")
+    r = subprocess.run([APP, "-in", "in2.cac"], cwd=tmp_path, capture_output=True, text=True, timeout=600)
+    assert r.returncode != 0 and "Illegal min_style command" in r.stdout + r.stderr
