@@ -67,13 +67,14 @@ def batch_share(specs, rank: int, ws: int):
     return shard.balanced_partition([ta + 8 * te for ta, te, _, _, _ in specs], ws)[rank]
 
 
-def build_workload(name: str, seed: int, rank: int = 0, ws: int = 1):
+def build_workload(name: str, seed: int, rank: int = 0, ws: int = 1, replicas: int = 256):
     """A rank's workload.  Single systems: one replica per rank (seeded by
-    rank).  Batches: one global set of 256 replicas per GPU, split over the
-    ranks by the size-balanced greedy rule (each rank builds its own share)."""
+    rank).  Batches: one global set of `replicas` (256) replicas per GPU, split
+    over the ranks by the size-balanced greedy rule (each rank builds its own
+    share); a smaller set is the first replicas of the full one."""
     from cac_b200 import gen, shard
     if name == "batch256" and ws > 1:
-        specs = gen.replica_specs(256 * ws, seed=13)
+        specs = gen.replica_specs(replicas * ws, seed=13)
         return [gen.replica_from_spec(specs[i]) for i in batch_share(specs, rank, ws)], "eam"
     if name == "eam_1m":
         return gen.eam_1m(seed=seed), "eam"
@@ -84,7 +85,7 @@ def build_workload(name: str, seed: int, rank: int = 0, ws: int = 1):
     if name == "eam_4m_strained":
         return gen.eam_4m_strained(seed=seed), "eam"
     if name == "batch256":
-        return gen.replica_set(256, seed=11 + seed), "eam"
+        return gen.replica_set(replicas, seed=11 + seed), "eam"
     raise SystemExit(f"unknown workload {name}")
 
 
@@ -261,7 +262,7 @@ def reference_arm(args, rank, ws):
     cores, kind_sample = 1, f"full workload, run {args.warmup} then run {args.steps} steps; rate from Loop time"
     par = "1 core (reference CPU path, single MPI rank)"
     if args.workload.startswith("batch"):
-        systems, pair = build_workload(args.workload, 2)
+        systems, pair = build_workload(args.workload, 2, replicas=args.replicas)
         cores = min(os.cpu_count() or 1, len(systems))
         sample = systems[:cores]
         value, nrep = run_reference_many(sample, pair, args.steps, args.warmup, cores)
@@ -375,7 +376,7 @@ def b200_arm(args, rank, local, ws, dist):
 
     from cac_b200 import shard
     seed = rank_seed(2, rank)
-    s, pair = build_workload(args.workload, seed, rank, ws)
+    s, pair = build_workload(args.workload, seed, rank, ws, replicas=args.replicas)
     units, natoms, nelements = totals(s)
     dev = torch.device("cuda", local)
     units_all = shard.sum_over_ranks(units, dist, dev)
@@ -743,6 +744,8 @@ def main():
     ap.add_argument("--serial-jobs", type=int, default=8,
                     help="serve workload: jobs of the stream timed one at a time in FP64")
     ap.add_argument("--pair", default="lj", choices=["lj", "eam"], help="serve workload: pair style")
+    ap.add_argument("--replicas", type=int, default=256,
+                    help="batch workload: replicas per GPU (fewer = the first of the 256; profiling cases)")
     ap.add_argument("--segment", type=int, default=50,
                     help="steps per trajectory from the seeded initial state (the reference's CAC "
                          "dynamics heat up unboundedly after ~100 steps, so long runs restart)")
