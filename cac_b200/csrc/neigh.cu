@@ -744,7 +744,7 @@ __device__ __forceinline__ void finish_counts(const BuildArgs &A, int i, int nf,
 // the cutoff, which take the exact FP64 test.  The image of a candidate cell
 // relative to each lane's atom is fixed per cell.
 template <class RP>
-__global__ void __launch_bounds__(32) k_build_atoms(BuildArgs A, RP P, int ncell) {
+__device__ __forceinline__ void build_atoms_cells(BuildArgs A, RP P, int ncell) {
   const int lane = threadIdx.x & 31;
   const float fcut2 = (float)A.cutforcesq;
   {
@@ -820,6 +820,17 @@ __global__ void __launch_bounds__(32) k_build_atoms(BuildArgs A, RP P, int ncell
       }
     }
   }
+}
+
+// The single-system form as the compiler allocates it (64 registers); the
+// batch form capped at 64 registers (from 80, a few bytes spilled) so that
+// 32 warps instead of 24 are resident per SM: 10 % faster on a 64-replica
+// batch, where the same cap slowed the single-system form.
+__global__ void __launch_bounds__(32) k_build_atoms(BuildArgs A, OneRep P, int ncell) {
+  build_atoms_cells(A, P, ncell);
+}
+__global__ void __launch_bounds__(32, 32) k_build_atoms(BuildArgs A, ManyRep P, int ncell) {
+  build_atoms_cells(A, P, ncell);
 }
 
 // Phase A over every list slot: the element walk of each atom and Gauss
