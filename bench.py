@@ -488,6 +488,7 @@ def b200_arm(args, rank, local, ws, dist):
 
     # end to end through the C ABI with pinned host buffers: every step copies the
     # state in (x, v, nodes), runs one step, and reads the state back
+    # (cacb200_run_nve_host: the position copy runs beside the step's forces)
     x_h = torch.empty((natoms, 3), dtype=torch.float64).pin_memory().numpy()
     v_h = torch.empty((natoms, 3), dtype=torch.float64).pin_memory().numpy()
     nx_h = torch.empty((nelements, 8, 3), dtype=torch.float64).pin_memory().numpy()
@@ -498,14 +499,10 @@ def b200_arm(args, rank, local, ws, dist):
     nx_h[:] = nx0
     nv_h[:] = nv0
     k_e2e = max(5, min(args.steps, seg))
-    import ctypes as C
-    _p = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))
     torch.cuda.synchronize(local)
     t0 = time.perf_counter()
     for _ in range(k_e2e):
-        eng._check(eng.lib.cacb200_set_state(eng.h, _p(x_h), _p(v_h), _p(nx_h), _p(nv_h)), "set_state")
-        eng.run_nve(1, 0.001)
-        eng._check(eng.lib.cacb200_get_state(eng.h, _p(x_h), _p(v_h), _p(nx_h), _p(nv_h)), "get_state")
+        eng.run_nve_host(1, x_h, v_h, nx_h, nv_h, 0.001)
     e2e_s = max_over_ranks(time.perf_counter() - t0, dist, torch.device("cuda", local))
     e2e_value = units_all * k_e2e / e2e_s
     bytes_state = 8 * (6 * natoms + 48 * nelements)

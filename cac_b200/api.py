@@ -113,6 +113,8 @@ SIGNATURES = [
     ("cacb200_nve_final", C.c_int, [C.c_void_p, C.c_double]),
     ("cacb200_setup", C.c_int, [C.c_void_p]),
     ("cacb200_run_nve", C.c_int, [C.c_void_p, C.c_int, C.c_double, C.c_int, C.c_int]),
+    ("cacb200_run_nve_host", C.c_int, [C.c_void_p, C.c_int, C.c_double, C.POINTER(C.c_double),
+                                      C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     ("cacb200_set_fire_params", C.c_int, [C.c_void_p, C.c_int, C.c_double, C.c_double, C.c_double,
                                           C.c_double, C.c_double, C.c_double, C.c_double, C.c_int,
                                           C.c_int, C.c_int]),
@@ -430,6 +432,18 @@ class Engine:
 
     def run_nve(self, nsteps: int, dt: float = 0.001, eflag: int = 0, vflag: int = 0) -> None:
         self._check(self.lib.cacb200_run_nve(self.h, nsteps, dt, eflag, vflag), "run_nve")
+
+    def run_nve_host(self, nsteps: int, x, v, nodex, nodev, dt: float = 0.001) -> None:
+        """State in from host arrays, nsteps of NVE, state back into the same
+        arrays (float64, C order; pinned memory lets the position copy run
+        beside the last step's forces)."""
+        arrs = []
+        for a in (x, v, nodex, nodev):
+            if not (isinstance(a, np.ndarray) and a.dtype == np.float64 and a.flags.c_contiguous
+                    and a.flags.writeable):
+                raise ValueError("run_nve_host needs writable C-contiguous float64 arrays")
+            arrs.append(_p(a))
+        self._check(self.lib.cacb200_run_nve_host(self.h, nsteps, dt, *arrs), "run_nve_host")
 
     def fire_params(self, delaystep=20, dtgrow=1.1, dtshrink=0.5, alpha0=0.25, alphashrink=0.99,
                     tmax=10.0, tmin=0.02, dmax=0.1, halfstepback=True, delaystep_start=True,

@@ -61,6 +61,8 @@ Ctx::Ctx(int dev) : device(dev) {
   CACB200_CUDA(cudaEventCreateWithFlags(&fork_ev, cudaEventDisableTiming));
   CACB200_CUDA(cudaEventCreateWithFlags(&join_ev, cudaEventDisableTiming));
   CACB200_CUDA(cudaEventCreateWithFlags(&items_ev, cudaEventDisableTiming));
+  CACB200_CUDA(cudaStreamCreateWithFlags(&copy, cudaStreamNonBlocking));
+  CACB200_CUDA(cudaEventCreateWithFlags(&pos_ev, cudaEventDisableTiming));
 }
 
 Ctx::~Ctx() {
@@ -73,6 +75,11 @@ Ctx::~Ctx() {
   if (fork_ev) cudaEventDestroy(fork_ev);
   if (join_ev) cudaEventDestroy(join_ev);
   if (items_ev) cudaEventDestroy(items_ev);
+  if (copy) {
+    cudaStreamSynchronize(copy);
+    cudaStreamDestroy(copy);
+  }
+  if (pos_ev) cudaEventDestroy(pos_ev);
   if (stream) {
     cudaStreamSynchronize(stream);
     auto &pend = pending_for(*this);
@@ -554,6 +561,57 @@ void run_nve(Ctx &c, int nsteps, double dt, int eflag, int vflag) {
   run_steps(c, nsteps, dt, eflag, vflag);
 }
 
+// A run from host state to host state: the state is copied in (as by
+// set_state), nsteps are run, and the state is copied out.  The positions
+// are final once the last step's drift and its list rebuild (which wraps
+// them into the box) are done, so their copy to the host runs on a second
+// stream while that step's forces are evaluated; the velocities follow its
+// second half-kick.  (A deforming box remaps positions at the end of the
+// step: then every copy waits for the step.)
+void run_nve_host(Ctx &c, int nsteps, double dt, double *x, double *v, double *nodex, double *nodev) {
+  c.check_system();
+  if (nsteps < 0) throw Error(CACB200_EINVAL, "negative step count");
+  set_state(c, x, v, nodex, nodev);
+  run_begin(c, nsteps, dt, 0, 0);
+  if (nsteps == 0) {
+    get_state(c, x, v, nodex, nodev);
+    return;
+  }
+  run_steps(c, nsteps - 1, dt, 0, 0);
+  nve_initial(c, dt);
+  c.step++;
+  if (rebuild_due(c)) build(c, false);
+  const bool overlap = !c.dfm.on;
+  if (overlap) {
+    CACB200_CUDA(cudaEventRecord(c.pos_ev, c.stream));
+    CACB200_CUDA(cudaStreamWaitEvent(c.copy, c.pos_ev, 0));
+    if (x && c.na) {
+      c.stage.reserve(3 * (size_t)c.na);
+      k_unpack_x<<<(c.na + 255) / 256, 256, 0, c.copy>>>(c.xs.p, c.stage.p, c.na);
+      CACB200_CUDA(cudaMemcpyAsync(x, c.stage.p, sizeof(double) * 3 * c.na, cudaMemcpyDeviceToHost, c.copy));
+    }
+    if (nodex && c.ne)
+      CACB200_CUDA(cudaMemcpyAsync(nodex, c.nodex.p, sizeof(double) * 24 * c.ne, cudaMemcpyDeviceToHost, c.copy));
+  }
+  forces(c, 0, 0);
+  langevin_post_force(c, dt);
+  nve_final(c, dt);
+  deform_end_of_step(c, dt);
+  c.run_left -= 1;
+  CACB200_CUDA(cudaGetLastError());
+  if (overlap) {
+    if (v && c.na)
+      CACB200_CUDA(cudaMemcpyAsync(v, c.v.p, sizeof(double) * 3 * c.na, cudaMemcpyDeviceToHost, c.stream));
+    if (nodev && c.ne)
+      CACB200_CUDA(cudaMemcpyAsync(nodev, c.nodev.p, sizeof(double) * 24 * c.ne, cudaMemcpyDeviceToHost,
+                                   c.stream));
+    CACB200_CUDA(cudaStreamSynchronize(c.copy));
+    CACB200_CUDA(cudaStreamSynchronize(c.stream));
+  } else {
+    get_state(c, x, v, nodex, nodev);
+  }
+}
+
 // Minimize::command + Min::setup/run with a FIRE iterate (minimize.cpp:21-70,
 // min.cpp:182-463): nodal_energy_weight 1 for the duration (minimize.cpp:37),
 // lists rebuilt every `every` iterations, energy evaluated every iteration.
@@ -926,6 +984,13 @@ int cacb200_set_neighbor(cacb200_ctx *ctx, double skin, int every) {
   c.lists_valid = false;
   c.planned = false;
   c.gen++;
+  API_END
+}
+
+int cacb200_run_nve_host(cacb200_ctx *ctx, int nsteps, double dt, double *x, double *v, double *nodex,
+                         double *nodev) {
+  API_BEGIN
+  run_nve_host(c, nsteps, dt, x, v, nodex, nodev);
   API_END
 }
 

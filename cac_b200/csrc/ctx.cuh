@@ -166,6 +166,8 @@ struct Ctx {
   // `stream` with events, so it is part of the same order and of graphs
   cudaStream_t side = nullptr;
   cudaEvent_t fork_ev = nullptr, join_ev = nullptr, items_ev = nullptr;
+  cudaStream_t copy = nullptr;   // host copies overlapped with the last step's forces
+  cudaEvent_t pos_ev = nullptr;
   std::string last_error;
   int precision = CACB200_FP64;
 

@@ -264,6 +264,16 @@ int cacb200_nve_final(cacb200_ctx *ctx, double dt);
  * step is queued on the context's stream (list rebuilds synchronise). */
 int cacb200_setup(cacb200_ctx *ctx);
 int cacb200_run_nve(cacb200_ctx *ctx, int nsteps, double dt, int eflag, int vflag);
+/* A run from host arrays to host arrays, for a host loop that owns the state
+ * between runs (the reference's x / v / nodex / nodev, atom.h:36-60,
+ * element.h:94): x, v, nodex, nodev are read (cacb200_set_state), nsteps
+ * are run as by cacb200_run_nve (no tallies), and the state is written back
+ * into the same arrays (cacb200_get_state).  The positions' copy to the host
+ * overlaps the last step's force evaluation (it needs nothing after the
+ * drift and the list rebuild); use pinned host memory for copies that run
+ * beside the kernels.  Null arrays are neither read nor written. */
+int cacb200_run_nve_host(cacb200_ctx *ctx, int nsteps, double dt, double *x, double *v, double *nodex,
+                         double *nodev);
 /* cacb200_run_nve in two parts, so that a host can act between steps of one
  * run (e.g. print the reference's thermo lines): cacb200_run_begin is
  * Verlet::setup for a run of nsteps (forces of the starting positions, with

@@ -40,3 +40,32 @@ def test_device_arrays_equal_host_readouts(tmp_path):
     stress = -NKTV2P * e.device_array("vatom")
     assert np.array_equal(stress.cpu().numpy(), -NKTV2P * ev["vatom"])
     e.close()
+
+
+@pytest.mark.parametrize("nsteps", [1, 13])
+def test_run_from_host_arrays_equals_set_run_get(nsteps):
+    """cacb200_run_nve_host (state in, steps, state out, the position copy
+    beside the last step's forces) gives what set_state + run_nve +
+    get_state give, bit for bit, step after step (a list rebuild included)."""
+    import torch
+    from cac_b200.api import Engine
+    s = CASES["tiny_lj"][0]()
+    out = []
+    for host in (True, False):
+        e = Engine(0)
+        e.upload(s)
+        e.pair_lj(*LJ)
+        e.neighbor(SKIN, 10)
+        e.setup()
+        x, v, nx, nv = (torch.from_numpy(a.copy()).pin_memory().numpy() for a in e.state())
+        for _ in range(3):
+            if host:
+                e.run_nve_host(nsteps, x, v, nx, nv)
+            else:
+                e.set_state(x, v, nx, nv)
+                e.run_nve(nsteps)
+                x, v, nx, nv = e.state()
+        out.append((x.copy(), v.copy(), nx.copy(), nv.copy()))
+        e.close()
+    for a, b in zip(out[0], out[1]):
+        assert np.array_equal(a, b)
