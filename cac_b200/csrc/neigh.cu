@@ -543,7 +543,7 @@ __device__ __forceinline__ void warp_emit(const BuildArgs &A, int slot, int &n, 
   n += __popc(m);
 }
 
-// Phase B for one query: its items in groups of up to 32.  Lane k stages
+// Phase B for one query: its items in groups of up to 16.  Lane k stages
 // item k of a group in the warp's shared scratch (the 24 ghost node
 // coordinates and the FP32 affine frame relative to the query), then the
 // lanes walk the group's sites flattened in (item, a, bb, cc) order -- the
@@ -551,12 +551,13 @@ __device__ __forceinline__ void warp_emit(const BuildArgs &A, int slot, int &n, 
 // FP32 affine screen; the sites that pass are queued in that order and take
 // the reference's exact FP64 distance 32 at a time, so the FP64 work runs on
 // full warps and the entries are emitted in the serial order.
+constexpr int ITEM_GROUP = 16;   // items staged at a time (a query has a few)
 struct ItemStage {
-  double g[32][24];   // ghost node coordinates nodex + s L
-  float fr[32][13];   // frame columns a, b, c; query minus frame origin; screen radius^2
-  int mg[32][2];      // ceil(2^16 / n) of the box's z and y extents (division by multiply-shift)
-  int2 item[32];      // the group's items
-  int queue[64];      // screened sites: item lane << 10 | lattice site
+  double g[ITEM_GROUP][24];   // ghost node coordinates nodex + s L
+  float fr[ITEM_GROUP][13];   // frame columns a, b, c; query minus frame origin; screen radius^2
+  int mg[ITEM_GROUP][2];      // ceil(2^16 / n) of the box's z and y extents (division by multiply-shift)
+  int2 item[ITEM_GROUP];      // the group's items
+  int queue[64];              // screened sites: item lane << 10 | lattice site
 };
 
 // The exact test of one queued site (active lanes only) and the warp's
@@ -616,12 +617,12 @@ __device__ __forceinline__ void items_exact(const BuildArgs &A, const Query &q, 
 __device__ void items_warp(const BuildArgs &A, const Query &q, const int2 *items, int n, ItemStage &st, int &nf,
                            int &nh) {
   const int lane = threadIdx.x & 31;
-  for (int g0 = 0; g0 < n; g0 += 32) {
+  for (int g0 = 0; g0 < n; g0 += ITEM_GROUP) {
     const int gi = g0 + lane;
     int2 it = make_int2(0, 0);
     int nbox = 0;
     __syncwarp();
-    if (gi < n) {
+    if (lane < ITEM_GROUP && gi < n) {
       it = items[gi];
       st.item[lane] = it;
       int e, sv[3], lo[3], hi[3];
@@ -652,14 +653,14 @@ __device__ void items_warp(const BuildArgs &A, const Query &q, const int2 *items
     }
     const int excl = incl - nbox;
     const int total = __shfl_sync(0xffffffffu, incl, 31);
-    const int ng = min(32, n - g0);
+    const int ng = min(ITEM_GROUP, n - g0);
     int qn = 0;   // queued sites (warp-uniform)
     for (int base = 0; base < total; base += 32) {
       const int f = base + lane;
       // item of flattened site f: the last lane m < ng with excl[m] <= f
       int m = 0;
 #pragma unroll
-      for (int step = 16; step > 0; step >>= 1) {
+      for (int step = ITEM_GROUP / 2; step > 0; step >>= 1) {
         const int cand = m + step;
         const int v = __shfl_sync(0xffffffffu, excl, cand & 31);
         if (cand < ng && v <= f) m = cand;
@@ -837,8 +838,8 @@ __global__ void __launch_bounds__(32, 32) k_build_atoms(BuildArgs A, ManyRep P, 
 // point; atoms with at least one item go on the work list of phase B (its
 // order does not matter: an atom's entries depend on that atom alone).
 template <class RP>
-__global__ void __launch_bounds__(128) k_elem_items(BuildArgs A, RP P, int2 *items, int *nitems, int icap,
-                                                    int *work, int *nwork) {
+__device__ __forceinline__ void elem_items_slot(BuildArgs A, RP P, int2 *items, int *nitems, int icap, int *work,
+                                                int *nwork) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= A.nsi) return;
   Query q;
@@ -857,10 +858,22 @@ __global__ void __launch_bounds__(128) k_elem_items(BuildArgs A, RP P, int2 *ite
   if (t < A.na && n > 0) work[atomicAdd(nwork, 1)] = t;
 }
 
+// The single-system form as the compiler allocates it; the batch form capped
+// at 64 registers (from 70) for 8 resident blocks per SM: 4 % faster on a
+// 64-replica batch, where the same cap slowed the single-system form.
+__global__ void __launch_bounds__(128) k_elem_items(BuildArgs A, OneRep P, int2 *items, int *nitems, int icap,
+                                                    int *work, int *nwork) {
+  elem_items_slot(A, P, items, nitems, icap, work, nwork);
+}
+__global__ void __launch_bounds__(128, 8) k_elem_items(BuildArgs A, ManyRep P, int2 *items, int *nitems, int icap,
+                                                       int *work, int *nwork) {
+  elem_items_slot(A, P, items, nitems, icap, work, nwork);
+}
+
 // Phase B for atoms: one warp per listed atom, its element sites appended
 // after its atom neighbours.
 template <class RP>
-__global__ void __launch_bounds__(128) k_build_atom_sites(BuildArgs A, RP P, const int2 *items, const int *nitems,
+__global__ void __launch_bounds__(128, 8) k_build_atom_sites(BuildArgs A, RP P, const int2 *items, const int *nitems,
                                                           int icap, const int *work, const int *nwork) {
   __shared__ ItemStage stage[4];
   ItemStage &st = stage[threadIdx.x >> 5];
@@ -881,7 +894,7 @@ __global__ void __launch_bounds__(128) k_build_atom_sites(BuildArgs A, RP P, con
 // Phase B for Gauss points: one warp each; atoms from the 27 surrounding atom
 // cells (full list only), 32 candidates at a time, then the element sites.
 template <class RP>
-__global__ void __launch_bounds__(128) k_build_gauss(BuildArgs A, RP P, const int2 *items, const int *nitems,
+__global__ void __launch_bounds__(128, 8) k_build_gauss(BuildArgs A, RP P, const int2 *items, const int *nitems,
                                                      int icap) {
   __shared__ ItemStage stage[4];
   ItemStage &st = stage[threadIdx.x >> 5];
