@@ -276,3 +276,28 @@ def test_min_style_fire_b200_under_reference_minimize(case, stop, tmp_path):
         assert abs(got - it) <= max(2, it // 50)
         assert np.abs(d["x"] - x).max() < 1e-5
         assert np.abs(d["nodex"] - nx).max() < 1e-5
+
+
+def test_run_b200_check_yes_follows_the_reference(oracle_mod, tmp_path):
+    """neigh_modify every 1 delay 3 check yes on a hot system (rebuilds only
+    after a move past half the skin; the same system rebuilds at least twice
+    in test_gpu_neigh_rule): run_b200 with lj/cut/b200 ends in the state the
+    reference executable's own `run` reaches with lj/cut on the same deck."""
+    if not os.path.exists(oracle_mod.REF_EXE):
+        pytest.fail("reference executable oracle/_ref/cac is missing: build it with make -C oracle reference")
+    s = gen.tiny(seed=32, temperature=1500.0)
+    gen.write_data(s, str(tmp_path / "data.cac"))
+    tail = ("neighbor 1.0 bin\nneigh_modify every 1 delay 3 check yes\ntimestep 0.001\nfix 1 all nve\n"
+            "thermo 50\n")
+    ends = []
+    for exe, style, run in ((APP, "lj/cut/b200", "run_b200"), (oracle_mod.REF_EXE, "lj/cut", "run")):
+        (tmp_path / "in.cac").write_text(HEADER + f"pair_style {style} 5.5\npair_coeff 1 1 0.4093 2.338\n" + tail +
+                                         f"{run} 150\noracle_dump end.txt state\n")
+        r = subprocess.run([exe, "-in", "in.cac"], cwd=tmp_path, capture_output=True, text=True, timeout=600)
+        assert r.returncode == 0, r.stdout[-3000:] + r.stderr[-3000:]
+        ends.append((oracle_mod.read_dump(str(tmp_path / "end.txt")), r.stdout))
+    (d, out), (ref, ref_out) = ends
+    assert np.abs(d["x"] - ref["x"]).max() < 1e-10
+    assert np.abs(d["nodex"] - ref["nodex"]).max() < 1e-10
+    assert rel_err(d["v"], ref["v"]) < TOL
+    assert rel_err(d["nodev"], ref["nodev"]) < TOL
