@@ -1,12 +1,26 @@
 #!/usr/bin/env python
 """Benchmark of the CAC per-timestep force path on B200.
 
-Workload (default): the EAM system at scale -- 1,049,760 atoms (162 atomic
-layers) between two coarse regions of 20,000 8-node elements (9 lattice sites
-per edge, 2x2x2 Gauss points), 1,209,760 atom+IP sites; analytic EAM tabulated
-to 10,000 points, cutoff 5.0 A, skin 1.0 A, list rebuilt every 10 steps,
-velocity Verlet at dt = 1 fs from 300 K Maxwell-Boltzmann velocities; FP64.
-Seeded synthetic input (no dataset exists for this path).
+Workload (default): the mixed-precision configuration at scale -- the EAM
+system enlarged to 4,179,600 atoms (129 atomic layers of 32,400) between two
+coarse regions of 100,000 8-node elements (9 lattice sites per edge, 2x2x2
+Gauss points), 4,979,600 atom+IP sites, under a uniaxial 3 % strain along x
+applied as an affine map to atoms, nodes and box; analytic EAM tabulated to
+10,000 points, cutoff 5.0 A, skin 1.0 A, list rebuilt every 10 steps, velocity
+Verlet at dt = 1 fs from 300 K Maxwell-Boltzmann velocities.  Seeded
+synthetic input (no dataset exists for this path).
+
+The line's ``value`` is the mixed form (FP32 pair arithmetic on cell-relative
+fixed-point positions; FP64 integration, nodal assembly and energy/virial
+sums).  The plain FP64 form runs on the same system in the same process with
+the same steps (``fp64``), and the line carries their ratio
+(``mixed_over_fp64``) and the mixed form's force error against FP64 on the
+seeded state (``accuracy``: largest and RMS per-site force error relative to
+the largest FP64 per-site force, nodal forces, energy and virial).  The EAM
+workload of 1,049,760 atoms + 20,000 elements (1,209,760 sites) in FP64 is a
+second entry (``secondary``).  ``--workload`` / ``--form`` select another
+system or form alone (``eam_1m``, ``eam_small``, ``lj_small``, ``batch256``,
+``serve``); ``--compare none`` and ``--secondary none`` drop the extra runs.
 
 One step = one velocity-Verlet timestep of the whole system (force evaluation
 with both EAM passes, nodal assembly, integration; a list rebuild every 10th
@@ -31,6 +45,10 @@ GPU, with no collective on the data path ("replicas only"); value is the sum.
 ``--impl reference`` times the CAC reference's own CPU path (oracle/_ref/cac,
 built from the reference sources with a single-rank MPI stand-in; one core)
 on the same workload: ``run W`` then ``run K``, rate from its "Loop time".
+At this size a reference step takes seconds, so the reference runs at most
+``--ref-max-steps`` timed steps and ``--ref-max-warmup`` warm-up steps; the
+line states the requested and the timed counts (``steps_requested``,
+``steps``).
 """
 from __future__ import annotations
 
@@ -259,30 +277,35 @@ def reference_arm(args, rank, ws):
     if not os.path.exists(REF_EXE):
         print(json.dumps({"impl": "reference", "unavailable": "reference executable oracle/_ref/cac was not built"}))
         return
-    cores, kind_sample = 1, f"full workload, run {args.warmup} then run {args.steps} steps; rate from Loop time"
+    steps = min(args.steps, args.ref_max_steps)
+    warmup = min(args.warmup, args.ref_max_warmup)
+    cores, kind_sample = 1, (f"full workload, run {warmup} then run {steps} steps (of {args.steps} and "
+                             f"{args.warmup} requested: at most --ref-max-steps / --ref-max-warmup); rate "
+                             f"from Loop time")
     par = "1 core (reference CPU path, single MPI rank)"
     if args.workload.startswith("batch"):
         systems, pair = build_workload(args.workload, 2, replicas=args.replicas)
         cores = min(os.cpu_count() or 1, len(systems))
         sample = systems[:cores]
-        value, nrep = run_reference_many(sample, pair, args.steps, args.warmup, cores)
+        value, nrep = run_reference_many(sample, pair, steps, warmup, cores)
         units = totals(systems)[0]
-        secs = units * args.steps / value
+        secs = units * steps / value
         kind_sample = (f"{nrep} of the {len(systems)} replicas as concurrent single-rank processes on {cores} "
-                       f"cores, run {args.warmup} then run {args.steps} steps each; rate = sum over processes "
-                       f"of sites x steps / Loop time")
+                       f"cores, run {warmup} then run {steps} steps each (of {args.steps} and {args.warmup} "
+                       f"requested); rate = sum over processes of sites x steps / Loop time")
         par = f"{cores} concurrent single-rank reference processes (one replica each)"
     else:
-        units, secs, _ = run_reference(args.workload, args.steps, args.warmup)
-        value = units * args.steps / secs
+        units, secs, _ = run_reference(args.workload, steps, warmup)
+        value = units * steps / secs
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * secs / args.steps,
+        "steps": steps, "warmup": warmup, "steps_requested": args.steps, "warmup_requested": args.warmup,
+        "ms_per_step": 1000.0 * secs / steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded generator)",
         "config": {"workload": args.workload, "sites": units,
                    "pair": "lj/cut" if args.workload.startswith("lj") else "eam/alloy",
-                   "precision": "fp64", "parallelism": par},
+                   "precision": "fp64 (the reference has no other form)", "parallelism": par},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference",
                          "sample": kind_sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -369,77 +392,147 @@ def pipe_peak(fp64: bool, device: int) -> float:
     return best
 
 
+def make_engine(s, pair, form: str, local: int, setfl: str, fix: str):
+    """A context holding the workload, set up at the seeded state (lists,
+    forces) and snapshotted for the restarts."""
+    from cac_b200 import api
+    eng = api.Engine(local)
+    if isinstance(s, list):
+        eng.upload_batch(s)
+    else:
+        eng.upload(s)
+    if pair == "eam":
+        eng.pair_eam(setfl)
+    else:
+        eng.pair_lj(0.4093, 2.338, 5.5)
+    eng.set_precision(api.MIXED if form == "mixed" else api.FP64)
+    eng.neighbor(1.0, 10)
+    if fix == "langevin":
+        eng.langevin(300.0, 300.0, 0.1, 4928459)
+    elif fix == "deform":
+        if isinstance(s, list):
+            raise SystemExit("--fix deform times a single system")
+        eng.deform(1, x=("erate", 0.1), y=("volume",))
+    return eng
+
+
+class Trajectories:
+    """Velocity-Verlet steps as segments of at most `seg` steps, each from
+    the seeded initial state (restore + list build + forces; with a deforming
+    box, the seeded box too)."""
+
+    def __init__(self, eng, seg: int, box0=None):
+        self.eng, self.seg, self.box0 = eng, seg, box0
+
+    def run(self, nsteps: int, first: bool):
+        done = 0
+        while done < nsteps:
+            if not (first and done == 0):
+                self.eng.restore()
+                if self.box0 is not None:
+                    self.eng.set_box(*self.box0)
+                self.eng.setup()
+            k = min(self.seg, nsteps - done)
+            self.eng.run_nve(k, 0.001)
+            done += k
+
+
+def timed_region(eng, tr: Trajectories, steps: int, warmup: int, local: int, dist, clocks: bool):
+    """W warm-up steps, then K steps between barriers and synchronisations,
+    timed with CUDA events on the context's stream; (slowest rank's ms, clock
+    summary or None)."""
+    import torch
+    stream = torch.cuda.ExternalStream(eng.stream, device=torch.device("cuda", local))
+    tr.run(warmup, True)
+    torch.cuda.synchronize(local)
+    if dist:
+        dist.barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    clk = ClockSampler(local) if clocks else None
+    if clk:
+        clk.__enter__()
+    try:
+        torch.cuda.synchronize(local)
+        if dist:
+            dist.barrier()
+        e0.record(stream)
+        tr.run(steps, False)
+        e1.record(stream)
+        torch.cuda.synchronize(local)
+        if dist:
+            dist.barrier()
+    finally:
+        if clk:
+            clk.__exit__(None, None, None)
+    ms = e0.elapsed_time(e1)
+    return max_over_ranks(ms, dist, torch.device("cuda", local)), (clk.summary() if clk else None)
+
+
+def force_accuracy(ref, mix, nelements: int) -> dict:
+    """Mixed against FP64 on the same state: largest and RMS per-site force
+    error (atoms and Gauss points) relative to the largest FP64 per-site
+    force, the same for nodal forces, and the relative energy and virial
+    errors."""
+    import numpy as np
+    from cac_b200 import api
+    for e in (ref, mix):
+        e.compute(api.ENERGY_GLOBAL, api.VIRIAL_GLOBAL)
+    f64, nf64, gf64 = ref.forces()
+    f32, nf32, gf32 = mix.forces()
+    site64 = np.concatenate([f64, gf64.reshape(-1, 3)])
+    site32 = np.concatenate([f32, gf32.reshape(-1, 3)])
+    err = np.linalg.norm(site32 - site64, axis=1) / np.linalg.norm(site64, axis=1).max()
+    out = {"force_err_max": float(err.max()), "force_err_rms": float(np.sqrt(np.mean(err ** 2)))}
+    if nelements:
+        nerr = np.linalg.norm((nf32 - nf64).reshape(-1, 3), axis=1) / np.linalg.norm(nf64.reshape(-1, 3),
+                                                                                      axis=1).max()
+        out["node_force_err_max"] = float(nerr.max())
+    e64, e32 = ref.energy(peratom=False), mix.energy(peratom=False)
+    out["energy_rel_err"] = abs(e32["energy"] - e64["energy"]) / abs(e64["energy"])
+    out["virial_rel_err"] = float(np.abs(e32["virial"] - e64["virial"]).max() / np.abs(e64["virial"]).max())
+    out["against"] = "FP64 form on the same seeded state (same process)"
+    return out
+
+
 def b200_arm(args, rank, local, ws, dist):
     import numpy as np
     import torch
-    from cac_b200 import api, gen
+    from cac_b200 import gen, shard
 
-    from cac_b200 import shard
     seed = rank_seed(2, rank)
     s, pair = build_workload(args.workload, seed, rank, ws, replicas=args.replicas)
     units, natoms, nelements = totals(s)
     dev = torch.device("cuda", local)
     units_all = shard.sum_over_ranks(units, dist, dev)
     batch = isinstance(s, list)
-    eng = api.Engine(local)
-    if batch:
-        eng.upload_batch(s)
-    else:
-        eng.upload(s)
     tmp = tempfile.mkdtemp()
-    if pair == "eam":
-        p = os.path.join(tmp, "cu.setfl")
-        gen.write_setfl(gen.EamParams(), p)
-        eng.pair_eam(p)
-    else:
-        eng.pair_lj(0.4093, 2.338, 5.5)
-    eng.set_precision(api.MIXED if args.form == "mixed" else api.FP64)
-    eng.neighbor(1.0, 10)
-    if args.fix == "langevin":
-        eng.langevin(300.0, 300.0, 0.1, 4928459)
-    elif args.fix == "deform":
-        if batch:
-            raise SystemExit("--fix deform times a single system")
+    setfl = os.path.join(tmp, "cu.setfl")
+    gen.write_setfl(gen.EamParams(), setfl)
+    box0 = None
+    if args.fix == "deform":
         box0 = (np.asarray(s.boxlo, dtype=np.float64), np.asarray(s.boxhi, dtype=np.float64))
-        eng.deform(1, x=("erate", 0.1), y=("volume",))
+    seg = max(1, min(args.segment, args.steps))
+    compare = args.compare == "fp64" and args.form == "mixed"
+
+    # the FP64 form on the same system: accuracy of the mixed form on the
+    # seeded state, then its own timed steps
+    fp64_entry, accuracy = None, None
+    eng = make_engine(s, pair, args.form, local, setfl, args.fix)
+    if compare:
+        ref = make_engine(s, pair, "fp64", local, setfl, args.fix)
+        accuracy = force_accuracy(ref, eng, nelements)
+        ref.setup()
+        ref.snapshot()
+        ms64, clk64 = timed_region(ref, Trajectories(ref, seg, box0), args.steps, args.warmup, local, dist, True)
+        fp64_entry = {"value": units_all * args.steps / (ms64 / 1000.0), "ms_per_step": ms64 / args.steps,
+                      "steps": args.steps, "warmup": args.warmup, "clocks": clk64}
+        ref.close()
+        del ref
     eng.setup()
     eng.snapshot()
-    stream = torch.cuda.ExternalStream(eng.stream, device=torch.device("cuda", local))
-    seg = max(1, min(args.segment, args.steps))
-
-    def trajectory(nsteps: int, first: bool):
-        """nsteps of velocity Verlet as segments of at most `seg` steps, each
-        from the seeded initial state (restore + list build + forces; with a
-        deforming box, the seeded box too)."""
-        done = 0
-        while done < nsteps:
-            if not (first and done == 0):
-                eng.restore()
-                if args.fix == "deform":
-                    eng.set_box(*box0)
-                eng.setup()
-            k = min(seg, nsteps - done)
-            eng.run_nve(k, 0.001)
-            done += k
-
-    trajectory(args.warmup, True)
-    torch.cuda.synchronize(local)
-    if dist:
-        dist.barrier()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    with ClockSampler(local) as clk:
-        torch.cuda.synchronize(local)
-        if dist:
-            dist.barrier()
-        e0.record(stream)
-        trajectory(args.steps, False)
-        e1.record(stream)
-        torch.cuda.synchronize(local)
-        if dist:
-            dist.barrier()
-    ms = e0.elapsed_time(e1)
-    ms_max = max_over_ranks(ms, dist, torch.device("cuda", local))
+    tr = Trajectories(eng, seg, box0)
+    ms_max, clocks = timed_region(eng, tr, args.steps, args.warmup, local, dist, True)
     value = units_all * args.steps / (ms_max / 1000.0)
 
     # per-kernel device times (CUDA events around every launch) for the roofline
@@ -506,6 +599,24 @@ def b200_arm(args, rank, local, ws, dist):
     e2e_s = max_over_ranks(time.perf_counter() - t0, dist, torch.device("cuda", local))
     e2e_value = units_all * k_e2e / e2e_s
     bytes_state = 8 * (6 * natoms + 48 * nelements)
+    eng.close()
+    del eng
+
+    # second workloads, each timed alone the same way (value, ms per step)
+    secondary = {}
+    for spec in ([] if args.secondary == "none" else args.secondary.split(",")):
+        wname, wform = spec.split(":")
+        s2, pair2 = build_workload(wname, seed, rank, ws, replicas=args.replicas)
+        u2 = shard.sum_over_ranks(totals(s2)[0], dist, dev)
+        e2 = make_engine(s2, pair2, wform, local, setfl, "none")
+        e2.setup()
+        e2.snapshot()
+        ms2, _ = timed_region(e2, Trajectories(e2, seg), args.steps, args.warmup, local, dist, False)
+        secondary[spec] = {"workload": wname, "form": wform, "sites": int(u2),
+                           "value": u2 * args.steps / (ms2 / 1000.0), "ms_per_step": ms2 / args.steps,
+                           "steps": args.steps, "warmup": args.warmup}
+        e2.close()
+        del e2, s2
 
     # CPU baseline: the reference on a bounded sample of the same workload
     cpu = None
@@ -546,6 +657,9 @@ def b200_arm(args, rank, local, ws, dist):
                        "fix": {"none": "nve", "langevin": "nve + langevin 300 300 0.1",
                                "deform": "nve + deform 1 x erate 0.1 y volume"}[args.fix],
                        "l2": "working set larger than L2 (site table + lists > 126 MB)"},
+            "fp64": fp64_entry,
+            "mixed_over_fp64": (value / fp64_entry["value"]) if fp64_entry else None,
+            "accuracy": accuracy,
             "roofline": {"bound": "hbm", "kernel": dom[0], "achieved": achieved, "peak": hbm,
                          "peak_kind": hbm_kind, "unit": "GB/s", "frac": achieved / hbm,
                          "traffic": traffic, "traffic_note": "ncu dram read+write per launch, per-site figure "
@@ -556,16 +670,16 @@ def b200_arm(args, rank, local, ws, dist):
             "kernels_ms_per_step": {k: v[0] / nprof for k, v in sorted(prof.items())},
             "hbm_by_kernel": hbm_by_kernel,
             "segment_steps": seg,
+            "secondary": secondary,
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": bytes_state,
                     "d2h_bytes_per_step": bytes_state, "steps": k_e2e},
             "gpu_launches": int(round(launches_per_step * args.steps)),
             "tuned_blocks": dict(zip(("rho", "force"), tuned)),
             "thermo_readout_ms": thermo_ms,
-            "clocks": clk.summary(),
+            "clocks": clocks,
         }
         print(json.dumps(line))
-    eng.close()
 
 
 def serve_specs(n: int, seed: int):
@@ -731,8 +845,16 @@ def main():
     ap.add_argument("--steps", type=int, default=500)
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="eam_1m")
-    ap.add_argument("--form", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--workload", default="eam_4m_strained")
+    ap.add_argument("--form", default="mixed", choices=["fp64", "mixed"])
+    ap.add_argument("--compare", default="fp64", choices=["fp64", "none"],
+                    help="mixed form: also time the FP64 form on the same system and report the ratio "
+                         "and the force error")
+    ap.add_argument("--secondary", default="eam_1m:fp64",
+                    help="comma-separated workload:form entries timed after the main one ('none': skip)")
+    ap.add_argument("--ref-max-steps", type=int, default=10,
+                    help="reference arm: timed steps at most (a reference step takes seconds at this size)")
+    ap.add_argument("--ref-max-warmup", type=int, default=1, help="reference arm: warm-up steps at most")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--fix", default="none", choices=["none", "langevin", "deform"],
                     help="integrate with fix langevin or fix deform besides fix nve")
@@ -750,10 +872,6 @@ def main():
     rank, local, ws, dist = dist_init()
     try:
         if args.impl == "reference":
-            if args.steps > 50:
-                args.steps = 20     # ~2 s per reference step at this size
-            if args.warmup > 5:
-                args.warmup = 3
             reference_arm(args, rank, ws)
         elif args.workload == "serve":
             serve_arm(args, rank, local, ws, dist)

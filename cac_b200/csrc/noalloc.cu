@@ -23,7 +23,8 @@ namespace {
 // loads the library holds it until the process exits.
 constexpr int NOALLOC_MAX_REPLICAS = CACB200_NOALLOC_MAX_REPLICAS;
 struct NoAllocScratch {
-  int meta[4][NOALLOC_MAX_REPLICAS];   // atom offset, atom count, element offset, element count
+  int meta[4 * NOALLOC_MAX_REPLICAS];  // per replica r: atom offset, atom count, element offset, element count
+                                       // at 4r .. 4r+3 (a call copies only its replicas' 16 bytes each)
   double sum[NOALLOC_MAX_REPLICAS];    // energy of each replica
 };
 static __device__ __align__(256) NoAllocScratch noalloc_scratch;
@@ -34,7 +35,8 @@ static __device__ __align__(256) NoAllocScratch noalloc_scratch;
 __global__ void k_replica_energy_fixed(const double *eatom, const double *enode, double node_weight,
                                        NoAllocScratch *sc) {
   const int r = blockIdx.x;
-  const int aoff = sc->meta[0][r], na = sc->meta[1][r], eoff = sc->meta[2][r], ne = sc->meta[3][r];
+  const int *m = sc->meta + 4 * r;
+  const int aoff = m[0], na = m[1], eoff = m[2], ne = m[3];
   double s = 0.0;
   for (int i = threadIdx.x; i < na; i += blockDim.x) s += eatom[aoff + i];
   double t = 0.0;
@@ -74,14 +76,14 @@ extern "C" int cacb200_replica_energy_noalloc(int device, const double *eatom, c
     return CACB200_EINVAL;
   }
   if (!natoms || !nelements || !energy || device < 0 || device >= MAX_DEVICES) return CACB200_EINVAL;
-  std::vector<int> meta(4 * (size_t)NOALLOC_MAX_REPLICAS, 0);
+  std::vector<int> meta(4 * (size_t)nreplicas, 0);
   long a = 0, e = 0;
   for (int r = 0; r < nreplicas; r++) {
     if (natoms[r] < 0 || nelements[r] < 0) return CACB200_EINVAL;
-    meta[r] = (int)a;
-    meta[NOALLOC_MAX_REPLICAS + r] = natoms[r];
-    meta[2 * NOALLOC_MAX_REPLICAS + r] = (int)e;
-    meta[3 * NOALLOC_MAX_REPLICAS + r] = nelements[r];
+    meta[4 * r] = (int)a;
+    meta[4 * r + 1] = natoms[r];
+    meta[4 * r + 2] = (int)e;
+    meta[4 * r + 3] = nelements[r];
     a += natoms[r];
     e += nelements[r];
   }

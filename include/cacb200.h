@@ -221,7 +221,14 @@ int cacb200_set_neighbor(cacb200_ctx *ctx, double skin, int every);
  * The reference's minimiser runs with every 1 delay 0 check yes (Min::init,
  * min.cpp:155-169).  Honoured by cacb200_run_nve / cacb200_run_steps (which
  * replay no graphs under check yes or a delay above every) and
- * cacb200_minimize_fire. */
+ * cacb200_minimize_fire.  In a batch the rule is applied to the batch as a
+ * whole: under check yes one replica that has moved past the trigger
+ * rebuilds every replica (a rebuild also wraps positions into the box), and
+ * under a deforming box the trigger is the smallest over the replicas, so a
+ * batched replica's rebuild steps and wrapped coordinates can differ from
+ * the same replica run alone; forces and unwrapped positions agree within
+ * the FP64 tolerance.  The bit-for-bit batch-equals-alone property holds
+ * under every/delay alone (check no). */
 int cacb200_set_neighbor_modify(cacb200_ctx *ctx, int delay, int check);
 /* The inner prefix of the lists (no reference counterpart; an evaluation
  * order, not a different result): entries within cutoff + margin at the
@@ -383,7 +390,11 @@ int cacb200_restore(cacb200_ctx *ctx);
  * CACB200_NOALLOC_MAX_REPLICAS replicas (more: CACB200_EINVAL and a message
  * on stderr), held by every GPU that loads the library until exit.  The
  * first call on a device looks up that array's device address; make it
- * before any stream capture.  Every call shares the array, so calls that
+ * before any stream capture.  The address is kept for the life of the
+ * process: a device reset (cudaDeviceReset, or another framework resetting
+ * the primary context) after that first call is not supported, since the
+ * library's module would be loaded again at another address.  A call copies
+ * 16 bytes of offsets and counts per replica.  Every call shares the array, so calls that
  * overlap on the GPU (other streams, other threads) race; each call waits
  * for its stream before returning. */
 #define CACB200_NOALLOC_MAX_REPLICAS 4096

@@ -558,12 +558,12 @@ def read_dump(path: str) -> dict:
             out["virial"] = np.array([float(t) for t in w[1:]])
         elif w[0] == "atoms":
             n = out["natoms"]
-            a = np.array([[float(t) for t in lines[i + 1 + k].split()] for k in range(n)]).reshape(n, 17)
+            a = np.array(" ".join(lines[i + 1:i + 1 + n]).split(), dtype=np.float64).reshape(n, 17)
             out["atoms"] = a
             i += n
         elif w[0] == "nodes":
             n = out["nelements"] * 8
-            a = np.array([[float(t) for t in lines[i + 1 + k].split()] for k in range(n)]).reshape(n, 21)
+            a = np.array(" ".join(lines[i + 1:i + 1 + n]).split(), dtype=np.float64).reshape(n, 21)
             out["nodes"] = a
             i += n
         i += 1
@@ -597,6 +597,14 @@ def read_neigh(path: str, natoms: int) -> np.ndarray:
                 _, kind, tag, site, sx, sy, sz = ln.split()
                 rows.append((cur, int(kind), int(tag) - 1, int(site), int(sx), int(sy), int(sz)))
     a = np.array(rows, dtype=np.int64).reshape(-1, 7)
+    order = np.lexsort(a.T[::-1])
+    return a[order]
+
+
+def read_neigh_binary(path: str) -> np.ndarray:
+    """Parse ``oracle_dump_neigh FILE binary`` output (rows of 7 int32 written
+    in sorted order) into the int64 rows of ``read_neigh``."""
+    a = np.fromfile(path, dtype="<i4").reshape(-1, 7).astype(np.int64)
     order = np.lexsort(a.T[::-1])
     return a[order]
 

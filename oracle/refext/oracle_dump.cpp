@@ -198,7 +198,13 @@ OracleDumpNeigh::OracleDumpNeigh(CAC *cac) : Pointers(cac) {}
 
 void OracleDumpNeigh::command(int narg, char **arg)
 {
-  if (narg != 1) error->all(FLERR, "Illegal oracle_dump_neigh command: oracle_dump_neigh FILE");
+  if (narg != 1 && narg != 2)
+    error->all(FLERR, "Illegal oracle_dump_neigh command: oracle_dump_neigh FILE [binary]");
+  int binary = 0;
+  if (narg == 2) {
+    if (strcmp(arg[1], "binary") != 0) error->all(FLERR, "Illegal oracle_dump_neigh mode");
+    binary = 1;
+  }
   if (force->pair == nullptr) error->all(FLERR, "oracle_dump_neigh needs a pair style");
   NeighList *list = force->pair->get_list();
   if (list == nullptr) error->all(FLERR, "oracle_dump_neigh: no neighbour list (run 0 first)");
@@ -254,6 +260,28 @@ void OracleDumpNeigh::command(int narg, char **arg)
   }
   std::sort(entries.begin(), entries.end(),
             [](const Entry &a, const Entry &b) { return a.i < b.i; });
+
+  if (binary) {
+    // rows of 7 int32 in canonical numbering, already in sorted order:
+    // i-site (atom tag-1, or natoms + 8*(element tag-1) + Gauss point),
+    // j kind, j tag-1, j site, image sx, sy, sz
+    FILE *fb = fopen(arg[0], "wb");
+    if (!fb) error->one(FLERR, "oracle_dump_neigh: cannot open file");
+    const long natoms = (long) atom->natoms;
+    std::vector<int> buf;
+    for (auto &en : entries) {
+      long isite = en.i.kind == 0 ? en.i.tag - 1L : natoms + 8L * (en.i.tag - 1) + en.i.site;
+      buf.clear();
+      for (auto &k : en.js) {
+        int row[7] = {(int) isite, k.kind, k.tag - 1, k.site, k.sx, k.sy, k.sz};
+        buf.insert(buf.end(), row, row + 7);
+      }
+      if (!buf.empty() && fwrite(buf.data(), sizeof(int), buf.size(), fb) != buf.size())
+        error->one(FLERR, "oracle_dump_neigh: write failed");
+    }
+    fclose(fb);
+    return;
+  }
 
   FILE *fp = fopen(arg[0], "w");
   if (!fp) error->one(FLERR, "oracle_dump_neigh: cannot open file");

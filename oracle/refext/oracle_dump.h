@@ -8,9 +8,12 @@
  *                              the pair style with global+per-atom energy and
  *                              virial, fold ghost contributions into owners,
  *                              assemble nodal forces, then dump
- *   oracle_dump_neigh FILE     dump the pair style's neighbour list as
+ *   oracle_dump_neigh FILE [binary]
+ *                              dump the pair style's neighbour list as
  *                              canonical keys (atom tag or element tag + lattice
- *                              site) with the periodic image of every neighbour
+ *                              site) with the periodic image of every neighbour;
+ *                              binary: sorted rows of 7 int32 (i-site, j kind,
+ *                              j tag-1, j site, sx, sy, sz) for large systems
  */
 #ifdef COMMAND_CLASS
 
