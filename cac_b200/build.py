@@ -11,7 +11,7 @@ CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libcacb200.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-shared",
-         "--expt-relaxed-constexpr", "-Xptxas", "-warn-spills"]
+         "--expt-relaxed-constexpr", "-Xptxas", "-warn-spills", "--threads", "8"]
 
 
 def sources():

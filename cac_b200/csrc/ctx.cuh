@@ -266,9 +266,13 @@ struct Ctx {
   std::vector<double> build_box; // [nrep*6] replica boxes (lo, hi) at the last build
   DBuf<int> moved;               // flag of the displacement check
   int cap = 160;
+  // full lists, [cap][nsite_i]: a site's num_in entries within cut +
+  // inner_margin at the build fill rows [0, num_in) and its other
+  // num_full - num_in entries rows [cap - (num_full - num_in), cap); the two
+  // segments meet only when a list overflows (then the build is repeated)
   DBuf<int> nbr_full, num_full;
-  // inner prefix of the full lists: entries within cut + inner_margin at the
-  // build come first, num_in of them; inner_ok[replica] (device) is nonzero
+  DBuf<int2> site_from;          // per slot: rows of each segment before its element-site entries
+  // inner prefix of the full lists: inner_ok[replica] (device) is nonzero
   // while no site of the replica has moved inner_limit() since the build
   // (positions in xbuild / nodex_build), and the pair loops then stop at num_in
   double inner_margin = 0.4;
@@ -278,7 +282,7 @@ struct Ctx {
   DBuf<double> nodex_build;
   DBuf<int> nbr_half, num_half;
   bool have_half = false, lists_valid = false;
-  DBuf<int> raw_full, raw_half;  // build-time entries before compaction
+  DBuf<int> raw_full, raw_half;  // build-time element-site entries (full) and half lists before compaction
   DBuf<unsigned char> img_full, img_half;
   DBuf<int> site_flag;           // [ne*729 + 1] marks
   DBuf<int> site_pref;           // [ne*729 + 1] exclusive prefix of the marks

@@ -19,6 +19,15 @@
 // space).  Both prunings are exact supersets, so they change cost, not
 // membership.
 //
+// Full lists are written in their final form: an entry packs the neighbour's
+// pair-table index (atoms by list slot) with its image; a site's entries
+// inside the inner radius at build time fill its list from row 0 up, the
+// others from row cap-1 down, so no pass reorders them.  Element-site entries
+// are first written as lattice-site ids (the pair-table index of a lattice
+// site is known only once every list has marked the sites it uses) and
+// converted by k_remap_sites.  Half lists (read only by the list download)
+// are written as raw entries and compacted by k_remap.
+//
 // Storage rules (the reference's, restated):
 //   full  (npair_full_bin.cpp:23-358): every neighbour except the site itself.
 //   half  (npair_half_bin_newton.cpp:25-392): an atom keeps atom j when j's
@@ -284,7 +293,10 @@ struct BuildArgs {
   double cutneigh, cutneighsq;
   double cutforcesq;          // pairs inside the inner radius (force cutoff + margin) at build time go first
   int want_half;
-  int *raw_full, *num_full;
+  int *nbr_full;              // final full-list entries (atoms; element sites after k_remap_sites)
+  int *num_in;                // per slot: entries in the front segment
+  int2 *site_from;            // per slot: front / back rows before the element-site entries
+  int *raw_full, *num_full;   // raw_full / img_full: element-site entries at their final rows
   unsigned char *img_full;
   int *raw_half, *num_half;
   unsigned char *img_half;
@@ -388,8 +400,10 @@ __device__ __forceinline__ void make_query(const BuildArgs &A, const RP &P, int 
 
 // A candidate atom j seen in a cell with wrap count W: exact test and storage
 // rules (atoms are inside the box after pbc, so their own wrap is zero).
-__device__ __forceinline__ void try_atom(const BuildArgs &A, const Query &q, int j, const int W[3],
-                                         int &nf, int &nh) {
+// Full-list entries go to `full(j, code)`; half-list entries are stored here.
+template <class FullSink>
+__device__ __forceinline__ void try_atom(const BuildArgs &A, const Query &q, int j, const int W[3], int &nh,
+                                         FullSink &&full) {
   int s[3] = {W[0] - q.ti[0], W[1] - q.ti[1], W[2] - q.ti[2]};
   bool zero = (s[0] == 0 && s[1] == 0 && s[2] == 0);
   if (q.iatom && j == q.i && zero) return;
@@ -409,7 +423,7 @@ __device__ __forceinline__ void try_atom(const BuildArgs &A, const Query &q, int
     return;
   }
   int code = img_code(s[0], s[1], s[2]) | (rsq < A.cutforcesq ? IN_CUT : 0);
-  emit(A, q.slot, nf, A.raw_full, A.img_full, j, code);
+  full(j, code);
   if (A.want_half && q.iatom) {
     int ord = ref_bin_order(A.rb, q.xi, qq);
     bool keep = ord > 0 || (ord == 0 && (zero ? (j > q.i) : above_right(qq, q.xi)));
@@ -543,6 +557,26 @@ __device__ __forceinline__ void warp_emit(const BuildArgs &A, int slot, int &n, 
   n += __popc(m);
 }
 
+// The same for full lists: accepted entries go to the front segment (inside
+// the inner radius) or the back segment, each in lane order; dst gets the
+// entry and img (when given) the image code at the same place.  Rows
+// outside [0, cap) are not written (the count still grows and flags the
+// overflow).
+__device__ __forceinline__ void warp_emit_full(const BuildArgs &A, int slot, int &nin, int &nout, int *dst,
+                                               unsigned char *img, bool pass, bool incut, int val, int code) {
+  const unsigned mi = __ballot_sync(0xffffffffu, pass && incut);
+  const unsigned mo = __ballot_sync(0xffffffffu, pass && !incut);
+  if (pass) {
+    const int row = incut ? nin + __popc(mi & lanemask_lt()) : A.cap - 1 - (nout + __popc(mo & lanemask_lt()));
+    if (row >= 0 && row < A.cap) {
+      dst[(size_t)row * A.nsi + slot] = val;
+      if (img) img[(size_t)row * A.nsi + slot] = (unsigned char)code;
+    }
+  }
+  nin += __popc(mi);
+  nout += __popc(mo);
+}
+
 // Phase B for one query: its items in groups of up to 16.  Lane k stages
 // item k of a group in the warp's shared scratch (the 24 ghost node
 // coordinates and the FP32 affine frame relative to the query), then the
@@ -563,7 +597,7 @@ struct ItemStage {
 // The exact test of one queued site (active lanes only) and the warp's
 // emission of the accepted ones.
 __device__ __forceinline__ void items_exact(const BuildArgs &A, const Query &q, const ItemStage &st, bool active,
-                                            int entry, int &nf, int &nh) {
+                                            int entry, int &nin, int &nout, int &nh) {
   bool pf = false, ph = false;
   int val = 0, codef = 0, code = 0;
   if (active) {
@@ -610,12 +644,12 @@ __device__ __forceinline__ void items_exact(const BuildArgs &A, const Query &q, 
       }
     }
   }
-  warp_emit(A, q.slot, nf, A.raw_full, A.img_full, pf, val, codef);
+  warp_emit_full(A, q.slot, nin, nout, A.raw_full, A.img_full, pf, (codef & IN_CUT) != 0, val, code);
   if (A.want_half) warp_emit(A, q.slot, nh, A.raw_half, A.img_half, ph, val, code);
 }
 
-__device__ void items_warp(const BuildArgs &A, const Query &q, const int2 *items, int n, ItemStage &st, int &nf,
-                           int &nh) {
+__device__ void items_warp(const BuildArgs &A, const Query &q, const int2 *items, int n, ItemStage &st, int &nin,
+                           int &nout, int &nh) {
   const int lane = threadIdx.x & 31;
   for (int g0 = 0; g0 < n; g0 += ITEM_GROUP) {
     const int gi = g0 + lane;
@@ -694,7 +728,7 @@ __device__ void items_warp(const BuildArgs &A, const Query &q, const int2 *items
       qn += __popc(mask);
       __syncwarp();
       if (qn >= 32) {
-        items_exact(A, q, st, true, st.queue[lane], nf, nh);
+        items_exact(A, q, st, true, st.queue[lane], nin, nout, nh);
         qn -= 32;
         const int rest = lane < qn ? st.queue[32 + lane] : 0;
         __syncwarp();
@@ -702,7 +736,7 @@ __device__ void items_warp(const BuildArgs &A, const Query &q, const int2 *items
         __syncwarp();
       }
     }
-    if (qn > 0) items_exact(A, q, st, lane < qn, lane < qn ? st.queue[lane] : 0, nf, nh);
+    if (qn > 0) items_exact(A, q, st, lane < qn, lane < qn ? st.queue[lane] : 0, nin, nout, nh);
   }
 }
 
@@ -727,10 +761,11 @@ __device__ __forceinline__ bool gauss_atom_test(const BuildArgs &A, const Query 
   return true;
 }
 
-__device__ __forceinline__ void finish_counts(const BuildArgs &A, int i, int nf, int nh) {
-  A.num_full[i] = nf;
+__device__ __forceinline__ void finish_counts(const BuildArgs &A, int i, int nin, int nout, int nh) {
+  A.num_full[i] = nin + nout;
+  A.num_in[i] = nin;
   if (A.want_half) A.num_half[i] = nh;
-  int m = max(nf, nh);
+  int m = max(nin + nout, nh);
   if (m > A.cap) {
     atomicExch(&A.overflow[0], 1);
     atomicMax(&A.overflow[1], m);
@@ -744,10 +779,21 @@ __device__ __forceinline__ void finish_counts(const BuildArgs &A, int i, int nf,
 // a float copy of the wrapped positions) decides all but the candidates near
 // the cutoff, which take the exact FP64 test.  The image of a candidate cell
 // relative to each lane's atom is fixed per cell.
+//
+// Full-list entries are written in their final form (the candidate's sorted
+// position is its list slot) and staged per lane in two 32-row rings in
+// shared memory, one per segment (lane = column, so a lane only ever touches
+// its own bank); the warp writes them out row by row: the lanes' list slots
+// are consecutive, so each row is one coalesced store across the warp
+// instead of one scattered store per entry (the lists are transposed,
+// [entry][slot]).  The warp flushes whenever a lane's ring is full and once
+// at the end.
+constexpr int STAGE_ROWS = 32;
 template <class RP>
 __device__ __forceinline__ void build_atoms_cells(BuildArgs A, RP P, int ncell) {
   const int lane = threadIdx.x & 31;
   const float fcut2 = (float)A.cutforcesq;
+  __shared__ int st_in[STAGE_ROWS][32], st_out[STAGE_ROWS][32];   // front / back segment rings
   {
     const int home = blockIdx.x;
     const int hbeg = A.acell_start[home], hend = A.acell_start[home + 1];
@@ -764,7 +810,8 @@ __device__ __forceinline__ void build_atoms_cells(BuildArgs A, RP P, int ncell) 
       const int h = base + lane;
       const bool active = h < hend;
       Query q;
-      int nf = 0, nh = 0;
+      int nin = 0, nout = 0, nh = 0;
+      int fin = 0, fout = 0;   // this lane's entries of each segment already written
       float wx = 0.f, wy = 0.f, wz = 0.f;
       if (active) {
         make_query(A, P, (int)__double_as_longlong(A.acell_pos[h].w), q);
@@ -774,6 +821,28 @@ __device__ __forceinline__ void build_atoms_cells(BuildArgs A, RP P, int ncell) 
         wy = w.y;
         wz = w.z;
       }
+      // entry = (neighbour's list slot << IMG_BITS) | image code
+      auto stage = [&](int val, bool incut) {
+        if (incut) st_in[nin++ & (STAGE_ROWS - 1)][lane] = val;
+        else st_out[nout++ & (STAGE_ROWS - 1)][lane] = val;
+      };
+      // every lane writes its staged entries, row by row: front segment
+      // entries [fin, nin) to rows fin.., back segment entries [fout, nout)
+      // to rows cap-1-fout down
+      auto flush = [&]() {
+        int lo = __reduce_min_sync(0xffffffffu, active ? fin : 0x7fffffff);
+        int hi = __reduce_max_sync(0xffffffffu, active ? nin : 0);
+        for (int k = lo; k < hi; k++)
+          if (active && k >= fin && k < nin && k < A.cap)
+            A.nbr_full[(size_t)k * A.nsi + q.slot] = st_in[k & (STAGE_ROWS - 1)][lane];
+        lo = __reduce_min_sync(0xffffffffu, active ? fout : 0x7fffffff);
+        hi = __reduce_max_sync(0xffffffffu, active ? nout : 0);
+        for (int k = lo; k < hi; k++)
+          if (active && k >= fout && k < nout && k < A.cap)
+            A.nbr_full[(size_t)(A.cap - 1 - k) * A.nsi + q.slot] = st_out[k & (STAGE_ROWS - 1)][lane];
+        fin = nin;
+        fout = nout;
+      };
       for (int oz = -1; oz <= 1; oz++) {
         int cz, Wz;
         wrap_cell(hz + oz, nc2, cz, Wz);
@@ -792,7 +861,8 @@ __device__ __forceinline__ void build_atoms_cells(BuildArgs A, RP P, int ncell) 
             const bool far = s0 < -1 || s0 > 1 || s1 < -1 || s1 > 1 || s2 < -1 || s2 > 1;
             const int code = far ? 0 : img_code(s0, s1, s2);
             int beg = A.acell_start[cell], end = A.acell_start[cell + 1];
-            auto consider = [&](const float4 &pj) {
+            // candidate pj at list slot ks
+            auto consider = [&](const float4 &pj, int ks) {
               float ex = wx - (pj.x + sx), ey = wy - (pj.y + sy), ez = wz - (pj.z + sz);
               const float r2 = ex * ex + ey * ey + ez * ez;
               if (r2 > pre2) return;
@@ -803,21 +873,27 @@ __device__ __forceinline__ void build_atoms_cells(BuildArgs A, RP P, int ncell) 
                   atomicExch(&A.overflow[2], 1);
                   return;
                 }
-                emit(A, q.slot, nf, A.raw_full, A.img_full, j, code | (r2 < fcut2 ? IN_CUT : 0));
+                stage((ks << IMG_BITS) | code, r2 < fcut2);
               } else {
-                try_atom(A, q, j, W, nf, nh);
+                try_atom(A, q, j, W, nh, [&](int, int c) {
+                  stage((ks << IMG_BITS) | (c & (IN_CUT - 1)), (c & IN_CUT) != 0);
+                });
               }
             };
             for (int k = beg; k < end; k++) {
               const float4 pj = A.acell_pos32[k];
-              if (active) consider(pj);
+              // room for one more entry in every lane's rings
+              if (__any_sync(0xffffffffu, active && (nin - fin >= STAGE_ROWS || nout - fout >= STAGE_ROWS)))
+                flush();
+              if (active) consider(pj, k);
             }
           }
         }
       }
+      flush();
       if (active) {
-        A.num_full[q.slot] = nf;
-        if (A.want_half) A.num_half[q.slot] = nh;
+        A.site_from[q.slot] = make_int2(nin, nout);
+        finish_counts(A, q.slot, nin, nout, nh);
       }
     }
   }
@@ -884,9 +960,9 @@ __global__ void __launch_bounds__(128, 8) k_build_atom_sites(BuildArgs A, RP P, 
     Query q;
     make_query(A, P, A.atom_of_slot[h], q);
     q.slot = h;
-    int nf = A.num_full[h], nh = A.want_half ? A.num_half[h] : 0;
-    items_warp(A, q, items + (size_t)h * icap, min(nitems[h], icap), st, nf, nh);
-    if (lane == 0) finish_counts(A, h, nf, nh);
+    int nin = A.num_in[h], nout = A.num_full[h] - nin, nh = A.want_half ? A.num_half[h] : 0;
+    items_warp(A, q, items + (size_t)h * icap, min(nitems[h], icap), st, nin, nout, nh);
+    if (lane == 0) finish_counts(A, h, nin, nout, nh);
     __syncwarp();
   }
 }
@@ -904,7 +980,7 @@ __global__ void __launch_bounds__(128, 8) k_build_gauss(BuildArgs A, RP P, const
   Query q;
   make_query(A, P, A.na + t, q);
   const Grid &ag = q.r.ag;
-  int nf = 0, nh = 0;
+  int nin = 0, nout = 0, nh = 0;
   if (A.na > 0) {
     const double pre = (A.cutneigh + 1e-6) * (A.cutneigh + 1e-6);
     int ci[3];
@@ -936,15 +1012,18 @@ __global__ void __launch_bounds__(128, 8) k_build_gauss(BuildArgs A, RP P, const
                 pass = gauss_atom_test(A, q, j, W, code);
               }
             }
-            warp_emit(A, q.slot, nf, A.raw_full, A.img_full, pass, j, code);
+            // the atom's list slot is its sorted position k
+            warp_emit_full(A, q.slot, nin, nout, A.nbr_full, nullptr, pass, (code & IN_CUT) != 0,
+                           (k << IMG_BITS) | (code & (IN_CUT - 1)), 0);
           }
         }
       }
     }
   }
   const int slot = A.na + t;
-  items_warp(A, q, items + (size_t)slot * icap, min(nitems[slot], icap), st, nf, nh);
-  if (lane == 0) finish_counts(A, q.slot, nf, nh);
+  if (lane == 0) A.site_from[slot] = make_int2(nin, nout);
+  items_warp(A, q, items + (size_t)slot * icap, min(nitems[slot], icap), st, nin, nout, nh);
+  if (lane == 0) finish_counts(A, q.slot, nin, nout, nh);
 }
 
 // ------------------------------------------------------------- compaction
@@ -993,6 +1072,29 @@ __global__ void k_remap(const int *raw, const unsigned char *img, const int *num
     const int w = (im & IN_CUT) ? a++ : b++;
     out[(size_t)w * nsi + i] = (sidx << IMG_BITS) | (im & (IN_CUT - 1));
   }
+}
+
+// Converts the element-site entries of the full lists (rows site_from.x ..
+// num_in - 1 of the front segment, cap - back .. cap - 1 - site_from.y of the
+// back one) from lattice-site ids to pair-table indices: Gauss points at
+// their fixed place, the other sites by their rank among the marked ones.
+__global__ void k_remap_sites(const int *raw, const unsigned char *img, const int *num, const int *num_in,
+                              const int2 *site_from, int nsi, int cap, const int *pref, int na, int ne, int *out) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nsi) return;
+  const int nin = num_in[i], nback = num[i] - nin;
+  if (nin + nback > cap) return;   // overflow: the build is repeated
+  const int2 from = site_from[i];
+  auto one = [&](int row) {
+    const size_t o = (size_t)row * nsi + i;
+    const int gid = raw[o] & ~KIND_SITE;
+    const int e = gid / NU, u = gid % NU;
+    const int g = site_gauss(u);
+    const int sidx = (g >= 0) ? na + NG * e + g : na + NG * ne + pref[gid];
+    out[o] = (sidx << IMG_BITS) | img[o];
+  };
+  for (int k = from.x; k < nin; k++) one(k);
+  for (int k = from.y; k < nback; k++) one(cap - 1 - k);
 }
 
 inline int nblk(long n, int t) { return (int)((n + t - 1) / t); }
@@ -1152,6 +1254,7 @@ void neigh_plan(Ctx &c, bool want_half) {
   c.raw_full.reserve(slots);
   c.img_full.reserve(slots);
   c.num_full.reserve(std::max(nsi, 1));
+  c.site_from.reserve(std::max(nsi, 1));
   c.nbr_full.reserve(slots);
   if (want_half) {
     c.raw_half.reserve(slots);
@@ -1292,6 +1395,9 @@ void neigh_build_async(Ctx &c, bool want_half) {
     A.cutneighsq = c.cutneighsq;
     A.cutforcesq = (c.pp.cut + c.inner_margin) * (c.pp.cut + c.inner_margin);
     A.want_half = want_half ? 1 : 0;
+    A.nbr_full = c.nbr_full.p;
+    A.num_in = c.num_in.p;
+    A.site_from = c.site_from.p;
     A.raw_full = c.raw_full.p;
     A.num_full = c.num_full.p;
     A.img_full = c.img_full.p;
@@ -1353,8 +1459,10 @@ void neigh_build_async(Ctx &c, bool want_half) {
       k_act_table<<<nblk((long)ngid, 256), 256, 0, c.stream>>>(flag, pref, (int)ngid, c.ne, nsi, c.act_gid.p,
                                                               c.act_off.p, c.dev_nact.p, c.overflow.p + 7);
     }
-    k_remap<<<nblk(nsi, 256), 256, 0, c.stream>>>(c.raw_full.p, c.img_full.p, c.num_full.p, nsi, c.cap, pref,
-                                                   c.atom_slot.p, c.na, c.ne, c.nbr_full.p, c.num_in.p);
+    if (c.ne)
+      k_remap_sites<<<nblk(nsi, 256), 256, 0, c.stream>>>(c.raw_full.p, c.img_full.p, c.num_full.p, c.num_in.p,
+                                                         c.site_from.p, nsi, c.cap, pref, c.na, c.ne,
+                                                         c.nbr_full.p);
     if (want_half)
       k_remap<<<nblk(nsi, 256), 256, 0, c.stream>>>(c.raw_half.p, c.img_half.p, c.num_half.p, nsi, c.cap, pref,
                                                      c.atom_slot.p, c.na, c.ne, c.nbr_half.p, nullptr);
@@ -1420,7 +1528,7 @@ void neigh_download(Ctx &c, bool half, int64_t *offset, int8_t *kind, int32_t *i
                     int8_t *img, int64_t *nentries) {
   if (!c.lists_valid || (half && !c.have_half)) throw Error(CACB200_ESTATE, "list not built");
   const int nsi = c.nsite_i();
-  std::vector<int> num_slot(nsi), num(nsi), slot_of(nsi);
+  std::vector<int> num_slot(nsi), num(nsi), slot_of(nsi), nin_slot(nsi, 0);
   std::vector<int> ent((size_t)c.cap * nsi);
   std::vector<int> atom_of(std::max(c.na, 1));
   device_nact(c);
@@ -1428,6 +1536,7 @@ void neigh_download(Ctx &c, bool half, int64_t *offset, int8_t *kind, int32_t *i
   CACB200_CUDA(cudaStreamSynchronize(c.stream));
   stream_copy(c, num_slot.data(), half ? c.num_half.p : c.num_full.p, sizeof(int) * nsi,
                           cudaMemcpyDeviceToHost);
+  if (!half) stream_copy(c, nin_slot.data(), c.num_in.p, sizeof(int) * nsi, cudaMemcpyDeviceToHost);
   if (c.na) stream_copy(c, atom_of.data(), c.slot_atom.p, sizeof(int) * c.na, cudaMemcpyDeviceToHost);
   for (int k = 0; k < nsi; k++) slot_of[k] = k;
   for (int h = 0; h < c.na; h++) slot_of[atom_of[h]] = h;
@@ -1445,8 +1554,11 @@ void neigh_download(Ctx &c, bool half, int64_t *offset, int8_t *kind, int32_t *i
   for (int i = 0; i < nsi; i++) {
     offset[i] = pos;
     row.clear();
+    const int sl = slot_of[i], nin = half ? num[i] : nin_slot[sl];
     for (int k = 0; k < num[i]; k++) {
-      int v = ent[(size_t)k * nsi + slot_of[i]];
+      // full lists: the front segment, then the back one from row cap - 1 down
+      const int r = k < nin ? k : c.cap - 1 - (k - nin);
+      int v = ent[(size_t)r * nsi + sl];
       int sidx = v >> IMG_BITS, code = v & ((1 << IMG_BITS) - 1);
       int sx, sy, sz;
       img_decode(code, sx, sy, sz);

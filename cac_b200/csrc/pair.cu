@@ -37,6 +37,7 @@ struct PairArgs {
   const int *inner_ok;              // ... usable while this is nonzero (per replica)
   const int *slot_atom;             // list slot -> atom (slots past the atoms are Gauss points)
   int na, ne, nsi;
+  int cap;                          // list rows: the rest of a list fills its last rows
   double L[3];                      // box of a single system
   const Rep *reps;                  // batches: replica descriptors ...
   const int *site_rep;              // ... and the replica of each i-site (null for one system)
@@ -100,10 +101,11 @@ __device__ __forceinline__ void for_each_neighbour(const PairArgs &A, int i, con
 }
 
 // A site's list in two walks: the inner prefix (entries within the cutoff
-// plus a margin at the build), then, unless no site has moved half the margin
-// since the build, the rest.  Each entry's arithmetic depends on its place in
-// the walk (the compiler may fuse multiply-adds differently in the grouped and
-// the remainder loop), so the prefix is always walked on its own: the sums are
+// plus a margin at the build, the list's first rows), then, unless no site
+// has moved half the margin since the build, the rest (the list's last
+// rows).  Each entry's arithmetic depends on its place in the walk (the
+// compiler may fuse multiply-adds differently in the grouped and the
+// remainder loop), so the prefix is always walked on its own: the sums are
 // the same whether the rest is walked or not.
 // The prefix flag belongs to the site's replica (one hot replica of a batch
 // does not end the shortcut for the others); one copy of the walk serves both
@@ -113,7 +115,8 @@ __device__ __forceinline__ void walk_list(const PairArgs &A, int i, const int *n
   const bool rest = n > n_in && !A.inner_ok[MANY ? A.site_rep[i] : 0];
 #pragma unroll 1
   for (int seg = 0; seg < (rest ? 2 : 1); seg++)
-    for_each_neighbour<MANY>(A, i, seg ? nb + (size_t)n_in * A.nsi : nb, seg ? n - n_in : n_in, f);
+    for_each_neighbour<MANY>(A, i, seg ? nb + (size_t)(A.cap - (n - n_in)) * A.nsi : nb, seg ? n - n_in : n_in,
+                             f);
 }
 
 // Writes force and per-site energy/virial of i-site i and accumulates the
@@ -506,6 +509,7 @@ void pair_compute(Ctx &c, int eflag, int vflag) {
   A.na = c.na;
   A.ne = c.ne;
   A.nsi = nsi;
+  A.cap = c.cap;
   for (int d = 0; d < 3; d++) A.L[d] = c.prd[d];
   A.reps = c.rep_d.p;
   A.site_rep = c.nrep > 1 ? c.site_rep.p : nullptr;

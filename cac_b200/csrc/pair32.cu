@@ -93,6 +93,7 @@ struct Args32 {
   const int *inner_ok;              // ... usable while this is nonzero (per replica)
   const int *slot_atom;    // list slot -> atom (slots past the atoms are Gauss points)
   int na, ne, nsi;
+  int cap;                 // list rows: the rest of a list fills its last rows
   FixGrid G;
   double *f, *gaussf;
   double *eatom, *vatom, *enode, *vnode;
@@ -179,7 +180,7 @@ __device__ __forceinline__ void for_each32(const Args32 &A, int t, int i, const 
   const bool rest = n > n_in && !A.inner_ok[A.G.reps ? A.G.site_rep[i] : 0];
 #pragma unroll 1
   for (int seg = 0; seg < (rest ? 2 : 1); seg++)
-    walk32(A, fx, oi, seg ? nb + (size_t)n_in * A.nsi : nb, seg ? n - n_in : n_in, f);
+    walk32(A, fx, oi, seg ? nb + (size_t)(A.cap - (n - n_in)) * A.nsi : nb, seg ? n - n_in : n_in, f);
 }
 
 __device__ __forceinline__ void finish32(const Args32 &A, int i, bool valid, const float fi[3], bool ev,
@@ -458,6 +459,7 @@ void pair_compute_mixed(Ctx &c, int eflag, int vflag) {
   A.na = c.na;
   A.ne = c.ne;
   A.nsi = nsi;
+  A.cap = c.cap;
   A.G = G;
   A.f = c.f.p;
   A.gaussf = c.gaussf.p;
