@@ -9,17 +9,22 @@
 #include <cstdlib>
 #include <cstring>
 #include <string>
+#include <cmath>
 #include <tuple>
+#include <unordered_map>
 #include <vector>
 
 #include "atom.h"
 #include "comm.h"
+#include "compute_b200.h"
 #include "domain.h"
 #include "element.h"
 #include "element_vec.h"
 #include "error.h"
 #include "force.h"
 #include "modify.h"
+#include "my_page.h"
+#include "neigh_list.h"
 #include "neighbor.h"
 #include "output.h"
 #include "pair.h"
@@ -204,7 +209,9 @@ void B200Bridge::compute(Pair *pair)
   }
 }
 
-void B200Bridge::run_nve(int nsteps, double dt, int every, const B200Fixes &fx, bool thermo_output)
+B200ThermoNow CAC_NS::b200_thermo_now;
+
+void B200Bridge::run_device(int nsteps, double dt, int every, const B200Fixes &fx, bool step0_output)
 {
   check_system();
   upload(true);
@@ -218,28 +225,39 @@ void B200Bridge::run_nve(int nsteps, double dt, int every, const B200Fixes &fx, 
     status(cacb200_set_deform(ctx, fx.deform_every, fx.deform_style, fx.deform_a, fx.deform_b,
                               fx.deform_remap_x),
            "set_deform");
-  // thermo output on the reference's schedule (Output::setup / Output::write,
-  // output.cpp:264-284, 378-392): step 0 with the header, every
-  // thermo_every steps, and the last step of the run
-  const int ev = thermo_output ? CACB200_ENERGY_GLOBAL : 0, vv = thermo_output ? CACB200_VIRIAL_GLOBAL : 0;
-  const bigint step0 = update->ntimestep;
-  status(cacb200_run_begin(ctx, nsteps, dt, ev, vv), "run_begin");
-  if (thermo_output) thermo_line(step0, true, fx.deform);
-  const bigint every_t = output->thermo_every;
-  int done = 0;
-  while (done < nsteps) {
-    int k = nsteps - done;
-    if (thermo_output && every_t > 0) {
-      const bigint now = step0 + done;
-      const bigint next = (now / every_t) * every_t + every_t;
-      k = (int)std::min<bigint>(next - now, (bigint)(nsteps - done));
-    }
-    const bool out = thermo_output && (every_t > 0 || k == nsteps - done);
-    status(cacb200_run_steps(ctx, k, dt, out ? ev : 0, out ? vv : 0), "run_steps");
-    done += k;
-    if (out) thermo_line(step0 + done, false, fx.deform);
+  // thermo and dumps that read only what the device output path provides
+  // need no state copy at thermo-only steps
+  output_copies_state = !b200_device_output_safe(cac);
+  const long long copies0 = state_copies;
+  // per-site tallies at output steps only when a dump may read them
+  const int ev_out = CACB200_ENERGY_GLOBAL | (output->ndump ? CACB200_ENERGY_ATOM : 0);
+  const int vv_out = CACB200_VIRIAL_GLOBAL | (output->ndump ? CACB200_VIRIAL_ATOM : 0);
+  const bigint step0 = update->ntimestep, end = step0 + nsteps;
+  status(cacb200_run_begin(ctx, nsteps, dt, step0_output ? ev_out : 0, step0_output ? vv_out : 0), "run_begin");
+  if (step0_output) output_step(step0, fx.deform, true);
+  // Verlet::run's loop (verlet.cpp:218-360): the device advances to the next
+  // step with output (Output::next), then the reference writes it
+  while (update->ntimestep < end) {
+    const bigint stop = std::min<bigint>(output->next, end);
+    const bool out = stop == output->next;
+    const int k = (int)(stop - update->ntimestep);
+    status(cacb200_run_steps(ctx, k, dt, out ? ev_out : 0, out ? vv_out : 0), "run_steps");
+    update->ntimestep = stop;
+    if (out) output_step(stop, fx.deform, false);
   }
   download_state(fx.deform);
+  download_forces();
+  uploaded_na = uploaded_ne = -1;   // the reference must set up again (ghosts are stale)
+  const long long copies = state_copies - copies0;
+  for (FILE *fp : {screen, logfile})
+    if (fp)
+      fprintf(fp, "b200 device run: %d steps, %lld output steps with a host copy of the state\n", nsteps, copies);
+}
+
+// Forces of the last evaluation into atom->f, element->nodef and
+// element->gaussf.
+void B200Bridge::download_forces()
+{
   int na = atom->nlocal, ne = element->nlocal;
   fbuf.resize(3 * (size_t)std::max(na, 1));
   gbuf.resize(24 * (size_t)std::max(ne, 1));
@@ -253,7 +271,6 @@ void B200Bridge::run_nve(int nsteps, double dt, int every, const B200Fixes &fx, 
         element->nodef[e][0][n][d] = nf[24 * (size_t)e + 3 * n + d];
         element->gaussf[e][0][n][d] = gbuf[24 * (size_t)e + 3 * n + d];
       }
-  uploaded_na = uploaded_ne = -1;   // the reference must set up again (ghosts are stale)
 }
 
 void B200Bridge::minimize_fire(double etol, double ftol, int maxiter, double dt, int normstyle,
@@ -309,23 +326,161 @@ void B200Bridge::download_state(bool box)
   }
 }
 
-// One thermo line of the reference (Thermo::header / Thermo::compute) at
-// `step`: the state and the pair's global tallies of that step go into the
-// reference's arrays, and its own Thermo evaluates and prints every keyword.
-void B200Bridge::thermo_line(bigint step, bool first, bool box)
+// One output step of a device run, written by the reference's own Output
+// (Output::setup on `first`, else Output::write): the box, the pair's
+// global tallies and the device thermo read-out for compute temp/b200, all
+// of a few doubles; a dump that may be due at this step (or computes that
+// read host per-site data) also get the state, the forces and the per-site
+// tallies in the reference's arrays.
+void B200Bridge::output_step(bigint step, bool box, bool first)
 {
-  download_state(box);
-  double e = 0.0, vir[6];
-  status(cacb200_get_energy(ctx, &e, vir, nullptr, nullptr, nullptr, nullptr), "get_energy");
+  const bool dump_due = output->ndump && (first || output->next_dump_any == step);
+  const bool copy = dump_due || output_copies_state;
+  if (copy) {
+    download_state(box);
+    download_forces();
+    state_copies++;
+  } else if (box) {
+    double lo[3], hi[3], m = 0.0;
+    status(cacb200_get_box(ctx, lo, hi, &m), "get_box");
+    for (int d = 0; d < 3; d++) {
+      domain->boxlo[d] = lo[d];
+      domain->boxhi[d] = hi[d];
+    }
+    domain->set_global_box();
+    domain->set_local_box();
+  }
   Pair *pair = force->pair;
+  double e = 0.0, vir[6];
+  if (dump_due) {
+    // the per-site tallies of this step for per-atom computes (pe/atom,
+    // stress/atom), as Pair::compute leaves them
+    const int na = atom->nlocal, ne = element->nlocal;
+    ebuf.resize(std::max(na, 1));
+    vbuf.resize(6 * (size_t)std::max(na, 1));
+    enbuf.resize(8 * (size_t)std::max(ne, 1));
+    vnbuf.resize(48 * (size_t)std::max(ne, 1));
+    status(cacb200_get_energy(ctx, &e, vir, ebuf.data(), vbuf.data(), enbuf.data(), vnbuf.data()), "get_energy");
+    if (pair->eatom && pair->vatom) {
+      for (int i = 0; i < na; i++) {
+        pair->eatom[i] = ebuf[i];
+        for (int k = 0; k < 6; k++) pair->vatom[i][k] = vbuf[6 * (size_t)i + k];
+      }
+      for (int i = na; i < na + atom->nghost; i++) {
+        pair->eatom[i] = 0.0;
+        for (int k = 0; k < 6; k++) pair->vatom[i][k] = 0.0;
+      }
+    }
+    if (pair->enode && pair->vnode) {
+      for (int el = 0; el < ne; el++)
+        for (int n = 0; n < 8; n++) {
+          pair->enode[el][0][n] = enbuf[8 * (size_t)el + n];
+          for (int k = 0; k < 6; k++) pair->vnode[el][0][n][k] = vnbuf[48 * (size_t)el + 6 * n + k];
+        }
+      for (int el = ne; el < ne + element->nghost; el++)
+        for (int n = 0; n < 8; n++) {
+          pair->enode[el][0][n] = 0.0;
+          for (int k = 0; k < 6; k++) pair->vnode[el][0][n][k] = 0.0;
+        }
+    }
+    update->eflag_atom = update->vflag_atom = step;
+  } else {
+    status(cacb200_get_energy(ctx, &e, vir, nullptr, nullptr, nullptr, nullptr), "get_energy");
+  }
   pair->eng_vdwl = e;
   pair->eng_coul = 0.0;
   for (int k = 0; k < 6; k++) pair->virial[k] = vir[k];
+  b200_thermo_now.step = step;
+  status(cacb200_thermo(ctx, strcmp(update->unit_style, "metal") == 0 ? CACB200_UNITS_METAL : CACB200_UNITS_METALGPA,
+                        b200_thermo_now.v),
+         "thermo");
+  b200_thermo_now.active = true;
   update->ntimestep = step;
   update->eflag_global = update->vflag_global = step;
   modify->clearstep_compute();
-  if (first) output->thermo->header();
-  output->thermo->compute(first ? 0 : 1);
+  if (first) output->setup(0);
+  else output->write(step);
+  b200_thermo_now.active = false;
+}
+
+void B200Bridge::fill_host_list(NeighList *list)
+{
+  check_system();
+  upload(false);
+  status(cacb200_set_neighbor(ctx, neighbor->skin, 0), "set_neighbor");
+  status(cacb200_build_lists(ctx, 1), "build_lists");
+  int64_t n = 0;
+  int nsites = 0;
+  status(cacb200_list_size(ctx, 1, &n, &nsites), "list_size");
+  std::vector<int64_t> off(nsites + 1);
+  std::vector<int8_t> kind(std::max<int64_t>(n, 1)), img(3 * std::max<int64_t>(n, 1));
+  std::vector<int32_t> idx(std::max<int64_t>(n, 1)), site(std::max<int64_t>(n, 1));
+  status(cacb200_get_list(ctx, 1, off.data(), kind.data(), idx.data(), site.data(), img.data()), "get_list");
+
+  // (owner, periodic image) -> the reference's local or ghost index: owners
+  // by tag, each ghost's image from its position relative to its owner
+  const int na = atom->nlocal, nag = na + atom->nghost;
+  const int ne = element->nlocal, neg = ne + element->nghost;
+  const double *prd = domain->prd;
+  auto key = [](long owner, int sx, int sy, int sz) {
+    return ((owner * 5 + (sx + 2)) * 5 + (sy + 2)) * 5 + (sz + 2);
+  };
+  auto image = [&](const double *xg, const double *xo, int d) {
+    return (int) std::lround((xg[d] - xo[d]) / prd[d]);
+  };
+  std::unordered_map<tagint, int> aown, eown;
+  for (int i = 0; i < na; i++) aown[atom->tag[i]] = i;
+  for (int i = 0; i < ne; i++) eown[element->tag[i]] = i;
+  std::unordered_map<long, int> aimg, eimg;
+  for (int g = na; g < nag; g++) {
+    auto it = aown.find(atom->tag[g]);
+    if (it == aown.end()) continue;
+    const double *xg = atom->x[g], *xo = atom->x[it->second];
+    aimg[key(it->second, image(xg, xo, 0), image(xg, xo, 1), image(xg, xo, 2))] = g;
+  }
+  for (int g = ne; g < neg; g++) {
+    auto it = eown.find(element->tag[g]);
+    if (it == eown.end()) continue;
+    const double *xg = element->x[g], *xo = element->x[it->second];
+    eimg[key(it->second, image(xg, xo, 0), image(xg, xo, 1), image(xg, xo, 2))] = g;
+  }
+
+  MyPage<int> *ipage = list->ipage, *indexpage = list->indexpage;
+  ipage->reset();
+  indexpage->reset();
+  int inum = 0;
+  for (int i = 0; i < nsites; i++) {
+    int *nptr = ipage->vget();
+    int *iptr = indexpage->vget();
+    int m = 0;
+    for (int64_t k = off[i]; k < off[i + 1]; k++) {
+      const int sx = img[3 * k], sy = img[3 * k + 1], sz = img[3 * k + 2];
+      int j = idx[k];
+      if (sx || sy || sz) {
+        auto &tab = kind[k] == 0 ? aimg : eimg;
+        auto it = tab.find(key(idx[k], sx, sy, sz));
+        if (it == tab.end()) error->one(FLERR, "b200: a device list neighbour has no ghost copy on this rank");
+        j = it->second;
+      }
+      nptr[m] = j;
+      iptr[m] = kind[k] == 0 ? -1 : site[k];   // jucell * apc + jbasis with apc 1
+      m++;
+    }
+    list->firstneigh[inum] = nptr;
+    list->firstneighindex[inum] = iptr;
+    list->numneigh[inum] = m;
+    ipage->vgot(m);
+    indexpage->vgot(m);
+    if (ipage->status() || indexpage->status())
+      error->one(FLERR, "Neighbor list overflow, boost neigh_modify one");
+    list->ilist[inum] = i < na ? i : (i - na) / 8;
+    list->iindexlist[inum] = i < na ? -1 : (i - na) % 8;   // igcell * apc + ibasis
+    inum++;
+  }
+  list->ainum = na;
+  list->einum = list->ninum = 0;
+  list->ginum = inum - na;
+  list->inum = inum;
 }
 
 void B200Bridge::dump_list(const char *file, int half)

@@ -46,6 +46,16 @@ struct B200Fire {
   int halfstepback = 1, delaystep_start = 1, max_vdotf_negatif = 2000;
 };
 
+// The device thermo read-out (cacb200_thermo) of the output step the
+// reference's Output is writing during a device run; compute temp/b200 reads
+// it instead of the host velocities while `active` and the step matches.
+struct B200ThermoNow {
+  bool active = false;
+  bigint step = -1;
+  double v[12] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+};
+extern B200ThermoNow b200_thermo_now;
+
 class B200Bridge : protected Pointers {
  public:
   explicit B200Bridge(class CAC *);
@@ -57,9 +67,21 @@ class B200Bridge : protected Pointers {
   // Pair::compute body: fills atom->f, element->gaussf, eng_vdwl, virial and
   // the per-site arrays of `pair` according to its ev flags.
   void compute(class Pair *pair);
-  // run N velocity-Verlet steps on the device (run_b200 command), with the
-  // given thermostat / deformation; thermo lines on the reference's schedule
-  void run_nve(int nsteps, double dt, int every, const B200Fixes &fixes, bool thermo_output);
+  // run N velocity-Verlet steps on the device (run_b200 command, run_style
+  // verlet/b200), with the given thermostat / deformation.  Output comes on
+  // the reference's schedule through its own Output: at every output step the
+  // device's global tallies go into the pair and its thermo read-out to
+  // compute temp/b200, so thermo lines copy no per-site data; a dump due at
+  // the step (or computes that read host per-site data) bring the state,
+  // the forces and the per-site tallies into the reference's arrays.
+  // step0_output: also write step 0 (run_b200; under run the integrator's
+  // setup did).
+  void run_device(int nsteps, double dt, int every, const B200Fixes &fixes, bool step0_output);
+  // per-site state copies to the host made for output during device runs
+  long long state_copies = 0;
+  // a device run copies the state at every output step (computes that read
+  // host per-site data are defined)
+  bool output_copies_state = false;
   // minimise on the device from the reference's current state (min_style
   // fire/b200) under the reference's current neighbour rule; the final
   // positions come back into atom->x / element->nodex (velocities are left
@@ -68,6 +90,10 @@ class B200Bridge : protected Pointers {
                      int &stop, int &niter, double &energy, double &fnorm);
   // canonical neighbour-list dump (write_b200_neighbor command)
   void dump_list(const char *file, int half);
+  // the device's half list into the reference's host list (NPair
+  // half/bin/newton/b200 outside a run): its site order, local and ghost
+  // indices, lattice-site index of element neighbours
+  void fill_host_list(class NeighList *list);
 
   cacb200_ctx *ctx = nullptr;
 
@@ -83,7 +109,8 @@ class B200Bridge : protected Pointers {
 
   void check_system();
   void download_state(bool box);
-  void thermo_line(bigint step, bool first, bool box);
+  void download_forces();
+  void output_step(bigint step, bool box, bool first);
   void upload(bool with_velocities);
   void configure_pair();
   void status(int rc, const char *what);

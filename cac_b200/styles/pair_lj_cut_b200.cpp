@@ -2,6 +2,7 @@
 
 #include "atom.h"
 #include "error.h"
+#include "neighbor.h"
 
 using namespace CAC_NS;
 
@@ -11,7 +12,11 @@ PairLJCutB200::~PairLJCutB200() { delete bridge; }
 
 void PairLJCutB200::init_style()
 {
-  // no host list: the device lists follow Neighbor::ago
+  // the default half list (as PairLJCut::init_style requests it); the NPair
+  // class serving it (half/bin/newton/b200) stores nothing during a run:
+  // the device lists follow Neighbor::ago.  The requestor is the Pair
+  // subobject: Neighbor::init casts it back to Pair *.
+  neighbor->request(static_cast<Pair *>(this), instance_me);
   cut_respa = nullptr;
 }
 

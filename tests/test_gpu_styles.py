@@ -66,10 +66,12 @@ def test_pair_style_drop_in_setup_forces(case, golden, tmp_path):
 
 
 @pytest.mark.parametrize("case", ["tiny_lj", "tiny_eam"])
-@pytest.mark.parametrize("mode", ["run", "run_b200"])
+@pytest.mark.parametrize("mode", ["run", "run_b200", "run_style verlet/b200\nrun"])
 def test_trajectory_in_reference_loop(case, mode, golden, tmp_path):
-    """`run N` (reference Verlet + fix nve, device forces) and `run_b200 N`
-    (whole loop on the device) both reproduce the reference trajectory."""
+    """`run N` (reference Verlet + fix nve, device forces), `run_b200 N`
+    and `run_style verlet/b200` + `run N` (the reference's run command with
+    the whole step loop on the device) all reproduce the reference
+    trajectory."""
     g = golden(case)
     n = int(g["nsteps"])
     s, O = run_app(tmp_path, case, f"{mode} {n}\noracle_dump end.txt state\n")
@@ -301,3 +303,86 @@ def test_run_b200_check_yes_follows_the_reference(oracle_mod, tmp_path):
     assert np.abs(d["nodex"] - ref["nodex"]).max() < 1e-10
     assert rel_err(d["v"], ref["v"]) < TOL
     assert rel_err(d["nodev"], ref["nodev"]) < TOL
+
+
+def test_verlet_b200_thermo_every_step_copies_no_state(tmp_path):
+    """run_style verlet/b200 with `thermo 1`: every step's thermo line comes
+    from the device read-out (compute temp/b200 in place of thermo_temp, the
+    pair's global tallies), equal to the reference's own run, and the device
+    run copies no per-site state to the host for them."""
+    import oracle as O
+    deck = THERMO.replace("thermo 10", "thermo 1")
+    out = app_log(tmp_path, "tiny_eam", deck + "run_style verlet/b200\nrun 25\n")
+    ours = O.read_thermo(out)
+    ref = O.read_thermo(reference_log(tmp_path, "tiny_eam", deck + "run 25\n", O.REF_EXE_EAMFIX))
+    assert list(ours[:, 0]) == list(range(26))
+    assert_thermo_rows(ours, ref, O)
+    assert "b200 device run: 25 steps, 0 output steps with a host copy of the state" in out
+
+
+def read_dump_frames(path):
+    """Numeric rows of a dump custom file (ITEM: ATOMS section), sorted by
+    their columns."""
+    rows, on = [], False
+    with open(path) as f:
+        for ln in f:
+            if ln.startswith("ITEM:"):
+                on = ln.startswith("ITEM: ATOMS")
+                continue
+            if on and ln.strip():
+                rows.append([float(t) for t in ln.split()])
+    a = np.array(rows)
+    return a[np.lexsort(a.T[::-1])]
+
+
+@pytest.mark.parametrize("case", ["tiny_lj", "tiny_eam"])
+def test_verlet_b200_dumps_with_device_peratom_computes(case, tmp_path):
+    """A deck with per-site computes and a dump every 10 steps, run by the
+    reference's `run` under run_style verlet/b200 with compute pe/atom/b200
+    and stress/atom/b200: the dump files equal the reference's own run with
+    compute pe/atom and stress/atom at the dump's print precision, and the
+    device run copies the state only at the two dump steps inside it."""
+    import oracle as O
+    pair = CASES[case][1]
+    dump = ("dump 1 all custom 10 d.* id type x y z fx fy fz c_pa c_sa[1] c_sa[2] c_sa[3] c_sa[4] "
+            "c_sa[5] c_sa[6]\n")
+    ours_deck = ("compute pa all pe/atom/b200\ncompute sa all stress/atom/b200 NULL\n" + dump + THERMO +
+                 "run_style verlet/b200\nrun 20\n")
+    ref_deck = "compute pa all pe/atom\ncompute sa all stress/atom NULL\n" + dump + THERMO + "run 20\n"
+    out = app_log(tmp_path, case, ours_deck)
+    exe = O.REF_EXE_EAMFIX if pair == "eam" else O.REF_EXE
+    reference_log(tmp_path, case, ref_deck, exe)
+    assert "b200 device run: 20 steps, 2 output steps with a host copy of the state" in out
+    for step in (0, 10, 20):
+        a = read_dump_frames(str(tmp_path / f"d.{step}"))
+        b = read_dump_frames(str(tmp_path / "ref" / f"d.{step}"))
+        assert a.shape == b.shape and a.shape[0] > 0
+        assert np.array_equal(a[:, :2], b[:, :2])
+        for c in range(2, a.shape[1]):
+            scale = max(np.abs(b[:, c]).max(), 1e-30)
+            assert np.abs(a[:, c] - b[:, c]).max() <= 1e-5 * scale, (step, c)
+
+
+@pytest.mark.parametrize("case", ["tiny_lj", "tiny_eam"])
+def test_reference_neighbor_debug_dump_reads_the_device_list(case, tmp_path):
+    """The reference's own write_dump_neighbor_debug with a /b200 pair style:
+    its list is served by NPair half/bin/newton/b200, which outside a run
+    fills the host list from the device's half list.  The whole-list dump
+    (per site: coordinates, tag, neighbour count) equals the reference's own
+    file, and one atom's and one Gauss point's neighbours (coordinates, tag,
+    lattice site) equal the reference's as sets."""
+    import oracle as O
+    body = ("write_dump_neighbor_debug nb\nwrite_dump_neighbor_debug na atom 5\n"
+            "write_dump_neighbor_debug ng gauss 3 0 2\n")
+    app_log(tmp_path, case, body)
+    reference_log(tmp_path, case, body, O.REF_EXE)
+    with open(tmp_path / "nb_proc_0.dat") as f1, open(tmp_path / "ref" / "nb_proc_0.dat") as f2:
+        assert f1.read() == f2.read()
+    for name in ("na_proc_0", "ng_proc_0"):
+        with open(tmp_path / name) as f1, open(tmp_path / "ref" / name) as f2:
+            a, b = f1.read().splitlines(), f2.read().splitlines()
+        head = next(k for k, ln in enumerate(b) if ln.startswith("ITEM: ATOMS")) + 2
+        assert a[:head] == b[:head]
+        assert len(a) == len(b) and len(a) > head + 10
+        assert sorted(" ".join(ln.split()[1:]) for ln in a[head:]) == \
+            sorted(" ".join(ln.split()[1:]) for ln in b[head:])
