@@ -880,9 +880,24 @@ __device__ __forceinline__ void build_atoms_cells(BuildArgs A, RP P, int ncell) 
                 });
               }
             };
-            for (int k = beg; k < end; k++) {
+            // candidates four at a time: the four broadcast loads are in
+            // flight together instead of one load's latency per candidate
+            int k = beg;
+            for (; k + 4 <= end; k += 4) {
+              const float4 p0 = A.acell_pos32[k], p1 = A.acell_pos32[k + 1];
+              const float4 p2 = A.acell_pos32[k + 2], p3 = A.acell_pos32[k + 3];
+              // room for four more entries in every lane's rings
+              if (__any_sync(0xffffffffu, active && (nin - fin > STAGE_ROWS - 4 || nout - fout > STAGE_ROWS - 4)))
+                flush();
+              if (active) {
+                consider(p0, k);
+                consider(p1, k + 1);
+                consider(p2, k + 2);
+                consider(p3, k + 3);
+              }
+            }
+            for (; k < end; k++) {
               const float4 pj = A.acell_pos32[k];
-              // room for one more entry in every lane's rings
               if (__any_sync(0xffffffffu, active && (nin - fin >= STAGE_ROWS || nout - fout >= STAGE_ROWS)))
                 flush();
               if (active) consider(pj, k);
