@@ -340,11 +340,16 @@ def alg_bytes_per_site(kernel: str) -> int:
 TRAFFIC_PER_SITE = {"eam_force": 112.05e6 / 313120, "eam_force32": 122.8e6 / 313120}
 
 
-def stream_bytes(kernel: str, na: int, ne: int, nact: int) -> int:
+def stream_bytes(kernel: str, na: int, ne: int, nact: int, mixed: bool = False) -> int:
     """Compulsory HBM bytes per launch of the streaming kernels (FP64 state):
     what each must read and write once, with per-element node data counted
-    once per element."""
+    once per element.  The mixed form's pair table is written as 16-byte
+    fixed-point records."""
     nsi = na + 8 * ne
+    if mixed and kernel == "interpolate":
+        # read atom (32) + slot (4), Gauss-point node (24), site id (4) and
+        # nodes once per element; write a 16-byte record per entry
+        return 52 * na + 40 * 8 * ne + 20 * nact + 192 * ne
     return {
         "nve_initial": 120 * nsi,                       # read x, v, f; write x, v (atoms and nodes)
         "nve_final": 72 * nsi,                          # read v, f; write v
@@ -561,7 +566,7 @@ def b200_arm(args, rank, local, ws, dist):
     nact = eng.counts()[2]
     hbm_by_kernel = {}
     for k, (tot_ms, nl) in sorted(prof.items()):
-        b = stream_bytes(k, natoms, nelements, nact)
+        b = stream_bytes(k, natoms, nelements, nact, args.form == "mixed")
         if b and nl:
             gbs = b / (tot_ms / nl / 1000.0) / 1e9
             hbm_by_kernel[k] = {"gbs": gbs, "frac": gbs / hbm, "bytes_per_launch": b}

@@ -405,6 +405,8 @@ void neigh_download(Ctx &c, bool half, int64_t *offset, int8_t *kind, int32_t *i
 void interpolate_sites(Ctx &c);
 void pair_compute(Ctx &c, int eflag, int vflag);
 void pair_compute_mixed(Ctx &c, int eflag, int vflag);
+// the mixed form's pair table as fixed-point records (interpolate_sites)
+void pair_table_mixed(Ctx &c);
 void assemble_nodef(Ctx &c);
 void nve_initial(Ctx &c, double dt);
 bool moved_past_trigger(Ctx &c);

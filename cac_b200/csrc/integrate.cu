@@ -147,6 +147,10 @@ __global__ void k_nve_final(double *v, const double *f, int n3, double *nodev, c
 void interpolate_sites(Ctx &c) {
   if (c.na + c.ne == 0 || !c.lists_valid) return;
   KernelTimer t(c, "interpolate");
+  if (c.precision == CACB200_MIXED) {
+    pair_table_mixed(c);   // fixed-point records directly (pair32.cu)
+    return;
+  }
   k_pair_table<<<stride_grid((long)c.na + (long)NG * c.ne + (long)c.ne * NU, 256), 256, 0, c.stream>>>(
       c.xs.p, c.xss.p, c.slot_atom.p, c.nodex.p, c.na, c.ne, c.act_gid.p, c.dev_nact.p);
 }

@@ -45,9 +45,11 @@ struct FixGrid {
   int na, nsi;
 };
 
-__device__ __forceinline__ void pack_one(const double4 *xs, int k, const FixGrid &G, int4 *pos, int *bad) {
-  double4 p = xs[k];
-  double q[3] = {p.x, p.y, p.z};
+// Fixed-point record of pair-table entry k at FP64 position (px, py, pz),
+// in the frame of its replica; w (F') is written later in the step.
+__device__ __forceinline__ void pack_pos(double px, double py, double pz, int k, const FixGrid &G, int4 *pos,
+                                         int *bad) {
+  double q[3] = {px, py, pz};
   double lo[3] = {G.lo[0], G.lo[1], G.lo[2]};
   double sc[3] = {G.scale[0], G.scale[1], G.scale[2]};
   if (G.reps) {
@@ -72,17 +74,43 @@ __device__ __forceinline__ void pack_one(const double4 *xs, int k, const FixGrid
     }
     o[d] = (int)(unsigned)(unsigned long long)__double2ll_rn(rel);   // modulo 2^32
   }
-  int4 v = pos[k];
-  pos[k] = make_int4(o[0], o[1], o[2], v.w);
+  pos[k] = make_int4(o[0], o[1], o[2], 0);
 }
 
-// Fixed-point copy of the pair table (list-slot order); w keeps F' for EAM
-// (written later in the step).  The active-site count is read on the device, so a
-// fixed grid strides over [atoms | Gauss points | active sites].
-__global__ void k_pack32(const double4 *xs, int nsi, const int *nact_dev, FixGrid G, int4 *pos, int *bad) {
-  const int n = nsi + *nact_dev;
-  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x)
-    pack_one(xs, k, G, pos, bad);
+// The mixed form's pair table in one pass: the slot-ordered atoms, the Gauss
+// points and the interpolated active lattice sites (the positions of
+// k_pair_table, integrate.cu, in the same FP64 operations) written straight
+// as fixed-point records, with no FP64 copy in between.
+__global__ void k_pair_table32(const double4 *xs, const int *slot_atom, const double *nodex, int na, int ne,
+                               const int *act_gid, const int *nact_dev, FixGrid G, int4 *pos, int *bad) {
+  const int ngp = NG * ne;
+  const int n = na + ngp + *nact_dev;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+    if (t < na) {
+      const double4 p = xs[slot_atom[t]];
+      pack_pos(p.x, p.y, p.z, t, G, pos, bad);
+      continue;
+    }
+    const int s = t - na;
+    if (s < ngp) {
+      const int e = s / NG, g = s % NG;
+      const double *nx = nodex + (size_t)e * 24 + 3 * gauss_node(g);
+      pack_pos(nx[0], nx[1], nx[2], t, G, pos, bad);
+      continue;
+    }
+    const int gid = act_gid[s - ngp];
+    const int e = gid / NU, u = gid % NU;
+    const double *nx = nodex + (size_t)e * 24;
+    double x = 0.0, y = 0.0, z = 0.0;
+#pragma unroll
+    for (int m = 0; m < NPE; m++) {
+      const double N = shape_val(u, m);
+      x += N * nx[3 * m];
+      y += N * nx[3 * m + 1];
+      z += N * nx[3 * m + 2];
+    }
+    pack_pos(x, y, z, t, G, pos, bad);
+  }
 }
 
 struct Args32 {
@@ -422,6 +450,16 @@ FixGrid make_fix_grid(const Ctx &c) {
 
 }  // namespace
 
+void pair_table_mixed(Ctx &c) {
+  const long ns = (long)c.nsite_i() + (long)c.ne * NU;   // capacity: every lattice site active
+  c.pos32.reserve(std::max(ns, 1L));
+  c.overflow.reserve(16);
+  FixGrid G = make_fix_grid(c);
+  k_pair_table32<<<stride_grid(ns, 256), 256, 0, c.stream>>>(c.xs.p, c.slot_atom.p, c.nodex.p, c.na, c.ne,
+                                                             c.act_gid.p, c.dev_nact.p, G, c.pos32.p,
+                                                             c.overflow.p + 6);
+}
+
 void mixed_tables(Ctx &c) {
   auto conv = [&](DBuf<double4> &src, DBuf<float4> &dst, int n) {
     std::vector<double4> h(n + 1);
@@ -442,13 +480,7 @@ void pair_compute_mixed(Ctx &c, int eflag, int vflag) {
   const int T = 128;
   const int nb = std::max(nblk(nsi, T), 1);
   FixGrid G = make_fix_grid(c);
-  c.pos32.reserve(std::max(ns, 1L));
-  c.overflow.reserve(16);
-  {
-    KernelTimer t(c, "pack32");
-    k_pack32<<<stride_grid(ns, 256), 256, 0, c.stream>>>(c.xss.p, nsi, c.dev_nact.p, G, c.pos32.p,
-                                                         c.overflow.p + 6);
-  }
+  (void)ns;   // the fixed-point records were written by pair_table_mixed
   Args32 A;
   A.pos = c.pos32.p;
   A.nbr = c.nbr_full.p;
