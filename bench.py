@@ -28,11 +28,13 @@ step).  value = atom+IP sites x steps / device time (max over ranks).
 
 The K timed steps run as trajectories of at most ``--segment`` (50) steps,
 each restarted from the seeded initial state on the device (state restore,
-list build and a force evaluation, all inside the timed region).  The
-reference's own dynamics on these systems gain energy without bound (its
-total energy rises by thousands of eV within 300 steps, LJ and EAM alike), so
-long trajectories stop being physical; the restarts keep the timed work on
-physical configurations.
+list build and a force evaluation).  The first trajectory's setup happens
+before the timer starts, as the reference's "Loop time" starts after its
+Verlet::setup; the restarts of later trajectories are inside the timed
+region.  The reference's own dynamics on these systems gain energy without
+bound (its total energy rises by thousands of eV within 300 steps, LJ and EAM
+alike), so long trajectories stop being physical; the restarts keep the
+timed work on physical configurations.
 
 ``--fix langevin`` / ``--fix deform`` time the same trajectories under the
 reference's fix langevin (300 K, damp 0.1 ps) or fix deform (x erate 0.1/ps,
@@ -424,19 +426,24 @@ def make_engine(s, pair, form: str, local: int, setfl: str, fix: str):
 class Trajectories:
     """Velocity-Verlet steps as segments of at most `seg` steps, each from
     the seeded initial state (restore + list build + forces; with a deforming
-    box, the seeded box too)."""
+    box, the seeded box too).  `prepare` sets a segment up (the reference's
+    Verlet::setup, outside its Loop time); `run` starts from a prepared
+    state and sets up every later segment itself."""
 
     def __init__(self, eng, seg: int, box0=None):
         self.eng, self.seg, self.box0 = eng, seg, box0
 
-    def run(self, nsteps: int, first: bool):
+    def prepare(self):
+        self.eng.restore()
+        if self.box0 is not None:
+            self.eng.set_box(*self.box0)
+        self.eng.setup()
+
+    def run(self, nsteps: int):
         done = 0
         while done < nsteps:
-            if not (first and done == 0):
-                self.eng.restore()
-                if self.box0 is not None:
-                    self.eng.set_box(*self.box0)
-                self.eng.setup()
+            if done:
+                self.prepare()
             k = min(self.seg, nsteps - done)
             self.eng.run_nve(k, 0.001)
             done += k
@@ -445,10 +452,13 @@ class Trajectories:
 def timed_region(eng, tr: Trajectories, steps: int, warmup: int, local: int, dist, clocks: bool):
     """W warm-up steps, then K steps between barriers and synchronisations,
     timed with CUDA events on the context's stream; (slowest rank's ms, clock
-    summary or None)."""
+    summary or None).  The timed run starts from a state set up before the
+    timer (lists and forces of the seeded state), as the reference's Loop
+    time starts after Verlet::setup; restarts of later segments are timed."""
     import torch
     stream = torch.cuda.ExternalStream(eng.stream, device=torch.device("cuda", local))
-    tr.run(warmup, True)
+    tr.run(warmup)
+    tr.prepare()
     torch.cuda.synchronize(local)
     if dist:
         dist.barrier()
@@ -462,7 +472,7 @@ def timed_region(eng, tr: Trajectories, steps: int, warmup: int, local: int, dis
         if dist:
             dist.barrier()
         e0.record(stream)
-        tr.run(steps, False)
+        tr.run(steps)
         e1.record(stream)
         torch.cuda.synchronize(local)
         if dist:
