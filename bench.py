@@ -745,12 +745,48 @@ def merge_serving(parts):
     return lat, site_steps, codes, failed, makespan
 
 
+def serve_stream(srv, api, stream, t_scale: float = 1.0):
+    """Submit a stream's jobs at their arrival times (scaled by t_scale),
+    wait for all; (latencies in arrival order, site-steps, FIRE stop codes,
+    failures, makespan)."""
+    t0 = time.perf_counter()
+    ids = []
+    for t_arr, s, fire in stream:
+        delay = t_arr * t_scale - (time.perf_counter() - t0)
+        if delay > 0:
+            time.sleep(delay)
+        if fire:
+            ids.append(srv.submit(s, api.JOB_FIRE, 5000, 0.001, 0.0, 1e-6))
+        else:
+            ids.append(srv.submit(s, api.JOB_NVE, 2000, 0.001))
+    lat, site_steps, codes, failed = [], 0.0, {}, {}
+    for j, (t_arr, s, fire) in zip(ids, stream):
+        rc = srv.wait(j)
+        if rc != 0:
+            msg = srv.last_error()
+            failed[msg] = failed.get(msg, 0) + 1
+            lat.append(srv.times(j)[2])
+            continue
+        _, _, _, _, _, it, code, times = srv.result(j)
+        lat.append(times[2])
+        site_steps += s.nsites * it
+        if fire:
+            codes[str(code)] = codes.get(str(code), 0) + 1
+        srv.release(j)
+    return lat, site_steps, codes, failed, time.perf_counter() - t0
+
+
 def serve_arm(args, rank: int = 0, local: int = 0, ws: int = 1, dist=None):
-    """Serve a Poisson stream of jobs; report throughput, latency percentiles
-    and the same jobs run one after another in FP64 through the single-system
-    engine (on a bounded prefix of the stream).  NVE jobs run as restarted
-    trajectories of --segment steps (the reference's dynamics heat up without
-    bound on longer runs)."""
+    """Serve a Poisson stream of jobs at the offered rate (50 jobs/s per GPU);
+    report throughput, latency percentiles and the same jobs run one after
+    another in FP64 through the single-system engine (on a bounded prefix of
+    the stream).  The offered run measures the server's capacity when the
+    offered rate exceeds it (saturated: the queue then grows with the stream
+    and latencies measure its drain); a second stream at 70 % of that
+    capacity gives the steady-state latencies, with the percentiles of its
+    first and second halves (by arrival) to show they do not grow.  NVE jobs
+    run as restarted trajectories of --segment steps (the reference's
+    dynamics heat up without bound on longer runs)."""
     import numpy as np
     from cac_b200 import api, gen, shard
     stream = serve_jobs(args.jobs, 101, rank, ws)
@@ -772,37 +808,38 @@ def serve_arm(args, rank: int = 0, local: int = 0, ws: int = 1, dist=None):
     srv.start()
     if dist:
         dist.barrier()
-    t0 = time.perf_counter()
-    ids = []
-    for t_arr, s, fire in stream:
-        delay = t_arr - (time.perf_counter() - t0)
-        if delay > 0:
-            time.sleep(delay)
-        if fire:
-            ids.append(srv.submit(s, api.JOB_FIRE, 5000, 0.001, 0.0, 1e-6))
-        else:
-            ids.append(srv.submit(s, api.JOB_NVE, 2000, 0.001))
-    lat, site_steps, codes, failed = [], 0.0, {}, {}
-    for j, (t_arr, s, fire) in zip(ids, stream):
-        rc = srv.wait(j)
-        if rc != 0:
-            msg = srv.last_error()
-            failed[msg] = failed.get(msg, 0) + 1
-            lat.append(srv.times(j)[2])
-            continue
-        _, _, _, _, _, it, code, times = srv.result(j)
-        lat.append(times[2])
-        site_steps += s.nsites * it
-        if fire:
-            codes[str(code)] = codes.get(str(code), 0) + 1
-        srv.release(j)
-    makespan = time.perf_counter() - t0
-    srv.close()
+    lat, site_steps, codes, failed, makespan = serve_stream(srv, api, stream)
     parts = shard.gather_objects({"lat": lat, "site_steps": site_steps, "codes": codes, "failed": failed,
                                   "makespan": makespan, "jobs": len(stream)}, dist)
     njobs = sum(p["jobs"] for p in parts)
     lat, site_steps, codes, failed, makespan = merge_serving(parts)
     lat = np.array(lat)
+    # capacity and saturation: the offered rate against the rate jobs were served
+    offered = 50.0 * ws
+    served = njobs / makespan
+    saturated = offered > 1.05 * served
+    # steady state: a second stream (its own seed) at 70 % of the capacity
+    steady = None
+    if args.steady_jobs > 0:
+        srate = min(offered, 0.7 * served)
+        sstream = serve_jobs(args.steady_jobs, 202, rank, ws)
+        slat, ssteps, scodes, sfailed, smake = serve_stream(srv, api, sstream, t_scale=offered / srate)
+        sparts = shard.gather_objects({"lat": slat, "site_steps": ssteps, "codes": scodes, "failed": sfailed,
+                                       "makespan": smake, "jobs": len(sstream)}, dist)
+        snj = sum(p["jobs"] for p in sparts)
+        slat_all, ssteps, scodes, sfailed, smake = merge_serving(sparts)
+        slat_all = np.array(slat_all)
+        half = len(slat_all) // 2
+        steady = {"arrival_rate_jobs_per_s": srate, "jobs": snj, "jobs_per_s": snj / smake,
+                  "latency_p50_s": float(np.percentile(slat_all, 50)),
+                  "latency_p99_s": float(np.percentile(slat_all, 99)),
+                  "first_half_p50_s": float(np.percentile(slat_all[:half], 50)),
+                  "second_half_p50_s": float(np.percentile(slat_all[half:], 50)),
+                  "first_half_p99_s": float(np.percentile(slat_all[:half], 99)),
+                  "second_half_p99_s": float(np.percentile(slat_all[half:], 99)),
+                  "fire_stop_codes": scodes, "failed": sfailed,
+                  "value": ssteps / smake}
+    srv.close()
     if rank != 0:
         return
 
@@ -844,7 +881,12 @@ def serve_arm(args, rank: int = 0, local: int = 0, ws: int = 1, dist=None):
                    "mix": "70% FIRE (ftol 1e-6 max-norm, cap 5000), 30% NVE 2000 steps "
                           f"(restarted every {args.segment})",
                    "workers": args.workers, "budget_gb": 120.0, "precision": args.form},
-        "serving": {"jobs_per_s": njobs / makespan, "makespan_s": makespan,
+        "serving": {"offered_jobs_per_s": offered, "saturated": bool(saturated),
+                    "capacity_note": ("the offered rate exceeds the server's: jobs queue up and the latencies "
+                                      "measure the drain of the stream" if saturated else
+                                      "the server keeps up with the offered rate"),
+                    "steady": steady,
+                    "jobs_per_s": njobs / makespan, "makespan_s": makespan,
                     "latency_p50_s": float(np.percentile(lat, 50)),
                     "latency_p99_s": float(np.percentile(lat, 99)), "fire_stop_codes": codes,
                     "failed": failed,
@@ -875,6 +917,8 @@ def main():
                     help="integrate with fix langevin or fix deform besides fix nve")
     ap.add_argument("--jobs", type=int, default=64, help="serve workload: jobs in the stream")
     ap.add_argument("--workers", type=int, default=8, help="serve workload: worker contexts")
+    ap.add_argument("--steady-jobs", type=int, default=48,
+                    help="serve workload: jobs of the second stream, at 70 %% of the measured capacity")
     ap.add_argument("--serial-jobs", type=int, default=8,
                     help="serve workload: jobs of the stream timed one at a time in FP64")
     ap.add_argument("--pair", default="lj", choices=["lj", "eam"], help="serve workload: pair style")
