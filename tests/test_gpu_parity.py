@@ -41,6 +41,22 @@ def test_lists_bit_exact_vs_reference(case, golden, tmp_path):
 
 
 @pytest.mark.parametrize("case", ["tiny_lj", "tiny_eam", "lj_small"])
+def test_full_list_built_alone_bit_exact_vs_reference(case, golden, tmp_path):
+    """The full list of a build that makes no half list (the build the step
+    loop runs) equals the reference's."""
+    g = golden(case)
+    build, pair, _ = CASES[case]
+    s = build()
+    e = make_engine(s, pair, tmp_path)
+    e.build_lists(half=False)
+    rows = e.neighbor_list(False)
+    nsites = s.natoms + 8 * s.nelements
+    assert np.array_equal(counts(rows, nsites), g["full_counts"])
+    assert digest(rows) == str(g["full_digest"])
+    e.close()
+
+
+@pytest.mark.parametrize("case", ["tiny_lj", "tiny_eam", "lj_small"])
 def test_forces_energy_vs_reference(case, golden, tmp_path):
     g = golden(case)
     build, pair, _ = CASES[case]

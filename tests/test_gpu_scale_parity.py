@@ -122,8 +122,13 @@ def test_strained_lists_bit_exact_vs_reference(strained):
     s, work, ref = strained
     assert s.natoms + 8 * s.nelements == 313120
     e = engine(s, work)
-    e.build_lists(half=True)
     nsites = s.natoms + 8 * s.nelements
+    # the full list of the step loop's build (no half list), then both
+    e.build_lists(half=False)
+    rows = e.neighbor_list(False)
+    assert np.array_equal(rows, ref["full"])
+    del rows
+    e.build_lists(half=True)
     for half, key in ((True, "half"), (False, "full")):
         rows = e.neighbor_list(half)
         assert np.array_equal(counts(rows, nsites), counts(ref[key], nsites)), key
