@@ -92,6 +92,7 @@ SIGNATURES = [
     ("cacb200_server_destroy", C.c_int, [C.c_void_p]),
     ("cacb200_graph_launches", C.c_int, [C.c_void_p, C.POINTER(C.c_longlong)]),
     ("cacb200_pair_blocks", C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    ("cacb200_work_queue", C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int)]),
     ("cacb200_set_state", C.c_int, [C.c_void_p, _dp, _dp, _dp, _dp]),
     ("cacb200_get_state", C.c_int, [C.c_void_p, _dp, _dp, _dp, _dp]),
     ("cacb200_get_forces", C.c_int, [C.c_void_p, _dp, _dp, _dp]),
@@ -308,6 +309,14 @@ class Engine:
         r, f = C.c_int(), C.c_int()
         self._check(self.lib.cacb200_pair_blocks(self.h, C.byref(r), C.byref(f)), "pair_blocks")
         return r.value, f.value
+
+    def work_queue(self, enable=None):
+        """Batches (mixed form): turn the persistent work-queue launches on or
+        off (None: unchanged); returns the tiles chosen per size class."""
+        t = (C.c_int * 3)()
+        self._check(self.lib.cacb200_work_queue(self.h, -1 if enable is None else int(bool(enable)), t),
+                    "work_queue")
+        return list(t)
 
     def graph_launches(self) -> int:
         n = C.c_longlong()

@@ -825,6 +825,17 @@ int cacb200_pair_blocks(cacb200_ctx *ctx, int *rho_threads, int *force_threads) 
   API_END
 }
 
+int cacb200_work_queue(cacb200_ctx *ctx, int enable, int tiles[3]) {
+  API_BEGIN
+  if (enable >= 0) {
+    c.work_queue = enable != 0;
+    c.work_gen = -1;
+  }
+  if (tiles)
+    for (int k = 0; k < 3; k++) tiles[k] = c.work_tile[k];
+  API_END
+}
+
 int cacb200_graph_launches(cacb200_ctx *ctx, long long *count) {
   API_BEGIN
   if (count) *count = c.graph_launches;

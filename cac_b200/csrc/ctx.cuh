@@ -320,6 +320,16 @@ struct Ctx {
   // tune_gen == gen); FP64 and mixed forms
   long tune_gen = -1, tune_gen32 = -1;
   int tb_rho = 128, tb_force = 128, tb_rho32 = 128, tb_force32 = 128;
+  // batches, mixed form: persistent work-queue launches of the EAM passes.
+  // Items are runs of consecutive list slots of one replica, the largest
+  // replicas first; the run length (tile) is chosen per replica size class
+  // (i-sites < 8192, < 32768, larger) by timing when the plan changes.
+  bool work_queue = true;
+  DBuf<int2> work_items;
+  DBuf<int> work_counter;
+  int nwork_items = 0;
+  long work_gen = -1;
+  int work_tile[3] = {0, 0, 0};
   double escale_node_last = 0.0;   // node energy scale of the last evaluation
   DBuf<int> rep_meta;              // [4][nrep] aoff, na, eoff, ne (per-replica energy)
   DBuf<double> rep_energy;         // [nrep]

@@ -319,11 +319,10 @@ __device__ __forceinline__ float fp32_of(const Eam32 &T, float rho, float *phi) 
   return fp;
 }
 
-template <int TB>
-__global__ void __launch_bounds__(TB, 1024 / TB) k_eam_rho32(Args32 A, Eam32 T, double *rho_out, double *phi_site,
-                                                      int4 *pos_w) {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;   // list slot
-  if (t >= A.nsi) return;
+// One list slot of the density pass: rho at the site, then F' into its
+// record (and F into phi_site for energies).
+__device__ __forceinline__ void rho32_slot(const Args32 &A, const Eam32 &T, int t, double *rho_out,
+                                           double *phi_site, int4 *pos_w) {
   const int i = site_of_slot(A, t);                       // site-table index
   int4 oi;
   site_frame(A, t, oi);
@@ -352,6 +351,39 @@ __global__ void __launch_bounds__(TB, 1024 / TB) k_eam_rho32(Args32 A, Eam32 T, 
   if (A.eflag) phi_site[i] = phi;
 }
 
+template <int TB>
+__global__ void __launch_bounds__(TB, 1024 / TB) k_eam_rho32(Args32 A, Eam32 T, double *rho_out, double *phi_site,
+                                                      int4 *pos_w) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;   // list slot
+  if (t >= A.nsi) return;
+  rho32_slot(A, T, t, rho_out, phi_site, pos_w);
+}
+
+// Persistent work-queue launches for batches: blocks stay resident and take
+// work items one after another from a counter (cleared before the launch);
+// an item is a run of consecutive list slots of one replica (x: first slot,
+// y: count), the largest replicas' items first.  Each slot is computed by
+// the same function as in the grid launch, so results do not change.
+__device__ __forceinline__ int next_item(int *counter) {
+  __shared__ int it;
+  __syncthreads();
+  if (threadIdx.x == 0) it = atomicAdd(counter, 1);
+  __syncthreads();
+  return it;
+}
+
+template <int TB>
+__global__ void __launch_bounds__(TB, 1024 / TB) k_eam_rho32_queue(Args32 A, Eam32 T, double *rho_out,
+                                                            double *phi_site, int4 *pos_w, const int2 *items,
+                                                            int nitems, int *counter) {
+  for (;;) {
+    const int k = next_item(counter);
+    if (k >= nitems) return;
+    const int2 w = items[k];
+    for (int t = w.x + threadIdx.x; t < w.x + w.y; t += TB) rho32_slot(A, T, t, rho_out, phi_site, pos_w);
+  }
+}
+
 __global__ void k_eam_site_fp32(int4 *pos, const int *act_gid, const int *nact_dev, int base, int na,
                                 const double *rho, Eam32 T) {
   const int nact = *nact_dev;
@@ -366,6 +398,55 @@ __global__ void k_eam_site_fp32(int4 *pos, const int *act_gid, const int *nact_d
   }
 }
 
+// One list slot of the force pass: the pair sums of a valid slot (force;
+// energy and virial with EV) and its embedding energy.
+template <bool EV>
+__device__ __forceinline__ void force32_slot(const Args32 &A, const Eam32 &T, int t, int i,
+                                             const double *phi_site, float fi[3], float &esum, float vsum[6],
+                                             double &eemb_site, double &eemb_global) {
+  int4 oi;
+  site_frame(A, t, oi);
+  const float fpi = __int_as_float(oi.w);
+  for_each32(A, t, i, oi, [&](float dx, float dy, float dz, float fpj) {
+    float rsq = dx * dx + dy * dy + dz * dz;
+    if (rsq < T.cutforcesq) {
+      float recip = rsqrtf(rsq);
+      float r = rsq * recip;
+      float p = r * T.rdr + 1.0f;
+      int m = (int)p;
+      m = max(1, min(m, T.nr - 1));
+      p -= (float)m;
+      p = fminf(p, 1.0f);
+      float4 rv, zv;
+      ldg256(T.rz + 2 * m, rv, zv);
+      float rhop = ((3.0f * rv.x * p + 2.0f * rv.y) * p + rv.z) * T.rdr;
+      float z2p = ((3.0f * zv.x * p + 2.0f * zv.y) * p + zv.z) * T.rdr;
+      float z2 = ((zv.x * p + zv.y) * p + zv.z) * p + zv.w;
+      float phi = z2 * recip;
+      float phip = z2p * recip - phi * recip;
+      float psip = (fpi + fpj) * rhop + phip;
+      float fpair = -psip * recip;
+      fi[0] += dx * fpair;
+      fi[1] += dy * fpair;
+      fi[2] += dz * fpair;
+      if (EV) {
+        esum += phi;
+        vsum[0] += dx * dx * fpair;
+        vsum[1] += dy * dy * fpair;
+        vsum[2] += dz * dz * fpair;
+        vsum[3] += dx * dy * fpair;
+        vsum[4] += dx * dz * fpair;
+        vsum[5] += dy * dz * fpair;
+      }
+    }
+  });
+  if (EV && A.eflag) {
+    double phi = phi_site[i];
+    eemb_site = phi;
+    eemb_global = (i < A.na) ? phi : phi * A.escale_node * 2.0;
+  }
+}
+
 template <int TB, bool EV>
 __global__ void __launch_bounds__(TB, (EV ? 512 : 1024) / TB) k_eam_force32(Args32 A, Eam32 T,
                                                                           const double *phi_site) {
@@ -374,50 +455,25 @@ __global__ void __launch_bounds__(TB, (EV ? 512 : 1024) / TB) k_eam_force32(Args
   const int i = valid ? site_of_slot(A, t) : 0;           // site-table index
   float fi[3] = {0, 0, 0}, esum = 0.f, vsum[6] = {0, 0, 0, 0, 0, 0};
   double eemb_site = 0.0, eemb_global = 0.0;
-  if (valid) {
-    int4 oi;
-    site_frame(A, t, oi);
-    const float fpi = __int_as_float(oi.w);
-    for_each32(A, t, i, oi, [&](float dx, float dy, float dz, float fpj) {
-      float rsq = dx * dx + dy * dy + dz * dz;
-      if (rsq < T.cutforcesq) {
-        float recip = rsqrtf(rsq);
-        float r = rsq * recip;
-        float p = r * T.rdr + 1.0f;
-        int m = (int)p;
-        m = max(1, min(m, T.nr - 1));
-        p -= (float)m;
-        p = fminf(p, 1.0f);
-        float4 rv, zv;
-        ldg256(T.rz + 2 * m, rv, zv);
-        float rhop = ((3.0f * rv.x * p + 2.0f * rv.y) * p + rv.z) * T.rdr;
-        float z2p = ((3.0f * zv.x * p + 2.0f * zv.y) * p + zv.z) * T.rdr;
-        float z2 = ((zv.x * p + zv.y) * p + zv.z) * p + zv.w;
-        float phi = z2 * recip;
-        float phip = z2p * recip - phi * recip;
-        float psip = (fpi + fpj) * rhop + phip;
-        float fpair = -psip * recip;
-        fi[0] += dx * fpair;
-        fi[1] += dy * fpair;
-        fi[2] += dz * fpair;
-        if (EV) {
-          esum += phi;
-          vsum[0] += dx * dx * fpair;
-          vsum[1] += dy * dy * fpair;
-          vsum[2] += dz * dz * fpair;
-          vsum[3] += dx * dy * fpair;
-          vsum[4] += dx * dz * fpair;
-          vsum[5] += dy * dz * fpair;
-        }
-      }
-    });
-    if (EV && A.eflag) {
-      double phi = phi_site[i];
-      eemb_site = phi;
-      eemb_global = (i < A.na) ? phi : phi * A.escale_node * 2.0;
+  if (valid) force32_slot<EV>(A, T, t, i, phi_site, fi, esum, vsum, eemb_site, eemb_global);
+  finish32(A, i, valid, fi, EV, esum, vsum, eemb_site, eemb_global);
+}
+
+template <int TB>
+__global__ void __launch_bounds__(TB, 1024 / TB) k_eam_force32_queue(Args32 A, Eam32 T, const double *phi_site,
+                                                              const int2 *items, int nitems, int *counter) {
+  for (;;) {
+    const int k = next_item(counter);
+    if (k >= nitems) return;
+    const int2 w = items[k];
+    for (int t = w.x + threadIdx.x; t < w.x + w.y; t += TB) {
+      const int i = site_of_slot(A, t);
+      float fi[3] = {0, 0, 0}, esum = 0.f, vsum[6] = {0, 0, 0, 0, 0, 0};
+      double eemb_site = 0.0, eemb_global = 0.0;
+      force32_slot<false>(A, T, t, i, phi_site, fi, esum, vsum, eemb_site, eemb_global);
+      finish32(A, i, true, fi, false, esum, vsum, eemb_site, eemb_global);
     }
   }
-  finish32(A, i, valid, fi, EV, esum, vsum, eemb_site, eemb_global);
 }
 
 __global__ void k_reduce_partials32(const double *partial, int nblocks, double *out) {
@@ -473,6 +529,50 @@ void mixed_tables(Ctx &c) {
   conv(c.frho_val, c.frho_val32, c.pp.nrho);
   conv(c.frho_der, c.frho_der32, c.pp.nrho);
 }
+
+namespace {
+
+// size class of a replica by its i-sites
+int size_class(long sites) { return sites < 8192 ? 0 : sites < 32768 ? 1 : 2; }
+
+// Work items of a batch: replicas by i-sites, largest first; each replica's
+// atom slots, then its Gauss-point slots, in runs of its class's tile.
+// only_class >= 0 keeps the items of that class alone (tuning).
+std::vector<int2> make_items(const Ctx &c, const int tile[3], int only_class) {
+  std::vector<int> order(c.nrep);
+  for (int r = 0; r < c.nrep; r++) order[r] = r;
+  auto sites = [&](int r) { return (long)c.rep_na[r] + 8L * c.rep_ne[r]; };
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return sites(a) > sites(b); });
+  std::vector<int2> items;
+  for (int r : order) {
+    const int cl = size_class(sites(r));
+    if (only_class >= 0 && cl != only_class) continue;
+    const int T = tile[cl];
+    const int a0 = c.rep_aoff[r], na = c.rep_na[r];
+    for (int o = 0; o < na; o += T) items.push_back(make_int2(a0 + o, std::min(T, na - o)));
+    const int g0 = c.na + 8 * c.rep_eoff[r], ng = 8 * c.rep_ne[r];
+    for (int o = 0; o < ng; o += T) items.push_back(make_int2(g0 + o, std::min(T, ng - o)));
+  }
+  return items;
+}
+
+int queue_grid(const Ctx &c) {
+  static const int per_sm = [] {
+    int b = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_eam_force32_queue<128>, 128, 0);
+    return b > 0 ? b : 1;
+  }();
+  return per_sm * c.num_sms;
+}
+
+void upload_items(Ctx &c, const std::vector<int2> &items) {
+  c.work_items.reserve(std::max<size_t>(items.size(), 1));
+  if (!items.empty())
+    stream_copy(c, c.work_items.p, items.data(), sizeof(int2) * items.size(), cudaMemcpyHostToDevice);
+  c.nwork_items = (int)items.size();
+}
+
+}  // namespace
 
 void pair_compute_mixed(Ctx &c, int eflag, int vflag) {
   const int nsi = c.nsite_i();
@@ -556,11 +656,64 @@ void pair_compute_mixed(Ctx &c, int eflag, int vflag) {
       else if (tb == 256) k_eam_force32<256, false><<<std::max(nblk(nsi, 256), 1), 256, 0, c.stream>>>(A, Tb, c.phi_site.p);
       else k_eam_force32<128, false><<<nb, 128, 0, c.stream>>>(A, Tb, c.phi_site.p);
     };
-    // block sizes of the force-only passes chosen by timing on first use (as
-    // in the FP64 form; results do not depend on them)
+    // batches: the persistent work-queue launches, their tiles tuned per
+    // replica size class when the plan changes (idempotent trial launches)
     cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
     CACB200_CUDA(cudaStreamIsCapturing(c.stream, &cs));
-    if (c.tune_gen32 != c.gen && !ev && cs == cudaStreamCaptureStatusNone) {
+    bool queue = c.nrep > 1 && c.work_queue;
+    c.work_counter.reserve(2);
+    auto rho_q = [&] {
+      CACB200_CUDA(cudaMemsetAsync(c.work_counter.p, 0, sizeof(int), c.stream));
+      k_eam_rho32_queue<128><<<queue_grid(c), 128, 0, c.stream>>>(A, Tb, c.rho.p, c.phi_site.p, c.pos32.p,
+                                                                 c.work_items.p, c.nwork_items, c.work_counter.p);
+    };
+    auto force_q = [&] {
+      CACB200_CUDA(cudaMemsetAsync(c.work_counter.p + 1, 0, sizeof(int), c.stream));
+      k_eam_force32_queue<128><<<queue_grid(c), 128, 0, c.stream>>>(A, Tb, c.phi_site.p, c.work_items.p,
+                                                                   c.nwork_items, c.work_counter.p + 1);
+    };
+    if (queue && c.work_gen != c.gen && cs == cudaStreamCaptureStatusNone) {
+      const int cand[3] = {512, 128, 2048};   // another tile replaces 512 only when >= 3 % faster
+      int tile[3] = {512, 512, 512};
+      {
+        // phase: densities and F' first, so the trial force passes read the step's F'
+        upload_items(c, make_items(c, tile, -1));
+        rho_q();
+        site_fp();
+        cudaEvent_t e0, e1;
+        CACB200_CUDA(cudaEventCreate(&e0));
+        CACB200_CUDA(cudaEventCreate(&e1));
+        for (int cl = 0; cl < 3; cl++) {
+          float best = 1e30f;
+          for (int T : cand) {
+            int trial[3] = {T, T, T};
+            upload_items(c, make_items(c, trial, cl));
+            if (c.nwork_items == 0) break;
+            float ms = 1e30f;
+            for (int rep = 0; rep < 3; rep++) {
+              CACB200_CUDA(cudaEventRecord(e0, c.stream));
+              force_q();
+              CACB200_CUDA(cudaEventRecord(e1, c.stream));
+              CACB200_CUDA(cudaEventSynchronize(e1));
+              float m = 0.f;
+              CACB200_CUDA(cudaEventElapsedTime(&m, e0, e1));
+              ms = std::min(ms, m);
+            }
+            if (T == 512 || ms < 0.97f * best) best = ms, tile[cl] = T;
+          }
+        }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+      }
+      for (int cl = 0; cl < 3; cl++) c.work_tile[cl] = tile[cl];
+      upload_items(c, make_items(c, tile, -1));
+      c.work_gen = c.gen;
+    }
+    // items are made outside stream capture; until then the grid launches
+    if (queue && c.work_gen != c.gen) queue = false;
+    // block sizes of the force-only passes chosen by timing on first use (as
+    // in the FP64 form; results do not depend on them)
+    if (!queue && c.tune_gen32 != c.gen && !ev && cs == cudaStreamCaptureStatusNone) {
       const int cand[3] = {128, 64, 256};   // another size replaces 128 only when >= 3 % faster
       cudaEvent_t e0, e1;
       CACB200_CUDA(cudaEventCreate(&e0));
@@ -596,7 +749,8 @@ void pair_compute_mixed(Ctx &c, int eflag, int vflag) {
     }
     {
       KernelTimer t(c, "eam_rho32");
-      rho(c.tb_rho32);
+      if (queue) rho_q();
+      else rho(c.tb_rho32);
     }
     if (c.ne) {
       KernelTimer t(c, "eam_site_fp32");
@@ -605,6 +759,7 @@ void pair_compute_mixed(Ctx &c, int eflag, int vflag) {
     {
       KernelTimer t(c, "eam_force32");
       if (ev) k_eam_force32<128, true><<<nb, T, 0, c.stream>>>(A, Tb, c.phi_site.p);
+      else if (queue) force_q();
       else force(c.tb_force32);
     }
   }

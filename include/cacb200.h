@@ -416,6 +416,17 @@ int cacb200_graph_launches(cacb200_ctx *ctx, long long *count);
  * context's own lists the first time they run (results do not depend on the
  * choice); 128 before that.  No reference counterpart. */
 int cacb200_pair_blocks(cacb200_ctx *ctx, int *rho_threads, int *force_threads);
+/* Batches in the mixed form run the EAM passes as persistent work-queue
+ * launches: resident blocks take items (a run of consecutive list slots of
+ * one replica, the largest replicas first) from a counter, so one launch
+ * serves replicas of every size without idle tails.  The run length (tile:
+ * 128, 512 or 2048 slots) is chosen per replica size class (i-sites below
+ * 8,192, below 32,768, larger) by timing the force pass when the capacity
+ * plan changes; results do not depend on it (each slot's arithmetic is that
+ * of the grid launch).  enable: 1 on (default), 0 off (one grid launch per
+ * pass), -1 unchanged; tiles [3] gets the chosen tiles (0: not chosen yet).
+ * No reference counterpart (the reference runs one system per process). */
+int cacb200_work_queue(cacb200_ctx *ctx, int enable, int tiles[3]);
 
 /* Kernel timing: when enabled, every launch is bracketed by CUDA events and
  * per-kernel totals accumulate (ms, launches) until reset. */

@@ -101,3 +101,31 @@ def test_batch_rejects_half_lists(tmp_path):
     with pytest.raises(CacB200Error):
         b.build_lists(half=True)
     b.close()
+
+
+def test_work_queue_launches_equal_grid_launches(tmp_path):
+    """Mixed-form batches run the EAM passes as persistent work-queue
+    launches with per-size-class tiles; the forces equal those of the grid
+    launches bit for bit (every slot's arithmetic is the same), over steps
+    with a rebuild and after the tiles were tuned."""
+    from cac_b200.api import MIXED, Engine
+    reps = gen.replica_set(12, seed=31, atoms=(600, 40000), elements=(20, 900))
+    out = []
+    for on in (True, False):
+        e = Engine(0)
+        e.upload_batch(reps)
+        e.pair_eam(setfl_path(tmp_path))
+        e.set_precision(MIXED)
+        e.neighbor(1.0, 10)
+        tiles = e.work_queue(on)
+        e.setup()
+        e.run_nve(12, 0.001)
+        f, nf, gf = e.forces()
+        x = e.state()[0]
+        tiles = e.work_queue()
+        out.append((f, gf, x, tiles))
+        e.close()
+    (f1, g1, x1, t1), (f0, g0, x0, t0) = out
+    assert all(t in (128, 512, 2048) for t in t1 if t)
+    assert any(t1)
+    assert np.array_equal(f1, f0) and np.array_equal(g1, g0) and np.array_equal(x1, x0)
