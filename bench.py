@@ -591,6 +591,7 @@ def b200_arm(args, rank, local, ws, dist):
                 "peak_kind": "measured here: cuBLAS " + ("DGEMM" if fp64 else "SGEMM, TF32 off"),
                 "flops_per_site": alg_flops_per_site(dom[0])}
     tuned = eng.pair_blocks()
+    work_tiles = eng.work_queue() if batch else None
     eng.restore()
     eng.setup()
 
@@ -691,6 +692,8 @@ def b200_arm(args, rank, local, ws, dist):
                     "d2h_bytes_per_step": bytes_state, "steps": k_e2e},
             "gpu_launches": int(round(launches_per_step * args.steps)),
             "tuned_blocks": dict(zip(("rho", "force"), tuned)),
+            "work_queue_tiles": (dict(zip(("below_8192_sites", "below_32768_sites", "larger"), work_tiles))
+                                 if work_tiles else None),
             "thermo_readout_ms": thermo_ms,
             "clocks": clocks,
         }
