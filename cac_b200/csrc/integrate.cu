@@ -52,9 +52,12 @@ __global__ void k_pair_table(const double4 *xs, double4 *xss, const int *slot_at
 // nodef[a] += sum_b Minv[a][b] fc[b] with the Hex inverse mass matrix
 // (element.cpp:1784-1850, the tensor product of [[4,-2],[-2,4]]).  With the
 // Gauss points on the nodes, wsa[g][n] = 1/8 when g sits on n, else 0; the
-// loops keep the reference's order of terms.  One thread per element.
+// loops keep the reference's order of terms.  One thread per (element,
+// node): the element's 8 threads read its 24 Gauss-point components
+// together and each writes its node's force.
 __global__ void k_assemble(const double *gaussf, double *nodef, int ne) {
-  int e = blockIdx.x * blockDim.x + threadIdx.x;
+  const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  const int e = (int)(t >> 3), a = (int)(t & 7);
   if (e >= ne) return;
   const double weight = (double)NU / (1.0 * 8) * 1.0;   // UNIFORM node weight
   const double *gf = gaussf + (size_t)e * 24;
@@ -72,20 +75,17 @@ __global__ void k_assemble(const double *gaussf, double *nodef, int ne) {
     }
   }
   double *nf = nodef + (size_t)e * 24;
+  double acc[3] = {0.0, 0.0, 0.0};
 #pragma unroll
-  for (int a = 0; a < NPE; a++) {
-    double acc[3] = {0.0, 0.0, 0.0};
+  for (int b = 0; b < NPE; b++) {
+    double m = (node_xi(a) == node_xi(b) ? 4.0 : -2.0) * (node_eta(a) == node_eta(b) ? 4.0 : -2.0) *
+               (node_zeta(a) == node_zeta(b) ? 4.0 : -2.0);
 #pragma unroll
-    for (int b = 0; b < NPE; b++) {
-      double m = (node_xi(a) == node_xi(b) ? 4.0 : -2.0) * (node_eta(a) == node_eta(b) ? 4.0 : -2.0) *
-                 (node_zeta(a) == node_zeta(b) ? 4.0 : -2.0);
-#pragma unroll
-      for (int d = 0; d < 3; d++) acc[d] += m * fc[b][d];
-    }
-    nf[3 * a] = acc[0];
-    nf[3 * a + 1] = acc[1];
-    nf[3 * a + 2] = acc[2];
+    for (int d = 0; d < 3; d++) acc[d] += m * fc[b][d];
   }
+  nf[3 * a] = acc[0];
+  nf[3 * a + 1] = acc[1];
+  nf[3 * a + 2] = acc[2];
 }
 
 // FixNVE::initial_integrate (fix_nve.cpp:62-145): half kick and drift for
@@ -158,7 +158,7 @@ void interpolate_sites(Ctx &c) {
 void assemble_nodef(Ctx &c) {
   if (c.ne == 0) return;
   KernelTimer t(c, "assemble");
-  k_assemble<<<nblk(c.ne, 128), 128, 0, c.stream>>>(c.gaussf.p, c.nodef.p, c.ne);
+  k_assemble<<<nblk(8L * c.ne, 128), 128, 0, c.stream>>>(c.gaussf.p, c.nodef.p, c.ne);
 }
 
 void nve_initial(Ctx &c, double dt) {
