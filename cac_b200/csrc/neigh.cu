@@ -1667,6 +1667,7 @@ void neigh_build_async(Ctx &c, bool want_half) {
   c.lists_valid = true;
   c.nact_known = false;
   c.build_count++;
+  build_windows(c);
   CACB200_CUDA(cudaGetLastError());
 }
 
