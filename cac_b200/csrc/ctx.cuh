@@ -271,7 +271,8 @@ struct Ctx {
   // num_full - num_in entries rows [cap - (num_full - num_in), cap); the two
   // segments meet only when a list overflows (then the build is repeated)
   DBuf<int> nbr_full, num_full;
-  DBuf<int2> site_from;          // per slot: rows of each segment before its element-site entries
+  DBuf<int2> site_from;
+  DBuf<unsigned char> ecell_near;   // single systems: element cells with an element in their 27-cell block          // per slot: rows of each segment before its element-site entries
   // inner prefix of the full lists: inner_ok[replica] (device) is nonzero
   // while no site of the replica has moved inner_limit() since the build
   // (positions in xbuild / nodex_build), and the pair loops then stop at num_in

@@ -249,6 +249,24 @@ __global__ void k_elem_keys(const double4 *ecenter, int ne, RP P, int *key, int 
   idx[e] = e;
 }
 
+// near[c]: some element cell of the 27-cell block around element cell c (a
+// single system's grid, periodic) holds an element
+__global__ void k_ecell_near(const int *start, Grid g, unsigned char *near) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= g.ncell) return;
+  const int cx = c % g.nc[0], cy = (c / g.nc[0]) % g.nc[1], cz = c / (g.nc[0] * g.nc[1]);
+  bool any = false;
+  for (int oz = -1; oz <= 1 && !any; oz++)
+    for (int oy = -1; oy <= 1 && !any; oy++)
+      for (int ox = -1; ox <= 1 && !any; ox++) {
+        const int x = (cx + ox + g.nc[0]) % g.nc[0], y = (cy + oy + g.nc[1]) % g.nc[1],
+                  z = (cz + oz + g.nc[2]) % g.nc[2];
+        const int k = (z * g.nc[1] + y) * g.nc[0] + x;
+        any = start[k + 1] > start[k];
+      }
+  near[c] = any ? 1 : 0;
+}
+
 // cell_start[c] = first sorted position with key >= c, for c in [0, ncell]
 // (lower bound by binary search, one thread per cell)
 __global__ void k_cell_start(const int *skey, int n, int ncell, int *start) {
@@ -286,6 +304,7 @@ struct BuildArgs {
   const double4 *acell_pos;
   const float4 *acell_pos32;  // wrapped positions as floats, w = atom index bits
   const int *ecell_start;
+  const unsigned char *ecell_near;   // single systems: element cell has an element in its 27-cell block (else null)
   const int *ecell_elems;
   const int *atom_of_slot;    // list slot (cell-sorted position) -> atom index
   int *site_flag;             // [ne * 729] marks the lattice sites some full list references
@@ -481,6 +500,8 @@ __device__ int element_items(const BuildArgs &A, const Query &q, int2 *out, int 
 #pragma unroll
   for (int d = 0; d < 3; d++)
     ci[d] = min(max((int)((q.wi[d] - q.r.b.lo[d]) * eg.inv[d]), 0), eg.nc[d] - 1);
+  // no element in the 27 cells around: nothing to walk
+  if (A.ecell_near && !A.ecell_near[q.r.ebase + (ci[2] * eg.nc[1] + ci[1]) * eg.nc[0] + ci[0]]) return 0;
   int n = 0;
   for (int oz = -1; oz <= 1; oz++) {
     int cz, Wz;
@@ -1438,6 +1459,7 @@ void neigh_plan(Ctx &c, bool want_half) {
   c.acell_pos.reserve(std::max(c.na, 1));
   c.acell_pos32.reserve(std::max(c.na, 1));
   c.ecell_start.reserve(c.egrid.ncell + 1);
+  c.ecell_near.reserve(c.egrid.ncell + 1);
   c.ecell_elems.reserve(std::max(c.ne, 1));
   size_t slots = (size_t)c.cap * std::max(nsi, 1);
   c.raw_full.reserve(slots);
@@ -1558,6 +1580,9 @@ void neigh_build_async(Ctx &c, bool want_half) {
                                                      c.stream));
         k_cell_start<<<nblk(c.egrid.ncell + 1, 256), 256, 0, c.stream>>>(c.cell_key2.p, c.ne, c.egrid.ncell,
                                                                         c.ecell_start.p);
+        if (c.nrep == 1)
+          k_ecell_near<<<nblk(c.egrid.ncell, 256), 256, 0, c.stream>>>(c.ecell_start.p, c.rep_h[0].eg,
+                                                                       c.ecell_near.p);
       } else {
         CACB200_CUDA(cudaMemsetAsync(c.ecell_start.p, 0, sizeof(int) * (c.egrid.ncell + 1), c.stream));
       }
@@ -1571,6 +1596,7 @@ void neigh_build_async(Ctx &c, bool want_half) {
     A.acell_pos = c.acell_pos.p;
     A.acell_pos32 = c.acell_pos32.p;
     A.ecell_start = c.ecell_start.p;
+    A.ecell_near = (c.nrep == 1 && c.ne) ? c.ecell_near.p : nullptr;
     A.ecell_elems = c.ecell_elems.p;
     A.atom_of_slot = c.slot_atom.p;
     A.site_flag = c.site_flag.p;
