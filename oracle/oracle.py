@@ -609,7 +609,7 @@ def read_neigh_binary(path: str) -> np.ndarray:
     return a[order]
 
 
-def run_reference(workdir: str, script: str, exe: str = REF_EXE, timeout: float = 3600.0) -> str:
+def run_reference(workdir: str, script: str, exe: str = REF_EXE, timeout: float = 900.0) -> str:
     """Run the reference executable on ``script`` (a file in ``workdir``)."""
     r = subprocess.run([exe, "-in", script], cwd=workdir, capture_output=True, text=True,
                        timeout=timeout)

@@ -193,7 +193,7 @@ def reference_log(tmp_path, case, body, exe):
     plain = ("pair_style lj/cut 5.5\npair_coeff 1 1 0.4093 2.338\n" if pair == "lj"
              else "pair_style eam/alloy\npair_coeff * * cu.setfl Cu\n")
     (work / "in.cac").write_text(HEADER + plain + TAIL + body)
-    return oracle.run_reference(str(work), "in.cac", exe=exe)
+    return oracle.run_reference(str(work), "in.cac", exe=exe, timeout=600)
 
 
 def assert_thermo_rows(ours, ref, O):
@@ -341,17 +341,19 @@ def test_verlet_b200_dumps_with_device_peratom_computes(case, tmp_path):
     reference's `run` under run_style verlet/b200 with compute pe/atom/b200
     and stress/atom/b200: the dump files equal the reference's own run with
     compute pe/atom and stress/atom at the dump's print precision, and the
-    device run copies the state only at the two dump steps inside it."""
+    device run copies the state only at the two dump steps inside it.  The
+    reference side runs cac_eamfix for both pair styles: the stock
+    ComputePEAtom never returns on a system with elements (its clear loop of
+    node_energy reuses the inner loop's variable in the outer loop,
+    compute_pe_atom.cpp:130), and that executable carries the one-line fix."""
     import oracle as O
-    pair = CASES[case][1]
     dump = ("dump 1 all custom 10 d.* id type x y z fx fy fz c_pa c_sa[1] c_sa[2] c_sa[3] c_sa[4] "
             "c_sa[5] c_sa[6]\n")
     ours_deck = ("compute pa all pe/atom/b200\ncompute sa all stress/atom/b200 NULL\n" + dump + THERMO +
                  "run_style verlet/b200\nrun 20\n")
     ref_deck = "compute pa all pe/atom\ncompute sa all stress/atom NULL\n" + dump + THERMO + "run 20\n"
     out = app_log(tmp_path, case, ours_deck)
-    exe = O.REF_EXE_EAMFIX if pair == "eam" else O.REF_EXE
-    reference_log(tmp_path, case, ref_deck, exe)
+    reference_log(tmp_path, case, ref_deck, O.REF_EXE_EAMFIX)
     assert "b200 device run: 20 steps, 2 output steps with a host copy of the state" in out
     for step in (0, 10, 20):
         a = read_dump_frames(str(tmp_path / f"d.{step}"))
