@@ -399,9 +399,6 @@ def pipe_peak(fp64: bool, device: int) -> float:
     return best
 
 
-WINDOWS = False   # --windows: neighbour windows for single systems in the mixed form
-
-
 def make_engine(s, pair, form: str, local: int, setfl: str, fix: str):
     """A context holding the workload, set up at the seeded state (lists,
     forces) and snapshotted for the restarts."""
@@ -417,8 +414,6 @@ def make_engine(s, pair, form: str, local: int, setfl: str, fix: str):
         eng.pair_lj(0.4093, 2.338, 5.5)
     eng.set_precision(api.MIXED if form == "mixed" else api.FP64)
     eng.neighbor(1.0, 10)
-    if WINDOWS and form == "mixed" and not isinstance(s, list):
-        eng.windows(True)
     if fix == "langevin":
         eng.langevin(300.0, 300.0, 0.1, 4928459)
     elif fix == "deform":
@@ -677,8 +672,7 @@ def b200_arm(args, rank, local, ws, dist):
                                        if batch and ws > 1 else f"replicas x{ws} (no data-path collective)"),
                        "fix": {"none": "nve", "langevin": "nve + langevin 300 300 0.1",
                                "deform": "nve + deform 1 x erate 0.1 y volume"}[args.fix],
-                       "l2": "working set larger than L2 (site table + lists > 126 MB)",
-                       "windows": WINDOWS, "atom_build": args.atom_build},
+                       "l2": "working set larger than L2 (site table + lists > 126 MB)"},
             "fp64": fp64_entry,
             "mixed_over_fp64": (value / fp64_entry["value"]) if fp64_entry else None,
             "accuracy": accuracy,
@@ -936,14 +930,7 @@ def main():
     ap.add_argument("--segment", type=int, default=50,
                     help="steps per trajectory from the seeded initial state (the reference's CAC "
                          "dynamics heat up unboundedly after ~100 steps, so long runs restart)")
-    ap.add_argument("--windows", default="off", choices=["on", "off"],
-                    help="mixed form, single systems: neighbour windows in shared memory for the EAM passes")
-    ap.add_argument("--atom-build", default="lanes", choices=["lanes", "pairs"],
-                    help="atom-list build: one lane per atom, or 32 (atom, candidate) pairs per warp step")
     args = ap.parse_args()
-    global WINDOWS
-    WINDOWS = args.windows == "on"
-    os.environ["CACB200_ATOM_BUILD"] = args.atom_build
     rank, local, ws, dist = dist_init()
     try:
         if args.impl == "reference":

@@ -93,7 +93,6 @@ SIGNATURES = [
     ("cacb200_graph_launches", C.c_int, [C.c_void_p, C.POINTER(C.c_longlong)]),
     ("cacb200_pair_blocks", C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     ("cacb200_work_queue", C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int)]),
-    ("cacb200_set_windows", C.c_int, [C.c_void_p, C.c_int]),
     ("cacb200_set_state", C.c_int, [C.c_void_p, _dp, _dp, _dp, _dp]),
     ("cacb200_get_state", C.c_int, [C.c_void_p, _dp, _dp, _dp, _dp]),
     ("cacb200_get_forces", C.c_int, [C.c_void_p, _dp, _dp, _dp]),
@@ -318,11 +317,6 @@ class Engine:
         self._check(self.lib.cacb200_work_queue(self.h, -1 if enable is None else int(bool(enable)), t),
                     "work_queue")
         return list(t)
-
-    def windows(self, enable: bool) -> None:
-        """Single systems, mixed form, EAM: neighbour windows in shared memory
-        for the pair passes (off by default); from the next list build."""
-        self._check(self.lib.cacb200_set_windows(self.h, int(bool(enable))), "set_windows")
 
     def graph_launches(self) -> int:
         n = C.c_longlong()

@@ -825,14 +825,6 @@ int cacb200_pair_blocks(cacb200_ctx *ctx, int *rho_threads, int *force_threads) 
   API_END
 }
 
-int cacb200_set_windows(cacb200_ctx *ctx, int enable) {
-  API_BEGIN
-  c.windows = enable != 0;
-  c.win_for = -1;   // windows come with the next list build
-  c.lists_valid = false;
-  API_END
-}
-
 int cacb200_work_queue(cacb200_ctx *ctx, int enable, int tiles[3]) {
   API_BEGIN
   if (enable >= 0) {

@@ -326,13 +326,6 @@ struct Ctx {
   // replicas first; the run length (tile) is chosen per replica size class
   // (i-sites < 8192, < 32768, larger) by timing when the plan changes.
   bool work_queue = true;
-  // single systems, mixed form, EAM: neighbour windows of each block of 128
-  // list slots (pair32.cu), rebuilt with the lists; win_for is the list
-  // build they belong to
-  bool windows = false;
-  long win_for = -1;
-  DBuf<int> win_keys, win_count;
-  DBuf<unsigned short> nbr16;
   DBuf<int2> work_items;
   DBuf<int> work_counter;
   int nwork_items = 0;
@@ -425,9 +418,6 @@ void pair_compute(Ctx &c, int eflag, int vflag);
 void pair_compute_mixed(Ctx &c, int eflag, int vflag);
 // the mixed form's pair table as fixed-point records (interpolate_sites)
 void pair_table_mixed(Ctx &c);
-// neighbour windows of the lists just built (neigh_build_async), when the
-// context uses them
-void build_windows(Ctx &c);
 void assemble_nodef(Ctx &c);
 void nve_initial(Ctx &c, double dt);
 bool moved_past_trigger(Ctx &c);

@@ -936,179 +936,6 @@ __device__ __forceinline__ void build_atoms_cells(BuildArgs A, RP P, int ncell) 
   }
 }
 
-// Full lists only (no half rule): the same lists from the pairs of the home
-// cell's atoms with each candidate cell's atoms, 32 pairs at a time, pair p
-// = (home atom p / nc, candidate p % nc) for nc candidates, so every lane
-// tests a pair even when the cell holds fewer than 32 atoms.  The per-atom
-// data the lanes share (wrapped FP32 and raw FP64 positions, wrap counts,
-// atom index) and the atoms' entry counts live in shared memory.  An
-// accepted pair goes to its home atom's ring at the atom's count plus its
-// place among the row's accepted pairs in the chunk (ballot), so a list is
-// written in the order of the one-lane-per-atom walk: candidate cells in
-// stencil order, candidates in sorted order.  Same decisions, same
-// arithmetic, same lists bit for bit.
-template <class RP>
-__device__ __forceinline__ void build_atoms_pairs(BuildArgs A, RP P) {
-  const int lane = threadIdx.x & 31;
-  const float fcut2 = (float)A.cutforcesq;
-  __shared__ int st_in[STAGE_ROWS][32], st_out[STAGE_ROWS][32];   // front / back segment rings
-  __shared__ float4 hw[32];        // home atoms: wrapped FP32 position
-  __shared__ double hx[32][3];     // raw FP64 position
-  __shared__ int hti[32][3];       // wrap counts
-  __shared__ int hidx[32];         // atom index
-  __shared__ int hcnt[2][32];      // entries in the front / back segment
-  const int home = blockIdx.x;
-  const int hbeg = A.acell_start[home], hend = A.acell_start[home + 1];
-  if (hbeg == hend) return;
-  const Rep R = P.acell(home);
-  const int local = home - R.abase;
-  const int nc0 = R.ag.nc[0], nc1 = R.ag.nc[1], nc2 = R.ag.nc[2];
-  const int hx0 = local % nc0, hy0 = (local / nc0) % nc1, hz0 = local / (nc0 * nc1);
-  const float pre = (float)A.cutneigh + R.fmargin, sure = (float)A.cutneigh - R.fmargin;
-  const float pre2 = pre * pre, sure2 = sure * sure;
-  for (int base = hbeg; base < hend; base += 32) {
-    const int nh = min(32, hend - base);
-    const bool active = lane < nh;
-    __syncwarp();
-    if (active) {
-      Query q;
-      make_query(A, P, (int)__double_as_longlong(A.acell_pos[base + lane].w), q);
-      hw[lane] = A.acell_pos32[base + lane];
-#pragma unroll
-      for (int d = 0; d < 3; d++) {
-        hx[lane][d] = q.xi[d];
-        hti[lane][d] = q.ti[d];
-      }
-      hidx[lane] = q.i;
-    }
-    hcnt[0][lane] = hcnt[1][lane] = 0;
-    __syncwarp();
-    int fin = 0, fout = 0;   // this lane's home atom: entries already written
-    const int slot = base + lane;
-    auto flush = [&]() {
-      __syncwarp();
-      const int nin = active ? hcnt[0][lane] : 0, nout = active ? hcnt[1][lane] : 0;
-      int lo = __reduce_min_sync(0xffffffffu, active ? fin : 0x7fffffff);
-      int hi = __reduce_max_sync(0xffffffffu, nin);
-      for (int k = lo; k < hi; k++)
-        if (active && k >= fin && k < nin && k < A.cap)
-          A.nbr_full[(size_t)k * A.nsi + slot] = st_in[k & (STAGE_ROWS - 1)][lane];
-      lo = __reduce_min_sync(0xffffffffu, active ? fout : 0x7fffffff);
-      hi = __reduce_max_sync(0xffffffffu, nout);
-      for (int k = lo; k < hi; k++)
-        if (active && k >= fout && k < nout && k < A.cap)
-          A.nbr_full[(size_t)(A.cap - 1 - k) * A.nsi + slot] = st_out[k & (STAGE_ROWS - 1)][lane];
-      fin = nin;
-      fout = nout;
-      __syncwarp();
-    };
-    for (int oz = -1; oz <= 1; oz++) {
-      int cz, Wz;
-      wrap_cell(hz0 + oz, nc2, cz, Wz);
-      for (int oy = -1; oy <= 1; oy++) {
-        int cy, Wy;
-        wrap_cell(hy0 + oy, nc1, cy, Wy);
-        for (int ox = -1; ox <= 1; ox++) {
-          int cx, Wx;
-          wrap_cell(hx0 + ox, nc0, cx, Wx);
-          const int cell = R.abase + (cz * nc1 + cy) * nc0 + cx;
-          const int beg = A.acell_start[cell], nc = A.acell_start[cell + 1] - beg;
-          if (nc == 0) continue;
-          const float sx = (float)(Wx * R.b.L[0]), sy = (float)(Wy * R.b.L[1]), sz = (float)(Wz * R.b.L[2]);
-          const int npairs = nh * nc;
-          const int gain = min(nc, 32);   // entries one atom can gain in one chunk
-          int h = lane / nc, jj = lane - (lane / nc) * nc;
-          for (int p0 = 0; p0 < npairs; p0 += 32) {
-            if (__any_sync(0xffffffffu, active && (hcnt[0][lane] - fin > STAGE_ROWS - gain ||
-                                                   hcnt[1][lane] - fout > STAGE_ROWS - gain)))
-              flush();
-            const bool valid = p0 + lane < npairs;
-            bool acc = false, incut = false;
-            int val = 0;
-            if (valid) {
-              const int ks = beg + jj;
-              const float4 pj = A.acell_pos32[ks];
-              const float4 w = hw[h];
-              const float ex = w.x - (pj.x + sx), ey = w.y - (pj.y + sy), ez = w.z - (pj.z + sz);
-              const float r2 = ex * ex + ey * ey + ez * ez;
-              if (r2 <= pre2) {
-                const int j = __float_as_int(pj.w);
-                const int s0 = Wx - hti[h][0], s1 = Wy - hti[h][1], s2 = Wz - hti[h][2];
-                const bool zero = (s0 == 0 && s1 == 0 && s2 == 0);
-                const bool far = s0 < -1 || s0 > 1 || s1 < -1 || s1 > 1 || s2 < -1 || s2 > 1;
-                if (r2 < sure2) {
-                  if (!(zero && j == hidx[h])) {
-                    if (far) {
-                      atomicExch(&A.overflow[2], 1);
-                    } else {
-                      acc = true;
-                      incut = r2 < fcut2;
-                      val = (ks << IMG_BITS) | img_code(s0, s1, s2);
-                    }
-                  }
-                } else if (!(zero && j == hidx[h])) {
-                  // the exact test of try_atom, in the same operations
-                  const double4 xj = A.xs[j];
-                  double qq[3] = {xj.x, xj.y, xj.z};
-                  if (!zero) {
-                    qq[0] = s0 ? __dadd_rn(qq[0], s0 * R.b.L[0]) : qq[0];
-                    qq[1] = s1 ? __dadd_rn(qq[1], s1 * R.b.L[1]) : qq[1];
-                    qq[2] = s2 ? __dadd_rn(qq[2], s2 * R.b.L[2]) : qq[2];
-                  }
-                  const double rsq = rsq_rn(__dsub_rn(hx[h][0], qq[0]), __dsub_rn(hx[h][1], qq[1]),
-                                            __dsub_rn(hx[h][2], qq[2]));
-                  if (rsq <= A.cutneighsq) {
-                    if (far) {
-                      atomicExch(&A.overflow[2], 1);
-                    } else {
-                      acc = true;
-                      incut = rsq < A.cutforcesq;
-                      val = (ks << IMG_BITS) | img_code(s0, s1, s2);
-                    }
-                  }
-                }
-              }
-            }
-            // the lanes of row h in this chunk: [lo_l, hi_l)
-            const int lo_l = max(h * nc - p0, 0), hi_l = min((h + 1) * nc - p0, 32);
-            const unsigned rowmask =
-                (hi_l >= 32 ? 0xffffffffu : ((1u << hi_l) - 1u)) & ~((lo_l <= 0) ? 0u : ((1u << lo_l) - 1u));
-            const unsigned m_in = __ballot_sync(0xffffffffu, acc && incut);
-            const unsigned m_out = __ballot_sync(0xffffffffu, acc && !incut);
-            if (acc) {
-              const unsigned mm = (incut ? m_in : m_out) & rowmask & lanemask_lt();
-              const int at = hcnt[incut ? 0 : 1][h] + __popc(mm);
-              if (incut) st_in[at & (STAGE_ROWS - 1)][h] = val;
-              else st_out[at & (STAGE_ROWS - 1)][h] = val;
-            }
-            __syncwarp();
-            if (valid && lane == hi_l - 1) {   // the row's last lane in the chunk
-              hcnt[0][h] += __popc(m_in & rowmask);
-              hcnt[1][h] += __popc(m_out & rowmask);
-            }
-            __syncwarp();
-            // next chunk: 32 pairs further
-            jj += 32;
-            while (jj >= nc) {
-              jj -= nc;
-              h++;
-            }
-          }
-        }
-      }
-    }
-    flush();
-    if (active) {
-      const int nin = hcnt[0][lane], nout = hcnt[1][lane];
-      A.site_from[slot] = make_int2(nin, nout);
-      finish_counts(A, slot, nin, nout, 0);
-    }
-  }
-}
-
-__global__ void __launch_bounds__(32) k_build_atoms_pairs(BuildArgs A, OneRep P) { build_atoms_pairs(A, P); }
-__global__ void __launch_bounds__(32) k_build_atoms_pairs(BuildArgs A, ManyRep P) { build_atoms_pairs(A, P); }
-
 // The single-system form as the compiler allocates it (64 registers); the
 // batch form capped at 64 registers (from 80, a few bytes spilled) so that
 // 32 warps instead of 24 are resident per SM: 10 % faster on a 64-replica
@@ -1647,14 +1474,7 @@ void neigh_build_async(Ctx &c, bool want_half) {
     }
     if (c.na) {
       KernelTimer t(c, "build_atoms");
-      // the one-lane-per-atom walk; the pair-chunk form for full lists
-      // when CACB200_ATOM_BUILD=pairs (the same lists)
-      static const bool pairs = [] {
-        const char *e = std::getenv("CACB200_ATOM_BUILD");
-        return e && std::strcmp(e, "pairs") == 0;
-      }();
-      if (want_half || !pairs) k_build_atoms<<<c.agrid.ncell, 32, 0, c.stream>>>(A, P, c.agrid.ncell);
-      else k_build_atoms_pairs<<<c.agrid.ncell, 32, 0, c.stream>>>(A, P);
+      k_build_atoms<<<c.agrid.ncell, 32, 0, c.stream>>>(A, P, c.agrid.ncell);
     }
     if (c.na && c.ne) {
       if (split) CACB200_CUDA(cudaStreamWaitEvent(c.stream, c.items_ev, 0));
@@ -1693,7 +1513,6 @@ void neigh_build_async(Ctx &c, bool want_half) {
   c.lists_valid = true;
   c.nact_known = false;
   c.build_count++;
-  build_windows(c);
   CACB200_CUDA(cudaGetLastError());
 }
 

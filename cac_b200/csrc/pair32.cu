@@ -211,165 +211,6 @@ __device__ __forceinline__ void for_each32(const Args32 &A, int t, int i, const 
     walk32(A, fx, oi, seg ? nb + (size_t)(A.cap - (n - n_in)) * A.nsi : nb, seg ? n - n_in : n_in, f);
 }
 
-// ------------------------------------------------------------ windows
-//
-// Single systems: every block of WIN_BLOCK consecutive list slots has a
-// window, the sorted set of the distinct list entries (neighbour and image)
-// of its slots, built at each rebuild; the lists are also kept as 16-bit
-// indices into the window (same rows as the entries).  The density and
-// force passes then load a block's window records into shared memory once
-// (the neighbour's fixed-point position with its image already applied,
-// q + s Lq mod 2^32, and F') and read each pair's neighbour from there: a
-// neighbour shared by many of the block's sites is gathered from memory once
-// instead of once per site.  The separation is the same integer difference
-// modulo 2^32 as fix_delta's, so every pair's arithmetic, and every sum, is
-// unchanged.  A block whose window exceeds WIN_MAX entries keeps the direct
-// gathers.
-constexpr int WIN_BLOCK = 128;
-constexpr int WIN_MAX = 2048;
-constexpr int WIN_HASH = 8192;   // open-addressing table of the build (a power of two)
-
-// Builds the windows of one block of slots: distinct entries through a
-// hash set in shared memory, sorted (bitonic), then each entry's place.
-__global__ void __launch_bounds__(WIN_BLOCK) k_build_windows(const int *nbr, const int *num, const int *num_in,
-                                                             int nsi, int cap, int *win_keys, int *win_count,
-                                                             unsigned short *nbr16) {
-  __shared__ int ht[WIN_HASH];
-  __shared__ int keys[WIN_MAX];
-  __shared__ int cnt;
-  const int b = blockIdx.x, t = b * WIN_BLOCK + threadIdx.x;
-  for (int k = threadIdx.x; k < WIN_HASH; k += WIN_BLOCK) ht[k] = -1;   // entries are >= 0
-  if (threadIdx.x == 0) cnt = 0;
-  __syncthreads();
-  int n = 0, nin = 0;
-  if (t < nsi) {
-    n = num[t];
-    nin = num_in[t];
-    if (n > cap) n = 0;   // an overflowed list is rebuilt before use
-  }
-  auto row = [&](int k) { return k < nin ? k : cap - 1 - (k - nin); };
-  for (int k = 0; k < n; k++) {
-    if (*(volatile int *)&cnt > WIN_MAX) break;   // too many: this block keeps the direct gathers
-    const int v = nbr[(size_t)row(k) * nsi + t];
-    unsigned h = ((unsigned)v * 2654435761u) >> (32 - 13);
-    for (int probe = 0; probe < WIN_HASH; probe++) {
-      const int old = atomicCAS(&ht[h], -1, v);
-      if (old == -1) {
-        const int idx = atomicAdd(&cnt, 1);
-        if (idx < WIN_MAX) keys[idx] = v;
-        break;
-      }
-      if (old == v) break;
-      h = (h + 1) & (WIN_HASH - 1);
-    }
-  }
-  __syncthreads();
-  const int W = cnt;
-  if (W > WIN_MAX) {
-    if (threadIdx.x == 0) win_count[b] = W;
-    return;
-  }
-  int P = 1;
-  while (P < W) P <<= 1;
-  for (int k = W + threadIdx.x; k < P; k += WIN_BLOCK) keys[k] = 0x7fffffff;
-  __syncthreads();
-  for (int size = 2; size <= P; size <<= 1)
-    for (int stride = size >> 1; stride > 0; stride >>= 1) {
-      for (int k = threadIdx.x; k < P; k += WIN_BLOCK) {
-        const int l = k ^ stride;
-        if (l > k) {
-          const bool up = (k & size) == 0;
-          const int a = keys[k], c = keys[l];
-          if ((a > c) == up) {
-            keys[k] = c;
-            keys[l] = a;
-          }
-        }
-      }
-      __syncthreads();
-    }
-  for (int k = threadIdx.x; k < W; k += WIN_BLOCK) win_keys[(size_t)b * WIN_MAX + k] = keys[k];
-  if (threadIdx.x == 0) win_count[b] = W;
-  for (int k = 0; k < n; k++) {
-    const int r = row(k);
-    const int v = nbr[(size_t)r * nsi + t];
-    int lo = 0, hi = W - 1;
-    while (lo < hi) {
-      const int mid = (lo + hi) >> 1;
-      if (keys[mid] < v) lo = mid + 1;
-      else hi = mid;
-    }
-    nbr16[(size_t)r * nsi + t] = (unsigned short)lo;
-  }
-}
-
-// Loads block b's window into shared memory; returns its size, or -1 when
-// the block keeps the direct gathers.
-__device__ __forceinline__ int load_window(const Args32 &A, const SiteFix &F, const int *win_keys,
-                                           const int *win_count, int4 *wrec) {
-  const int b = blockIdx.x;
-  const int W = win_count[b];
-  if (W > WIN_MAX) return -1;
-  for (int k = threadIdx.x; k < W; k += WIN_BLOCK) {
-    const int v = win_keys[(size_t)b * WIN_MAX + k];
-    const int j = v >> IMG_BITS, code = v & ((1 << IMG_BITS) - 1);
-    int4 oj = __ldg(A.pos + j);
-    if (code != IMG_ZERO) {
-      int s0, s1, s2;
-      img_decode(code, s0, s1, s2);
-      oj.x = (int)((unsigned)oj.x + (unsigned)s0 * (unsigned)F.Lq[0]);
-      oj.y = (int)((unsigned)oj.y + (unsigned)s1 * (unsigned)F.Lq[1]);
-      oj.z = (int)((unsigned)oj.z + (unsigned)s2 * (unsigned)F.Lq[2]);
-    }
-    wrec[k] = oj;
-  }
-  return W;
-}
-
-// separation of site i (record oi) from window record rj (image applied)
-__device__ __forceinline__ void sep32w(const SiteFix &F, const int4 &oi, const int4 &rj, float &dx, float &dy,
-                                       float &dz, float &wj) {
-  dx = (float)(int)((unsigned)oi.x - (unsigned)rj.x) * F.inv[0];
-  dy = (float)(int)((unsigned)oi.y - (unsigned)rj.y) * F.inv[1];
-  dz = (float)(int)((unsigned)oi.z - (unsigned)rj.z) * F.inv[2];
-  wj = __int_as_float(rj.w);
-}
-
-template <class F>
-__device__ __forceinline__ void walk32w(const Args32 &A, const SiteFix &fx, const int4 &oi,
-                                        const unsigned short *nb, int n, const int4 *wrec, F &&f) {
-  int k = 0;
-  for (; k + 4 <= n; k += 4) {
-    const int v0 = nb[(size_t)k * A.nsi], v1 = nb[(size_t)(k + 1) * A.nsi];
-    const int v2 = nb[(size_t)(k + 2) * A.nsi], v3 = nb[(size_t)(k + 3) * A.nsi];
-    float d[4][4];
-    sep32w(fx, oi, wrec[v0], d[0][0], d[0][1], d[0][2], d[0][3]);
-    sep32w(fx, oi, wrec[v1], d[1][0], d[1][1], d[1][2], d[1][3]);
-    sep32w(fx, oi, wrec[v2], d[2][0], d[2][1], d[2][2], d[2][3]);
-    sep32w(fx, oi, wrec[v3], d[3][0], d[3][1], d[3][2], d[3][3]);
-#pragma unroll
-    for (int u = 0; u < 4; u++) f(d[u][0], d[u][1], d[u][2], d[u][3]);
-  }
-  for (; k < n; k++) {
-    float dx, dy, dz, wj;
-    sep32w(fx, oi, wrec[nb[(size_t)k * A.nsi]], dx, dy, dz, wj);
-    f(dx, dy, dz, wj);
-  }
-}
-
-// for_each32 over the window (single systems)
-template <class F>
-__device__ __forceinline__ void for_each32w(const Args32 &A, int t, const int4 &oi, const unsigned short *nbr16,
-                                            const int4 *wrec, F &&f) {
-  const SiteFix fx = site_fix(A, 0);
-  const int n_in = A.num_in[t], n = A.num[t];
-  const unsigned short *nb = nbr16 + t;
-  const bool rest = n > n_in && !A.inner_ok[0];
-#pragma unroll 1
-  for (int seg = 0; seg < (rest ? 2 : 1); seg++)
-    walk32w(A, fx, oi, seg ? nb + (size_t)(A.cap - (n - n_in)) * A.nsi : nb, seg ? n - n_in : n_in, wrec, f);
-}
-
 __device__ __forceinline__ void finish32(const Args32 &A, int i, bool valid, const float fi[3], bool ev,
                                          float esum, const float vsum[6], double eextra_site,
                                          double eextra_global) {
@@ -498,17 +339,14 @@ struct RhoPair {
 };
 
 // One list slot of the density pass: rho at the site, then F' into its
-// record (and F into phi_site for energies).  wrec: the block's window, or
-// null for direct gathers.
+// record (and F into phi_site for energies).
 __device__ __forceinline__ void rho32_slot(const Args32 &A, const Eam32 &T, int t, double *rho_out,
-                                           double *phi_site, int4 *pos_w, const unsigned short *nbr16 = nullptr,
-                                           const int4 *wrec = nullptr) {
+                                           double *phi_site, int4 *pos_w) {
   const int i = site_of_slot(A, t);                       // site-table index
   int4 oi;
   site_frame(A, t, oi);
   float rho = 0.f;
-  if (wrec) for_each32w(A, t, oi, nbr16, wrec, RhoPair{T, rho});
-  else for_each32(A, t, i, oi, RhoPair{T, rho});
+  for_each32(A, t, i, oi, RhoPair{T, rho});
   int slot = i;
   if (i >= A.na) {
     int e = (i - A.na) / NG, g = (i - A.na) % NG;
@@ -612,18 +450,15 @@ struct ForcePair {
 };
 
 // One list slot of the force pass: the pair sums of a valid slot (force;
-// energy and virial with EV) and its embedding energy.  wrec: the block's
-// window, or null for direct gathers.
+// energy and virial with EV) and its embedding energy.
 template <bool EV>
 __device__ __forceinline__ void force32_slot(const Args32 &A, const Eam32 &T, int t, int i,
                                              const double *phi_site, float fi[3], float &esum, float vsum[6],
-                                             double &eemb_site, double &eemb_global,
-                                             const unsigned short *nbr16 = nullptr, const int4 *wrec = nullptr) {
+                                             double &eemb_site, double &eemb_global) {
   int4 oi;
   site_frame(A, t, oi);
   const float fpi = __int_as_float(oi.w);
-  if (wrec) for_each32w(A, t, oi, nbr16, wrec, ForcePair<EV>{T, fpi, fi, esum, vsum});
-  else for_each32(A, t, i, oi, ForcePair<EV>{T, fpi, fi, esum, vsum});
+  for_each32(A, t, i, oi, ForcePair<EV>{T, fpi, fi, esum, vsum});
   if (EV && A.eflag) {
     double phi = phi_site[i];
     eemb_site = phi;
@@ -660,39 +495,6 @@ __global__ void __launch_bounds__(TB, 1024 / TB) k_eam_force32_queue(Args32 A, E
   }
 }
 
-// The passes over windows (single systems, force only for the force pass):
-// the block's window into shared memory, then one slot per thread.
-__global__ void __launch_bounds__(WIN_BLOCK, 1024 / WIN_BLOCK) k_eam_rho32_win(Args32 A, Eam32 T, double *rho_out,
-                                                                         double *phi_site, int4 *pos_w,
-                                                                         const int *win_keys, const int *win_count,
-                                                                         const unsigned short *nbr16) {
-  __shared__ int4 wrec[WIN_MAX];
-  const int W = load_window(A, site_fix(A, 0), win_keys, win_count, wrec);
-  __syncthreads();
-  const int t = blockIdx.x * WIN_BLOCK + threadIdx.x;
-  if (t >= A.nsi) return;
-  if (W >= 0) rho32_slot(A, T, t, rho_out, phi_site, pos_w, nbr16, wrec);
-  else rho32_slot(A, T, t, rho_out, phi_site, pos_w);
-}
-
-__global__ void __launch_bounds__(WIN_BLOCK, 1024 / WIN_BLOCK) k_eam_force32_win(Args32 A, Eam32 T,
-                                                                           const double *phi_site,
-                                                                           const int *win_keys,
-                                                                           const int *win_count,
-                                                                           const unsigned short *nbr16) {
-  __shared__ int4 wrec[WIN_MAX];
-  const int W = load_window(A, site_fix(A, 0), win_keys, win_count, wrec);
-  __syncthreads();
-  const int t = blockIdx.x * WIN_BLOCK + threadIdx.x;
-  if (t >= A.nsi) return;
-  const int i = site_of_slot(A, t);
-  float fi[3] = {0, 0, 0}, esum = 0.f, vsum[6] = {0, 0, 0, 0, 0, 0};
-  double eemb_site = 0.0, eemb_global = 0.0;
-  if (W >= 0) force32_slot<false>(A, T, t, i, phi_site, fi, esum, vsum, eemb_site, eemb_global, nbr16, wrec);
-  else force32_slot<false>(A, T, t, i, phi_site, fi, esum, vsum, eemb_site, eemb_global);
-  finish32(A, i, true, fi, false, esum, vsum, eemb_site, eemb_global);
-}
-
 __global__ void k_reduce_partials32(const double *partial, int nblocks, double *out) {
   int k = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (k >= 7) return;
@@ -722,20 +524,6 @@ FixGrid make_fix_grid(const Ctx &c) {
 }
 
 }  // namespace
-
-void build_windows(Ctx &c) {
-  if (!(c.windows && c.precision == CACB200_MIXED && c.nrep == 1 && c.pp.style == CACB200_PAIR_EAM)) return;
-  const int nsi = c.nsite_i();
-  if (nsi == 0) return;
-  const int nb = nblk(nsi, WIN_BLOCK);
-  c.win_keys.reserve((size_t)nb * WIN_MAX);
-  c.win_count.reserve(nb);
-  c.nbr16.reserve((size_t)c.cap * nsi);
-  KernelTimer t(c, "windows");
-  k_build_windows<<<nb, WIN_BLOCK, 0, c.stream>>>(c.nbr_full.p, c.num_full.p, c.num_in.p, nsi, c.cap, c.win_keys.p,
-                                                 c.win_count.p, c.nbr16.p);
-  c.win_for = c.build_count;
-}
 
 void pair_table_mixed(Ctx &c) {
   const long ns = (long)c.nsite_i() + (long)c.ne * NU;   // capacity: every lattice site active
@@ -944,7 +732,7 @@ void pair_compute_mixed(Ctx &c, int eflag, int vflag) {
     if (queue && c.work_gen != c.gen) queue = false;
     // block sizes of the force-only passes chosen by timing on first use (as
     // in the FP64 form; results do not depend on them)
-    if (!queue && !(c.nrep == 1 && c.windows && c.win_for == c.build_count) && c.tune_gen32 != c.gen && !ev &&
+    if (!queue && c.tune_gen32 != c.gen && !ev &&
         cs == cudaStreamCaptureStatusNone) {
       const int cand[3] = {128, 64, 256};   // another size replaces 128 only when >= 3 % faster
       cudaEvent_t e0, e1;
@@ -979,14 +767,9 @@ void pair_compute_mixed(Ctx &c, int eflag, int vflag) {
       cudaEventDestroy(e1);
       c.tune_gen32 = c.gen;
     }
-    // single systems: the passes over neighbour windows when the lists have them
-    const bool win = c.nrep == 1 && c.windows && c.win_for == c.build_count;
     {
       KernelTimer t(c, "eam_rho32");
       if (queue) rho_q();
-      else if (win)
-        k_eam_rho32_win<<<nblk(nsi, WIN_BLOCK), WIN_BLOCK, 0, c.stream>>>(A, Tb, c.rho.p, c.phi_site.p, c.pos32.p,
-                                                                           c.win_keys.p, c.win_count.p, c.nbr16.p);
       else rho(c.tb_rho32);
     }
     if (c.ne) {
@@ -997,9 +780,6 @@ void pair_compute_mixed(Ctx &c, int eflag, int vflag) {
       KernelTimer t(c, "eam_force32");
       if (ev) k_eam_force32<128, true><<<nb, T, 0, c.stream>>>(A, Tb, c.phi_site.p);
       else if (queue) force_q();
-      else if (win)
-        k_eam_force32_win<<<nblk(nsi, WIN_BLOCK), WIN_BLOCK, 0, c.stream>>>(A, Tb, c.phi_site.p, c.win_keys.p,
-                                                                             c.win_count.p, c.nbr16.p);
       else force(c.tb_force32);
     }
   }

@@ -427,16 +427,6 @@ int cacb200_pair_blocks(cacb200_ctx *ctx, int *rho_threads, int *force_threads);
  * pass), -1 unchanged; tiles [3] gets the chosen tiles (0: not chosen yet).
  * No reference counterpart (the reference runs one system per process). */
 int cacb200_work_queue(cacb200_ctx *ctx, int enable, int tiles[3]);
-/* Single systems in the mixed form with EAM: with every list build, each
- * block of 128 list slots gets its window, the sorted distinct neighbour
- * entries of its slots (at most 2,048; a larger block keeps direct gathers),
- * and the lists a copy as 16-bit window indices; the density and force
- * passes load a block's window records into shared memory once and read
- * each pair's neighbour from there.  Results are the same bit for bit.
- * enable 1 or 0 (default); takes effect at the next list build.  No
- * reference counterpart (PairEAM::compute gathers per pair,
- * pair_eam.cpp:707-1028). */
-int cacb200_set_windows(cacb200_ctx *ctx, int enable);
 
 /* Kernel timing: when enabled, every launch is bracketed by CUDA events and
  * per-kernel totals accumulate (ms, launches) until reset. */
