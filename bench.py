@@ -399,6 +399,9 @@ def pipe_peak(fp64: bool, device: int) -> float:
     return best
 
 
+WORK_QUEUE = True   # --work-queue: persistent launches of the mixed EAM passes
+
+
 def make_engine(s, pair, form: str, local: int, setfl: str, fix: str):
     """A context holding the workload, set up at the seeded state (lists,
     forces) and snapshotted for the restarts."""
@@ -414,6 +417,7 @@ def make_engine(s, pair, form: str, local: int, setfl: str, fix: str):
         eng.pair_lj(0.4093, 2.338, 5.5)
     eng.set_precision(api.MIXED if form == "mixed" else api.FP64)
     eng.neighbor(1.0, 10)
+    eng.work_queue(WORK_QUEUE)
     if fix == "langevin":
         eng.langevin(300.0, 300.0, 0.1, 4928459)
     elif fix == "deform":
@@ -672,7 +676,8 @@ def b200_arm(args, rank, local, ws, dist):
                                        if batch and ws > 1 else f"replicas x{ws} (no data-path collective)"),
                        "fix": {"none": "nve", "langevin": "nve + langevin 300 300 0.1",
                                "deform": "nve + deform 1 x erate 0.1 y volume"}[args.fix],
-                       "l2": "working set larger than L2 (site table + lists > 126 MB)"},
+                       "l2": "working set larger than L2 (site table + lists > 126 MB)",
+                       "work_queue": WORK_QUEUE},
             "fp64": fp64_entry,
             "mixed_over_fp64": (value / fp64_entry["value"]) if fp64_entry else None,
             "accuracy": accuracy,
@@ -930,7 +935,12 @@ def main():
     ap.add_argument("--segment", type=int, default=50,
                     help="steps per trajectory from the seeded initial state (the reference's CAC "
                          "dynamics heat up unboundedly after ~100 steps, so long runs restart)")
+    ap.add_argument("--work-queue", default="on", choices=["on", "off"],
+                    help="mixed EAM passes as persistent launches (batches: work items per replica; "
+                         "single systems: SM-local runs of list slots) or one grid launch per pass")
     args = ap.parse_args()
+    global WORK_QUEUE
+    WORK_QUEUE = args.work_queue == "on"
     rank, local, ws, dist = dist_init()
     try:
         if args.impl == "reference":

@@ -328,6 +328,7 @@ struct Ctx {
   bool work_queue = true;
   DBuf<int2> work_items;
   DBuf<int> work_counter;
+  DBuf<int> sm_counter;   // single systems: run counters of the SM-local ranges (rho, force)
   int nwork_items = 0;
   long work_gen = -1;
   int work_tile[3] = {0, 0, 0};

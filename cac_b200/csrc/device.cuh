@@ -122,4 +122,55 @@ __device__ __forceinline__ void block_reduce_store(double (&vals)[NV], double *o
   }
 }
 
+// SM-local runs: work cut into nrun runs (of list slots, of cells), with SM
+// s owning runs [s*nrun/nsm, (s+1)*nrun/nsm), so that the blocks resident on
+// one SM work on neighbouring runs (cell-sorted: neighbouring space) and find
+// their neighbours' data in the SM's L1, instead of the hardware's spread of
+// consecutive blocks over all SMs.  A persistent block takes runs from a
+// range's counter (cleared before the launch), its own SM's range first;
+// once that is exhausted, warp 0 scans the other ranges 32 at a time for one
+// with runs left.  Counters only grow, so a range seen exhausted stays so and
+// the scan ends; every run is taken exactly once.  Returns the run, or -1
+// when none is left.  v: the block's current range (shared), initially
+// sm_id() % nsm.  Every thread of the block calls it.
+__device__ __forceinline__ int sm_id() {
+  unsigned s;
+  asm volatile("mov.u32 %0, %%smid;" : "=r"(s));
+  return (int)s;
+}
+
+__device__ __forceinline__ int sm_run(int *cnt, int nsm, int nrun, int &v) {
+  __shared__ int got;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    const int lane = threadIdx.x;
+    auto lo = [&](int u) { return (int)((long)u * nrun / nsm); };
+    int cur = v, res = -1;
+    for (;;) {
+      int k = 0;
+      if (lane == 0) k = atomicAdd(cnt + cur, 1);
+      k = __shfl_sync(0xffffffffu, k, 0);
+      if (lo(cur) + k < lo(cur + 1)) {
+        res = lo(cur) + k;
+        break;
+      }
+      int found = -1;
+      for (int base = 1; base <= nsm && found < 0; base += 32) {
+        const int u = (cur + base + lane) % nsm;
+        const bool left = base + lane <= nsm && lo(u) + *(volatile int *)(cnt + u) < lo(u + 1);
+        const unsigned b = __ballot_sync(0xffffffffu, left);
+        if (b) found = (cur + base + __ffs(b) - 1) % nsm;
+      }
+      if (found < 0) break;
+      cur = found;
+    }
+    if (lane == 0) {
+      got = res;
+      v = cur;
+    }
+  }
+  __syncthreads();
+  return got;
+}
+
 }  // namespace cacb200

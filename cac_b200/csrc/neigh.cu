@@ -44,6 +44,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <tuple>
+#include <type_traits>
 
 #include "ctx.cuh"
 #include "device.cuh"
@@ -812,12 +813,11 @@ __device__ __forceinline__ void finish_counts(const BuildArgs &A, int i, int nin
 // at the end.
 constexpr int STAGE_ROWS = 32;
 template <class RP>
-__device__ __forceinline__ void build_atoms_cells(BuildArgs A, RP P, int ncell) {
+__device__ __forceinline__ void build_atoms_cell(BuildArgs A, RP P, const int home) {
   const int lane = threadIdx.x & 31;
   const float fcut2 = (float)A.cutforcesq;
   __shared__ int st_in[STAGE_ROWS][32], st_out[STAGE_ROWS][32];   // front / back segment rings
   {
-    const int home = blockIdx.x;
     const int hbeg = A.acell_start[home], hend = A.acell_start[home + 1];
     if (hbeg == hend) return;
     const Rep R = P.acell(home);
@@ -936,15 +936,26 @@ __device__ __forceinline__ void build_atoms_cells(BuildArgs A, RP P, int ncell) 
   }
 }
 
-// The single-system form as the compiler allocates it (64 registers); the
-// batch form capped at 64 registers (from 80, a few bytes spilled) so that
-// 32 warps instead of 24 are resident per SM: 10 % faster on a 64-replica
-// batch, where the same cap slowed the single-system form.
-__global__ void __launch_bounds__(32) k_build_atoms(BuildArgs A, OneRep P, int ncell) {
-  build_atoms_cells(A, P, ncell);
+// The single-system form as the compiler allocates it (92 registers with the
+// candidate loads four at a time); the batch form capped at 64 registers (a
+// few bytes spilled) so that 32 warps are resident per SM: 10 % faster on a
+// 64-replica batch, where the same cap slowed the single-system form.
+__global__ void __launch_bounds__(32) k_build_atoms(BuildArgs A, OneRep P) { build_atoms_cell(A, P, blockIdx.x); }
+__global__ void __launch_bounds__(32, 32) k_build_atoms(BuildArgs A, ManyRep P) {
+  build_atoms_cell(A, P, blockIdx.x);
 }
-__global__ void __launch_bounds__(32, 32) k_build_atoms(BuildArgs A, ManyRep P, int ncell) {
-  build_atoms_cells(A, P, ncell);
+
+// Single systems: persistent warps taking the cells in SM-local runs (one
+// cell per run, sm_run in device.cuh), so that the warps resident on one SM
+// walk neighbouring cells and share their candidates in L1.  The same lists.
+__global__ void __launch_bounds__(32) k_build_atoms_sm(BuildArgs A, OneRep P, int ncell, int *cnt, int nsm) {
+  __shared__ int v;
+  if (threadIdx.x == 0) v = sm_id() % nsm;
+  for (;;) {
+    const int home = sm_run(cnt, nsm, ncell, v);
+    if (home < 0) return;
+    build_atoms_cell(A, P, home);
+  }
 }
 
 // Phase A over every list slot: the element walk of each atom and Gauss
@@ -1211,6 +1222,7 @@ void neigh_plan(Ctx &c, bool want_half) {
   c.num_in.reserve(std::max(c.nsite_i(), 1));
   c.reach_bits.reserve(c.nrep);
   c.rep_d.reserve(c.nrep);
+  c.sm_counter.reserve(2 * c.num_sms);
   CACB200_CUDA(cudaMemsetAsync(c.overflow.p, 0, 16 * sizeof(int), c.stream));
   CACB200_CUDA(cudaMemsetAsync(c.dev_nact.p, 0, sizeof(int), c.stream));
   CACB200_CUDA(cudaMemsetAsync(c.reach_bits.p, 0, sizeof(unsigned long long) * c.nrep, c.stream));
@@ -1474,7 +1486,22 @@ void neigh_build_async(Ctx &c, bool want_half) {
     }
     if (c.na) {
       KernelTimer t(c, "build_atoms");
-      k_build_atoms<<<c.agrid.ncell, 32, 0, c.stream>>>(A, P, c.agrid.ncell);
+      if constexpr (std::is_same_v<decltype(P), OneRep>) {
+        if (c.work_queue) {
+          static const int per_sm = [] {
+            int b = 0;
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_build_atoms_sm, 32, 0);
+            return b > 0 ? b : 1;
+          }();
+          CACB200_CUDA(cudaMemsetAsync(c.sm_counter.p, 0, sizeof(int) * c.num_sms, c.stream));
+          k_build_atoms_sm<<<per_sm * c.num_sms, 32, 0, c.stream>>>(A, P, c.agrid.ncell, c.sm_counter.p,
+                                                                   c.num_sms);
+        } else {
+          k_build_atoms<<<c.agrid.ncell, 32, 0, c.stream>>>(A, P);
+        }
+      } else {
+        k_build_atoms<<<c.agrid.ncell, 32, 0, c.stream>>>(A, P);
+      }
     }
     if (c.na && c.ne) {
       if (split) CACB200_CUDA(cudaStreamWaitEvent(c.stream, c.items_ev, 0));

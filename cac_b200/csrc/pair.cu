@@ -254,11 +254,9 @@ __device__ __forceinline__ double eam_fp(const EamTables &T, double rho, double 
 // pass 1: density at atoms and node Gauss points (pair_eam.cpp:707-812), then
 // F' at the site itself into xs[i].w (pair_eam.cpp:819-833 for atoms; for a
 // node the reference's rhoi = noderho at :901-903).
-template <int TB, bool MANY>
-__global__ void __launch_bounds__(TB, 1024 / TB) k_eam_rho(PairArgs A, EamTables T, double *rho_out,
-                                                       double *phi_site) {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;   // list slot
-  if (t >= A.nsi) return;
+template <bool MANY>
+__device__ __forceinline__ void rho_slot(const PairArgs &A, const EamTables &T, int t, double *rho_out,
+                                         double *phi_site) {
   const int i = site_of_slot(A, t);                       // site-table index
   double4 xi = A.xs[t];
   const int n_in = A.num_in[t], n = A.num[t];
@@ -290,6 +288,31 @@ __global__ void __launch_bounds__(TB, 1024 / TB) k_eam_rho(PairArgs A, EamTables
   if (A.eflag) phi_site[i] = phi;
 }
 
+template <int TB, bool MANY>
+__global__ void __launch_bounds__(TB, 1024 / TB) k_eam_rho(PairArgs A, EamTables T, double *rho_out,
+                                                       double *phi_site) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;   // list slot
+  if (t >= A.nsi) return;
+  rho_slot<MANY>(A, T, t, rho_out, phi_site);
+}
+
+// Single systems: the force-only passes over SM-local runs of list slots
+// (sm_run, device.cuh); each slot is computed by the same function as in the
+// grid launch, so the results are the grid launch's bit for bit.
+template <int TB>
+__global__ void __launch_bounds__(TB, 1024 / TB) k_eam_rho_sm(PairArgs A, EamTables T, double *rho_out,
+                                                          double *phi_site, int *cnt, int nsm) {
+  __shared__ int v;
+  if (threadIdx.x == 0) v = sm_id() % nsm;
+  const int nrun = (A.nsi + TB - 1) / TB;
+  for (;;) {
+    const int r = sm_run(cnt, nsm, nrun, v);
+    if (r < 0) return;
+    const int t = r * TB + threadIdx.x;
+    if (t < A.nsi) rho_slot<false>(A, T, t, rho_out, phi_site);
+  }
+}
+
 // F' at interpolated lattice sites from shape-weighted nodal density
 // (pair_eam.cpp:957-969)
 __global__ void k_eam_site_fp(double4 *xs, const int *act_gid, const int *nact_dev, int base, int na,
@@ -307,15 +330,11 @@ __global__ void k_eam_site_fp(double4 *xs, const int *act_gid, const int *nact_d
 }
 
 // pass 2: forces (pair_eam.cpp:845-1028)
-template <int TB, bool EV, bool MANY>
-__global__ void __launch_bounds__(TB, (EV ? 512 : 768) / TB) k_eam_force(PairArgs A, EamTables T,
-                                                                       const double *phi_site) {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;   // list slot
-  const bool valid = t < A.nsi;
-  const int i = valid ? site_of_slot(A, t) : 0;           // site-table index
-  double fi[3] = {0, 0, 0}, esum = 0.0, vsum[6] = {0, 0, 0, 0, 0, 0};
-  double eemb_site = 0.0, eemb_global = 0.0;
-  if (valid) {
+template <bool EV, bool MANY>
+__device__ __forceinline__ void force_slot(const PairArgs &A, const EamTables &T, int t, int i,
+                                           const double *phi_site, double fi[3], double &esum, double vsum[6],
+                                           double &eemb_site, double &eemb_global) {
+  {
     double4 xi = A.xs[t];
     double fpi = xi.w;
     const int n_in = A.num_in[t], n = A.num[t];
@@ -361,8 +380,39 @@ __global__ void __launch_bounds__(TB, (EV ? 512 : 768) / TB) k_eam_force(PairArg
       eemb_global = (i < A.na) ? phi : phi * A.escale_node * 2.0;
     }
   }
+}
+
+template <int TB, bool EV, bool MANY>
+__global__ void __launch_bounds__(TB, (EV ? 512 : 768) / TB) k_eam_force(PairArgs A, EamTables T,
+                                                                       const double *phi_site) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;   // list slot
+  const bool valid = t < A.nsi;
+  const int i = valid ? site_of_slot(A, t) : 0;           // site-table index
+  double fi[3] = {0, 0, 0}, esum = 0.0, vsum[6] = {0, 0, 0, 0, 0, 0};
+  double eemb_site = 0.0, eemb_global = 0.0;
+  if (valid) force_slot<EV, MANY>(A, T, t, i, phi_site, fi, esum, vsum, eemb_site, eemb_global);
   if (EV) finish_site(A, i, valid, fi, esum, vsum, eemb_site, eemb_global);
   else finish_force(A, i, valid, fi);
+}
+
+template <int TB>
+__global__ void __launch_bounds__(TB, 768 / TB) k_eam_force_sm(PairArgs A, EamTables T, const double *phi_site,
+                                                           int *cnt, int nsm) {
+  __shared__ int v;
+  if (threadIdx.x == 0) v = sm_id() % nsm;
+  const int nrun = (A.nsi + TB - 1) / TB;
+  for (;;) {
+    const int r = sm_run(cnt, nsm, nrun, v);
+    if (r < 0) return;
+    const int t = r * TB + threadIdx.x;
+    if (t < A.nsi) {
+      const int i = site_of_slot(A, t);
+      double fi[3] = {0, 0, 0}, esum = 0.0, vsum[6] = {0, 0, 0, 0, 0, 0};
+      double eemb_site = 0.0, eemb_global = 0.0;
+      force_slot<false, false>(A, T, t, i, phi_site, fi, esum, vsum, eemb_site, eemb_global);
+      finish_force(A, i, true, fi);
+    }
+  }
 }
 
 __global__ void k_reduce_partials(const double *partial, int nblocks, double *out) {
@@ -576,7 +626,29 @@ void pair_compute(Ctx &c, int eflag, int vflag) {
       if (many) launch_force<true>(tb, nsi, c.stream, A, Tb, c.phi_site.p);
       else launch_force<false>(tb, nsi, c.stream, A, Tb, c.phi_site.p);
     };
-    if (c.tune_gen != c.gen && !eflag && !vflag && !capturing(c.stream)) {
+    // single systems: the force-only passes over SM-local runs
+    const bool smq = !many && c.work_queue;
+    c.sm_counter.reserve(2 * c.num_sms);
+    auto sm_grid = [&](auto kernel, int &cache) {
+      if (!cache) {
+        int b = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kernel, 128, 0);
+        cache = (b > 0 ? b : 1) * c.num_sms;
+      }
+      return cache;
+    };
+    static int grid_rho_sm = 0, grid_force_sm = 0;
+    auto rho_s = [&] {
+      CACB200_CUDA(cudaMemsetAsync(c.sm_counter.p, 0, sizeof(int) * c.num_sms, c.stream));
+      k_eam_rho_sm<128><<<sm_grid(k_eam_rho_sm<128>, grid_rho_sm), 128, 0, c.stream>>>(
+          A, Tb, c.rho.p, c.phi_site.p, c.sm_counter.p, c.num_sms);
+    };
+    auto force_s = [&] {
+      CACB200_CUDA(cudaMemsetAsync(c.sm_counter.p + c.num_sms, 0, sizeof(int) * c.num_sms, c.stream));
+      k_eam_force_sm<128><<<sm_grid(k_eam_force_sm<128>, grid_force_sm), 128, 0, c.stream>>>(
+          A, Tb, c.phi_site.p, c.sm_counter.p + c.num_sms, c.num_sms);
+    };
+    if (!smq && c.tune_gen != c.gen && !eflag && !vflag && !capturing(c.stream)) {
       // another size replaces 128 only when it is at least 3 % faster
       const int cand[3] = {128, 64, 256};
       float best = 1e30f;
@@ -595,7 +667,8 @@ void pair_compute(Ctx &c, int eflag, int vflag) {
     }
     {
       KernelTimer t(c, "eam_rho");
-      rho(c.tb_rho);
+      if (smq) rho_s();
+      else rho(c.tb_rho);
     }
     {
       KernelTimer t(c, "eam_site_fp");
@@ -606,6 +679,8 @@ void pair_compute(Ctx &c, int eflag, int vflag) {
       if (eflag || vflag) {
         if (many) k_eam_force<128, true, true><<<nb, T, 0, c.stream>>>(A, Tb, c.phi_site.p);
         else k_eam_force<128, true, false><<<nb, T, 0, c.stream>>>(A, Tb, c.phi_site.p);
+      } else if (smq) {
+        force_s();
       } else {
         force(c.tb_force);
       }

@@ -129,3 +129,31 @@ def test_work_queue_launches_equal_grid_launches(tmp_path):
     assert all(t in (128, 512, 2048) for t in t1 if t)
     assert any(t1)
     assert np.array_equal(f1, f0) and np.array_equal(g1, g0) and np.array_equal(x1, x0)
+
+
+@pytest.mark.parametrize("form,strain", [(0, 0.0), (1, 0.0), (1, 0.03)])
+def test_sm_local_runs_equal_grid_launches(form, strain, tmp_path):
+    """A single system runs the atom-list build and the force-only EAM passes
+    over SM-local runs of cells and list slots (work queue on, the default);
+    the lists, forces and trajectory equal those of the grid launches (work
+    queue off) bit for bit, over steps with rebuilds (FP64 and mixed)."""
+    from cac_b200.api import Engine
+    s = gen.build_slab(6, 3, 8, 24, temperature=300.0, strain=strain, seed=14)
+    out = []
+    for on in (True, False):
+        e = Engine(0)
+        e.upload(s)
+        e.pair_eam(setfl_path(tmp_path))
+        e.set_precision(form)
+        e.neighbor(1.0, 10)
+        e.work_queue(on)
+        e.setup()
+        e.run_nve(25, 0.001)
+        f, nf, gf = e.forces()
+        x, v, nx, nv = e.state()
+        e.build_lists()
+        lst = e.neighbor_list()
+        out.append((f, nf, gf, x, v, nx, nv, lst))
+        e.close()
+    for a, b in zip(*out):
+        assert np.array_equal(a, b)
