@@ -345,7 +345,8 @@ def test_verlet_b200_dumps_with_device_peratom_computes(case, tmp_path):
     reference side runs cac_eamfix for both pair styles: the stock
     ComputePEAtom never returns on a system with elements (its clear loop of
     node_energy reuses the inner loop's variable in the outer loop,
-    compute_pe_atom.cpp:130), and that executable carries the one-line fix."""
+    compute_pe_atom.cpp:130) and folds only node 0 of ghost elements into
+    their owners (:235, :254); that executable carries the fixes."""
     import oracle as O
     dump = ("dump 1 all custom 10 d.* id type x y z fx fy fz c_pa c_sa[1] c_sa[2] c_sa[3] c_sa[4] "
             "c_sa[5] c_sa[6]\n")
@@ -372,12 +373,16 @@ def test_reference_neighbor_debug_dump_reads_the_device_list(case, tmp_path):
     fills the host list from the device's half list.  The whole-list dump
     (per site: coordinates, tag, neighbour count) equals the reference's own
     file, and one atom's and one Gauss point's neighbours (coordinates, tag,
-    lattice site) equal the reference's as sets."""
+    lattice site) equal the reference's as sets.  Both sides run the
+    command with its three defects fixed (cac_eamfix, and the same objects in
+    the harness): the stock code reads an unset element index in its header
+    and gauss form, and leaves a deleted atom map in use after the atom form
+    (write_dump_neighbor_debug.cpp:48, 220, 302), so its third call crashes."""
     import oracle as O
     body = ("write_dump_neighbor_debug nb\nwrite_dump_neighbor_debug na atom 5\n"
             "write_dump_neighbor_debug ng gauss 3 0 2\n")
     app_log(tmp_path, case, body)
-    reference_log(tmp_path, case, body, O.REF_EXE)
+    reference_log(tmp_path, case, body, O.REF_EXE_EAMFIX)
     with open(tmp_path / "nb_proc_0.dat") as f1, open(tmp_path / "ref" / "nb_proc_0.dat") as f2:
         assert f1.read() == f2.read()
     for name in ("na_proc_0", "ng_proc_0"):
