@@ -884,9 +884,15 @@ __device__ __forceinline__ void build_atoms_cell(BuildArgs A, RP P, const int ho
             const int code = far ? 0 : img_code(s0, s1, s2);
             int beg = A.acell_start[cell], end = A.acell_start[cell + 1];
             // candidate pj at list slot ks
+            // the FP32 distance in explicitly rounded operations: the
+            // in-cutoff mark below decides an entry's list segment, so every
+            // kernel that builds these lists (grid and SM-local forms) must
+            // round it the same way, whatever the compiler would contract
             auto consider = [&](const float4 &pj, int ks) {
-              float ex = wx - (pj.x + sx), ey = wy - (pj.y + sy), ez = wz - (pj.z + sz);
-              const float r2 = ex * ex + ey * ey + ez * ez;
+              const float ex = __fsub_rn(wx, __fadd_rn(pj.x, sx));
+              const float ey = __fsub_rn(wy, __fadd_rn(pj.y, sy));
+              const float ez = __fsub_rn(wz, __fadd_rn(pj.z, sz));
+              const float r2 = __fmaf_rn(ez, ez, __fmaf_rn(ey, ey, __fmul_rn(ex, ex)));
               if (r2 > pre2) return;
               const int j = __float_as_int(pj.w);
               if (r2 < sure2 && !A.want_half) {
