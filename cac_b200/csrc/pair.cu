@@ -50,6 +50,15 @@ struct PairArgs {
 
 __device__ __forceinline__ int site_of_slot(const PairArgs &A, int t) { return t < A.na ? A.slot_atom[t] : t; }
 
+// The FP64 EAM arithmetic in explicitly rounded operations, with no fused
+// multiply-add: the operation order of the reference's source (compiled
+// there without contraction), and the same rounding in every kernel that
+// inlines it (grid and SM-local launches, grouped and remainder walks), where
+// the compiler would otherwise contract each copy its own way.
+__device__ __forceinline__ double rmul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double radd(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double rsub(double a, double b) { return __dsub_rn(a, b); }
+
 __device__ __forceinline__ void neighbour_pos(const PairArgs &A, double Lx, double Ly, double Lz, int v,
                                               double4 &xj) {
   int j = v >> IMG_BITS, code = v & ((1 << IMG_BITS) - 1);
@@ -57,9 +66,9 @@ __device__ __forceinline__ void neighbour_pos(const PairArgs &A, double Lx, doub
   if (code != IMG_ZERO) {
     int sx, sy, sz;
     img_decode(code, sx, sy, sz);
-    xj.x += sx * Lx;
-    xj.y += sy * Ly;
-    xj.z += sz * Lz;
+    xj.x = radd(xj.x, rmul((double)sx, Lx));
+    xj.y = radd(xj.y, rmul((double)sy, Ly));
+    xj.z = radd(xj.z, rmul((double)sz, Lz));
   }
 }
 
@@ -235,17 +244,17 @@ struct EamTables {
 // pair_eam.cpp:1160-1169; the energy read on the same row, i.e. the
 // reference with its coefficient pointer returned to the caller)
 __device__ __forceinline__ double eam_fp(const EamTables &T, double rho, double *phi) {
-  double p = rho * T.rdrho + 1.0;
+  double p = radd(rmul(rho, T.rdrho), 1.0);
   int m = (int)p;
   m = max(1, min(m, T.nrho - 1));
-  p -= m;
+  p = rsub(p, (double)m);
   p = fmin(p, 1.0);
   double4 d = T.frho_der[m];
-  double fp = (d.x * p + d.y) * p + d.z;
+  double fp = radd(rmul(radd(rmul(d.x, p), d.y), p), d.z);
   if (phi) {
     double4 v = T.frho_val[m];
-    double e = ((v.x * p + v.y) * p + v.z) * p + v.w;
-    if (rho > T.rhomax) e += fp * (rho - T.rhomax);
+    double e = radd(rmul(radd(rmul(radd(rmul(v.x, p), v.y), p), v.z), p), v.w);
+    if (rho > T.rhomax) e = radd(e, rmul(fp, rsub(rho, T.rhomax)));
     *phi = e;
   }
   return fp;
@@ -263,16 +272,16 @@ __device__ __forceinline__ void rho_slot(const PairArgs &A, const EamTables &T, 
   const int *nb = A.nbr + t;
   double rho = 0.0;
   auto pair = [&](const double4 &xj) {
-    double dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
-    double rsq = dx * dx + dy * dy + dz * dz;
+    const double dx = rsub(xi.x, xj.x), dy = rsub(xi.y, xj.y), dz = rsub(xi.z, xj.z);
+    const double rsq = radd(radd(rmul(dx, dx), rmul(dy, dy)), rmul(dz, dz));
     if (rsq < T.cutforcesq) {
-      double p = sqrt(rsq) * T.rdr + 1.0;
+      double p = radd(rmul(sqrt(rsq), T.rdr), 1.0);
       int m = (int)p;
       m = max(1, min(m, T.nr - 1));
-      p -= m;
+      p = rsub(p, (double)m);
       p = fmin(p, 1.0);
       double4 c = ldg256(T.rz + 2 * m);
-      rho += ((c.x * p + c.y) * p + c.z) * p + c.w;
+      rho = radd(rho, radd(rmul(radd(rmul(radd(rmul(c.x, p), c.y), p), c.z), p), c.w));
     }
   };
   walk_list<MANY>(A, i, nb, n_in, n, pair);
@@ -324,7 +333,7 @@ __global__ void k_eam_site_fp(double4 *xs, const int *act_gid, const int *nact_d
     const double *rn = rho + na + 8 * (size_t)e;
     double r = 0.0;
 #pragma unroll
-    for (int n = 0; n < NPE; n++) r += shape_val(u, n) * rn[n];
+    for (int n = 0; n < NPE; n++) r = radd(r, rmul(shape_val(u, n), rn[n]));
     xs[base + k].w = eam_fp(T, r, nullptr);
   }
 }
@@ -340,36 +349,36 @@ __device__ __forceinline__ void force_slot(const PairArgs &A, const EamTables &T
     const int n_in = A.num_in[t], n = A.num[t];
     const int *nb = A.nbr + t;
     auto pair = [&](const double4 &xj) {
-      double dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
-      double rsq = dx * dx + dy * dy + dz * dz;
+      const double dx = rsub(xi.x, xj.x), dy = rsub(xi.y, xj.y), dz = rsub(xi.z, xj.z);
+      const double rsq = radd(radd(rmul(dx, dx), rmul(dy, dy)), rmul(dz, dz));
       if (rsq < T.cutforcesq) {
-        double r = sqrt(rsq);
-        double p = r * T.rdr + 1.0;
+        const double r = sqrt(rsq);
+        double p = radd(rmul(r, T.rdr), 1.0);
         int m = (int)p;
         m = max(1, min(m, T.nr - 1));
-        p -= m;
+        p = rsub(p, (double)m);
         p = fmin(p, 1.0);
         double4 rv = ldg256(T.rz + 2 * m);
         double4 zv = ldg256(T.rz + 2 * m + 1);
-        double rhop = ((3.0 * rv.x * p + 2.0 * rv.y) * p + rv.z) * T.rdr;
-        double z2p = ((3.0 * zv.x * p + 2.0 * zv.y) * p + zv.z) * T.rdr;
-        double z2 = ((zv.x * p + zv.y) * p + zv.z) * p + zv.w;
-        double recip = 1.0 / r;
-        double phi = z2 * recip;
-        double phip = z2p * recip - phi * recip;
-        double psip = fpi * rhop + xj.w * rhop + phip;
-        double fpair = -psip * recip;
-        fi[0] += dx * fpair;
-        fi[1] += dy * fpair;
-        fi[2] += dz * fpair;
-        if (EV && A.eflag) esum += phi;
+        const double rhop = rmul(radd(rmul(radd(rmul(rmul(3.0, rv.x), p), rmul(2.0, rv.y)), p), rv.z), T.rdr);
+        const double z2p = rmul(radd(rmul(radd(rmul(rmul(3.0, zv.x), p), rmul(2.0, zv.y)), p), zv.z), T.rdr);
+        const double z2 = radd(rmul(radd(rmul(radd(rmul(zv.x, p), zv.y), p), zv.z), p), zv.w);
+        const double recip = 1.0 / r;
+        const double phi = rmul(z2, recip);
+        const double phip = rsub(rmul(z2p, recip), rmul(phi, recip));
+        const double psip = radd(radd(rmul(fpi, rhop), rmul(xj.w, rhop)), phip);
+        const double fpair = -rmul(psip, recip);
+        fi[0] = radd(fi[0], rmul(dx, fpair));
+        fi[1] = radd(fi[1], rmul(dy, fpair));
+        fi[2] = radd(fi[2], rmul(dz, fpair));
+        if (EV && A.eflag) esum = radd(esum, phi);
         if (EV && A.vflag) {
-          vsum[0] += dx * dx * fpair;
-          vsum[1] += dy * dy * fpair;
-          vsum[2] += dz * dz * fpair;
-          vsum[3] += dx * dy * fpair;
-          vsum[4] += dx * dz * fpair;
-          vsum[5] += dy * dz * fpair;
+          vsum[0] = radd(vsum[0], rmul(rmul(dx, dx), fpair));
+          vsum[1] = radd(vsum[1], rmul(rmul(dy, dy), fpair));
+          vsum[2] = radd(vsum[2], rmul(rmul(dz, dz), fpair));
+          vsum[3] = radd(vsum[3], rmul(rmul(dx, dy), fpair));
+          vsum[4] = radd(vsum[4], rmul(rmul(dx, dz), fpair));
+          vsum[5] = radd(vsum[5], rmul(rmul(dy, dz), fpair));
         }
       }
     };
