@@ -380,23 +380,6 @@ __device__ __forceinline__ int next_item(int *counter) {
   return it;
 }
 
-// Single systems: the force-only passes over SM-local runs of list slots
-// (sm_run, device.cuh); each slot is computed by the same function as in the
-// grid launch, so the results are the grid launch's bit for bit.
-template <int TB>
-__global__ void __launch_bounds__(TB, 1024 / TB) k_eam_rho32_sm(Args32 A, Eam32 T, double *rho_out,
-                                                         double *phi_site, int4 *pos_w, int *cnt, int nsm) {
-  __shared__ int v;
-  if (threadIdx.x == 0) v = sm_id() % nsm;
-  const int nrun = (A.nsi + TB - 1) / TB;
-  for (;;) {
-    const int r = sm_run(cnt, nsm, nrun, v);
-    if (r < 0) return;
-    const int t = r * TB + threadIdx.x;
-    if (t < A.nsi) rho32_slot(A, T, t, rho_out, phi_site, pos_w);
-  }
-}
-
 template <int TB>
 __global__ void __launch_bounds__(TB, 1024 / TB) k_eam_rho32_queue(Args32 A, Eam32 T, double *rho_out,
                                                             double *phi_site, int4 *pos_w, const int2 *items,
@@ -512,26 +495,6 @@ __global__ void __launch_bounds__(TB, 1024 / TB) k_eam_force32_queue(Args32 A, E
   }
 }
 
-template <int TB>
-__global__ void __launch_bounds__(TB, 1024 / TB) k_eam_force32_sm(Args32 A, Eam32 T, const double *phi_site,
-                                                           int *cnt, int nsm) {
-  __shared__ int v;
-  if (threadIdx.x == 0) v = sm_id() % nsm;
-  const int nrun = (A.nsi + TB - 1) / TB;
-  for (;;) {
-    const int r = sm_run(cnt, nsm, nrun, v);
-    if (r < 0) return;
-    const int t = r * TB + threadIdx.x;
-    if (t < A.nsi) {
-      const int i = site_of_slot(A, t);
-      float fi[3] = {0, 0, 0}, esum = 0.f, vsum[6] = {0, 0, 0, 0, 0, 0};
-      double eemb_site = 0.0, eemb_global = 0.0;
-      force32_slot<false>(A, T, t, i, phi_site, fi, esum, vsum, eemb_site, eemb_global);
-      finish32(A, i, true, fi, false, esum, vsum, eemb_site, eemb_global);
-    }
-  }
-}
-
 __global__ void k_reduce_partials32(const double *partial, int nblocks, double *out) {
   int k = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (k >= 7) return;
@@ -610,15 +573,6 @@ std::vector<int2> make_items(const Ctx &c, const int tile[3], int only_class) {
     for (int o = 0; o < ng; o += T) items.push_back(make_int2(g0 + o, std::min(T, ng - o)));
   }
   return items;
-}
-
-int sm_grid(const Ctx &c) {
-  static const int per_sm = [] {
-    int b = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_eam_force32_sm<128>, 128, 0);
-    return b > 0 ? b : 1;
-  }();
-  return per_sm * c.num_sms;
 }
 
 int queue_grid(const Ctx &c) {
@@ -726,20 +680,7 @@ void pair_compute_mixed(Ctx &c, int eflag, int vflag) {
     cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
     CACB200_CUDA(cudaStreamIsCapturing(c.stream, &cs));
     bool queue = c.nrep > 1 && c.work_queue;
-    // single systems: the force-only passes over SM-local runs
-    const bool smq = c.nrep == 1 && c.work_queue;
     c.work_counter.reserve(2);
-    c.sm_counter.reserve(2 * c.num_sms);
-    auto rho_s = [&] {
-      CACB200_CUDA(cudaMemsetAsync(c.sm_counter.p, 0, sizeof(int) * c.num_sms, c.stream));
-      k_eam_rho32_sm<128><<<sm_grid(c), 128, 0, c.stream>>>(A, Tb, c.rho.p, c.phi_site.p, c.pos32.p,
-                                                             c.sm_counter.p, c.num_sms);
-    };
-    auto force_s = [&] {
-      CACB200_CUDA(cudaMemsetAsync(c.sm_counter.p + c.num_sms, 0, sizeof(int) * c.num_sms, c.stream));
-      k_eam_force32_sm<128><<<sm_grid(c), 128, 0, c.stream>>>(A, Tb, c.phi_site.p, c.sm_counter.p + c.num_sms,
-                                                               c.num_sms);
-    };
     auto rho_q = [&] {
       CACB200_CUDA(cudaMemsetAsync(c.work_counter.p, 0, sizeof(int), c.stream));
       k_eam_rho32_queue<128><<<queue_grid(c), 128, 0, c.stream>>>(A, Tb, c.rho.p, c.phi_site.p, c.pos32.p,
@@ -791,7 +732,7 @@ void pair_compute_mixed(Ctx &c, int eflag, int vflag) {
     if (queue && c.work_gen != c.gen) queue = false;
     // block sizes of the force-only passes chosen by timing on first use (as
     // in the FP64 form; results do not depend on them)
-    if (!queue && !smq && c.tune_gen32 != c.gen && !ev && cs == cudaStreamCaptureStatusNone) {
+    if (!queue && c.tune_gen32 != c.gen && !ev && cs == cudaStreamCaptureStatusNone) {
       const int cand[3] = {128, 64, 256};   // another size replaces 128 only when >= 3 % faster
       cudaEvent_t e0, e1;
       CACB200_CUDA(cudaEventCreate(&e0));
@@ -828,7 +769,6 @@ void pair_compute_mixed(Ctx &c, int eflag, int vflag) {
     {
       KernelTimer t(c, "eam_rho32");
       if (queue) rho_q();
-      else if (smq) rho_s();
       else rho(c.tb_rho32);
     }
     if (c.ne) {
@@ -839,7 +779,6 @@ void pair_compute_mixed(Ctx &c, int eflag, int vflag) {
       KernelTimer t(c, "eam_force32");
       if (ev) k_eam_force32<128, true><<<nb, T, 0, c.stream>>>(A, Tb, c.phi_site.p);
       else if (queue) force_q();
-      else if (smq) force_s();
       else force(c.tb_force32);
     }
   }

@@ -423,12 +423,13 @@ int cacb200_pair_blocks(cacb200_ctx *ctx, int *rho_threads, int *force_threads);
  * 128, 512 or 2048 slots) is chosen per replica size class (i-sites below
  * 8,192, below 32,768, larger) by timing the force pass when the capacity
  * plan changes; results do not depend on it (each slot's arithmetic is that
- * of the grid launch).  Single systems in the mixed form run the force-only
- * EAM passes over SM-local runs instead: the list slots are cut into runs of
- * 128 and each multiprocessor owns a contiguous range of runs, so the blocks
- * resident on one multiprocessor share their neighbours' records in its L1;
- * a block whose own range is exhausted takes runs from another range (same
- * results as the grid launch, bit for bit).  enable: 1 on (default), 0 off
+ * of the grid launch).  Single systems run the atom-list build, and in the
+ * FP64 form the force-only EAM passes, over SM-local runs instead: the cells
+ * or list slots are cut into runs (one cell; 128 slots) and each
+ * multiprocessor owns a contiguous range of runs, so the blocks resident on
+ * one multiprocessor share their neighbours' data in its L1; a block whose
+ * own range is exhausted takes runs from another range (same lists and
+ * results as the grid launches, bit for bit).  enable: 1 on (default), 0 off
  * (one grid launch per pass), -1 unchanged; tiles [3] gets the chosen tiles
  * of batches (0: not chosen yet).  No reference counterpart (the reference
  * runs one system per process). */

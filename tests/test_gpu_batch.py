@@ -133,10 +133,11 @@ def test_work_queue_launches_equal_grid_launches(tmp_path):
 
 @pytest.mark.parametrize("form,strain", [(0, 0.0), (1, 0.0), (1, 0.03)])
 def test_sm_local_runs_equal_grid_launches(form, strain, tmp_path):
-    """A single system runs the atom-list build and the force-only EAM passes
-    over SM-local runs of cells and list slots (work queue on, the default);
-    the lists, forces and trajectory equal those of the grid launches (work
-    queue off) bit for bit, over steps with rebuilds (FP64 and mixed)."""
+    """A single system runs the atom-list build, and in the FP64 form the
+    force-only EAM passes, over SM-local runs of cells and list slots (work
+    queue on, the default); the lists, forces and trajectory equal those of
+    the grid launches (work queue off) bit for bit, over steps with rebuilds
+    (FP64 and mixed)."""
     from cac_b200.api import Engine
     s = gen.build_slab(6, 3, 8, 24, temperature=300.0, strain=strain, seed=14)
     out = []
