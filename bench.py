@@ -337,9 +337,10 @@ def alg_bytes_per_site(kernel: str) -> int:
 # slab, where the whole working set exceeds L2; the list stream grows with the
 # sites, so the per-site figure carries over to larger systems of the same
 # lattice.
-# ncu dram read + write per launch of the force pass on the 313,120-site slab
-# (profiles/): FP64 with the inner list prefix; mixed form
-TRAFFIC_PER_SITE = {"eam_force": 112.05e6 / 313120, "eam_force32": 122.8e6 / 313120}
+# ncu dram read + write per launch on the 313,120-site slab (profiles/):
+# the FP64 force pass (SM-local form), the mixed force and density passes
+TRAFFIC_PER_SITE = {"eam_force": 110.80e6 / 313120, "eam_force32": 92.55e6 / 313120,
+                    "eam_rho32": 92.36e6 / 313120}
 
 
 def stream_bytes(kernel: str, na: int, ne: int, nact: int, mixed: bool = False) -> int:
