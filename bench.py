@@ -28,10 +28,11 @@ step).  value = atom+IP sites x steps / device time (max over ranks).
 
 The K timed steps run as trajectories of at most ``--segment`` (50) steps,
 each restarted from the seeded initial state on the device (state restore,
-list build and a force evaluation).  The first trajectory's setup happens
-before the timer starts, as the reference's "Loop time" starts after its
-Verlet::setup; the restarts of later trajectories are inside the timed
-region.  The reference's own dynamics on these systems gain energy without
+list build and a force evaluation).  Each trajectory's steps are timed on
+the device between CUDA events and the K steps' time is their sum: every
+set-up (the first before the timed region, the restarts between the
+segments) stays outside, as the reference's "Loop time" of each run starts
+after its Verlet::setup.  The reference's own dynamics on these systems gain energy without
 bound (its total energy rises by thousands of eV within 300 steps, LJ and EAM
 alike), so long trajectories stop being physical; the restarts keep the
 timed work on physical configurations.
@@ -401,6 +402,7 @@ def pipe_peak(fp64: bool, device: int) -> float:
 
 
 WORK_QUEUE = True   # --work-queue: persistent launches of the mixed EAM passes
+PREFIX_MARGIN = None   # --prefix-margin: inner list prefix margin (A; default 0.4 x skin)
 
 
 def make_engine(s, pair, form: str, local: int, setfl: str, fix: str):
@@ -419,6 +421,8 @@ def make_engine(s, pair, form: str, local: int, setfl: str, fix: str):
     eng.set_precision(api.MIXED if form == "mixed" else api.FP64)
     eng.neighbor(1.0, 10)
     eng.work_queue(WORK_QUEUE)
+    if PREFIX_MARGIN is not None:
+        eng.list_prefix(PREFIX_MARGIN)
     if fix == "langevin":
         eng.langevin(300.0, 300.0, 0.1, 4928459)
     elif fix == "deform":
@@ -444,22 +448,38 @@ class Trajectories:
             self.eng.set_box(*self.box0)
         self.eng.setup()
 
-    def run(self, nsteps: int):
-        done = 0
+    def run(self, nsteps: int, stream=None):
+        """nsteps in segments; with a stream, each segment's steps are
+        bracketed by CUDA events on it and the summed device time (ms) is
+        returned: the set-up of a later segment (restore, lists, forces) is
+        left out, as the reference leaves Verlet::setup out of each run's
+        Loop time."""
+        import torch
+        done, ms = 0, 0.0
         while done < nsteps:
             if done:
                 self.prepare()
             k = min(self.seg, nsteps - done)
+            if stream is not None:
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
             self.eng.run_nve(k, 0.001)
+            if stream is not None:
+                e1.record(stream)
+                e1.synchronize()
+                ms += e0.elapsed_time(e1)
             done += k
+        return ms
 
 
 def timed_region(eng, tr: Trajectories, steps: int, warmup: int, local: int, dist, clocks: bool):
     """W warm-up steps, then K steps between barriers and synchronisations,
     timed with CUDA events on the context's stream; (slowest rank's ms, clock
-    summary or None).  The timed run starts from a state set up before the
+    summary or None).  Every segment starts from a state set up outside its
     timer (lists and forces of the seeded state), as the reference's Loop
-    time starts after Verlet::setup; restarts of later segments are timed."""
+    time of each run starts after Verlet::setup; the K steps' device time is
+    the sum over the segments."""
     import torch
     stream = torch.cuda.ExternalStream(eng.stream, device=torch.device("cuda", local))
     tr.run(warmup)
@@ -467,8 +487,6 @@ def timed_region(eng, tr: Trajectories, steps: int, warmup: int, local: int, dis
     torch.cuda.synchronize(local)
     if dist:
         dist.barrier()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
     clk = ClockSampler(local) if clocks else None
     if clk:
         clk.__enter__()
@@ -476,16 +494,13 @@ def timed_region(eng, tr: Trajectories, steps: int, warmup: int, local: int, dis
         torch.cuda.synchronize(local)
         if dist:
             dist.barrier()
-        e0.record(stream)
-        tr.run(steps)
-        e1.record(stream)
+        ms = tr.run(steps, stream)
         torch.cuda.synchronize(local)
         if dist:
             dist.barrier()
     finally:
         if clk:
             clk.__exit__(None, None, None)
-    ms = e0.elapsed_time(e1)
     return max_over_ranks(ms, dist, torch.device("cuda", local)), (clk.summary() if clk else None)
 
 
@@ -678,7 +693,7 @@ def b200_arm(args, rank, local, ws, dist):
                        "fix": {"none": "nve", "langevin": "nve + langevin 300 300 0.1",
                                "deform": "nve + deform 1 x erate 0.1 y volume"}[args.fix],
                        "l2": "working set larger than L2 (site table + lists > 126 MB)",
-                       "work_queue": WORK_QUEUE},
+                       "work_queue": WORK_QUEUE, "prefix_margin": PREFIX_MARGIN},
             "fp64": fp64_entry,
             "mixed_over_fp64": (value / fp64_entry["value"]) if fp64_entry else None,
             "accuracy": accuracy,
@@ -939,9 +954,12 @@ def main():
     ap.add_argument("--work-queue", default="on", choices=["on", "off"],
                     help="mixed EAM passes as persistent launches (batches: work items per replica; "
                          "single systems: SM-local runs of list slots) or one grid launch per pass")
+    ap.add_argument("--prefix-margin", type=float, default=None,
+                    help="margin of the lists' inner prefix in A (default: the library's, 0.4 x skin; 0: off)")
     args = ap.parse_args()
-    global WORK_QUEUE
+    global WORK_QUEUE, PREFIX_MARGIN
     WORK_QUEUE = args.work_queue == "on"
+    PREFIX_MARGIN = args.prefix_margin
     rank, local, ws, dist = dist_init()
     try:
         if args.impl == "reference":
