@@ -402,7 +402,7 @@ def pipe_peak(fp64: bool, device: int) -> float:
 
 
 WORK_QUEUE = True   # --work-queue: persistent launches of the mixed EAM passes
-PREFIX_MARGIN = None   # --prefix-margin: inner list prefix margin (A; default 0.4 x skin)
+PREFIX_MARGIN = None   # --prefix-margin: inner list prefix margin (A; default 0.5 x skin)
 
 
 def make_engine(s, pair, form: str, local: int, setfl: str, fix: str):
@@ -955,7 +955,7 @@ def main():
                     help="mixed EAM passes as persistent launches (batches: work items per replica; "
                          "single systems: SM-local runs of list slots) or one grid launch per pass")
     ap.add_argument("--prefix-margin", type=float, default=None,
-                    help="margin of the lists' inner prefix in A (default: the library's, 0.4 x skin; 0: off)")
+                    help="margin of the lists' inner prefix in A (default: the library's, 0.5 x skin; 0: off)")
     args = ap.parse_args()
     global WORK_QUEUE, PREFIX_MARGIN
     WORK_QUEUE = args.work_queue == "on"

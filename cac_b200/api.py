@@ -298,7 +298,7 @@ class Engine:
                     "set_neighbor_modify")
 
     def list_prefix(self, margin: float) -> None:
-        """Inner-prefix margin of the lists (< 0: default 0.4 x skin, 0: off)."""
+        """Inner-prefix margin of the lists (< 0: default 0.5 x skin, 0: off)."""
         self._check(self.lib.cacb200_set_list_prefix(self.h, margin), "set_list_prefix")
 
     def graphs(self, enable: bool) -> None:

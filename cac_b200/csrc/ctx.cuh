@@ -277,7 +277,7 @@ struct Ctx {
   // while no site of the replica has moved inner_limit() since the build
   // (positions in xbuild / nodex_build), and the pair loops then stop at num_in
   double inner_margin = 0.4;
-  double inner_margin_set = -1.0;   // cacb200_set_list_prefix (< 0: 0.4 x skin)
+  double inner_margin_set = -1.0;   // cacb200_set_list_prefix (< 0: 0.5 x skin)
   DBuf<int> num_in, inner_ok;
   DBuf<double4> xbuild;
   DBuf<double> nodex_build;

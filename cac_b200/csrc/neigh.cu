@@ -1221,7 +1221,7 @@ void neigh_plan(Ctx &c, bool want_half) {
   c.eframe.reserve((size_t)std::max(c.ne, 1) * EFR);
   c.overflow.reserve(16);
   c.dev_nact.reserve(1);
-  c.inner_margin = c.inner_margin_set >= 0.0 ? c.inner_margin_set : 0.4 * c.skin;
+  c.inner_margin = c.inner_margin_set >= 0.0 ? c.inner_margin_set : 0.5 * c.skin;
   c.inner_ok.reserve(c.nrep);
   c.xbuild.reserve(std::max(c.na, 1));
   c.nodex_build.reserve(24 * (size_t)std::max(c.ne, 1));

@@ -235,7 +235,7 @@ int cacb200_set_neighbor_modify(cacb200_ctx *ctx, int delay, int check);
  * build are stored first, and while no site has moved half the margin since
  * the build the pair loops stop after them; every pair inside the cutoff is
  * in the prefix in the same order, so forces and energies are those of the
- * whole lists bit for bit.  margin < 0: 0.4 x skin (default); 0: always the
+ * whole lists bit for bit.  margin < 0: 0.5 x skin (default); 0: always the
  * whole lists.  Takes effect at the next list build. */
 int cacb200_set_list_prefix(cacb200_ctx *ctx, double margin);
 /* Bin and build the lists now (Neighbor::build, neighbor.cpp:1704-1876).
