@@ -3,6 +3,7 @@
 
 #include <cuda_runtime.h>
 
+#include <cmath>
 #include <cstdint>
 #include <functional>
 #include <stdexcept>
@@ -273,12 +274,20 @@ struct Ctx {
   DBuf<int> nbr_full, num_full;
   DBuf<int2> site_from;
   DBuf<unsigned char> ecell_near;   // single systems: element cells with an element in their 27-cell block          // per slot: rows of each segment before its element-site entries
-  // inner prefix of the full lists: inner_ok[replica] (device) is nonzero
-  // while no site of the replica has moved inner_limit() since the build
-  // (positions in xbuild / nodex_build), and the pair loops then stop at num_in
-  double inner_margin = 0.4;
+  // inner prefix of the full lists (entries within cutoff + inner_margin at
+  // the build, rows [0, num_in)).  inner_ok[replica] (device) is nonzero
+  // until positions move other than by the drift (then every site walks its
+  // whole list until the next build); while it is set, the drift keeps each
+  // site's displacement since the build (xbuild / nodex_build): disp per
+  // atom, edisp per element (its largest node displacement, which bounds
+  // every lattice site of the element), dmax per replica (the largest of
+  // all, as float bits), and a site walks the rest of its list only when
+  // its displacement plus dmax could close the margin (PrefixRule)
+  double inner_margin = 0.5;
   double inner_margin_set = -1.0;   // cacb200_set_list_prefix (< 0: 0.5 x skin)
   DBuf<int> num_in, inner_ok;
+  DBuf<float> disp, edisp;
+  DBuf<unsigned> dmax;
   DBuf<double4> xbuild;
   DBuf<double> nodex_build;
   DBuf<int> nbr_half, num_half;
@@ -371,6 +380,32 @@ struct Ctx {
 // holds every pair inside the cutoff: half the margin, less an allowance for
 // the FP32 screen of the build's classification.
 inline double inner_limit(const Ctx &c) { return 0.5 * (c.inner_margin - 1e-3); }
+
+// The per-site prefix rule as the pair kernels see it.  A pair (i, j) kept
+// out of the prefix was at least cutoff + margin apart at the build (less
+// the FP32 screen's allowance), so it is still outside the cutoff while
+// disp_i + disp_j <= margin less that allowance; disp_j <= dmax.  Site i
+// (site-table index) walks its whole list when its replica's flag is clear
+// or disp_i + dmax exceeds lim.
+struct PrefixRule {
+  const int *inner_ok;
+  const float *disp, *edisp;
+  const unsigned *dmax;
+  float lim;
+  int na;
+};
+
+inline PrefixRule prefix_rule(const Ctx &c) {
+  PrefixRule r;
+  r.inner_ok = c.inner_ok.p;
+  r.disp = c.disp.p;
+  r.edisp = c.edisp.p;
+  r.dmax = c.dmax.p;
+  // twice the per-site allowance of inner_limit, rounded down
+  r.lim = std::nextafter((float)(c.inner_margin - 2e-3), 0.0f);
+  r.na = c.na;
+  return r;
+}
 
 // Positions moved by something other than the checked drift: the pair loops
 // use the whole lists until the next build.

@@ -173,4 +173,12 @@ __device__ __forceinline__ int sm_run(int *cnt, int nsm, int nrun, int &v) {
   return got;
 }
 
+// PrefixRule (ctx.cuh) for list site i (site-table index) of replica rep:
+// does it walk the rest of its list?  The sum is rounded up.
+__device__ __forceinline__ bool walk_rest(const PrefixRule &p, int i, int rep) {
+  if (!p.inner_ok[rep]) return true;
+  const float d = i < p.na ? p.disp[i] : p.edisp[(i - p.na) / NG];
+  return __fadd_ru(d, __uint_as_float(p.dmax[rep])) > p.lim;
+}
+
 }  // namespace cacb200

@@ -89,15 +89,21 @@ __global__ void k_assemble(const double *gaussf, double *nodef, int ne) {
 }
 
 // FixNVE::initial_integrate (fix_nve.cpp:62-145): half kick and drift for
-// atoms (positions live in the site table) and nodes.  The drift also tests
-// the displacement since the last list build: an atom farther than `lim`
-// (a node component farther than lim / sqrt 3, which bounds every lattice
-// site of its element) ends the inner-prefix shortcut until the next build.
-__global__ void k_nve_initial(double4 *xs, double *v, const double *f, int na, double *nodex,
-                              double *nodev, const double *nodef, int nn3, double dtfm, double dtv,
-                              const double4 *xb, const double *nxb, int *inner_ok, double lim2, double limc,
+// atoms (positions live in the site table; threads [0, na)) and nodes (one
+// thread per node from napad, a multiple of 32, so that every warp holds
+// whole elements).  With xb, the drift also records each site's distance
+// from where the lists were built, rounded up, for the prefix rule
+// (PrefixRule, ctx.cuh): disp per atom, edisp per element (its largest node
+// displacement), and the largest of all per replica into dmax (cleared
+// before the launch; non-negative floats as bits, whose integer order is
+// theirs).
+__global__ void k_nve_initial(double4 *xs, double *v, const double *f, int na, int napad, double *nodex,
+                              double *nodev, const double *nodef, int nnode, double dtfm, double dtv,
+                              const double4 *xb, const double *nxb, float *disp, float *edisp, unsigned *dmax,
                               const int *site_rep, const int *elem_rep) {
-  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  float d = 0.0f;
+  int rep = 0;
   if (t < na) {
     double4 p = xs[t];
     double *vi = v + 3 * (size_t)t;
@@ -116,17 +122,63 @@ __global__ void k_nve_initial(double4 *xs, double *v, const double *f, int na, d
     if (xb) {
       const double4 b = xb[t];
       const double dx = p.x - b.x, dy = p.y - b.y, dz = p.z - b.z;
-      if (dx * dx + dy * dy + dz * dz > lim2) inner_ok[site_rep ? site_rep[t] : 0] = 0;
+      d = __double2float_ru(__dsqrt_ru(__dadd_ru(__dadd_ru(__dmul_ru(dx, dx), __dmul_ru(dy, dy)), __dmul_ru(dz, dz))));
+      disp[t] = d;
+      if (site_rep) rep = site_rep[t];
     }
-    return;
+  } else if (t >= napad) {
+    const int k = t - napad;   // node 8 e + n of element e
+    if (k < nnode) {
+      double dd = 0.0;
+#pragma unroll
+      for (int c = 0; c < 3; c++) {
+        const size_t m = 3 * (size_t)k + c;
+        const double vn = __dadd_rn(nodev[m], __dmul_rn(dtfm, nodef[m]));
+        nodev[m] = vn;
+        const double xn = __dadd_rn(nodex[m], __dmul_rn(dtv, vn));
+        nodex[m] = xn;
+        if (nxb) {
+          const double e = xn - nxb[m];
+          dd = __dadd_ru(dd, __dmul_ru(e, e));
+        }
+      }
+      if (nxb) {
+        d = __double2float_ru(__dsqrt_ru(dd));
+        if (elem_rep) rep = elem_rep[k / 8];
+      }
+    }
+    if (nxb) {
+      // the element's largest node displacement over its 8 lanes
+      float m = d;
+      m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, 4));
+      m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, 2));
+      m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, 1));
+      if ((k & 7) == 0 && k < nnode) edisp[k / 8] = m;
+    }
   }
-  int k = t - na;
-  if (k >= nn3) return;
-  double vn = __dadd_rn(nodev[k], __dmul_rn(dtfm, nodef[k]));
-  nodev[k] = vn;
-  const double xn = __dadd_rn(nodex[k], __dmul_rn(dtv, vn));
-  nodex[k] = xn;
-  if (nxb && fabs(xn - nxb[k]) > limc) inner_ok[elem_rep ? elem_rep[k / 24] : 0] = 0;
+  if (!dmax) return;
+  const unsigned bits = __float_as_uint(d);
+  if (!site_rep) {
+    // one system: the block's largest, one atomic per block
+    __shared__ unsigned wmax[32];
+    const unsigned m = __reduce_max_sync(0xffffffffu, bits);
+    if ((threadIdx.x & 31) == 0) wmax[threadIdx.x >> 5] = m;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      unsigned mm = 0;
+      for (int w = 0; w < (int)(blockDim.x >> 5); w++) mm = max(mm, wmax[w]);
+      if (mm) atomicMax(dmax, mm);
+    }
+  } else {
+    // a batch: one atomic per warp when its sites share a replica
+    const int r0 = __shfl_sync(0xffffffffu, rep, 0);
+    if (__all_sync(0xffffffffu, rep == r0)) {
+      const unsigned m = __reduce_max_sync(0xffffffffu, bits);
+      if ((threadIdx.x & 31) == 0 && m) atomicMax(dmax + r0, m);
+    } else if (bits) {
+      atomicMax(dmax + rep, bits);
+    }
+  }
 }
 
 // FixNVE::final_integrate (fix_nve.cpp:148-219)
@@ -165,15 +217,17 @@ void nve_initial(Ctx &c, double dt) {
   c.forces_current = false;   // the drift moves every site
   double dtf = 0.5 * dt * (1.0 / 1.0364269e-4);   // metal units, update.cpp:161-164
   double dtfm = dtf / c.mass;
-  int n = c.na + 24 * c.ne;
-  if (n == 0) return;
+  if (c.na + c.ne == 0) return;
   KernelTimer t(c, "nve_initial");
-  const bool check = c.lists_valid && c.inner_ok.p && c.xbuild.p && inner_limit(c) > 0.0;
-  const double lim = inner_limit(c);
+  const bool check = c.lists_valid && c.inner_ok.p && c.xbuild.p && c.disp.p && inner_limit(c) > 0.0;
+  if (check) CACB200_CUDA(cudaMemsetAsync(c.dmax.p, 0, sizeof(unsigned) * c.nrep, c.stream));
+  const int napad = (c.na + 31) & ~31;
+  const long n = (long)napad + 8L * c.ne;
+  const bool many = c.nrep > 1;
   k_nve_initial<<<nblk(n, 256), 256, 0, c.stream>>>(
-      c.xs.p, c.v.p, c.f.p, c.na, c.nodex.p, c.nodev.p, c.nodef.p, 24 * c.ne, dtfm, dt,
-      check ? c.xbuild.p : nullptr, check ? c.nodex_build.p : nullptr, c.inner_ok.p, lim * lim,
-      lim / 1.7320508075688772, c.nrep > 1 ? c.site_rep.p : nullptr, c.nrep > 1 ? c.elem_rep.p : nullptr);
+      c.xs.p, c.v.p, c.f.p, c.na, napad, c.nodex.p, c.nodev.p, c.nodef.p, 8 * c.ne, dtfm, dt,
+      check ? c.xbuild.p : nullptr, check ? c.nodex_build.p : nullptr, c.disp.p, c.edisp.p,
+      check ? c.dmax.p : nullptr, many ? c.site_rep.p : nullptr, many ? c.elem_rep.p : nullptr);
 }
 
 // Neighbor::check_distance (neighbor.cpp:1617-1683): does any atom or node

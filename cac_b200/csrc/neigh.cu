@@ -1223,6 +1223,9 @@ void neigh_plan(Ctx &c, bool want_half) {
   c.dev_nact.reserve(1);
   c.inner_margin = c.inner_margin_set >= 0.0 ? c.inner_margin_set : 0.5 * c.skin;
   c.inner_ok.reserve(c.nrep);
+  c.disp.reserve(std::max(c.na, 1));
+  c.edisp.reserve(std::max(c.ne, 1));
+  c.dmax.reserve(c.nrep);
   c.xbuild.reserve(std::max(c.na, 1));
   c.nodex_build.reserve(24 * (size_t)std::max(c.ne, 1));
   c.num_in.reserve(std::max(c.nsite_i(), 1));
@@ -1402,6 +1405,10 @@ void neigh_build_async(Ctx &c, bool want_half) {
       CACB200_CUDA(cudaMemcpyAsync(c.nodex_build.p, c.nodex.p, sizeof(double) * 24 * c.ne,
                                    cudaMemcpyDeviceToDevice, c.stream));
     CACB200_CUDA(cudaMemsetAsync(c.inner_ok.p, inner_limit(c) > 0.0 ? 1 : 0, sizeof(int) * c.nrep, c.stream));
+    // every site is where the lists are built from
+    if (c.na) CACB200_CUDA(cudaMemsetAsync(c.disp.p, 0, sizeof(float) * c.na, c.stream));
+    if (c.ne) CACB200_CUDA(cudaMemsetAsync(c.edisp.p, 0, sizeof(float) * c.ne, c.stream));
+    CACB200_CUDA(cudaMemsetAsync(c.dmax.p, 0, sizeof(unsigned) * c.nrep, c.stream));
     {
       KernelTimer t(c, "bin");
       size_t bytes = c.cub_bytes;

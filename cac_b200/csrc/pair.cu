@@ -34,7 +34,7 @@ struct PairArgs {
   const int *nbr;                   // lists and counts indexed by list slot
   const int *num;
   const int *num_in;                // inner prefix length of each list ...
-  const int *inner_ok;              // ... usable while this is nonzero (per replica)
+  PrefixRule prefix;                // ... and the rule for walking the rest
   const int *slot_atom;             // list slot -> atom (slots past the atoms are Gauss points)
   int na, ne, nsi;
   int cap;                          // list rows: the rest of a list fills its last rows
@@ -110,18 +110,19 @@ __device__ __forceinline__ void for_each_neighbour(const PairArgs &A, int i, con
 }
 
 // A site's list in two walks: the inner prefix (entries within the cutoff
-// plus a margin at the build, the list's first rows), then, unless no site
-// has moved half the margin since the build, the rest (the list's last
-// rows).  Each entry's arithmetic depends on its place in the walk (the
+// plus a margin at the build, the list's first rows), then, unless the
+// site's displacement since the build and the largest one cannot close the
+// margin (walk_rest, device.cuh), the rest (the list's last rows).  Each entry's arithmetic depends on its place in the walk (the
 // compiler may fuse multiply-adds differently in the grouped and the
 // remainder loop), so the prefix is always walked on its own: the sums are
 // the same whether the rest is walked or not.
-// The prefix flag belongs to the site's replica (one hot replica of a batch
-// does not end the shortcut for the others); one copy of the walk serves both
-// segments, which keeps the register count of the unrolled body.
+// The rule's flag and largest displacement belong to the site's replica (one
+// hot replica of a batch does not end the shortcut for the others); one copy
+// of the walk serves both segments, which keeps the register count of the
+// unrolled body.
 template <bool MANY, class F>
 __device__ __forceinline__ void walk_list(const PairArgs &A, int i, const int *nb, int n_in, int n, F &&f) {
-  const bool rest = n > n_in && !A.inner_ok[MANY ? A.site_rep[i] : 0];
+  const bool rest = n > n_in && walk_rest(A.prefix, i, MANY ? A.site_rep[i] : 0);
 #pragma unroll 1
   for (int seg = 0; seg < (rest ? 2 : 1); seg++)
     for_each_neighbour<MANY>(A, i, seg ? nb + (size_t)(A.cap - (n - n_in)) * A.nsi : nb, seg ? n - n_in : n_in,
@@ -563,7 +564,7 @@ void pair_compute(Ctx &c, int eflag, int vflag) {
   A.nbr = c.nbr_full.p;
   A.num = c.num_full.p;
   A.num_in = c.num_in.p;
-  A.inner_ok = c.inner_ok.p;
+  A.prefix = prefix_rule(c);
   A.slot_atom = c.slot_atom.p;
   A.na = c.na;
   A.ne = c.ne;

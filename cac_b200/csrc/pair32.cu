@@ -118,7 +118,7 @@ struct Args32 {
   const int *nbr;          // lists and counts indexed by list slot
   const int *num;
   const int *num_in;                // inner prefix length of each list ...
-  const int *inner_ok;              // ... usable while this is nonzero (per replica)
+  PrefixRule prefix;                // ... and the rule for walking the rest
   const int *slot_atom;    // list slot -> atom (slots past the atoms are Gauss points)
   int na, ne, nsi;
   int cap;                 // list rows: the rest of a list fills its last rows
@@ -198,14 +198,15 @@ __device__ __forceinline__ void walk32(const Args32 &A, const SiteFix &fx, const
 }
 
 // A site's list: the inner prefix on its own, then the rest unless the
-// prefix still holds every pair inside the cutoff (an entry's arithmetic
-// depends on its place in a walk, so the prefix is always walked alone).
+// prefix still holds every pair of the site inside the cutoff (walk_rest,
+// device.cuh; an entry's arithmetic depends on its place in a walk, so the
+// prefix is always walked alone).
 template <class F>
 __device__ __forceinline__ void for_each32(const Args32 &A, int t, int i, const int4 &oi, F &&f) {
   const SiteFix fx = site_fix(A, i);
   const int n_in = A.num_in[t], n = A.num[t];
   const int *nb = A.nbr + t;
-  const bool rest = n > n_in && !A.inner_ok[A.G.reps ? A.G.site_rep[i] : 0];
+  const bool rest = n > n_in && walk_rest(A.prefix, i, A.G.reps ? A.G.site_rep[i] : 0);
 #pragma unroll 1
   for (int seg = 0; seg < (rest ? 2 : 1); seg++)
     walk32(A, fx, oi, seg ? nb + (size_t)(A.cap - (n - n_in)) * A.nsi : nb, seg ? n - n_in : n_in, f);
@@ -605,7 +606,7 @@ void pair_compute_mixed(Ctx &c, int eflag, int vflag) {
   A.nbr = c.nbr_full.p;
   A.num = c.num_full.p;
   A.num_in = c.num_in.p;
-  A.inner_ok = c.inner_ok.p;
+  A.prefix = prefix_rule(c);
   A.slot_atom = c.slot_atom.p;
   A.na = c.na;
   A.ne = c.ne;

@@ -232,10 +232,13 @@ int cacb200_set_neighbor(cacb200_ctx *ctx, double skin, int every);
 int cacb200_set_neighbor_modify(cacb200_ctx *ctx, int delay, int check);
 /* The inner prefix of the lists (no reference counterpart; an evaluation
  * order, not a different result): entries within cutoff + margin at the
- * build are stored first, and while no site has moved half the margin since
- * the build the pair loops stop after them; every pair inside the cutoff is
- * in the prefix in the same order, so forces and energies are those of the
- * whole lists bit for bit.  margin < 0: 0.5 x skin (default); 0: always the
+ * build are stored first, and a site's pair loop stops after them while its
+ * own displacement since the build plus the largest displacement of its
+ * system cannot close the margin (the velocity-Verlet drift records them;
+ * other moves of the sites send every site to its whole list until the next
+ * build, and a FIRE move that takes a site half the margin away does too);
+ * every pair inside the cutoff is in the prefix in the same order, so forces
+ * and energies are those of the whole lists bit for bit.  margin < 0: 0.5 x skin (default); 0: always the
  * whole lists.  Takes effect at the next list build. */
 int cacb200_set_list_prefix(cacb200_ctx *ctx, double margin);
 /* Bin and build the lists now (Neighbor::build, neighbor.cpp:1704-1876).

@@ -1,11 +1,12 @@
 """The inner prefix of the neighbour lists (cacb200_set_list_prefix): entries
-within the cutoff plus a margin at the build come first, and the pair loops
-stop after them while no site has moved half the margin since the build.
+within the cutoff plus a margin at the build come first, and a site's pair
+loop stops after them while its own displacement since the build plus the
+largest one cannot close the margin.
 
 * Same state, same lists: forces with the prefix and with the whole lists
   are equal bit for bit (the prefix is walked on its own either way).
 * A hot system whose atoms outrun half the margin within a rebuild cycle:
-  the drift's displacement test switches to the whole lists, and the
+  the drift's displacements switch sites to their whole lists, and the
   trajectory follows the one with the prefix off to rounding (1e-9 A after
   20 steps; a neighbour missed near the cutoff would move atoms ~1e-4 A)."""
 import numpy as np
@@ -46,10 +47,15 @@ def test_prefix_and_whole_lists_equal_at_one_state(pair, form, tmp_path):
     assert np.array_equal(f1, f2) and np.array_equal(nf1, nf2) and np.array_equal(gf1, gf2)
 
 
-@pytest.mark.parametrize("pair,form,tol", [("lj", 0, 1e-9), ("eam", 0, 1e-9), ("eam", 1, 1e-5)])
-def test_hot_system_switches_to_whole_lists(pair, form, tol, tmp_path):
-    """(mixed form: FP32 sums in another order differ by FP32 rounding.)"""
-    s = gen.replica(3000, 60, temperature=3000.0, strain=0.0, seed=92)
+@pytest.mark.parametrize("pair,form,tol,temp", [("lj", 0, 1e-9, 3000.0), ("eam", 0, 1e-9, 3000.0),
+                                                ("eam", 1, 1e-5, 3000.0), ("eam", 0, 1e-9, 900.0),
+                                                ("lj", 0, 1e-9, 1500.0)])
+def test_hot_system_switches_to_whole_lists(pair, form, tol, temp, tmp_path):
+    """(mixed form: FP32 sums in another order differ by FP32 rounding.)
+    At 900 K and 1500 K the fastest sites pass half the margin while most
+    do not: each site's own displacement decides whether it walks its whole
+    list, and the trajectory still follows the prefix-off one."""
+    s = gen.replica(3000, 60, temperature=temp, strain=0.0, seed=92)
     out = []
     for margin in (-1.0, 0.0):
         e = make(s, pair, tmp_path, margin, form)
