@@ -280,19 +280,14 @@ struct Ctx {
   // whole list until the next build); while it is set, the drift keeps each
   // site's displacement since the build (xbuild / nodex_build): disp per
   // atom, edisp per element (its largest node displacement, which bounds
-  // every lattice site of the element), dmax[replica] the largest of all
-  // and dmax[nrep + replica] the largest of the elements (float bits); for
-  // a single system also cellmax, the largest atom displacement per atom
-  // cell of the build (atom_cell), and nbmax, the largest over each cell's
-  // 27-cell block.  A site walks the rest of its list only when its
-  // displacement plus the largest one its rest can hold could close the
-  // margin (PrefixRule)
+  // every lattice site of the element), dmax per replica (the largest of
+  // all, as float bits), and a site walks the rest of its list only when
+  // its displacement plus dmax could close the margin (PrefixRule)
   double inner_margin = 0.5;
   double inner_margin_set = -1.0;   // cacb200_set_list_prefix (< 0: 0.5 x skin)
   DBuf<int> num_in, inner_ok;
   DBuf<float> disp, edisp;
-  DBuf<unsigned> dmax, cellmax, nbmax;
-  DBuf<int> atom_cell;
+  DBuf<unsigned> dmax;
   DBuf<double4> xbuild;
   DBuf<double> nodex_build;
   DBuf<int> nbr_half, num_half;
@@ -389,23 +384,15 @@ inline double inner_limit(const Ctx &c) { return 0.5 * (c.inner_margin - 1e-3); 
 // The per-site prefix rule as the pair kernels see it.  A pair (i, j) kept
 // out of the prefix was at least cutoff + margin apart at the build (less
 // the FP32 screen's allowance), so it is still outside the cutoff while
-// disp_i + disp_j <= margin less that allowance.  Site i (site-table index)
-// walks its whole list when its replica's flag is clear or disp_i plus a
-// bound on disp_j exceeds lim.  The bound: for an atom of a single system,
-// the largest atom displacement over the 27 build cells around its own
-// (every atom of its list was in one of them at the build; cells are at
-// least cutoff + skin wide), and the largest element displacement when the
-// element walk found element boxes near it (nitems); otherwise the largest
-// displacement of its replica.
+// disp_i + disp_j <= margin less that allowance; disp_j <= dmax.  Site i
+// (site-table index) walks its whole list when its replica's flag is clear
+// or disp_i + dmax exceeds lim.
 struct PrefixRule {
   const int *inner_ok;
   const float *disp, *edisp;
-  const unsigned *dmax;        // [replica] all sites, [nrep + replica] elements
-  const unsigned *nbmax;       // single systems: per atom cell (else null)
-  const int *atom_cell;
-  const int *nitems;           // element items per list slot (null without elements)
+  const unsigned *dmax;
   float lim;
-  int na, nrep;
+  int na;
 };
 
 inline PrefixRule prefix_rule(const Ctx &c) {
@@ -414,10 +401,6 @@ inline PrefixRule prefix_rule(const Ctx &c) {
   r.disp = c.disp.p;
   r.edisp = c.edisp.p;
   r.dmax = c.dmax.p;
-  r.nbmax = (c.nrep == 1 && c.na) ? c.nbmax.p : nullptr;
-  r.atom_cell = c.atom_cell.p;
-  r.nitems = c.ne ? c.nitems.p : nullptr;
-  r.nrep = c.nrep;
   // twice the per-site allowance of inner_limit, rounded down
   r.lim = std::nextafter((float)(c.inner_margin - 2e-3), 0.0f);
   r.na = c.na;

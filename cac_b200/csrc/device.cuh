@@ -173,24 +173,12 @@ __device__ __forceinline__ int sm_run(int *cnt, int nsm, int nrun, int &v) {
   return got;
 }
 
-// PrefixRule (ctx.cuh) for list slot t, site i (site-table index) of
-// replica rep: does it walk the rest of its list?  The sum is rounded up.
-__device__ __forceinline__ bool walk_rest(const PrefixRule &p, int t, int i, int rep) {
+// PrefixRule (ctx.cuh) for list site i (site-table index) of replica rep:
+// does it walk the rest of its list?  The sum is rounded up.
+__device__ __forceinline__ bool walk_rest(const PrefixRule &p, int i, int rep) {
   if (!p.inner_ok[rep]) return true;
-  float d, bound;
-  if (i < p.na) {
-    d = p.disp[i];
-    if (p.nbmax) {
-      bound = __uint_as_float(p.nbmax[p.atom_cell[i]]);
-      if (p.nitems && p.nitems[t] > 0) bound = fmaxf(bound, __uint_as_float(p.dmax[p.nrep + rep]));
-    } else {
-      bound = __uint_as_float(p.dmax[rep]);
-    }
-  } else {
-    d = p.edisp[(i - p.na) / NG];
-    bound = __uint_as_float(p.dmax[rep]);
-  }
-  return __fadd_ru(d, bound) > p.lim;
+  const float d = i < p.na ? p.disp[i] : p.edisp[(i - p.na) / NG];
+  return __fadd_ru(d, __uint_as_float(p.dmax[rep])) > p.lim;
 }
 
 }  // namespace cacb200

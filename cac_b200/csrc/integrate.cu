@@ -100,7 +100,7 @@ __global__ void k_assemble(const double *gaussf, double *nodef, int ne) {
 __global__ void k_nve_initial(double4 *xs, double *v, const double *f, int na, int napad, double *nodex,
                               double *nodev, const double *nodef, int nnode, double dtfm, double dtv,
                               const double4 *xb, const double *nxb, float *disp, float *edisp, unsigned *dmax,
-                              unsigned *cellmax, const int *atom_cell, const int *site_rep, const int *elem_rep) {
+                              const int *site_rep, const int *elem_rep) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   float d = 0.0f;
   int rep = 0;
@@ -124,7 +124,6 @@ __global__ void k_nve_initial(double4 *xs, double *v, const double *f, int na, i
       const double dx = p.x - b.x, dy = p.y - b.y, dz = p.z - b.z;
       d = __double2float_ru(__dsqrt_ru(__dadd_ru(__dadd_ru(__dmul_ru(dx, dx), __dmul_ru(dy, dy)), __dmul_ru(dz, dz))));
       disp[t] = d;
-      if (cellmax && d > 0.0f) atomicMax(cellmax + atom_cell[t], __float_as_uint(d));
       if (site_rep) rep = site_rep[t];
     }
   } else if (t >= napad) {
@@ -160,24 +159,15 @@ __global__ void k_nve_initial(double4 *xs, double *v, const double *f, int na, i
   if (!dmax) return;
   const unsigned bits = __float_as_uint(d);
   if (!site_rep) {
-    // one system: the block's largest, of all sites (dmax[0]) and of the
-    // element nodes (dmax[1]), one atomic each per block
-    __shared__ unsigned wmax[32], wmaxe[32];
+    // one system: the block's largest, one atomic per block
+    __shared__ unsigned wmax[32];
     const unsigned m = __reduce_max_sync(0xffffffffu, bits);
-    const unsigned me = __reduce_max_sync(0xffffffffu, t >= napad ? bits : 0u);
-    if ((threadIdx.x & 31) == 0) {
-      wmax[threadIdx.x >> 5] = m;
-      wmaxe[threadIdx.x >> 5] = me;
-    }
+    if ((threadIdx.x & 31) == 0) wmax[threadIdx.x >> 5] = m;
     __syncthreads();
     if (threadIdx.x == 0) {
-      unsigned mm = 0, mme = 0;
-      for (int w = 0; w < (int)(blockDim.x >> 5); w++) {
-        mm = max(mm, wmax[w]);
-        mme = max(mme, wmaxe[w]);
-      }
+      unsigned mm = 0;
+      for (int w = 0; w < (int)(blockDim.x >> 5); w++) mm = max(mm, wmax[w]);
       if (mm) atomicMax(dmax, mm);
-      if (mme) atomicMax(dmax + 1, mme);
     }
   } else {
     // a batch: one atomic per warp when its sites share a replica
@@ -189,23 +179,6 @@ __global__ void k_nve_initial(double4 *xs, double *v, const double *f, int na, i
       atomicMax(dmax + rep, bits);
     }
   }
-}
-
-// Single systems: the largest atom displacement over each atom cell's
-// 27-cell block (periodic), for the prefix rule.
-__global__ void k_cell_nbmax(const unsigned *cellmax, int nx, int ny, int nz, unsigned *nbmax) {
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= nx * ny * nz) return;
-  const int x = c % nx, y = (c / nx) % ny, z = c / (nx * ny);
-  unsigned m = 0;
-  for (int dz = -1; dz <= 1; dz++) {
-    const int zz = (z + dz + nz) % nz;
-    for (int dy = -1; dy <= 1; dy++) {
-      const int yy = (y + dy + ny) % ny;
-      for (int dx = -1; dx <= 1; dx++) m = max(m, cellmax[(zz * ny + yy) * nx + (x + dx + nx) % nx]);
-    }
-  }
-  nbmax[c] = m;
 }
 
 // FixNVE::final_integrate (fix_nve.cpp:148-219)
@@ -247,23 +220,14 @@ void nve_initial(Ctx &c, double dt) {
   if (c.na + c.ne == 0) return;
   KernelTimer t(c, "nve_initial");
   const bool check = c.lists_valid && c.inner_ok.p && c.xbuild.p && c.disp.p && inner_limit(c) > 0.0;
-  const bool many = c.nrep > 1;
-  // single systems: largest atom displacement per build cell, then per block
-  const bool cells = check && !many && c.na && c.agrid.ncell > 0;
-  if (check) CACB200_CUDA(cudaMemsetAsync(c.dmax.p, 0, sizeof(unsigned) * 2 * c.nrep, c.stream));
-  if (cells) CACB200_CUDA(cudaMemsetAsync(c.cellmax.p, 0, sizeof(unsigned) * c.agrid.ncell, c.stream));
+  if (check) CACB200_CUDA(cudaMemsetAsync(c.dmax.p, 0, sizeof(unsigned) * c.nrep, c.stream));
   const int napad = (c.na + 31) & ~31;
   const long n = (long)napad + 8L * c.ne;
+  const bool many = c.nrep > 1;
   k_nve_initial<<<nblk(n, 256), 256, 0, c.stream>>>(
       c.xs.p, c.v.p, c.f.p, c.na, napad, c.nodex.p, c.nodev.p, c.nodef.p, 8 * c.ne, dtfm, dt,
       check ? c.xbuild.p : nullptr, check ? c.nodex_build.p : nullptr, c.disp.p, c.edisp.p,
-      check ? c.dmax.p : nullptr, cells ? c.cellmax.p : nullptr, c.atom_cell.p, many ? c.site_rep.p : nullptr,
-      many ? c.elem_rep.p : nullptr);
-  if (cells) {
-    const Grid &g = c.rep_h[0].ag;
-    k_cell_nbmax<<<nblk(c.agrid.ncell, 256), 256, 0, c.stream>>>(c.cellmax.p, g.nc[0], g.nc[1], g.nc[2],
-                                                                c.nbmax.p);
-  }
+      check ? c.dmax.p : nullptr, many ? c.site_rep.p : nullptr, many ? c.elem_rep.p : nullptr);
 }
 
 // Neighbor::check_distance (neighbor.cpp:1617-1683): does any atom or node

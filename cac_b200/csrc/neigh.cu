@@ -282,13 +282,12 @@ __global__ void k_cell_start(const int *skey, int n, int ncell, int *start) {
   start[c] = lo;
 }
 
-__global__ void k_gather_pos(const double4 *xs, const int *sidx, const int *skey, int n, double4 *out,
-                             float4 *out32, int *atom_slot, int *atom_cell) {
+__global__ void k_gather_pos(const double4 *xs, const int *sidx, int n, double4 *out, float4 *out32,
+                             int *atom_slot) {
   int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= n) return;
   int i = sidx[k];
   atom_slot[i] = k;
-  atom_cell[i] = skey[k];
   double4 p = xs[i];
   out32[k] = make_float4((float)p.x, (float)p.y, (float)p.z, __int_as_float(i));
   p.w = __longlong_as_double((long long)i);
@@ -1226,8 +1225,7 @@ void neigh_plan(Ctx &c, bool want_half) {
   c.inner_ok.reserve(c.nrep);
   c.disp.reserve(std::max(c.na, 1));
   c.edisp.reserve(std::max(c.ne, 1));
-  c.dmax.reserve(2 * c.nrep);
-  c.atom_cell.reserve(std::max(c.na, 1));
+  c.dmax.reserve(c.nrep);
   c.xbuild.reserve(std::max(c.na, 1));
   c.nodex_build.reserve(24 * (size_t)std::max(c.ne, 1));
   c.num_in.reserve(std::max(c.nsite_i(), 1));
@@ -1306,8 +1304,6 @@ void neigh_plan(Ctx &c, bool want_half) {
   c.atom_slot.reserve(std::max(c.na, 1));
   c.xss.reserve(std::max(c.xs.n, (size_t)1));
   c.acell_start.reserve(c.agrid.ncell + 1);
-  c.cellmax.reserve(std::max(c.agrid.ncell, 1));
-  c.nbmax.reserve(std::max(c.agrid.ncell, 1));
   c.acell_pos.reserve(std::max(c.na, 1));
   c.acell_pos32.reserve(std::max(c.na, 1));
   c.ecell_start.reserve(c.egrid.ncell + 1);
@@ -1412,8 +1408,7 @@ void neigh_build_async(Ctx &c, bool want_half) {
     // every site is where the lists are built from
     if (c.na) CACB200_CUDA(cudaMemsetAsync(c.disp.p, 0, sizeof(float) * c.na, c.stream));
     if (c.ne) CACB200_CUDA(cudaMemsetAsync(c.edisp.p, 0, sizeof(float) * c.ne, c.stream));
-    if (c.agrid.ncell) CACB200_CUDA(cudaMemsetAsync(c.nbmax.p, 0, sizeof(unsigned) * c.agrid.ncell, c.stream));
-    CACB200_CUDA(cudaMemsetAsync(c.dmax.p, 0, sizeof(unsigned) * 2 * c.nrep, c.stream));
+    CACB200_CUDA(cudaMemsetAsync(c.dmax.p, 0, sizeof(unsigned) * c.nrep, c.stream));
     {
       KernelTimer t(c, "bin");
       size_t bytes = c.cub_bytes;
@@ -1424,9 +1419,8 @@ void neigh_build_async(Ctx &c, bool want_half) {
                                                      c.stream));
         k_cell_start<<<nblk(c.agrid.ncell + 1, 256), 256, 0, c.stream>>>(c.cell_key2.p, c.na, c.agrid.ncell,
                                                                         c.acell_start.p);
-        k_gather_pos<<<nblk(c.na, 256), 256, 0, c.stream>>>(c.xs.p, c.slot_atom.p, c.cell_key2.p, c.na,
-                                                            c.acell_pos.p, c.acell_pos32.p, c.atom_slot.p,
-                                                            c.atom_cell.p);
+        k_gather_pos<<<nblk(c.na, 256), 256, 0, c.stream>>>(c.xs.p, c.slot_atom.p, c.na, c.acell_pos.p,
+                                                            c.acell_pos32.p, c.atom_slot.p);
       } else {
         CACB200_CUDA(cudaMemsetAsync(c.acell_start.p, 0, sizeof(int) * (c.agrid.ncell + 1), c.stream));
       }

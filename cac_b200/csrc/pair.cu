@@ -121,8 +121,8 @@ __device__ __forceinline__ void for_each_neighbour(const PairArgs &A, int i, con
 // of the walk serves both segments, which keeps the register count of the
 // unrolled body.
 template <bool MANY, class F>
-__device__ __forceinline__ void walk_list(const PairArgs &A, int t, int i, const int *nb, int n_in, int n, F &&f) {
-  const bool rest = n > n_in && walk_rest(A.prefix, t, i, MANY ? A.site_rep[i] : 0);
+__device__ __forceinline__ void walk_list(const PairArgs &A, int i, const int *nb, int n_in, int n, F &&f) {
+  const bool rest = n > n_in && walk_rest(A.prefix, i, MANY ? A.site_rep[i] : 0);
 #pragma unroll 1
   for (int seg = 0; seg < (rest ? 2 : 1); seg++)
     for_each_neighbour<MANY>(A, i, seg ? nb + (size_t)(A.cap - (n - n_in)) * A.nsi : nb, seg ? n - n_in : n_in,
@@ -222,7 +222,7 @@ __global__ void __launch_bounds__(128, EV ? 4 : 8) k_lj(PairArgs A, LjParams P) 
         }
       }
     };
-    walk_list<MANY>(A, t, i, nb, n_in, n, pair);
+    walk_list<MANY>(A, i, nb, n_in, n, pair);
   }
   if (EV) finish_site(A, i, valid, fi, esum, vsum, 0.0, 0.0);
   else finish_force(A, i, valid, fi);
@@ -285,7 +285,7 @@ __device__ __forceinline__ void rho_slot(const PairArgs &A, const EamTables &T, 
       rho = radd(rho, radd(rmul(radd(rmul(radd(rmul(c.x, p), c.y), p), c.z), p), c.w));
     }
   };
-  walk_list<MANY>(A, t, i, nb, n_in, n, pair);
+  walk_list<MANY>(A, i, nb, n_in, n, pair);
   int slot = i;
   if (i >= A.na) {
     int e = (i - A.na) / NG, g = (i - A.na) % NG;
@@ -383,7 +383,7 @@ __device__ __forceinline__ void force_slot(const PairArgs &A, const EamTables &T
         }
       }
     };
-    walk_list<MANY>(A, t, i, nb, n_in, n, pair);
+    walk_list<MANY>(A, i, nb, n_in, n, pair);
     if (EV && A.eflag) {
       double phi = phi_site[i];
       eemb_site = phi;

@@ -206,7 +206,7 @@ __device__ __forceinline__ void for_each32(const Args32 &A, int t, int i, const 
   const SiteFix fx = site_fix(A, i);
   const int n_in = A.num_in[t], n = A.num[t];
   const int *nb = A.nbr + t;
-  const bool rest = n > n_in && walk_rest(A.prefix, t, i, A.G.reps ? A.G.site_rep[i] : 0);
+  const bool rest = n > n_in && walk_rest(A.prefix, i, A.G.reps ? A.G.site_rep[i] : 0);
 #pragma unroll 1
   for (int seg = 0; seg < (rest ? 2 : 1); seg++)
     walk32(A, fx, oi, seg ? nb + (size_t)(A.cap - (n - n_in)) * A.nsi : nb, seg ? n - n_in : n_in, f);
