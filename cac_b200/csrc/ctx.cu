@@ -452,16 +452,17 @@ void nve_cycle(Ctx &c, double dt) {
       nve_initial(c, dt);
       neigh_build_async(c, false);
     });
+    // between two steps of the cycle nothing reads the velocities, so each
+    // step's second half-kick runs inside the next step's drift kernel
     c.g_steps = capture(c, [&] {
       forces(c, 0, 0);
       langevin_post_force(c, dt);
-      nve_final(c, dt);
       for (int k = 1; k < every; k++) {
-        nve_initial(c, dt);
+        nve_initial(c, dt, true);
         forces(c, 0, 0);
         langevin_post_force(c, dt);
-        nve_final(c, dt);
       }
+      nve_final(c, dt);
     });
     c.graph_gen = c.gen;
     c.graph_dt = dt;

@@ -455,7 +455,9 @@ void pair_compute_mixed(Ctx &c, int eflag, int vflag);
 // the mixed form's pair table as fixed-point records (interpolate_sites)
 void pair_table_mixed(Ctx &c);
 void assemble_nodef(Ctx &c);
-void nve_initial(Ctx &c, double dt);
+// prekick: first the previous step's second half-kick (nve_final) on the
+// same forces, in the same operations (one pass over the state for both)
+void nve_initial(Ctx &c, double dt, bool prekick = false);
 bool moved_past_trigger(Ctx &c);
 void nve_final(Ctx &c, double dt);
 void eam_tables(Ctx &c, const double *frho, const double *rhor, const double *z2r);

@@ -98,7 +98,7 @@ __global__ void k_assemble(const double *gaussf, double *nodef, int ne) {
 // before the launch; non-negative floats as bits, whose integer order is
 // theirs).
 __global__ void k_nve_initial(double4 *xs, double *v, const double *f, int na, int napad, double *nodex,
-                              double *nodev, const double *nodef, int nnode, double dtfm, double dtv,
+                              double *nodev, const double *nodef, int nnode, double dtfm, double dtv, int prekick,
                               const double4 *xb, const double *nxb, float *disp, float *edisp, unsigned *dmax,
                               const int *site_rep, const int *elem_rep) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -108,10 +108,18 @@ __global__ void k_nve_initial(double4 *xs, double *v, const double *f, int na, i
     double4 p = xs[t];
     double *vi = v + 3 * (size_t)t;
     const double *fi = f + 3 * (size_t)t;
-    // separate roundings, as the reference's x86-64 build evaluates them
-    double vx = __dadd_rn(vi[0], __dmul_rn(dtfm, fi[0]));
-    double vy = __dadd_rn(vi[1], __dmul_rn(dtfm, fi[1]));
-    double vz = __dadd_rn(vi[2], __dmul_rn(dtfm, fi[2]));
+    // separate roundings, as the reference's x86-64 build evaluates them;
+    // prekick: the previous step's second half-kick first (k_nve_final's
+    // operations on the same forces)
+    double vx = vi[0], vy = vi[1], vz = vi[2];
+    if (prekick) {
+      vx = __dadd_rn(vx, __dmul_rn(dtfm, fi[0]));
+      vy = __dadd_rn(vy, __dmul_rn(dtfm, fi[1]));
+      vz = __dadd_rn(vz, __dmul_rn(dtfm, fi[2]));
+    }
+    vx = __dadd_rn(vx, __dmul_rn(dtfm, fi[0]));
+    vy = __dadd_rn(vy, __dmul_rn(dtfm, fi[1]));
+    vz = __dadd_rn(vz, __dmul_rn(dtfm, fi[2]));
     vi[0] = vx;
     vi[1] = vy;
     vi[2] = vz;
@@ -133,7 +141,9 @@ __global__ void k_nve_initial(double4 *xs, double *v, const double *f, int na, i
 #pragma unroll
       for (int c = 0; c < 3; c++) {
         const size_t m = 3 * (size_t)k + c;
-        const double vn = __dadd_rn(nodev[m], __dmul_rn(dtfm, nodef[m]));
+        double vn = nodev[m];
+        if (prekick) vn = __dadd_rn(vn, __dmul_rn(dtfm, nodef[m]));
+        vn = __dadd_rn(vn, __dmul_rn(dtfm, nodef[m]));
         nodev[m] = vn;
         const double xn = __dadd_rn(nodex[m], __dmul_rn(dtv, vn));
         nodex[m] = xn;
@@ -213,7 +223,7 @@ void assemble_nodef(Ctx &c) {
   k_assemble<<<nblk(8L * c.ne, 128), 128, 0, c.stream>>>(c.gaussf.p, c.nodef.p, c.ne);
 }
 
-void nve_initial(Ctx &c, double dt) {
+void nve_initial(Ctx &c, double dt, bool prekick) {
   c.forces_current = false;   // the drift moves every site
   double dtf = 0.5 * dt * (1.0 / 1.0364269e-4);   // metal units, update.cpp:161-164
   double dtfm = dtf / c.mass;
@@ -225,7 +235,7 @@ void nve_initial(Ctx &c, double dt) {
   const long n = (long)napad + 8L * c.ne;
   const bool many = c.nrep > 1;
   k_nve_initial<<<nblk(n, 256), 256, 0, c.stream>>>(
-      c.xs.p, c.v.p, c.f.p, c.na, napad, c.nodex.p, c.nodev.p, c.nodef.p, 8 * c.ne, dtfm, dt,
+      c.xs.p, c.v.p, c.f.p, c.na, napad, c.nodex.p, c.nodev.p, c.nodef.p, 8 * c.ne, dtfm, dt, prekick ? 1 : 0,
       check ? c.xbuild.p : nullptr, check ? c.nodex_build.p : nullptr, c.disp.p, c.edisp.p,
       check ? c.dmax.p : nullptr, many ? c.site_rep.p : nullptr, many ? c.elem_rep.p : nullptr);
 }
