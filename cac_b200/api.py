@@ -70,6 +70,7 @@ SIGNATURES = [
     ("cacb200_device_array", C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_void_p), C.POINTER(C.c_int64)]),
     ("cacb200_replica_energy_noalloc", C.c_int, [C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.POINTER(C.c_int),
                                                  C.POINTER(C.c_int), C.c_double, _dp, C.c_void_p]),
+    ("cacb200_noalloc_last_error", C.c_char_p, []),
     ("cacb200_server_create", C.c_int, [C.c_int, C.c_int, C.c_double, C.c_int, C.POINTER(C.c_void_p)]),
     ("cacb200_server_set_lj", C.c_int, [C.c_void_p, C.c_double, C.c_double, C.c_double]),
     ("cacb200_server_set_eam", C.c_int, [C.c_void_p, C.c_int, C.c_double, C.c_int, C.c_double, C.c_double,

@@ -66,20 +66,33 @@ cudaError_t scratch_for(int device, NoAllocScratch **out) {
 }  // namespace
 }  // namespace cacb200
 
+namespace {
+// the calling thread's last failure of cacb200_replica_energy_noalloc
+thread_local char noalloc_error[160] = "";
+
+int noalloc_fail(int code, const char *what) {
+  std::snprintf(noalloc_error, sizeof noalloc_error, "cacb200_replica_energy_noalloc: %s", what);
+  return code;
+}
+}  // namespace
+
+extern "C" const char *cacb200_noalloc_last_error(void) { return noalloc_error; }
+
 extern "C" int cacb200_replica_energy_noalloc(int device, const double *eatom, const double *enode,
                                               int nreplicas, const int *natoms, const int *nelements,
                                               double node_weight, double *energy, void *stream) {
   using namespace cacb200;
   if (nreplicas < 1 || nreplicas > NOALLOC_MAX_REPLICAS) {
-    std::fprintf(stderr, "cacb200_replica_energy_noalloc: %d replicas; the fixed scratch holds 1 to %d\n",
-                 nreplicas, NOALLOC_MAX_REPLICAS);
-    return CACB200_EINVAL;
+    char m[120];
+    std::snprintf(m, sizeof m, "%d replicas; the fixed scratch holds 1 to %d", nreplicas, NOALLOC_MAX_REPLICAS);
+    return noalloc_fail(CACB200_EINVAL, m);
   }
-  if (!natoms || !nelements || !energy || device < 0 || device >= MAX_DEVICES) return CACB200_EINVAL;
+  if (!natoms || !nelements || !energy) return noalloc_fail(CACB200_EINVAL, "null count or output array");
+  if (device < 0 || device >= MAX_DEVICES) return noalloc_fail(CACB200_EINVAL, "device index out of range");
   std::vector<int> meta(4 * (size_t)nreplicas, 0);
   long a = 0, e = 0;
   for (int r = 0; r < nreplicas; r++) {
-    if (natoms[r] < 0 || nelements[r] < 0) return CACB200_EINVAL;
+    if (natoms[r] < 0 || nelements[r] < 0) return noalloc_fail(CACB200_EINVAL, "negative site count");
     meta[4 * r] = (int)a;
     meta[4 * r + 1] = natoms[r];
     meta[4 * r + 2] = (int)e;
@@ -87,13 +100,13 @@ extern "C" int cacb200_replica_energy_noalloc(int device, const double *eatom, c
     a += natoms[r];
     e += nelements[r];
   }
-  if (a >= (1L << 31) || 8 * e >= (1L << 31)) return CACB200_EINVAL;
-  if ((a > 0 && !eatom) || (e > 0 && !enode)) return CACB200_EINVAL;
+  if (a >= (1L << 31) || 8 * e >= (1L << 31)) return noalloc_fail(CACB200_EINVAL, "more than 2^31 sites");
+  if ((a > 0 && !eatom) || (e > 0 && !enode)) return noalloc_fail(CACB200_EINVAL, "null per-site energy array");
   int prev = 0;
-  if (cudaGetDevice(&prev) != cudaSuccess) return CACB200_ECUDA;
+  if (cudaGetDevice(&prev) != cudaSuccess) return noalloc_fail(CACB200_ECUDA, "cudaGetDevice failed");
   if (cudaSetDevice(device) != cudaSuccess) {
     cudaGetLastError();
-    return CACB200_ECUDA;
+    return noalloc_fail(CACB200_ECUDA, "cudaSetDevice failed");
   }
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   NoAllocScratch *sc = nullptr;
@@ -110,7 +123,8 @@ extern "C" int cacb200_replica_energy_noalloc(int device, const double *eatom, c
   cudaSetDevice(prev);
   if (err != cudaSuccess) {
     cudaGetLastError();
-    return CACB200_ECUDA;
+    return noalloc_fail(CACB200_ECUDA, cudaGetErrorString(err));
   }
+  noalloc_error[0] = '\0';
   return CACB200_OK;
 }

@@ -390,8 +390,10 @@ int cacb200_restore(cacb200_ctx *ctx);
  * energy [nreplicas] are host arrays; node_weight multiplies node energies
  * (729/8 for the UNIFORM Hex element; 1 for EAM during minimisation).  The
  * scratch is one fixed device array of this library for at most
- * CACB200_NOALLOC_MAX_REPLICAS replicas (more: CACB200_EINVAL and a message
- * on stderr), held by every GPU that loads the library until exit.  The
+ * CACB200_NOALLOC_MAX_REPLICAS replicas (more: CACB200_EINVAL), held by
+ * every GPU that loads the library until exit.  A failed call leaves its
+ * reason in cacb200_noalloc_last_error() (per thread; empty after a
+ * success).  The
  * first call on a device looks up that array's device address; make it
  * before any stream capture.  The address is kept for the life of the
  * process: a device reset (cudaDeviceReset, or another framework resetting
@@ -405,6 +407,7 @@ int cacb200_replica_energy_noalloc(int device, const double *eatom, const double
                                    int nreplicas, const int *natoms, const int *nelements,
                                    double node_weight, double *energy /* [nreplicas] */,
                                    void *stream /* cudaStream_t */);
+const char *cacb200_noalloc_last_error(void);
 
 /* cacb200_run_nve replays each rebuild cycle (every steps) as two CUDA
  * graphs, with one host wait per cycle to read the rebuild's overflow flags.

@@ -67,3 +67,5 @@ def test_noalloc_rejects_more_replicas_than_its_scratch():
     rc = lib.cacb200_replica_energy_noalloc(0, None, None, n, counts.ctypes.data_as(ip), counts.ctypes.data_as(ip),
                                             1.0, out.ctypes.data_as(C.POINTER(C.c_double)), None)
     assert rc != 0
+    lib.cacb200_noalloc_last_error.restype = C.c_char_p
+    assert b"4097 replicas" in lib.cacb200_noalloc_last_error()
