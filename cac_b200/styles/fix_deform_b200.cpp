@@ -35,7 +35,11 @@ bool FixDeformB200::device_ok() const
   if (domain->triclinic || igroup != 0) return false;
   for (int d = 3; d < 6; d++)
     if (set[d].style != R_NONE) return false;
-  return remapflag == Domain::X_REMAP || remapflag == Domain::NO_REMAP;
+  // remap v moves nothing in this reference: the velocity terms of
+  // Domain::remap are commented out (domain.cpp:566-633) and the border
+  // packing only affects ghost velocities, which no /b200 pair style reads;
+  // the device runs it as remap none
+  return remapflag == Domain::X_REMAP || remapflag == Domain::NO_REMAP || remapflag == Domain::V_REMAP;
 }
 
 int FixDeformB200::remap_x() const { return remapflag == Domain::X_REMAP; }

@@ -60,7 +60,7 @@ FixLangevinB200 *CAC_NS::b200_device_fixes(CAC *cac, const char *who, B200Fixes 
   if (dfm) {
     if (!dfm->device_ok())
       error->all(FLERR, (std::string(who) + ": fix deform/b200 needs group all, an orthogonal box, no tilt and "
-                                            "remap x or none").c_str());
+                                            "remap x, v or none").c_str());
     fx.deform = true;
     fx.deform_every = dfm->every();
     fx.deform_remap_x = dfm->remap_x();

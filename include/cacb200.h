@@ -335,7 +335,10 @@ int cacb200_unset_langevin(cacb200_ctx *ctx);
  * Replicas of a batch deform alike, each from its own box.  Runs with a
  * deforming box queue their steps without graph replay; the neighbour grids
  * follow the box at each rebuild.  A new system or cacb200_unset_deform
- * removes the fix.  remap v and tilt (triclinic) styles are not offered. */
+ * removes the fix.  Tilt (triclinic) styles are not offered; the reference's
+ * remap v moves neither positions nor velocities (its velocity terms in
+ * Domain::remap are commented out, domain.cpp:566-633), so its decks pass
+ * remap_x = 0. */
 #define CACB200_DEFORM_NONE 0
 #define CACB200_DEFORM_FINAL 1
 #define CACB200_DEFORM_DELTA 2

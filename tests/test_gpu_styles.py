@@ -156,6 +156,28 @@ def test_deform_style_mixes_reference_loop_and_device(case, order, golden, tmp_p
     assert_state(e, g, "dfm_end_")
 
 
+@pytest.mark.parametrize("case", ["tiny_lj", "tiny_eam"])
+def test_deform_remap_v_on_device_vs_reference(case, golden, tmp_path):
+    """remap v: in the reference it moves neither positions nor velocities
+    (the velocity terms of Domain::remap are commented out), so run_b200 with
+    fix deform/b200 ... remap v ends where the reference's own run with fix
+    deform ... remap v does: the same box, positions and velocities."""
+    import oracle as O
+    g = golden(case)
+    n = int(g["dfm_runs"][0])
+    fix = dfm_fix(g).replace("remap x", "remap v")
+    run_app(tmp_path, case, fix + f"run_b200 {n}\noracle_dump end.txt state\n")
+    exe = O.REF_EXE_EAMFIX if CASES[case][1] == "eam" else O.REF_EXE
+    reference_log(tmp_path, case, fix.replace("deform/b200", "deform") + f"run {n}\noracle_dump end.txt state\n", exe)
+    a = O.read_dump(str(tmp_path / "end.txt"))
+    b = O.read_dump(str(tmp_path / "ref" / "end.txt"))
+    assert np.array_equal(a["box"], b["box"])
+    assert np.abs(a["x"] - b["x"]).max() < 1e-10
+    assert np.abs(a["nodex"] - b["nodex"]).max() < 1e-10
+    assert rel_err(a["v"], b["v"]) < TOL
+    assert rel_err(a["nodev"], b["nodev"]) < TOL
+
+
 def test_run_b200_refuses_plain_langevin(tmp_path):
     import oracle  # noqa: F401
     build, pair, _ = CASES["tiny_lj"]
