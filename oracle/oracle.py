@@ -581,6 +581,31 @@ def read_dump(path: str) -> dict:
     return out
 
 
+def read_dump_binary(path: str) -> dict:
+    """Parse ``oracle_dump FILE state|compute binary`` (oracle_dump.cpp: the
+    magic, 16 float64 header values, then 17-value atom rows and 21-value
+    node rows) into the dictionary of :func:`read_dump`."""
+    raw = np.fromfile(path, dtype=np.uint8)
+    if raw[:8].tobytes() != b"CACODMP1":
+        raise ValueError(f"{path}: not a binary oracle dump")
+    v = raw[8:].view(np.float64)
+    out = {"step": int(v[0]), "box": v[1:7].copy(), "natoms": int(v[7]), "nelements": int(v[8]),
+           "energy": float(v[9]), "virial": v[10:16].copy()}
+    na, ne = out["natoms"], out["nelements"]
+    a = v[16:16 + 17 * na].reshape(na, 17)
+    nd = v[16 + 17 * na:16 + 17 * na + 21 * 8 * ne].reshape(8 * ne, 21)
+    out["atoms"], out["nodes"] = a, nd
+    out["x"], out["v"], out["f"] = a[:, 1:4], a[:, 4:7], a[:, 7:10]
+    out["eatom"], out["vatom"] = a[:, 10], a[:, 11:17]
+    out["nodex"] = nd[:, 2:5].reshape(ne, 8, 3)
+    out["nodev"] = nd[:, 5:8].reshape(ne, 8, 3)
+    out["nodef"] = nd[:, 8:11].reshape(ne, 8, 3)
+    out["gaussf_at_node"] = nd[:, 11:14].reshape(ne, 8, 3)
+    out["enode"] = nd[:, 14].reshape(ne, 8)
+    out["vnode"] = nd[:, 15:21].reshape(ne, 8, 6)
+    return out
+
+
 def read_neigh(path: str, natoms: int) -> np.ndarray:
     """Parse ``oracle_dump_neigh`` output into sorted int64 rows
     (i_site, kind, idx, site, sx, sy, sz) in the restatement's numbering:

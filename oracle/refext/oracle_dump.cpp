@@ -2,7 +2,8 @@
  * Oracle read-out commands (see oracle_dump.h).  Test infrastructure only.
  *
  * Output is plain text with every double printed as %.17g so that a reader
- * recovers the exact binary value.
+ * recovers the exact binary value, or with `binary` the same values as raw
+ * float64 (for systems of millions of sites).
  */
 #include "oracle_dump.h"
 
@@ -54,12 +55,17 @@ OracleDump::OracleDump(CAC *cac) : Pointers(cac) {}
 
 void OracleDump::command(int narg, char **arg)
 {
-  if (narg != 2) error->all(FLERR, "Illegal oracle_dump command: oracle_dump FILE state|compute");
+  if (narg != 2 && narg != 3) error->all(FLERR, "Illegal oracle_dump command: oracle_dump FILE state|compute [binary]");
   int compute = 0;
   if (strcmp(arg[1], "compute") == 0) compute = 1;
   else if (strcmp(arg[1], "state") != 0) error->all(FLERR, "Illegal oracle_dump mode");
+  int binary = 0;
+  if (narg == 3) {
+    if (strcmp(arg[2], "binary") != 0) error->all(FLERR, "Illegal oracle_dump format");
+    binary = 1;
+  }
   if (compute) setup_and_compute();
-  write(arg[0], compute);
+  write(arg[0], compute, binary);
 }
 
 /* ----------------------------------------------------------------------
@@ -128,47 +134,70 @@ void OracleDump::setup_and_compute()
   }
 }
 
-void OracleDump::write(const char *file, int with_energy)
+// Text (one line per header field, atom and node) or binary: the magic
+// "CACODMP1", then float64 values: step, box (lo/hi x, y, z), natoms,
+// nelements, energy, virial[6], then natoms rows of 17 and 8 x nelements
+// rows of 21 values, the columns of the text form.
+void OracleDump::write(const char *file, int with_energy, int binary)
 {
-  FILE *fp = fopen(file, "w");
+  FILE *fp = fopen(file, binary ? "wb" : "w");
   if (!fp) error->one(FLERR, "oracle_dump: cannot open file");
   Pair *pair = force->pair;
-  fprintf(fp, "# cac oracle dump v1\n");
-  fprintf(fp, "step %ld\n", (long) update->ntimestep);
-  fprintf(fp, "box %.17g %.17g %.17g %.17g %.17g %.17g\n",
-          domain->boxlo[0], domain->boxhi[0], domain->boxlo[1], domain->boxhi[1],
-          domain->boxlo[2], domain->boxhi[2]);
-  fprintf(fp, "natoms %d nelements %d\n", atom->nlocal, element->nlocal);
-  if (with_energy && pair) {
-    fprintf(fp, "energy %.17g\n", pair->eng_vdwl);
-    fprintf(fp, "virial %.17g %.17g %.17g %.17g %.17g %.17g\n", pair->virial[0],
-            pair->virial[1], pair->virial[2], pair->virial[3], pair->virial[4], pair->virial[5]);
+  const bool ev = with_energy && pair;
+  const double energy = ev ? pair->eng_vdwl : 0.0;
+  double virial[6] = {0, 0, 0, 0, 0, 0};
+  if (ev)
+    for (int k = 0; k < 6; k++) virial[k] = pair->virial[k];
+  if (binary) {
+    fwrite("CACODMP1", 1, 8, fp);
+    const double head[15] = {(double) update->ntimestep, domain->boxlo[0], domain->boxhi[0], domain->boxlo[1],
+                             domain->boxhi[1], domain->boxlo[2], domain->boxhi[2], (double) atom->nlocal,
+                             (double) element->nlocal, energy, virial[0], virial[1], virial[2], virial[3],
+                             virial[4]};
+    fwrite(head, sizeof(double), 15, fp);
+    fwrite(&virial[5], sizeof(double), 1, fp);
   } else {
-    fprintf(fp, "energy 0\nvirial 0 0 0 0 0 0\n");
+    fprintf(fp, "# cac oracle dump v1\n");
+    fprintf(fp, "step %ld\n", (long) update->ntimestep);
+    fprintf(fp, "box %.17g %.17g %.17g %.17g %.17g %.17g\n", domain->boxlo[0], domain->boxhi[0],
+            domain->boxlo[1], domain->boxhi[1], domain->boxlo[2], domain->boxhi[2]);
+    fprintf(fp, "natoms %d nelements %d\n", atom->nlocal, element->nlocal);
+    if (ev) {
+      fprintf(fp, "energy %.17g\n", energy);
+      fprintf(fp, "virial %.17g %.17g %.17g %.17g %.17g %.17g\n", virial[0], virial[1], virial[2], virial[3],
+              virial[4], virial[5]);
+    } else {
+      fprintf(fp, "energy 0\nvirial 0 0 0 0 0 0\n");
+    }
   }
 
   std::vector<int> order(atom->nlocal);
   for (int i = 0; i < atom->nlocal; i++) order[i] = i;
   std::sort(order.begin(), order.end(), [&](int a, int b) { return atom->tag[a] < atom->tag[b]; });
-  fprintf(fp, "atoms\n");
+  if (!binary) fprintf(fp, "atoms\n");
   for (int i : order) {
     double e = 0.0, v[6] = {0, 0, 0, 0, 0, 0};
-    if (with_energy && pair) {
+    if (ev) {
       e = pair->eatom[i];
       for (int k = 0; k < 6; k++) v[k] = pair->vatom[i][k];
     }
-    fprintf(fp, "%d %.17g %.17g %.17g %.17g %.17g %.17g %.17g %.17g %.17g %.17g"
-            " %.17g %.17g %.17g %.17g %.17g %.17g\n",
-            (int) atom->tag[i], atom->x[i][0], atom->x[i][1], atom->x[i][2],
-            atom->v[i][0], atom->v[i][1], atom->v[i][2],
-            atom->f[i][0], atom->f[i][1], atom->f[i][2], e, v[0], v[1], v[2], v[3], v[4], v[5]);
+    const double row[17] = {(double) atom->tag[i], atom->x[i][0], atom->x[i][1], atom->x[i][2],
+                            atom->v[i][0], atom->v[i][1], atom->v[i][2], atom->f[i][0], atom->f[i][1],
+                            atom->f[i][2], e, v[0], v[1], v[2], v[3], v[4], v[5]};
+    if (binary) {
+      fwrite(row, sizeof(double), 17, fp);
+    } else {
+      fprintf(fp, "%d", (int) atom->tag[i]);
+      for (int k = 1; k < 17; k++) fprintf(fp, " %.17g", row[k]);
+      fprintf(fp, "\n");
+    }
   }
 
   std::vector<int> eorder(element->nlocal);
   for (int i = 0; i < element->nlocal; i++) eorder[i] = i;
   std::sort(eorder.begin(), eorder.end(),
             [&](int a, int b) { return element->tag[a] < element->tag[b]; });
-  fprintf(fp, "nodes\n");
+  if (!binary) fprintf(fp, "nodes\n");
   for (int i : eorder) {
     int t = element->etype[i];
     for (int b = 0; b < element->apc[t]; b++)
@@ -176,17 +205,22 @@ void OracleDump::write(const char *file, int with_energy)
         int g = element->n2g[t][n];
         double *gf = element->gaussf[i][b][g];
         double e = 0.0, v[6] = {0, 0, 0, 0, 0, 0};
-        if (with_energy && pair) {
+        if (ev) {
           e = pair->enode[i][b][n];
           for (int k = 0; k < 6; k++) v[k] = pair->vnode[i][b][n][k];
         }
-        fprintf(fp, "%d %d %.17g %.17g %.17g %.17g %.17g %.17g %.17g %.17g %.17g"
-                " %.17g %.17g %.17g %.17g %.17g %.17g %.17g %.17g %.17g %.17g\n",
-                (int) element->tag[i], n,
-                element->nodex[i][b][n][0], element->nodex[i][b][n][1], element->nodex[i][b][n][2],
-                element->nodev[i][b][n][0], element->nodev[i][b][n][1], element->nodev[i][b][n][2],
-                element->nodef[i][b][n][0], element->nodef[i][b][n][1], element->nodef[i][b][n][2],
-                gf[0], gf[1], gf[2], e, v[0], v[1], v[2], v[3], v[4], v[5]);
+        const double row[21] = {(double) element->tag[i], (double) n,
+                                element->nodex[i][b][n][0], element->nodex[i][b][n][1], element->nodex[i][b][n][2],
+                                element->nodev[i][b][n][0], element->nodev[i][b][n][1], element->nodev[i][b][n][2],
+                                element->nodef[i][b][n][0], element->nodef[i][b][n][1], element->nodef[i][b][n][2],
+                                gf[0], gf[1], gf[2], e, v[0], v[1], v[2], v[3], v[4], v[5]};
+        if (binary) {
+          fwrite(row, sizeof(double), 21, fp);
+        } else {
+          fprintf(fp, "%d %d", (int) element->tag[i], n);
+          for (int k = 2; k < 21; k++) fprintf(fp, " %.17g", row[k]);
+          fprintf(fp, "\n");
+        }
       }
   }
   fclose(fp);

@@ -36,7 +36,7 @@ class OracleDump : protected Pointers {
 
  private:
   void setup_and_compute();
-  void write(const char *file, int with_energy);
+  void write(const char *file, int with_energy, int binary);
 };
 
 class OracleDumpNeigh : protected Pointers {

@@ -6,9 +6,10 @@ its sources, EAM energies read on the F(rho) row) runs on the same host as the
 GPU, on the same seeded inputs, for
 
 * the EAM workload at scale (1,049,760 atoms + 20,000 elements, 1,209,760
-  sites, 300 K): setup forces (atoms, nodes, Gauss points), energy, virial and
-  per-site energy and virial after one evaluation (``Verlet::setup``,
-  verlet.cpp:64-152);
+  sites, 300 K) and the 3 %-strained mixed-precision workload's system
+  (4,179,600 atoms + 100,000 elements, 4,979,600 sites) in FP64: setup
+  forces (atoms, nodes, Gauss points), energy, virial and per-site energy
+  and virial after one evaluation (``Verlet::setup``, verlet.cpp:64-152);
 * a 3 %-strained slab of 313,120 sites (272,160 atoms + 5,120 elements, the
   strained shape of the mixed-precision workload at a quarter of its height):
   half and full neighbour lists as sorted index sets, bit for bit
@@ -96,6 +97,22 @@ def test_eam_1m_setup_vs_reference(tmp_path):
     O = reference(work, s, "run 0\noracle_dump setup.txt compute\n")
     d = O.read_dump(os.path.join(work, "setup.txt"))
     assert d["natoms"] == s.natoms and d["nelements"] == s.nelements
+    e = engine(s, work)
+    check_setup(e, d)
+    e.close()
+
+
+def test_eam_4m_strained_setup_vs_reference(tmp_path):
+    """4,979,600 sites (4,179,600 atoms + 100,000 elements, 3 % strain: the
+    mixed-precision workload's own system), FP64: one evaluation, every
+    read-out of the reference (its dump in binary form)."""
+    s = gen.eam_4m_strained()
+    work = str(tmp_path)
+    O = reference(work, s, "run 0\noracle_dump setup.bin compute binary\n")
+    d = O.read_dump_binary(os.path.join(work, "setup.bin"))
+    os.remove(os.path.join(work, "data.cac"))
+    assert d["natoms"] == s.natoms and d["nelements"] == s.nelements
+    assert s.natoms + 8 * s.nelements == 4979600
     e = engine(s, work)
     check_setup(e, d)
     e.close()
