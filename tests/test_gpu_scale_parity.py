@@ -104,8 +104,9 @@ def test_eam_1m_setup_vs_reference(tmp_path):
 
 def test_eam_4m_strained_setup_vs_reference(tmp_path):
     """4,979,600 sites (4,179,600 atoms + 100,000 elements, 3 % strain: the
-    mixed-precision workload's own system), FP64: one evaluation, every
-    read-out of the reference (its dump in binary form)."""
+    mixed-precision workload's own system): one evaluation, every read-out of
+    the reference (its dump in binary form) in FP64, and the mixed form's
+    forces, energy and virial against the same reference read-out."""
     s = gen.eam_4m_strained()
     work = str(tmp_path)
     O = reference(work, s, "run 0\noracle_dump setup.bin compute binary\n")
@@ -116,6 +117,19 @@ def test_eam_4m_strained_setup_vs_reference(tmp_path):
     e = engine(s, work)
     check_setup(e, d)
     e.close()
+    # the mixed form against the same reference read-out: largest per-site
+    # force error under 1e-5 of the largest force, energy and virial to 1e-6
+    from cac_b200.api import MIXED
+    e = engine(s, work)
+    e.set_precision(MIXED)
+    e.compute()
+    f, nf, _ = e.forces()
+    ev = e.energy(peratom=False)
+    e.close()
+    assert rel_err(f, d["f"]) < 1e-5
+    assert rel_err(nf, d["nodef"]) < 1e-5
+    assert abs(ev["energy"] - d["energy"]) / abs(d["energy"]) < 1e-6
+    assert np.abs(ev["virial"] - d["virial"]).max() / np.abs(d["virial"]).max() < 1e-6
 
 
 @pytest.fixture(scope="module")
