@@ -213,7 +213,8 @@ void interpolate_sites(Ctx &c) {
     pair_table_mixed(c);   // fixed-point records directly (pair32.cu)
     return;
   }
-  k_pair_table<<<stride_grid((long)c.na + (long)NG * c.ne + (long)c.ne * NU, 256), 256, 0, c.stream>>>(
+  // 64 blocks per SM, as the mixed form's pair table
+  k_pair_table<<<std::min(nblk((long)c.na + (long)NG * c.ne + (long)c.ne * NU, 256), 148 * 64), 256, 0, c.stream>>>(
       c.xs.p, c.xss.p, c.slot_atom.p, c.nodex.p, c.na, c.ne, c.act_gid.p, c.dev_nact.p);
 }
 
