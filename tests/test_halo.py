@@ -1,5 +1,5 @@
 """The spatial decomposition of one system over ranks (cac_b200.halo) on the
-CPU: two gloo ranks, each evaluating its slab plus ghosts with the C
+CPU: two and three gloo ranks, each evaluating its slab plus ghosts with the C
 restatement standing in for the rank's GPU context, against the
 restatement's own run of the whole periodic system.  The decomposition is
 what is under test here (ownership, ghost shells, the forward halo of
@@ -114,8 +114,8 @@ def wrapped_diff(a, b, L):
     return float(np.abs(d).max())
 
 
-@pytest.mark.parametrize("pair", ["lj", "eam"])
-def test_two_gloo_ranks_equal_one_system(pair, tmp_path):
+@pytest.mark.parametrize("pair,ws", [("lj", 2), ("eam", 2), ("lj", 3)])
+def test_gloo_ranks_equal_one_system(pair, ws, tmp_path):
     import socket
     import torch.multiprocessing as mp
     sys.path.insert(0, ROOT)
@@ -127,7 +127,7 @@ def test_two_gloo_ranks_equal_one_system(pair, tmp_path):
         port = sk.getsockname()[1]
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
-    procs = [ctx.Process(target=_worker, args=(r, 2, port, pair, setfl, q)) for r in range(2)]
+    procs = [ctx.Process(target=_worker, args=(r, ws, port, pair, setfl, q)) for r in range(ws)]
     for p in procs:
         p.start()
     res = sorted((q.get(timeout=600) for _ in procs), key=lambda t: t[0])
@@ -137,12 +137,14 @@ def test_two_gloo_ranks_equal_one_system(pair, tmp_path):
     s = system()
     ref = reference(pair, setfl)
     L = np.asarray(s.boxhi) - np.asarray(s.boxlo)
-    # both ranks hold a share and ghosts, and gather the same global state
+    # every rank owns sites (three slabs: the outer ones hold only elements)
+    # and ghosts, and gathers the same global state
     for (_, nown, *_a) in res:
-        assert nown[0] > 0 and nown[2] > 0
+        assert nown[0] + nown[1] > 0 and nown[2] + nown[3] > 0
     assert sum(r[1][0] for r in res) == s.natoms and sum(r[1][1] for r in res) == s.nelements
-    for k in range(2, 8):
-        assert np.array_equal(res[0][k], res[1][k])
+    for other in res[1:]:
+        for k in range(2, 8):
+            assert np.array_equal(res[0][k], other[k])
     _, _, x, v, nx, nv, f, nf = res[0]
     assert wrapped_diff(x, ref.x, L) < 1e-10
     assert wrapped_diff(nx, ref.nodex, L) < 1e-10
