@@ -654,9 +654,11 @@ def b200_arm(args, rank, local, ws, dist):
         e2.close()
         del e2, s2
 
-    # CPU baseline: the reference on a bounded sample of the same workload
+    # CPU baseline: the reference on a bounded sample of the same workload,
+    # at N = 1 only (under torchrun the other ranks would wait for rank 0's
+    # CPU run in their next collective)
     cpu = None
-    if rank == 0 and not args.no_cpu_baseline:
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         if os.path.exists(REF_EXE):
             try:
                 if batch:
