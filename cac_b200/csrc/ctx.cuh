@@ -273,7 +273,8 @@ struct Ctx {
   // segments meet only when a list overflows (then the build is repeated)
   DBuf<int> nbr_full, num_full;
   DBuf<int2> site_from;
-  DBuf<unsigned char> ecell_near;   // single systems: element cells with an element in their 27-cell block          // per slot: rows of each segment before its element-site entries
+  DBuf<unsigned char> ecell_near;   // single systems: element cells with an element in their 27-cell block
+  DBuf<unsigned char> acell_near;   // single systems: atom cells with an atom in their 27-cell block
   // inner prefix of the full lists (entries within cutoff + inner_margin at
   // the build, rows [0, num_in)).  inner_ok[replica] (device) is nonzero
   // until positions move other than by the drift (then every site walks its

@@ -250,8 +250,9 @@ __global__ void k_elem_keys(const double4 *ecenter, int ne, RP P, int *key, int 
   idx[e] = e;
 }
 
-// near[c]: some element cell of the 27-cell block around element cell c (a
-// single system's grid, periodic) holds an element
+// near[c]: some cell of the 27-cell block around cell c (a single system's
+// grid, periodic) holds an entry (element grid: an element; atom grid: an
+// atom)
 __global__ void k_ecell_near(const int *start, Grid g, unsigned char *near) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= g.ncell) return;
@@ -306,6 +307,7 @@ struct BuildArgs {
   const float4 *acell_pos32;  // wrapped positions as floats, w = atom index bits
   const int *ecell_start;
   const unsigned char *ecell_near;   // single systems: element cell has an element in its 27-cell block (else null)
+  const unsigned char *acell_near;   // single systems: atom cell has an atom in its 27-cell block (else null)
   const int *ecell_elems;
   const int *atom_of_slot;    // list slot (cell-sorted position) -> atom index
   int *site_flag;             // [ne * 729] marks the lattice sites some full list references
@@ -1041,6 +1043,10 @@ __global__ void __launch_bounds__(128, 8) k_build_gauss(BuildArgs A, RP P, const
 #pragma unroll
     for (int d = 0; d < 3; d++)
       ci[d] = min(max((int)((q.wi[d] - q.r.b.lo[d]) * ag.inv[d]), 0), ag.nc[d] - 1);
+    // no atom in the 27 cells around (most Gauss points of an element
+    // region): no atom candidates, the walk below would find none
+    const bool atoms_near = !A.acell_near || A.acell_near[q.r.abase + (ci[2] * ag.nc[1] + ci[1]) * ag.nc[0] + ci[0]];
+    if (atoms_near)
     for (int oz = -1; oz <= 1; oz++) {
       int cz, Wz;
       wrap_cell(ci[2] + oz, ag.nc[2], cz, Wz);
@@ -1308,6 +1314,7 @@ void neigh_plan(Ctx &c, bool want_half) {
   c.acell_pos32.reserve(std::max(c.na, 1));
   c.ecell_start.reserve(c.egrid.ncell + 1);
   c.ecell_near.reserve(c.egrid.ncell + 1);
+  c.acell_near.reserve(c.agrid.ncell + 1);
   c.ecell_elems.reserve(std::max(c.ne, 1));
   size_t slots = (size_t)c.cap * std::max(nsi, 1);
   c.raw_full.reserve(slots);
@@ -1419,6 +1426,9 @@ void neigh_build_async(Ctx &c, bool want_half) {
                                                      c.stream));
         k_cell_start<<<nblk(c.agrid.ncell + 1, 256), 256, 0, c.stream>>>(c.cell_key2.p, c.na, c.agrid.ncell,
                                                                         c.acell_start.p);
+        if (c.nrep == 1 && c.ne)
+          k_ecell_near<<<nblk(c.agrid.ncell, 256), 256, 0, c.stream>>>(c.acell_start.p, c.rep_h[0].ag,
+                                                                       c.acell_near.p);
         k_gather_pos<<<nblk(c.na, 256), 256, 0, c.stream>>>(c.xs.p, c.slot_atom.p, c.na, c.acell_pos.p,
                                                             c.acell_pos32.p, c.atom_slot.p);
       } else {
@@ -1449,6 +1459,7 @@ void neigh_build_async(Ctx &c, bool want_half) {
     A.acell_pos32 = c.acell_pos32.p;
     A.ecell_start = c.ecell_start.p;
     A.ecell_near = (c.nrep == 1 && c.ne) ? c.ecell_near.p : nullptr;
+    A.acell_near = (c.nrep == 1 && c.na && c.ne) ? c.acell_near.p : nullptr;
     A.ecell_elems = c.ecell_elems.p;
     A.atom_of_slot = c.slot_atom.p;
     A.site_flag = c.site_flag.p;

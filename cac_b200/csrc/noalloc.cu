@@ -9,7 +9,6 @@
 // per-replica sums) lives in one fixed array of this file, set up once per
 // device, instead of buffers a context allocates.
 #include <cstdio>
-#include <mutex>
 #include <vector>
 
 #include "../../include/cacb200.h"
@@ -45,21 +44,17 @@ __global__ void k_replica_energy_fixed(const double *eatom, const double *enode,
   block_reduce_store<1>(v, sc->sum);   // sum[r] for block r: every used slot is overwritten
 }
 
-// Device address of the scratch, looked up once per device with that device
-// current.  In host code `noalloc_scratch` only names a host-side stand-in.
+// Device address of the scratch on the current device, looked up on every
+// call (a few microseconds): a cached address would dangle after a device
+// reset reloads the module.  In host code `noalloc_scratch` only names a
+// host-side stand-in.
 constexpr int MAX_DEVICES = 64;
-std::mutex scratch_mutex;
-NoAllocScratch *scratch_ptr[MAX_DEVICES] = {};
 
-cudaError_t scratch_for(int device, NoAllocScratch **out) {
-  std::lock_guard<std::mutex> g(scratch_mutex);
-  if (!scratch_ptr[device]) {
-    void *p = nullptr;
-    cudaError_t e = cudaGetSymbolAddress(&p, noalloc_scratch);
-    if (e != cudaSuccess) return e;
-    scratch_ptr[device] = static_cast<NoAllocScratch *>(p);
-  }
-  *out = scratch_ptr[device];
+cudaError_t scratch_for(NoAllocScratch **out) {
+  void *p = nullptr;
+  cudaError_t e = cudaGetSymbolAddress(&p, noalloc_scratch);
+  if (e != cudaSuccess) return e;
+  *out = static_cast<NoAllocScratch *>(p);
   return cudaSuccess;
 }
 
@@ -110,7 +105,7 @@ extern "C" int cacb200_replica_energy_noalloc(int device, const double *eatom, c
   }
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   NoAllocScratch *sc = nullptr;
-  cudaError_t err = scratch_for(device, &sc);
+  cudaError_t err = scratch_for(&sc);
   if (err == cudaSuccess)
     err = cudaMemcpyAsync(sc->meta, meta.data(), sizeof(int) * meta.size(), cudaMemcpyHostToDevice, st);
   if (err == cudaSuccess) {
