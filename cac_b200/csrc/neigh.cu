@@ -873,18 +873,32 @@ __device__ __forceinline__ void build_atoms_cell(BuildArgs A, RP P, const int ho
         for (int oy = -1; oy <= 1; oy++) {
           int cy, Wy;
           wrap_cell(hy + oy, nc1, cy, Wy);
-          for (int ox = -1; ox <= 1; ox++) {
-            int cx, Wx;
-            wrap_cell(hx + ox, nc0, cx, Wx);
-            int cell = R.abase + (cz * nc1 + cy) * nc0 + cx;
-            int W[3] = {Wx, Wy, Wz};
-            const float sx = (float)(Wx * R.b.L[0]), sy = (float)(Wy * R.b.L[1]), sz = (float)(Wz * R.b.L[2]);
-            // this cell's image relative to the lane's atom
-            const int s0 = Wx - q.ti[0], s1 = Wy - q.ti[1], s2 = Wz - q.ti[2];
+          // the row's three cells in runs of consecutive cells under one
+          // image (one run away from the box's x faces): the cells are
+          // consecutive in sorted order, so a run is one candidate range,
+          // visited in the same order as cell by cell
+          int first = 0, last = -2, Wx = 0;
+          for (int ox = -1; ox <= 2; ox++) {
+            int cx = 0, wx_ = 0;
+            if (ox <= 1) wrap_cell(hx + ox, nc0, cx, wx_);
+            const int next = R.abase + (cz * nc1 + cy) * nc0 + cx;
+            if (ox <= 1 && wx_ == Wx && next == last + 1) {
+              last = next;
+              continue;
+            }
+            const int cell = first, cell_last = last;
+            first = last = next;
+            const int Wrun = Wx;
+            Wx = wx_;
+            if (ox == -1) continue;
+            int W[3] = {Wrun, Wy, Wz};
+            const float sx = (float)(Wrun * R.b.L[0]), sy = (float)(Wy * R.b.L[1]), sz = (float)(Wz * R.b.L[2]);
+            // this run's image relative to the lane's atom
+            const int s0 = Wrun - q.ti[0], s1 = Wy - q.ti[1], s2 = Wz - q.ti[2];
             const bool zero = (s0 == 0 && s1 == 0 && s2 == 0);
             const bool far = s0 < -1 || s0 > 1 || s1 < -1 || s1 > 1 || s2 < -1 || s2 > 1;
             const int code = far ? 0 : img_code(s0, s1, s2);
-            int beg = A.acell_start[cell], end = A.acell_start[cell + 1];
+            int beg = A.acell_start[cell], end = A.acell_start[cell_last + 1];
             // candidate pj at list slot ks
             // the FP32 distance in explicitly rounded operations: the
             // in-cutoff mark below decides an entry's list segment, so every
