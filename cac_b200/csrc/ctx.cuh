@@ -234,6 +234,7 @@ struct Ctx {
   DBuf<int> acell_atoms;         // [na] atom ids sorted by cell
   DBuf<double4> acell_pos;       // [na] wrapped positions sorted by cell, w = bitcast(id)
   DBuf<float4> acell_pos32;      // [na] the same as floats, w = bitcast(int id)
+  DBuf<int> acell_of;            // [na] cell of each sorted atom
   DBuf<int> ecell_start, ecell_elems;
   DBuf<int> cell_key, cell_key2, idx_tmp;
   DBuf<int> atom_work, atom_nwork;   // atoms with element sites in reach (rebuild work list)

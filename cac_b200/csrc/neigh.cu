@@ -283,12 +283,13 @@ __global__ void k_cell_start(const int *skey, int n, int ncell, int *start) {
   start[c] = lo;
 }
 
-__global__ void k_gather_pos(const double4 *xs, const int *sidx, int n, double4 *out, float4 *out32,
-                             int *atom_slot) {
+__global__ void k_gather_pos(const double4 *xs, const int *sidx, const int *skey, int n, double4 *out,
+                             float4 *out32, int *atom_slot, int *slot_cell) {
   int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= n) return;
   int i = sidx[k];
   atom_slot[i] = k;
+  slot_cell[k] = skey[k];
   double4 p = xs[i];
   out32[k] = make_float4((float)p.x, (float)p.y, (float)p.z, __int_as_float(i));
   p.w = __longlong_as_double((long long)i);
@@ -305,6 +306,7 @@ struct BuildArgs {
   const int *acell_start;
   const double4 *acell_pos;
   const float4 *acell_pos32;  // wrapped positions as floats, w = atom index bits
+  const int *acell_of;        // [na] cell of each sorted atom (list slot)
   const int *ecell_start;
   const unsigned char *ecell_near;   // single systems: element cell has an element in its 27-cell block (else null)
   const unsigned char *acell_near;   // single systems: atom cell has an atom in its 27-cell block (else null)
@@ -797,13 +799,21 @@ __device__ __forceinline__ void finish_counts(const BuildArgs &A, int i, int nin
   }
 }
 
-// Atoms, atom neighbours: one block (one warp) per cell of the atom grid
-// (cell >= cutneigh); the lanes are the cell's
-// atoms and walk the 27 surrounding cells together, so every candidate is one
-// broadcast load shared by the warp.  A conservative FP32 distance test (from
-// a float copy of the wrapped positions) decides all but the candidates near
-// the cutoff, which take the exact FP64 test.  The image of a candidate cell
-// relative to each lane's atom is fixed per cell.
+// Atoms, atom neighbours: one block (one warp) per chunk of 32 consecutive
+// sorted atoms (list slots).  Cells (>= cutneigh) are sorted x fastest, so a
+// chunk lies in one row of cells, or in two at a row's end (then the warp
+// takes the two parts in turn).  For each of the 9 rows around the part's
+// row the lanes walk together the cells from one left of the part's first
+// cell to one right of its last, as at most three runs of consecutive cells
+// under one image (the left and right wraps and the middle), so every
+// candidate is one broadcast load shared by the warp and all 32 lanes hold
+// an atom.  A lane meets the cells of its own 27-cell block in the order a
+// walk of that block alone would take (ascending x in each row) and the
+// others only beyond its reach, so its list is the same entry for entry.
+// A conservative FP32 distance test (from a float copy of the wrapped
+// positions) decides all but the candidates near the cutoff, which take the
+// exact FP64 test.  The image of a run relative to each lane's atom is fixed
+// per run.
 //
 // Full-list entries are written in their final form (the candidate's sorted
 // position is its list slot) and staged per lane in two 32-row rings in
@@ -815,168 +825,166 @@ __device__ __forceinline__ void finish_counts(const BuildArgs &A, int i, int nin
 // at the end.
 constexpr int STAGE_ROWS = 32;
 template <class RP>
-__device__ __forceinline__ void build_atoms_cell(BuildArgs A, RP P, const int home) {
+__device__ __forceinline__ void build_atoms_chunk(BuildArgs A, RP P, const int chunk) {
   const int lane = threadIdx.x & 31;
   const float fcut2 = (float)A.cutforcesq;
   __shared__ int st_in[STAGE_ROWS][32], st_out[STAGE_ROWS][32];   // front / back segment rings
-  {
-    const int hbeg = A.acell_start[home], hend = A.acell_start[home + 1];
-    if (hbeg == hend) return;
-    const Rep R = P.acell(home);
-    const int local = home - R.abase;
+  const int h = chunk * 32 + lane;
+  const bool mine = h < A.na;
+  const int key = mine ? A.acell_of[h] : -1;
+  Query q;
+  float wx = 0.f, wy = 0.f, wz = 0.f;
+  if (mine) {
+    make_query(A, P, (int)__double_as_longlong(A.acell_pos[h].w), q);
+    q.slot = h;
+    float4 w = A.acell_pos32[h];
+    wx = w.x;
+    wy = w.y;
+    wz = w.z;
+  }
+  // the chunk's parts, one row of cells each, lowest lanes first
+  unsigned todo = __ballot_sync(0xffffffffu, mine);
+  while (todo) {
+    const int lkey = __shfl_sync(0xffffffffu, key, __ffs(todo) - 1);
+    const Rep R = P.acell(lkey);
     const int nc0 = R.ag.nc[0], nc1 = R.ag.nc[1], nc2 = R.ag.nc[2];
-    const int hx = local % nc0, hy = (local / nc0) % nc1, hz = local / (nc0 * nc1);
+    const int row = (lkey - R.abase) / nc0;   // cz * nc1 + cy of the part
+    const int hx = key - R.abase - row * nc0;
+    const bool active = mine && ((todo >> lane) & 1u) && hx >= 0 && hx < nc0;
+    todo &= ~__ballot_sync(0xffffffffu, active);
+    const int hy = row % nc1, hz = row / nc1;
+    // unwrapped x range of the candidate cells
+    const int xlo = __reduce_min_sync(0xffffffffu, active ? hx : 0x7fffffff) - 1;
+    const int xhi = __reduce_max_sync(0xffffffffu, active ? hx : -1) + 1;
     // FP32 screen: beyond cutneigh + margin never a neighbour, within
     // cutneigh - margin always one; only the band between takes the FP64 test
     const float pre = (float)A.cutneigh + R.fmargin, sure = (float)A.cutneigh - R.fmargin;
     const float pre2 = pre * pre, sure2 = sure * sure;
-    for (int base = hbeg; base < hend; base += 32) {
-      const int h = base + lane;
-      const bool active = h < hend;
-      Query q;
-      int nin = 0, nout = 0, nh = 0;
-      int fin = 0, fout = 0;   // this lane's entries of each segment already written
-      float wx = 0.f, wy = 0.f, wz = 0.f;
-      if (active) {
-        make_query(A, P, (int)__double_as_longlong(A.acell_pos[h].w), q);
-        q.slot = h;
-        float4 w = A.acell_pos32[h];
-        wx = w.x;
-        wy = w.y;
-        wz = w.z;
-      }
-      // entry = (neighbour's list slot << IMG_BITS) | image code
-      auto stage = [&](int val, bool incut) {
-        if (incut) st_in[nin++ & (STAGE_ROWS - 1)][lane] = val;
-        else st_out[nout++ & (STAGE_ROWS - 1)][lane] = val;
-      };
-      // every lane writes its staged entries, row by row: front segment
-      // entries [fin, nin) to rows fin.., back segment entries [fout, nout)
-      // to rows cap-1-fout down
-      auto flush = [&]() {
-        int lo = __reduce_min_sync(0xffffffffu, active ? fin : 0x7fffffff);
-        int hi = __reduce_max_sync(0xffffffffu, active ? nin : 0);
-        for (int k = lo; k < hi; k++)
-          if (active && k >= fin && k < nin && k < A.cap)
-            A.nbr_full[(size_t)k * A.nsi + q.slot] = st_in[k & (STAGE_ROWS - 1)][lane];
-        lo = __reduce_min_sync(0xffffffffu, active ? fout : 0x7fffffff);
-        hi = __reduce_max_sync(0xffffffffu, active ? nout : 0);
-        for (int k = lo; k < hi; k++)
-          if (active && k >= fout && k < nout && k < A.cap)
-            A.nbr_full[(size_t)(A.cap - 1 - k) * A.nsi + q.slot] = st_out[k & (STAGE_ROWS - 1)][lane];
-        fin = nin;
-        fout = nout;
-      };
-      for (int oz = -1; oz <= 1; oz++) {
-        int cz, Wz;
-        wrap_cell(hz + oz, nc2, cz, Wz);
-        for (int oy = -1; oy <= 1; oy++) {
-          int cy, Wy;
-          wrap_cell(hy + oy, nc1, cy, Wy);
-          // the row's three cells in runs of consecutive cells under one
-          // image (one run away from the box's x faces): the cells are
-          // consecutive in sorted order, so a run is one candidate range,
-          // visited in the same order as cell by cell
-          int first = 0, last = -2, Wx = 0;
-          for (int ox = -1; ox <= 2; ox++) {
-            int cx = 0, wx_ = 0;
-            if (ox <= 1) wrap_cell(hx + ox, nc0, cx, wx_);
-            const int next = R.abase + (cz * nc1 + cy) * nc0 + cx;
-            if (ox <= 1 && wx_ == Wx && next == last + 1) {
-              last = next;
-              continue;
-            }
-            const int cell = first, cell_last = last;
-            first = last = next;
-            const int Wrun = Wx;
-            Wx = wx_;
-            if (ox == -1) continue;
-            int W[3] = {Wrun, Wy, Wz};
-            const float sx = (float)(Wrun * R.b.L[0]), sy = (float)(Wy * R.b.L[1]), sz = (float)(Wz * R.b.L[2]);
-            // this run's image relative to the lane's atom
-            const int s0 = Wrun - q.ti[0], s1 = Wy - q.ti[1], s2 = Wz - q.ti[2];
-            const bool zero = (s0 == 0 && s1 == 0 && s2 == 0);
-            const bool far = s0 < -1 || s0 > 1 || s1 < -1 || s1 > 1 || s2 < -1 || s2 > 1;
-            const int code = far ? 0 : img_code(s0, s1, s2);
-            int beg = A.acell_start[cell], end = A.acell_start[cell_last + 1];
-            // candidate pj at list slot ks
-            // the FP32 distance in explicitly rounded operations: the
-            // in-cutoff mark below decides an entry's list segment, so every
-            // kernel that builds these lists (grid and SM-local forms) must
-            // round it the same way, whatever the compiler would contract
-            auto consider = [&](const float4 &pj, int ks) {
-              const float ex = __fsub_rn(wx, __fadd_rn(pj.x, sx));
-              const float ey = __fsub_rn(wy, __fadd_rn(pj.y, sy));
-              const float ez = __fsub_rn(wz, __fadd_rn(pj.z, sz));
-              const float r2 = __fmaf_rn(ez, ez, __fmaf_rn(ey, ey, __fmul_rn(ex, ex)));
-              if (r2 > pre2) return;
-              const int j = __float_as_int(pj.w);
-              if (r2 < sure2 && !A.want_half) {
-                if (zero && j == q.i) return;
-                if (far) {
-                  atomicExch(&A.overflow[2], 1);
-                  return;
-                }
-                stage((ks << IMG_BITS) | code, r2 < fcut2);
-              } else {
-                try_atom(A, q, j, W, nh, [&](int, int c) {
-                  stage((ks << IMG_BITS) | (c & (IN_CUT - 1)), (c & IN_CUT) != 0);
-                });
+    int nin = 0, nout = 0, nh = 0;
+    int fin = 0, fout = 0;   // this lane's entries of each segment already written
+    // entry = (neighbour's list slot << IMG_BITS) | image code
+    auto stage = [&](int val, bool incut) {
+      if (incut) st_in[nin++ & (STAGE_ROWS - 1)][lane] = val;
+      else st_out[nout++ & (STAGE_ROWS - 1)][lane] = val;
+    };
+    // every lane writes its staged entries, row by row: front segment
+    // entries [fin, nin) to rows fin.., back segment entries [fout, nout)
+    // to rows cap-1-fout down
+    auto flush = [&]() {
+      int lo = __reduce_min_sync(0xffffffffu, active ? fin : 0x7fffffff);
+      int hi = __reduce_max_sync(0xffffffffu, active ? nin : 0);
+      for (int k = lo; k < hi; k++)
+        if (active && k >= fin && k < nin && k < A.cap)
+          A.nbr_full[(size_t)k * A.nsi + q.slot] = st_in[k & (STAGE_ROWS - 1)][lane];
+      lo = __reduce_min_sync(0xffffffffu, active ? fout : 0x7fffffff);
+      hi = __reduce_max_sync(0xffffffffu, active ? nout : 0);
+      for (int k = lo; k < hi; k++)
+        if (active && k >= fout && k < nout && k < A.cap)
+          A.nbr_full[(size_t)(A.cap - 1 - k) * A.nsi + q.slot] = st_out[k & (STAGE_ROWS - 1)][lane];
+      fin = nin;
+      fout = nout;
+    };
+    for (int oz = -1; oz <= 1; oz++) {
+      int cz, Wz;
+      wrap_cell(hz + oz, nc2, cz, Wz);
+      for (int oy = -1; oy <= 1; oy++) {
+        int cy, Wy;
+        wrap_cell(hy + oy, nc1, cy, Wy);
+        const int rowbase = R.abase + (cz * nc1 + cy) * nc0;
+        // runs: unwrapped x in [xlo, -1] (the cell nc0 - 1 one image left),
+        // [0, nc0 - 1], [nc0, xhi] (the cell 0 one image right)
+        for (int run = -1; run <= 1; run++) {
+          const int u0 = run < 0 ? xlo : (run == 0 ? max(xlo, 0) : max(xlo, nc0));
+          const int u1 = run < 0 ? min(xhi, -1) : (run == 0 ? min(xhi, nc0 - 1) : xhi);
+          if (u0 > u1) continue;
+          const int Wx = run;
+          int W[3] = {Wx, Wy, Wz};
+          const float sx = (float)(Wx * R.b.L[0]), sy = (float)(Wy * R.b.L[1]), sz = (float)(Wz * R.b.L[2]);
+          // this run's image relative to the lane's atom
+          const int s0 = Wx - q.ti[0], s1 = Wy - q.ti[1], s2 = Wz - q.ti[2];
+          const bool zero = (s0 == 0 && s1 == 0 && s2 == 0);
+          const bool far = s0 < -1 || s0 > 1 || s1 < -1 || s1 > 1 || s2 < -1 || s2 > 1;
+          const int code = far ? 0 : img_code(s0, s1, s2);
+          const int beg = A.acell_start[rowbase + u0 - Wx * nc0], end = A.acell_start[rowbase + u1 - Wx * nc0 + 1];
+          // candidate pj at list slot ks
+          // the FP32 distance in explicitly rounded operations: the
+          // in-cutoff mark below decides an entry's list segment, so every
+          // kernel that builds these lists (grid and SM-local forms) must
+          // round it the same way, whatever the compiler would contract
+          auto consider = [&](const float4 &pj, int ks) {
+            const float ex = __fsub_rn(wx, __fadd_rn(pj.x, sx));
+            const float ey = __fsub_rn(wy, __fadd_rn(pj.y, sy));
+            const float ez = __fsub_rn(wz, __fadd_rn(pj.z, sz));
+            const float r2 = __fmaf_rn(ez, ez, __fmaf_rn(ey, ey, __fmul_rn(ex, ex)));
+            if (r2 > pre2) return;
+            const int j = __float_as_int(pj.w);
+            if (r2 < sure2 && !A.want_half) {
+              if (zero && j == q.i) return;
+              if (far) {
+                atomicExch(&A.overflow[2], 1);
+                return;
               }
-            };
-            // candidates four at a time: the four broadcast loads are in
-            // flight together instead of one load's latency per candidate
-            int k = beg;
-            for (; k + 4 <= end; k += 4) {
-              const float4 p0 = A.acell_pos32[k], p1 = A.acell_pos32[k + 1];
-              const float4 p2 = A.acell_pos32[k + 2], p3 = A.acell_pos32[k + 3];
-              // room for four more entries in every lane's rings
-              if (__any_sync(0xffffffffu, active && (nin - fin > STAGE_ROWS - 4 || nout - fout > STAGE_ROWS - 4)))
-                flush();
-              if (active) {
-                consider(p0, k);
-                consider(p1, k + 1);
-                consider(p2, k + 2);
-                consider(p3, k + 3);
-              }
+              stage((ks << IMG_BITS) | code, r2 < fcut2);
+            } else {
+              try_atom(A, q, j, W, nh, [&](int, int c) {
+                stage((ks << IMG_BITS) | (c & (IN_CUT - 1)), (c & IN_CUT) != 0);
+              });
             }
-            for (; k < end; k++) {
-              const float4 pj = A.acell_pos32[k];
-              if (__any_sync(0xffffffffu, active && (nin - fin >= STAGE_ROWS || nout - fout >= STAGE_ROWS)))
-                flush();
-              if (active) consider(pj, k);
+          };
+          // candidates four at a time: the four broadcast loads are in
+          // flight together instead of one load's latency per candidate
+          int k = beg;
+          for (; k + 4 <= end; k += 4) {
+            const float4 p0 = A.acell_pos32[k], p1 = A.acell_pos32[k + 1];
+            const float4 p2 = A.acell_pos32[k + 2], p3 = A.acell_pos32[k + 3];
+            // room for four more entries in every lane's rings
+            if (__any_sync(0xffffffffu, active && (nin - fin > STAGE_ROWS - 4 || nout - fout > STAGE_ROWS - 4)))
+              flush();
+            if (active) {
+              consider(p0, k);
+              consider(p1, k + 1);
+              consider(p2, k + 2);
+              consider(p3, k + 3);
             }
+          }
+          for (; k < end; k++) {
+            const float4 pj = A.acell_pos32[k];
+            if (__any_sync(0xffffffffu, active && (nin - fin >= STAGE_ROWS || nout - fout >= STAGE_ROWS)))
+              flush();
+            if (active) consider(pj, k);
           }
         }
       }
-      flush();
-      if (active) {
-        A.site_from[q.slot] = make_int2(nin, nout);
-        finish_counts(A, q.slot, nin, nout, nh);
-      }
+    }
+    flush();
+    if (active) {
+      A.site_from[q.slot] = make_int2(nin, nout);
+      finish_counts(A, q.slot, nin, nout, nh);
     }
   }
 }
 
-// The single-system form as the compiler allocates it (92 registers with the
-// candidate loads four at a time); the batch form capped at 64 registers (a
-// few bytes spilled) so that 32 warps are resident per SM: 10 % faster on a
-// 64-replica batch, where the same cap slowed the single-system form.
-__global__ void __launch_bounds__(32) k_build_atoms(BuildArgs A, OneRep P) { build_atoms_cell(A, P, blockIdx.x); }
+// The single-system forms as the compiler allocates them (96 registers with
+// the candidate loads four at a time, 118 in the persistent form: a cap at 20
+// resident warps per SM, 88 registers, was 10 % slower); the batch form
+// capped at 64 registers (a few bytes spilled) so that 32 warps are resident
+// per SM: 10 % faster on a 64-replica batch, where the same cap slowed the
+// single-system form.
+__global__ void __launch_bounds__(32) k_build_atoms(BuildArgs A, OneRep P) { build_atoms_chunk(A, P, blockIdx.x); }
 __global__ void __launch_bounds__(32, 32) k_build_atoms(BuildArgs A, ManyRep P) {
-  build_atoms_cell(A, P, blockIdx.x);
+  build_atoms_chunk(A, P, blockIdx.x);
 }
 
-// Single systems: persistent warps taking the cells in SM-local runs (one
-// cell per run, sm_run in device.cuh), so that the warps resident on one SM
+// Single systems: persistent warps taking the chunks in SM-local runs (one
+// chunk per run, sm_run in device.cuh), so that the warps resident on one SM
 // walk neighbouring cells and share their candidates in L1.  The same lists.
-__global__ void __launch_bounds__(32) k_build_atoms_sm(BuildArgs A, OneRep P, int ncell, int *cnt, int nsm) {
+__global__ void __launch_bounds__(32) k_build_atoms_sm(BuildArgs A, OneRep P, int nchunk, int *cnt, int nsm) {
   __shared__ int v;
   if (threadIdx.x == 0) v = sm_id() % nsm;
   for (;;) {
-    const int home = sm_run(cnt, nsm, ncell, v);
-    if (home < 0) return;
-    build_atoms_cell(A, P, home);
+    const int chunk = sm_run(cnt, nsm, nchunk, v);
+    if (chunk < 0) return;
+    build_atoms_chunk(A, P, chunk);
   }
 }
 
@@ -1326,6 +1334,7 @@ void neigh_plan(Ctx &c, bool want_half) {
   c.acell_start.reserve(c.agrid.ncell + 1);
   c.acell_pos.reserve(std::max(c.na, 1));
   c.acell_pos32.reserve(std::max(c.na, 1));
+  c.acell_of.reserve(std::max(c.na, 1));
   c.ecell_start.reserve(c.egrid.ncell + 1);
   c.ecell_near.reserve(c.egrid.ncell + 1);
   c.acell_near.reserve(c.agrid.ncell + 1);
@@ -1443,8 +1452,9 @@ void neigh_build_async(Ctx &c, bool want_half) {
         if (c.nrep == 1 && c.ne)
           k_ecell_near<<<nblk(c.agrid.ncell, 256), 256, 0, c.stream>>>(c.acell_start.p, c.rep_h[0].ag,
                                                                        c.acell_near.p);
-        k_gather_pos<<<nblk(c.na, 256), 256, 0, c.stream>>>(c.xs.p, c.slot_atom.p, c.na, c.acell_pos.p,
-                                                            c.acell_pos32.p, c.atom_slot.p);
+        k_gather_pos<<<nblk(c.na, 256), 256, 0, c.stream>>>(c.xs.p, c.slot_atom.p, c.cell_key2.p, c.na,
+                                                            c.acell_pos.p, c.acell_pos32.p, c.atom_slot.p,
+                                                            c.acell_of.p);
       } else {
         CACB200_CUDA(cudaMemsetAsync(c.acell_start.p, 0, sizeof(int) * (c.agrid.ncell + 1), c.stream));
       }
@@ -1471,6 +1481,7 @@ void neigh_build_async(Ctx &c, bool want_half) {
     A.acell_start = c.acell_start.p;
     A.acell_pos = c.acell_pos.p;
     A.acell_pos32 = c.acell_pos32.p;
+    A.acell_of = c.acell_of.p;
     A.ecell_start = c.ecell_start.p;
     A.ecell_near = (c.nrep == 1 && c.ne) ? c.ecell_near.p : nullptr;
     A.acell_near = (c.nrep == 1 && c.na && c.ne) ? c.acell_near.p : nullptr;
@@ -1532,13 +1543,13 @@ void neigh_build_async(Ctx &c, bool want_half) {
             return b > 0 ? b : 1;
           }();
           CACB200_CUDA(cudaMemsetAsync(c.sm_counter.p, 0, sizeof(int) * c.num_sms, c.stream));
-          k_build_atoms_sm<<<per_sm * c.num_sms, 32, 0, c.stream>>>(A, P, c.agrid.ncell, c.sm_counter.p,
+          k_build_atoms_sm<<<per_sm * c.num_sms, 32, 0, c.stream>>>(A, P, (c.na + 31) / 32, c.sm_counter.p,
                                                                    c.num_sms);
         } else {
-          k_build_atoms<<<c.agrid.ncell, 32, 0, c.stream>>>(A, P);
+          k_build_atoms<<<(c.na + 31) / 32, 32, 0, c.stream>>>(A, P);
         }
       } else {
-        k_build_atoms<<<c.agrid.ncell, 32, 0, c.stream>>>(A, P);
+        k_build_atoms<<<(c.na + 31) / 32, 32, 0, c.stream>>>(A, P);
       }
     }
     if (c.na && c.ne) {

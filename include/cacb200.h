@@ -433,8 +433,8 @@ int cacb200_pair_blocks(cacb200_ctx *ctx, int *rho_threads, int *force_threads);
  * 8,192, below 32,768, larger) by timing the force pass when the capacity
  * plan changes; results do not depend on it (each slot's arithmetic is that
  * of the grid launch).  Single systems run the atom-list build, and in the
- * FP64 form the force-only EAM passes, over SM-local runs instead: the cells
- * or list slots are cut into runs (one cell; 128 slots) and each
+ * FP64 form the force-only EAM passes, over SM-local runs instead: the
+ * sorted atoms or list slots are cut into runs (32 atoms; 128 slots) and each
  * multiprocessor owns a contiguous range of runs, so the blocks resident on
  * one multiprocessor share their neighbours' data in its L1; a block whose
  * own range is exhausted takes runs from another range (same lists and
