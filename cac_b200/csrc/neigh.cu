@@ -11,8 +11,9 @@
 //
 // Candidates come from two periodic cell grids instead of the reference's
 // bin/stencil/sub-element walk: atoms from a grid of cell >= cutneigh with a
-// 3x3x3 stencil (atoms: one block per cell, the cell's atoms as lanes sharing
-// broadcast candidate loads; Gauss points: one thread each), element sites
+// 3x3x3 stencil (atoms: one block per chunk of 32 cell-sorted atoms, the
+// atoms as lanes sharing broadcast candidate loads; Gauss points: one warp
+// each, the lanes over the candidates), element sites
 // from a grid over element centres of cell >= cutneigh + (centre-to-node
 // radius + affine deviation), and for each candidate element only the lattice
 // sites whose affine position can lie within cutneigh (a box in lattice-index
