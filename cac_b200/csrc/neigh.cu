@@ -900,7 +900,10 @@ __device__ __forceinline__ void build_atoms_chunk(BuildArgs A, RP P, const int c
           if (u0 > u1) continue;
           const int Wx = run;
           int W[3] = {Wx, Wy, Wz};
-          const float sx = (float)(Wx * R.b.L[0]), sy = (float)(Wy * R.b.L[1]), sz = (float)(Wz * R.b.L[2]);
+          // the lane's position less the run's image shift (once per run)
+          const float hx_ = __fsub_rn(wx, (float)(Wx * R.b.L[0]));
+          const float hy_ = __fsub_rn(wy, (float)(Wy * R.b.L[1]));
+          const float hz_ = __fsub_rn(wz, (float)(Wz * R.b.L[2]));
           // this run's image relative to the lane's atom
           const int s0 = Wx - q.ti[0], s1 = Wy - q.ti[1], s2 = Wz - q.ti[2];
           const bool zero = (s0 == 0 && s1 == 0 && s2 == 0);
@@ -913,9 +916,9 @@ __device__ __forceinline__ void build_atoms_chunk(BuildArgs A, RP P, const int c
           // kernel that builds these lists (grid and SM-local forms) must
           // round it the same way, whatever the compiler would contract
           auto consider = [&](const float4 &pj, int ks) {
-            const float ex = __fsub_rn(wx, __fadd_rn(pj.x, sx));
-            const float ey = __fsub_rn(wy, __fadd_rn(pj.y, sy));
-            const float ez = __fsub_rn(wz, __fadd_rn(pj.z, sz));
+            const float ex = __fsub_rn(hx_, pj.x);
+            const float ey = __fsub_rn(hy_, pj.y);
+            const float ez = __fsub_rn(hz_, pj.z);
             const float r2 = __fmaf_rn(ez, ez, __fmaf_rn(ey, ey, __fmul_rn(ex, ex)));
             if (r2 > pre2) return;
             const int j = __float_as_int(pj.w);
@@ -1290,9 +1293,10 @@ void neigh_plan(Ctx &c, bool want_half) {
       R.reach_budget = std::max(ereach, std::min(std::max(1.2 * ereach, ereach + 2.0), room));
     }
     setup_grids(c, R, c.rep_ne[r] > 0);
-    // FP32 separations of wrapped positions and shifted candidates (|x| <=
-    // X = |lo| + |hi| + L) carry at most ~4 ulp(X) of rounding per distance;
-    // 16 ulp of 2X bounds it with room to spare
+    // FP32 separations (a wrapped position less an image shift, |.| <= 2X
+    // with X = |lo| + |hi| + L, minus a wrapped candidate) carry at most ~4
+    // ulp(X) of rounding per distance; 16 ulp of 2X bounds it with room to
+    // spare
     {
       double X = 1.0;
       for (int d = 0; d < 3; d++) X = std::max(X, std::fabs(R.b.lo[d]) + std::fabs(R.b.hi[d]) + R.b.L[d]);
