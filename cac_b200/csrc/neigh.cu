@@ -901,9 +901,9 @@ __device__ __forceinline__ void build_atoms_chunk(BuildArgs A, RP P, const int c
           const int Wx = run;
           int W[3] = {Wx, Wy, Wz};
           // the lane's position less the run's image shift (once per run)
-          const float hx_ = __fsub_rn(wx, (float)(Wx * R.b.L[0]));
-          const float hy_ = __fsub_rn(wy, (float)(Wy * R.b.L[1]));
-          const float hz_ = __fsub_rn(wz, (float)(Wz * R.b.L[2]));
+          const float rx = __fsub_rn(wx, (float)(Wx * R.b.L[0]));
+          const float ry = __fsub_rn(wy, (float)(Wy * R.b.L[1]));
+          const float rz = __fsub_rn(wz, (float)(Wz * R.b.L[2]));
           // this run's image relative to the lane's atom
           const int s0 = Wx - q.ti[0], s1 = Wy - q.ti[1], s2 = Wz - q.ti[2];
           const bool zero = (s0 == 0 && s1 == 0 && s2 == 0);
@@ -916,9 +916,9 @@ __device__ __forceinline__ void build_atoms_chunk(BuildArgs A, RP P, const int c
           // kernel that builds these lists (grid and SM-local forms) must
           // round it the same way, whatever the compiler would contract
           auto consider = [&](const float4 &pj, int ks) {
-            const float ex = __fsub_rn(hx_, pj.x);
-            const float ey = __fsub_rn(hy_, pj.y);
-            const float ez = __fsub_rn(hz_, pj.z);
+            const float ex = __fsub_rn(rx, pj.x);
+            const float ey = __fsub_rn(ry, pj.y);
+            const float ez = __fsub_rn(rz, pj.z);
             const float r2 = __fmaf_rn(ez, ez, __fmaf_rn(ey, ey, __fmul_rn(ex, ex)));
             if (r2 > pre2) return;
             const int j = __float_as_int(pj.w);
