@@ -91,3 +91,60 @@ def test_named_workload_sizes():
     ]:
         assert 162 * nx * ny * la == na
         assert 2 * 2 * nx * ny * le == ne
+
+
+def _noalloc_call(lib, device, n, natoms, nelements, out, eatom=None, enode=None):
+    ip = ctypes.POINTER(ctypes.c_int)
+    return lib.cacb200_replica_energy_noalloc(
+        device, eatom, enode, n, natoms.ctypes.data_as(ip) if natoms is not None else None,
+        nelements.ctypes.data_as(ip) if nelements is not None else None, 1.0,
+        out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)) if out is not None else None, None)
+
+
+def test_noalloc_rejects_bad_arguments_before_any_device_work():
+    """cacb200_replica_energy_noalloc checks its arguments before it touches a
+    device (so these run without one): each bad argument returns
+    CACB200_EINVAL with its own message in cacb200_noalloc_last_error."""
+    lib = api.load()
+    lib.cacb200_noalloc_last_error.restype = ctypes.c_char_p
+    ok = np.zeros(4, dtype=np.int32)
+    out = np.zeros(4)
+    cases = [
+        ((0, 4097, np.zeros(4097, np.int32), np.zeros(4097, np.int32), np.zeros(4097)), b"4097 replicas"),
+        ((0, 0, ok, ok, out), b"0 replicas"),
+        ((0, 4, None, ok, out), b"null count or output array"),
+        ((0, 4, ok, ok, None), b"null count or output array"),
+        ((-1, 4, ok, ok, out), b"device index out of range"),
+        ((0, 4, np.array([1, -2, 0, 0], np.int32), ok, out), b"negative site count"),
+        ((0, 4, np.array([1, 0, 0, 0], np.int32), ok, out), b"null per-site energy array"),
+    ]
+    for args, msg in cases:
+        assert _noalloc_call(lib, *args) == -1, msg
+        assert msg in lib.cacb200_noalloc_last_error(), (msg, lib.cacb200_noalloc_last_error())
+
+
+def test_noalloc_error_message_is_per_thread():
+    """The last-error message belongs to the calling thread: two threads that
+    fail differently each read back their own message."""
+    import threading
+    lib = api.load()
+    lib.cacb200_noalloc_last_error.restype = ctypes.c_char_p
+    got = {}
+
+    def worker(name, n, natoms, gate_in, gate_out):
+        out = np.zeros(max(n, 1))
+        zeros = np.zeros(max(n, 1), np.int32)
+        _noalloc_call(lib, 0, n, natoms if natoms is not None else zeros, zeros, out)
+        gate_out.set()
+        gate_in.wait(10)
+        got[name] = lib.cacb200_noalloc_last_error()
+
+    a_done, b_done = threading.Event(), threading.Event()
+    ta = threading.Thread(target=worker, args=("a", 5000, None, b_done, a_done))
+    tb = threading.Thread(target=worker, args=("b", 2, np.array([3, -1], np.int32), a_done, b_done))
+    ta.start()
+    tb.start()
+    ta.join(20)
+    tb.join(20)
+    assert b"5000 replicas" in got["a"]
+    assert b"negative site count" in got["b"]
